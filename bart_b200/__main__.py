@@ -1,0 +1,108 @@
+"""Command line mirror of ``bart nufft`` and ``bart pics -t`` with .cfl I/O.
+
+  python -m bart_b200 nufft [-a] [-x X:Y:Z] [-P] [-r|-t] traj input output
+  python -m bart_b200 pics -l2 -r lambda [-i iter] -t traj [-w scale] [-S]
+                           [--no-toeplitz] ksp sens output
+
+Options follow src/nufft.c:75-101 and src/pics.c:137-199; options of the
+reference that are not built here are rejected with an error.
+"""
+
+from __future__ import annotations
+
+import argparse
+import sys
+
+import numpy as np
+
+from .cfl import readcfl, writecfl
+from .nufft import NufftConf, nufft_create2
+from .pics import Pics, PicsConf
+
+
+def _vec3(s: str):
+    v = [int(x) for x in s.split(":")]
+    if len(v) != 3:
+        raise argparse.ArgumentTypeError("expected x:y:z")
+    return v
+
+
+def estimate_im_dims(traj: np.ndarray):
+    """estimate_im_dims (src/noncart/traj.c): 2 * ceil(max |k|) per axis, 1 if all zero."""
+    t = np.abs(np.real(traj.reshape(3, -1, order="F")))
+    dims = []
+    for ax in range(3):
+        m = float(t[ax].max()) if t.shape[1] else 0.0
+        dims.append(1 if m == 0.0 else int(2 * np.ceil(m)))
+    return dims
+
+
+def main_nufft(argv) -> int:
+    ap = argparse.ArgumentParser(prog="nufft")
+    ap.add_argument("-a", dest="adjoint", action="store_true")
+    ap.add_argument("-i", dest="inverse", action="store_true")
+    ap.add_argument("-x", dest="dims", type=_vec3)
+    ap.add_argument("-t", dest="toeplitz", action="store_true")
+    ap.add_argument("-r", dest="no_toeplitz", action="store_true")
+    ap.add_argument("-P", dest="periodic", action="store_true")
+    ap.add_argument("-g", dest="gpu", action="store_true")
+    ap.add_argument("traj")
+    ap.add_argument("input")
+    ap.add_argument("output")
+    a = ap.parse_args(argv)
+    if a.inverse:
+        sys.stderr.write("nufft -i is not built yet (use pics)\n")
+        return 1
+    traj = readcfl(a.traj)
+    tdims = list(traj.shape)
+    conf = NufftConf(toeplitz=False, periodic=a.periodic)   # no PSF unless inverse (src/nufft.c:121-122)
+    inp = readcfl(a.input)
+    if a.adjoint:
+        kd = list(inp.shape)
+        cd = (a.dims or estimate_im_dims(traj)) + kd[3:]
+        op = nufft_create2(kd, cd, tdims, traj, conf=conf)
+        writecfl(a.output, op.adjoint(inp).reshape(cd, order="F"))
+    else:
+        cd = list(inp.shape)
+        kd = [1, tdims[1], tdims[2]] + cd[3:]
+        op = nufft_create2(kd, cd, tdims, traj, conf=conf)
+        writecfl(a.output, op.forward(inp).reshape(kd, order="F"))
+    op.free()
+    return 0
+
+
+def main_pics(argv) -> int:
+    ap = argparse.ArgumentParser(prog="pics")
+    ap.add_argument("-l", dest="reg", choices=["2"], help="only -l2 (CG) is built")
+    ap.add_argument("-r", dest="lam", type=float, default=0.0)
+    ap.add_argument("-i", dest="iters", type=int, default=30)
+    ap.add_argument("-t", dest="traj", required=True)
+    ap.add_argument("-w", dest="scaling", type=float, default=0.0)
+    ap.add_argument("-S", dest="rescale", action="store_true")
+    ap.add_argument("-g", dest="gpu", action="store_true")
+    ap.add_argument("--no-toeplitz", dest="no_toeplitz", action="store_true")
+    ap.add_argument("ksp")
+    ap.add_argument("sens")
+    ap.add_argument("output")
+    a = ap.parse_args(argv)
+    traj = readcfl(a.traj)
+    ksp = readcfl(a.ksp)
+    sens = readcfl(a.sens)
+    conf = PicsConf(lam=a.lam, maxiter=a.iters, scaling=a.scaling, rescale=a.rescale, toeplitz=not a.no_toeplitz)
+    p = Pics(traj, sens, ksp_dims=list(ksp.shape), conf=conf)
+    img = p.run(ksp)
+    p.free()
+    writecfl(a.output, img.reshape(list(sens.shape[:3]), order="F"))
+    return 0
+
+
+def main(argv=None) -> int:
+    argv = list(sys.argv[1:] if argv is None else argv)
+    if not argv or argv[0] not in ("nufft", "pics"):
+        sys.stderr.write(__doc__)
+        return 2
+    return {"nufft": main_nufft, "pics": main_pics}[argv[0]](argv[1:])
+
+
+if __name__ == "__main__":
+    sys.exit(main())

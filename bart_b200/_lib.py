@@ -1,0 +1,87 @@
+"""ctypes binding of the C ABI in include/bnufft.h (``bart_b200/lib/libbnufft.so``).
+
+The library is the product; this module only declares its signatures. There
+is no fallback: if the shared library or a CUDA device is missing, loading or
+the first call fails loudly.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libbnufft.so")
+
+c_long_p = ctypes.POINTER(ctypes.c_long)
+
+
+class NufftConfC(ctypes.Structure):
+    _fields_ = [("toeplitz", ctypes.c_int), ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int),
+                ("os", ctypes.c_float), ("width", ctypes.c_float)]
+
+
+class PicsConfC(ctypes.Structure):
+    _fields_ = [("lambda_", ctypes.c_float), ("maxiter", ctypes.c_int), ("tol", ctypes.c_float),
+                ("scaling", ctypes.c_float), ("rescale", ctypes.c_int), ("toeplitz", ctypes.c_int),
+                ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libbnufft.so once and declare the prototypes."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"bnufft shared library not found at {path}; run `python -m bart_b200.build`")
+    lib = ctypes.CDLL(path)
+    vp, i, cl = ctypes.c_void_p, ctypes.c_int, c_long_p
+
+    def sig(name, res, *args):
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = list(args)
+
+    sig("bnufft_conf_defaults", None, ctypes.POINTER(NufftConfC))
+    sig("bnufft_create2", i, ctypes.POINTER(vp), i, cl, cl, cl, vp, cl, vp, cl, vp, ctypes.POINTER(NufftConfC), vp)
+    sig("bnufft_apply_forward", i, vp, vp, vp, vp)
+    sig("bnufft_apply_adjoint", i, vp, vp, vp, vp)
+    sig("bnufft_apply_normal", i, vp, vp, vp, vp)
+    sig("bnufft_get_psf_dims", i, vp, i, cl)
+    sig("bnufft_get_psf", i, vp, i, cl, vp, vp)
+    sig("bnufft_update_traj", i, vp, i, cl, vp, vp)
+    sig("bnufft_free", None, vp)
+    sig("bnufft_pics_conf_defaults", None, ctypes.POINTER(PicsConfC))
+    sig("bnufft_pics_create", i, ctypes.POINTER(vp), i, cl, cl, cl, vp, vp, ctypes.POINTER(PicsConfC), vp)
+    sig("bnufft_pics_run", i, vp, vp, vp, vp)
+    sig("bnufft_pics_normal", i, vp, vp, vp, vp)
+    sig("bnufft_pics_stats", i, vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+        ctypes.POINTER(ctypes.c_float), vp)
+    sig("bnufft_pics_free", None, vp)
+    sig("bnufft_last_error", ctypes.c_char_p)
+    sig("bnufft_launch_count", ctypes.c_long)
+    sig("bnufft_prof_start", i, ctypes.c_char_p)
+    sig("bnufft_prof_stop", i, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_long))
+    _lib = lib
+    return lib
+
+
+class BnufftError(RuntimeError):
+    """A bnufft call returned a non-zero status."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"bnufft error {status}: {msg}")
+        self.status = status
+
+
+def check(status: int) -> None:
+    if status != 0:
+        msg = load().bnufft_last_error().decode(errors="replace")
+        raise BnufftError(status, msg)
+
+
+def dims_array(dims) -> ctypes.Array:
+    return (ctypes.c_long * len(dims))(*[int(d) for d in dims])

@@ -1,0 +1,1384 @@
+// bnufft host side: plans, pass scheduling and the C ABI (include/bnufft.h).
+//
+// Built for sm_100a only. Every entry point returns a status code instead of
+// aborting (the reference aborts through error(), src/misc/misc.c:95).
+#include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
+
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/bnufft.h"
+#include "nufft_kernels.cuh"
+#include "cg_kernels.cuh"
+
+using namespace bn;
+
+// ----------------------------------------------------------------------------
+// errors and launch accounting
+// ----------------------------------------------------------------------------
+
+static thread_local std::string g_err;
+static std::atomic<long> g_launches{0};
+
+static int fail(int code, const char* fmt, ...)
+{
+	char buf[512];
+	va_list ap;
+	va_start(ap, fmt);
+	vsnprintf(buf, sizeof buf, fmt, ap);
+	va_end(ap);
+	g_err = buf;
+	return code;
+}
+
+#define CUDA_TRY(call) do { cudaError_t e_ = (call); if (cudaSuccess != e_) \
+	return fail(BNUFFT_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); } while (0)
+
+#define LAUNCHED() do { g_launches.fetch_add(1, std::memory_order_relaxed); \
+	cudaError_t e_ = cudaGetLastError(); if (cudaSuccess != e_) \
+	return fail(BNUFFT_ERR_CUDA, "%s:%d launch: %s", __FILE__, __LINE__, cudaGetErrorString(e_)); } while (0)
+
+#define TRY(call) do { int s_ = (call); if (BNUFFT_OK != s_) return s_; } while (0)
+
+// Optional timing of one kernel class (bnufft_prof_start): a pair of CUDA
+// events on the launching stream around every launch of that class.
+static std::mutex g_prof_mutex;
+static std::string g_prof_target;
+static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
+
+static cudaEvent_t prof_begin(const char* kind, cudaStream_t st)
+{
+	std::lock_guard<std::mutex> lock(g_prof_mutex);
+
+	if (g_prof_target.empty() || (g_prof_target != kind))
+		return nullptr;
+
+	cudaEvent_t a, b;
+	cudaEventCreate(&a);
+	cudaEventCreate(&b);
+	cudaEventRecord(a, st);
+	g_prof_events.push_back({ a, b });
+	return b;
+}
+
+static void prof_end(cudaEvent_t e, cudaStream_t st)
+{
+	if (e)
+		cudaEventRecord(e, st);
+}
+
+static cudaStream_t S(void* stream) { return (cudaStream_t)stream; }
+
+// ----------------------------------------------------------------------------
+// Kaiser-Bessel table, roll-off and twiddles (host, float64)
+// ----------------------------------------------------------------------------
+
+// I0 from its power series (float64-accurate for |x| <= 30)
+static double bessel_i0(double x)
+{
+	x = fabs(x);
+	double q = 0.25 * x * x, term = 1., sum = 1.;
+
+	for (int k = 1; k < 500; k++) {
+
+		term *= q / ((double)k * (double)k);
+		sum += term;
+
+		if (term < 1e-18 * sum)
+			break;
+	}
+
+	return sum;
+}
+
+// calc_beta (src/noncart/grid.c:516-519); width/os is a float division
+static double calc_beta(float os, float width)
+{
+	double wos = (double)(width / os);
+	return M_PI * sqrt(pow(wos * ((double)os - 0.5), 2.) - 0.8);
+}
+
+// beta of the KB table: rolloff_correction() initialises it with a float beta
+static double kernel_beta(float os, float width) { return (double)(float)calc_beta(os, width); }
+
+// kb_precompute (src/noncart/grid.c:86-97)
+static void kb_precompute(double beta, int n, float* table)
+{
+	double i0b = bessel_i0(beta);
+
+	for (int i = 0; i < n + 1; i++) {
+
+		double x = (double)i / (double)(n - 1) / 2.;
+		table[i] = (fabs(x) >= 0.5) ? 0.f : (float)(bessel_i0(beta * sqrt(1. - pow(2. * x, 2.))) / i0b);
+	}
+}
+
+// ftkb / rolloff / pos (src/noncart/grid.c:100-117, 522-533)
+static double ftkb(double beta, double x, double i0b)
+{
+	double a = beta * beta - pow(M_PI * x, 2.);
+
+	if (0. == a)
+		return 1. / i0b;
+
+	return (a > 0) ? (sinh(sqrt(a)) / sqrt(a)) / i0b : (sin(sqrt(-a)) / sqrt(-a)) / i0b;
+}
+
+static double rolloff_axis(int d, int i, float os, float width, double beta, double i0b)
+{
+	if (1 == d)
+		return 1.;
+
+	int od = (int)(os * d);
+	int oi = i + (od / 2 - d / 2);
+	float p = ((float)oi - (float)(od / 2)) / (float)od;
+
+	return 1. / ftkb(beta, (double)p * (double)width, i0b) / (double)width;
+}
+
+// ----------------------------------------------------------------------------
+// per-device constant tables
+// ----------------------------------------------------------------------------
+
+struct DevTables {
+
+	std::map<int, float2*> twiddle;		// L -> exp(-2 pi i m / L)
+	std::map<std::pair<float, float>, float*> kb;	// (os, width) -> table
+};
+
+static std::mutex g_tab_mutex;
+static std::map<int, DevTables> g_tabs;
+
+static int get_twiddles(int L, const float2** out)
+{
+	int dev;
+	CUDA_TRY(cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lock(g_tab_mutex);
+	auto& t = g_tabs[dev].twiddle;
+	auto it = t.find(L);
+
+	if (it != t.end()) {
+
+		*out = it->second;
+		return BNUFFT_OK;
+	}
+
+	std::vector<float2> h(L);
+
+	for (int m = 0; m < L; m++) {
+
+		double a = -2. * M_PI * (double)m / (double)L;
+		h[m] = make_float2((float)cos(a), (float)sin(a));
+	}
+
+	float2* d = nullptr;
+	CUDA_TRY(cudaMalloc(&d, sizeof(float2) * L));
+	CUDA_TRY(cudaMemcpy(d, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
+	t[L] = d;
+	*out = d;
+	return BNUFFT_OK;
+}
+
+static int get_kb_table(float os, float width, const float** out)
+{
+	int dev;
+	CUDA_TRY(cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lock(g_tab_mutex);
+	auto& t = g_tabs[dev].kb;
+	auto key = std::make_pair(os, width);
+	auto it = t.find(key);
+
+	if (it != t.end()) {
+
+		*out = it->second;
+		return BNUFFT_OK;
+	}
+
+	std::vector<float> h(KB_TABLE_N + 1);
+	kb_precompute(kernel_beta(os, width), KB_TABLE_N, h.data());
+	float* d = nullptr;
+	CUDA_TRY(cudaMalloc(&d, sizeof(float) * (KB_TABLE_N + 1)));
+	CUDA_TRY(cudaMemcpy(d, h.data(), sizeof(float) * (KB_TABLE_N + 1), cudaMemcpyHostToDevice));
+	t[key] = d;
+	*out = d;
+	return BNUFFT_OK;
+}
+
+// ----------------------------------------------------------------------------
+// FFT pass launchers
+// ----------------------------------------------------------------------------
+
+static bool supported_len(int L) { return (L >= 16) && (L <= 2048) && (0 == (L & (L - 1))); }
+
+static size_t pass_smem(int L, int B) { return sizeof(float2) * (size_t)L * (size_t)(smem_stride(B) + 1); }
+
+// sequences per block: B * L / 8 threads (<= 1024), at most 16 sequences,
+// fewer when the launch would have too few blocks
+static int choose_B(int L, long nseq, int max_b = 16)
+{
+	int B = std::min(max_b, 8192 / L);
+
+	while ((B > 1) && ((nseq + B - 1) / B < 2 * 148))
+		B /= 2;
+
+	return std::max(B, 1);
+}
+
+template <typename K>
+static int prep_kernel(K kernel, size_t smem)
+{
+	if (smem > 48 * 1024)
+		CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+
+	return BNUFFT_OK;
+}
+
+template <int L>
+static int launch_rows_fwd_L(const float2* img, const float2* maps, const float* ax, const float* ayz,
+		int X, long YZ, long R, float2* out, cudaStream_t st)
+{
+	const float2* tw;
+	TRY(get_twiddles(L, &tw));
+	int B = choose_B(L, R);
+	size_t smem = pass_smem(L, B);
+	TRY(prep_kernel(k_rows_fwd<L>, smem));
+	cudaEvent_t pe = prof_begin("rows_fwd", st);
+	k_rows_fwd<L><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(img, maps, ax, ayz, X, YZ, R, B, out, tw);
+	prof_end(pe, st);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+template <int L, int MODE>
+static int launch_cols_L(const float2* in, long ies, long ios, int n_in, int wrap_in,
+		float2* out, long oes, long oos, int n_out, int wrap_out, int W, long O,
+		const float2* psf, long pes, long pmod, long pos, cudaStream_t st)
+{
+	const float2* tw;
+	TRY(get_twiddles(L, &tw));
+	int B = choose_B(L, (long)W * O);
+
+	while ((B > 1) && (B > W))
+		B /= 2;
+
+	size_t smem = pass_smem(L, B);
+	TRY(prep_kernel(k_cols<L, MODE>, smem));
+
+	if (O > 65535)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "column pass with %ld outer sequences", O);
+
+	dim3 grid((unsigned)((W + B - 1) / B), (unsigned)O);
+	cudaEvent_t pe = prof_begin((2 == MODE) ? "cols_toeplitz" : ((1 == MODE) ? "cols_inv" : "cols_fwd"), st);
+	k_cols<L, MODE><<<grid, B * L / 8, smem, st>>>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out,
+			W, B, psf, pes, pmod, pos, tw);
+	prof_end(pe, st);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+template <int L>
+static int launch_rows_inv_L(const float2* in, const float2* maps, const float* ax, const float* ayz,
+		int X, long YZ, int C, int cpg, float2* out, cudaStream_t st)
+{
+	const float2* tw;
+	TRY(get_twiddles(L, &tw));
+	int groups = (C + cpg - 1) / cpg;
+	int B = choose_B(L, YZ * groups);
+	size_t smem = pass_smem(L, B);
+	TRY(prep_kernel(k_rows_inv<L>, smem));
+	dim3 grid((unsigned)((YZ + B - 1) / B), (unsigned)groups);
+	cudaEvent_t pe = prof_begin("rows_inv", st);
+	k_rows_inv<L><<<grid, B * L / 8, smem, st>>>(in, maps, ax, ayz, X, YZ, C, cpg, B, out, tw);
+	prof_end(pe, st);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+#define DISPATCH_L(L, CALL) \
+	switch (L) { \
+	case 16: { constexpr int LL = 16; return CALL; } \
+	case 32: { constexpr int LL = 32; return CALL; } \
+	case 64: { constexpr int LL = 64; return CALL; } \
+	case 128: { constexpr int LL = 128; return CALL; } \
+	case 256: { constexpr int LL = 256; return CALL; } \
+	case 512: { constexpr int LL = 512; return CALL; } \
+	case 1024: { constexpr int LL = 1024; return CALL; } \
+	case 2048: { constexpr int LL = 2048; return CALL; } \
+	default: return fail(BNUFFT_ERR_UNSUPPORTED, "FFT length %d (powers of two 16..2048 are built)", L); }
+
+static int rows_fwd(int L, const float2* img, const float2* maps, const float* ax, const float* ayz,
+		int X, long YZ, long R, float2* out, cudaStream_t st)
+{
+	DISPATCH_L(L, (launch_rows_fwd_L<LL>(img, maps, ax, ayz, X, YZ, R, out, st)));
+}
+
+static int cols(int L, int mode, const float2* in, long ies, long ios, int n_in, int wrap_in,
+		float2* out, long oes, long oos, int n_out, int wrap_out, int W, long O,
+		const float2* psf, long pes, long pmod, long pos, cudaStream_t st)
+{
+	if (0 == mode)
+		DISPATCH_L(L, (launch_cols_L<LL, 0>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, st)))
+	else if (1 == mode)
+		DISPATCH_L(L, (launch_cols_L<LL, 1>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, st)))
+	else
+		DISPATCH_L(L, (launch_cols_L<LL, 2>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, st)))
+}
+
+static int rows_inv(int L, const float2* in, const float2* maps, const float* ax, const float* ayz,
+		int X, long YZ, int C, int cpg, float2* out, cudaStream_t st)
+{
+	DISPATCH_L(L, (launch_rows_inv_L<LL>(in, maps, ax, ayz, X, YZ, C, cpg, out, st)));
+}
+
+static unsigned vec_blocks(long n, int threads = RED_THREADS, int maxb = 4 * 148)
+{
+	long b = (n + threads - 1) / threads;
+	return (unsigned)std::max(1L, std::min<long>(b, maxb));
+}
+
+// ----------------------------------------------------------------------------
+// geometry and the three NUFFT operators on device buffers
+// ----------------------------------------------------------------------------
+
+struct Geom {
+
+	int N[3];	// image dims
+	int G[3];	// oversampled dims (2N or 1)
+	int nd;		// number of transformed (non-singleton) axes
+	long npix;	// N0*N1*N2
+	long gsz;	// G0*G1*G2
+	long M;		// samples
+	float os, width;
+	int periodic;
+};
+
+struct Work {
+
+	float2* grid = nullptr;	// [gsz * C]
+	float2* t1 = nullptr;	// [G0 * N1 * N2 * C]
+	float2* t2 = nullptr;	// 3D: [G0 * G1 * N2 * C]
+	long cap = 0;		// channels the buffers hold
+};
+
+struct OpCtx {
+
+	Geom g;
+	const float4* traj;	// [M]
+	const float* kb;
+	float* ax = nullptr;	// [N0] roll-off along x
+	float* ayz = nullptr;	// [N1*N2] roll-off along y,z with 1/sqrt(npix)
+	Work w;
+};
+
+static GridGeom grid_geom(const Geom& g)
+{
+	GridGeom gg;
+
+	for (int i = 0; i < 3; i++) {
+
+		gg.N[i] = g.N[i];
+		gg.G[i] = g.G[i];
+	}
+
+	gg.gsz = g.gsz;
+	gg.hw = g.width / 2.f;
+	gg.periodic = g.periodic;
+	return gg;
+}
+
+static int alloc_work(Work& w, const Geom& g, long C, cudaStream_t st)
+{
+	if (w.cap >= C)
+		return BNUFFT_OK;
+
+	if (w.grid) cudaFreeAsync(w.grid, st);
+	if (w.t1) cudaFreeAsync(w.t1, st);
+	if (w.t2) cudaFreeAsync(w.t2, st);
+	w = Work{};
+
+	CUDA_TRY(cudaMallocAsync(&w.grid, sizeof(float2) * g.gsz * C, st));
+	CUDA_TRY(cudaMallocAsync(&w.t1, sizeof(float2) * (long)g.G[0] * g.N[1] * g.N[2] * C, st));
+
+	if (g.G[2] > 1)
+		CUDA_TRY(cudaMallocAsync(&w.t2, sizeof(float2) * (long)g.G[0] * g.G[1] * g.N[2] * C, st));
+
+	w.cap = C;
+	return BNUFFT_OK;
+}
+
+static void free_work(Work& w, cudaStream_t st)
+{
+	if (w.grid) cudaFreeAsync(w.grid, st);
+	if (w.t1) cudaFreeAsync(w.t1, st);
+	if (w.t2) cudaFreeAsync(w.t2, st);
+	w = Work{};
+}
+
+static int init_geom(Geom& g, const long dims3[3], long M, float os, float width, int periodic)
+{
+	g.nd = 0;
+	g.npix = 1;
+	g.gsz = 1;
+
+	for (int i = 0; i < 3; i++) {
+
+		g.N[i] = (int)dims3[i];
+		g.G[i] = (dims3[i] > 1) ? (int)(2 * dims3[i]) : 1;
+
+		if (dims3[i] > 1) {
+
+			g.nd++;
+
+			if (0 != dims3[i] % 2)
+				return fail(BNUFFT_ERR_UNSUPPORTED, "odd image size %ld (even sizes are built)", dims3[i]);
+
+			if (!supported_len(g.G[i]))
+				return fail(BNUFFT_ERR_UNSUPPORTED, "grid length %d on axis %d", g.G[i], i);
+		}
+
+		g.npix *= g.N[i];
+		g.gsz *= g.G[i];
+	}
+
+	if (dims3[0] <= 1)
+		return fail(BNUFFT_ERR_ARG, "dim 0 must be transformed");
+
+	if ((dims3[2] > 1) && (dims3[1] <= 1))
+		return fail(BNUFFT_ERR_UNSUPPORTED, "3D with singleton y");
+
+	g.M = M;
+	g.os = os;
+	g.width = width;
+	g.periodic = periodic;
+	return BNUFFT_OK;
+}
+
+static int init_rolloff(OpCtx& op, cudaStream_t st)
+{
+	const Geom& g = op.g;
+	double beta = kernel_beta(g.os, g.width);
+	double i0b = bessel_i0(beta);
+	std::vector<float> ax(g.N[0]);
+	std::vector<float> ayz((size_t)g.N[1] * g.N[2]);
+	double sc = 1. / sqrt((double)g.npix);
+
+	for (int x = 0; x < g.N[0]; x++)
+		ax[x] = (float)rolloff_axis(g.N[0], x, g.os, g.width, beta, i0b);
+
+	for (int z = 0; z < g.N[2]; z++)
+		for (int y = 0; y < g.N[1]; y++)
+			ayz[y + (size_t)g.N[1] * z] = (float)(rolloff_axis(g.N[1], y, g.os, g.width, beta, i0b)
+						* rolloff_axis(g.N[2], z, g.os, g.width, beta, i0b) * sc);
+
+	CUDA_TRY(cudaMallocAsync(&op.ax, sizeof(float) * ax.size(), st));
+	CUDA_TRY(cudaMallocAsync(&op.ayz, sizeof(float) * ayz.size(), st));
+	CUDA_TRY(cudaMemcpyAsync(op.ax, ax.data(), sizeof(float) * ax.size(), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(op.ayz, ayz.data(), sizeof(float) * ayz.size(), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaStreamSynchronize(st));	// host vectors go out of scope
+	return BNUFFT_OK;
+}
+
+// image [N0, N1*N2, C] (maps: image [N0, N1*N2] times maps [.., C]) -> grid
+static int op_spectrum(OpCtx& op, const float2* img, const float2* maps, bool apod, long C, float2* grid, cudaStream_t st)
+{
+	const Geom& g = op.g;
+	long YZ = (long)g.N[1] * g.N[2];
+
+	TRY(rows_fwd(g.G[0], img, maps, apod ? op.ax : nullptr, op.ayz, g.N[0], YZ, YZ * C, op.w.t1, st));
+
+	if (1 == g.G[1]) {	// 1D: row pass is the whole transform
+
+		CUDA_TRY(cudaMemcpyAsync(grid, op.w.t1, sizeof(float2) * g.gsz * C, cudaMemcpyDeviceToDevice, st));
+		return BNUFFT_OK;
+	}
+
+	if (1 == g.G[2]) {
+
+		return cols(g.G[1], 0, op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1,
+				grid, g.G[0], (long)g.G[0] * g.G[1], g.G[1], 0, g.G[0], C, nullptr, 0, 1, 0, st);
+	}
+
+	TRY(cols(g.G[1], 0, op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1,
+			op.w.t2, g.G[0], (long)g.G[0] * g.G[1], g.G[1], 0, g.G[0], (long)g.N[2] * C, nullptr, 0, 1, 0, st));
+
+	long plane = (long)g.G[0] * g.G[1];
+
+	return cols(g.G[2], 0, op.w.t2, plane, plane * g.N[2], g.N[2], 1,
+			grid, plane, plane * g.G[2], g.G[2], 0, (int)plane, C, nullptr, 0, 1, 0, st);
+}
+
+// grid -> image (maps: sum over coils into `groups` partials of [N0, N1*N2])
+static int op_spectrum_adjoint(OpCtx& op, const float2* grid, const float2* maps, bool apod, long C, int cpg,
+		float2* out, cudaStream_t st)
+{
+	const Geom& g = op.g;
+	long YZ = (long)g.N[1] * g.N[2];
+	const float2* rows_in = grid;
+
+	if (g.G[1] > 1) {
+
+		if (1 == g.G[2]) {
+
+			TRY(cols(g.G[1], 1, grid, g.G[0], (long)g.G[0] * g.G[1], g.G[1], 0,
+					op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1, g.G[0], C, nullptr, 0, 1, 0, st));
+
+		} else {
+
+			long plane = (long)g.G[0] * g.G[1];
+
+			TRY(cols(g.G[2], 1, grid, plane, plane * g.G[2], g.G[2], 0,
+					op.w.t2, plane, plane * g.N[2], g.N[2], 1, (int)plane, C, nullptr, 0, 1, 0, st));
+			TRY(cols(g.G[1], 1, op.w.t2, g.G[0], plane, g.G[1], 0,
+					op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1, g.G[0], (long)g.N[2] * C, nullptr, 0, 1, 0, st));
+		}
+
+		rows_in = op.w.t1;
+	}
+
+	return rows_inv(g.G[0], rows_in, maps, apod ? op.ax : nullptr, op.ayz, g.N[0], YZ, (int)C, maps ? cpg : 1, out, st);
+}
+
+static int degrid(OpCtx& op, const float2* grid, long C, float2* ksp, cudaStream_t st)
+{
+	int cpc = (int)std::min<long>(C, 8);
+	dim3 blocks((unsigned)((op.g.M + 127) / 128), (unsigned)((C + cpc - 1) / cpc));
+	cudaEvent_t pe = prof_begin("degrid", st);
+	k_degrid<<<blocks, 128, 0, st>>>(op.traj, op.g.M, grid_geom(op.g), (int)C, cpc, grid, ksp, op.kb);
+	prof_end(pe, st);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+static int grid_adj(OpCtx& op, const float2* ksp, long C, float2* grid, cudaStream_t st)
+{
+	CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(float2) * op.g.gsz * C, st));
+	int cpc = (int)std::min<long>(C, 8);
+	dim3 blocks((unsigned)((op.g.M + 127) / 128), (unsigned)((C + cpc - 1) / cpc));
+	cudaEvent_t pe = prof_begin("grid", st);
+	k_grid_atomic<<<blocks, 128, 0, st>>>(op.traj, op.g.M, grid_geom(op.g), (int)C, cpc, ksp, grid, op.kb);
+	prof_end(pe, st);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+// forward NUFFT: cim [npix, C] -> ksp [M, C] (maps: single image times maps)
+static int op_forward(OpCtx& op, const float2* cim, const float2* maps, long C, float2* ksp, cudaStream_t st)
+{
+	TRY(alloc_work(op.w, op.g, C, st));
+	TRY(op_spectrum(op, cim, maps, true, C, op.w.grid, st));
+	return degrid(op, op.w.grid, C, ksp, st);
+}
+
+// adjoint NUFFT: ksp [M, C] -> cim [npix, C] (maps: partial coil sums)
+static int op_adjoint(OpCtx& op, const float2* ksp, const float2* maps, long C, int cpg, float2* out, cudaStream_t st)
+{
+	TRY(alloc_work(op.w, op.g, C, st));
+	TRY(grid_adj(op, ksp, C, op.w.grid, st));
+	return op_spectrum_adjoint(op, op.w.grid, maps, true, C, cpg, out, st);
+}
+
+// Toeplitz normal: E^H (psf . E x) per coil (maps: partial coil sums)
+static int op_toeplitz(OpCtx& op, const float2* psf, const float2* x, const float2* maps, long C, int cpg,
+		float2* out, cudaStream_t st)
+{
+	const Geom& g = op.g;
+	long YZ = (long)g.N[1] * g.N[2];
+	TRY(alloc_work(op.w, g, C, st));
+	TRY(rows_fwd(g.G[0], x, maps, nullptr, nullptr, g.N[0], YZ, YZ * C, op.w.t1, st));
+
+	if (1 == g.G[1]) {
+
+		return fail(BNUFFT_ERR_UNSUPPORTED, "Toeplitz normal for 1D");
+
+	} else if (1 == g.G[2]) {
+
+		TRY(cols(g.G[1], 2, op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1,
+				op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1, g.G[0], C, psf, g.G[0], 1, 0, st));
+
+	} else {
+
+		long plane = (long)g.G[0] * g.G[1];
+
+		TRY(cols(g.G[1], 0, op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1,
+				op.w.t2, g.G[0], plane, g.G[1], 0, g.G[0], (long)g.N[2] * C, nullptr, 0, 1, 0, st));
+		TRY(cols(g.G[2], 2, op.w.t2, plane, plane * g.N[2], g.N[2], 1,
+				op.w.t2, plane, plane * g.N[2], g.N[2], 1, (int)plane, C, psf, plane, 1, 0, st));
+		TRY(cols(g.G[1], 1, op.w.t2, g.G[0], plane, g.G[1], 0,
+				op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1, g.G[0], (long)g.N[2] * C, nullptr, 0, 1, 0, st));
+	}
+
+	return rows_inv(g.G[0], op.w.t1, maps, nullptr, nullptr, g.N[0], YZ, (int)C, maps ? cpg : 1, out, st);
+}
+
+// PSF on the 2N grid in DFT order, scaled by 1/npix so that the Toeplitz
+// product needs no further normalisation (compute_psf2, src/noncart/nufft.c:727-776):
+// psft = adjoint NUFFT of ones with trajectory 2*traj onto the 2N image,
+// periodic gridding; psf = fftuc(psft) / npix.
+static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, float2** psf_out, cudaStream_t st)
+{
+	OpCtx in;
+	long d2[3] = { g.G[0], g.G[1], g.G[2] };
+	TRY(init_geom(in.g, d2, g.M, g.os, g.width, 1));
+
+	float4* t2 = nullptr;
+	float2* ones = nullptr;
+	float2* psft = nullptr;
+	float2* psf = nullptr;
+	CUDA_TRY(cudaMallocAsync(&t2, sizeof(float4) * g.M, st));
+	CUDA_TRY(cudaMallocAsync(&ones, sizeof(float2) * g.M, st));
+	CUDA_TRY(cudaMallocAsync(&psft, sizeof(float2) * in.g.npix, st));
+	CUDA_TRY(cudaMallocAsync(&psf, sizeof(float2) * g.gsz, st));
+
+	k_traj_convert<<<vec_blocks(g.M), RED_THREADS, 0, st>>>(t2, traj_c, g.M, 2.f);
+	LAUNCHED();
+	k_fill<<<vec_blocks(g.M), RED_THREADS, 0, st>>>(ones, g.M, make_float2(1.f, 0.f));
+	LAUNCHED();
+
+	in.traj = t2;
+	in.kb = kb;
+	TRY(init_rolloff(in, st));
+	TRY(op_adjoint(in, ones, nullptr, 1, 1, psft, st));
+
+	// full 2N-point transform of the 2N image: input centred (ifftshift), output in DFT order
+	OpCtx full;
+	full.g = g;
+	full.traj = nullptr;
+	full.kb = kb;
+
+	for (int i = 0; i < 3; i++)
+		full.g.N[i] = g.G[i];	// input length L on every axis
+
+	full.g.npix = g.gsz;
+	TRY(alloc_work(full.w, full.g, 1, st));
+
+	long YZ = (long)g.G[1] * g.G[2];
+	TRY(rows_fwd(g.G[0], psft, nullptr, nullptr, nullptr, g.G[0], YZ, YZ, full.w.t1, st));
+
+	if (1 == g.G[2]) {
+
+		TRY(cols(g.G[1], 0, full.w.t1, g.G[0], (long)g.G[0] * g.G[1], g.G[1], 1,
+				psf, g.G[0], (long)g.G[0] * g.G[1], g.G[1], 0, g.G[0], 1, nullptr, 0, 1, 0, st));
+
+	} else {
+
+		long plane = (long)g.G[0] * g.G[1];
+
+		TRY(cols(g.G[1], 0, full.w.t1, g.G[0], plane, g.G[1], 1,
+				full.w.t2, g.G[0], plane, g.G[1], 0, g.G[0], (long)g.G[2], nullptr, 0, 1, 0, st));
+		TRY(cols(g.G[2], 0, full.w.t2, plane, plane * g.G[2], g.G[2], 1,
+				psf, plane, plane * g.G[2], g.G[2], 0, (int)plane, 1, nullptr, 0, 1, 0, st));
+	}
+
+	double sc = 1. / sqrt((double)g.gsz) / (double)g.npix;
+	k_scale<<<vec_blocks(g.gsz), RED_THREADS, 0, st>>>(psf, psf, g.gsz, (float)sc);
+	LAUNCHED();
+
+	free_work(full.w, st);
+	free_work(in.w, st);
+	cudaFreeAsync(in.ax, st);
+	cudaFreeAsync(in.ayz, st);
+	cudaFreeAsync(t2, st);
+	cudaFreeAsync(ones, st);
+	cudaFreeAsync(psft, st);
+
+	*psf_out = psf;
+	return BNUFFT_OK;
+}
+
+// ----------------------------------------------------------------------------
+// dims helpers
+// ----------------------------------------------------------------------------
+
+static long prod(int n, const long* d)
+{
+	long p = 1;
+
+	for (int i = 0; i < n; i++)
+		p *= d[i];
+
+	return p;
+}
+
+static bool on_device(const void* p)
+{
+	cudaPointerAttributes a;
+
+	if (cudaSuccess != cudaPointerGetAttributes(&a, p)) {
+
+		cudaGetLastError();
+		return false;
+	}
+
+	return (cudaMemoryTypeDevice == a.type) || (cudaMemoryTypeManaged == a.type);
+}
+
+// staging of host data through device buffers (the e2e path)
+struct Staged {
+
+	void* dev = nullptr;
+	bool owned = false;
+
+	~Staged() { if (owned && dev) cudaFree(dev); }
+};
+
+static int stage_in(Staged& s, const void* p, size_t bytes, cudaStream_t st)
+{
+	if (on_device(p)) {
+
+		s.dev = (void*)p;
+		return BNUFFT_OK;
+	}
+
+	CUDA_TRY(cudaMalloc(&s.dev, bytes));
+	s.owned = true;
+	CUDA_TRY(cudaMemcpyAsync(s.dev, p, bytes, cudaMemcpyHostToDevice, st));
+	return BNUFFT_OK;
+}
+
+static int stage_out_alloc(Staged& s, void* p, size_t bytes)
+{
+	if (on_device(p)) {
+
+		s.dev = p;
+		return BNUFFT_OK;
+	}
+
+	CUDA_TRY(cudaMalloc(&s.dev, bytes));
+	s.owned = true;
+	return BNUFFT_OK;
+}
+
+static int stage_out_copy(Staged& s, void* p, size_t bytes, cudaStream_t st)
+{
+	if (!s.owned)
+		return BNUFFT_OK;
+
+	CUDA_TRY(cudaMemcpyAsync(p, s.dev, bytes, cudaMemcpyDeviceToHost, st));
+	CUDA_TRY(cudaStreamSynchronize(st));
+	return BNUFFT_OK;
+}
+
+// ----------------------------------------------------------------------------
+// NUFFT plan (C ABI)
+// ----------------------------------------------------------------------------
+
+struct bnufft_plan_s {
+
+	int N;
+	std::vector<long> ksp_dims, cim_dims, trj_dims;
+	bnufft_conf conf;
+	long C;			// batch (product of cim dims >= 3)
+	OpCtx op;
+	float4* traj = nullptr;
+	float2* psf = nullptr;	// DFT order, includes 1/npix
+	cudaStream_t st0;
+};
+
+extern "C" void bnufft_conf_defaults(struct bnufft_conf* conf)
+{
+	conf->toeplitz = 1;
+	conf->periodic = 0;
+	conf->deterministic = 0;
+	conf->os = 2.f;
+	conf->width = 6.f;
+}
+
+static int check_conf(const bnufft_conf* conf)
+{
+	if (2.f != conf->os)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "oversampling %g (os = 2 is built; the reference chains other os)", conf->os);
+
+	if ((conf->width <= 0.f) || (conf->width > 8.f))
+		return fail(BNUFFT_ERR_UNSUPPORTED, "kernel width %g", conf->width);
+
+	if (conf->deterministic)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "deterministic gridding is not built yet");
+
+	return BNUFFT_OK;
+}
+
+static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
+{
+	Staged t;
+	TRY(stage_in(t, traj, sizeof(float2) * 3 * p->op.g.M, st));
+	k_traj_convert<<<vec_blocks(p->op.g.M), RED_THREADS, 0, st>>>(p->traj, (const float2*)t.dev, p->op.g.M, 1.f);
+	LAUNCHED();
+
+	if (p->conf.toeplitz) {
+
+		if (p->psf)
+			cudaFreeAsync(p->psf, st);
+
+		p->psf = nullptr;
+		TRY(compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, st));
+	}
+
+	if (t.owned)
+		CUDA_TRY(cudaStreamSynchronize(st));
+
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[], const long cim_dims[],
+		const long traj_dims[], const void* traj,
+		const long wgh_dims[], const void* weights,
+		const long bas_dims[], const void* basis,
+		const struct bnufft_conf* conf_in, void* stream)
+{
+	(void)wgh_dims;
+	(void)bas_dims;
+	*plan = nullptr;
+	cudaStream_t st = S(stream);
+
+	if ((N < 4) || (nullptr == traj))
+		return fail(BNUFFT_ERR_ARG, "need N >= 4 dims and a trajectory");
+
+	if (weights || basis)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "weights / basis are not built yet");
+
+	bnufft_conf conf;
+
+	if (conf_in)
+		conf = *conf_in;
+	else
+		bnufft_conf_defaults(&conf);
+
+	TRY(check_conf(&conf));
+
+	if (3 != traj_dims[0] || 1 != ksp_dims[0])
+		return fail(BNUFFT_ERR_ARG, "traj dims[0] must be 3 and ksp dims[0] 1");
+
+	if (ksp_dims[1] != traj_dims[1] || ksp_dims[2] != traj_dims[2])
+		return fail(BNUFFT_ERR_ARG, "k-space and trajectory sample dims differ");
+
+	for (int i = 3; i < N; i++) {
+
+		if (ksp_dims[i] != cim_dims[i])
+			return fail(BNUFFT_ERR_UNSUPPORTED, "ksp/cim dim %d differ (%ld, %ld)", i, ksp_dims[i], cim_dims[i]);
+
+		if (1 != traj_dims[i])
+			return fail(BNUFFT_ERR_UNSUPPORTED, "trajectory varying along dim %d", i);
+	}
+
+	auto p = new bnufft_plan_s();
+	p->N = N;
+	p->ksp_dims.assign(ksp_dims, ksp_dims + N);
+	p->cim_dims.assign(cim_dims, cim_dims + N);
+	p->trj_dims.assign(traj_dims, traj_dims + N);
+	p->conf = conf;
+	p->C = prod(N - 3, cim_dims + 3);
+	p->st0 = st;
+
+	long M = traj_dims[1] * traj_dims[2];
+	int s = init_geom(p->op.g, cim_dims, M, conf.os, conf.width, conf.periodic);
+
+	if (BNUFFT_OK == s)
+		s = get_kb_table(conf.os, conf.width, &p->op.kb);
+
+	if (BNUFFT_OK == s)
+		s = init_rolloff(p->op, st);
+
+	if ((BNUFFT_OK == s) && (cudaSuccess != cudaMallocAsync(&p->traj, sizeof(float4) * M, st)))
+		s = fail(BNUFFT_ERR_NOMEM, "trajectory buffer");
+
+	p->op.traj = p->traj;
+
+	if (BNUFFT_OK == s)
+		s = upload_traj(p, traj, st);
+
+	if (BNUFFT_OK != s) {
+
+		std::string msg = g_err;
+		bnufft_free(p);
+		g_err = msg;
+		return s;
+	}
+
+	*plan = p;
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_update_traj(bnufft_plan_t p, int N, const long traj_dims[], const void* traj, void* stream)
+{
+	if (!p || (N != p->N))
+		return fail(BNUFFT_ERR_ARG, "bad plan or dims");
+
+	for (int i = 0; i < N; i++)
+		if (traj_dims[i] != p->trj_dims[i])
+			return fail(BNUFFT_ERR_ARG, "trajectory dims changed (dim %d)", i);
+
+	return upload_traj(p, traj, S(stream));
+}
+
+extern "C" int bnufft_apply_forward(bnufft_plan_t p, void* dst, const void* src, void* stream)
+{
+	cudaStream_t st = S(stream);
+	size_t in_b = sizeof(float2) * p->op.g.npix * p->C;
+	size_t out_b = sizeof(float2) * p->op.g.M * p->C;
+	Staged i, o;
+	TRY(stage_in(i, src, in_b, st));
+	TRY(stage_out_alloc(o, dst, out_b));
+	TRY(op_forward(p->op, (const float2*)i.dev, nullptr, p->C, (float2*)o.dev, st));
+	return stage_out_copy(o, dst, out_b, st);
+}
+
+extern "C" int bnufft_apply_adjoint(bnufft_plan_t p, void* dst, const void* src, void* stream)
+{
+	cudaStream_t st = S(stream);
+	size_t in_b = sizeof(float2) * p->op.g.M * p->C;
+	size_t out_b = sizeof(float2) * p->op.g.npix * p->C;
+	Staged i, o;
+	TRY(stage_in(i, src, in_b, st));
+	TRY(stage_out_alloc(o, dst, out_b));
+	TRY(op_adjoint(p->op, (const float2*)i.dev, nullptr, p->C, 1, (float2*)o.dev, st));
+	return stage_out_copy(o, dst, out_b, st);
+}
+
+extern "C" int bnufft_apply_normal(bnufft_plan_t p, void* dst, const void* src, void* stream)
+{
+	cudaStream_t st = S(stream);
+	size_t b = sizeof(float2) * p->op.g.npix * p->C;
+	Staged i, o;
+	TRY(stage_in(i, src, b, st));
+	TRY(stage_out_alloc(o, dst, b));
+
+	if (p->psf) {
+
+		TRY(op_toeplitz(p->op, p->psf, (const float2*)i.dev, nullptr, p->C, 1, (float2*)o.dev, st));
+
+	} else {
+
+		float2* k = nullptr;
+		CUDA_TRY(cudaMallocAsync(&k, sizeof(float2) * p->op.g.M * p->C, st));
+		TRY(op_forward(p->op, (const float2*)i.dev, nullptr, p->C, k, st));
+		TRY(op_adjoint(p->op, k, nullptr, p->C, 1, (float2*)o.dev, st));
+		cudaFreeAsync(k, st);
+	}
+
+	return stage_out_copy(o, dst, b, st);
+}
+
+extern "C" int bnufft_get_psf_dims(bnufft_plan_t p, int ND, long psf_dims[])
+{
+	if (!p || !p->psf)
+		return fail(BNUFFT_ERR_ARG, "plan has no PSF");
+
+	if (ND != p->N + 1)
+		return fail(BNUFFT_ERR_ARG, "PSF has N+1 = %d dims", p->N + 1);
+
+	for (int i = 0; i < ND; i++)
+		psf_dims[i] = 1;
+
+	long sub = 1;
+
+	for (int i = 0; i < 3; i++) {
+
+		psf_dims[i] = p->op.g.N[i];
+		sub *= (p->op.g.G[i] > 1) ? 2 : 1;
+	}
+
+	psf_dims[p->N] = sub;
+	return BNUFFT_OK;
+}
+
+// decomposed layout of the reference: psf[w + N*..., s] = P_centred[2w + s] * npix
+__global__ static void k_psf_decompose(float2* dst, const float2* psf, GridGeom g, float npix)
+{
+	long n = (long)g.N[0] * g.N[1] * g.N[2];
+	long tot = n * ((g.G[0] > 1 ? 2 : 1) * (g.G[1] > 1 ? 2 : 1) * (g.G[2] > 1 ? 2 : 1));
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (long)gridDim.x * blockDim.x) {
+
+		long pix = i % n;
+		long sidx = i / n;
+		int w[3] = { (int)(pix % g.N[0]), (int)((pix / g.N[0]) % g.N[1]), (int)(pix / ((long)g.N[0] * g.N[1])) };
+		long cell = 0;
+		long stride = 1;
+
+		for (int a = 0; a < 3; a++) {
+
+			int s = 0;
+
+			if (g.G[a] > 1) {
+
+				s = (int)(sidx & 1);
+				sidx >>= 1;
+			}
+
+			int j = (g.G[a] > 1) ? (2 * w[a] + s + g.N[a]) % g.G[a] : 0;
+			cell += j * stride;
+			stride *= g.G[a];
+		}
+
+		dst[i] = cscale(psf[cell], npix);
+	}
+}
+
+extern "C" int bnufft_get_psf(bnufft_plan_t p, int ND, const long psf_dims[], void* psf, void* stream)
+{
+	long d[32];
+
+	if (ND > 32)
+		return fail(BNUFFT_ERR_ARG, "too many dims");
+
+	TRY(bnufft_get_psf_dims(p, ND, d));
+
+	for (int i = 0; i < ND; i++)
+		if (d[i] != psf_dims[i])
+			return fail(BNUFFT_ERR_ARG, "PSF dim %d is %ld, not %ld", i, d[i], psf_dims[i]);
+
+	cudaStream_t st = S(stream);
+	size_t b = sizeof(float2) * p->op.g.gsz;
+	Staged o;
+	TRY(stage_out_alloc(o, psf, b));
+	k_psf_decompose<<<vec_blocks(p->op.g.gsz), RED_THREADS, 0, st>>>((float2*)o.dev, p->psf, grid_geom(p->op.g), (float)p->op.g.npix);
+	LAUNCHED();
+	return stage_out_copy(o, psf, b, st);
+}
+
+extern "C" void bnufft_free(bnufft_plan_t p)
+{
+	if (!p)
+		return;
+
+	cudaStream_t st = p->st0;
+	free_work(p->op.w, st);
+
+	if (p->op.ax) cudaFreeAsync(p->op.ax, st);
+	if (p->op.ayz) cudaFreeAsync(p->op.ayz, st);
+	if (p->traj) cudaFreeAsync(p->traj, st);
+	if (p->psf) cudaFreeAsync(p->psf, st);
+
+	cudaStreamSynchronize(st);
+	delete p;
+}
+
+// ----------------------------------------------------------------------------
+// CG-SENSE (C ABI)
+// ----------------------------------------------------------------------------
+
+struct bnufft_pics_s {
+
+	bnufft_plan_t nufft;
+	bnufft_pics_conf conf;
+	long C, npix, M;
+	int cpg, groups;
+	float2* sens = nullptr;		// [npix, C]
+	float2* part = nullptr;		// [npix, groups] coil-sum partials
+	float2 *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr, *b = nullptr;
+	float2* kbuf = nullptr;		// [M, C] (non-Toeplitz normal)
+	float* mag = nullptr;		// [npix] |adj|
+	float* mag_sorted = nullptr;
+	void* sort_tmp = nullptr;
+	size_t sort_tmp_bytes = 0;
+	double* pap_part = nullptr;
+	double* rs_part = nullptr;
+	int nparts;
+	CgScalars* scal = nullptr;
+};
+
+extern "C" void bnufft_pics_conf_defaults(struct bnufft_pics_conf* c)
+{
+	c->lambda = 0.f;
+	c->maxiter = 30;
+	c->tol = 0.f;
+	c->scaling = 0.f;
+	c->rescale = 0;
+	c->toeplitz = 1;
+	c->periodic = 0;
+	c->deterministic = 0;
+}
+
+// A^H A x (+ lam x), with optional per-block Re<x, out> partials
+static int sense_normal(bnufft_pics_s* ps, const float2* x, float2* out, float lam, double* dot_part,
+		const int* done, cudaStream_t st)
+{
+	OpCtx& op = ps->nufft->op;
+
+	if (ps->nufft->psf) {
+
+		TRY(op_toeplitz(op, ps->nufft->psf, x, ps->sens, ps->C, ps->cpg, ps->part, st));
+
+	} else {
+
+		TRY(op_forward(op, x, ps->sens, ps->C, ps->kbuf, st));
+		TRY(op_adjoint(op, ps->kbuf, ps->sens, ps->C, ps->cpg, ps->part, st));
+	}
+
+	k_combine<<<ps->nparts, RED_THREADS, 0, st>>>(out, ps->part, ps->groups, ps->npix, x, lam, dot_part, done);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims[], const long sens_dims[],
+		const long traj_dims[], const void* traj, const void* sens,
+		const struct bnufft_pics_conf* conf_in, void* stream)
+{
+	*out = nullptr;
+	cudaStream_t st = S(stream);
+	bnufft_pics_conf conf;
+
+	if (conf_in)
+		conf = *conf_in;
+	else
+		bnufft_pics_conf_defaults(&conf);
+
+	if (N < 5)
+		return fail(BNUFFT_ERR_ARG, "need N >= 5 dims");
+
+	for (int i = 4; i < N; i++)
+		if ((1 != ksp_dims[i]) || (1 != sens_dims[i]))
+			return fail(BNUFFT_ERR_UNSUPPORTED, "dim %d must be 1 (one set of maps, one image)", i);
+
+	if (ksp_dims[3] != sens_dims[3])
+		return fail(BNUFFT_ERR_ARG, "coil dims differ (%ld, %ld)", ksp_dims[3], sens_dims[3]);
+
+	if (conf.maxiter < 0)
+		return fail(BNUFFT_ERR_ARG, "maxiter < 0");
+
+	bnufft_conf nc;
+	bnufft_conf_defaults(&nc);
+	nc.toeplitz = conf.toeplitz;
+	nc.periodic = conf.periodic;
+	nc.deterministic = conf.deterministic;
+
+	auto ps = new bnufft_pics_s();
+	ps->conf = conf;
+	int s = bnufft_create2(&ps->nufft, N, ksp_dims, sens_dims, traj_dims, traj, nullptr, nullptr, nullptr, nullptr, &nc, stream);
+
+	if (BNUFFT_OK != s) {
+
+		delete ps;
+		return s;
+	}
+
+	ps->C = sens_dims[3];
+	ps->npix = ps->nufft->op.g.npix;
+	ps->M = ps->nufft->op.g.M;
+
+	// coil groups: enough blocks in the final row pass, few partials to combine
+	long YZ = (long)ps->nufft->op.g.N[1] * ps->nufft->op.g.N[2];
+	int Brow = choose_B(ps->nufft->op.g.G[0], YZ * ps->C);
+	long rowblocks = (YZ + Brow - 1) / Brow;
+	ps->cpg = (int)std::max<long>(1, std::min<long>(ps->C, (rowblocks * ps->C) / (2 * 148)));
+	ps->groups = (int)((ps->C + ps->cpg - 1) / ps->cpg);
+	ps->nparts = (int)vec_blocks(ps->npix);
+
+	auto ck = [&](cudaError_t e) { if (cudaSuccess != e && BNUFFT_OK == s) s = fail(BNUFFT_ERR_NOMEM, "pics buffers: %s", cudaGetErrorString(e)); };
+	ck(cudaMallocAsync(&ps->sens, sizeof(float2) * ps->npix * ps->C, st));
+	ck(cudaMallocAsync(&ps->part, sizeof(float2) * ps->npix * ps->groups, st));
+	ck(cudaMallocAsync(&ps->x, sizeof(float2) * ps->npix, st));
+	ck(cudaMallocAsync(&ps->r, sizeof(float2) * ps->npix, st));
+	ck(cudaMallocAsync(&ps->p, sizeof(float2) * ps->npix, st));
+	ck(cudaMallocAsync(&ps->Ap, sizeof(float2) * ps->npix, st));
+	ck(cudaMallocAsync(&ps->b, sizeof(float2) * ps->npix, st));
+	ck(cudaMallocAsync(&ps->mag, sizeof(float) * ps->npix, st));
+	ck(cudaMallocAsync(&ps->mag_sorted, sizeof(float) * ps->npix, st));
+	ck(cudaMallocAsync(&ps->pap_part, sizeof(double) * ps->nparts, st));
+	ck(cudaMallocAsync(&ps->rs_part, sizeof(double) * ps->nparts, st));
+	ck(cudaMallocAsync(&ps->scal, sizeof(CgScalars), st));
+
+	if (!conf.toeplitz)
+		ck(cudaMallocAsync(&ps->kbuf, sizeof(float2) * ps->M * ps->C, st));
+
+	if (BNUFFT_OK == s) {
+
+		cub::DeviceRadixSort::SortKeys(nullptr, ps->sort_tmp_bytes, ps->mag, ps->mag_sorted, (int)ps->npix, 0, 32, st);
+		ck(cudaMallocAsync(&ps->sort_tmp, ps->sort_tmp_bytes, st));
+	}
+
+	if (BNUFFT_OK == s) {
+
+		Staged sm;
+		s = stage_in(sm, sens, sizeof(float2) * ps->npix * ps->C, st);
+
+		if (BNUFFT_OK == s) {
+
+			cudaError_t e = cudaMemcpyAsync(ps->sens, sm.dev, sizeof(float2) * ps->npix * ps->C, cudaMemcpyDeviceToDevice, st);
+
+			if (cudaSuccess == e)
+				e = cudaStreamSynchronize(st);
+
+			if (cudaSuccess != e)
+				s = fail(BNUFFT_ERR_CUDA, "maps upload: %s", cudaGetErrorString(e));
+		}
+	}
+
+	if (BNUFFT_OK != s) {
+
+		std::string msg = g_err;
+		bnufft_pics_free(ps);
+		g_err = msg;
+		return s;
+	}
+
+	*out = ps;
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_pics_normal(bnufft_pics_t ps, void* dst, const void* src, void* stream)
+{
+	cudaStream_t st = S(stream);
+	size_t b = sizeof(float2) * ps->npix;
+	Staged i, o;
+	TRY(stage_in(i, src, b, st));
+	TRY(stage_out_alloc(o, dst, b));
+	TRY(sense_normal(ps, (const float2*)i.dev, (float2*)o.dev, 0.f, nullptr, nullptr, st));
+	return stage_out_copy(o, dst, b, st);
+}
+
+extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, void* stream)
+{
+	cudaStream_t st = S(stream);
+	size_t kb = sizeof(float2) * ps->M * ps->C;
+	size_t ib = sizeof(float2) * ps->npix;
+	Staged ki, io;
+	TRY(stage_in(ki, ksp, kb, st));
+	TRY(stage_out_alloc(io, img, ib));
+
+	OpCtx& op = ps->nufft->op;
+	float2* x = (float2*)io.dev;
+	unsigned nb = (unsigned)ps->nparts;
+
+	// adjoint of the data: A^H y (coil-sum partials, then combine)
+	TRY(op_adjoint(op, (const float2*)ki.dev, ps->sens, ps->C, ps->cpg, ps->part, st));
+	k_combine<<<nb, RED_THREADS, 0, st>>>(ps->b, ps->part, ps->groups, ps->npix, nullptr, 0.f, nullptr, nullptr);
+	LAUNCHED();
+
+	// data scaling (src/pics.c:499-530): y /= scale  <=>  A^H y /= scale
+	if (0.f == ps->conf.scaling) {
+
+		k_abs<<<nb, RED_THREADS, 0, st>>>(ps->mag, ps->b, ps->npix);
+		LAUNCHED();
+		CUDA_TRY(cub::DeviceRadixSort::SortKeys(ps->sort_tmp, ps->sort_tmp_bytes, ps->mag, ps->mag_sorted, (int)ps->npix, 0, 32, st));
+		g_launches.fetch_add(1, std::memory_order_relaxed);
+		k_scaling_from_sorted<<<1, 1, 0, st>>>(ps->mag_sorted, ps->npix, ps->scal);
+		LAUNCHED();
+
+	} else {
+
+		k_set_scaling<<<1, 1, 0, st>>>(ps->scal, ps->conf.scaling);
+		LAUNCHED();
+	}
+
+	k_scale_dev<<<nb, RED_THREADS, 0, st>>>(ps->b, ps->b, ps->npix, &ps->scal->inv_scale);
+	LAUNCHED();
+
+	// CG from zero on (A^H A + lambda) x = b
+	k_cg_init<<<nb, RED_THREADS, 0, st>>>(x, ps->r, ps->p, ps->b, ps->npix, ps->rs_part);
+	LAUNCHED();
+	k_cg_start<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->rs_part, ps->nparts, ps->conf.tol);
+	LAUNCHED();
+
+	for (int it = 0; it < ps->conf.maxiter; it++) {
+
+		int parity = it & 1;
+		TRY(sense_normal(ps, ps->p, ps->Ap, ps->conf.lambda, ps->pap_part, &ps->scal->done, st));
+		k_cg_update<<<nb, RED_THREADS, 0, st>>>(x, ps->r, ps->p, ps->Ap, ps->npix, ps->scal, parity,
+				ps->pap_part, ps->nparts, ps->rs_part);
+		LAUNCHED();
+		k_cg_direction<<<nb, RED_THREADS, 0, st>>>(ps->p, ps->r, ps->npix, ps->scal, parity,
+				ps->pap_part, ps->nparts, ps->rs_part, ps->nparts);
+		LAUNCHED();
+	}
+
+	if (ps->conf.rescale) {
+
+		k_scale_dev<<<nb, RED_THREADS, 0, st>>>(x, x, ps->npix, &ps->scal->scale);
+		LAUNCHED();
+	}
+
+	return stage_out_copy(io, img, ib, st);
+}
+
+extern "C" int bnufft_pics_stats(bnufft_pics_t ps, int* iters, double* rel_resid, float* scaling, void* stream)
+{
+	CgScalars h;
+	CUDA_TRY(cudaMemcpyAsync(&h, ps->scal, sizeof h, cudaMemcpyDeviceToHost, S(stream)));
+	CUDA_TRY(cudaStreamSynchronize(S(stream)));
+
+	if (iters)
+		*iters = h.iters;
+
+	if (rel_resid)
+		*rel_resid = (h.b2 > 0.) ? sqrt(h.rs[h.iters & 1] / h.b2) : 0.;
+
+	if (scaling)
+		*scaling = h.scale;
+
+	return BNUFFT_OK;
+}
+
+extern "C" void bnufft_pics_free(bnufft_pics_t ps)
+{
+	if (!ps)
+		return;
+
+	cudaStream_t st = ps->nufft ? ps->nufft->st0 : nullptr;
+	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->p, ps->Ap, ps->b, ps->kbuf, ps->mag, ps->mag_sorted,
+			 ps->sort_tmp, ps->pap_part, ps->rs_part, ps->scal };
+
+	for (void* b : bufs)
+		if (b)
+			cudaFreeAsync(b, st);
+
+	bnufft_free(ps->nufft);
+	delete ps;
+}
+
+extern "C" const char* bnufft_last_error(void) { return g_err.c_str(); }
+
+extern "C" int bnufft_prof_start(const char* kind)
+{
+	std::lock_guard<std::mutex> lock(g_prof_mutex);
+
+	for (auto& e : g_prof_events) {
+
+		cudaEventDestroy(e.first);
+		cudaEventDestroy(e.second);
+	}
+
+	g_prof_events.clear();
+	g_prof_target = kind ? kind : "";
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_prof_stop(double* total_ms, long* launches)
+{
+	std::lock_guard<std::mutex> lock(g_prof_mutex);
+	double tot = 0.;
+
+	for (auto& e : g_prof_events) {
+
+		float ms = 0.f;
+		CUDA_TRY(cudaEventSynchronize(e.second));
+		CUDA_TRY(cudaEventElapsedTime(&ms, e.first, e.second));
+		tot += ms;
+	}
+
+	if (total_ms)
+		*total_ms = tot;
+
+	if (launches)
+		*launches = (long)g_prof_events.size();
+
+	for (auto& e : g_prof_events) {
+
+		cudaEventDestroy(e.first);
+		cudaEventDestroy(e.second);
+	}
+
+	g_prof_events.clear();
+	g_prof_target.clear();
+	return BNUFFT_OK;
+}
+
+extern "C" long bnufft_launch_count(void) { return g_launches.load(); }

@@ -1,0 +1,310 @@
+// Vector kernels of the CG-SENSE solve, fused into single passes.
+//
+// The reference runs CG (src/iter/italgos.c:497-572) with one kernel per
+// vector op and a device->host copy for every dot product
+// (src/num/gpuops.c:633-665). Here the scalars stay on the device in float64:
+// each pass writes per-block float64 partial sums, and the next pass reduces
+// them in a fixed order (every block redundantly), so the iteration needs no
+// host synchronisation and the sums are bit-reproducible run to run.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fft_core.cuh"
+
+namespace bn {
+
+enum { RED_THREADS = 256 };
+
+// device-side CG state
+struct CgScalars {
+
+	double rs[2];		// ||r||^2, double-buffered by iteration parity
+	double eps2;		// stop when ||r||^2 <= eps2
+	double b2;		// ||A^H y||^2
+	int done;		// set once converged (or pAp == 0)
+	int iters;		// iterations completed
+	float scale;		// data scaling used
+	float inv_scale;	// float(1 / scale)
+};
+
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* sh)
+{
+	for (int o = 16; o > 0; o >>= 1)
+		v += __shfl_down_sync(0xffffffffu, v, o);
+
+	int w = threadIdx.x / 32;
+	int l = threadIdx.x % 32;
+
+	if (0 == l)
+		sh[w] = v;
+
+	__syncthreads();
+
+	T r = 0;
+
+	if (threadIdx.x < 32) {
+
+		r = (threadIdx.x < blockDim.x / 32) ? sh[threadIdx.x] : (T)0;
+
+		for (int o = 16; o > 0; o >>= 1)
+			r += __shfl_down_sync(0xffffffffu, r, o);
+	}
+
+	return r;	// valid in thread 0
+}
+
+// fixed-order sum of n partials, identical in every block
+__device__ __forceinline__ double sum_partials(const double* part, int n, double* sh)
+{
+	double v = 0.;
+
+	for (int i = threadIdx.x; i < n; i += blockDim.x)
+		v += part[i];
+
+	double r = block_sum(v, sh);
+
+	__syncthreads();
+
+	if (0 == threadIdx.x)
+		sh[0] = r;
+
+	__syncthreads();
+
+	double out = sh[0];
+
+	__syncthreads();
+
+	return out;
+}
+
+// dst[i] = sum_g part[i + n*g] (+ lam * x[i]); optional per-block partial of
+// Re<x, dst> into dot_part. n complex elements.
+__global__ void k_combine(float2* __restrict__ dst, const float2* __restrict__ part, int groups, long n,
+		const float2* __restrict__ x, float lam, double* __restrict__ dot_part, const int* done)
+{
+	__shared__ double sh[32];
+
+	if (done && *done)
+		return;
+
+	double acc = 0.;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		float2 v = part[i];
+
+		for (int g = 1; g < groups; g++)
+			v = cadd(v, part[i + n * g]);
+
+		if (x) {
+
+			float2 xv = x[i];
+			v.x = fmaf(lam, xv.x, v.x);
+			v.y = fmaf(lam, xv.y, v.y);
+			acc += (double)xv.x * (double)v.x + (double)xv.y * (double)v.y;
+		}
+
+		dst[i] = v;
+	}
+
+	if (dot_part) {
+
+		double r = block_sum(acc, sh);
+
+		if (0 == threadIdx.x)
+			dot_part[blockIdx.x] = r;
+	}
+}
+
+// CG start from x = 0: x = 0, r = p = b; partial ||b||^2.
+__global__ void k_cg_init(float2* __restrict__ x, float2* __restrict__ r, float2* __restrict__ p,
+		const float2* __restrict__ b, long n, double* __restrict__ part)
+{
+	__shared__ double sh[32];
+	double acc = 0.;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		float2 v = b[i];
+		x[i] = make_float2(0.f, 0.f);
+		r[i] = v;
+		p[i] = v;
+		acc += (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+	}
+
+	double s = block_sum(acc, sh);
+
+	if (0 == threadIdx.x)
+		part[blockIdx.x] = s;
+}
+
+// rs[0] = ||b||^2 = b2, eps2 = (tol*||b||)^2, iters = 0, done = (b2 == 0)
+__global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float tol)
+{
+	__shared__ double sh[32];
+	double b2 = sum_partials(part, nparts, sh);
+
+	if (0 == threadIdx.x) {
+
+		st->b2 = b2;
+		st->rs[0] = b2;
+		double eps = (double)tol * sqrt(b2);
+		st->eps2 = eps * eps;
+		st->iters = 0;
+		st->done = (0. == b2);
+	}
+}
+
+// alpha = rs_old / pAp; x += alpha p; r -= alpha Ap; partial ||r||^2.
+__global__ void k_cg_update(float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
+		const float2* __restrict__ Ap, long n, CgScalars* st, int parity,
+		const double* __restrict__ pap_part, int nparts, double* __restrict__ rs_part)
+{
+	__shared__ double sh[32];
+
+	if (st->done)
+		return;
+
+	double pAp = sum_partials(pap_part, nparts, sh);
+
+	if (0. == pAp)
+		return;	// the direction step below marks the solve done
+
+	// alpha in float64 (the reference rounds rsold/pAp to float)
+	double alpha = st->rs[parity] / pAp;
+	float a = (float)alpha;
+	double acc = 0.;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		float2 pv = p[i];
+		float2 av = Ap[i];
+		float2 xv = x[i];
+		float2 rv = r[i];
+		xv.x = fmaf(a, pv.x, xv.x);
+		xv.y = fmaf(a, pv.y, xv.y);
+		rv.x = fmaf(-a, av.x, rv.x);
+		rv.y = fmaf(-a, av.y, rv.y);
+		x[i] = xv;
+		r[i] = rv;
+		acc += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+	}
+
+	double s = block_sum(acc, sh);
+
+	if (0 == threadIdx.x)
+		rs_part[blockIdx.x] = s;
+}
+
+// rs_new = ||r||^2; beta = rs_new / rs_old; p = r + beta p (unless converged).
+__global__ void k_cg_direction(float2* __restrict__ p, const float2* __restrict__ r, long n,
+		CgScalars* st, int parity, const double* __restrict__ pap_part, int npap,
+		const double* __restrict__ rs_part, int nparts)
+{
+	__shared__ double sh[32];
+
+	if (st->done)
+		return;
+
+	double pAp = sum_partials(pap_part, npap, sh);
+
+	if (0. == pAp) {
+
+		__syncthreads();
+
+		if ((0 == blockIdx.x) && (0 == threadIdx.x))
+			st->done = 1;
+
+		return;
+	}
+
+	double rs_new = sum_partials(rs_part, nparts, sh);
+	double rs_old = st->rs[parity];
+	bool stop = (rs_new <= st->eps2);
+
+	if (!stop) {
+
+		float beta = (float)(rs_new / rs_old);
+
+		for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+			float2 pv = p[i];
+			float2 rv = r[i];
+			pv.x = fmaf(beta, pv.x, rv.x);
+			pv.y = fmaf(beta, pv.y, rv.y);
+			p[i] = pv;
+		}
+	}
+
+	if ((0 == blockIdx.x) && (0 == threadIdx.x)) {
+
+		st->rs[parity ^ 1] = rs_new;
+		st->iters += 1;
+
+		if (stop)
+			st->done = 1;
+	}
+}
+
+// dst = src * scalar (scalar read from device memory, float)
+__global__ void k_scale_dev(float2* __restrict__ dst, const float2* __restrict__ src, long n, const float* s)
+{
+	float f = *s;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+		dst[i] = cscale(src[i], f);
+}
+
+__global__ void k_scale(float2* __restrict__ dst, const float2* __restrict__ src, long n, float f)
+{
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+		dst[i] = cscale(src[i], f);
+}
+
+__global__ void k_abs(float* __restrict__ dst, const float2* __restrict__ src, long n)
+{
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		float2 v = src[i];
+		dst[i] = hypotf(v.x, v.y);	// cabsf
+	}
+}
+
+// estimate_scaling_norm (src/sense/optcom.c:74-109) on magnitudes sorted
+// ascending: p90 unless (max - p90) >= 2 (p90 - median), then max; 0 -> 1.
+__global__ void k_scaling_from_sorted(const float* sorted, long n, CgScalars* st)
+{
+	float median = sorted[n / 2];
+	float p90 = sorted[(long)trunc(n * 0.9)];
+	float mx = sorted[n - 1];
+	float scale = ((mx - p90) < 2 * (p90 - median)) ? p90 : mx;
+
+	if (0.f == scale)
+		scale = 1.f;
+
+	st->scale = scale;
+	st->inv_scale = (float)(1. / scale);
+}
+
+__global__ void k_set_scaling(CgScalars* st, float scale)
+{
+	st->scale = scale;
+	st->inv_scale = (float)(1. / scale);
+}
+
+__global__ void k_fill(float2* dst, long n, float2 v)
+{
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+		dst[i] = v;
+}
+
+// trajectory [3, M] complex float -> float4 (kx, ky, kz, 0) * factor
+__global__ void k_traj_convert(float4* __restrict__ dst, const float2* __restrict__ src, long M, float factor)
+{
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += (long)gridDim.x * blockDim.x)
+		dst[i] = make_float4(src[3 * i + 0].x * factor, src[3 * i + 1].x * factor, src[3 * i + 2].x * factor, 0.f);
+}
+
+} // namespace bn

@@ -1,0 +1,137 @@
+/* bnufft: B200-native NUFFT and CG-SENSE, C ABI.
+ *
+ * Drop-in boundary for the NUFFT linop and the CG-SENSE solve of
+ * mrirecon/bart v1.0.00. Every entry point takes plain pointers and sizes and
+ * returns a status code (0 = success); on failure bnufft_last_error() gives
+ * a message. Arrays are BART arrays: column-major complex float with N (16)
+ * dimensions in the reference's order (src/misc/mri.h:12-35). Data pointers
+ * may be host or device memory (decided per call from the pointer, as the
+ * reference does with cuda_ondevice(), src/num/gpuops.c:445); host data is
+ * staged through device buffers. "stream" is a cudaStream_t (NULL: default
+ * stream). There is no CPU fallback: without a usable CUDA device every
+ * call fails with BNUFFT_ERR_CUDA.
+ */
+#ifndef BNUFFT_H
+#define BNUFFT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum bnufft_status {
+	BNUFFT_OK = 0,
+	BNUFFT_ERR_ARG = 1,		/* bad dimensions / options */
+	BNUFFT_ERR_UNSUPPORTED = 2,	/* valid for the reference, not built here */
+	BNUFFT_ERR_CUDA = 3,		/* CUDA runtime error (message has details) */
+	BNUFFT_ERR_NOMEM = 4,
+};
+
+/* NUFFT configuration: the subset of struct nufft_conf_s
+ * (src/noncart/nufft.h:7-30) this build implements. Defaults as
+ * nufft_conf_defaults (src/noncart/nufft.c:53-74): toeplitz 1, periodic 0,
+ * os 2, width 6. deterministic selects fixed-order (atomic-free) gridding. */
+struct bnufft_conf {
+
+	int toeplitz;
+	int periodic;
+	int deterministic;
+	float os;
+	float width;
+};
+
+typedef struct bnufft_plan_s* bnufft_plan_t;
+
+/* Defaults as nufft_conf_defaults. */
+void bnufft_conf_defaults(struct bnufft_conf* conf);
+
+/* Replaces nufft_create2() (src/noncart/nufft.h:48-57, src/noncart/nufft.c:1174).
+ * ksp_dims [1, Mr, Ms, C, ...], cim_dims [X, Y, Z, C, ...], traj_dims
+ * [3, Mr, Ms, 1, ...], traj complex float (real parts used). Weights and
+ * basis must be NULL here (BNUFFT_ERR_UNSUPPORTED otherwise). The plan
+ * copies the trajectory (the caller keeps its buffer) and, with
+ * conf->toeplitz, computes the PSF on the device (compute_psf2,
+ * src/noncart/nufft.c:727-776). */
+int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[], const long cim_dims[],
+		const long traj_dims[], const void* traj,
+		const long wgh_dims[], const void* weights,
+		const long bas_dims[], const void* basis,
+		const struct bnufft_conf* conf, void* stream);
+
+/* Linop callbacks of the NUFFT (lop_fun_t, src/linops/linop.c:300):
+ * forward  = nufft_apply_forward (src/noncart/nufft.c:1388), cim -> ksp
+ * adjoint  = nufft_apply_adjoint (src/noncart/nufft.c:1462), ksp -> cim
+ * normal   = nufft_apply_normal (src/noncart/nufft.c:1740), cim -> cim;
+ *            Toeplitz embedding when the plan has a PSF, else adjoint(forward). */
+int bnufft_apply_forward(bnufft_plan_t plan, void* dst, const void* src, void* stream);
+int bnufft_apply_adjoint(bnufft_plan_t plan, void* dst, const void* src, void* stream);
+int bnufft_apply_normal(bnufft_plan_t plan, void* dst, const void* src, void* stream);
+
+/* Replaces nufft_get_psf_dims / nufft_get_psf (src/noncart/nufft.c:2008-2039):
+ * the PSF in the reference's decomposed layout [X, Y, Z, 1, ..., 2^d] with
+ * N+1 dims. psf_dims receives N+1 entries. */
+int bnufft_get_psf_dims(bnufft_plan_t plan, int ND, long psf_dims[]);
+int bnufft_get_psf(bnufft_plan_t plan, int ND, const long psf_dims[], void* psf, void* stream);
+
+/* Replaces nufft_update_traj (src/noncart/nufft.c:2041-2054) for a
+ * trajectory of unchanged dims (weights / basis must be NULL). */
+int bnufft_update_traj(bnufft_plan_t plan, int N, const long traj_dims[], const void* traj, void* stream);
+
+/* linop_free() of a NUFFT linop (nufft_free_data, src/noncart/nufft.c:1334). */
+void bnufft_free(bnufft_plan_t plan);
+
+/* --- CG-SENSE: bart pics -l2 -r lambda -i iter -t traj ksp sens out ------- */
+
+struct bnufft_pics_conf {
+
+	float lambda;		/* -r (l2 regularisation), src/grecon/optreg.c:382-393 */
+	int maxiter;		/* -i, default 30 (src/pics.c:82) */
+	float tol;		/* CG stop: ||r|| <= tol * ||A^H y|| (iter_conjgrad_defaults.tol = 0) */
+	float scaling;		/* -w: 0 = estimate (src/pics.c:499-530) */
+	int rescale;		/* -S */
+	int toeplitz;		/* default 1 (src/pics.c:90-91); 0 = --no-toeplitz */
+	int periodic;
+	int deterministic;
+};
+
+typedef struct bnufft_pics_s* bnufft_pics_t;
+
+void bnufft_pics_conf_defaults(struct bnufft_pics_conf* conf);
+
+/* Builds the SENSE model A = NUFFT o maps (sense_nc_init,
+ * src/sense/modelnc.c:28-67; maps2_create src/sense/model.c:93) for
+ * ksp_dims [1, Mr, Ms, C], sens_dims [X, Y, Z, C], traj_dims [3, Mr, Ms]. */
+int bnufft_pics_create(bnufft_pics_t* pics, int N, const long ksp_dims[], const long sens_dims[],
+		const long traj_dims[], const void* traj, const void* sens,
+		const struct bnufft_pics_conf* conf, void* stream);
+
+/* One reconstruction (main_pics CG branch, src/pics.c:499-760): data
+ * scaling, x = argmin ||A x - y||^2 + lambda ||x||^2 by CG from zero
+ * (conjgrad, src/iter/italgos.c:497-572). img is [X, Y, Z, 1]. */
+int bnufft_pics_run(bnufft_pics_t pics, void* img, const void* ksp, void* stream);
+
+/* Normal operator of the SENSE model, A^H A x (no lambda), img -> img. */
+int bnufft_pics_normal(bnufft_pics_t pics, void* dst, const void* src, void* stream);
+
+/* Statistics of the last run: iterations done, recursive relative residual
+ * ||r||/||A^H y||, scaling used. Synchronises the stream. */
+int bnufft_pics_stats(bnufft_pics_t pics, int* iters, double* rel_resid, float* scaling, void* stream);
+
+void bnufft_pics_free(bnufft_pics_t pics);
+
+/* Message of the last failure on this thread ("" if none). */
+const char* bnufft_last_error(void);
+
+/* Number of kernel launches issued by this library since load. */
+long bnufft_launch_count(void);
+
+/* Instrumentation (no counterpart in the reference): time every launch of
+ * one kernel class ("rows_fwd", "cols_fwd", "cols_inv", "cols_toeplitz",
+ * "rows_inv", "degrid", "grid") with CUDA events on its stream until
+ * bnufft_prof_stop(), which returns the summed device time and launch count. */
+int bnufft_prof_start(const char* kind);
+int bnufft_prof_stop(double* total_ms, long* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,107 @@
+"""Regenerate the golden fixtures from the reference's own CPU tools.
+
+Runs the mrirecon/bart v1.0.00 tools built by ``oracle/refbuild/Makefile``
+(``oracle/_ref/bin``: nufft, pics, traj and the refnormal checker) on
+seeded synthetic inputs and stores inputs and outputs as compressed .npz
+files next to this script. Only needed when the fixtures change; the tests
+read the .npz files and never run the reference.
+
+    make -f oracle/refbuild/Makefile -j8
+    python tests/golden/make_golden.py
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+import zlib
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from bart_b200 import synth  # noqa: E402
+from bart_b200.cfl import readcfl, writecfl  # noqa: E402
+
+BIN = os.path.join(ROOT, "oracle", "_ref", "bin")
+
+
+def run(*args, cwd):
+    r = subprocess.run([os.path.join(BIN, args[0])] + list(args[1:]), cwd=cwd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"{args}: {r.stderr}")
+
+
+def cplx(rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+def nufft_case(name, traj, img, periodic=False, normal=True):
+    with tempfile.TemporaryDirectory() as d:
+        rng = np.random.default_rng(zlib.crc32(name.encode()))
+        writecfl(os.path.join(d, "t"), traj)
+        writecfl(os.path.join(d, "x"), img)
+        P = ["-P"] if periodic else []
+        run("nufft", *P, "t", "x", "k", cwd=d)
+        fwd = readcfl(os.path.join(d, "k"))
+        ksp = cplx(rng, fwd.shape)
+        writecfl(os.path.join(d, "y"), ksp)
+        dims = ":".join(str(s) for s in (list(img.shape) + [1, 1])[:3])
+        run("nufft", *P, "-a", f"-x{dims}", "t", "y", "a", cwd=d)
+        adj = readcfl(os.path.join(d, "a"))
+        out = dict(traj=traj, img=img, fwd=fwd, ksp=ksp, adj=adj)
+        if normal:
+            run("refnormal", *P, "t", "x", "n", "p", cwd=d)
+            out["normal"] = readcfl(os.path.join(d, "n"))
+            out["psf"] = readcfl(os.path.join(d, "p"))
+            run("refnormal", *P, "--no-toeplitz", "t", "x", "ne", cwd=d)
+            out["normal_explicit"] = readcfl(os.path.join(d, "ne"))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **{k: np.asarray(v) for k, v in out.items()})
+    print(name, {k: np.shape(v) for k, v in out.items()})
+
+
+def pics_case(name, N, C, spokes, seed):
+    from oracle.nufft_oracle import SenseOracle
+    rng = np.random.default_rng(seed)
+    traj = synth.radial_traj(N, spokes)
+    truth = synth.ellipse_phantom(N, 20, rng)
+    sens = synth.coil_maps(N, C, rng)
+    A = SenseOracle(traj.real.reshape(3, -1, order="F"), sens)
+    y = A.forward(truth.reshape(N, N, 1, 1))
+    y = synth.add_noise(y, 40.0, rng)
+    ksp = y.reshape(1, traj.shape[1], traj.shape[2], C, order="F")
+    out = dict(traj=traj, sens=sens, ksp=ksp, truth=truth)
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "t"), traj)
+        writecfl(os.path.join(d, "s"), sens)
+        writecfl(os.path.join(d, "k"), ksp)
+        for key, args in [("x5_w1", ["-i5", "-w1"]), ("x30_w1", ["-i30", "-w1"]), ("x30", ["-i30"]),
+                          ("x5_w1_notoep", ["-i5", "-w1", "--no-toeplitz"]), ("x30_rescale", ["-i30", "-S"])]:
+            run("pics", "-l2", "-r0.01", *args, "-t", "t", "k", "s", "o", cwd=d)
+            out[key] = readcfl(os.path.join(d, "o"))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, {k: np.shape(v) for k, v in out.items()})
+
+
+def main():
+    rng = np.random.default_rng(20261203)
+    with tempfile.TemporaryDirectory() as d:
+        run("traj", "-r", "-G", "-x64", "-o2", "-y24", "t", cwd=d)
+        t64 = readcfl(os.path.join(d, "t"))
+        run("traj", "-r", "-G", "-x32", "-o2", "-y16", "t", cwd=d)
+        t32 = readcfl(os.path.join(d, "t"))
+    img64 = cplx(rng, (64, 64))
+    nufft_case("nufft2d_n64", t64, img64)
+    nufft_case("nufft2d_n64_periodic", t64, img64, periodic=True)
+    nufft_case("nufft2d_n32_coils3", t32, cplx(rng, (32, 32, 1, 3)), normal=False)
+    t3 = synth.kooshball_traj(16, 96)
+    nufft_case("nufft3d_n16", t3, cplx(rng, (16, 16, 16)))
+    pics_case("pics2d_n64_c4", 64, 4, 24, seed=7)
+
+
+if __name__ == "__main__":
+    main()

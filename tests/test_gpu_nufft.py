@@ -1,0 +1,130 @@
+"""GPU NUFFT through the C ABI against the reference's outputs and the oracle.
+
+Bar: relative L2 <= 1e-5 per operator apply (forward, adjoint, Toeplitz
+normal, PSF), on the golden fixtures (reference outputs) and on fresh seeded
+inputs against the oracle.
+"""
+
+import numpy as np
+import pytest
+
+from bart_b200 import synth
+from bart_b200.nufft import NufftConf, nufft_create2
+from conftest import golden, rel
+from oracle import nufft_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _dims(img_shape):
+    s = list(img_shape) + [1] * (4 - len(img_shape))
+    return s
+
+
+def _plan(g, periodic=False, toeplitz=True):
+    img = g["img"]
+    cd = _dims(img.shape)
+    td = list(g["traj"].shape)
+    kd = [1, td[1], td[2], cd[3]]
+    return nufft_create2(kd, cd, td, g["traj"], conf=NufftConf(toeplitz=toeplitz, periodic=periodic)), cd, kd
+
+
+@pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
+                                           ("nufft3d_n16", False), ("nufft2d_n32_coils3", False)])
+def test_forward_adjoint_vs_reference(name, periodic):
+    g = golden(name)
+    op, cd, kd = _plan(g, periodic, toeplitz=False)
+    fwd = op.forward(g["img"].reshape(cd, order="F"))
+    assert rel(fwd, g["fwd"]) < TOL
+    adj = op.adjoint(g["ksp"].reshape(kd, order="F"))
+    assert rel(adj, g["adj"]) < TOL
+    op.free()
+
+
+@pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
+                                           ("nufft3d_n16", False)])
+def test_toeplitz_normal_and_psf_vs_reference(name, periodic):
+    g = golden(name)
+    op, cd, kd = _plan(g, periodic, toeplitz=True)
+    n = op.normal(g["img"].reshape(cd, order="F"))
+    assert rel(n, g["normal"]) < TOL
+    psf = op.psf()
+    assert rel(psf, g["psf"].reshape(psf.shape, order="F")) < TOL
+    op.free()
+    op, cd, kd = _plan(g, periodic, toeplitz=False)
+    n = op.normal(g["img"].reshape(cd, order="F"))     # explicit adjoint(forward)
+    assert rel(n, g["normal_explicit"]) < TOL
+    op.free()
+
+
+@pytest.mark.parametrize("N,spokes,coils", [(128, 64, 1), (96 * 2, 40, 2), (256, 402, 1)])
+def test_2d_vs_oracle(N, spokes, coils):
+    rng = np.random.default_rng(N + spokes)
+    t = synth.radial_traj(N, spokes)
+    img = (rng.standard_normal((N, N, 1, coils)) + 1j * rng.standard_normal((N, N, 1, coils))).astype(np.complex64)
+    cd = [N, N, 1, coils]
+    kd = [1, t.shape[1], t.shape[2], coils]
+    op = nufft_create2(kd, cd, list(t.shape), t, conf=NufftConf(toeplitz=True))
+    o = orc.NufftOracle(t.real.reshape(3, -1, order="F"), (N, N, 1))
+    assert rel(op.forward(img), o.forward(img)) < TOL
+    y = (rng.standard_normal((t.shape[1] * t.shape[2], coils)) + 1j * rng.standard_normal((t.shape[1] * t.shape[2], coils))).astype(np.complex64)
+    assert rel(op.adjoint(y.reshape(kd, order="F")), o.adjoint(y)) < TOL
+    assert rel(op.normal(img), o.normal_toeplitz(img)) < TOL
+    op.free()
+
+
+def test_3d_vs_oracle():
+    rng = np.random.default_rng(5)
+    N = 32
+    t = synth.kooshball_traj(N, 300)
+    img = (rng.standard_normal((N, N, N, 1)) + 1j * rng.standard_normal((N, N, N, 1))).astype(np.complex64)
+    cd = [N, N, N, 1]
+    kd = [1, t.shape[1], t.shape[2], 1]
+    op = nufft_create2(kd, cd, list(t.shape), t, conf=NufftConf(toeplitz=True))
+    o = orc.NufftOracle(t.real.reshape(3, -1, order="F"), (N, N, N))
+    assert rel(op.forward(img), o.forward(img)) < TOL
+    y = (rng.standard_normal(kd[1] * kd[2]) + 1j * rng.standard_normal(kd[1] * kd[2])).astype(np.complex64)
+    assert rel(op.adjoint(y.reshape(kd, order="F")), o.adjoint(y[:, None])) < TOL
+    assert rel(op.normal(img), o.normal_toeplitz(img)) < TOL
+    op.free()
+
+
+def test_device_and_host_pointers_agree(cuda):
+    import torch
+    g = golden("nufft2d_n64")
+    op, cd, kd = _plan(g, toeplitz=False)
+    x = g["img"].reshape(cd, order="F").astype(np.complex64)
+    host = op.forward(x)
+    xd = torch.from_numpy(np.asfortranarray(x).ravel(order="F")).to(cuda)
+    dev = op.forward(xd)
+    torch.cuda.synchronize()
+    assert np.array_equal(dev.cpu().numpy(), np.asarray(host).ravel(order="F"))
+    op.free()
+
+
+def test_adjointness_full_size():
+    """<A x, y> = <x, A^H y> at the 256^2, 402x512 single-coil size."""
+    rng = np.random.default_rng(11)
+    t = synth.radial_traj(256, 402)
+    cd = [256, 256, 1, 1]
+    kd = [1, 512, 402, 1]
+    op = nufft_create2(kd, cd, list(t.shape), t, conf=NufftConf(toeplitz=False))
+    x = (rng.standard_normal(cd) + 1j * rng.standard_normal(cd)).astype(np.complex64)
+    y = (rng.standard_normal(kd) + 1j * rng.standard_normal(kd)).astype(np.complex64)
+    ax = np.asarray(op.forward(x)).astype(np.complex128)
+    ay = np.asarray(op.adjoint(y)).astype(np.complex128)
+    lhs = np.vdot(ax.ravel(order="F"), y.astype(np.complex128).ravel(order="F"))
+    rhs = np.vdot(x.astype(np.complex128).ravel(order="F"), ay.ravel(order="F"))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+    op.free()
+
+
+def test_unsupported_options_fail_loudly():
+    from bart_b200._lib import BnufftError
+    t = synth.radial_traj(32, 8)
+    with pytest.raises(BnufftError):
+        nufft_create2([1, 64, 8, 1], [32, 32, 1, 1], list(t.shape), t, conf=NufftConf(os=1.5))
+    with pytest.raises(BnufftError):
+        nufft_create2([1, 64, 8, 1], [33, 33, 1, 1], list(t.shape), t)

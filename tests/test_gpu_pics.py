@@ -1,0 +1,65 @@
+"""GPU CG-SENSE (pics -l2) through the C ABI against the reference and the oracle."""
+
+import numpy as np
+import pytest
+
+from bart_b200.pics import Pics, PicsConf
+from conftest import golden, rel
+from oracle import nufft_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(g, **kw):
+    p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape), conf=PicsConf(lam=0.01, **kw))
+    x = p.run(g["ksp"])
+    st = p.stats()
+    p.free()
+    return np.asarray(x), st
+
+
+def test_pics_5_iterations_vs_reference():
+    g = golden("pics2d_n64_c4")
+    x, st = _run(g, maxiter=5, scaling=1.0)
+    assert st[0] == 5
+    assert rel(x, g["x5_w1"]) < 1e-5
+    x, st = _run(g, maxiter=5, scaling=1.0, toeplitz=False)
+    assert rel(x, g["x5_w1_notoep"]) < 1e-5
+
+
+def test_pics_30_iterations_vs_reference():
+    """Unconverged float32 CG drifts with rounding; the reference itself moves
+    by ~1e-4..1e-2 between float32 orderings. Scaling must match exactly."""
+    g = golden("pics2d_n64_c4")
+    x, st = _run(g, maxiter=30)
+    assert rel(x, g["x30"]) < 2e-2
+    xs, st2 = _run(g, maxiter=30, rescale=True)
+    assert st2[2] == st[2]
+    assert rel(xs, g["x30_rescale"]) < 2e-2
+
+
+def test_pics_converged_vs_fp64_oracle():
+    """Run to a tight tolerance: GPU (FP32 vectors, FP64 scalars) and the
+    FP64 oracle converge to the same solution (<= 1e-4)."""
+    g = golden("pics2d_n64_c4")
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    C = g["sens"].shape[3]
+    y = g["ksp"].reshape(-1, C, order="F")
+    A = orc.SenseOracle(traj, g["sens"])
+    b = A.adjoint(y)
+    xo, _ = orc.conjgrad(A.normal, b, 0.01, 500, tol=1e-9)
+    x, st = _run(g, maxiter=300, scaling=1.0, tol=1e-6)
+    assert st[1] <= 1e-6
+    assert rel(x, xo) < 1e-4
+    assert orc.normal_residual(A, x.reshape(xo.shape, order="F"), b, 0.01) < 1e-5
+
+
+def test_sense_normal_vs_oracle():
+    g = golden("pics2d_n64_c4")
+    p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape), conf=PicsConf(lam=0.01))
+    rng = np.random.default_rng(3)
+    x = (rng.standard_normal((64, 64)) + 1j * rng.standard_normal((64, 64))).astype(np.complex64)
+    n = np.asarray(p.normal(np.asfortranarray(x.reshape(64, 64, 1))))
+    p.free()
+    A = orc.SenseOracle(g["traj"].real.reshape(3, -1, order="F"), g["sens"])
+    assert rel(n, A.normal(x.reshape(64, 64, 1, 1))) < 1e-5

@@ -1,0 +1,99 @@
+"""The oracle against the reference's own outputs (golden fixtures).
+
+The fixtures were produced by the reference's CPU tools built from its
+sources (tests/golden/make_golden.py). The oracle must reproduce every
+operator apply to float32 rounding of the reference (<= 1e-6 relative L2).
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden, rel
+from oracle import nufft_oracle as orc
+
+OPS_TOL = 1e-6
+
+
+def _op(g, periodic=False):
+    img = g["img"]
+    while img.ndim < 4:
+        img = img[..., None]
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    return orc.NufftOracle(traj, img.shape[:3], periodic=periodic), img
+
+
+@pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
+                                           ("nufft3d_n16", False), ("nufft2d_n32_coils3", False)])
+def test_forward_adjoint(name, periodic):
+    g = golden(name)
+    o, img = _op(g, periodic)
+    C = img.shape[3]
+    fwd = o.forward(img)
+    assert rel(fwd, g["fwd"].reshape(-1, C, order="F")) < OPS_TOL
+    adj = o.adjoint(g["ksp"].reshape(-1, C, order="F"))
+    assert rel(adj, g["adj"].reshape(img.shape, order="F")) < OPS_TOL
+
+
+@pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
+                                           ("nufft3d_n16", False)])
+def test_toeplitz_normal_and_psf(name, periodic):
+    g = golden(name)
+    o, img = _op(g, periodic)
+    assert rel(o.normal_toeplitz(img), g["normal"].reshape(img.shape, order="F")) < OPS_TOL
+    assert rel(o.normal_explicit(img), g["normal_explicit"].reshape(img.shape, order="F")) < OPS_TOL
+    # PSF: reference sub-grid s, index w  <->  centred 2N cell 2w + s
+    psf = g["psf"]
+    dims3 = img.shape[:3]
+    nd = sum(1 for d in dims3 if d > 1)
+    P = o.psf()
+    sub = psf.reshape(dims3 + (2 ** nd,), order="F")
+    rec = np.zeros(P.shape, dtype=np.complex128)
+    for s in range(2 ** nd):
+        sl = []
+        b = s
+        for d in dims3:
+            if d > 1:
+                sl.append(slice(b & 1, None, 2))
+                b >>= 1
+            else:
+                sl.append(slice(None))
+        rec[tuple(sl)] = sub[..., s]
+    assert rel(P, rec) < OPS_TOL
+
+
+def test_nufft_close_to_ndft():
+    """The NUFFT approximates the exact NDFT (accuracy of KB w=6, os=2)."""
+    g = golden("nufft2d_n64_periodic")
+    o, img = _op(g, periodic=True)
+    exact = orc.ndft_forward(g["traj"].real.reshape(3, -1, order="F"), img)
+    assert rel(o.forward(img), exact) < 1e-4
+
+
+def test_pics_few_iterations():
+    """CG-SENSE at 5 iterations matches the reference's pics (float32 CG)."""
+    g = golden("pics2d_n64_c4")
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    C = g["sens"].shape[3]
+    y = g["ksp"].reshape(-1, C, order="F")
+    x, sc = orc.pics_l2(traj, y, g["sens"], lam=0.01, maxiter=5, scaling=1.0)
+    assert rel(x, g["x5_w1"].reshape(x.shape, order="F")) < 1e-5
+    x, sc = orc.pics_l2(traj, y, g["sens"], lam=0.01, maxiter=5, scaling=1.0, toeplitz=False)
+    assert rel(x, g["x5_w1_notoep"].reshape(x.shape, order="F")) < 1e-5
+
+
+def test_pics_scaling_and_30_iterations():
+    """30 iterations: float32 CG (reference) and float64 CG (oracle) drift
+    apart through rounding (not converged: residual ~1e-3); the data scaling
+    rule and the -S rescale are exact."""
+    g = golden("pics2d_n64_c4")
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    C = g["sens"].shape[3]
+    y = g["ksp"].reshape(-1, C, order="F")
+    x, sc = orc.pics_l2(traj, y, g["sens"], lam=0.01, maxiter=30)
+    ref = g["x30"].reshape(x.shape, order="F")
+    assert rel(x, ref) < 2e-2
+    xs, sc2 = orc.pics_l2(traj, y, g["sens"], lam=0.01, maxiter=30, rescale=True)
+    assert sc2 == sc
+    # two reference runs differ slightly: its CPU gridding adds with OpenMP
+    # atomics in a varying order (doc/performance.txt:67-69)
+    assert rel(g["x30_rescale"], g["x30"] * sc) < 1e-4
