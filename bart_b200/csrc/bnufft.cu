@@ -62,8 +62,22 @@ static cudaEvent_t prof_begin(const char* kind, cudaStream_t st)
 		return nullptr;
 
 	cudaEvent_t a, b;
-	cudaEventCreate(&a);
-	cudaEventCreate(&b);
+	static std::vector<cudaEvent_t> pool;
+
+	if (pool.size() < 2) {
+
+		for (int i = 0; i < 256; i++) {
+
+			cudaEvent_t e;
+			cudaEventCreate(&e);
+			pool.push_back(e);
+		}
+	}
+
+	a = pool.back();
+	pool.pop_back();
+	b = pool.back();
+	pool.pop_back();
 	cudaEventRecord(a, st);
 	g_prof_events.push_back({ a, b });
 	return b;
@@ -220,122 +234,180 @@ static bool supported_len(int L) { return (L >= 16) && (L <= 2048) && (0 == (L &
 
 static size_t pass_smem(int L, int B) { return sizeof(float2) * (size_t)L * (size_t)(smem_stride(B) + 1); }
 
-// sequences per block: B * L / 8 threads (<= 1024), at most 16 sequences,
-// fewer when the launch would have too few blocks
-static int choose_B(int L, long nseq, int max_b = 16)
+// sequences per block (B in {4, 8, 16}, B * L / 8 threads <= 1024): as many
+// as fit, fewer when the launch would have too few blocks to fill the GPU
+static int choose_B(int L, long nseq)
 {
-	int B = std::min(max_b, 8192 / L);
+	int B = std::min(16, 8192 / L);
+	int Bmin = std::min(16, std::max(4, 256 / L));	// at least one warp per block
 
-	while ((B > 1) && ((nseq + B - 1) / B < 2 * 148))
+	while ((B > Bmin) && ((nseq + B - 1) / B < 2 * 148))
 		B /= 2;
 
-	return std::max(B, 1);
+	return B;
 }
+
+// opt in to large dynamic shared memory once per kernel and device
+static std::mutex g_attr_mutex;
+static std::map<std::pair<const void*, int>, bool> g_attr_done;
 
 template <typename K>
 static int prep_kernel(K kernel, size_t smem)
 {
-	if (smem > 48 * 1024)
-		CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	if (smem <= 48 * 1024)
+		return BNUFFT_OK;
 
+	int dev;
+	CUDA_TRY(cudaGetDevice(&dev));
+	auto key = std::make_pair((const void*)kernel, dev);
+	std::lock_guard<std::mutex> lock(g_attr_mutex);
+
+	if (g_attr_done.count(key))
+		return BNUFFT_OK;
+
+	CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+	g_attr_done[key] = true;
 	return BNUFFT_OK;
 }
 
-template <int L>
-static int launch_rows_fwd_L(const float2* img, const float2* maps, const float* ax, const float* ayz,
+template <int L, int B>
+static int launch_rows_fwd_LB(const float2* img, const float2* maps, const float* ax, const float* ayz,
 		int X, long YZ, long R, float2* out, cudaStream_t st)
 {
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
-	int B = choose_B(L, R);
 	size_t smem = pass_smem(L, B);
-	TRY(prep_kernel(k_rows_fwd<L>, smem));
+	TRY(prep_kernel(k_rows_fwd<L, B>, smem));
 	cudaEvent_t pe = prof_begin("rows_fwd", st);
-	k_rows_fwd<L><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(img, maps, ax, ayz, X, YZ, R, B, out, tw);
+	k_rows_fwd<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(img, maps, ax, ayz, X, YZ, R, out, tw);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
 }
 
-template <int L, int MODE>
-static int launch_cols_L(const float2* in, long ies, long ios, int n_in, int wrap_in,
+template <int L, int B, int MODE>
+static int launch_cols_LB(const float2* in, long ies, long ios, int n_in, int wrap_in,
 		float2* out, long oes, long oos, int n_out, int wrap_out, int W, long O,
-		const float2* psf, long pes, long pmod, long pos, cudaStream_t st)
+		const float2* psf, long pes, long pmod, long pos, const int* done, cudaStream_t st)
 {
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
-	int B = choose_B(L, (long)W * O);
-
-	while ((B > 1) && (B > W))
-		B /= 2;
-
 	size_t smem = pass_smem(L, B);
-	TRY(prep_kernel(k_cols<L, MODE>, smem));
+	TRY(prep_kernel(k_cols<L, B, MODE>, smem));
 
 	if (O > 65535)
 		return fail(BNUFFT_ERR_UNSUPPORTED, "column pass with %ld outer sequences", O);
 
 	dim3 grid((unsigned)((W + B - 1) / B), (unsigned)O);
 	cudaEvent_t pe = prof_begin((2 == MODE) ? "cols_toeplitz" : ((1 == MODE) ? "cols_inv" : "cols_fwd"), st);
-	k_cols<L, MODE><<<grid, B * L / 8, smem, st>>>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out,
-			W, B, psf, pes, pmod, pos, tw);
+	k_cols<L, B, MODE><<<grid, B * L / 8, smem, st>>>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out,
+			W, psf, pes, pmod, pos, tw, done);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
 }
 
-template <int L>
-static int launch_rows_inv_L(const float2* in, const float2* maps, const float* ax, const float* ayz,
-		int X, long YZ, int C, int cpg, float2* out, cudaStream_t st)
+template <int L, int B>
+static int launch_rows_inv_LB(const float2* in, const float2* maps, const float* ax, const float* ayz,
+		int X, long YZ, int C, int cpg, float2* out, const float2* pdot, double* dot_part, const int* done,
+		cudaStream_t st)
 {
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
 	int groups = (C + cpg - 1) / cpg;
-	int B = choose_B(L, YZ * groups);
 	size_t smem = pass_smem(L, B);
-	TRY(prep_kernel(k_rows_inv<L>, smem));
+	TRY(prep_kernel(k_rows_inv<L, B>, smem));
 	dim3 grid((unsigned)((YZ + B - 1) / B), (unsigned)groups);
 	cudaEvent_t pe = prof_begin("rows_inv", st);
-	k_rows_inv<L><<<grid, B * L / 8, smem, st>>>(in, maps, ax, ayz, X, YZ, C, cpg, B, out, tw);
+	k_rows_inv<L, B><<<grid, B * L / 8, smem, st>>>(in, maps, ax, ayz, X, YZ, C, cpg, out, tw, pdot, dot_part, done);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
 }
 
-#define DISPATCH_L(L, CALL) \
+template <int L, int B>
+static int launch_rows_fwd_cg_LB(const float2* bvec, const float2* r, const float2* p_prev, float2* p_cur,
+		const float2* maps, const float* ax, const float* ayz, int X, long YZ, long R, float2* out,
+		CgScalars* stt, int it, const double* rs_part, int nrs, double* pp_part, cudaStream_t st)
+{
+	const float2* tw;
+	TRY(get_twiddles(L, &tw));
+	size_t smem = pass_smem(L, B);
+	TRY(prep_kernel(k_rows_fwd_cg<L, B>, smem));
+	cudaEvent_t pe = prof_begin("rows_fwd", st);
+	k_rows_fwd_cg<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(bvec, r, p_prev, p_cur, maps, ax, ayz,
+			X, YZ, R, out, tw, stt, it, rs_part, nrs, pp_part);
+	prof_end(pe, st);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+// run CALL with compile-time LL (FFT length) and BB (sequences per block)
+#define DISPATCH_LB(L, B, CALL) \
 	switch (L) { \
-	case 16: { constexpr int LL = 16; return CALL; } \
-	case 32: { constexpr int LL = 32; return CALL; } \
-	case 64: { constexpr int LL = 64; return CALL; } \
-	case 128: { constexpr int LL = 128; return CALL; } \
-	case 256: { constexpr int LL = 256; return CALL; } \
-	case 512: { constexpr int LL = 512; return CALL; } \
-	case 1024: { constexpr int LL = 1024; return CALL; } \
-	case 2048: { constexpr int LL = 2048; return CALL; } \
+	case 16: { constexpr int LL = 16; DISPATCH_B(B, CALL) } \
+	case 32: { constexpr int LL = 32; DISPATCH_B(B, CALL) } \
+	case 64: { constexpr int LL = 64; DISPATCH_B(B, CALL) } \
+	case 128: { constexpr int LL = 128; DISPATCH_B(B, CALL) } \
+	case 256: { constexpr int LL = 256; DISPATCH_B(B, CALL) } \
+	case 512: { constexpr int LL = 512; DISPATCH_B(B, CALL) } \
+	case 1024: { constexpr int LL = 1024; DISPATCH_B(B, CALL) } \
+	case 2048: { constexpr int LL = 2048; DISPATCH_B(B, CALL) } \
 	default: return fail(BNUFFT_ERR_UNSUPPORTED, "FFT length %d (powers of two 16..2048 are built)", L); }
+
+#define DISPATCH_B(B, CALL) \
+	switch (B) { \
+	case 4: { constexpr int BB = 4; if constexpr (BB * LL / 8 <= 1024 && BB * LL / 8 >= 32) return CALL; break; } \
+	case 8: { constexpr int BB = 8; if constexpr (BB * LL / 8 <= 1024 && BB * LL / 8 >= 32) return CALL; break; } \
+	case 16: { constexpr int BB = 16; if constexpr (BB * LL / 8 <= 1024 && BB * LL / 8 >= 32) return CALL; break; } \
+	} \
+	return fail(BNUFFT_ERR_ARG, "no FFT pass instance for L=%d B=%d", L, B);
 
 static int rows_fwd(int L, const float2* img, const float2* maps, const float* ax, const float* ayz,
 		int X, long YZ, long R, float2* out, cudaStream_t st)
 {
-	DISPATCH_L(L, (launch_rows_fwd_L<LL>(img, maps, ax, ayz, X, YZ, R, out, st)));
+	int B = choose_B(L, R);
+	DISPATCH_LB(L, B, (launch_rows_fwd_LB<LL, BB>(img, maps, ax, ayz, X, YZ, R, out, st)));
 }
 
 static int cols(int L, int mode, const float2* in, long ies, long ios, int n_in, int wrap_in,
 		float2* out, long oes, long oos, int n_out, int wrap_out, int W, long O,
-		const float2* psf, long pes, long pmod, long pos, cudaStream_t st)
+		const float2* psf, long pes, long pmod, long pos, cudaStream_t st, const int* done = nullptr)
 {
+	int B = choose_B(L, (long)W * O);
+
+	while ((B > std::max(4, 256 / L)) && (B > W))
+		B /= 2;
+
 	if (0 == mode)
-		DISPATCH_L(L, (launch_cols_L<LL, 0>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, st)))
+		DISPATCH_LB(L, B, (launch_cols_LB<LL, BB, 0>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, done, st)))
 	else if (1 == mode)
-		DISPATCH_L(L, (launch_cols_L<LL, 1>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, st)))
+		DISPATCH_LB(L, B, (launch_cols_LB<LL, BB, 1>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, done, st)))
 	else
-		DISPATCH_L(L, (launch_cols_L<LL, 2>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, st)))
+		DISPATCH_LB(L, B, (launch_cols_LB<LL, BB, 2>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, done, st)))
 }
 
 static int rows_inv(int L, const float2* in, const float2* maps, const float* ax, const float* ayz,
-		int X, long YZ, int C, int cpg, float2* out, cudaStream_t st)
+		int X, long YZ, int C, int cpg, float2* out, cudaStream_t st,
+		const float2* pdot = nullptr, double* dot_part = nullptr, const int* done = nullptr, int* nblocks = nullptr)
 {
-	DISPATCH_L(L, (launch_rows_inv_L<LL>(in, maps, ax, ayz, X, YZ, C, cpg, out, st)));
+	int groups = (C + cpg - 1) / cpg;
+	int B = choose_B(L, YZ * groups);
+
+	if (nblocks)
+		*nblocks = (int)(((YZ + B - 1) / B) * groups);
+
+	DISPATCH_LB(L, B, (launch_rows_inv_LB<LL, BB>(in, maps, ax, ayz, X, YZ, C, cpg, out, pdot, dot_part, done, st)));
+}
+
+static int rows_fwd_cg(int L, const float2* bvec, const float2* r, const float2* p_prev, float2* p_cur,
+		const float2* maps, const float* ax, const float* ayz, int X, long YZ, long R, float2* out,
+		CgScalars* stt, int it, const double* rs_part, int nrs, double* pp_part, int* nblocks, cudaStream_t st)
+{
+	int B = choose_B(L, R);
+	*nblocks = (int)((R + B - 1) / B);
+	DISPATCH_LB(L, B, (launch_rows_fwd_cg_LB<LL, BB>(bvec, r, p_prev, p_cur, maps, ax, ayz, X, YZ, R, out,
+			stt, it, rs_part, nrs, pp_part, st)));
 }
 
 static unsigned vec_blocks(long n, int threads = RED_THREADS, int maxb = 4 * 148)
@@ -461,9 +533,44 @@ static int init_geom(Geom& g, const long dims3[3], long M, float os, float width
 	return BNUFFT_OK;
 }
 
+// roll-off tables of a geometry, cached per device (computed once on the host)
+struct RollKey {
+
+	int n[3];
+	float os, width;
+
+	bool operator<(const RollKey& o) const
+	{
+		return std::memcmp(this, &o, sizeof *this) < 0;
+	}
+};
+
+static std::map<std::pair<int, RollKey>, std::pair<float*, float*>> g_roll;
+
 static int init_rolloff(OpCtx& op, cudaStream_t st)
 {
 	const Geom& g = op.g;
+	RollKey key;
+	std::memset(&key, 0, sizeof key);
+
+	for (int i = 0; i < 3; i++)
+		key.n[i] = g.N[i];
+
+	key.os = g.os;
+	key.width = g.width;
+
+	int dev;
+	CUDA_TRY(cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lock(g_tab_mutex);
+	auto it = g_roll.find(std::make_pair(dev, key));
+
+	if (it != g_roll.end()) {
+
+		op.ax = it->second.first;
+		op.ayz = it->second.second;
+		return BNUFFT_OK;
+	}
+
 	double beta = kernel_beta(g.os, g.width);
 	double i0b = bessel_i0(beta);
 	std::vector<float> ax(g.N[0]);
@@ -478,21 +585,23 @@ static int init_rolloff(OpCtx& op, cudaStream_t st)
 			ayz[y + (size_t)g.N[1] * z] = (float)(rolloff_axis(g.N[1], y, g.os, g.width, beta, i0b)
 						* rolloff_axis(g.N[2], z, g.os, g.width, beta, i0b) * sc);
 
-	CUDA_TRY(cudaMallocAsync(&op.ax, sizeof(float) * ax.size(), st));
-	CUDA_TRY(cudaMallocAsync(&op.ayz, sizeof(float) * ayz.size(), st));
-	CUDA_TRY(cudaMemcpyAsync(op.ax, ax.data(), sizeof(float) * ax.size(), cudaMemcpyHostToDevice, st));
-	CUDA_TRY(cudaMemcpyAsync(op.ayz, ayz.data(), sizeof(float) * ayz.size(), cudaMemcpyHostToDevice, st));
-	CUDA_TRY(cudaStreamSynchronize(st));	// host vectors go out of scope
+	float* dax = nullptr;
+	float* dayz = nullptr;
+	CUDA_TRY(cudaMalloc(&dax, sizeof(float) * ax.size()));
+	CUDA_TRY(cudaMalloc(&dayz, sizeof(float) * ayz.size()));
+	CUDA_TRY(cudaMemcpy(dax, ax.data(), sizeof(float) * ax.size(), cudaMemcpyHostToDevice));
+	CUDA_TRY(cudaMemcpy(dayz, ayz.data(), sizeof(float) * ayz.size(), cudaMemcpyHostToDevice));
+	g_roll[std::make_pair(dev, key)] = std::make_pair(dax, dayz);
+	op.ax = dax;
+	op.ayz = dayz;
+	(void)st;
 	return BNUFFT_OK;
 }
 
-// image [N0, N1*N2, C] (maps: image [N0, N1*N2] times maps [.., C]) -> grid
-static int op_spectrum(OpCtx& op, const float2* img, const float2* maps, bool apod, long C, float2* grid, cudaStream_t st)
+// column passes of the forward spectrum: row-transformed t1 -> grid
+static int op_spectrum_cols(OpCtx& op, long C, float2* grid, cudaStream_t st)
 {
 	const Geom& g = op.g;
-	long YZ = (long)g.N[1] * g.N[2];
-
-	TRY(rows_fwd(g.G[0], img, maps, apod ? op.ax : nullptr, op.ayz, g.N[0], YZ, YZ * C, op.w.t1, st));
 
 	if (1 == g.G[1]) {	// 1D: row pass is the whole transform
 
@@ -515,9 +624,28 @@ static int op_spectrum(OpCtx& op, const float2* img, const float2* maps, bool ap
 			grid, plane, plane * g.G[2], g.G[2], 0, (int)plane, C, nullptr, 0, 1, 0, st);
 }
 
+// image [N0, N1*N2, C] (maps: image [N0, N1*N2] times maps [.., C]) -> grid
+static int op_spectrum(OpCtx& op, const float2* img, const float2* maps, bool apod, long C, float2* grid, cudaStream_t st)
+{
+	const Geom& g = op.g;
+	long YZ = (long)g.N[1] * g.N[2];
+
+	TRY(rows_fwd(g.G[0], img, maps, apod ? op.ax : nullptr, op.ayz, g.N[0], YZ, YZ * C, op.w.t1, st));
+	return op_spectrum_cols(op, C, grid, st);
+}
+
+// CG hooks of the final row pass: p for the partial p^H (partial sums)
+struct DotHook {
+
+	const float2* p = nullptr;
+	double* part = nullptr;
+	const int* done = nullptr;
+	int* nblocks = nullptr;
+};
+
 // grid -> image (maps: sum over coils into `groups` partials of [N0, N1*N2])
 static int op_spectrum_adjoint(OpCtx& op, const float2* grid, const float2* maps, bool apod, long C, int cpg,
-		float2* out, cudaStream_t st)
+		float2* out, cudaStream_t st, const DotHook& dh = DotHook())
 {
 	const Geom& g = op.g;
 	long YZ = (long)g.N[1] * g.N[2];
@@ -543,7 +671,8 @@ static int op_spectrum_adjoint(OpCtx& op, const float2* grid, const float2* maps
 		rows_in = op.w.t1;
 	}
 
-	return rows_inv(g.G[0], rows_in, maps, apod ? op.ax : nullptr, op.ayz, g.N[0], YZ, (int)C, maps ? cpg : 1, out, st);
+	return rows_inv(g.G[0], rows_in, maps, apod ? op.ax : nullptr, op.ayz, g.N[0], YZ, (int)C, maps ? cpg : 1, out, st,
+			dh.p, dh.part, dh.done, dh.nblocks);
 }
 
 static int degrid(OpCtx& op, const float2* grid, long C, float2* ksp, cudaStream_t st)
@@ -578,11 +707,34 @@ static int op_forward(OpCtx& op, const float2* cim, const float2* maps, long C, 
 }
 
 // adjoint NUFFT: ksp [M, C] -> cim [npix, C] (maps: partial coil sums)
-static int op_adjoint(OpCtx& op, const float2* ksp, const float2* maps, long C, int cpg, float2* out, cudaStream_t st)
+static int op_adjoint(OpCtx& op, const float2* ksp, const float2* maps, long C, int cpg, float2* out, cudaStream_t st,
+		const DotHook& dh = DotHook())
 {
 	TRY(alloc_work(op.w, op.g, C, st));
 	TRY(grid_adj(op, ksp, C, op.w.grid, st));
-	return op_spectrum_adjoint(op, op.w.grid, maps, true, C, cpg, out, st);
+	return op_spectrum_adjoint(op, op.w.grid, maps, true, C, cpg, out, st, dh);
+}
+
+// column passes of the Toeplitz product on the row-transformed t1 (in place)
+static int op_toeplitz_cols(OpCtx& op, const float2* psf, long C, cudaStream_t st, const int* done = nullptr)
+{
+	const Geom& g = op.g;
+
+	if (1 == g.G[1])
+		return fail(BNUFFT_ERR_UNSUPPORTED, "Toeplitz normal for 1D");
+
+	if (1 == g.G[2])
+		return cols(g.G[1], 2, op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1,
+				op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1, g.G[0], C, psf, g.G[0], 1, 0, st, done);
+
+	long plane = (long)g.G[0] * g.G[1];
+
+	TRY(cols(g.G[1], 0, op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1,
+			op.w.t2, g.G[0], plane, g.G[1], 0, g.G[0], (long)g.N[2] * C, nullptr, 0, 1, 0, st, done));
+	TRY(cols(g.G[2], 2, op.w.t2, plane, plane * g.N[2], g.N[2], 1,
+			op.w.t2, plane, plane * g.N[2], g.N[2], 1, (int)plane, C, psf, plane, 1, 0, st, done));
+	return cols(g.G[1], 1, op.w.t2, g.G[0], plane, g.G[1], 0,
+			op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1, g.G[0], (long)g.N[2] * C, nullptr, 0, 1, 0, st, done);
 }
 
 // Toeplitz normal: E^H (psf . E x) per coil (maps: partial coil sums)
@@ -593,28 +745,7 @@ static int op_toeplitz(OpCtx& op, const float2* psf, const float2* x, const floa
 	long YZ = (long)g.N[1] * g.N[2];
 	TRY(alloc_work(op.w, g, C, st));
 	TRY(rows_fwd(g.G[0], x, maps, nullptr, nullptr, g.N[0], YZ, YZ * C, op.w.t1, st));
-
-	if (1 == g.G[1]) {
-
-		return fail(BNUFFT_ERR_UNSUPPORTED, "Toeplitz normal for 1D");
-
-	} else if (1 == g.G[2]) {
-
-		TRY(cols(g.G[1], 2, op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1,
-				op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1, g.G[0], C, psf, g.G[0], 1, 0, st));
-
-	} else {
-
-		long plane = (long)g.G[0] * g.G[1];
-
-		TRY(cols(g.G[1], 0, op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1,
-				op.w.t2, g.G[0], plane, g.G[1], 0, g.G[0], (long)g.N[2] * C, nullptr, 0, 1, 0, st));
-		TRY(cols(g.G[2], 2, op.w.t2, plane, plane * g.N[2], g.N[2], 1,
-				op.w.t2, plane, plane * g.N[2], g.N[2], 1, (int)plane, C, psf, plane, 1, 0, st));
-		TRY(cols(g.G[1], 1, op.w.t2, g.G[0], plane, g.G[1], 0,
-				op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1, g.G[0], (long)g.N[2] * C, nullptr, 0, 1, 0, st));
-	}
-
+	TRY(op_toeplitz_cols(op, psf, C, st));
 	return rows_inv(g.G[0], op.w.t1, maps, nullptr, nullptr, g.N[0], YZ, (int)C, maps ? cpg : 1, out, st);
 }
 
@@ -683,8 +814,6 @@ static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, flo
 
 	free_work(full.w, st);
 	free_work(in.w, st);
-	cudaFreeAsync(in.ax, st);
-	cudaFreeAsync(in.ayz, st);
 	cudaFreeAsync(t2, st);
 	cudaFreeAsync(ones, st);
 	cudaFreeAsync(psft, st);
@@ -1052,13 +1181,10 @@ extern "C" void bnufft_free(bnufft_plan_t p)
 	cudaStream_t st = p->st0;
 	free_work(p->op.w, st);
 
-	if (p->op.ax) cudaFreeAsync(p->op.ax, st);
-	if (p->op.ayz) cudaFreeAsync(p->op.ayz, st);
 	if (p->traj) cudaFreeAsync(p->traj, st);
 	if (p->psf) cudaFreeAsync(p->psf, st);
 
-	cudaStreamSynchronize(st);
-	delete p;
+	delete p;	// device frees are stream-ordered; host state can go now
 }
 
 // ----------------------------------------------------------------------------
@@ -1073,14 +1199,17 @@ struct bnufft_pics_s {
 	int cpg, groups;
 	float2* sens = nullptr;		// [npix, C]
 	float2* part = nullptr;		// [npix, groups] coil-sum partials
-	float2 *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr, *b = nullptr;
+	float2 *x = nullptr, *r = nullptr, *b = nullptr;
+	float2* pbuf[2] = { nullptr, nullptr };	// search direction, alternating by iteration
 	float2* kbuf = nullptr;		// [M, C] (non-Toeplitz normal)
 	float* mag = nullptr;		// [npix] |adj|
 	float* mag_sorted = nullptr;
 	void* sort_tmp = nullptr;
 	size_t sort_tmp_bytes = 0;
-	double* pap_part = nullptr;
-	double* rs_part = nullptr;
+	double* pap_part = nullptr;	// p^H partial, one per final row-pass block
+	double* pp_part = nullptr;	// ||p||^2, one per first row-pass block
+	double* rs_part = nullptr;	// ||r||^2, one per CG step block
+	long max_row_blocks;
 	int nparts;
 	CgScalars* scal = nullptr;
 };
@@ -1177,12 +1306,15 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 	ck(cudaMallocAsync(&ps->part, sizeof(float2) * ps->npix * ps->groups, st));
 	ck(cudaMallocAsync(&ps->x, sizeof(float2) * ps->npix, st));
 	ck(cudaMallocAsync(&ps->r, sizeof(float2) * ps->npix, st));
-	ck(cudaMallocAsync(&ps->p, sizeof(float2) * ps->npix, st));
-	ck(cudaMallocAsync(&ps->Ap, sizeof(float2) * ps->npix, st));
+	ck(cudaMallocAsync(&ps->pbuf[0], sizeof(float2) * ps->npix, st));
+	ck(cudaMallocAsync(&ps->pbuf[1], sizeof(float2) * ps->npix, st));
 	ck(cudaMallocAsync(&ps->b, sizeof(float2) * ps->npix, st));
 	ck(cudaMallocAsync(&ps->mag, sizeof(float) * ps->npix, st));
 	ck(cudaMallocAsync(&ps->mag_sorted, sizeof(float) * ps->npix, st));
-	ck(cudaMallocAsync(&ps->pap_part, sizeof(double) * ps->nparts, st));
+	// row-pass blocks hold at least 4 rows: bounds for the partial arrays
+	ps->max_row_blocks = (YZ + 3) / 4 * ps->C + 1;
+	ck(cudaMallocAsync(&ps->pap_part, sizeof(double) * ps->max_row_blocks, st));
+	ck(cudaMallocAsync(&ps->pp_part, sizeof(double) * ps->max_row_blocks, st));
 	ck(cudaMallocAsync(&ps->rs_part, sizeof(double) * ps->nparts, st));
 	ck(cudaMallocAsync(&ps->scal, sizeof(CgScalars), st));
 
@@ -1204,7 +1336,7 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 
 			cudaError_t e = cudaMemcpyAsync(ps->sens, sm.dev, sizeof(float2) * ps->npix * ps->C, cudaMemcpyDeviceToDevice, st);
 
-			if (cudaSuccess == e)
+			if ((cudaSuccess == e) && sm.owned)	// staging buffer is freed on return
 				e = cudaStreamSynchronize(st);
 
 			if (cudaSuccess != e)
@@ -1272,23 +1404,59 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 	k_scale_dev<<<nb, RED_THREADS, 0, st>>>(ps->b, ps->b, ps->npix, &ps->scal->inv_scale);
 	LAUNCHED();
 
-	// CG from zero on (A^H A + lambda) x = b
-	k_cg_init<<<nb, RED_THREADS, 0, st>>>(x, ps->r, ps->p, ps->b, ps->npix, ps->rs_part);
+	// CG from zero on (A^H A + lambda) x = b; per iteration four passes:
+	// direction update fused into the first row pass, the normal operator's
+	// column passes, the final row pass with the p^H A p partials, and the
+	// x / r step with the ||r||^2 partials
+	k_cg_init<<<nb, RED_THREADS, 0, st>>>(x, ps->r, ps->pbuf[1], ps->b, ps->npix, ps->rs_part);
 	LAUNCHED();
 	k_cg_start<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->rs_part, ps->nparts, ps->conf.tol);
 	LAUNCHED();
 
+	const Geom& g = op.g;
+	long YZ = (long)g.N[1] * g.N[2];
+	const int* done = &ps->scal->done;
+	TRY(alloc_work(op.w, g, ps->C, st));
+
 	for (int it = 0; it < ps->conf.maxiter; it++) {
 
-		int parity = it & 1;
-		TRY(sense_normal(ps, ps->p, ps->Ap, ps->conf.lambda, ps->pap_part, &ps->scal->done, st));
-		k_cg_update<<<nb, RED_THREADS, 0, st>>>(x, ps->r, ps->p, ps->Ap, ps->npix, ps->scal, parity,
-				ps->pap_part, ps->nparts, ps->rs_part);
-		LAUNCHED();
-		k_cg_direction<<<nb, RED_THREADS, 0, st>>>(ps->p, ps->r, ps->npix, ps->scal, parity,
-				ps->pap_part, ps->nparts, ps->rs_part, ps->nparts);
+		float2* p_cur = ps->pbuf[it & 1];
+		const float2* p_prev = ps->pbuf[(it + 1) & 1];
+		bool toep = (nullptr != ps->nufft->psf);
+		int npp = 0, npap = 0;
+
+		TRY(rows_fwd_cg(g.G[0], ps->b, ps->r, p_prev, p_cur, ps->sens, toep ? nullptr : op.ax, op.ayz,
+				g.N[0], YZ, YZ * ps->C, op.w.t1, ps->scal, it, ps->rs_part, ps->nparts, ps->pp_part, &npp, st));
+
+		DotHook dh;
+		dh.p = p_cur;
+		dh.part = ps->pap_part;
+		dh.done = done;
+		dh.nblocks = &npap;
+
+		if (toep) {
+
+			TRY(op_toeplitz_cols(op, ps->nufft->psf, ps->C, st, done));
+			TRY(rows_inv(g.G[0], op.w.t1, ps->sens, nullptr, nullptr, g.N[0], YZ, (int)ps->C, ps->cpg, ps->part, st,
+					dh.p, dh.part, dh.done, dh.nblocks));
+
+		} else {
+
+			TRY(op_spectrum_cols(op, ps->C, op.w.grid, st));
+			TRY(degrid(op, op.w.grid, ps->C, ps->kbuf, st));
+			TRY(op_adjoint(op, ps->kbuf, ps->sens, ps->C, ps->cpg, ps->part, st, dh));
+		}
+
+		if ((npp > ps->max_row_blocks) || (npap > ps->max_row_blocks))
+			return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
+
+		k_cg_step<<<nb, RED_THREADS, 0, st>>>(x, ps->r, p_cur, ps->part, ps->groups, ps->npix, ps->conf.lambda,
+				ps->scal, it, ps->pap_part, npap, ps->pp_part, npp, ps->rs_part);
 		LAUNCHED();
 	}
+
+	k_cg_finish<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->conf.maxiter, ps->rs_part, ps->nparts);
+	LAUNCHED();
 
 	if (ps->conf.rescale) {
 
@@ -1309,7 +1477,7 @@ extern "C" int bnufft_pics_stats(bnufft_pics_t ps, int* iters, double* rel_resid
 		*iters = h.iters;
 
 	if (rel_resid)
-		*rel_resid = (h.b2 > 0.) ? sqrt(h.rs[h.iters & 1] / h.b2) : 0.;
+		*rel_resid = (h.b2 > 0.) ? sqrt(h.rs[h.iters & 1] / h.b2) : 0.;	// rs of the last completed iteration
 
 	if (scaling)
 		*scaling = h.scale;
@@ -1323,8 +1491,8 @@ extern "C" void bnufft_pics_free(bnufft_pics_t ps)
 		return;
 
 	cudaStream_t st = ps->nufft ? ps->nufft->st0 : nullptr;
-	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->p, ps->Ap, ps->b, ps->kbuf, ps->mag, ps->mag_sorted,
-			 ps->sort_tmp, ps->pap_part, ps->rs_part, ps->scal };
+	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->pbuf[0], ps->pbuf[1], ps->b, ps->kbuf, ps->mag, ps->mag_sorted,
+			 ps->sort_tmp, ps->pap_part, ps->pp_part, ps->rs_part, ps->scal };
 
 	for (void* b : bufs)
 		if (b)

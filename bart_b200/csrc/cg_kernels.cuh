@@ -11,22 +11,11 @@
 #include <cuda_runtime.h>
 
 #include "fft_core.cuh"
+#include "nufft_kernels.cuh"
 
 namespace bn {
 
 enum { RED_THREADS = 256 };
-
-// device-side CG state
-struct CgScalars {
-
-	double rs[2];		// ||r||^2, double-buffered by iteration parity
-	double eps2;		// stop when ||r||^2 <= eps2
-	double b2;		// ||A^H y||^2
-	int done;		// set once converged (or pAp == 0)
-	int iters;		// iterations completed
-	float scale;		// data scaling used
-	float inv_scale;	// float(1 / scale)
-};
 
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T* sh)
@@ -55,28 +44,9 @@ __device__ __forceinline__ T block_sum(T v, T* sh)
 	return r;	// valid in thread 0
 }
 
-// fixed-order sum of n partials, identical in every block
 __device__ __forceinline__ double sum_partials(const double* part, int n, double* sh)
 {
-	double v = 0.;
-
-	for (int i = threadIdx.x; i < n; i += blockDim.x)
-		v += part[i];
-
-	double r = block_sum(v, sh);
-
-	__syncthreads();
-
-	if (0 == threadIdx.x)
-		sh[0] = r;
-
-	__syncthreads();
-
-	double out = sh[0];
-
-	__syncthreads();
-
-	return out;
+	return sum_partials_d(part, n, sh);
 }
 
 // dst[i] = sum_g part[i + n*g] (+ lam * x[i]); optional per-block partial of
@@ -157,30 +127,47 @@ __global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float 
 	}
 }
 
-// alpha = rs_old / pAp; x += alpha p; r -= alpha Ap; partial ||r||^2.
-__global__ void k_cg_update(float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
-		const float2* __restrict__ Ap, long n, CgScalars* st, int parity,
-		const double* __restrict__ pap_part, int nparts, double* __restrict__ rs_part)
+// Second step of a CG iteration: p^H (A^H A + lambda) p from the partials of
+// the last row pass and of ||p||^2; alpha = rs / p^H A p (float64); then per
+// element Ap = sum_g part_g + lambda p, x += alpha p, r -= alpha Ap, and
+// partial ||r||^2 for the next iteration's direction update.
+__global__ void k_cg_step(float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
+		const float2* __restrict__ part, int groups, long n, float lam, CgScalars* st, int it,
+		const double* __restrict__ pap_part, int npap, const double* __restrict__ pp_part, int npp,
+		double* __restrict__ rs_part)
 {
 	__shared__ double sh[32];
 
 	if (st->done)
 		return;
 
-	double pAp = sum_partials(pap_part, nparts, sh);
+	double pAp = sum_partials(pap_part, npap, sh) + (double)lam * sum_partials(pp_part, npp, sh);
 
-	if (0. == pAp)
-		return;	// the direction step below marks the solve done
+	if (0. == pAp) {
 
-	// alpha in float64 (the reference rounds rsold/pAp to float)
-	double alpha = st->rs[parity] / pAp;
-	float a = (float)alpha;
+		if ((0 == blockIdx.x) && (0 == threadIdx.x)) {
+
+			st->done = 1;
+			st->iters = it;
+		}
+
+		return;
+	}
+
+	float a = (float)(st->rs[it & 1] / pAp);
 	double acc = 0.;
 
 	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
 
 		float2 pv = p[i];
-		float2 av = Ap[i];
+		float2 av = part[i];
+
+		for (int g = 1; g < groups; g++)
+			av = cadd(av, part[i + n * g]);
+
+		av.x = fmaf(lam, pv.x, av.x);
+		av.y = fmaf(lam, pv.y, av.y);
+
 		float2 xv = x[i];
 		float2 rv = r[i];
 		xv.x = fmaf(a, pv.x, xv.x);
@@ -198,53 +185,20 @@ __global__ void k_cg_update(float2* __restrict__ x, float2* __restrict__ r, cons
 		rs_part[blockIdx.x] = s;
 }
 
-// rs_new = ||r||^2; beta = rs_new / rs_old; p = r + beta p (unless converged).
-__global__ void k_cg_direction(float2* __restrict__ p, const float2* __restrict__ r, long n,
-		CgScalars* st, int parity, const double* __restrict__ pap_part, int npap,
-		const double* __restrict__ rs_part, int nparts)
+// after the last iteration: ||r||^2 and the iteration count
+__global__ void k_cg_finish(CgScalars* st, int maxiter, const double* rs_part, int nrs)
 {
 	__shared__ double sh[32];
 
 	if (st->done)
 		return;
 
-	double pAp = sum_partials(pap_part, npap, sh);
+	double rs = sum_partials(rs_part, nrs, sh);
 
-	if (0. == pAp) {
+	if (0 == threadIdx.x) {
 
-		__syncthreads();
-
-		if ((0 == blockIdx.x) && (0 == threadIdx.x))
-			st->done = 1;
-
-		return;
-	}
-
-	double rs_new = sum_partials(rs_part, nparts, sh);
-	double rs_old = st->rs[parity];
-	bool stop = (rs_new <= st->eps2);
-
-	if (!stop) {
-
-		float beta = (float)(rs_new / rs_old);
-
-		for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-
-			float2 pv = p[i];
-			float2 rv = r[i];
-			pv.x = fmaf(beta, pv.x, rv.x);
-			pv.y = fmaf(beta, pv.y, rv.y);
-			p[i] = pv;
-		}
-	}
-
-	if ((0 == blockIdx.x) && (0 == threadIdx.x)) {
-
-		st->rs[parity ^ 1] = rs_new;
-		st->iters += 1;
-
-		if (stop)
-			st->done = 1;
+		st->rs[maxiter & 1] = rs;
+		st->iters = maxiter;
 	}
 }
 

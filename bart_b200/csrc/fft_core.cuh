@@ -1,16 +1,24 @@
 // Shared-memory Stockham FFT core for sm_100a.
 //
-// A thread block transforms B sequences of length L (power of two, 16..2048)
-// held in shared memory as s[p * SB + b] (element p of sequence b; SB = B|1 so
-// that the element stride is odd and 8-byte accesses of a half-warp hit
-// distinct banks). Each sequence is served by L/8 threads; one radix-8 (or a
-// final radix-4/2) butterfly per thread per stage, autosorting (Stockham), so
-// the result lands in natural order without a bit-reversal pass.
+// A thread block transforms B sequences of length L (power of two, 16..2048).
+// Each sequence is served by T = L/8 threads; thread t of the block works on
+// sequence b = t % B with index jt = t / B. Between stages the data lives in
+// shared memory as s[p * SB + b] (element p of sequence b; SB = B|1 keeps the
+// element stride odd so that 8-byte accesses of a half-warp hit distinct
+// banks). Stages are radix 8 with a final radix 4 or 2 (Stockham autosort, so
+// the result is in natural order without a bit-reversal pass).
 //
-// Forward = exp(-2 pi i jk / L), inverse = exp(+2 pi i jk / L), both
-// unnormalised, as FFTW's / the reference's FFT (src/num/fft_plan.c:227).
-// Twiddles come from a table tw[m] = exp(-2 pi i m / L) computed on the host
-// in float64, so the transform is accurate to a few float32 ulps.
+// Register ownership: before the first stage and after the last stage a
+// thread holds the eight elements at positions jt + T*m (m = 0..7) in
+// v[m]. The first stage reads exactly these positions and the last stage
+// writes them, so the caller loads stage-1 input straight from global memory
+// and consumes the last-stage output in registers (e.g. the Toeplitz PSF
+// product between a forward and an inverse transform needs no shared-memory
+// pass at all).
+//
+// Forward = exp(-2 pi i jk / L), inverse = exp(+2 pi i jk / L), unnormalised,
+// as FFTW's / the reference's FFT (src/num/fft_plan.c:227). Twiddles come
+// from a table tw[m] = exp(-2 pi i m / L) computed on the host in float64.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -94,71 +102,108 @@ __device__ __forceinline__ void butterfly(float2* v)
 		dft2<INV>(v);
 }
 
-// One Stockham stage per recursion level; Ns = product of the radices done.
-template <int L, int Ns, bool INV>
-__device__ __forceinline__ void fft_stages(float2* s, int SB, int b, int jt, const float2* tw)
+template <int L>
+struct FftShape {
+
+	static_assert(L >= 16 && L <= 2048 && (L & (L - 1)) == 0, "power-of-two length 16..2048");
+	static constexpr int T = L / 8;		// threads per sequence
+};
+
+// twiddle v[i] *= w^(i*k), w = exp(-+2 pi i / (Ns*R)), from tw[m] = exp(-2 pi i m / L)
+template <int L, int Ns, int R, bool INV>
+__device__ __forceinline__ void twiddle(float2* v, int k, const float2* tw)
 {
-	if constexpr (Ns < L) {
-
-		constexpr int REM = L / Ns;
-		constexpr int R = (REM >= 8) ? 8 : REM;
-		constexpr int NB = L / R;	// butterflies per sequence
-		constexpr int T = L / 8;	// threads per sequence
-		constexpr int PER = NB / T;	// butterflies per thread this stage
-
-		float2 v[PER][R];
-
+	if constexpr (Ns > 1) {
 #pragma unroll
-		for (int q = 0; q < PER; q++) {
+		for (int i = 1; i < R; i++) {
 
-			int j = jt + q * T;
-#pragma unroll
-			for (int i = 0; i < R; i++)
-				v[q][i] = s[(j + i * NB) * SB + b];
+			float2 w = tw[i * k * (L / (Ns * R))];
+
+			if (INV)
+				w.y = -w.y;
+
+			v[i] = cmul(v[i], w);
 		}
+	}
+}
 
+// Stage with Ns = product of earlier radices, Ns > 1, smem -> smem
+// (middle stages), or smem -> registers (last stage, LAST = true).
+template <int L, int B, int Ns, bool INV>
+__device__ __forceinline__ void fft_tail(float2 (&v)[8], float2* s, int b, int jt, const float2* tw)
+{
+	constexpr int SB = B | 1;
+	constexpr int REM = L / Ns;
+	constexpr int R = (REM >= 8) ? 8 : REM;
+	constexpr int NB = L / R;
+	constexpr int T = L / 8;
+	constexpr int PER = NB / T;
+	constexpr bool LAST = (Ns * R == L);
+
+	float2 u[PER][R];
+
+#pragma unroll
+	for (int q = 0; q < PER; q++) {
+#pragma unroll
+		for (int i = 0; i < R; i++)
+			u[q][i] = s[(jt + q * T + i * NB) * SB + b];
+	}
+
+	if constexpr (!LAST)
 		__syncthreads();
 
 #pragma unroll
-		for (int q = 0; q < PER; q++) {
+	for (int q = 0; q < PER; q++) {
 
-			int j = jt + q * T;
-			int k = j & (Ns - 1);
+		int j = jt + q * T;
+		int k = j % Ns;
+		twiddle<L, Ns, R, INV>(u[q], k, tw);
+		butterfly<R, INV>(u[q]);
 
-			if constexpr (Ns > 1) {
+		if constexpr (LAST) {
+			// outputs at j + NB*i = jt + T*(q + PER*i)
 #pragma unroll
-				for (int i = 1; i < R; i++) {
+			for (int i = 0; i < R; i++)
+				v[q + PER * i] = u[q][i];
 
-					float2 w = tw[i * k * (L / (Ns * R))];
-					if (INV)
-						w.y = -w.y;
-					v[q][i] = cmul(v[q][i], w);
-				}
-			}
-
-			butterfly<R, INV>(v[q]);
+		} else {
 
 			int idxD = (j / Ns) * Ns * R + k;
 #pragma unroll
 			for (int i = 0; i < R; i++)
-				s[(idxD + i * Ns) * SB + b] = v[q][i];
+				s[(idxD + i * Ns) * SB + b] = u[q][i];
 		}
+	}
+
+	if constexpr (!LAST) {
 
 		__syncthreads();
-
-		fft_stages<L, Ns * R, INV>(s, SB, b, jt, tw);
+		fft_tail<L, B, Ns * R, INV>(v, s, b, jt, tw);
 	}
 }
 
-// Transform all B sequences in s. Must be called by exactly B * L / 8 threads
-// (the whole block), thread t serving sequence t % B.
-template <int L, bool INV>
-__device__ __forceinline__ void fft_block(float2* s, int SB, int B, const float2* tw)
+// Full transform of the register set v (positions jt + T*m in, same out).
+// Begins with a barrier, so the caller may have been reading s just before.
+template <int L, int B, bool INV>
+__device__ __forceinline__ void fft_regs(float2 (&v)[8], float2* s, const float2* tw)
 {
-	static_assert(L >= 16 && (L & (L - 1)) == 0, "power-of-two length >= 16");
-	int b = threadIdx.x % B;
-	int jt = threadIdx.x / B;
-	fft_stages<L, 1, INV>(s, SB, b, jt, tw);
+	constexpr int SB = B | 1;
+	const int b = threadIdx.x % B;
+	const int jt = threadIdx.x / B;
+
+	// stage 1 (Ns = 1, radix 8, no twiddles): registers -> smem at 8*jt + i
+	butterfly<8, INV>(v);
+	__syncthreads();
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+		s[(8 * jt + i) * SB + b] = v[i];
+	__syncthreads();
+
+	fft_tail<L, B, 8, INV>(v, s, b, jt, tw);
 }
+
+// stage-1 position of register m for this thread
+template <int L, int B>
+__device__ __forceinline__ int reg_pos(int m) { return threadIdx.x / B + (L / 8) * m; }
 
 } // namespace bn

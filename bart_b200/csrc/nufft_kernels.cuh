@@ -41,32 +41,222 @@ __device__ __forceinline__ int unwrap_pos(int p, int n_in, int L)
 	return (n >= L) ? n - L : n;
 }
 
+// float64 block reduction; the result is valid in thread 0. blockDim.x must be
+// a multiple of 32.
+__device__ __forceinline__ double block_sum_d(double v, double* sh)
+{
+	for (int o = 16; o > 0; o >>= 1)
+		v += __shfl_down_sync(0xffffffffu, v, o);
+
+	__syncthreads();
+
+	if (0 == threadIdx.x % 32)
+		sh[threadIdx.x / 32] = v;
+
+	__syncthreads();
+
+	double r = 0.;
+
+	if (threadIdx.x < 32) {
+
+		r = (threadIdx.x < blockDim.x / 32) ? sh[threadIdx.x] : 0.;
+
+		for (int o = 16; o > 0; o >>= 1)
+			r += __shfl_down_sync(0xffffffffu, r, o);
+	}
+
+	return r;
+}
+
+// fixed-order sum of n float64 partials, the same value in every thread
+__device__ __forceinline__ double sum_partials_d(const double* part, int n, double* sh)
+{
+	double v = 0.;
+
+	for (int i = threadIdx.x; i < n; i += blockDim.x)
+		v += part[i];
+
+	double r = block_sum_d(v, sh);
+
+	if (0 == threadIdx.x)
+		sh[0] = r;
+
+	__syncthreads();
+	r = sh[0];
+	__syncthreads();
+	return r;
+}
+
+// device-side state of the CG solve
+struct CgScalars {
+
+	double rs[2];		// ||r||^2 of iteration it in rs[it & 1]
+	double eps2;		// stop when ||r||^2 <= eps2
+	double b2;		// ||A^H y||^2
+	int done;		// set once converged (or p^H A p == 0)
+	int iters;		// iterations completed
+	float scale;		// data scaling used
+	float inv_scale;	// float(1 / scale)
+};
+
+// Row pass, forward, first step of a CG iteration (conjgrad,
+// src/iter/italgos.c:538-566, reordered so that the direction update of the
+// previous iteration happens while loading):
+//   it == 0: p = b;  else: rs = ||r||^2 (from the update's partials),
+//   stop if rs <= eps2, beta = rs / rs_prev, p = r + beta p_prev.
+// Rows of coil 0 write p and the partial ||p||^2 (for lambda ||p||^2 in
+// p^H (A^H A + lambda) p); every row multiplies by its coil's map and runs the
+// forward transform like k_rows_fwd.
+template <int L, int B>
+__global__ void __launch_bounds__(B * L / 8) k_rows_fwd_cg(const float2* __restrict__ bvec, const float2* __restrict__ r,
+		const float2* __restrict__ p_prev, float2* __restrict__ p_cur, const float2* __restrict__ maps,
+		const float* __restrict__ ax, const float* __restrict__ ayz,
+		int X, long YZ, long R, float2* __restrict__ out, const float2* __restrict__ twg,
+		CgScalars* st, int it, const double* __restrict__ rs_part, int nrs, double* __restrict__ pp_part)
+{
+	constexpr int SB = B | 1;
+	constexpr int NT = B * L / 8;
+	extern __shared__ float2 smem[];
+	__shared__ double red[32];
+	float2* s = smem;
+	float2* tw = smem + L * SB;
+
+	if (st->done)
+		return;
+
+	float beta = 0.f;
+
+	if (it > 0) {
+
+		double rs = sum_partials_d(rs_part, nrs, red);
+		double rs_prev = st->rs[(it - 1) & 1];
+		bool stop = (rs <= st->eps2);
+
+		if (0 == blockIdx.x && 0 == threadIdx.x) {
+
+			st->rs[it & 1] = rs;
+
+			if (stop) {
+
+				st->done = 1;
+				st->iters = it;
+			}
+		}
+
+		if (stop)
+			return;
+
+		beta = (float)(rs / rs_prev);
+	}
+
+	for (int i = threadIdx.x; i < L; i += NT)
+		tw[i] = twg[i];
+
+	const long r0 = (long)blockIdx.x * B;
+	double pp = 0.;
+
+	for (int e = threadIdx.x; e < L * B; e += NT) {
+
+		int b = e / L;
+		int q = e % L;
+		long row = r0 + b;
+		int n = unwrap_pos(q, X, L);
+		float2 v = make_float2(0.f, 0.f);
+
+		if ((n < X) && (row < R)) {
+
+			long yz = row % YZ;
+			long c = row / YZ;
+			long i = n + X * yz;
+			float2 pv;
+
+			if (0 == it) {
+
+				pv = bvec[i];
+
+			} else {
+
+				float2 rv = r[i];
+				float2 po = p_prev[i];
+				pv.x = fmaf(beta, po.x, rv.x);
+				pv.y = fmaf(beta, po.y, rv.y);
+			}
+
+			if (0 == c) {
+
+				p_cur[i] = pv;
+				pp += (double)pv.x * (double)pv.x + (double)pv.y * (double)pv.y;
+			}
+
+			v = cmul(pv, maps[i + X * YZ * c]);
+
+			if (ax)
+				v = cscale(v, ax[n] * ayz[yz]);
+		}
+
+		s[q * SB + b] = v;
+	}
+
+	double t = block_sum_d(pp, red);
+
+	if (0 == threadIdx.x)
+		pp_part[blockIdx.x] = t;
+
+	__syncthreads();
+
+	float2 v[8];
+	const int b = threadIdx.x % B;
+#pragma unroll
+	for (int m = 0; m < 8; m++)
+		v[m] = s[reg_pos<L, B>(m) * SB + b];
+
+	fft_regs<L, B, false>(v, s, tw);
+
+	__syncthreads();
+#pragma unroll
+	for (int m = 0; m < 8; m++)
+		s[reg_pos<L, B>(m) * SB + b] = v[m];
+	__syncthreads();
+
+	for (int e = threadIdx.x; e < L * B; e += NT) {
+
+		int b = e / L;
+		int q = e % L;
+		long row = r0 + b;
+
+		if (row < R)
+			out[q + (long)L * row] = s[q * SB + b];
+	}
+}
+
 // Row pass, forward ----------------------------------------------------------
 //
 // Rows r in [0, R): yz = r % YZ, c = r / YZ. Input row x in [0, X):
 //   v = img[x + X*yz (+ X*YZ*c unless maps)] (* maps[x + X*yz + X*YZ*c])
 //       * ax[x] * ayz[yz]                          (apodisation, optional)
 // placed at wrap_pos(x, X, L), transformed, written to out[p + L*r].
-// One block: B rows, B*L/8 threads.
-template <int L>
-__global__ void __launch_bounds__(1024) k_rows_fwd(const float2* __restrict__ img, const float2* __restrict__ maps,
+// One block: B rows, B*L/8 threads. Global traffic is staged through shared
+// memory so that loads and stores run along the contiguous rows.
+template <int L, int B>
+__global__ void __launch_bounds__(B * L / 8) k_rows_fwd(const float2* __restrict__ img, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
-		int X, long YZ, long R, int B, float2* __restrict__ out, const float2* __restrict__ twg)
+		int X, long YZ, long R, float2* __restrict__ out, const float2* __restrict__ twg)
 {
+	constexpr int SB = B | 1;
+	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
-	const int SB = smem_stride(B);
 	float2* s = smem;
 	float2* tw = smem + L * SB;
 
-	for (int i = threadIdx.x; i < L; i += blockDim.x)
+	for (int i = threadIdx.x; i < L; i += NT)
 		tw[i] = twg[i];
 
 	const long r0 = (long)blockIdx.x * B;
 
-	for (int e = threadIdx.x; e < L * B; e += blockDim.x) {
+	for (int e = threadIdx.x; e < L * B; e += NT) {
 
 		int b = e / L;
-		int p = e - b * L;
+		int p = e % L;
 		long r = r0 + b;
 		int n = unwrap_pos(p, X, L);
 		float2 v = make_float2(0.f, 0.f);
@@ -94,12 +284,24 @@ __global__ void __launch_bounds__(1024) k_rows_fwd(const float2* __restrict__ im
 
 	__syncthreads();
 
-	fft_block<L, false>(s, SB, B, tw);
+	float2 v[8];
+	const int b = threadIdx.x % B;
+#pragma unroll
+	for (int m = 0; m < 8; m++)
+		v[m] = s[reg_pos<L, B>(m) * SB + b];
 
-	for (int e = threadIdx.x; e < L * B; e += blockDim.x) {
+	fft_regs<L, B, false>(v, s, tw);
+
+	__syncthreads();
+#pragma unroll
+	for (int m = 0; m < 8; m++)
+		s[reg_pos<L, B>(m) * SB + b] = v[m];
+	__syncthreads();
+
+	for (int e = threadIdx.x; e < L * B; e += NT) {
 
 		int b = e / L;
-		int p = e - b * L;
+		int p = e % L;
 		long r = r0 + b;
 
 		if (r < R)
@@ -117,76 +319,74 @@ __global__ void __launch_bounds__(1024) k_rows_fwd(const float2* __restrict__ im
 // when wrap_out, else n', and written to out[cx + n'*oes + o*oos].
 // psf element for position p: psf[cx + p*pes + (o % pmod)*pos].
 // One block: B columns of one outer index, B*L/8 threads; grid (ceil(W/B), O).
-template <int L, int MODE>
-__global__ void __launch_bounds__(1024) k_cols(const float2* __restrict__ in, long ies, long ios, int n_in, int wrap_in,
+// Global loads go straight into the first FFT stage's registers and results
+// leave from the last stage's registers (B consecutive columns per access).
+template <int L, int B, int MODE>
+__global__ void __launch_bounds__(B * L / 8) k_cols(const float2* __restrict__ in, long ies, long ios, int n_in, int wrap_in,
 		float2* __restrict__ out, long oes, long oos, int n_out, int wrap_out,
-		int W, int B, const float2* __restrict__ psf, long pes, long pmod, long pos,
-		const float2* __restrict__ twg)
+		int W, const float2* __restrict__ psf, long pes, long pmod, long pos,
+		const float2* __restrict__ twg, const int* done)
 {
+	constexpr int SB = B | 1;
+	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
-	const int SB = smem_stride(B);
 	float2* s = smem;
 	float2* tw = smem + L * SB;
 
-	for (int i = threadIdx.x; i < L; i += blockDim.x)
+	if (done && *done)
+		return;
+
+	for (int i = threadIdx.x; i < L; i += NT)
 		tw[i] = twg[i];
 
-	const int cx0 = blockIdx.x * B;
+	const int b = threadIdx.x % B;
+	const int cx = blockIdx.x * B + b;
+	const bool valid = (cx < W);
 	const long o = blockIdx.y;
-	const float2* inp = in + o * ios + cx0;
+	const float2* inp = in + o * ios + cx;
 
-	for (int e = threadIdx.x; e < L * B; e += blockDim.x) {
+	float2 v[8];
+#pragma unroll
+	for (int m = 0; m < 8; m++) {
 
-		int p = e / B;
-		int b = e - p * B;
+		int p = reg_pos<L, B>(m);
 		int n = wrap_in ? unwrap_pos(p, n_in, L) : p;
-		float2 v = make_float2(0.f, 0.f);
-
-		if ((n < n_in) && (cx0 + b < W))
-			v = inp[b + n * ies];
-
-		s[p * SB + b] = v;
+		v[m] = (valid && (n < n_in)) ? inp[n * ies] : make_float2(0.f, 0.f);
 	}
 
-	__syncthreads();
-
+	// the twiddle table must be complete before the first stage reads it
 	if constexpr (MODE == 1) {
 
-		fft_block<L, true>(s, SB, B, tw);
+		fft_regs<L, B, true>(v, s, tw);
 
 	} else {
 
-		fft_block<L, false>(s, SB, B, tw);
+		fft_regs<L, B, false>(v, s, tw);
 	}
 
 	if constexpr (MODE == 2) {
 
-		const float2* pp = psf + (o % pmod) * pos + cx0;
+		const float2* pp = psf + (o % pmod) * pos + cx;
+#pragma unroll
+		for (int m = 0; m < 8; m++)
+			if (valid)
+				v[m] = cmul(v[m], pp[reg_pos<L, B>(m) * pes]);
 
-		for (int e = threadIdx.x; e < L * B; e += blockDim.x) {
-
-			int p = e / B;
-			int b = e - p * B;
-
-			if (cx0 + b < W)
-				s[p * SB + b] = cmul(s[p * SB + b], pp[b + p * pes]);
-		}
-
-		__syncthreads();
-
-		fft_block<L, true>(s, SB, B, tw);
+		fft_regs<L, B, true>(v, s, tw);
 	}
 
-	float2* outp = out + o * oos + cx0;
+	float2* outp = out + o * oos + cx;
 
-	for (int e = threadIdx.x; e < n_out * B; e += blockDim.x) {
+	if (valid) {
+#pragma unroll
+		for (int m = 0; m < 8; m++) {
 
-		int n = e / B;
-		int b = e - n * B;
-		int p = wrap_out ? wrap_pos(n, n_out, L) : n;
+			int p = reg_pos<L, B>(m);
+			int n = wrap_out ? unwrap_pos(p, n_out, L) : p;
 
-		if (cx0 + b < W)
-			outp[b + n * oes] = s[p * SB + b];
+			if (n < n_out)
+				outp[n * oes] = v[m];
+		}
 	}
 }
 
@@ -199,99 +399,134 @@ __global__ void __launch_bounds__(1024) k_cols(const float2* __restrict__ in, lo
 //              into out[x + X*yz + X*YZ*g] (g = blockIdx.y, partial per group)
 //   maps == 0: write out[x + X*yz + X*YZ*c] per coil.
 // grid (ceil(YZ/B), groups); coils per group cpg.
-template <int L>
-__global__ void __launch_bounds__(1024) k_rows_inv(const float2* __restrict__ in, const float2* __restrict__ maps,
+template <int L, int B>
+__global__ void __launch_bounds__(B * L / 8) k_rows_inv(const float2* __restrict__ in, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
-		int X, long YZ, int C, int cpg, int B, float2* __restrict__ out, const float2* __restrict__ twg)
+		int X, long YZ, int C, int cpg, float2* __restrict__ out, const float2* __restrict__ twg,
+		const float2* __restrict__ pdot, double* __restrict__ dot_part, const int* done)
 {
+	constexpr int SB = B | 1;
+	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
-	const int SB = smem_stride(B);
+	__shared__ double red[32];
 	float2* s = smem;
 	float2* tw = smem + L * SB;
 
-	for (int i = threadIdx.x; i < L; i += blockDim.x)
+	if (done && *done)
+		return;
+
+	for (int i = threadIdx.x; i < L; i += NT)
 		tw[i] = twg[i];
 
 	const long yz0 = (long)blockIdx.x * B;
 	const int g = blockIdx.y;
 	const int c0 = g * cpg;
 	const int c1 = min(C, c0 + cpg);
+	const int b = threadIdx.x % B;
 
-	// each thread owns up to OWN output elements (x, b) across the coil loop
-	constexpr int OWN = 8;
-	float2 acc[OWN];
+	// each thread owns output elements e = tid + k*NT (X*B <= 8*NT)
+	float2 acc[8];
 #pragma unroll
-	for (int k = 0; k < OWN; k++)
+	for (int k = 0; k < 8; k++)
 		acc[k] = make_float2(0.f, 0.f);
 
 	for (int c = c0; c < c1; c++) {
 
-		for (int e = threadIdx.x; e < L * B; e += blockDim.x) {
+		__syncthreads();	// previous coil's readers are done with s
 
-			int b = e / L;
-			int p = e - b * L;
-			long yz = yz0 + b;
+		for (int e = threadIdx.x; e < L * B; e += NT) {
+
+			int bb = e / L;
+			int p = e % L;
+			long yz = yz0 + bb;
 			float2 v = make_float2(0.f, 0.f);
 
 			if (yz < YZ)
 				v = in[p + (long)L * (yz + YZ * c)];
 
-			s[p * SB + b] = v;
+			s[p * SB + bb] = v;
 		}
 
 		__syncthreads();
 
-		fft_block<L, true>(s, SB, B, tw);
+		float2 v[8];
+#pragma unroll
+		for (int m = 0; m < 8; m++)
+			v[m] = s[reg_pos<L, B>(m) * SB + b];
+
+		fft_regs<L, B, true>(v, s, tw);
+
+		__syncthreads();
+#pragma unroll
+		for (int m = 0; m < 8; m++)
+			s[reg_pos<L, B>(m) * SB + b] = v[m];
+		__syncthreads();
 
 #pragma unroll
-		for (int k = 0; k < OWN; k++) {
+		for (int k = 0; k < 8; k++) {
 
-			int e = threadIdx.x + k * blockDim.x;
+			int e = threadIdx.x + k * NT;
 
 			if (e >= X * B)
 				break;
 
-			int b = e / X;
-			int x = e - b * X;
-			long yz = yz0 + b;
+			int bb = e / X;
+			int x = e % X;
+			long yz = yz0 + bb;
 
 			if (yz >= YZ)
 				continue;
 
-			float2 v = s[wrap_pos(x, X, L) * SB + b];
+			float2 w = s[wrap_pos(x, X, L) * SB + bb];
 
 			if (ax)
-				v = cscale(v, ax[x] * ayz[yz]);
+				w = cscale(w, ax[x] * ayz[yz]);
 
 			if (maps) {
 
-				float2 m = maps[x + X * yz + X * YZ * c];
-				acc[k] = cadd(acc[k], cmulc(v, m));
+				float2 mp = maps[x + X * yz + X * YZ * c];
+				acc[k] = cadd(acc[k], cmulc(w, mp));
 
 			} else {
 
-				out[x + X * yz + X * YZ * c] = v;
+				out[x + X * yz + X * YZ * c] = w;
 			}
 		}
-
-		__syncthreads();
 	}
 
 	if (maps) {
-#pragma unroll
-		for (int k = 0; k < OWN; k++) {
 
-			int e = threadIdx.x + k * blockDim.x;
+		double dot = 0.;
+#pragma unroll
+		for (int k = 0; k < 8; k++) {
+
+			int e = threadIdx.x + k * NT;
 
 			if (e >= X * B)
 				break;
 
-			int b = e / X;
-			int x = e - b * X;
-			long yz = yz0 + b;
+			int bb = e / X;
+			int x = e % X;
+			long yz = yz0 + bb;
 
-			if (yz < YZ)
+			if (yz < YZ) {
+
 				out[x + X * yz + X * YZ * g] = acc[k];
+
+				if (pdot) {	// Re<p, partial> for the CG step length
+
+					float2 pv = pdot[x + X * yz];
+					dot += (double)pv.x * (double)acc[k].x + (double)pv.y * (double)acc[k].y;
+				}
+			}
+		}
+
+		if (pdot) {
+
+			double t = block_sum_d(dot, red);
+
+			if (0 == threadIdx.x)
+				dot_part[blockIdx.x + gridDim.x * blockIdx.y] = t;
 		}
 	}
 }

@@ -59,7 +59,7 @@ def test_toeplitz_normal_and_psf_vs_reference(name, periodic):
     op.free()
 
 
-@pytest.mark.parametrize("N,spokes,coils", [(128, 64, 1), (96 * 2, 40, 2), (256, 402, 1)])
+@pytest.mark.parametrize("N,spokes,coils", [(128, 64, 1), (64, 40, 2), (256, 402, 1), (512, 100, 1)])
 def test_2d_vs_oracle(N, spokes, coils):
     rng = np.random.default_rng(N + spokes)
     t = synth.radial_traj(N, spokes)
