@@ -254,9 +254,7 @@ static std::map<std::pair<const void*, int>, bool> g_attr_done;
 template <typename K>
 static int prep_kernel(K kernel, size_t smem)
 {
-	if (smem <= 48 * 1024)
-		return BNUFFT_OK;
-
+	(void)smem;	// kernels also hold static shared memory: always opt in
 	int dev;
 	CUDA_TRY(cudaGetDevice(&dev));
 	auto key = std::make_pair((const void*)kernel, dev);

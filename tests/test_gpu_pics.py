@@ -34,7 +34,8 @@ def test_pics_30_iterations_vs_reference():
     x, st = _run(g, maxiter=30)
     assert rel(x, g["x30"]) < 2e-2
     xs, st2 = _run(g, maxiter=30, rescale=True)
-    assert st2[2] == st[2]
+    # gridding adds with atomics, so the adjoint's p90 moves in the last bit
+    assert abs(st2[2] - st[2]) <= 1e-6 * st[2]
     assert rel(xs, g["x30_rescale"]) < 2e-2
 
 
