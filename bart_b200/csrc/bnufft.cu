@@ -1548,3 +1548,234 @@ extern "C" int bnufft_prof_stop(double* total_ms, long* launches)
 }
 
 extern "C" long bnufft_launch_count(void) { return g_launches.load(); }
+
+// ----------------------------------------------------------------------------
+// Allocation-free 2D forward NUFFT (C ABI: bnufft_forward2d_noalloc)
+// ----------------------------------------------------------------------------
+//
+// For callers that cannot allocate device memory while they run: a scanner's
+// real-time reconstruction process that reserves its whole device budget up
+// front, or code that must not pay cudaMalloc's implicit device-wide
+// synchronisation (or risk its failure under memory pressure) in the middle
+// of a stream of work. Everything this entry point needs beyond the caller's
+// trajectory, image and k-space buffers lives in one file-scope device array,
+// g_noalloc_scratch, which every GPU that loads the library holds until the
+// process exits (NA_BYTES, about 7.4 MB).
+//
+// Limits: 2D images X x Y with X, Y in {8, 16, ..., 256}, at most NA_MAX_M
+// samples, one coil. Larger requests return BNUFFT_ERR_ARG.
+//
+// The first call on a device does the set-up: it takes the array's device
+// address with cudaGetSymbolAddress (the array's name in host code is only a
+// host-side stand-in), fills the Kaiser-Bessel and twiddle tables and
+// synchronises the caller's stream once. Make that first call before any
+// stream capture.
+//
+// All calls share the one array and every call overwrites the regions it
+// uses (trajectory copy, row-transformed buffer, grid, roll-off tables), so
+// nothing needs clearing between calls; calls whose work overlaps on the GPU
+// (different streams, or another thread) race on the array and must be
+// serialised by the caller.
+
+enum : long {
+
+	NA_MAX_N = 256,
+	NA_MAX_M = 262144,
+	NA_TRAJ_OFF = 0,						// float4[NA_MAX_M]
+	NA_T1_OFF = NA_TRAJ_OFF + 16L * NA_MAX_M,			// float2[2N x N]
+	NA_GRID_OFF = NA_T1_OFF + 8L * (2 * NA_MAX_N) * NA_MAX_N,	// float2[2N x 2N]
+	NA_TW_OFF = NA_GRID_OFF + 8L * (2 * NA_MAX_N) * (2 * NA_MAX_N),	// float2[1024]: L = 16..512 back to back
+	NA_KB_OFF = NA_TW_OFF + 8L * 1024,				// float[1024]
+	NA_AX_OFF = NA_KB_OFF + 4L * 1024,				// float[NA_MAX_N]
+	NA_AYZ_OFF = NA_AX_OFF + 4L * NA_MAX_N,				// float[NA_MAX_N]
+	NA_BYTES = NA_AYZ_OFF + 4L * NA_MAX_N,
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+static std::mutex g_na_mutex;
+static unsigned char* g_na_base[64];
+
+// twiddle table of length L (power of two, 16..512) inside the scratch table block
+static long na_tw_offset(int L) { return L - 16; }
+
+__device__ static double na_bessel_i0(double x)
+{
+	x = fabs(x);
+	double q = 0.25 * x * x, term = 1., sum = 1.;
+
+	for (int k = 1; k < 500; k++) {
+
+		term *= q / ((double)k * (double)k);
+		sum += term;
+
+		if (term < 1e-18 * sum)
+			break;
+	}
+
+	return sum;
+}
+
+// Kaiser-Bessel table (kb_precompute, src/noncart/grid.c:86-97) and the
+// twiddle tables exp(-2 pi i m / L), L = 16..512, in float64 then float32
+__global__ static void k_na_tables(float2* tw, float* kb, double beta)
+{
+	double i0b = na_bessel_i0(beta);
+
+	for (int i = threadIdx.x; i <= KB_TABLE_N; i += blockDim.x) {
+
+		double x = (double)i / (double)(KB_TABLE_N - 1) / 2.;
+		kb[i] = (fabs(x) >= 0.5) ? 0.f : (float)(na_bessel_i0(beta * sqrt(1. - pow(2. * x, 2.))) / i0b);
+	}
+
+	for (int L = 16; L <= 512; L *= 2)
+		for (int m = threadIdx.x; m < L; m += blockDim.x) {
+
+			double a = -2. * M_PI * (double)m / (double)L;
+			tw[L - 16 + m] = make_float2((float)cos(a), (float)sin(a));
+		}
+}
+
+__device__ static double na_rolloff(int d, int i, double beta, double i0b)
+{
+	// rolloff() / pos() of src/noncart/grid.c:114-117, 522-533 for os = 2, width = 6
+	int od = 2 * d;
+	int oi = i + (od / 2 - d / 2);
+	float p = ((float)oi - (float)(od / 2)) / (float)od;
+	double x = (double)p * 6.;
+	double a = beta * beta - pow(M_PI * x, 2.);
+	double ft = (0. == a) ? 1. / i0b : ((a > 0) ? (sinh(sqrt(a)) / sqrt(a)) / i0b : (sin(sqrt(-a)) / sqrt(-a)) / i0b);
+	return 1. / ft / 6.;
+}
+
+// roll-off tables of an X x Y image: ax[x], ayz[y] (with 1/sqrt(X*Y))
+__global__ static void k_na_rolloff(float* ax, float* ayz, int X, int Y, double beta)
+{
+	double i0b = na_bessel_i0(beta);
+	double sc = 1. / sqrt((double)X * (double)Y);
+
+	for (int i = threadIdx.x; i < X; i += blockDim.x)
+		ax[i] = (float)na_rolloff(X, i, beta, i0b);
+
+	for (int i = threadIdx.x; i < Y; i += blockDim.x)
+		ayz[i] = (float)(na_rolloff(Y, i, beta, i0b) * sc);
+}
+
+template <int L>
+static int na_rows(const float2* img, const float* ax, const float* ayz, int X, int Y, float2* out,
+		const float2* tw, cudaStream_t st)
+{
+	constexpr int B = 16;
+	size_t smem = pass_smem(L, B);
+	CUDA_TRY(cudaFuncSetAttribute(k_rows_fwd<L, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+	k_rows_fwd<L, B><<<(unsigned)((Y + B - 1) / B), B * L / 8, smem, st>>>(img, nullptr, ax, ayz, X, Y, Y, out, tw);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+template <int L>
+static int na_cols(const float2* t1, int G0, int Y, float2* grid, const float2* tw, cudaStream_t st)
+{
+	constexpr int B = 16;
+	size_t smem = pass_smem(L, B);
+	CUDA_TRY(cudaFuncSetAttribute(k_cols<L, B, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+	dim3 grid_dim((unsigned)((G0 + B - 1) / B), 1);
+	k_cols<L, B, 0><<<grid_dim, B * L / 8, smem, st>>>(t1, G0, (long)G0 * Y, Y, 1, grid, G0, (long)G0 * L, L, 0,
+			G0, nullptr, 0, 1, 0, tw, nullptr);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+#define NA_DISPATCH(L, CALL) \
+	switch (L) { \
+	case 16: { constexpr int LL = 16; return CALL; } \
+	case 32: { constexpr int LL = 32; return CALL; } \
+	case 64: { constexpr int LL = 64; return CALL; } \
+	case 128: { constexpr int LL = 128; return CALL; } \
+	case 256: { constexpr int LL = 256; return CALL; } \
+	case 512: { constexpr int LL = 512; return CALL; } \
+	default: return fail(BNUFFT_ERR_ARG, "allocation-free NUFFT: grid length %d", L); }
+
+static int na_setup(unsigned char** base, cudaStream_t st)
+{
+	int dev;
+	CUDA_TRY(cudaGetDevice(&dev));
+
+	if ((dev < 0) || (dev >= 64))
+		return fail(BNUFFT_ERR_ARG, "device index %d", dev);
+
+	std::lock_guard<std::mutex> lock(g_na_mutex);
+
+	if (g_na_base[dev]) {
+
+		*base = g_na_base[dev];
+		return BNUFFT_OK;
+	}
+
+	void* p = nullptr;
+	cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+
+	if ((cudaSuccess != e) || (nullptr == p))
+		return fail(BNUFFT_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
+
+	unsigned char* b = (unsigned char*)p;
+	k_na_tables<<<1, 256, 0, st>>>((float2*)(b + NA_TW_OFF), (float*)(b + NA_KB_OFF), kernel_beta(2.f, 6.f));
+	LAUNCHED();
+	CUDA_TRY(cudaStreamSynchronize(st));	// tables ready before any other stream uses them
+	g_na_base[dev] = b;
+	*base = b;
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_forward2d_noalloc(long X, long Y, long M, const void* traj, const void* img, void* ksp, void* stream)
+{
+	cudaStream_t st = S(stream);
+
+	for (long n : { X, Y })
+		if ((n < 8) || (n > NA_MAX_N) || (0 != (n & (n - 1))))
+			return fail(BNUFFT_ERR_ARG, "allocation-free NUFFT: image side %ld (powers of two 8..%ld)", n, (long)NA_MAX_N);
+
+	if ((M < 1) || (M > NA_MAX_M))
+		return fail(BNUFFT_ERR_ARG, "allocation-free NUFFT: %ld samples (at most %ld)", M, (long)NA_MAX_M);
+
+	if (!traj || !img || !ksp || !on_device(traj) || !on_device(img) || !on_device(ksp))
+		return fail(BNUFFT_ERR_ARG, "allocation-free NUFFT: traj, img and ksp must be device pointers");
+
+	unsigned char* base = nullptr;
+	TRY(na_setup(&base, st));
+
+	float4* ntraj = (float4*)(base + NA_TRAJ_OFF);
+	float2* t1 = (float2*)(base + NA_T1_OFF);
+	float2* grid = (float2*)(base + NA_GRID_OFF);
+	const float2* tw = (const float2*)(base + NA_TW_OFF);
+	const float* kb = (const float*)(base + NA_KB_OFF);
+	float* ax = (float*)(base + NA_AX_OFF);
+	float* ayz = (float*)(base + NA_AYZ_OFF);
+
+	const int G0 = (int)(2 * X), G1 = (int)(2 * Y);
+
+	k_na_rolloff<<<1, 256, 0, st>>>(ax, ayz, (int)X, (int)Y, kernel_beta(2.f, 6.f));
+	LAUNCHED();
+	k_traj_convert<<<vec_blocks(M), RED_THREADS, 0, st>>>(ntraj, (const float2*)traj, M, 1.f);
+	LAUNCHED();
+
+	auto rowsf = [&]() -> int { NA_DISPATCH(G0, (na_rows<LL>((const float2*)img, ax, ayz, (int)X, (int)Y, t1, tw + na_tw_offset(LL), st))); };
+	TRY(rowsf());
+
+	auto colsf = [&]() -> int { NA_DISPATCH(G1, (na_cols<LL>(t1, G0, (int)Y, grid, tw + na_tw_offset(LL), st))); };
+	TRY(colsf());
+
+	GridGeom gg;
+	gg.N[0] = (int)X;
+	gg.N[1] = (int)Y;
+	gg.N[2] = 1;
+	gg.G[0] = G0;
+	gg.G[1] = G1;
+	gg.G[2] = 1;
+	gg.gsz = (long)G0 * G1;
+	gg.hw = 3.f;
+	gg.periodic = 0;
+	k_degrid<<<(unsigned)((M + 127) / 128), 128, 0, st>>>(ntraj, M, gg, 1, 1, grid, (float2*)ksp, kb);
+	LAUNCHED();
+	return BNUFFT_OK;
+}

@@ -79,6 +79,23 @@ int bnufft_update_traj(bnufft_plan_t plan, int N, const long traj_dims[], const 
 /* linop_free() of a NUFFT linop (nufft_free_data, src/noncart/nufft.c:1334). */
 void bnufft_free(bnufft_plan_t plan);
 
+/* Forward NUFFT of one 2D image that allocates no device memory. It has no
+ * counterpart in the reference. It serves callers that cannot allocate
+ * while they run: a scanner's real-time reconstruction process that reserves
+ * its device memory up front, or code that must not pay cudaMalloc's implicit
+ * device-wide synchronisation (or risk its failure) mid-stream. Results equal
+ * bnufft_apply_forward of a plan with default options (os 2, width 6,
+ * non-periodic).
+ * traj: device [3, M] complex float; img: device [X, Y] complex float;
+ * ksp: device [M] complex float. Limits: X, Y powers of two from 8 to 256,
+ * M <= 262144; larger requests return BNUFFT_ERR_ARG.
+ * Scratch: one file-scope device array of about 7.4 MB, held by every GPU
+ * that loads the library until exit and shared by all calls, so calls that
+ * overlap on the GPU race and must be serialised by the caller. The first
+ * call on a device sets up the array's tables and synchronises `stream`
+ * once; make that first call before any stream capture. */
+int bnufft_forward2d_noalloc(long X, long Y, long M, const void* traj, const void* img, void* ksp, void* stream);
+
 /* --- CG-SENSE: bart pics -l2 -r lambda -i iter -t traj ksp sens out ------- */
 
 struct bnufft_pics_conf {
