@@ -4,6 +4,7 @@
 // aborting (the reference aborts through error(), src/misc/misc.c:95).
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <atomic>
 #include <cmath>
@@ -232,7 +233,9 @@ static int get_kb_table(float os, float width, const float** out)
 
 static bool supported_len(int L) { return (L >= 16) && (L <= 2048) && (0 == (L & (L - 1))); }
 
+// dynamic shared memory of a column pass (ColLayout) / row pass (RowLayout), twiddles included
 static size_t pass_smem(int L, int B) { return sizeof(float2) * (size_t)L * (size_t)(smem_stride(B) + 1); }
+static size_t rows_smem(int L, int B) { return sizeof(float2) * ((size_t)B * (size_t)(L + L / 8) + (size_t)L); }
 
 // sequences per block (B in {4, 8, 16}, B * L / 8 threads <= 1024): as many
 // as fit, fewer when the launch would have too few blocks to fill the GPU
@@ -274,7 +277,7 @@ static int launch_rows_fwd_LB(const float2* img, const float2* maps, const float
 {
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
-	size_t smem = pass_smem(L, B);
+	size_t smem = rows_smem(L, B);
 	TRY(prep_kernel(k_rows_fwd<L, B>, smem));
 	cudaEvent_t pe = prof_begin("rows_fwd", st);
 	k_rows_fwd<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(img, maps, ax, ayz, X, YZ, R, out, tw);
@@ -313,7 +316,7 @@ static int launch_rows_inv_LB(const float2* in, const float2* maps, const float*
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
 	int groups = (C + cpg - 1) / cpg;
-	size_t smem = pass_smem(L, B);
+	size_t smem = rows_smem(L, B);
 	TRY(prep_kernel(k_rows_inv<L, B>, smem));
 	dim3 grid((unsigned)((YZ + B - 1) / B), (unsigned)groups);
 	cudaEvent_t pe = prof_begin("rows_inv", st);
@@ -330,7 +333,7 @@ static int launch_rows_fwd_cg_LB(const float2* bvec, const float2* r, const floa
 {
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
-	size_t smem = pass_smem(L, B);
+	size_t smem = rows_smem(L, B);
 	TRY(prep_kernel(k_rows_fwd_cg<L, B>, smem));
 	cudaEvent_t pe = prof_begin("rows_fwd", st);
 	k_rows_fwd_cg<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(bvec, r, p_prev, p_cur, maps, ax, ayz,
@@ -438,6 +441,15 @@ struct Work {
 	long cap = 0;		// channels the buffers hold
 };
 
+// interpolation matrix in CSR form over grid cells (deterministic gridding)
+struct Csr {
+
+	long* row_ptr = nullptr;	// [gsz + 1]
+	int* col = nullptr;		// [nnz] sample index
+	float* val = nullptr;		// [nnz] weight
+	long nnz = 0;
+};
+
 struct OpCtx {
 
 	Geom g;
@@ -446,7 +458,16 @@ struct OpCtx {
 	float* ax = nullptr;	// [N0] roll-off along x
 	float* ayz = nullptr;	// [N1*N2] roll-off along y,z with 1/sqrt(npix)
 	Work w;
+	Csr csr;		// set in deterministic mode
 };
+
+static void free_csr(Csr& c, cudaStream_t st)
+{
+	if (c.row_ptr) cudaFreeAsync(c.row_ptr, st);
+	if (c.col) cudaFreeAsync(c.col, st);
+	if (c.val) cudaFreeAsync(c.val, st);
+	c = Csr{};
+}
 
 static GridGeom grid_geom(const Geom& g)
 {
@@ -686,6 +707,17 @@ static int degrid(OpCtx& op, const float2* grid, long C, float2* ksp, cudaStream
 
 static int grid_adj(OpCtx& op, const float2* ksp, long C, float2* grid, cudaStream_t st)
 {
+	if (op.csr.row_ptr) {	// deterministic: fixed-order gather per cell
+
+		int cpc = (int)std::min<long>(C, 8);
+		dim3 blocks((unsigned)((op.g.gsz + 255) / 256), (unsigned)((C + cpc - 1) / cpc));
+		cudaEvent_t pe = prof_begin("grid", st);
+		k_grid_csr<<<blocks, 256, 0, st>>>(op.csr.row_ptr, op.csr.col, op.csr.val, op.g.gsz, op.g.M, (int)C, cpc, ksp, grid);
+		prof_end(pe, st);
+		LAUNCHED();
+		return BNUFFT_OK;
+	}
+
 	CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(float2) * op.g.gsz * C, st));
 	int cpc = (int)std::min<long>(C, 8);
 	dim3 blocks((unsigned)((op.g.M + 127) / 128), (unsigned)((C + cpc - 1) / cpc));
@@ -693,6 +725,73 @@ static int grid_adj(OpCtx& op, const float2* ksp, long C, float2* grid, cudaStre
 	k_grid_atomic<<<blocks, 128, 0, st>>>(op.traj, op.g.M, grid_geom(op.g), (int)C, cpc, ksp, grid, op.kb);
 	prof_end(pe, st);
 	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+// Build the CSR interpolation matrix of op's trajectory (stable sort by
+// cell * M + sample, so each row lists its samples in increasing order).
+static int build_csr(OpCtx& op, cudaStream_t st)
+{
+	const Geom& g = op.g;
+	int slots_z = (g.G[2] > 1) ? CSR_TAPS_AXIS : 1;
+	long slots = (long)CSR_TAPS_AXIS * CSR_TAPS_AXIS * slots_z;
+	long n = g.M * slots;
+
+	if ((g.M >= (1L << 31)) || ((unsigned long long)g.gsz * (unsigned long long)g.M >= (~0ull >> 1)) || (n >= (1L << 31)))
+		return fail(BNUFFT_ERR_UNSUPPORTED, "deterministic gridding: %ld samples x %ld cells is too large", g.M, g.gsz);
+
+	unsigned long long *keys = nullptr, *keys2 = nullptr;
+	float *vals = nullptr, *vals2 = nullptr;
+	int* counts = nullptr;
+	void* tmp = nullptr;
+	size_t tmp_bytes = 0;
+	CUDA_TRY(cudaMallocAsync(&keys, sizeof(unsigned long long) * n, st));
+	CUDA_TRY(cudaMallocAsync(&keys2, sizeof(unsigned long long) * n, st));
+	CUDA_TRY(cudaMallocAsync(&vals, sizeof(float) * n, st));
+	CUDA_TRY(cudaMallocAsync(&vals2, sizeof(float) * n, st));
+
+	k_csr_keys<<<(unsigned)((g.M + 127) / 128), 128, 0, st>>>(op.traj, g.M, grid_geom(g), op.kb, keys, vals, slots_z);
+	LAUNCHED();
+
+	CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, vals, vals2, (int)n, 0, 64, st));
+	CUDA_TRY(cudaMallocAsync(&tmp, tmp_bytes, st));
+	CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, vals, vals2, (int)n, 0, 64, st));
+	g_launches.fetch_add(1, std::memory_order_relaxed);
+
+	// entries with a valid key come first; count them per cell
+	Csr& c = op.csr;
+	CUDA_TRY(cudaMallocAsync(&counts, sizeof(int) * (g.gsz + 1), st));
+	CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int) * (g.gsz + 1), st));
+	CUDA_TRY(cudaMallocAsync(&c.row_ptr, sizeof(long) * (g.gsz + 1), st));
+
+	// number of valid entries: taps of every sample (host needs it for sizes)
+	int* col_all = nullptr;
+	CUDA_TRY(cudaMallocAsync(&col_all, sizeof(int) * n, st));
+	k_csr_fill_valid<<<vec_blocks(n), RED_THREADS, 0, st>>>(keys2, n, g.M, g.gsz, col_all, counts);
+	LAUNCHED();
+
+	size_t scan_bytes = 0;
+	void* scan_tmp = nullptr;
+	CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts, c.row_ptr, (int)(g.gsz + 1), st));
+	CUDA_TRY(cudaMallocAsync(&scan_tmp, scan_bytes, st));
+	CUDA_TRY(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, c.row_ptr, (int)(g.gsz + 1), st));
+	g_launches.fetch_add(1, std::memory_order_relaxed);
+
+	long nnz = 0;
+	CUDA_TRY(cudaMemcpyAsync(&nnz, c.row_ptr + g.gsz, sizeof(long), cudaMemcpyDeviceToHost, st));
+	CUDA_TRY(cudaStreamSynchronize(st));
+	c.nnz = nnz;
+
+	// valid entries are the first nnz of the sorted arrays
+	c.col = col_all;
+	c.val = vals2;
+
+	cudaFreeAsync(keys, st);
+	cudaFreeAsync(keys2, st);
+	cudaFreeAsync(vals, st);
+	cudaFreeAsync(counts, st);
+	cudaFreeAsync(tmp, st);
+	cudaFreeAsync(scan_tmp, st);
 	return BNUFFT_OK;
 }
 
@@ -751,7 +850,8 @@ static int op_toeplitz(OpCtx& op, const float2* psf, const float2* x, const floa
 // product needs no further normalisation (compute_psf2, src/noncart/nufft.c:727-776):
 // psft = adjoint NUFFT of ones with trajectory 2*traj onto the 2N image,
 // periodic gridding; psf = fftuc(psft) / npix.
-static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, float2** psf_out, cudaStream_t st)
+static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, float2** psf_out, cudaStream_t st,
+		bool deterministic)
 {
 	OpCtx in;
 	long d2[3] = { g.G[0], g.G[1], g.G[2] };
@@ -774,7 +874,12 @@ static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, flo
 	in.traj = t2;
 	in.kb = kb;
 	TRY(init_rolloff(in, st));
+
+	if (deterministic)
+		TRY(build_csr(in, st));
+
 	TRY(op_adjoint(in, ones, nullptr, 1, 1, psft, st));
+	free_csr(in.csr, st);
 
 	// full 2N-point transform of the 2N image: input centred (ifftshift), output in DFT order
 	OpCtx full;
@@ -926,9 +1031,6 @@ static int check_conf(const bnufft_conf* conf)
 	if ((conf->width <= 0.f) || (conf->width > 8.f))
 		return fail(BNUFFT_ERR_UNSUPPORTED, "kernel width %g", conf->width);
 
-	if (conf->deterministic)
-		return fail(BNUFFT_ERR_UNSUPPORTED, "deterministic gridding is not built yet");
-
 	return BNUFFT_OK;
 }
 
@@ -939,13 +1041,19 @@ static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
 	k_traj_convert<<<vec_blocks(p->op.g.M), RED_THREADS, 0, st>>>(p->traj, (const float2*)t.dev, p->op.g.M, 1.f);
 	LAUNCHED();
 
+	if (p->conf.deterministic) {
+
+		free_csr(p->op.csr, st);
+		TRY(build_csr(p->op, st));
+	}
+
 	if (p->conf.toeplitz) {
 
 		if (p->psf)
 			cudaFreeAsync(p->psf, st);
 
 		p->psf = nullptr;
-		TRY(compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, st));
+		TRY(compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, st, 0 != p->conf.deterministic));
 	}
 
 	if (t.owned)
@@ -1178,6 +1286,7 @@ extern "C" void bnufft_free(bnufft_plan_t p)
 
 	cudaStream_t st = p->st0;
 	free_work(p->op.w, st);
+	free_csr(p->op.csr, st);
 
 	if (p->traj) cudaFreeAsync(p->traj, st);
 	if (p->psf) cudaFreeAsync(p->psf, st);
@@ -1666,7 +1775,7 @@ static int na_rows(const float2* img, const float* ax, const float* ayz, int X, 
 		const float2* tw, cudaStream_t st)
 {
 	constexpr int B = 16;
-	size_t smem = pass_smem(L, B);
+	size_t smem = rows_smem(L, B);
 	CUDA_TRY(cudaFuncSetAttribute(k_rows_fwd<L, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
 	k_rows_fwd<L, B><<<(unsigned)((Y + B - 1) / B), B * L / 8, smem, st>>>(img, nullptr, ax, ayz, X, Y, Y, out, tw);
 	LAUNCHED();

@@ -1,12 +1,12 @@
 // Shared-memory Stockham FFT core for sm_100a.
 //
 // A thread block transforms B sequences of length L (power of two, 16..2048).
-// Each sequence is served by T = L/8 threads; thread t of the block works on
-// sequence b = t % B with index jt = t / B. Between stages the data lives in
-// shared memory as s[p * SB + b] (element p of sequence b; SB = B|1 keeps the
-// element stride odd so that 8-byte accesses of a half-warp hit distinct
-// banks). Stages are radix 8 with a final radix 4 or 2 (Stockham autosort, so
-// the result is in natural order without a bit-reversal pass).
+// Each sequence is served by T = L/8 threads (index jt). Between stages the
+// data lives in shared memory in one of two layouts (ColLayout for column
+// passes, RowLayout for row passes; see below), chosen so that both the
+// global accesses and the shared-memory stages stay conflict-free. Stages are
+// radix 8 with a final radix 4 or 2 (Stockham autosort, so the result is in
+// natural order without a bit-reversal pass).
 //
 // Register ownership: before the first stage and after the last stage a
 // thread holds the eight elements at positions jt + T*m (m = 0..7) in
@@ -102,13 +102,6 @@ __device__ __forceinline__ void butterfly(float2* v)
 		dft2<INV>(v);
 }
 
-template <int L>
-struct FftShape {
-
-	static_assert(L >= 16 && L <= 2048 && (L & (L - 1)) == 0, "power-of-two length 16..2048");
-	static constexpr int T = L / 8;		// threads per sequence
-};
-
 // twiddle v[i] *= w^(i*k), w = exp(-+2 pi i / (Ns*R)), from tw[m] = exp(-2 pi i m / L)
 template <int L, int Ns, int R, bool INV>
 __device__ __forceinline__ void twiddle(float2* v, int k, const float2* tw)
@@ -127,12 +120,44 @@ __device__ __forceinline__ void twiddle(float2* v, int k, const float2* tw)
 	}
 }
 
-// Stage with Ns = product of earlier radices, Ns > 1, smem -> smem
-// (middle stages), or smem -> registers (last stage, LAST = true).
-template <int L, int B, int Ns, bool INV>
+// Shared-memory layouts of B sequences of length L (element indices).
+//
+// ColLayout: sequences interleaved, element p of sequence b at p*SB + b
+// (SB = B|1 odd, so a half-warp's 8-byte accesses hit distinct banks);
+// thread t serves sequence t % B with index t / B. A warp covers the same
+// element of consecutive sequences: coalesced for columns of an x-fastest
+// array.
+template <int L, int B>
+struct ColLayout {
+
+	static constexpr int SB = B | 1;
+	static constexpr int SMEM = L * SB;
+
+	__device__ static __forceinline__ int idx(int p, int b) { return p * SB + b; }
+	__device__ static __forceinline__ int seq() { return threadIdx.x % B; }
+	__device__ static __forceinline__ int jt() { return threadIdx.x / B; }
+};
+
+// RowLayout: each sequence contiguous with one pad element after every 8
+// (p + p/8 breaks the stride-8 bank pattern of the first stage's stores);
+// thread t serves sequence t / (L/8) with index t % (L/8). A warp covers
+// consecutive elements of one sequence: coalesced for contiguous rows.
+template <int L, int B>
+struct RowLayout {
+
+	static constexpr int SL = L + L / 8;
+	static constexpr int SMEM = B * SL;
+
+	__device__ static __forceinline__ int idx(int p, int b) { return b * SL + p + (p >> 3); }
+	__device__ static __forceinline__ int seq() { return threadIdx.x / (L / 8); }
+	__device__ static __forceinline__ int jt() { return threadIdx.x % (L / 8); }
+};
+
+// Stage with Ns = product of earlier radices, Ns > 1: smem -> smem (middle
+// stages) or smem -> registers (the last stage).
+template <int L, typename LAY, int Ns, bool INV>
 __device__ __forceinline__ void fft_tail(float2 (&v)[8], float2* s, int b, int jt, const float2* tw)
 {
-	constexpr int SB = B | 1;
 	constexpr int REM = L / Ns;
 	constexpr int R = (REM >= 8) ? 8 : REM;
 	constexpr int NB = L / R;
@@ -146,7 +171,7 @@ __device__ __forceinline__ void fft_tail(float2 (&v)[8], float2* s, int b, int j
 	for (int q = 0; q < PER; q++) {
 #pragma unroll
 		for (int i = 0; i < R; i++)
-			u[q][i] = s[(jt + q * T + i * NB) * SB + b];
+			u[q][i] = s[LAY::idx(jt + q * T + i * NB, b)];
 	}
 
 	if constexpr (!LAST)
@@ -171,39 +196,40 @@ __device__ __forceinline__ void fft_tail(float2 (&v)[8], float2* s, int b, int j
 			int idxD = (j / Ns) * Ns * R + k;
 #pragma unroll
 			for (int i = 0; i < R; i++)
-				s[(idxD + i * Ns) * SB + b] = u[q][i];
+				s[LAY::idx(idxD + i * Ns, b)] = u[q][i];
 		}
 	}
 
 	if constexpr (!LAST) {
 
 		__syncthreads();
-		fft_tail<L, B, Ns * R, INV>(v, s, b, jt, tw);
+		fft_tail<L, LAY, Ns * R, INV>(v, s, b, jt, tw);
 	}
 }
 
-// Full transform of the register set v (positions jt + T*m in, same out).
-// Begins with a barrier, so the caller may have been reading s just before.
-template <int L, int B, bool INV>
+// Full transform of the register set v (positions jt + (L/8)*m in, same
+// out). Begins with a barrier, so the caller may have been reading s just
+// before; the caller must barrier before writing s after it returns.
+template <int L, typename LAY, bool INV>
 __device__ __forceinline__ void fft_regs(float2 (&v)[8], float2* s, const float2* tw)
 {
-	constexpr int SB = B | 1;
-	const int b = threadIdx.x % B;
-	const int jt = threadIdx.x / B;
+	static_assert(L >= 16 && L <= 2048 && (L & (L - 1)) == 0, "power-of-two length 16..2048");
+	const int b = LAY::seq();
+	const int jt = LAY::jt();
 
 	// stage 1 (Ns = 1, radix 8, no twiddles): registers -> smem at 8*jt + i
 	butterfly<8, INV>(v);
 	__syncthreads();
 #pragma unroll
 	for (int i = 0; i < 8; i++)
-		s[(8 * jt + i) * SB + b] = v[i];
+		s[LAY::idx(8 * jt + i, b)] = v[i];
 	__syncthreads();
 
-	fft_tail<L, B, 8, INV>(v, s, b, jt, tw);
+	fft_tail<L, LAY, 8, INV>(v, s, b, jt, tw);
 }
 
 // stage-1 position of register m for this thread
-template <int L, int B>
-__device__ __forceinline__ int reg_pos(int m) { return threadIdx.x / B + (L / 8) * m; }
+template <int L, typename LAY>
+__device__ __forceinline__ int reg_pos(int m) { return LAY::jt() + (L / 8) * m; }
 
 } // namespace bn

@@ -108,18 +108,18 @@ struct CgScalars {
 // p^H (A^H A + lambda) p); every row multiplies by its coil's map and runs the
 // forward transform like k_rows_fwd.
 template <int L, int B>
-__global__ void __launch_bounds__(B * L / 8) k_rows_fwd_cg(const float2* __restrict__ bvec, const float2* __restrict__ r,
+__global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_rows_fwd_cg(const float2* __restrict__ bvec, const float2* __restrict__ r,
 		const float2* __restrict__ p_prev, float2* __restrict__ p_cur, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
 		int X, long YZ, long R, float2* __restrict__ out, const float2* __restrict__ twg,
 		CgScalars* st, int it, const double* __restrict__ rs_part, int nrs, double* __restrict__ pp_part)
 {
-	constexpr int SB = B | 1;
+	using LAY = RowLayout<L, B>;
 	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
 	__shared__ double red[32];
 	float2* s = smem;
-	float2* tw = smem + L * SB;
+	float2* tw = smem + LAY::SMEM;
 
 	if (st->done)
 		return;
@@ -152,21 +152,21 @@ __global__ void __launch_bounds__(B * L / 8) k_rows_fwd_cg(const float2* __restr
 	for (int i = threadIdx.x; i < L; i += NT)
 		tw[i] = twg[i];
 
-	const long r0 = (long)blockIdx.x * B;
+	const long row = (long)blockIdx.x * B + LAY::seq();
+	const bool valid = (row < R);
+	const long yz = valid ? row % YZ : 0;
+	const long c = valid ? row / YZ : 0;
 	double pp = 0.;
+	float2 v[8];
 
-	for (int e = threadIdx.x; e < L * B; e += NT) {
+#pragma unroll
+	for (int m = 0; m < 8; m++) {
 
-		int b = e / L;
-		int q = e % L;
-		long row = r0 + b;
-		int n = unwrap_pos(q, X, L);
-		float2 v = make_float2(0.f, 0.f);
+		int n = unwrap_pos(reg_pos<L, LAY>(m), X, L);
+		v[m] = make_float2(0.f, 0.f);
 
-		if ((n < X) && (row < R)) {
+		if (valid && (n < X)) {
 
-			long yz = row % YZ;
-			long c = row / YZ;
 			long i = n + X * yz;
 			float2 pv;
 
@@ -188,13 +188,9 @@ __global__ void __launch_bounds__(B * L / 8) k_rows_fwd_cg(const float2* __restr
 				pp += (double)pv.x * (double)pv.x + (double)pv.y * (double)pv.y;
 			}
 
-			v = cmul(pv, maps[i + X * YZ * c]);
-
-			if (ax)
-				v = cscale(v, ax[n] * ayz[yz]);
+			float2 w = cmul(pv, maps[i + X * YZ * c]);
+			v[m] = ax ? cscale(w, ax[n] * ayz[yz]) : w;
 		}
-
-		s[q * SB + b] = v;
 	}
 
 	double t = block_sum_d(pp, red);
@@ -202,30 +198,12 @@ __global__ void __launch_bounds__(B * L / 8) k_rows_fwd_cg(const float2* __restr
 	if (0 == threadIdx.x)
 		pp_part[blockIdx.x] = t;
 
-	__syncthreads();
+	fft_regs<L, LAY, false>(v, s, tw);
 
-	float2 v[8];
-	const int b = threadIdx.x % B;
+	if (valid) {
 #pragma unroll
-	for (int m = 0; m < 8; m++)
-		v[m] = s[reg_pos<L, B>(m) * SB + b];
-
-	fft_regs<L, B, false>(v, s, tw);
-
-	__syncthreads();
-#pragma unroll
-	for (int m = 0; m < 8; m++)
-		s[reg_pos<L, B>(m) * SB + b] = v[m];
-	__syncthreads();
-
-	for (int e = threadIdx.x; e < L * B; e += NT) {
-
-		int b = e / L;
-		int q = e % L;
-		long row = r0 + b;
-
-		if (row < R)
-			out[q + (long)L * row] = s[q * SB + b];
+		for (int m = 0; m < 8; m++)
+			out[reg_pos<L, LAY>(m) + (long)L * row] = v[m];
 	}
 }
 
@@ -235,77 +213,48 @@ __global__ void __launch_bounds__(B * L / 8) k_rows_fwd_cg(const float2* __restr
 //   v = img[x + X*yz (+ X*YZ*c unless maps)] (* maps[x + X*yz + X*YZ*c])
 //       * ax[x] * ayz[yz]                          (apodisation, optional)
 // placed at wrap_pos(x, X, L), transformed, written to out[p + L*r].
-// One block: B rows, B*L/8 threads. Global traffic is staged through shared
-// memory so that loads and stores run along the contiguous rows.
+// One block: B rows, B*L/8 threads; a warp reads and writes consecutive
+// elements of one row straight from / into the FFT's registers.
 template <int L, int B>
-__global__ void __launch_bounds__(B * L / 8) k_rows_fwd(const float2* __restrict__ img, const float2* __restrict__ maps,
+__global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_rows_fwd(const float2* __restrict__ img, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
 		int X, long YZ, long R, float2* __restrict__ out, const float2* __restrict__ twg)
 {
-	constexpr int SB = B | 1;
+	using LAY = RowLayout<L, B>;
 	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
 	float2* s = smem;
-	float2* tw = smem + L * SB;
+	float2* tw = smem + LAY::SMEM;
 
 	for (int i = threadIdx.x; i < L; i += NT)
 		tw[i] = twg[i];
 
-	const long r0 = (long)blockIdx.x * B;
+	const long row = (long)blockIdx.x * B + LAY::seq();
+	const bool valid = (row < R);
+	const long yz = valid ? row % YZ : 0;
+	const long c = valid ? row / YZ : 0;
+	float2 v[8];
 
-	for (int e = threadIdx.x; e < L * B; e += NT) {
+#pragma unroll
+	for (int m = 0; m < 8; m++) {
 
-		int b = e / L;
-		int p = e % L;
-		long r = r0 + b;
-		int n = unwrap_pos(p, X, L);
-		float2 v = make_float2(0.f, 0.f);
+		int n = unwrap_pos(reg_pos<L, LAY>(m), X, L);
+		v[m] = make_float2(0.f, 0.f);
 
-		if ((n < X) && (r < R)) {
+		if (valid && (n < X)) {
 
-			long yz = r % YZ;
-			long c = r / YZ;
-
-			if (maps) {
-
-				v = cmul(img[n + X * yz], maps[n + X * yz + X * YZ * c]);
-
-			} else {
-
-				v = img[n + X * yz + X * YZ * c];
-			}
-
-			if (ax)
-				v = cscale(v, ax[n] * ayz[yz]);
+			float2 w = maps ? cmul(img[n + X * yz], maps[n + X * yz + X * YZ * c])
+					: img[n + X * yz + X * YZ * c];
+			v[m] = ax ? cscale(w, ax[n] * ayz[yz]) : w;
 		}
-
-		s[p * SB + b] = v;
 	}
 
-	__syncthreads();
+	fft_regs<L, LAY, false>(v, s, tw);
 
-	float2 v[8];
-	const int b = threadIdx.x % B;
+	if (valid) {
 #pragma unroll
-	for (int m = 0; m < 8; m++)
-		v[m] = s[reg_pos<L, B>(m) * SB + b];
-
-	fft_regs<L, B, false>(v, s, tw);
-
-	__syncthreads();
-#pragma unroll
-	for (int m = 0; m < 8; m++)
-		s[reg_pos<L, B>(m) * SB + b] = v[m];
-	__syncthreads();
-
-	for (int e = threadIdx.x; e < L * B; e += NT) {
-
-		int b = e / L;
-		int p = e % L;
-		long r = r0 + b;
-
-		if (r < R)
-			out[p + (long)L * r] = s[p * SB + b];
+		for (int m = 0; m < 8; m++)
+			out[reg_pos<L, LAY>(m) + (long)L * row] = v[m];
 	}
 }
 
@@ -322,16 +271,16 @@ __global__ void __launch_bounds__(B * L / 8) k_rows_fwd(const float2* __restrict
 // Global loads go straight into the first FFT stage's registers and results
 // leave from the last stage's registers (B consecutive columns per access).
 template <int L, int B, int MODE>
-__global__ void __launch_bounds__(B * L / 8) k_cols(const float2* __restrict__ in, long ies, long ios, int n_in, int wrap_in,
+__global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_cols(const float2* __restrict__ in, long ies, long ios, int n_in, int wrap_in,
 		float2* __restrict__ out, long oes, long oos, int n_out, int wrap_out,
 		int W, const float2* __restrict__ psf, long pes, long pmod, long pos,
 		const float2* __restrict__ twg, const int* done)
 {
-	constexpr int SB = B | 1;
+	using LAY = ColLayout<L, B>;
 	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
 	float2* s = smem;
-	float2* tw = smem + L * SB;
+	float2* tw = smem + LAY::SMEM;
 
 	if (done && *done)
 		return;
@@ -339,8 +288,7 @@ __global__ void __launch_bounds__(B * L / 8) k_cols(const float2* __restrict__ i
 	for (int i = threadIdx.x; i < L; i += NT)
 		tw[i] = twg[i];
 
-	const int b = threadIdx.x % B;
-	const int cx = blockIdx.x * B + b;
+	const int cx = blockIdx.x * B + LAY::seq();
 	const bool valid = (cx < W);
 	const long o = blockIdx.y;
 	const float2* inp = in + o * ios + cx;
@@ -349,7 +297,7 @@ __global__ void __launch_bounds__(B * L / 8) k_cols(const float2* __restrict__ i
 #pragma unroll
 	for (int m = 0; m < 8; m++) {
 
-		int p = reg_pos<L, B>(m);
+		int p = reg_pos<L, LAY>(m);
 		int n = wrap_in ? unwrap_pos(p, n_in, L) : p;
 		v[m] = (valid && (n < n_in)) ? inp[n * ies] : make_float2(0.f, 0.f);
 	}
@@ -357,11 +305,11 @@ __global__ void __launch_bounds__(B * L / 8) k_cols(const float2* __restrict__ i
 	// the twiddle table must be complete before the first stage reads it
 	if constexpr (MODE == 1) {
 
-		fft_regs<L, B, true>(v, s, tw);
+		fft_regs<L, LAY, true>(v, s, tw);
 
 	} else {
 
-		fft_regs<L, B, false>(v, s, tw);
+		fft_regs<L, LAY, false>(v, s, tw);
 	}
 
 	if constexpr (MODE == 2) {
@@ -370,9 +318,9 @@ __global__ void __launch_bounds__(B * L / 8) k_cols(const float2* __restrict__ i
 #pragma unroll
 		for (int m = 0; m < 8; m++)
 			if (valid)
-				v[m] = cmul(v[m], pp[reg_pos<L, B>(m) * pes]);
+				v[m] = cmul(v[m], pp[reg_pos<L, LAY>(m) * pes]);
 
-		fft_regs<L, B, true>(v, s, tw);
+		fft_regs<L, LAY, true>(v, s, tw);
 	}
 
 	float2* outp = out + o * oos + cx;
@@ -381,7 +329,7 @@ __global__ void __launch_bounds__(B * L / 8) k_cols(const float2* __restrict__ i
 #pragma unroll
 		for (int m = 0; m < 8; m++) {
 
-			int p = reg_pos<L, B>(m);
+			int p = reg_pos<L, LAY>(m);
 			int n = wrap_out ? unwrap_pos(p, n_out, L) : p;
 
 			if (n < n_out)
@@ -393,24 +341,25 @@ __global__ void __launch_bounds__(B * L / 8) k_cols(const float2* __restrict__ i
 // Row pass, inverse --------------------------------------------------------------
 //
 // Input rows in[p + L*(yz + YZ*c)], p < L. Each block takes B consecutive yz
-// rows and coils [c0, c1): inverse FFT per row, keep x < X from
+// rows and coils [c0, c1) (a thread keeps its output pixels in registers
+// across the coil loop): inverse FFT per row, keep x < X from
 // wrap_pos(x, X, L), scale by ax[x]*ayz[yz] (optional) and either
 //   maps != 0: accumulate sum_c conj(maps[x + X*yz + X*YZ*c]) * row
 //              into out[x + X*yz + X*YZ*g] (g = blockIdx.y, partial per group)
 //   maps == 0: write out[x + X*yz + X*YZ*c] per coil.
 // grid (ceil(YZ/B), groups); coils per group cpg.
 template <int L, int B>
-__global__ void __launch_bounds__(B * L / 8) k_rows_inv(const float2* __restrict__ in, const float2* __restrict__ maps,
+__global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_rows_inv(const float2* __restrict__ in, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
 		int X, long YZ, int C, int cpg, float2* __restrict__ out, const float2* __restrict__ twg,
 		const float2* __restrict__ pdot, double* __restrict__ dot_part, const int* done)
 {
-	constexpr int SB = B | 1;
+	using LAY = RowLayout<L, B>;
 	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
 	__shared__ double red[32];
 	float2* s = smem;
-	float2* tw = smem + L * SB;
+	float2* tw = smem + LAY::SMEM;
 
 	if (done && *done)
 		return;
@@ -418,78 +367,45 @@ __global__ void __launch_bounds__(B * L / 8) k_rows_inv(const float2* __restrict
 	for (int i = threadIdx.x; i < L; i += NT)
 		tw[i] = twg[i];
 
-	const long yz0 = (long)blockIdx.x * B;
+	const long yz = (long)blockIdx.x * B + LAY::seq();
+	const bool valid = (yz < YZ);
 	const int g = blockIdx.y;
 	const int c0 = g * cpg;
 	const int c1 = min(C, c0 + cpg);
-	const int b = threadIdx.x % B;
 
-	// each thread owns output elements e = tid + k*NT (X*B <= 8*NT)
+	// this thread's output pixels: x = unwrap(jt + (L/8) m) where < X
 	float2 acc[8];
 #pragma unroll
-	for (int k = 0; k < 8; k++)
-		acc[k] = make_float2(0.f, 0.f);
+	for (int m = 0; m < 8; m++)
+		acc[m] = make_float2(0.f, 0.f);
 
 	for (int c = c0; c < c1; c++) {
-
-		__syncthreads();	// previous coil's readers are done with s
-
-		for (int e = threadIdx.x; e < L * B; e += NT) {
-
-			int bb = e / L;
-			int p = e % L;
-			long yz = yz0 + bb;
-			float2 v = make_float2(0.f, 0.f);
-
-			if (yz < YZ)
-				v = in[p + (long)L * (yz + YZ * c)];
-
-			s[p * SB + bb] = v;
-		}
-
-		__syncthreads();
 
 		float2 v[8];
 #pragma unroll
 		for (int m = 0; m < 8; m++)
-			v[m] = s[reg_pos<L, B>(m) * SB + b];
+			v[m] = valid ? in[reg_pos<L, LAY>(m) + (long)L * (yz + YZ * c)] : make_float2(0.f, 0.f);
 
-		fft_regs<L, B, true>(v, s, tw);
+		fft_regs<L, LAY, true>(v, s, tw);
 
-		__syncthreads();
+		if (valid) {
 #pragma unroll
-		for (int m = 0; m < 8; m++)
-			s[reg_pos<L, B>(m) * SB + b] = v[m];
-		__syncthreads();
+			for (int m = 0; m < 8; m++) {
 
-#pragma unroll
-		for (int k = 0; k < 8; k++) {
+				int x = unwrap_pos(reg_pos<L, LAY>(m), X, L);
 
-			int e = threadIdx.x + k * NT;
+				if (x >= X)
+					continue;
 
-			if (e >= X * B)
-				break;
+				float2 w = v[m];
 
-			int bb = e / X;
-			int x = e % X;
-			long yz = yz0 + bb;
+				if (ax)
+					w = cscale(w, ax[x] * ayz[yz]);
 
-			if (yz >= YZ)
-				continue;
-
-			float2 w = s[wrap_pos(x, X, L) * SB + bb];
-
-			if (ax)
-				w = cscale(w, ax[x] * ayz[yz]);
-
-			if (maps) {
-
-				float2 mp = maps[x + X * yz + X * YZ * c];
-				acc[k] = cadd(acc[k], cmulc(w, mp));
-
-			} else {
-
-				out[x + X * yz + X * YZ * c] = w;
+				if (maps)
+					acc[m] = cadd(acc[m], cmulc(w, maps[x + X * yz + X * YZ * c]));
+				else
+					out[x + X * yz + X * YZ * c] = w;
 			}
 		}
 	}
@@ -497,26 +413,22 @@ __global__ void __launch_bounds__(B * L / 8) k_rows_inv(const float2* __restrict
 	if (maps) {
 
 		double dot = 0.;
+
+		if (valid) {
 #pragma unroll
-		for (int k = 0; k < 8; k++) {
+			for (int m = 0; m < 8; m++) {
 
-			int e = threadIdx.x + k * NT;
+				int x = unwrap_pos(reg_pos<L, LAY>(m), X, L);
 
-			if (e >= X * B)
-				break;
+				if (x >= X)
+					continue;
 
-			int bb = e / X;
-			int x = e % X;
-			long yz = yz0 + bb;
-
-			if (yz < YZ) {
-
-				out[x + X * yz + X * YZ * g] = acc[k];
+				out[x + X * yz + X * YZ * g] = acc[m];
 
 				if (pdot) {	// Re<p, partial> for the CG step length
 
 					float2 pv = pdot[x + X * yz];
-					dot += (double)pv.x * (double)acc[k].x + (double)pv.y * (double)acc[k].y;
+					dot += (double)pv.x * (double)acc[m].x + (double)pv.y * (double)acc[m].y;
 				}
 			}
 		}
@@ -729,6 +641,141 @@ __global__ void k_grid_atomic(const float4* __restrict__ traj, long M, GridGeom 
 				}
 			}
 		}
+	}
+}
+
+// Deterministic gridding --------------------------------------------------------
+//
+// The adjoint interpolation as a sparse matrix in CSR form over grid cells:
+// row = cell, entries (sample, weight) in increasing sample order. It is
+// built once per trajectory (k_csr_keys + a stable radix sort by
+// cell * M + sample + k_csr_fill), after which gridding is a gather per
+// cell in that fixed order: no atomics, bit-identical results run to run,
+// and every cell is written (no clearing pass). The weights are the same
+// float32 products as in k_grid_atomic.
+
+enum { CSR_TAPS_AXIS = 8 };	// per axis: two sub-grids x up to 4 taps (width <= 6)
+
+// one key (cell * M + m, or ~0 for an unused slot) and weight per (sample, tap slot)
+__global__ void k_csr_keys(const float4* __restrict__ traj, long M, GridGeom g, const float* __restrict__ kbg,
+		unsigned long long* __restrict__ keys, float* __restrict__ vals, int slots_z)
+{
+	__shared__ float kb[KB_TABLE_N + 1];
+
+	for (int i = threadIdx.x; i <= KB_TABLE_N; i += blockDim.x)
+		kb[i] = kbg[i];
+
+	__syncthreads();
+
+	long m = (long)blockIdx.x * blockDim.x + threadIdx.x;
+
+	if (m >= M)
+		return;
+
+	float4 k = traj[m];
+	AxisTaps tx, ty, tz;
+	axis_taps(k.x, g.N[0], g.hw, g.periodic, kb, tx);
+	axis_taps(k.y, g.N[1], g.hw, g.periodic, kb, ty);
+	axis_taps(k.z, g.N[2], g.hw, g.periodic, kb, tz);
+
+	const int slots = CSR_TAPS_AXIS * CSR_TAPS_AXIS * slots_z;
+	unsigned long long* kp = keys + m * slots;
+	float* vp = vals + m * slots;
+	int t = 0;
+
+	for (int a = 0; a < tz.n; a++) {
+
+		float dz = tz.w[a];
+		long oz = (long)tz.cell[a] * g.G[1];
+
+		for (int bb = 0; bb < ty.n; bb++) {
+
+			float dzy = __fmul_rn(dz, ty.w[bb]);
+			long oy = (oz + ty.cell[bb]) * g.G[0];
+
+			for (int cc = 0; cc < tx.n; cc++) {
+
+				if (t < slots) {
+
+					kp[t] = (unsigned long long)(oy + tx.cell[cc]) * (unsigned long long)M + (unsigned long long)m;
+					vp[t] = __fmul_rn(dzy, tx.w[cc]);
+					t++;
+				}
+			}
+		}
+	}
+
+	for (; t < slots; t++) {
+
+		kp[t] = ~0ull;
+		vp[t] = 0.f;
+	}
+}
+
+// sorted keys -> column (sample) indices and per-cell counts; unused slots
+// (key ~0) sort to the end and are not counted
+__global__ void k_csr_fill_valid(const unsigned long long* __restrict__ keys, long nnz, long M, long gsz,
+		int* __restrict__ col, int* __restrict__ counts)
+{
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nnz; i += (long)gridDim.x * blockDim.x) {
+
+		unsigned long long key = keys[i];
+
+		if (~0ull == key) {
+
+			col[i] = 0;
+			continue;
+		}
+
+		long cell = (long)(key / (unsigned long long)M);
+		col[i] = (int)(key % (unsigned long long)M);
+
+		if (cell < gsz)
+			atomicAdd(&counts[cell], 1);	// integer counts: order-independent
+	}
+}
+
+// grid[cell + gsz*c] = sum over the cell's row, in row order, of w * ksp[m + M*c]
+__global__ void k_grid_csr(const long* __restrict__ row_ptr, const int* __restrict__ col, const float* __restrict__ val,
+		long gsz, long M, int C, int cpc, const float2* __restrict__ ksp, float2* __restrict__ grid)
+{
+	long cell = (long)blockIdx.x * blockDim.x + threadIdx.x;
+
+	if (cell >= gsz)
+		return;
+
+	const long r0 = row_ptr[cell];
+	const long r1 = row_ptr[cell + 1];
+	const int c0 = blockIdx.y * cpc;
+	const int c1 = min(C, c0 + cpc);
+
+	for (int cb = c0; cb < c1; cb += 4) {
+
+		float2 acc[4];
+#pragma unroll
+		for (int q = 0; q < 4; q++)
+			acc[q] = make_float2(0.f, 0.f);
+
+		for (long i = r0; i < r1; i++) {
+
+			float w = val[i];
+			long m = col[i];
+#pragma unroll
+			for (int q = 0; q < 4; q++) {
+
+				if (cb + q < c1) {
+
+					float2 y = ksp[m + M * (cb + q)];
+					acc[q].x = fmaf(y.x, w, acc[q].x);
+					acc[q].y = fmaf(y.y, w, acc[q].y);
+				}
+			}
+		}
+
+#pragma unroll
+		for (int q = 0; q < 4; q++)
+			if (cb + q < c1)
+				grid[cell + gsz * (cb + q)] = acc[q];
 	}
 }
 

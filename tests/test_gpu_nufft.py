@@ -128,3 +128,37 @@ def test_unsupported_options_fail_loudly():
         nufft_create2([1, 64, 8, 1], [32, 32, 1, 1], list(t.shape), t, conf=NufftConf(os=1.5))
     with pytest.raises(BnufftError):
         nufft_create2([1, 64, 8, 1], [33, 33, 1, 1], list(t.shape), t)
+
+
+@pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
+                                           ("nufft3d_n16", False), ("nufft2d_n32_coils3", False)])
+def test_deterministic_mode_vs_reference(name, periodic):
+    """Fixed-order (atomic-free) gridding: same parity bar as the default."""
+    g = golden(name)
+    img = g["img"]
+    cd = _dims(img.shape)
+    td = list(g["traj"].shape)
+    kd = [1, td[1], td[2], cd[3]]
+    toep = "normal" in g
+    op = nufft_create2(kd, cd, td, g["traj"], conf=NufftConf(toeplitz=toep, periodic=periodic, deterministic=True))
+    assert rel(op.forward(img.reshape(cd, order="F")), g["fwd"]) < TOL
+    assert rel(op.adjoint(g["ksp"].reshape(kd, order="F")), g["adj"]) < TOL
+    if toep:
+        assert rel(op.normal(img.reshape(cd, order="F")), g["normal"]) < TOL
+    op.free()
+
+
+def test_deterministic_mode_is_bit_identical():
+    """Two plans, two adjoints (and PSFs) of the same data: identical bits."""
+    rng = np.random.default_rng(9)
+    t = synth.radial_traj(256, 402)
+    kd = [1, 512, 402, 4]
+    cd = [256, 256, 1, 4]
+    y = (rng.standard_normal(kd) + 1j * rng.standard_normal(kd)).astype(np.complex64)
+    outs = []
+    for _ in range(2):
+        op = nufft_create2(kd, cd, list(t.shape), t, conf=NufftConf(toeplitz=True, deterministic=True))
+        outs.append((np.asarray(op.adjoint(y)).copy(), op.psf().copy()))
+        op.free()
+    assert np.array_equal(outs[0][0].view(np.uint32), outs[1][0].view(np.uint32))
+    assert np.array_equal(outs[0][1].view(np.uint32), outs[1][1].view(np.uint32))

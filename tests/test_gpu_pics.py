@@ -73,3 +73,15 @@ def test_sense_normal_vs_oracle():
     p.free()
     A = orc.SenseOracle(g["traj"].real.reshape(3, -1, order="F"), g["sens"])
     assert rel(n, A.normal(x.reshape(64, 64, 1, 1))) < 1e-5
+
+
+def test_pics_deterministic_mode_bit_identical():
+    """Deterministic mode: two full reconstructions give identical bits, and
+    the result still matches the reference at 5 iterations."""
+    g = golden("pics2d_n64_c4")
+    x1, st1 = _run(g, maxiter=30, deterministic=True)
+    x2, st2 = _run(g, maxiter=30, deterministic=True)
+    assert np.array_equal(np.asarray(x1).view(np.uint32), np.asarray(x2).view(np.uint32))
+    assert st1 == st2
+    x5, _ = _run(g, maxiter=5, scaling=1.0, deterministic=True)
+    assert rel(x5, g["x5_w1"]) < 1e-5
