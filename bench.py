@@ -106,6 +106,133 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def nufft_throughput(dev, steps=50, warmup=5):
+    """NUFFT GB/s on the 2D single-coil workload: 256^2
+    i.i.d. complex Gaussian image, 402 golden-angle spokes x 512 samples,
+    os 2, width 6. One step = forward + adjoint on device-resident data with
+    the plan reused; bytes = compulsory I/O of both directions (image, k-space,
+    trajectory as 2 float32 per sample)."""
+    import torch
+    from bart_b200 import synth
+    from bart_b200.nufft import NufftConf, nufft_create2
+    rng = np.random.default_rng(1)
+    t = synth.radial_traj(256, 402)
+    img = synth.random_image(256, rng)
+    M = t.shape[1] * t.shape[2]
+    op = nufft_create2([1, t.shape[1], t.shape[2], 1], [256, 256, 1, 1], list(t.shape), t,
+                       conf=NufftConf(toeplitz=False))
+    x = torch.from_numpy(np.asfortranarray(img).ravel(order="F").copy()).to(dev)
+    k = torch.empty(M, dtype=torch.complex64, device=dev)
+    a = torch.empty(256 * 256, dtype=torch.complex64, device=dev)
+    for _ in range(warmup):
+        op.forward(x, k)
+        op.adjoint(k, a)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        op.forward(x, k)
+        op.adjoint(k, a)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    op.free()
+    nbytes = 2 * (256 * 256 * 8 + M * 8 + M * 8)
+    return {"workload": "nufft2d_256_r402x512_c1_fwd+adj", "value": nbytes / (ms * 1e-3) / 1e9, "unit": "GB/s",
+            "us_per_fwd_adj": ms * 1e3, "bytes_per_step": nbytes}
+
+
+def cg_to_tolerance(dev, traj, sens, ksp, tol=1e-4, maxiter=300, runs=5):
+    """Plain CG on the CG-SENSE workload until ||r|| <= tol ||A^H y|| (the
+    recursive residual), model reused; reports iterations, time per solve and
+    the true relative normal-equation residual of the result."""
+    import torch
+    from bart_b200.nufft import NufftConf, nufft_create2
+    from bart_b200.pics import Pics, PicsConf
+
+    def dt(a):
+        return torch.from_numpy(np.asfortranarray(a).ravel(order="F").copy()).to(dev)
+
+    traj_d, sens_d, ksp_d = dt(traj), dt(sens), dt(ksp)
+    p = Pics(traj_d, sens_d, ksp_dims=list(ksp.shape), conf=PicsConf(lam=LAM, maxiter=maxiter, tol=tol),
+             traj_dims=list(traj.shape), sens_dims=list(sens.shape))
+    x = p.run(ksp_d)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(runs):
+        p.run(ksp_d, out=x)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / runs
+    iters, rres, scale = p.stats()
+    # true residual: b = A^H y / scale, r = b - (A^H A + lambda) x
+    kd = list(ksp.shape)
+    op = nufft_create2(kd, [N_IMG, N_IMG, 1, COILS], list(traj.shape), traj_d, conf=NufftConf(toeplitz=False))
+    adj = op.adjoint(ksp_d).reshape(COILS, N_IMG * N_IMG)
+    b = (torch.conj(sens_d.reshape(COILS, N_IMG * N_IMG)) * adj).sum(0) / scale
+    r = b - (p.normal(x) + LAM * x)
+    true_res = float(torch.linalg.vector_norm(r) / torch.linalg.vector_norm(b))
+    op.free()
+    p.free()
+    return {"tol": tol, "iterations": iters, "ms_per_recon_model_reused": ms, "recons_per_s_model_reused": 1e3 / ms,
+            "recursive_rel_residual": rres, "true_rel_residual": true_res}
+
+
+def run_nufft3d(dev, steps, warmup):
+    """3D radial kooshball NUFFT: 128^3 image, 8 coils,
+    20000 spokes x 256 samples on 3D golden means (5.12 M samples per coil).
+    One step = forward + adjoint of all 8 coil images, device-resident, plan
+    reused. Also times a 10-iteration Toeplitz CG-SENSE solve (model reused)."""
+    import torch
+    from bart_b200 import synth
+    from bart_b200.nufft import NufftConf, nufft_create2
+    from bart_b200.pics import Pics, PicsConf
+    N, C, spokes, readout = 128, 8, 20000, 128
+    rng = np.random.default_rng(3)
+    t = synth.kooshball_traj(readout, spokes)
+    M = t.shape[1] * t.shape[2]
+    sens = synth.coil_maps(N, C, rng, ndim=3)
+    truth = synth.ellipse_phantom(N, 20, rng, ndim=3)
+    cd = [N, N, N, C]
+    kd = [1, t.shape[1], t.shape[2], C]
+    t_d = torch.from_numpy(np.asfortranarray(t).ravel(order="F").copy()).to(dev)
+    cim = torch.from_numpy(np.asfortranarray(truth.reshape(N, N, N, 1) * sens).ravel(order="F").copy()).to(dev)
+    op = nufft_create2(kd, cd, list(t.shape), t_d, conf=NufftConf(toeplitz=False))
+    k = torch.empty(M * C, dtype=torch.complex64, device=dev)
+    a = torch.empty(N ** 3 * C, dtype=torch.complex64, device=dev)
+    for _ in range(warmup):
+        op.forward(cim, k)
+        op.adjoint(k, a)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        op.forward(cim, k)
+        op.adjoint(k, a)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    op.free()
+    nbytes = 2 * (N ** 3 * C * 8 + M * C * 8 + M * 12)
+    sens_d = torch.from_numpy(np.asfortranarray(sens).ravel(order="F").copy()).to(dev)
+    t0 = time.perf_counter()
+    p = Pics(t_d, sens_d, ksp_dims=kd, conf=PicsConf(lam=LAM, maxiter=10), traj_dims=list(t.shape), sens_dims=cd)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    x = p.run(k)
+    torch.cuda.synchronize()
+    e0.record()
+    p.run(k, out=x)
+    e1.record()
+    torch.cuda.synchronize()
+    cg_ms = e0.elapsed_time(e1)
+    p.free()
+    return {"workload": "nufft3d_128_c8_kooshball_20000x256", "nufft_fwd_adj_ms": ms,
+            "nufft_gbs": nbytes / (ms * 1e-3) / 1e9, "bytes_per_step": nbytes,
+            "cgsense_setup_s": setup_s, "cgsense_10iter_ms": cg_ms}
+
+
 def reference_pics_seconds(traj, sens, ksp, iters=ITERS, threads=None):
     """Wall time of the reference's own CPU ``pics`` (built from its sources
     into oracle/_ref) on this workload, or None if it is not built."""
@@ -183,6 +310,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d"])
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -206,7 +334,14 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
     lib = _lib.load()
-    traj, truth, sens, rng = make_problem(1000 + rank)
+
+    if args.workload == "nufft3d":
+        if rank == 0:
+            print(json.dumps(run_nufft3d(dev, args.steps, args.warmup)), flush=True)
+        return
+
+    from bart_b200.dist import aggregate_rate, rank_seed, reduce_max
+    traj, truth, sens, rng = make_problem(rank_seed(1000, rank))
     ksp = simulate_ksp(traj, truth, sens, rng)
 
     def dev_tensor(a):
@@ -245,11 +380,9 @@ def main():
     kms, kn = ctypes.c_double(), ctypes.c_long()
     lib.bnufft_prof_stop(ctypes.byref(kms), ctypes.byref(kn))
 
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    ms_max = reduce_max(ms, dev)
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    ms_max = float(t.item())
 
     # end to end through the host API: host arrays in, host image out
     h2d = traj.nbytes + sens.nbytes + ksp.nbytes
@@ -270,9 +403,7 @@ def main():
     for _ in range(e2e_steps):
         step_host()
     torch.cuda.synchronize()
-    e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+    e2e_s = reduce_max(time.perf_counter() - t0, dev)
 
     # roofline of the dominant kernel: Toeplitz column pass, per launch
     # reads + writes the [2X, Y, C] row-transformed buffer and reads the PSF
@@ -291,17 +422,28 @@ def main():
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get(DOMINANT)
 
+    nufft = nufft_throughput(dev) if rank == 0 else None
+    to_tol = cg_to_tolerance(dev, traj, sens, ksp) if rank == 0 else None
+    # residual reached by the timed 30-iteration solve
+    p30 = Pics(traj_d, sens_d, ksp_dims=list(ksp.shape), conf=conf, traj_dims=list(traj.shape),
+               sens_dims=list(sens.shape))
+    p30.run(ksp_d, out=img_d)
+    it30, res30, _ = p30.stats()
+    p30.free()
+
     if rank == 0:
-        value = world * args.steps / (ms_max / 1e3)
+        value = aggregate_rate(world, args.steps, ms_max / 1e3)
         line = {"metric": METRIC, "value": value, "unit": "recons/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "image": N_IMG, "coils": COILS, "spokes": SPOKES, "samples": 512,
                            "iters": ITERS, "lambda": LAM, "toeplitz": True, "parallelism": f"replicas{world}",
                            "l2": "inputs and work buffers (~60 MB) are L2-resident; no flush between steps"},
-                "e2e": {"value": world * e2e_steps / float(e2e_s.item()), "unit": "recons/s",
+                "e2e": {"value": aggregate_rate(world, e2e_steps, e2e_s), "unit": "recons/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches,
+                "cg": {"iterations": it30, "recursive_rel_residual": res30, "to_1e-4": to_tol},
+                "nufft": nufft,
                 "roofline": {"bound": "hbm", "kernel": DOMINANT, "achieved": achieved, "peak": peak,
                              "peak_source": peak_src, "unit": "GB/s",
                              "frac": (achieved / peak) if achieved else None,
