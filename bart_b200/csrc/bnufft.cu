@@ -19,6 +19,7 @@
 #include "../../include/bnufft.h"
 #include "nufft_kernels.cuh"
 #include "cg_kernels.cuh"
+#include "gridding.cuh"
 
 using namespace bn;
 
@@ -450,6 +451,19 @@ struct Csr {
 	long nnz = 0;
 };
 
+// samples sorted by bin of the oversampled grid, cut into sub-blocks
+struct Bins {
+
+	BinGeom bg;
+	int* perm = nullptr;		// [M] sorted position -> sample index
+	float4* traj = nullptr;		// [M] trajectory in sorted order
+	int* sub_bin = nullptr;
+	int* sub_first = nullptr;
+	int* sub_count = nullptr;
+	int nsub = 0;
+	int cc = 1;			// coil tiles held in shared memory at once
+};
+
 struct OpCtx {
 
 	Geom g;
@@ -459,7 +473,19 @@ struct OpCtx {
 	float* ayz = nullptr;	// [N1*N2] roll-off along y,z with 1/sqrt(npix)
 	Work w;
 	Csr csr;		// set in deterministic mode
+	Bins bins;		// binned gridding (all modes)
 };
+
+static void free_bins(Bins& b, cudaStream_t st)
+{
+	void* ptrs[] = { b.perm, b.traj, b.sub_bin, b.sub_first, b.sub_count };
+
+	for (void* q : ptrs)
+		if (q)
+			cudaFreeAsync(q, st);
+
+	b = Bins{};
+}
 
 static void free_csr(Csr& c, cudaStream_t st)
 {
@@ -696,6 +722,23 @@ static int op_spectrum_adjoint(OpCtx& op, const float2* grid, const float2* maps
 
 static int degrid(OpCtx& op, const float2* grid, long C, float2* ksp, cudaStream_t st)
 {
+	if (op.bins.perm) {
+
+		const Bins& b = op.bins;
+		int cc = (int)std::min<long>(b.cc, C);
+		size_t smem = sizeof(float2) * b.bg.ncells * cc;
+		TRY(prep_kernel(k_degrid_binned, smem));
+		cudaEvent_t pe = prof_begin("degrid", st);
+
+		if (b.nsub > 0)
+			k_degrid_binned<<<b.nsub, BIN_THREADS, smem, st>>>(b.traj, b.perm, op.g.M, grid_geom(op.g), b.bg,
+					b.sub_bin, b.sub_first, b.sub_count, (int)C, cc, grid, ksp, op.kb);
+
+		prof_end(pe, st);
+		LAUNCHED();
+		return BNUFFT_OK;
+	}
+
 	int cpc = (int)std::min<long>(C, 8);
 	dim3 blocks((unsigned)((op.g.M + 127) / 128), (unsigned)((C + cpc - 1) / cpc));
 	cudaEvent_t pe = prof_begin("degrid", st);
@@ -719,6 +762,24 @@ static int grid_adj(OpCtx& op, const float2* ksp, long C, float2* grid, cudaStre
 	}
 
 	CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(float2) * op.g.gsz * C, st));
+
+	if (op.bins.perm) {
+
+		const Bins& b = op.bins;
+		int cc = (int)std::min<long>(b.cc, C);
+		size_t smem = sizeof(float2) * b.bg.ncells * cc;
+		TRY(prep_kernel(k_grid_binned, smem));
+		cudaEvent_t pe = prof_begin("grid", st);
+
+		if (b.nsub > 0)
+			k_grid_binned<<<b.nsub, BIN_THREADS, smem, st>>>(b.traj, b.perm, op.g.M, grid_geom(op.g), b.bg,
+					b.sub_bin, b.sub_first, b.sub_count, (int)C, cc, ksp, grid, op.kb);
+
+		prof_end(pe, st);
+		LAUNCHED();
+		return BNUFFT_OK;
+	}
+
 	int cpc = (int)std::min<long>(C, 8);
 	dim3 blocks((unsigned)((op.g.M + 127) / 128), (unsigned)((C + cpc - 1) / cpc));
 	cudaEvent_t pe = prof_begin("grid", st);
@@ -792,6 +853,91 @@ static int build_csr(OpCtx& op, cudaStream_t st)
 	cudaFreeAsync(counts, st);
 	cudaFreeAsync(tmp, st);
 	cudaFreeAsync(scan_tmp, st);
+	return BNUFFT_OK;
+}
+
+// Sort the samples by bin and cut bins into sub-blocks (plan time).
+static int build_bins(OpCtx& op, cudaStream_t st)
+{
+	const Geom& g = op.g;
+	Bins& b = op.bins;
+	BinGeom& bg = b.bg;
+	const int bs_axis = (g.G[2] > 1) ? 16 : 32;
+	long nbins = 1;
+	bg.ncells = 1;
+
+	for (int a = 0; a < 3; a++) {
+
+		bg.bs[a] = (g.G[a] > 1) ? std::min(bs_axis, g.G[a]) : 1;
+		bg.nb[a] = (g.G[a] + bg.bs[a] - 1) / bg.bs[a];
+		bg.tile[a] = (g.G[a] > 1) ? bg.bs[a] + 2 * BIN_HALO : 1;
+		nbins *= bg.nb[a];
+		bg.ncells *= bg.tile[a];
+	}
+
+	if ((g.M >= (1L << 31)) || (nbins >= (1L << 31)))
+		return fail(BNUFFT_ERR_UNSUPPORTED, "binning: %ld samples, %ld bins", g.M, nbins);
+
+	unsigned *keys = nullptr, *keys2 = nullptr;
+	int *vals = nullptr, *counts = nullptr, *bin_start = nullptr, *nsub = nullptr, *sub_start = nullptr;
+	void* tmp = nullptr;
+	size_t tmp_bytes = 0, tmp2 = 0;
+	long M = g.M;
+
+	CUDA_TRY(cudaMallocAsync(&keys, sizeof(unsigned) * M, st));
+	CUDA_TRY(cudaMallocAsync(&keys2, sizeof(unsigned) * M, st));
+	CUDA_TRY(cudaMallocAsync(&vals, sizeof(int) * M, st));
+	CUDA_TRY(cudaMallocAsync(&b.perm, sizeof(int) * M, st));
+	CUDA_TRY(cudaMallocAsync(&b.traj, sizeof(float4) * M, st));
+	CUDA_TRY(cudaMallocAsync(&counts, sizeof(int) * (nbins + 1), st));
+	CUDA_TRY(cudaMallocAsync(&bin_start, sizeof(int) * (nbins + 1), st));
+	CUDA_TRY(cudaMallocAsync(&nsub, sizeof(int) * (nbins + 1), st));
+	CUDA_TRY(cudaMallocAsync(&sub_start, sizeof(int) * (nbins + 1), st));
+	CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int) * (nbins + 1), st));
+
+	k_bin_keys<<<vec_blocks(M), RED_THREADS, 0, st>>>(op.traj, M, grid_geom(g), bg, keys, vals, counts);
+	LAUNCHED();
+
+	int end_bit = 1;
+
+	while ((1L << end_bit) < nbins)
+		end_bit++;
+
+	CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, vals, b.perm, (int)M, 0, end_bit, st));
+	CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, counts, bin_start, (int)(nbins + 1), st));
+	tmp_bytes = std::max(tmp_bytes, tmp2);
+	CUDA_TRY(cudaMallocAsync(&tmp, tmp_bytes, st));
+	CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys2, vals, b.perm, (int)M, 0, end_bit, st));
+	CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, counts, bin_start, (int)(nbins + 1), st));
+	g_launches.fetch_add(2, std::memory_order_relaxed);
+
+	// sub-blocks per bin: ceil(count / BIN_SUB); their start indices
+	k_bin_nsub<<<vec_blocks(nbins + 1), RED_THREADS, 0, st>>>(bin_start, (int)nbins, nsub);
+	LAUNCHED();
+	CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, nsub, sub_start, (int)(nbins + 1), st));
+	g_launches.fetch_add(1, std::memory_order_relaxed);
+
+	int total = 0;
+	CUDA_TRY(cudaMemcpyAsync(&total, sub_start + nbins, sizeof(int), cudaMemcpyDeviceToHost, st));
+	CUDA_TRY(cudaStreamSynchronize(st));
+	b.nsub = total;
+
+	CUDA_TRY(cudaMallocAsync(&b.sub_bin, sizeof(int) * std::max(1, total), st));
+	CUDA_TRY(cudaMallocAsync(&b.sub_first, sizeof(int) * std::max(1, total), st));
+	CUDA_TRY(cudaMallocAsync(&b.sub_count, sizeof(int) * std::max(1, total), st));
+	k_sub_fill<<<vec_blocks(nbins), RED_THREADS, 0, st>>>(bin_start, sub_start, (int)nbins, b.sub_bin, b.sub_first, b.sub_count);
+	LAUNCHED();
+	k_gather_traj<<<vec_blocks(M), RED_THREADS, 0, st>>>(b.traj, op.traj, b.perm, M);
+	LAUNCHED();
+
+	// coil tiles per pass: as many as fit in ~110 KB of shared memory
+	b.cc = (int)std::max(1L, std::min(8L, (110L * 1024) / (long)(sizeof(float2) * bg.ncells)));
+
+	void* frees[] = { keys, keys2, vals, counts, bin_start, nsub, sub_start, tmp };
+
+	for (void* q : frees)
+		cudaFreeAsync(q, st);
+
 	return BNUFFT_OK;
 }
 
@@ -875,11 +1021,14 @@ static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, flo
 	in.kb = kb;
 	TRY(init_rolloff(in, st));
 
+	TRY(build_bins(in, st));
+
 	if (deterministic)
 		TRY(build_csr(in, st));
 
 	TRY(op_adjoint(in, ones, nullptr, 1, 1, psft, st));
 	free_csr(in.csr, st);
+	free_bins(in.bins, st);
 
 	// full 2N-point transform of the 2N image: input centred (ifftshift), output in DFT order
 	OpCtx full;
@@ -1040,6 +1189,9 @@ static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
 	TRY(stage_in(t, traj, sizeof(float2) * 3 * p->op.g.M, st));
 	k_traj_convert<<<vec_blocks(p->op.g.M), RED_THREADS, 0, st>>>(p->traj, (const float2*)t.dev, p->op.g.M, 1.f);
 	LAUNCHED();
+
+	free_bins(p->op.bins, st);
+	TRY(build_bins(p->op, st));
 
 	if (p->conf.deterministic) {
 
@@ -1287,6 +1439,7 @@ extern "C" void bnufft_free(bnufft_plan_t p)
 	cudaStream_t st = p->st0;
 	free_work(p->op.w, st);
 	free_csr(p->op.csr, st);
+	free_bins(p->op.bins, st);
 
 	if (p->traj) cudaFreeAsync(p->traj, st);
 	if (p->psf) cudaFreeAsync(p->psf, st);
