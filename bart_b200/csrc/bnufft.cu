@@ -460,7 +460,9 @@ struct Bins {
 	int* sub_bin = nullptr;
 	int* sub_first = nullptr;
 	int* sub_count = nullptr;
-	int nsub = 0;
+	int* sub_start = nullptr;	// [nbins + 1]; sub_start[nbins] = number of sub-blocks
+	const int* nsub_dev = nullptr;
+	int nsub = 0;			// upper bound of sub-blocks (launch size)
 	int cc = 1;			// coil tiles held in shared memory at once
 };
 
@@ -478,7 +480,7 @@ struct OpCtx {
 
 static void free_bins(Bins& b, cudaStream_t st)
 {
-	void* ptrs[] = { b.perm, b.traj, b.sub_bin, b.sub_first, b.sub_count };
+	void* ptrs[] = { b.perm, b.traj, b.sub_bin, b.sub_first, b.sub_count, b.sub_start };
 
 	for (void* q : ptrs)
 		if (q)
@@ -722,17 +724,16 @@ static int op_spectrum_adjoint(OpCtx& op, const float2* grid, const float2* maps
 
 static int degrid(OpCtx& op, const float2* grid, long C, float2* ksp, cudaStream_t st)
 {
-	if (op.bins.perm) {
+	if (op.bins.perm && (6.f == op.g.width)) {
 
 		const Bins& b = op.bins;
-		int cc = (int)std::min<long>(b.cc, C);
-		size_t smem = sizeof(float2) * b.bg.ncells * cc;
-		TRY(prep_kernel(k_degrid_binned, smem));
 		cudaEvent_t pe = prof_begin("degrid", st);
+		unsigned nb = (unsigned)((op.g.M + BIN_THREADS - 1) / BIN_THREADS);
 
-		if (b.nsub > 0)
-			k_degrid_binned<<<b.nsub, BIN_THREADS, smem, st>>>(b.traj, b.perm, op.g.M, grid_geom(op.g), b.bg,
-					b.sub_bin, b.sub_first, b.sub_count, (int)C, cc, grid, ksp, op.kb);
+		if (op.g.G[2] > 1)
+			k_degrid6<6><<<nb, BIN_THREADS, 0, st>>>(b.traj, b.perm, op.g.M, grid_geom(op.g), (int)C, grid, ksp, op.kb);
+		else
+			k_degrid6<1><<<nb, BIN_THREADS, 0, st>>>(b.traj, b.perm, op.g.M, grid_geom(op.g), (int)C, grid, ksp, op.kb);
 
 		prof_end(pe, st);
 		LAUNCHED();
@@ -763,17 +764,25 @@ static int grid_adj(OpCtx& op, const float2* ksp, long C, float2* grid, cudaStre
 
 	CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(float2) * op.g.gsz * C, st));
 
-	if (op.bins.perm) {
+	if (op.bins.perm && (6.f == op.g.width)) {
 
 		const Bins& b = op.bins;
 		int cc = (int)std::min<long>(b.cc, C);
 		size_t smem = sizeof(float2) * b.bg.ncells * cc;
-		TRY(prep_kernel(k_grid_binned, smem));
 		cudaEvent_t pe = prof_begin("grid", st);
 
-		if (b.nsub > 0)
-			k_grid_binned<<<b.nsub, BIN_THREADS, smem, st>>>(b.traj, b.perm, op.g.M, grid_geom(op.g), b.bg,
-					b.sub_bin, b.sub_first, b.sub_count, (int)C, cc, ksp, grid, op.kb);
+		if (op.g.G[2] > 1) {
+
+			TRY(prep_kernel(k_grid6_binned<6>, smem));
+			k_grid6_binned<6><<<b.nsub, BIN_THREADS, smem, st>>>(b.traj, b.perm, op.g.M, grid_geom(op.g), b.bg,
+					b.sub_bin, b.sub_first, b.sub_count, b.nsub_dev, (int)C, cc, ksp, grid, op.kb);
+
+		} else {
+
+			TRY(prep_kernel(k_grid6_binned<1>, smem));
+			k_grid6_binned<1><<<b.nsub, BIN_THREADS, smem, st>>>(b.traj, b.perm, op.g.M, grid_geom(op.g), b.bg,
+					b.sub_bin, b.sub_first, b.sub_count, b.nsub_dev, (int)C, cc, ksp, grid, op.kb);
+		}
 
 		prof_end(pe, st);
 		LAUNCHED();
@@ -917,14 +926,16 @@ static int build_bins(OpCtx& op, cudaStream_t st)
 	CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, nsub, sub_start, (int)(nbins + 1), st));
 	g_launches.fetch_add(1, std::memory_order_relaxed);
 
-	int total = 0;
-	CUDA_TRY(cudaMemcpyAsync(&total, sub_start + nbins, sizeof(int), cudaMemcpyDeviceToHost, st));
-	CUDA_TRY(cudaStreamSynchronize(st));
-	b.nsub = total;
+	// the number of sub-blocks stays on the device (no host round trip);
+	// launches use the upper bound nbins + M / BIN_SUB and surplus blocks exit
+	long total = nbins + M / BIN_SUB + 1;
+	b.nsub = (int)total;
+	b.sub_start = sub_start;
+	b.nsub_dev = sub_start + nbins;
 
-	CUDA_TRY(cudaMallocAsync(&b.sub_bin, sizeof(int) * std::max(1, total), st));
-	CUDA_TRY(cudaMallocAsync(&b.sub_first, sizeof(int) * std::max(1, total), st));
-	CUDA_TRY(cudaMallocAsync(&b.sub_count, sizeof(int) * std::max(1, total), st));
+	CUDA_TRY(cudaMallocAsync(&b.sub_bin, sizeof(int) * total, st));
+	CUDA_TRY(cudaMallocAsync(&b.sub_first, sizeof(int) * total, st));
+	CUDA_TRY(cudaMallocAsync(&b.sub_count, sizeof(int) * total, st));
 	k_sub_fill<<<vec_blocks(nbins), RED_THREADS, 0, st>>>(bin_start, sub_start, (int)nbins, b.sub_bin, b.sub_first, b.sub_count);
 	LAUNCHED();
 	k_gather_traj<<<vec_blocks(M), RED_THREADS, 0, st>>>(b.traj, op.traj, b.perm, M);
@@ -933,7 +944,7 @@ static int build_bins(OpCtx& op, cudaStream_t st)
 	// coil tiles per pass: as many as fit in ~110 KB of shared memory
 	b.cc = (int)std::max(1L, std::min(8L, (110L * 1024) / (long)(sizeof(float2) * bg.ncells)));
 
-	void* frees[] = { keys, keys2, vals, counts, bin_start, nsub, sub_start, tmp };
+	void* frees[] = { keys, keys2, vals, counts, bin_start, nsub, tmp };
 
 	for (void* q : frees)
 		cudaFreeAsync(q, st);

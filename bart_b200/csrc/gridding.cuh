@@ -6,13 +6,14 @@
 // (dense bins at the k-space centre become several sub-blocks, so the work
 // is balanced). The sorted trajectory is stored as float4 (coalesced loads).
 //
-// Degridding (gather): a block takes one sub-block, loads its bin's tile plus
-// a halo of HALO cells per side for a chunk of coils into shared memory
-// (coalesced rows), then every sample gathers its taps from the tile.
-// Gridding (scatter): a block accumulates its samples' taps into a zeroed
-// shared-memory tile with shared-memory atomics and flushes the touched cells
-// to the grid with one global float2 atomic each, instead of one global atomic
-// per tap.
+// Degridding (gather): one thread per sample in bin order; neighbouring
+// threads read overlapping taps, so the gathers hit L1, and the weights are
+// computed once per sample for all coils.
+// Gridding (scatter): a block takes one sub-block, accumulates its samples'
+// taps into a zeroed shared-memory tile (the bin plus a halo of HALO cells per
+// side, for a chunk of coils) with shared-memory atomics, and flushes the
+// touched cells to the grid with one global float2 atomic each, instead of one
+// global atomic per tap.
 //
 // Taps and weights are those of axis_taps (bit-identical to the reference's,
 // src/noncart/grid.c:403-465); only the cell index changes from the DFT-order
@@ -34,57 +35,6 @@ struct BinGeom {
 	int tile[3];	// tile extent per axis (bs + 2 * halo, or 1)
 	long ncells;	// tile cells
 };
-
-// Taps of one axis relative to a tile origin (centred 2N index of the tile's
-// first cell). Same taps / weights as axis_taps; cell = tile-local index.
-__device__ __forceinline__ void axis_taps_local(float k, int N, float hw, int periodic, const float* kb,
-		int origin, int extent, AxisTaps& t)
-{
-	t.n = 0;
-
-	if (1 == N) {
-
-		t.cell[0] = 0;
-		t.w[0] = kb_lookup(kb, 0.f);
-		t.n = 1;
-		return;
-	}
-
-	const int L = 2 * N;
-	const float half = (float)(N / 2);
-	const double h2 = 0.5 * (double)hw;
-
-#pragma unroll
-	for (int s = 0; s < 2; s++) {
-
-		float pos = __fadd_rn(__fadd_rn(k, s ? -0.5f : -0.0f), half);
-		int sti = (int)ceil((double)pos - h2);
-		int eni = (int)floor((double)pos + h2);
-
-		if (!periodic) {
-
-			sti = max(sti, 0);
-			eni = min(eni, N - 1);
-		}
-
-		for (int w = sti; (w <= eni) && (t.n < MAX_AXIS_TAPS); w++) {
-
-			float frac = fabsf(__fsub_rn((float)w, pos));
-			float val = kb_lookup(kb, __fdiv_rn(frac, hw));
-			int local = 2 * w + s - origin;
-
-			if (periodic)	// the tap may sit one period away from the tile
-				local = ((local % L) + L) % L;
-
-			if ((local < 0) || (local >= extent))
-				continue;	// cannot happen for a sample of this bin
-
-			t.cell[t.n] = local;
-			t.w[t.n] = val;
-			t.n++;
-		}
-	}
-}
 
 // centred 2N position of a sample along an axis -> bin index
 __device__ __forceinline__ int bin_of(float k, int N, int bs, int nb, int periodic)
@@ -208,99 +158,159 @@ __device__ __forceinline__ long tile_to_grid(int lx, int ly, int lz, const TileO
 	return idx;
 }
 
-// Degridding: ksp[perm[i] + M*c] for the samples of each sub-block, coils in
-// chunks of cc tiles held in shared memory at once.
-__global__ void __launch_bounds__(BIN_THREADS) k_degrid_binned(const float4* __restrict__ traj_sorted,
-		const int* __restrict__ perm, long M, GridGeom g, BinGeom bg,
-		const int* __restrict__ sub_bin, const int* __restrict__ sub_first, const int* __restrict__ sub_count,
-		int C, int cc, const float2* __restrict__ grid, float2* __restrict__ ksp, const float* __restrict__ kbg)
+// Width-6 fast path ------------------------------------------------------------
+//
+// For the default kernel width 6 (hw = 3 on the N-grid) each sub-grid has
+// exactly three taps with weight: the window [pos - 1.5, pos + 1.5] holds
+// three integers, or four when pos - 1.5 is an integer, and then both end
+// taps sit at |t - pos| = 1.5 where the table is exactly 0 (kb(0.5) = 0,
+// src/noncart/grid.c:75-76); the lower one is dropped. Taps clipped by a
+// non-periodic grid keep weight 0 and a harmless cell index. The fixed trip
+// count lets every tap loop unroll into registers.
+struct Taps6 {
+
+	int cell[6];
+	float w[6];
+};
+
+// MODE 0: cell = DFT-order grid index; MODE 1: cell = tile-local index
+template <int MODE>
+__device__ __forceinline__ void axis_taps6(float k, int N, int periodic, const float* kb, int origin, Taps6& t)
 {
-	extern __shared__ float2 tiles[];	// [cc][ncells]
-	__shared__ float kb[KB_TABLE_N + 1];
+	if (1 == N) {
+#pragma unroll
+		for (int q = 0; q < 6; q++) {
 
-	for (int i = threadIdx.x; i <= KB_TABLE_N; i += blockDim.x)
-		kb[i] = kbg[i];
-
-	const int sb = blockIdx.x;
-	const int bin = sub_bin[sb];
-	const int first = sub_first[sb];
-	const int count = sub_count[sb];
-	const TileOrigin to = tile_origin(bin, bg, g);
-	const int tx = bg.tile[0], ty = bg.tile[1];
-
-	for (int c0 = 0; c0 < C; c0 += cc) {
-
-		const int cn = min(cc, C - c0);
-
-		__syncthreads();	// previous chunk's readers are done
-
-		for (long t = threadIdx.x; t < bg.ncells * cn; t += blockDim.x) {
-
-			int c = (int)(t / bg.ncells);
-			long cell = t - (long)c * bg.ncells;
-			int lx = (int)(cell % tx);
-			int ly = (int)((cell / tx) % ty);
-			int lz = (int)(cell / ((long)tx * ty));
-			long gi = tile_to_grid(lx, ly, lz, to, g);
-			tiles[(long)c * bg.ncells + cell] = (gi >= 0) ? grid[gi + g.gsz * (c0 + c)] : make_float2(0.f, 0.f);
+			t.cell[q] = 0;
+			t.w[q] = (0 == q) ? kb_lookup(kb, 0.f) : 0.f;
 		}
 
-		__syncthreads();
+		return;
+	}
 
-		for (int i = threadIdx.x; i < count; i += blockDim.x) {
+	const int L = 2 * N;
+	const float half = (float)(N / 2);
 
-			float4 k = traj_sorted[first + i];
-			AxisTaps ax, ay, az;
-			axis_taps_local(k.x, g.N[0], g.hw, g.periodic, kb, to.o[0], bg.tile[0], ax);
-			axis_taps_local(k.y, g.N[1], g.hw, g.periodic, kb, to.o[1], bg.tile[1], ay);
-			axis_taps_local(k.z, g.N[2], g.hw, g.periodic, kb, to.o[2], bg.tile[2], az);
-			const long m = perm[first + i];
+#pragma unroll
+	for (int s = 0; s < 2; s++) {
 
-			for (int c = 0; c < cn; c++) {
+		float pos = __fadd_rn(__fadd_rn(k, s ? -0.5f : -0.0f), half);
+		double lo = (double)pos - 1.5;
+		int sti = (int)ceil(lo);
 
-				const float2* tl = tiles + (long)c * bg.ncells;
-				float2 acc = make_float2(0.f, 0.f);
+		if ((double)sti == lo)
+			sti += 1;
 
-				for (int a = 0; a < az.n; a++) {
+#pragma unroll
+		for (int q = 0; q < 3; q++) {
 
-					float dz = az.w[a];
-					int oz = az.cell[a] * ty;
+			int w = sti + q;
+			float frac = fabsf(__fsub_rn((float)w, pos));
+			float val = kb_lookup(kb, __fdiv_rn(frac, 3.0f));
+			bool valid = periodic || ((w >= 0) && (w <= N - 1));
+			int cell;
 
-					for (int b = 0; b < ay.n; b++) {
+			if (0 == MODE) {
 
-						float dzy = __fmul_rn(dz, ay.w[b]);
-						int oy = (oz + ay.cell[b]) * tx;
+				int wm = periodic ? (((w % N) + N) % N) : min(max(w, 0), N - 1);
+				cell = 2 * wm + s + N;
 
-						for (int e = 0; e < ax.n; e++) {
+				if (cell >= L)
+					cell -= L;
 
-							float d = __fmul_rn(dzy, ax.w[e]);
-							float2 v = tl[oy + ax.cell[e]];
-							acc.x = fmaf(v.x, d, acc.x);
-							acc.y = fmaf(v.y, d, acc.y);
-						}
-					}
-				}
+			} else {
 
-				ksp[m + M * (c0 + c)] = acc;
+				cell = 2 * w + s - origin;
+
+				if (periodic)
+					cell = ((cell % L) + L) % L;
+
+				cell = max(cell, 0);	// clipped taps (weight 0) may fall left of the tile
 			}
+
+			t.cell[3 * s + q] = cell;
+			t.w[3 * s + q] = valid ? val : 0.f;
 		}
 	}
 }
 
-// Gridding: per sub-block, shared-memory accumulation then one global atomic
-// per touched tile cell. The grid must be zeroed.
-__global__ void __launch_bounds__(BIN_THREADS) k_grid_binned(const float4* __restrict__ traj_sorted,
-		const int* __restrict__ perm, long M, GridGeom g, BinGeom bg,
-		const int* __restrict__ sub_bin, const int* __restrict__ sub_first, const int* __restrict__ sub_count,
-		int C, int cc, const float2* __restrict__ ksp, float2* __restrict__ grid, const float* __restrict__ kbg)
+// Degridding, width 6: one thread per sample in bin order (coalesced float4
+// trajectory loads, neighbouring threads share taps in L1), weights computed
+// once and reused for every coil. TZ = 6 for 3D, 1 for 2D.
+template <int TZ>
+__global__ void __launch_bounds__(BIN_THREADS, 2) k_degrid6(const float4* __restrict__ traj_sorted,
+		const int* __restrict__ perm, long M, GridGeom g, int C,
+		const float2* __restrict__ grid, float2* __restrict__ ksp, const float* __restrict__ kbg)
 {
-	extern __shared__ float2 tiles[];	// [cc][ncells]
 	__shared__ float kb[KB_TABLE_N + 1];
 
 	for (int i = threadIdx.x; i <= KB_TABLE_N; i += blockDim.x)
 		kb[i] = kbg[i];
 
+	__syncthreads();
+
+	long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+
+	if (i >= M)
+		return;
+
+	float4 k = traj_sorted[i];
+	Taps6 tx, ty, tz;
+	axis_taps6<0>(k.x, g.N[0], g.periodic, kb, 0, tx);
+	axis_taps6<0>(k.y, g.N[1], g.periodic, kb, 0, ty);
+	axis_taps6<0>(k.z, g.N[2], g.periodic, kb, 0, tz);
+	const long m = perm[i];
+
+	for (int c = 0; c < C; c++) {
+
+		const float2* gc = grid + g.gsz * c;
+		float2 acc = make_float2(0.f, 0.f);
+#pragma unroll 1
+		for (int a = 0; a < TZ; a++) {
+
+			float dz = tz.w[a];
+			long oz = (long)tz.cell[a] * g.G[1];
+#pragma unroll
+			for (int b = 0; b < 6; b++) {
+
+				float dzy = __fmul_rn(dz, ty.w[b]);
+				long oy = (oz + ty.cell[b]) * g.G[0];
+#pragma unroll
+				for (int e = 0; e < 6; e++) {
+
+					float d = __fmul_rn(dzy, tx.w[e]);
+					float2 v = gc[oy + tx.cell[e]];
+					acc.x = fmaf(v.x, d, acc.x);
+					acc.y = fmaf(v.y, d, acc.y);
+				}
+			}
+		}
+
+		ksp[m + M * c] = acc;
+	}
+}
+
+// Gridding, width 6: per sub-block, accumulate into shared-memory tiles of cc
+// coils with shared-memory atomics, then flush touched cells with one global
+// float2 atomic each. The grid must be zeroed.
+template <int TZ>
+__global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_binned(const float4* __restrict__ traj_sorted,
+		const int* __restrict__ perm, long M, GridGeom g, BinGeom bg,
+		const int* __restrict__ sub_bin, const int* __restrict__ sub_first, const int* __restrict__ sub_count,
+		const int* __restrict__ nsub_dev, int C, int cc, const float2* __restrict__ ksp, float2* __restrict__ grid,
+		const float* __restrict__ kbg)
+{
+	extern __shared__ float2 tiles[];	// [cc][ncells]
+	__shared__ float kb[KB_TABLE_N + 1];
+
 	const int sb = blockIdx.x;
+
+	if (sb >= *nsub_dev)
+		return;
+
+	for (int i = threadIdx.x; i <= KB_TABLE_N; i += blockDim.x)
+		kb[i] = kbg[i];
+
 	const int bin = sub_bin[sb];
 	const int first = sub_first[sb];
 	const int count = sub_count[sb];
@@ -321,10 +331,10 @@ __global__ void __launch_bounds__(BIN_THREADS) k_grid_binned(const float4* __res
 		for (int i = threadIdx.x; i < count; i += blockDim.x) {
 
 			float4 k = traj_sorted[first + i];
-			AxisTaps ax, ay, az;
-			axis_taps_local(k.x, g.N[0], g.hw, g.periodic, kb, to.o[0], bg.tile[0], ax);
-			axis_taps_local(k.y, g.N[1], g.hw, g.periodic, kb, to.o[1], bg.tile[1], ay);
-			axis_taps_local(k.z, g.N[2], g.hw, g.periodic, kb, to.o[2], bg.tile[2], az);
+			Taps6 ax, ay, az;
+			axis_taps6<1>(k.x, g.N[0], g.periodic, kb, to.o[0], ax);
+			axis_taps6<1>(k.y, g.N[1], g.periodic, kb, to.o[1], ay);
+			axis_taps6<1>(k.z, g.N[2], g.periodic, kb, to.o[2], az);
 			const long m = perm[first + i];
 
 			for (int c = 0; c < cn; c++) {
@@ -335,23 +345,27 @@ __global__ void __launch_bounds__(BIN_THREADS) k_grid_binned(const float4* __res
 					continue;
 
 				float* tl = (float*)(tiles + (long)c * bg.ncells);
-
-				for (int a = 0; a < az.n; a++) {
+#pragma unroll 1
+				for (int a = 0; a < TZ; a++) {
 
 					float dz = az.w[a];
 					int oz = az.cell[a] * ty;
-
-					for (int b = 0; b < ay.n; b++) {
+#pragma unroll
+					for (int b = 0; b < 6; b++) {
 
 						float dzy = __fmul_rn(dz, ay.w[b]);
 						int oy = (oz + ay.cell[b]) * tx;
-
-						for (int e = 0; e < ax.n; e++) {
+#pragma unroll
+						for (int e = 0; e < 6; e++) {
 
 							float d = __fmul_rn(dzy, ax.w[e]);
-							int cell = oy + ax.cell[e];
-							atomicAdd(&tl[2 * cell + 0], val.x * d);
-							atomicAdd(&tl[2 * cell + 1], val.y * d);
+
+							if (0.f != d) {
+
+								int cell = oy + ax.cell[e];
+								atomicAdd(&tl[2 * cell + 0], val.x * d);
+								atomicAdd(&tl[2 * cell + 1], val.y * d);
+							}
 						}
 					}
 				}
