@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <string>
@@ -92,6 +93,21 @@ static void prof_end(cudaEvent_t e, cudaStream_t st)
 }
 
 static cudaStream_t S(void* stream) { return (cudaStream_t)stream; }
+
+// scatter variant of the width-6 gridding: 0 = shared-memory tiles,
+// 1 = global atomics on bin-sorted samples (BNUFFT_GRIDDING=tiles|atomic)
+static int gridding_kind()
+{
+	static int kind = -1;
+
+	if (kind < 0) {
+
+		const char* e = getenv("BNUFFT_GRIDDING");
+		kind = (e && 0 == strcmp(e, "atomic")) ? 1 : 0;
+	}
+
+	return kind;
+}
 
 // ----------------------------------------------------------------------------
 // Kaiser-Bessel table, roll-off and twiddles (host, float64)
@@ -763,6 +779,22 @@ static int grid_adj(OpCtx& op, const float2* ksp, long C, float2* grid, cudaStre
 	}
 
 	CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(float2) * op.g.gsz * C, st));
+
+	if (op.bins.perm && (6.f == op.g.width) && (gridding_kind() == 1)) {
+
+		const Bins& b = op.bins;
+		cudaEvent_t pe = prof_begin("grid", st);
+		unsigned nb = (unsigned)((op.g.M + BIN_THREADS - 1) / BIN_THREADS);
+
+		if (op.g.G[2] > 1)
+			k_grid6_atomic<6><<<nb, BIN_THREADS, 0, st>>>(b.traj, b.perm, op.g.M, grid_geom(op.g), (int)C, ksp, grid, op.kb);
+		else
+			k_grid6_atomic<1><<<nb, BIN_THREADS, 0, st>>>(b.traj, b.perm, op.g.M, grid_geom(op.g), (int)C, ksp, grid, op.kb);
+
+		prof_end(pe, st);
+		LAUNCHED();
+		return BNUFFT_OK;
+	}
 
 	if (op.bins.perm && (6.f == op.g.width)) {
 

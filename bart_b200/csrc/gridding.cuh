@@ -328,7 +328,18 @@ __global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_binned(const float4* _
 
 		__syncthreads();
 
-		for (int i = threadIdx.x; i < count; i += blockDim.x) {
+		// lanes of a warp take samples 8 apart in bin order: neighbouring
+		// samples of a trajectory share taps, so this spreads the
+		// shared-memory atomics of one instruction over distinct cells
+		const int per = (count + blockDim.x - 1) / blockDim.x;
+
+		for (int r = 0; r < per; r++) {
+
+			int t = threadIdx.x + r * blockDim.x;
+			int i = (t % 32) * 8 + (t / 32) % 8 + (t / 256) * 256;
+
+			if (i >= count)
+				continue;
 
 			float4 k = traj_sorted[first + i];
 			Taps6 ax, ay, az;
@@ -390,6 +401,63 @@ __global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_binned(const float4* _
 
 			if (gi >= 0)
 				atomicAdd(&grid[gi + g.gsz * (c0 + c)], v);
+		}
+	}
+}
+
+// Gridding, width 6, without tiles: one thread per sample in bin order,
+// weights computed once for all coils, one global float2 atomic per tap.
+template <int TZ>
+__global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_atomic(const float4* __restrict__ traj_sorted,
+		const int* __restrict__ perm, long M, GridGeom g, int C,
+		const float2* __restrict__ ksp, float2* __restrict__ grid, const float* __restrict__ kbg)
+{
+	__shared__ float kb[KB_TABLE_N + 1];
+
+	for (int i = threadIdx.x; i <= KB_TABLE_N; i += blockDim.x)
+		kb[i] = kbg[i];
+
+	__syncthreads();
+
+	long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+
+	if (i >= M)
+		return;
+
+	float4 k = traj_sorted[i];
+	Taps6 tx, ty, tz;
+	axis_taps6<0>(k.x, g.N[0], g.periodic, kb, 0, tx);
+	axis_taps6<0>(k.y, g.N[1], g.periodic, kb, 0, ty);
+	axis_taps6<0>(k.z, g.N[2], g.periodic, kb, 0, tz);
+	const long m = perm[i];
+
+	for (int c = 0; c < C; c++) {
+
+		float2 val = ksp[m + M * c];
+
+		if ((0.f == val.x) && (0.f == val.y))
+			continue;
+
+		float2* gc = grid + g.gsz * c;
+#pragma unroll 1
+		for (int a = 0; a < TZ; a++) {
+
+			float dz = tz.w[a];
+			long oz = (long)tz.cell[a] * g.G[1];
+#pragma unroll
+			for (int b = 0; b < 6; b++) {
+
+				float dzy = __fmul_rn(dz, ty.w[b]);
+				long oy = (oz + ty.cell[b]) * g.G[0];
+#pragma unroll
+				for (int e = 0; e < 6; e++) {
+
+					float d = __fmul_rn(dzy, tx.w[e]);
+
+					if (0.f != d)
+						atomicAdd(&gc[oy + tx.cell[e]], make_float2(val.x * d, val.y * d));
+				}
+			}
 		}
 	}
 }
