@@ -492,6 +492,9 @@ struct OpCtx {
 	Work w;
 	Csr csr;		// set in deterministic mode
 	Bins bins;		// binned gridding (all modes)
+	const float2* wgt = nullptr;	// [M, wgt_c] weights (optional)
+	long wgt_c = 1;
+	float2* wbuf = nullptr;		// [M, C] weighted k-space for the adjoint
 };
 
 static void free_bins(Bins& b, cudaStream_t st)
@@ -770,7 +773,7 @@ static int grid_adj(OpCtx& op, const float2* ksp, long C, float2* grid, cudaStre
 	if (op.csr.row_ptr) {	// deterministic: fixed-order gather per cell
 
 		int cpc = (int)std::min<long>(C, 8);
-		dim3 blocks((unsigned)((op.g.gsz + 255) / 256), (unsigned)((C + cpc - 1) / cpc));
+		dim3 blocks((unsigned)((op.g.gsz * 32 + 255) / 256), (unsigned)((C + cpc - 1) / cpc));
 		cudaEvent_t pe = prof_begin("grid", st);
 		k_grid_csr<<<blocks, 256, 0, st>>>(op.csr.row_ptr, op.csr.col, op.csr.val, op.g.gsz, op.g.M, (int)C, cpc, ksp, grid);
 		prof_end(pe, st);
@@ -989,7 +992,15 @@ static int op_forward(OpCtx& op, const float2* cim, const float2* maps, long C, 
 {
 	TRY(alloc_work(op.w, op.g, C, st));
 	TRY(op_spectrum(op, cim, maps, true, C, op.w.grid, st));
-	return degrid(op, op.w.grid, C, ksp, st);
+	TRY(degrid(op, op.w.grid, C, ksp, st));
+
+	if (op.wgt) {
+
+		k_weight<<<vec_blocks(op.g.M * C), RED_THREADS, 0, st>>>(ksp, ksp, op.wgt, op.g.M, C, op.wgt_c, 0);
+		LAUNCHED();
+	}
+
+	return BNUFFT_OK;
 }
 
 // adjoint NUFFT: ksp [M, C] -> cim [npix, C] (maps: partial coil sums)
@@ -997,6 +1008,17 @@ static int op_adjoint(OpCtx& op, const float2* ksp, const float2* maps, long C, 
 		const DotHook& dh = DotHook())
 {
 	TRY(alloc_work(op.w, op.g, C, st));
+
+	if (op.wgt) {
+
+		if (!op.wbuf)
+			CUDA_TRY(cudaMallocAsync(&op.wbuf, sizeof(float2) * op.g.M * C, st));
+
+		k_weight<<<vec_blocks(op.g.M * C), RED_THREADS, 0, st>>>(op.wbuf, ksp, op.wgt, op.g.M, C, op.wgt_c, 1);
+		LAUNCHED();
+		ksp = op.wbuf;
+	}
+
 	TRY(grid_adj(op, ksp, C, op.w.grid, st));
 	return op_spectrum_adjoint(op, op.w.grid, maps, true, C, cpg, out, st, dh);
 }
@@ -1040,7 +1062,7 @@ static int op_toeplitz(OpCtx& op, const float2* psf, const float2* x, const floa
 // psft = adjoint NUFFT of ones with trajectory 2*traj onto the 2N image,
 // periodic gridding; psf = fftuc(psft) / npix.
 static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, float2** psf_out, cudaStream_t st,
-		bool deterministic)
+		bool deterministic, const float2* wgt)
 {
 	OpCtx in;
 	long d2[3] = { g.G[0], g.G[1], g.G[2] };
@@ -1057,7 +1079,11 @@ static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, flo
 
 	k_traj_convert<<<vec_blocks(g.M), RED_THREADS, 0, st>>>(t2, traj_c, g.M, 2.f);
 	LAUNCHED();
-	k_fill<<<vec_blocks(g.M), RED_THREADS, 0, st>>>(ones, g.M, make_float2(1.f, 0.f));
+	if (wgt)	// compute_square_weights (src/noncart/nufft.c:509-518)
+		k_weight_sq<<<vec_blocks(g.M), RED_THREADS, 0, st>>>(ones, wgt, g.M);
+	else
+		k_fill<<<vec_blocks(g.M), RED_THREADS, 0, st>>>(ones, g.M, make_float2(1.f, 0.f));
+
 	LAUNCHED();
 
 	in.traj = t2;
@@ -1203,6 +1229,7 @@ struct bnufft_plan_s {
 	OpCtx op;
 	float4* traj = nullptr;
 	float2* psf = nullptr;	// DFT order, includes 1/npix
+	float2* wgt = nullptr;	// weights copy [M, wgt_c]
 	cudaStream_t st0;
 };
 
@@ -1248,7 +1275,7 @@ static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
 			cudaFreeAsync(p->psf, st);
 
 		p->psf = nullptr;
-		TRY(compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, st, 0 != p->conf.deterministic));
+		TRY(compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, st, 0 != p->conf.deterministic, p->op.wgt));
 	}
 
 	if (t.owned)
@@ -1271,8 +1298,8 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 	if ((N < 4) || (nullptr == traj))
 		return fail(BNUFFT_ERR_ARG, "need N >= 4 dims and a trajectory");
 
-	if (weights || basis)
-		return fail(BNUFFT_ERR_UNSUPPORTED, "weights / basis are not built yet");
+	if (basis)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "subspace basis is not built yet");
 
 	bnufft_conf conf;
 
@@ -1320,6 +1347,35 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 		s = fail(BNUFFT_ERR_NOMEM, "trajectory buffer");
 
 	p->op.traj = p->traj;
+
+	// weights [1, Mr, Ms, 1 or C, 1...] (nufft_set_traj, src/noncart/nufft.c:1041-1049)
+	if ((BNUFFT_OK == s) && weights) {
+
+		long wc = prod(N - 3, wgh_dims + 3);
+
+		if ((1 != wgh_dims[0]) || (wgh_dims[1] != ksp_dims[1]) || (wgh_dims[2] != ksp_dims[2]) || ((1 != wc) && (p->C != wc)))
+			s = fail(BNUFFT_ERR_UNSUPPORTED, "weights must be [1, Mr, Ms] or match the k-space dims");
+		else if (conf.toeplitz && (1 != wc))
+			s = fail(BNUFFT_ERR_UNSUPPORTED, "per-channel weights with the Toeplitz PSF");
+
+		if (BNUFFT_OK == s) {
+
+			Staged ws;
+			s = stage_in(ws, weights, sizeof(float2) * M * wc, st);
+
+			if ((BNUFFT_OK == s) && (cudaSuccess != cudaMallocAsync(&p->wgt, sizeof(float2) * M * wc, st)))
+				s = fail(BNUFFT_ERR_NOMEM, "weights buffer");
+
+			if ((BNUFFT_OK == s) && (cudaSuccess != cudaMemcpyAsync(p->wgt, ws.dev, sizeof(float2) * M * wc, cudaMemcpyDeviceToDevice, st)))
+				s = fail(BNUFFT_ERR_CUDA, "weights copy");
+
+			if ((BNUFFT_OK == s) && ws.owned)
+				cudaStreamSynchronize(st);
+
+			p->op.wgt = p->wgt;
+			p->op.wgt_c = wc;
+		}
+	}
 
 	if (BNUFFT_OK == s)
 		s = upload_traj(p, traj, st);
@@ -1486,6 +1542,8 @@ extern "C" void bnufft_free(bnufft_plan_t p)
 
 	if (p->traj) cudaFreeAsync(p->traj, st);
 	if (p->psf) cudaFreeAsync(p->psf, st);
+	if (p->wgt) cudaFreeAsync(p->wgt, st);
+	if (p->op.wbuf) cudaFreeAsync(p->op.wbuf, st);
 
 	delete p;	// device frees are stream-ordered; host state can go now
 }

@@ -254,6 +254,32 @@ __global__ void k_fill(float2* dst, long n, float2 v)
 		dst[i] = v;
 }
 
+// y[m + M*c] = x[m + M*c] * w[m + M*(c % cw)] (conj(w) when conj): density
+// weights / sampling pattern of the NUFFT (src/noncart/nufft.c:1456, 1474)
+__global__ void k_weight(float2* __restrict__ y, const float2* __restrict__ x, const float2* __restrict__ w,
+		long M, long C, long cw, int conj)
+{
+	long n = M * C;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		long m = i % M;
+		long c = i / M;
+		float2 wv = w[m + M * (c % cw)];
+		y[i] = conj ? cmulc(x[i], wv) : cmul(x[i], wv);
+	}
+}
+
+// |w|^2 (real) into a complex buffer: the PSF's "ones" with weights
+__global__ void k_weight_sq(float2* __restrict__ y, const float2* __restrict__ w, long M)
+{
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += (long)gridDim.x * blockDim.x) {
+
+		float2 v = w[i];
+		y[i] = cmulc(v, v);
+	}
+}
+
 // trajectory [3, M] complex float -> float4 (kx, ky, kz, 0) * factor
 __global__ void k_traj_convert(float4* __restrict__ dst, const float2* __restrict__ src, long M, float factor)
 {

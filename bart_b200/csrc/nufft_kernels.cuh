@@ -735,11 +735,15 @@ __global__ void k_csr_fill_valid(const unsigned long long* __restrict__ keys, lo
 	}
 }
 
-// grid[cell + gsz*c] = sum over the cell's row, in row order, of w * ksp[m + M*c]
+// grid[cell + gsz*c] = sum over the cell's row of w * ksp[m + M*c]: one warp
+// per cell, lane l sums entries l, l+32, ... in order, then a fixed shuffle
+// tree combines the lanes, so the summation order is the same every run (and
+// long rows at the k-space centre are spread over 32 lanes).
 __global__ void k_grid_csr(const long* __restrict__ row_ptr, const int* __restrict__ col, const float* __restrict__ val,
 		long gsz, long M, int C, int cpc, const float2* __restrict__ ksp, float2* __restrict__ grid)
 {
-	long cell = (long)blockIdx.x * blockDim.x + threadIdx.x;
+	const int lane = threadIdx.x % 32;
+	long cell = ((long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
 
 	if (cell >= gsz)
 		return;
@@ -756,7 +760,7 @@ __global__ void k_grid_csr(const long* __restrict__ row_ptr, const int* __restri
 		for (int q = 0; q < 4; q++)
 			acc[q] = make_float2(0.f, 0.f);
 
-		for (long i = r0; i < r1; i++) {
+		for (long i = r0 + lane; i < r1; i += 32) {
 
 			float w = val[i];
 			long m = col[i];
@@ -773,9 +777,17 @@ __global__ void k_grid_csr(const long* __restrict__ row_ptr, const int* __restri
 		}
 
 #pragma unroll
-		for (int q = 0; q < 4; q++)
-			if (cb + q < c1)
+		for (int q = 0; q < 4; q++) {
+
+			for (int o = 16; o > 0; o >>= 1) {
+
+				acc[q].x += __shfl_xor_sync(0xffffffffu, acc[q].x, o);
+				acc[q].y += __shfl_xor_sync(0xffffffffu, acc[q].y, o);
+			}
+
+			if ((0 == lane) && (cb + q < c1))
 				grid[cell + gsz * (cb + q)] = acc[q];
+		}
 	}
 }
 

@@ -149,18 +149,28 @@ def nufft_create2(ksp_dims, cim_dims, traj_dims, traj, wgh_dims=None, weights=No
     """nufft_create2 (src/noncart/nufft.c:1174): NUFFT linop for a trajectory.
 
     ``traj`` is the reference's [3, Mr, Ms] complex64 trajectory (numpy, or a
-    torch tensor on the device). Weights and basis are not built yet.
+    torch tensor on the device). ``weights`` (density compensation / sampling
+    pattern, ``bart nufft -p``) is [1, Mr, Ms] or [1, Mr, Ms, C]; with the
+    Toeplitz PSF it must be shared by all channels. A subspace basis is not
+    built yet.
     """
     lib = _lib.load()
     conf = conf or NufftConf()
     kd, cd, td = dims16(ksp_dims), dims16(cim_dims), dims16(traj_dims)
     pt, keep = _ptr_in(traj, int(np.prod(td)))
+    wd_arr, pw, keep_w = None, None, None
+    if weights is not None:
+        wd = dims16(wgh_dims if wgh_dims is not None else np.shape(weights))
+        wd_arr = _lib.dims_array(wd)
+        pw, keep_w = _ptr_in(weights, int(np.prod(wd)))
+    if basis is not None:
+        raise _lib.BnufftError(2, "subspace basis is not built yet")
     h = ctypes.c_void_p()
     cc = conf.c()
     _lib.check(lib.bnufft_create2(ctypes.byref(h), 16, _lib.dims_array(kd), _lib.dims_array(cd),
-                                  _lib.dims_array(td), pt, None, weights, None, basis, ctypes.byref(cc),
+                                  _lib.dims_array(td), pt, wd_arr, pw, None, None, ctypes.byref(cc),
                                   _stream_of(traj)))
-    del keep
+    del keep, keep_w
     op = Linop(h, cd, kd, has_normal=True)
     op._traj_dims = td
     return op
@@ -168,4 +178,5 @@ def nufft_create2(ksp_dims, cim_dims, traj_dims, traj, wgh_dims=None, weights=No
 
 def nufft_create(ksp_dims, cim_dims, traj_dims, traj, weights=None, conf: NufftConf | None = None) -> Linop:
     """nufft_create (src/noncart/nufft.c:1315): weights share the traj dims."""
-    return nufft_create2(ksp_dims, cim_dims, traj_dims, traj, None, weights, None, None, conf)
+    wd = None if weights is None else [1] + list(dims16(traj_dims))[1:]
+    return nufft_create2(ksp_dims, cim_dims, traj_dims, traj, wd, weights, None, None, conf)

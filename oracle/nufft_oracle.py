@@ -303,7 +303,8 @@ class NufftOracle:
     FOV (the real parts of the reference's trajectory array).
     """
 
-    def __init__(self, traj, dims, periodic=False, width=6.0, os=2.0):
+    def __init__(self, traj, dims, periodic=False, width=6.0, os=2.0, weights=None):
+        self.weights = None if weights is None else np.asarray(weights).reshape(-1, order="F").astype(np.complex64)
         self.dims3 = tuple(int(d) for d in dims)
         self.traj = np.asarray(traj, dtype=F32).reshape(3, -1)
         self.M = self.traj.shape[1]
@@ -340,12 +341,17 @@ class NufftOracle:
         """img [X,Y,Z,C] -> ksp [M,C] (nufft_apply_forward, :1388-1458)."""
         img = _as4(img)
         x = img * self.roll[..., None]
-        return self.degrid(spectrum(x))
+        y = self.degrid(spectrum(x))
+        if self.weights is not None:     # md_zmul2 by the weights (:1456)
+            y = y * self.weights.astype(np.complex128)[:, None]
+        return y
 
     def adjoint(self, ksp):
         """ksp [M,C] -> img [X,Y,Z,C] (nufft_apply_adjoint, :1462-1540)."""
-        ksp = np.asarray(ksp).reshape(self.M, -1)
-        g = self.grid(ksp.astype(np.complex128))
+        ksp = np.asarray(ksp).reshape(self.M, -1).astype(np.complex128)
+        if self.weights is not None:     # md_zmulc2 by the weights (:1474)
+            ksp = ksp * np.conj(self.weights.astype(np.complex128))[:, None]
+        g = self.grid(ksp)
         x = spectrum_adjoint(g, self.dims3)
         return x * self.roll[..., None]
 
@@ -362,6 +368,9 @@ class NufftOracle:
             dims2 = self.g2
             inner = NufftOracle((self.traj.astype(F32) * F32(2.0)), dims2, periodic=True)
             ones = np.ones((self.M, 1), dtype=np.complex128)
+            if self.weights is not None:  # squared weights (compute_square_weights, :509-518)
+                w = self.weights
+                ones = (w * np.conj(w)).astype(np.complex64).astype(np.complex128)[:, None]
             psft = inner.adjoint(ones)[..., 0]
             axes = _axes(dims2)
             tot = float(np.prod([dims2[a] for a in axes]))

@@ -3,7 +3,7 @@
  * normal operator and the PSF, which the reference's command-line tools do
  * not print directly. Test infrastructure only.
  *
- *   refnormal [-P] [--no-toeplitz] traj img out [psf_out]
+ *   refnormal [-P] [--no-toeplitz] [-p pattern] traj img out [psf_out]
  *
  * out = N^H N img, with N = nufft_create2(..., conf) and conf.toeplitz set
  * (src/noncart/nufft.c:1174-1276, normal at :1740 -> toeplitz_mult :1546).
@@ -28,6 +28,7 @@ int main(int argc, char* argv[])
 {
 	bool periodic = false;
 	bool toeplitz = true;
+	const char* pattern_file = NULL;
 	int a = 1;
 
 	while ((a < argc) && ('-' == argv[a][0])) {
@@ -36,6 +37,8 @@ int main(int argc, char* argv[])
 			periodic = true;
 		else if (0 == strcmp(argv[a], "--no-toeplitz"))
 			toeplitz = false;
+		else if ((0 == strcmp(argv[a], "-p")) && (a + 1 < argc))
+			pattern_file = argv[++a];
 		else
 			error("unknown option %s\n", argv[a]);
 		a++;
@@ -59,7 +62,10 @@ int main(int argc, char* argv[])
 	conf.toeplitz = toeplitz;
 	conf.periodic = periodic;
 
-	const struct linop_s* op = nufft_create2(DIMS, ksp_dims, img_dims, trj_dims, traj, NULL, NULL, NULL, NULL, conf);
+	long pat_dims[DIMS];
+	complex float* pattern = (NULL != pattern_file) ? load_cfl(pattern_file, DIMS, pat_dims) : NULL;
+
+	const struct linop_s* op = nufft_create2(DIMS, ksp_dims, img_dims, trj_dims, traj, pat_dims, pattern, NULL, NULL, conf);
 
 	complex float* out = create_cfl(argv[a + 2], DIMS, img_dims);
 

@@ -40,12 +40,15 @@ def cplx(rng, shape):
     return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
 
 
-def nufft_case(name, traj, img, periodic=False, normal=True):
+def nufft_case(name, traj, img, periodic=False, normal=True, pattern=None):
     with tempfile.TemporaryDirectory() as d:
         rng = np.random.default_rng(zlib.crc32(name.encode()))
         writecfl(os.path.join(d, "t"), traj)
         writecfl(os.path.join(d, "x"), img)
         P = ["-P"] if periodic else []
+        if pattern is not None:
+            writecfl(os.path.join(d, "w"), pattern)
+            P += ["-p", "w"]
         run("nufft", *P, "t", "x", "k", cwd=d)
         fwd = readcfl(os.path.join(d, "k"))
         ksp = cplx(rng, fwd.shape)
@@ -54,6 +57,8 @@ def nufft_case(name, traj, img, periodic=False, normal=True):
         run("nufft", *P, "-a", f"-x{dims}", "t", "y", "a", cwd=d)
         adj = readcfl(os.path.join(d, "a"))
         out = dict(traj=traj, img=img, fwd=fwd, ksp=ksp, adj=adj)
+        if pattern is not None:
+            out["pattern"] = pattern
         if normal:
             run("refnormal", *P, "t", "x", "n", "p", cwd=d)
             out["normal"] = readcfl(os.path.join(d, "n"))
@@ -98,6 +103,8 @@ def main():
     nufft_case("nufft2d_n64", t64, img64)
     nufft_case("nufft2d_n64_periodic", t64, img64, periodic=True)
     nufft_case("nufft2d_n32_coils3", t32, cplx(rng, (32, 32, 1, 3)), normal=False)
+    w64 = (0.2 + rng.random((1,) + t64.shape[1:3])).astype(np.complex64)   # real positive density weights
+    nufft_case("nufft2d_n64_weights", t64, img64, pattern=w64)
     t3 = synth.kooshball_traj(16, 96)
     nufft_case("nufft3d_n16", t3, cplx(rng, (16, 16, 16)))
     pics_case("pics2d_n64_c4", 64, 4, 24, seed=7)

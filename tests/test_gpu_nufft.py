@@ -28,11 +28,14 @@ def _plan(g, periodic=False, toeplitz=True):
     cd = _dims(img.shape)
     td = list(g["traj"].shape)
     kd = [1, td[1], td[2], cd[3]]
-    return nufft_create2(kd, cd, td, g["traj"], conf=NufftConf(toeplitz=toeplitz, periodic=periodic)), cd, kd
+    w = g.get("pattern")
+    wd = None if w is None else list(w.shape)
+    return nufft_create2(kd, cd, td, g["traj"], wd, w, conf=NufftConf(toeplitz=toeplitz, periodic=periodic)), cd, kd
 
 
 @pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
-                                           ("nufft3d_n16", False), ("nufft2d_n32_coils3", False)])
+                                           ("nufft3d_n16", False), ("nufft2d_n32_coils3", False),
+                                           ("nufft2d_n64_weights", False)])
 def test_forward_adjoint_vs_reference(name, periodic):
     g = golden(name)
     op, cd, kd = _plan(g, periodic, toeplitz=False)
@@ -44,7 +47,7 @@ def test_forward_adjoint_vs_reference(name, periodic):
 
 
 @pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
-                                           ("nufft3d_n16", False)])
+                                           ("nufft3d_n16", False), ("nufft2d_n64_weights", False)])
 def test_toeplitz_normal_and_psf_vs_reference(name, periodic):
     g = golden(name)
     op, cd, kd = _plan(g, periodic, toeplitz=True)

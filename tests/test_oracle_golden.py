@@ -19,11 +19,12 @@ def _op(g, periodic=False):
     while img.ndim < 4:
         img = img[..., None]
     traj = g["traj"].real.reshape(3, -1, order="F")
-    return orc.NufftOracle(traj, img.shape[:3], periodic=periodic), img
+    return orc.NufftOracle(traj, img.shape[:3], periodic=periodic, weights=g.get("pattern")), img
 
 
 @pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
-                                           ("nufft3d_n16", False), ("nufft2d_n32_coils3", False)])
+                                           ("nufft3d_n16", False), ("nufft2d_n32_coils3", False),
+                                           ("nufft2d_n64_weights", False)])
 def test_forward_adjoint(name, periodic):
     g = golden(name)
     o, img = _op(g, periodic)
@@ -35,7 +36,7 @@ def test_forward_adjoint(name, periodic):
 
 
 @pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
-                                           ("nufft3d_n16", False)])
+                                           ("nufft3d_n16", False), ("nufft2d_n64_weights", False)])
 def test_toeplitz_normal_and_psf(name, periodic):
     g = golden(name)
     o, img = _op(g, periodic)
