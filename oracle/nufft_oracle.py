@@ -389,6 +389,70 @@ class NufftOracle:
         return self.adjoint(self.forward(img))
 
 
+def _fftmod_axis(n):
+    """fftmod phases of one axis (src/num/fft.c:62-67 with phase 0)."""
+    c = n // 2
+    j = np.arange(n)
+    return np.exp(2j * np.pi * (j - c / 2.0) * (c / n)) if n > 1 else np.ones(1)
+
+
+def _fftuc(x, axes):
+    tot = float(np.prod([x.shape[a] for a in axes]))
+    return np.fft.fftshift(np.fft.fftn(np.fft.ifftshift(x, axes=axes), axes=axes), axes=axes) / math.sqrt(tot)
+
+
+def _ifftuc(x, axes):
+    tot = float(np.prod([x.shape[a] for a in axes]))
+    return np.fft.fftshift(np.fft.ifftn(np.fft.ifftshift(x, axes=axes), axes=axes), axes=axes) * math.sqrt(tot)
+
+
+def circulant_precond(op: "NufftOracle") -> np.ndarray:
+    """Strang circulant preconditioner of the Toeplitz normal operator,
+    restating compute_precond (src/noncart/precond.c:36-64) literally on the
+    reference's decomposed PSF: pre = sum_s conj(linphase_s) ifftuc(psf_s),
+    then |fftuc(pre)| + 1e-3, kept in the array order fftuc returns (it is
+    applied element-wise after an uncentred FFT, precond.c:82-91)."""
+    dims3 = op.dims3
+    axes = _axes(dims3)
+    Pc = op.psf()
+    fm = np.ones(dims3, dtype=np.complex128)
+    for a in axes:
+        sh = [1, 1, 1]
+        sh[a] = dims3[a]
+        fm = fm * _fftmod_axis(dims3[a]).reshape(sh)
+    E1 = spectrum(np.ones(dims3 + (1,)))[..., 0]
+    pre = np.zeros(dims3, dtype=np.complex128)
+    for s in _subgrid_shifts(dims3):
+        sl = tuple(slice(s[a], None, 2) if dims3[a] > 1 else slice(None) for a in range(3))
+        Ls = np.fft.ifftn(np.conj(fm) * E1[sl], axes=axes)     # linphase_s as a multiplier
+        pre += np.conj(Ls) * _ifftuc(Pc[sl], axes)
+    return np.abs(_fftuc(pre, axes)) + 1e-3
+
+
+def nufft_inverse(op: "NufftOracle", ksp, lam=0.0, maxiter=50, precond=False):
+    """``bart nufft -i [-c] -l lam -m maxiter`` (src/nufft.c:250-263): CG
+    (l2lambda 0) on P^-1 (N^H N + lam) x = P^-1 N^H y over all coil images
+    jointly (lsqr2_create, src/iter/lsqr.c:78-167); P^-1 v = ifft(fft(v)/pre)
+    with the uncentred, unnormalised FFT (precond.c:82-91)."""
+    dims3 = op.dims3
+    axes = _axes(dims3)
+    y = np.asarray(ksp).reshape(op.M, -1)
+    pre = circulant_precond(op)[..., None] if precond else None
+
+    def pinv(v):
+        if pre is None:
+            return v
+        tot = float(np.prod([dims3[a] for a in axes]))
+        return np.fft.ifftn(np.fft.fftn(v, axes=axes) / pre, axes=axes) * tot
+
+    def normal(v):
+        return pinv(op.normal_toeplitz(v) + lam * v)
+
+    b = pinv(op.adjoint(y))
+    x, _ = conjgrad(normal, b, 0.0, maxiter)
+    return x
+
+
 def _as4(a):
     a = np.asarray(a)
     while a.ndim < 4:

@@ -69,6 +69,20 @@ def nufft_case(name, traj, img, periodic=False, normal=True, pattern=None):
     print(name, {k: np.shape(v) for k, v in out.items()})
 
 
+def inverse_case(name, traj, ksp, dims):
+    out = dict(traj=traj, ksp=ksp)
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "t"), traj)
+        writecfl(os.path.join(d, "k"), ksp)
+        x = ":".join(str(v) for v in dims)
+        for key, args in [("inv_m5", ["-m5"]), ("inv_m5_l", ["-m5", "-l0.1"]), ("inv_m5_c", ["-m5", "-c"]),
+                          ("inv_m5_c_l", ["-m5", "-c", "-l0.1"]), ("inv_m30_c", ["-m30", "-c"])]:
+            run("nufft", "-i", f"-x{x}", *args, "t", "k", "o", cwd=d)
+            out[key] = readcfl(os.path.join(d, "o"))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, {k: np.shape(v) for k, v in out.items()})
+
+
 def pics_case(name, N, C, spokes, seed):
     from oracle.nufft_oracle import SenseOracle
     rng = np.random.default_rng(seed)
@@ -108,6 +122,8 @@ def main():
     t3 = synth.kooshball_traj(16, 96)
     nufft_case("nufft3d_n16", t3, cplx(rng, (16, 16, 16)))
     pics_case("pics2d_n64_c4", 64, 4, 24, seed=7)
+    g = np.load(os.path.join(HERE, "nufft2d_n32_coils3.npz"))
+    inverse_case("inverse2d_n32_coils3", g["traj"], g["fwd"], (32, 32, 1))
 
 
 if __name__ == "__main__":

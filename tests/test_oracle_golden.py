@@ -98,3 +98,14 @@ def test_pics_scaling_and_30_iterations():
     # two reference runs differ slightly: its CPU gridding adds with OpenMP
     # atomics in a varying order (doc/performance.txt:67-69)
     assert rel(g["x30_rescale"], g["x30"] * sc) < 1e-4
+
+
+@pytest.mark.parametrize("key,kw", [("inv_m5", dict(maxiter=5)), ("inv_m5_l", dict(maxiter=5, lam=0.1)),
+                                    ("inv_m5_c", dict(maxiter=5, precond=True)),
+                                    ("inv_m5_c_l", dict(maxiter=5, precond=True, lam=0.1))])
+def test_nufft_inverse_and_circulant_precond(key, kw):
+    """bart nufft -i [-c] [-l]: CG on (P^-1)(N^H N + lam) x = (P^-1) N^H y."""
+    g = golden("inverse2d_n32_coils3")
+    o = orc.NufftOracle(g["traj"].real.reshape(3, -1, order="F"), (32, 32, 1))
+    x = orc.nufft_inverse(o, g["ksp"].reshape(-1, 3, order="F"), **kw)
+    assert rel(x, g[key].reshape(32, 32, 1, 3, order="F")) < 1e-5
