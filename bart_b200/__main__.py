@@ -1,6 +1,7 @@
 """Command line mirror of ``bart nufft`` and ``bart pics -t`` with .cfl I/O.
 
-  python -m bart_b200 nufft [-a] [-x X:Y:Z] [-P] [-r|-t] traj input output
+  python -m bart_b200 nufft [-a|-i [-c] [-l lambda] [-m iter]] [-x X:Y:Z] [-P] [-r|-t]
+                            [-p pattern] traj input output
   python -m bart_b200 pics -l2 -r lambda [-i iter] -t traj [-w scale] [-S]
                            [--no-toeplitz] ksp sens output
 
@@ -46,26 +47,39 @@ def main_nufft(argv) -> int:
     ap.add_argument("-r", dest="no_toeplitz", action="store_true")
     ap.add_argument("-P", dest="periodic", action="store_true")
     ap.add_argument("-g", dest="gpu", action="store_true")
+    ap.add_argument("-c", dest="precond", action="store_true")
+    ap.add_argument("-l", dest="lam", type=float, default=0.0)
+    ap.add_argument("-m", dest="iters", type=int, default=50)
+    ap.add_argument("-p", dest="pattern")
     ap.add_argument("traj")
     ap.add_argument("input")
     ap.add_argument("output")
     a = ap.parse_args(argv)
-    if a.inverse:
-        sys.stderr.write("nufft -i is not built yet (use pics)\n")
+    if a.adjoint and a.inverse:
+        sys.stderr.write("Adjoint and inverse requested at the same time.\n")
         return 1
     traj = readcfl(a.traj)
     tdims = list(traj.shape)
-    conf = NufftConf(toeplitz=False, periodic=a.periodic)   # no PSF unless inverse (src/nufft.c:121-122)
+    # the PSF is only built for the inverse (src/nufft.c:121-122); Toeplitz is on by default there
+    conf = NufftConf(toeplitz=a.inverse and not a.no_toeplitz, periodic=a.periodic)
     inp = readcfl(a.input)
+    pat = readcfl(a.pattern) if a.pattern else None
+    if a.inverse:
+        kd = list(inp.shape)
+        cd = (a.dims or estimate_im_dims(traj)) + kd[3:]
+        op = nufft_create2(kd, cd, tdims, traj, None if pat is None else list(pat.shape), pat, conf=conf)
+        writecfl(a.output, op.inverse(inp, lam=a.lam, maxiter=a.iters, precond=a.precond).reshape(cd, order="F"))
+        op.free()
+        return 0
     if a.adjoint:
         kd = list(inp.shape)
         cd = (a.dims or estimate_im_dims(traj)) + kd[3:]
-        op = nufft_create2(kd, cd, tdims, traj, conf=conf)
+        op = nufft_create2(kd, cd, tdims, traj, None if pat is None else list(pat.shape), pat, conf=conf)
         writecfl(a.output, op.adjoint(inp).reshape(cd, order="F"))
     else:
         cd = list(inp.shape)
         kd = [1, tdims[1], tdims[2]] + cd[3:]
-        op = nufft_create2(kd, cd, tdims, traj, conf=conf)
+        op = nufft_create2(kd, cd, tdims, traj, None if pat is None else list(pat.shape), pat, conf=conf)
         writecfl(a.output, op.forward(inp).reshape(kd, order="F"))
     op.free()
     return 0

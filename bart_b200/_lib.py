@@ -54,6 +54,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     sig("bnufft_get_psf", i, vp, i, cl, vp, vp)
     sig("bnufft_update_traj", i, vp, i, cl, vp, vp)
     sig("bnufft_free", None, vp)
+    sig("bnufft_nufft_inverse", i, vp, vp, vp, ctypes.c_float, i, i, vp)
     sig("bnufft_forward2d_noalloc", i, ctypes.c_long, ctypes.c_long, ctypes.c_long, vp, vp, vp, vp)
     sig("bnufft_pics_conf_defaults", None, ctypes.POINTER(PicsConfC))
     sig("bnufft_pics_create", i, ctypes.POINTER(vp), i, cl, cl, cl, vp, vp, ctypes.POINTER(PicsConfC), vp)

@@ -1230,6 +1230,7 @@ struct bnufft_plan_s {
 	float4* traj = nullptr;
 	float2* psf = nullptr;	// DFT order, includes 1/npix
 	float2* wgt = nullptr;	// weights copy [M, wgt_c]
+	float2* pinv = nullptr;	// circulant preconditioner 1/pre, [N0, N1*N2] DFT order (on demand)
 	cudaStream_t st0;
 };
 
@@ -1543,9 +1544,161 @@ extern "C" void bnufft_free(bnufft_plan_t p)
 	if (p->traj) cudaFreeAsync(p->traj, st);
 	if (p->psf) cudaFreeAsync(p->psf, st);
 	if (p->wgt) cudaFreeAsync(p->wgt, st);
+	if (p->pinv) cudaFreeAsync(p->pinv, st);
 	if (p->op.wbuf) cudaFreeAsync(p->op.wbuf, st);
 
 	delete p;	// device frees are stream-ordered; host state can go now
+}
+
+// ----------------------------------------------------------------------------
+// nufft -i: CG over coil images, optional circulant preconditioner
+// ----------------------------------------------------------------------------
+
+// Circulant preconditioner of the Toeplitz normal (nufft_precond_create,
+// src/noncart/precond.c:36-64, 95-130). Its kernel is the central N-cell part
+// of the PSF's image-domain kernel h; the reference assembles it from the 2^d
+// decomposed sub-grids with their linear phases, which equals 2^d h(x - N/2)
+// and, through the fftmod factor in those phases, leaves the spectrum in
+// uncentred order. Here: crop = unnormalised inverse 2N transform of the PSF
+// (DFT order, already 1/npix) with the central crop (= 2^d h), forward
+// N-point transform with the centred placement, pre = |.|/sqrt(npix) + 1e-3.
+static int build_precond(bnufft_plan_s* p, cudaStream_t st)
+{
+	if (p->pinv)
+		return BNUFFT_OK;
+
+	if (!p->psf)
+		return fail(BNUFFT_ERR_ARG, "the circulant preconditioner needs the Toeplitz PSF");
+
+	OpCtx& op = p->op;
+	const Geom& g = op.g;
+	TRY(alloc_work(op.w, g, 1, st));
+	float2* crop = nullptr;
+	float2* F = nullptr;
+	CUDA_TRY(cudaMallocAsync(&crop, sizeof(float2) * g.npix, st));
+	CUDA_TRY(cudaMallocAsync(&F, sizeof(float2) * g.npix, st));
+	TRY(op_spectrum_adjoint(op, p->psf, nullptr, false, 1, 1, crop, st));
+
+	// forward N-point transform (no zero padding): a geometry with L = N
+	OpCtx full;
+	full.g = g;
+
+	for (int a = 0; a < 3; a++)
+		full.g.G[a] = g.N[a];
+
+	full.g.gsz = g.npix;
+	full.kb = op.kb;
+	full.traj = nullptr;
+	TRY(alloc_work(full.w, full.g, 1, st));
+	TRY(op_spectrum(full, crop, nullptr, false, 1, F, st));
+	CUDA_TRY(cudaMallocAsync(&p->pinv, sizeof(float2) * g.npix, st));
+	k_precond_from_spectrum<<<vec_blocks(g.npix), RED_THREADS, 0, st>>>(p->pinv, F, g.npix, (float)(1. / sqrt((double)g.npix)));
+	LAUNCHED();
+	free_work(full.w, st);
+	cudaFreeAsync(crop, st);
+	cudaFreeAsync(F, st);
+	return BNUFFT_OK;
+}
+
+// v <- P^-1 v = ifft(fft(v) / pre) per coil (uncentred, unnormalised)
+static int apply_precond(bnufft_plan_s* p, float2* v, long C, cudaStream_t st)
+{
+	OpCtx full;
+	full.g = p->op.g;
+
+	for (int a = 0; a < 3; a++)
+		full.g.G[a] = full.g.N[a];
+
+	full.g.gsz = full.g.npix;
+	full.kb = p->op.kb;
+	full.traj = nullptr;
+	full.w = p->op.w;	// borrow the plan's buffers (large enough: N <= 2N)
+	const Geom& g = full.g;
+	long YZ = (long)g.N[1] * g.N[2];
+	TRY(rows_fwd(g.G[0], v, nullptr, nullptr, nullptr, g.N[0], YZ, YZ * C, full.w.t1, st));
+	TRY(op_toeplitz_cols(full, p->pinv, C, st));
+	return rows_inv(g.G[0], full.w.t1, nullptr, nullptr, nullptr, g.N[0], YZ, (int)C, 1, v, st);
+}
+
+extern "C" int bnufft_nufft_inverse(bnufft_plan_t p, void* img, const void* ksp, float lambda, int maxiter,
+		int precond, void* stream)
+{
+	cudaStream_t st = S(stream);
+
+	if (!p || (maxiter < 0))
+		return fail(BNUFFT_ERR_ARG, "bad plan or iteration count");
+
+	OpCtx& op = p->op;
+	const long C = p->C;
+	const long n = op.g.npix * C;
+	size_t kb = sizeof(float2) * op.g.M * C;
+	size_t ib = sizeof(float2) * n;
+	Staged ki, io;
+	TRY(stage_in(ki, ksp, kb, st));
+	TRY(stage_out_alloc(io, img, ib));
+	float2* x = (float2*)io.dev;
+
+	if (precond)
+		TRY(build_precond(p, st));
+
+	float2 *r = nullptr, *pv = nullptr, *Ap = nullptr;
+	double *pap = nullptr, *rsp = nullptr;
+	CgScalars* sc = nullptr;
+	unsigned nb = vec_blocks(n);
+	CUDA_TRY(cudaMallocAsync(&r, ib, st));
+	CUDA_TRY(cudaMallocAsync(&pv, ib, st));
+	CUDA_TRY(cudaMallocAsync(&Ap, ib, st));
+	CUDA_TRY(cudaMallocAsync(&pap, sizeof(double) * nb, st));
+	CUDA_TRY(cudaMallocAsync(&rsp, sizeof(double) * nb, st));
+	CUDA_TRY(cudaMallocAsync(&sc, sizeof(CgScalars), st));
+
+	// b = P^-1 N^H y  (into r, then CG start from x = 0)
+	TRY(op_adjoint(op, (const float2*)ki.dev, nullptr, C, 1, Ap, st));
+
+	if (precond)
+		TRY(apply_precond(p, Ap, C, st));
+
+	k_cg_init<<<nb, RED_THREADS, 0, st>>>(x, r, pv, Ap, n, rsp);
+	LAUNCHED();
+	k_cg_start<<<1, RED_THREADS, 0, st>>>(sc, rsp, (int)nb, 0.f);
+	LAUNCHED();
+
+	for (int it = 0; it < maxiter; it++) {
+
+		// Ap = P^-1 (N^H N p + lambda p); partial p^H Ap
+		if (p->psf) {
+
+			TRY(op_toeplitz(op, p->psf, pv, nullptr, C, 1, Ap, st));
+
+		} else {
+
+			float2* k = nullptr;
+			CUDA_TRY(cudaMallocAsync(&k, kb, st));
+			TRY(op_forward(op, pv, nullptr, C, k, st));
+			TRY(op_adjoint(op, k, nullptr, C, 1, Ap, st));
+			cudaFreeAsync(k, st);
+		}
+
+		k_combine<<<nb, RED_THREADS, 0, st>>>(Ap, Ap, 1, n, pv, lambda, nullptr, &sc->done);
+		LAUNCHED();
+
+		if (precond)
+			TRY(apply_precond(p, Ap, C, st));
+
+		k_combine<<<nb, RED_THREADS, 0, st>>>(Ap, Ap, 1, n, pv, 0.f, pap, &sc->done);
+		LAUNCHED();
+		k_cg_step<<<nb, RED_THREADS, 0, st>>>(x, r, pv, Ap, 1, n, 0.f, sc, it, pap, (int)nb, nullptr, 0, rsp);
+		LAUNCHED();
+		k_cg_dir<<<nb, RED_THREADS, 0, st>>>(pv, r, n, sc, it, rsp, (int)nb);
+		LAUNCHED();
+	}
+
+	void* frees[] = { r, pv, Ap, pap, rsp, sc };
+
+	for (void* q : frees)
+		cudaFreeAsync(q, st);
+
+	return stage_out_copy(io, img, ib, st);
 }
 
 // ----------------------------------------------------------------------------

@@ -185,6 +185,58 @@ __global__ void k_cg_step(float2* __restrict__ x, float2* __restrict__ r, const 
 		rs_part[blockIdx.x] = s;
 }
 
+// Direction update of the plain CG (conjgrad, src/iter/italgos.c:558-566):
+// rs_new = ||r||^2 from the step's partials; stop if rs_new <= eps2, else
+// p = r + (rs_new / rs_old) p. rs of iteration it+1 goes to rs[(it+1) & 1].
+__global__ void k_cg_dir(float2* __restrict__ p, const float2* __restrict__ r, long n, CgScalars* st, int it,
+		const double* __restrict__ rs_part, int nrs)
+{
+	__shared__ double sh[32];
+
+	if (st->done)
+		return;
+
+	double rs_new = sum_partials(rs_part, nrs, sh);
+	double rs_old = st->rs[it & 1];
+	bool stop = (rs_new <= st->eps2);
+
+	if (!stop) {
+
+		float beta = (float)(rs_new / rs_old);
+
+		for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+			float2 pv = p[i];
+			float2 rv = r[i];
+			pv.x = fmaf(beta, pv.x, rv.x);
+			pv.y = fmaf(beta, pv.y, rv.y);
+			p[i] = pv;
+		}
+	}
+
+	if ((0 == blockIdx.x) && (0 == threadIdx.x)) {
+
+		st->rs[(it + 1) & 1] = rs_new;
+		st->iters = it + 1;
+
+		if (stop)
+			st->done = 1;
+	}
+}
+
+// 1 / (|F| / sqrt(npix) + 1e-3) as a complex multiplier: the reference's
+// circulant preconditioner (compute_precond, src/noncart/precond.c:56-60)
+// from the N-point spectrum F of its kernel
+__global__ void k_precond_from_spectrum(float2* __restrict__ pinv, const float2* __restrict__ F, long n, float inv_sqrt_npix)
+{
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		float2 v = F[i];
+		float pre = hypotf(v.x, v.y) * inv_sqrt_npix + 1e-3f;
+		pinv[i] = make_float2(1.f / pre, 0.f);
+	}
+}
+
 // after the last iteration: ||r||^2 and the iteration count
 __global__ void k_cg_finish(CgScalars* st, int maxiter, const double* rs_part, int nrs)
 {

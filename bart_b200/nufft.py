@@ -111,6 +111,22 @@ class Linop:
         """linop_normal: domain -> domain (Toeplitz when the plan has a PSF)."""
         return self._call(_lib.load().bnufft_apply_normal, src, dst, self.domain_dims, self.domain_dims)
 
+    def inverse(self, ksp, lam=0.0, maxiter=50, precond=False, dst=None):
+        """``bart nufft -i [-c] -l lam -m maxiter``: CG over the coil images
+        on (N^H N + lam) x = N^H y, optionally with the reference's circulant
+        preconditioner (needs the Toeplitz PSF)."""
+        if self._h is None:
+            raise RuntimeError("linop was freed")
+        nin, nout = int(np.prod(self.codomain_dims)), int(np.prod(self.domain_dims))
+        if dst is None:
+            dst = _alloc_like(ksp, self.domain_dims)
+        pk, keep = _ptr_in(ksp, nin)
+        pd = _ptr_out(dst, nout)
+        _lib.check(_lib.load().bnufft_nufft_inverse(self._h, pd, pk, float(lam), int(maxiter), int(precond),
+                                                    _stream_of(ksp, dst)))
+        del keep
+        return dst
+
     def psf(self):
         """nufft_get_psf: the Toeplitz PSF in the reference's decomposed layout."""
         lib = _lib.load()

@@ -76,6 +76,15 @@ int bnufft_get_psf(bnufft_plan_t plan, int ND, const long psf_dims[], void* psf,
  * trajectory of unchanged dims (weights / basis must be NULL). */
 int bnufft_update_traj(bnufft_plan_t plan, int N, const long traj_dims[], const void* traj, void* stream);
 
+/* bart nufft -i [-c] -l lambda -m maxiter (src/nufft.c:250-263): CG
+ * (conjgrad, src/iter/italgos.c:497) over all coil images jointly on
+ * (N^H N + lambda) x = N^H y, through lsqr2_create (src/iter/lsqr.c:78-167);
+ * with precond the reference's circulant preconditioner
+ * (nufft_precond_create, src/noncart/precond.c:95) is chained in front of
+ * the normal operator and the right-hand side. img: cim dims; ksp: ksp dims. */
+int bnufft_nufft_inverse(bnufft_plan_t plan, void* img, const void* ksp, float lambda, int maxiter,
+		int precond, void* stream);
+
 /* linop_free() of a NUFFT linop (nufft_free_data, src/noncart/nufft.c:1334). */
 void bnufft_free(bnufft_plan_t plan);
 

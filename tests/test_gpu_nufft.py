@@ -165,3 +165,27 @@ def test_deterministic_mode_is_bit_identical():
         op.free()
     assert np.array_equal(outs[0][0].view(np.uint32), outs[1][0].view(np.uint32))
     assert np.array_equal(outs[0][1].view(np.uint32), outs[1][1].view(np.uint32))
+
+
+@pytest.mark.parametrize("key,kw", [("inv_m5", dict(maxiter=5)), ("inv_m5_l", dict(maxiter=5, lam=0.1)),
+                                    ("inv_m5_c", dict(maxiter=5, precond=True)),
+                                    ("inv_m5_c_l", dict(maxiter=5, precond=True, lam=0.1))])
+def test_nufft_inverse_vs_reference(key, kw):
+    """bart nufft -i [-c] [-l] -m5 on three coil images."""
+    g = golden("inverse2d_n32_coils3")
+    td = list(g["traj"].shape)
+    kd = [1, td[1], td[2], 3]
+    op = nufft_create2(kd, [32, 32, 1, 3], td, g["traj"], conf=NufftConf(toeplitz=True))
+    x = op.inverse(g["ksp"].reshape(kd, order="F"), **kw)
+    op.free()
+    assert rel(x, g[key]) < TOL
+
+
+def test_nufft_inverse_30_iterations_precond():
+    g = golden("inverse2d_n32_coils3")
+    td = list(g["traj"].shape)
+    kd = [1, td[1], td[2], 3]
+    op = nufft_create2(kd, [32, 32, 1, 3], td, g["traj"], conf=NufftConf(toeplitz=True))
+    x = op.inverse(g["ksp"].reshape(kd, order="F"), maxiter=30, precond=True)
+    op.free()
+    assert rel(x, g["inv_m30_c"]) < 1e-3
