@@ -9,11 +9,13 @@
 // Degridding (gather): one thread per sample in bin order; neighbouring
 // threads read overlapping taps, so the gathers hit L1, and the weights are
 // computed once per sample for all coils.
-// Gridding (scatter): a block takes one sub-block, accumulates its samples'
-// taps into a zeroed shared-memory tile (the bin plus a halo of HALO cells per
-// side, for a chunk of coils) with shared-memory atomics, and flushes the
-// touched cells to the grid with one global float2 atomic each, instead of one
-// global atomic per tap.
+// Gridding (scatter), default: one thread per sample in bin order with one
+// global float2 atomic per tap (bin order keeps a block's atomics within a
+// few L2 lines). Alternative (BNUFFT_GRIDDING=tiles): a block takes one
+// sub-block, accumulates its samples' taps into a zeroed shared-memory tile
+// (bin plus HALO cells per side, a chunk of coils) with shared-memory atomics
+// and flushes touched cells with one global atomic each; on B200 it measured
+// slower for radial and kooshball data (profiles/gridding_scatter_variants.md).
 //
 // Taps and weights are those of axis_taps (bit-identical to the reference's,
 // src/noncart/grid.c:403-465); only the cell index changes from the DFT-order
