@@ -1211,12 +1211,18 @@ static bool on_device(const void* p)
 }
 
 // staging of host data through device buffers (the e2e path)
+// Staging buffers come from the stream-ordered pool (cudaMallocAsync) and go
+// back to it in stream order, so host-pointer calls neither synchronise the
+// device nor pay cudaMalloc. Host inputs are read asynchronously from pinned
+// memory: keep them unchanged until the stream has caught up (as with
+// cudaMemcpyAsync); calls with host outputs synchronise before returning.
 struct Staged {
 
 	void* dev = nullptr;
 	bool owned = false;
+	cudaStream_t st = nullptr;
 
-	~Staged() { if (owned && dev) cudaFree(dev); }
+	~Staged() { if (owned && dev) cudaFreeAsync(dev, st); }
 };
 
 static int stage_in(Staged& s, const void* p, size_t bytes, cudaStream_t st)
@@ -1227,13 +1233,14 @@ static int stage_in(Staged& s, const void* p, size_t bytes, cudaStream_t st)
 		return BNUFFT_OK;
 	}
 
-	CUDA_TRY(cudaMalloc(&s.dev, bytes));
+	CUDA_TRY(cudaMallocAsync(&s.dev, bytes, st));
 	s.owned = true;
+	s.st = st;
 	CUDA_TRY(cudaMemcpyAsync(s.dev, p, bytes, cudaMemcpyHostToDevice, st));
 	return BNUFFT_OK;
 }
 
-static int stage_out_alloc(Staged& s, void* p, size_t bytes)
+static int stage_out_alloc(Staged& s, void* p, size_t bytes, cudaStream_t st = nullptr)
 {
 	if (on_device(p)) {
 
@@ -1241,8 +1248,9 @@ static int stage_out_alloc(Staged& s, void* p, size_t bytes)
 		return BNUFFT_OK;
 	}
 
-	CUDA_TRY(cudaMalloc(&s.dev, bytes));
+	CUDA_TRY(cudaMallocAsync(&s.dev, bytes, st));
 	s.owned = true;
+	s.st = st;
 	return BNUFFT_OK;
 }
 
@@ -1452,7 +1460,7 @@ extern "C" int bnufft_apply_forward(bnufft_plan_t p, void* dst, const void* src,
 	size_t out_b = sizeof(float2) * p->op.g.M * p->C;
 	Staged i, o;
 	TRY(stage_in(i, src, in_b, st));
-	TRY(stage_out_alloc(o, dst, out_b));
+	TRY(stage_out_alloc(o, dst, out_b, st));
 	TRY(op_forward(p->op, (const float2*)i.dev, nullptr, p->C, (float2*)o.dev, st));
 	return stage_out_copy(o, dst, out_b, st);
 }
@@ -1464,7 +1472,7 @@ extern "C" int bnufft_apply_adjoint(bnufft_plan_t p, void* dst, const void* src,
 	size_t out_b = sizeof(float2) * p->op.g.npix * p->C;
 	Staged i, o;
 	TRY(stage_in(i, src, in_b, st));
-	TRY(stage_out_alloc(o, dst, out_b));
+	TRY(stage_out_alloc(o, dst, out_b, st));
 	TRY(op_adjoint(p->op, (const float2*)i.dev, nullptr, p->C, 1, (float2*)o.dev, st));
 	return stage_out_copy(o, dst, out_b, st);
 }
@@ -1475,7 +1483,7 @@ extern "C" int bnufft_apply_normal(bnufft_plan_t p, void* dst, const void* src, 
 	size_t b = sizeof(float2) * p->op.g.npix * p->C;
 	Staged i, o;
 	TRY(stage_in(i, src, b, st));
-	TRY(stage_out_alloc(o, dst, b));
+	TRY(stage_out_alloc(o, dst, b, st));
 
 	if (p->psf) {
 
@@ -1565,7 +1573,7 @@ extern "C" int bnufft_get_psf(bnufft_plan_t p, int ND, const long psf_dims[], vo
 	cudaStream_t st = S(stream);
 	size_t b = sizeof(float2) * p->op.g.gsz;
 	Staged o;
-	TRY(stage_out_alloc(o, psf, b));
+	TRY(stage_out_alloc(o, psf, b, st));
 	k_psf_decompose<<<vec_blocks(p->op.g.gsz), RED_THREADS, 0, st>>>((float2*)o.dev, p->psf, grid_geom(p->op.g), (float)p->op.g.npix);
 	LAUNCHED();
 	return stage_out_copy(o, psf, b, st);
@@ -1675,7 +1683,7 @@ extern "C" int bnufft_nufft_inverse(bnufft_plan_t p, void* img, const void* ksp,
 	size_t ib = sizeof(float2) * n;
 	Staged ki, io;
 	TRY(stage_in(ki, ksp, kb, st));
-	TRY(stage_out_alloc(io, img, ib));
+	TRY(stage_out_alloc(io, img, ib, st));
 	float2* x = (float2*)io.dev;
 
 	if (precond)
@@ -1916,7 +1924,7 @@ extern "C" int bnufft_pics_normal(bnufft_pics_t ps, void* dst, const void* src, 
 	size_t b = sizeof(float2) * ps->npix;
 	Staged i, o;
 	TRY(stage_in(i, src, b, st));
-	TRY(stage_out_alloc(o, dst, b));
+	TRY(stage_out_alloc(o, dst, b, st));
 	TRY(sense_normal(ps, (const float2*)i.dev, (float2*)o.dev, 0.f, nullptr, nullptr, st));
 	return stage_out_copy(o, dst, b, st);
 }
@@ -1928,7 +1936,7 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 	size_t ib = sizeof(float2) * ps->npix;
 	Staged ki, io;
 	TRY(stage_in(ki, ksp, kb, st));
-	TRY(stage_out_alloc(io, img, ib));
+	TRY(stage_out_alloc(io, img, ib, st));
 
 	OpCtx& op = ps->nufft->op;
 	float2* x = (float2*)io.dev;

@@ -384,15 +384,23 @@ def main():
     if world > 1:
         dist.barrier()
 
-    # end to end through the host API: host arrays in, host image out
+    # end to end through the host API: pinned host arrays in, host image out
+    # (the library stages them through device buffers inside the call)
+    def pinned(a):
+        t = torch.empty(a.size, dtype=torch.complex64, pin_memory=True)
+        v = t.numpy().reshape(a.shape, order="F")
+        v[...] = a
+        return t, v
+
+    _keep = [pinned(traj), pinned(sens), pinned(ksp), pinned(np.zeros((N_IMG, N_IMG, 1), dtype=np.complex64))]
+    traj_h, sens_h, ksp_h, img_h = (v for _, v in _keep)
     h2d = traj.nbytes + sens.nbytes + ksp.nbytes
     d2h = N_IMG * N_IMG * 8
-    img_h = np.zeros((N_IMG, N_IMG, 1), dtype=np.complex64, order="F")
     e2e_steps = max(3, args.steps // 2)
 
     def step_host():
-        p = Pics(traj, sens, ksp_dims=list(ksp.shape), conf=conf)
-        p.run(ksp, out=img_h)
+        p = Pics(traj_h, sens_h, ksp_dims=list(ksp.shape), conf=conf)
+        p.run(ksp_h, out=img_h)
         p.free()
 
     step_host()
