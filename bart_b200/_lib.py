@@ -62,6 +62,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     sig("bnufft_pics_normal", i, vp, vp, vp, vp)
     sig("bnufft_pics_stats", i, vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
         ctypes.POINTER(ctypes.c_float), vp)
+    sig("bnufft_pics_kernels", i, vp, ctypes.POINTER(ctypes.c_long), vp)
     sig("bnufft_pics_free", None, vp)
     sig("bnufft_last_error", ctypes.c_char_p)
     sig("bnufft_launch_count", ctypes.c_long)

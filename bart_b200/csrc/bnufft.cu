@@ -1735,7 +1735,7 @@ extern "C" int bnufft_nufft_inverse(bnufft_plan_t p, void* img, const void* ksp,
 
 		k_combine<<<nb, RED_THREADS, 0, st>>>(Ap, Ap, 1, n, pv, 0.f, pap, &sc->done);
 		LAUNCHED();
-		k_cg_step<<<nb, RED_THREADS, 0, st>>>(x, r, pv, Ap, 1, n, 0.f, sc, it, pap, (int)nb, nullptr, 0, rsp);
+		k_cg_step<<<nb, RED_THREADS, 0, st>>>(x, r, pv, Ap, 1, n, 0.f, sc, it, pap, (int)nb, nullptr, 0, rsp, nullptr);
 		LAUNCHED();
 		k_cg_dir<<<nb, RED_THREADS, 0, st>>>(pv, r, n, sc, it, rsp, (int)nb);
 		LAUNCHED();
@@ -1774,6 +1774,13 @@ struct bnufft_pics_s {
 	long max_row_blocks;
 	int nparts;
 	CgScalars* scal = nullptr;
+	// the CG iterations as one graph: a while node whose body is one iteration
+	cudaStream_t cap = nullptr;	// capture stream
+	cudaGraph_t cg_graph = nullptr;
+	cudaGraphExec_t cg_exec = nullptr;
+	int body_kernels = 0;
+	long last_host_kernels = 0;	// launched from the host by the last run
+	bool last_graph = false;	// last run's CG loop ran as the graph
 };
 
 extern "C" void bnufft_pics_conf_defaults(struct bnufft_pics_conf* c)
@@ -1891,19 +1898,10 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 
 	if (BNUFFT_OK == s) {
 
-		Staged sm;
-		s = stage_in(sm, sens, sizeof(float2) * ps->npix * ps->C, st);
+		cudaError_t e = cudaMemcpyAsync(ps->sens, sens, sizeof(float2) * ps->npix * ps->C, cudaMemcpyDefault, st);
 
-		if (BNUFFT_OK == s) {
-
-			cudaError_t e = cudaMemcpyAsync(ps->sens, sm.dev, sizeof(float2) * ps->npix * ps->C, cudaMemcpyDeviceToDevice, st);
-
-			if ((cudaSuccess == e) && sm.owned)	// staging buffer is freed on return
-				e = cudaStreamSynchronize(st);
-
-			if (cudaSuccess != e)
-				s = fail(BNUFFT_ERR_CUDA, "maps upload: %s", cudaGetErrorString(e));
-		}
+		if (cudaSuccess != e)
+			s = fail(BNUFFT_ERR_CUDA, "maps upload: %s", cudaGetErrorString(e));
 	}
 
 	if (BNUFFT_OK != s) {
@@ -1929,6 +1927,115 @@ extern "C" int bnufft_pics_normal(bnufft_pics_t ps, void* dst, const void* src, 
 	return stage_out_copy(o, dst, b, st);
 }
 
+// One CG iteration on (A^H A + lambda) x = b in four passes: the direction
+// update fused into the first row pass, the normal operator's column passes,
+// the final row pass with the p^H A p partials, and the x / r step with the
+// ||r||^2 partials. it < 0: the kernels take the iteration index from the
+// device counter (the loop runs inside a graph).
+static int pics_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
+{
+	OpCtx& op = ps->nufft->op;
+	const Geom& g = op.g;
+	long YZ = (long)g.N[1] * g.N[2];
+	const int* done = &ps->scal->done;
+	float2* p_prev = ps->pbuf[0];
+	float2* p_cur = ps->pbuf[1];
+	bool toep = (nullptr != ps->nufft->psf);
+	int npp = 0, npap = 0;
+
+	TRY(rows_fwd_cg(g.G[0], ps->b, ps->r, p_prev, p_cur, ps->sens, toep ? nullptr : op.ax, op.ayz,
+			g.N[0], YZ, YZ * ps->C, op.w.t1, ps->scal, it, ps->rs_part, ps->nparts, ps->pp_part, &npp, st));
+
+	DotHook dh;
+	dh.p = p_cur;
+	dh.part = ps->pap_part;
+	dh.done = done;
+	dh.nblocks = &npap;
+
+	if (toep) {
+
+		TRY(op_toeplitz_cols(op, ps->nufft->psf, ps->C, st, done));
+		TRY(rows_inv(g.G[0], op.w.t1, ps->sens, nullptr, nullptr, g.N[0], YZ, (int)ps->C, ps->cpg, ps->part, st,
+				dh.p, dh.part, dh.done, dh.nblocks));
+
+	} else {
+
+		TRY(op_spectrum_cols(op, ps->C, op.w.grid, st));
+		TRY(degrid(op, op.w.grid, ps->C, ps->kbuf, st));
+		TRY(op_adjoint(op, ps->kbuf, ps->sens, ps->C, ps->cpg, ps->part, st, dh));
+	}
+
+	if ((npp > ps->max_row_blocks) || (npap > ps->max_row_blocks))
+		return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
+
+	k_cg_step<<<(unsigned)ps->nparts, RED_THREADS, 0, st>>>(ps->x, ps->r, p_cur, ps->part, ps->groups, ps->npix,
+			ps->conf.lambda, ps->scal, it, ps->pap_part, npap, ps->pp_part, npp, ps->rs_part, p_prev);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+// Capture the CG loop once: a graph holding one while node whose body is an
+// iteration followed by k_cg_advance, which continues the loop until the
+// solve converged or reached maxiter. One graph launch then runs the whole
+// loop with no host round trip and no launches past convergence.
+static int capture_cg_loop(bnufft_pics_s* ps)
+{
+	if (!ps->cap)
+		CUDA_TRY(cudaStreamCreateWithFlags(&ps->cap, cudaStreamNonBlocking));
+
+	CUDA_TRY(cudaGraphCreate(&ps->cg_graph, 0));
+	cudaGraphConditionalHandle loop;
+	CUDA_TRY(cudaGraphConditionalHandleCreate(&loop, ps->cg_graph, 1, cudaGraphCondAssignDefault));
+
+	cudaGraphNodeParams np = {};
+	np.type = cudaGraphNodeTypeConditional;
+	np.conditional.handle = loop;
+	np.conditional.type = cudaGraphCondTypeWhile;
+	np.conditional.size = 1;
+	cudaGraphNode_t node;
+	CUDA_TRY(cudaGraphAddNode(&node, ps->cg_graph, nullptr, 0, &np));
+	cudaGraph_t body = np.conditional.phGraph_out[0];
+
+	CUDA_TRY(cudaStreamBeginCaptureToGraph(ps->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+	long before = g_launches.load();
+	int s = pics_iteration(ps, -1, ps->cap);
+
+	if (BNUFFT_OK == s) {
+
+		k_cg_advance<<<1, 1, 0, ps->cap>>>(ps->scal, ps->conf.maxiter, loop);
+		cudaError_t e = cudaGetLastError();
+
+		if (cudaSuccess != e)
+			s = fail(BNUFFT_ERR_CUDA, "loop capture: %s", cudaGetErrorString(e));
+
+		g_launches.fetch_add(1);
+	}
+
+	// captured kernels are not launches: counted when the graph runs
+	ps->body_kernels = (int)(g_launches.load() - before);
+	g_launches.fetch_sub(ps->body_kernels);
+
+	cudaGraph_t captured = nullptr;
+	cudaError_t e = cudaStreamEndCapture(ps->cap, &captured);
+
+	if (BNUFFT_OK != s)
+		return s;
+
+	CUDA_TRY(e);
+	CUDA_TRY(cudaGraphInstantiate(&ps->cg_exec, ps->cg_graph, 0));
+	return BNUFFT_OK;
+}
+
+static bool cg_graph_enabled()
+{
+	// per-launch profiling needs the kernels launched one by one
+	if (g_prof_active.load(std::memory_order_relaxed))
+		return false;
+
+	const char* e = getenv("BNUFFT_CG_GRAPH");
+	return !(e && (0 == strcmp(e, "0")));
+}
+
 extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, void* stream)
 {
 	cudaStream_t st = S(stream);
@@ -1939,8 +2046,9 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 	TRY(stage_out_alloc(io, img, ib, st));
 
 	OpCtx& op = ps->nufft->op;
-	float2* x = (float2*)io.dev;
 	unsigned nb = (unsigned)ps->nparts;
+	long launches0 = g_launches.load();
+	ps->last_graph = false;
 
 	// adjoint of the data: A^H y (coil-sum partials, then combine)
 	TRY(op_adjoint(op, (const float2*)ki.dev, ps->sens, ps->C, ps->cpg, ps->part, st));
@@ -1966,55 +2074,29 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 	k_scale_dev<<<nb, RED_THREADS, 0, st>>>(ps->b, ps->b, ps->npix, &ps->scal->inv_scale);
 	LAUNCHED();
 
-	// CG from zero on (A^H A + lambda) x = b; per iteration four passes:
-	// direction update fused into the first row pass, the normal operator's
-	// column passes, the final row pass with the p^H A p partials, and the
-	// x / r step with the ||r||^2 partials
-	k_cg_init<<<nb, RED_THREADS, 0, st>>>(x, ps->r, ps->pbuf[1], ps->b, ps->npix, ps->rs_part);
+	// CG from zero (conjgrad, src/iter/italgos.c:497-572)
+	k_cg_init<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, ps->pbuf[1], ps->b, ps->npix, ps->rs_part);
 	LAUNCHED();
 	k_cg_start<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->rs_part, ps->nparts, ps->conf.tol);
 	LAUNCHED();
 
-	const Geom& g = op.g;
-	long YZ = (long)g.N[1] * g.N[2];
-	const int* done = &ps->scal->done;
-	TRY(alloc_work(op.w, g, ps->C, st));
+	TRY(alloc_work(op.w, op.g, ps->C, st));
 
-	for (int it = 0; it < ps->conf.maxiter; it++) {
+	if (ps->conf.maxiter > 0) {
 
-		float2* p_cur = ps->pbuf[it & 1];
-		const float2* p_prev = ps->pbuf[(it + 1) & 1];
-		bool toep = (nullptr != ps->nufft->psf);
-		int npp = 0, npap = 0;
+		if (cg_graph_enabled()) {
 
-		TRY(rows_fwd_cg(g.G[0], ps->b, ps->r, p_prev, p_cur, ps->sens, toep ? nullptr : op.ax, op.ayz,
-				g.N[0], YZ, YZ * ps->C, op.w.t1, ps->scal, it, ps->rs_part, ps->nparts, ps->pp_part, &npp, st));
+			if (!ps->cg_exec)
+				TRY(capture_cg_loop(ps));
 
-		DotHook dh;
-		dh.p = p_cur;
-		dh.part = ps->pap_part;
-		dh.done = done;
-		dh.nblocks = &npap;
-
-		if (toep) {
-
-			TRY(op_toeplitz_cols(op, ps->nufft->psf, ps->C, st, done));
-			TRY(rows_inv(g.G[0], op.w.t1, ps->sens, nullptr, nullptr, g.N[0], YZ, (int)ps->C, ps->cpg, ps->part, st,
-					dh.p, dh.part, dh.done, dh.nblocks));
+			CUDA_TRY(cudaGraphLaunch(ps->cg_exec, st));
+			ps->last_graph = true;
 
 		} else {
 
-			TRY(op_spectrum_cols(op, ps->C, op.w.grid, st));
-			TRY(degrid(op, op.w.grid, ps->C, ps->kbuf, st));
-			TRY(op_adjoint(op, ps->kbuf, ps->sens, ps->C, ps->cpg, ps->part, st, dh));
+			for (int it = 0; it < ps->conf.maxiter; it++)
+				TRY(pics_iteration(ps, it, st));
 		}
-
-		if ((npp > ps->max_row_blocks) || (npap > ps->max_row_blocks))
-			return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
-
-		k_cg_step<<<nb, RED_THREADS, 0, st>>>(x, ps->r, p_cur, ps->part, ps->groups, ps->npix, ps->conf.lambda,
-				ps->scal, it, ps->pap_part, npap, ps->pp_part, npp, ps->rs_part);
-		LAUNCHED();
 	}
 
 	k_cg_finish<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->conf.maxiter, ps->rs_part, ps->nparts);
@@ -2022,11 +2104,25 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 
 	if (ps->conf.rescale) {
 
-		k_scale_dev<<<nb, RED_THREADS, 0, st>>>(x, x, ps->npix, &ps->scal->scale);
+		k_scale_dev<<<nb, RED_THREADS, 0, st>>>((float2*)io.dev, ps->x, ps->npix, &ps->scal->scale);
 		LAUNCHED();
+
+	} else {
+
+		CUDA_TRY(cudaMemcpyAsync(io.dev, ps->x, ib, cudaMemcpyDeviceToDevice, st));
 	}
 
+	ps->last_host_kernels = g_launches.load() - launches0;
 	return stage_out_copy(io, img, ib, st);
+}
+
+extern "C" int bnufft_pics_kernels(bnufft_pics_t ps, long* kernels, void* stream)
+{
+	CgScalars h;
+	CUDA_TRY(cudaMemcpyAsync(&h, ps->scal, sizeof h, cudaMemcpyDeviceToHost, S(stream)));
+	CUDA_TRY(cudaStreamSynchronize(S(stream)));
+	*kernels = ps->last_host_kernels + (ps->last_graph ? (long)h.it * ps->body_kernels : 0L);
+	return BNUFFT_OK;
 }
 
 extern "C" int bnufft_pics_stats(bnufft_pics_t ps, int* iters, double* rel_resid, float* scaling, void* stream)
@@ -2053,6 +2149,16 @@ extern "C" void bnufft_pics_free(bnufft_pics_t ps)
 		return;
 
 	cudaStream_t st = ps->nufft ? ps->nufft->st0 : nullptr;
+
+	if (ps->cg_exec)
+		cudaGraphExecDestroy(ps->cg_exec);
+
+	if (ps->cg_graph)
+		cudaGraphDestroy(ps->cg_graph);
+
+	if (ps->cap)
+		cudaStreamDestroy(ps->cap);
+
 	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->pbuf[0], ps->pbuf[1], ps->b, ps->kbuf, ps->mag, ps->mag_sorted,
 			 ps->sort_tmp, ps->pap_part, ps->pp_part, ps->rs_part, ps->scal };
 

@@ -123,6 +123,7 @@ __global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float 
 		double eps = (double)tol * sqrt(b2);
 		st->eps2 = eps * eps;
 		st->iters = 0;
+		st->it = 0;
 		st->done = (0. == b2);
 	}
 }
@@ -130,16 +131,19 @@ __global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float 
 // Second step of a CG iteration: p^H (A^H A + lambda) p from the partials of
 // the last row pass and of ||p||^2; alpha = rs / p^H A p (float64); then per
 // element Ap = sum_g part_g + lambda p, x += alpha p, r -= alpha Ap, and
-// partial ||r||^2 for the next iteration's direction update.
+// partial ||r||^2 for the next iteration's direction update. p is also
+// copied to p_keep (the next iteration's previous direction) when given.
 __global__ void k_cg_step(float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
 		const float2* __restrict__ part, int groups, long n, float lam, CgScalars* st, int it,
 		const double* __restrict__ pap_part, int npap, const double* __restrict__ pp_part, int npp,
-		double* __restrict__ rs_part)
+		double* __restrict__ rs_part, float2* __restrict__ p_keep)
 {
 	__shared__ double sh[32];
 
 	if (st->done)
 		return;
+
+	it = cg_iter(it, st);
 
 	double pAp = sum_partials(pap_part, npap, sh) + (double)lam * sum_partials(pp_part, npp, sh);
 
@@ -161,6 +165,9 @@ __global__ void k_cg_step(float2* __restrict__ x, float2* __restrict__ r, const 
 
 		float2 pv = p[i];
 		float2 av = part[i];
+
+		if (p_keep)
+			p_keep[i] = pv;
 
 		for (int g = 1; g < groups; g++)
 			av = cadd(av, part[i + n * g]);
@@ -235,6 +242,15 @@ __global__ void k_precond_from_spectrum(float2* __restrict__ pinv, const float2*
 		float pre = hypotf(v.x, v.y) * inv_sqrt_npix + 1e-3f;
 		pinv[i] = make_float2(1.f / pre, 0.f);
 	}
+}
+
+// End of one CG iteration inside a graph: advance the device iteration
+// counter and continue the enclosing while node unless converged or at maxiter.
+__global__ void k_cg_advance(CgScalars* st, int maxiter, cudaGraphConditionalHandle loop)
+{
+	int it = st->it + 1;
+	st->it = it;
+	cudaGraphSetConditional(loop, (!st->done && (it < maxiter)) ? 1u : 0u);
 }
 
 // after the last iteration: ||r||^2 and the iteration count

@@ -95,15 +95,22 @@ struct CgScalars {
 	double b2;		// ||A^H y||^2
 	int done;		// set once converged (or p^H A p == 0)
 	int iters;		// iterations completed
+	int it;			// iteration being run (device-driven loop)
 	float scale;		// data scaling used
 	float inv_scale;	// float(1 / scale)
 };
+
+// iteration index of a CG pass: the host's, or the device counter when the
+// loop runs inside a graph (it < 0)
+__device__ __forceinline__ int cg_iter(int it, const CgScalars* st) { return (it < 0) ? st->it : it; }
 
 // Row pass, forward, first step of a CG iteration (conjgrad,
 // src/iter/italgos.c:538-566, reordered so that the direction update of the
 // previous iteration happens while loading):
 //   it == 0: p = b;  else: rs = ||r||^2 (from the update's partials),
 //   stop if rs <= eps2, beta = rs / rs_prev, p = r + beta p_prev.
+// p_prev and p_cur are distinct buffers (blocks of other coils still read
+// p_prev while coil 0 writes p_cur); the CG step copies p_cur back to p_prev.
 // Rows of coil 0 write p and the partial ||p||^2 (for lambda ||p||^2 in
 // p^H (A^H A + lambda) p); every row multiplies by its coil's map and runs the
 // forward transform like k_rows_fwd.
@@ -124,6 +131,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 	if (st->done)
 		return;
 
+	it = cg_iter(it, st);
 	float beta = 0.f;
 
 	if (it > 0) {

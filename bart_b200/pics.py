@@ -85,6 +85,13 @@ class Pics:
                                                  ctypes.byref(sc), stream))
         return it.value, res.value, sc.value
 
+    def kernels(self, stream=None):
+        """Kernels the last run executed on the device (host launches plus the
+        CG loop graph's body once per iteration it ran)."""
+        n = ctypes.c_long()
+        _lib.check(_lib.load().bnufft_pics_kernels(self._h, ctypes.byref(n), stream))
+        return n.value
+
     def free(self):
         if getattr(self, "_h", None) is not None:
             _lib.load().bnufft_pics_free(self._h)

@@ -2,10 +2,13 @@
 
 Workload (default): 2D radial CG-SENSE, 256x256 image, 16 coils with smooth
 polynomial maps, 96 golden-angle spokes x 512 samples, 40 dB noise,
-lambda 0.01, 30 CG iterations, Toeplitz normal operator, automatic data
-scaling -- ``bart pics -l2 -r0.01 -i30 -t traj ksp sens out``. One step is
-one full reconstruction from device-resident trajectory, maps and k-space:
-model set-up (trajectory upload, PSF on the device), adjoint, scaling, CG.
+lambda 0.01, Toeplitz normal operator, automatic data scaling, plain CG run
+until the relative normal-equation residual reaches 1e-4
+(``bart pics -l2 -r0.01 -t traj ksp sens out`` with the iteration count that
+reaches it). One step is one full reconstruction from device-resident
+trajectory, maps and k-space: model set-up (trajectory upload, PSF on the
+device), adjoint, scaling, CG. L2 is flushed before every timed step. The
+same solve at a fixed 30 iterations, Toeplitz on and off, is reported beside.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -33,9 +36,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_IMG, COILS, SPOKES, READ_OS, LAM, ITERS, SNR_DB = 256, 16, 96, 2, 0.01, 30, 40.0
-METRIC = "CG-SENSE recons/s (2D radial 256^2, 16 coils, 96 spokes x 512, lambda 0.01, 30 CG iters)"
-WORKLOAD = "cgsense2d_256_c16_s96_i30_toeplitz"
+TOL, MAXITER = 1e-4, 300
+# CG iterations that take this seeded problem (seed 1000) to 1e-4: the GPU
+# solve stops there, and the reference's pics (no tolerance option) runs
+# exactly this many
+REF_ITERS_TO_TOL = 50
+METRIC = ("CG-SENSE recons/s to 1e-4 rel. normal-equation residual "
+          "(plain CG; 2D radial 256^2, 16 coils, 96 spokes x 512, lambda 0.01)")
+WORKLOAD = "cgsense2d_256_c16_s96_tol1e-4_toeplitz"
 DOMINANT = "cols_toeplitz"
+L2_FLUSH_BYTES = 512 << 20     # > 126 MB L2
 
 
 def make_problem(seed: int):
@@ -142,41 +152,33 @@ def nufft_throughput(dev, steps=50, warmup=5):
             "us_per_fwd_adj": ms * 1e3, "bytes_per_step": nbytes}
 
 
-def cg_to_tolerance(dev, traj, sens, ksp, tol=1e-4, maxiter=300, runs=5):
-    """Plain CG on the CG-SENSE workload until ||r|| <= tol ||A^H y|| (the
-    recursive residual), model reused; reports iterations, time per solve and
-    the true relative normal-equation residual of the result."""
+def true_residual(dev, p, traj_d, sens_d, ksp_d, x, ksp_shape, traj_shape, scale):
+    """||b - (A^H A + lambda) x|| / ||b|| with b = A^H y / scale, recomputed
+    from the operators (not CG's recursive residual)."""
     import torch
     from bart_b200.nufft import NufftConf, nufft_create2
-    from bart_b200.pics import Pics, PicsConf
-
-    def dt(a):
-        return torch.from_numpy(np.asfortranarray(a).ravel(order="F").copy()).to(dev)
-
-    traj_d, sens_d, ksp_d = dt(traj), dt(sens), dt(ksp)
-    p = Pics(traj_d, sens_d, ksp_dims=list(ksp.shape), conf=PicsConf(lam=LAM, maxiter=maxiter, tol=tol),
-             traj_dims=list(traj.shape), sens_dims=list(sens.shape))
-    x = p.run(ksp_d)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(runs):
-        p.run(ksp_d, out=x)
-    e1.record()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / runs
-    iters, rres, scale = p.stats()
-    # true residual: b = A^H y / scale, r = b - (A^H A + lambda) x
-    kd = list(ksp.shape)
-    op = nufft_create2(kd, [N_IMG, N_IMG, 1, COILS], list(traj.shape), traj_d, conf=NufftConf(toeplitz=False))
+    op = nufft_create2(list(ksp_shape), [N_IMG, N_IMG, 1, COILS], list(traj_shape), traj_d,
+                       conf=NufftConf(toeplitz=False))
     adj = op.adjoint(ksp_d).reshape(COILS, N_IMG * N_IMG)
     b = (torch.conj(sens_d.reshape(COILS, N_IMG * N_IMG)) * adj).sum(0) / scale
     r = b - (p.normal(x) + LAM * x)
-    true_res = float(torch.linalg.vector_norm(r) / torch.linalg.vector_norm(b))
     op.free()
-    p.free()
-    return {"tol": tol, "iterations": iters, "ms_per_recon_model_reused": ms, "recons_per_s_model_reused": 1e3 / ms,
-            "recursive_rel_residual": rres, "true_rel_residual": true_res}
+    return float(torch.linalg.vector_norm(r) / torch.linalg.vector_norm(b))
+
+
+def timed_steps(step, steps, flush, stream):
+    """Device time (ms) of `steps` calls of step(), each bracketed by CUDA
+    events on `stream` after an L2 flush (outside the bracket)."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        step()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return sum(e0.elapsed_time(e1) for e0, e1 in ev)
 
 
 def run_nufft3d(dev, steps, warmup):
@@ -233,7 +235,7 @@ def run_nufft3d(dev, steps, warmup):
             "cgsense_setup_s": setup_s, "cgsense_10iter_ms": cg_ms}
 
 
-def reference_pics_seconds(traj, sens, ksp, iters=ITERS, threads=None):
+def reference_pics_seconds(traj, sens, ksp, iters=REF_ITERS_TO_TOL, threads=None, out=None):
     """Wall time of the reference's own CPU ``pics`` (built from its sources
     into oracle/_ref) on this workload, or None if it is not built."""
     exe = os.path.join(ROOT, "oracle", "_ref", "bin", "pics")
@@ -250,26 +252,30 @@ def reference_pics_seconds(traj, sens, ksp, iters=ITERS, threads=None):
         r = subprocess.run([exe, "-l2", f"-r{LAM}", f"-i{iters}", "-t", "t", "k", "s", "o"], cwd=d, env=env,
                            capture_output=True, text=True)
         dt = time.perf_counter() - t0
+        if r.returncode == 0 and out is not None:
+            from bart_b200.cfl import readcfl
+            out.append(readcfl(os.path.join(d, "o")))
     if r.returncode != 0:
         raise RuntimeError("reference pics failed: " + r.stderr[-500:])
     return dt
 
 
-def oracle_pics_seconds(traj, sens, ksp):
+def oracle_pics_seconds(traj, sens, ksp, iters=REF_ITERS_TO_TOL):
     from oracle import nufft_oracle as orc
     t0 = time.perf_counter()
-    orc.pics_l2(traj.real.reshape(3, -1, order="F"), ksp.reshape(-1, COILS, order="F"), sens, lam=LAM, maxiter=ITERS)
+    orc.pics_l2(traj.real.reshape(3, -1, order="F"), ksp.reshape(-1, COILS, order="F"), sens, lam=LAM, maxiter=iters)
     return time.perf_counter() - t0
 
 
-def cpu_baseline(traj, sens, ksp):
-    dt = reference_pics_seconds(traj, sens, ksp)
+def cpu_baseline(traj, sens, ksp, iters):
+    dt = reference_pics_seconds(traj, sens, ksp, iters=iters)
     if dt is not None:
         return {"value": 1.0 / dt, "unit": "recons/s", "cores": os.cpu_count(), "kind": "reference",
-                "sample": "1 full recon with the reference's CPU pics (OpenMP, MKL FFT via FFTW shim), wall incl. .cfl I/O"}
-    dt = oracle_pics_seconds(traj, sens, ksp)
+                "sample": f"1 full recon with the reference's CPU pics -i{iters} (the GPU's iteration count to 1e-4; "
+                          "OpenMP, MKL FFT via FFTW shim), wall incl. .cfl I/O"}
+    dt = oracle_pics_seconds(traj, sens, ksp, iters)
     return {"value": 1.0 / dt, "unit": "recons/s", "cores": 1, "kind": "port",
-            "sample": "1 full recon with the NumPy oracle (float64)"}
+            "sample": f"1 full recon of {iters} CG iterations with the NumPy oracle (float64)"}
 
 
 def run_reference(args, rank, world):
@@ -284,23 +290,41 @@ def run_reference(args, rank, world):
     y = A.forward(truth.reshape(N_IMG, N_IMG, 1, 1))
     ksp = synth.add_noise(y, SNR_DB, rng).reshape(1, traj.shape[1], traj.shape[2], COILS, order="F")
     kind = "reference" if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "bin", "pics")) else "port"
-    run = (lambda: reference_pics_seconds(traj, sens, ksp)) if kind == "reference" else \
+    outs = []
+    run = (lambda: reference_pics_seconds(traj, sens, ksp, out=outs)) if kind == "reference" else \
         (lambda: oracle_pics_seconds(traj, sens, ksp))
     for _ in range(args.warmup):
         run()
     times = [run() for _ in range(args.steps)]
     tot = sum(times)
     value = args.steps / tot
+    true_res = None
+    if outs:
+        # the reference's result against the FP64 normal equations it solves
+        yk = ksp.reshape(-1, COILS, order="F")
+        adj = A.adjoint(yk)
+        scale = orc.estimate_scaling_norm(adj)
+        x = outs[-1].astype(np.complex128).reshape(adj.shape, order="F")
+        true_res = float(orc.normal_residual(A, x, adj / scale, LAM))
     line = {"metric": METRIC, "value": value, "unit": "recons/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": WORKLOAD, "image": N_IMG, "coils": COILS, "spokes": SPOKES, "samples": 512,
-                       "iters": ITERS, "lambda": LAM, "toeplitz": True},
+                       "tol": TOL, "iters": REF_ITERS_TO_TOL, "lambda": LAM, "toeplitz": True},
+            "true_rel_residual": true_res,
             "cpu_baseline": {"value": value, "unit": "recons/s", "cores": os.cpu_count() if kind == "reference" else 1,
-                             "kind": kind, "sample": "full recon per step, wall time incl. .cfl I/O"},
+                             "kind": kind, "sample": f"full recon per step (pics -l2 -r{LAM} -i{REF_ITERS_TO_TOL}), "
+                                                     "wall time incl. .cfl I/O"},
             "e2e": {"value": value, "unit": "recons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
 
 
 def main():
@@ -320,6 +344,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+
+    import ctypes
 
     import torch
     import torch.distributed as dist
@@ -349,40 +375,57 @@ def main():
 
     traj_d, sens_d, ksp_d = dev_tensor(traj), dev_tensor(sens), dev_tensor(ksp)
     img_d = torch.empty(N_IMG * N_IMG, dtype=torch.complex64, device=dev)
-    conf = PicsConf(lam=LAM, maxiter=ITERS, toeplitz=True)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    conf = PicsConf(lam=LAM, maxiter=MAXITER, tol=TOL, toeplitz=True)
 
-    def step():
-        p = Pics(traj_d, sens_d, ksp_dims=list(ksp.shape), conf=conf, traj_dims=list(traj.shape),
-                 sens_dims=list(sens.shape))
+    def make(c):
+        return Pics(traj_d, sens_d, ksp_dims=list(ksp.shape), conf=c, traj_dims=list(traj.shape),
+                    sens_dims=list(sens.shape))
+
+    def step(c=conf):
+        p = make(c)
         p.run(ksp_d, out=img_d)
         p.free()
 
     for _ in range(max(3, args.warmup)):
         step()
+
+    # iterations, residuals and device kernels of one step (untimed)
+    p = make(conf)
+    p.run(ksp_d, out=img_d)
+    iters, rres, scale = p.stats()
+    kernels_per_step = p.kernels()
+    tres = true_residual(dev, p, traj_d, sens_d, ksp_d, img_d, ksp.shape, traj.shape, scale)
+    p.free()
+
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-
-    stream = torch.cuda.current_stream(dev)
-    l0 = lib.bnufft_launch_count()
-    lib.bnufft_prof_start(DOMINANT.encode())
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(args.steps):
-            step()
-        e1.record(stream)
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    launches = lib.bnufft_launch_count() - l0
-    import ctypes
-    kms, kn = ctypes.c_double(), ctypes.c_long()
-    lib.bnufft_prof_stop(ctypes.byref(kms), ctypes.byref(kn))
-
+        ms = timed_steps(step, args.steps, flush, stream)
     ms_max = reduce_max(ms, dev)
     if world > 1:
         dist.barrier()
+
+    # dominant kernel: per-launch CUDA events over the same steps, run again
+    # with the CG loop launched from the host (events cannot sit inside the
+    # graph's while body) for exactly the iterations the solve took, so the
+    # same kernels run on the same inputs
+    conf_prof = PicsConf(lam=LAM, maxiter=iters, tol=0.0, toeplitz=True)
+    lib.bnufft_prof_start(DOMINANT.encode())
+    timed_steps(lambda: step(conf_prof), args.steps, flush, stream)
+    kms, kn = ctypes.c_double(), ctypes.c_long()
+    lib.bnufft_prof_stop(ctypes.byref(kms), ctypes.byref(kn))
+
+    # the same solve at a fixed 30 iterations (Toeplitz on and off)
+    fixed = {}
+    for toep in (True, False):
+        c = PicsConf(lam=LAM, maxiter=ITERS, toeplitz=toep)
+        step(c)
+        fms = timed_steps(lambda: step(c), max(3, args.steps // 4), flush, stream)
+        fixed["toeplitz" if toep else "no_toeplitz"] = {"recons_per_s": max(3, args.steps // 4) / (fms / 1e3),
+                                                        "ms_per_recon": fms / max(3, args.steps // 4)}
 
     # end to end through the host API: pinned host arrays in, host image out
     # (the library stages them through device buffers inside the call)
@@ -399,31 +442,29 @@ def main():
     e2e_steps = max(3, args.steps // 2)
 
     def step_host():
-        p = Pics(traj_h, sens_h, ksp_dims=list(ksp.shape), conf=conf)
-        p.run(ksp_h, out=img_h)
-        p.free()
+        ph = Pics(traj_h, sens_h, ksp_dims=list(ksp.shape), conf=conf)
+        ph.run(ksp_h, out=img_h)       # returns after the image is on the host
+        ph.free()
 
     step_host()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    t0 = time.perf_counter()
+    e2e_t = 0.0
     for _ in range(e2e_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         step_host()
-    torch.cuda.synchronize()
-    e2e_s = reduce_max(time.perf_counter() - t0, dev)
+        e2e_t += time.perf_counter() - t0
+    e2e_s = reduce_max(e2e_t, dev)
 
     # roofline of the dominant kernel: Toeplitz column pass, per launch
     # reads + writes the [2X, Y, C] row-transformed buffer and reads the PSF
     G0, G1 = 2 * N_IMG, 2 * N_IMG
     alg_bytes = 2 * (G0 * N_IMG * COILS * 8) + G0 * G1 * 8
     k_avg_s = (kms.value / 1e3) / max(1, kn.value)
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(peaks_path):
-        peak = float(json.load(open(peaks_path))["hbm_gbs"])
-        peak_src = "measured"
-    else:
-        peak, peak_src = 6650.0, "fallback"
+    peak, peak_src = peak_hbm()
     achieved = alg_bytes / k_avg_s / 1e9 if k_avg_s > 0 else None
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
@@ -431,13 +472,6 @@ def main():
         traffic = json.load(open(tpath)).get(DOMINANT)
 
     nufft = nufft_throughput(dev) if rank == 0 else None
-    to_tol = cg_to_tolerance(dev, traj, sens, ksp) if rank == 0 else None
-    # residual reached by the timed 30-iteration solve
-    p30 = Pics(traj_d, sens_d, ksp_dims=list(ksp.shape), conf=conf, traj_dims=list(traj.shape),
-               sens_dims=list(sens.shape))
-    p30.run(ksp_d, out=img_d)
-    it30, res30, _ = p30.stats()
-    p30.free()
 
     if rank == 0:
         value = aggregate_rate(world, args.steps, ms_max / 1e3)
@@ -445,21 +479,27 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "image": N_IMG, "coils": COILS, "spokes": SPOKES, "samples": 512,
-                           "iters": ITERS, "lambda": LAM, "toeplitz": True, "parallelism": f"replicas{world}",
-                           "l2": "inputs and work buffers (~60 MB) are L2-resident; no flush between steps"},
+                           "tol": TOL, "maxiter": MAXITER, "lambda": LAM, "toeplitz": True,
+                           "parallelism": f"replicas{world}",
+                           "l2": "flushed before every timed step (512 MB write); inside a step the ~60 MB "
+                                 "working set stays L2-resident across CG iterations"},
                 "e2e": {"value": aggregate_rate(world, e2e_steps, e2e_s), "unit": "recons/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "gpu_launches": launches,
-                "cg": {"iterations": it30, "recursive_rel_residual": res30, "to_1e-4": to_tol},
+                "gpu_launches": kernels_per_step * args.steps,
+                "cg": {"iterations": iters, "recursive_rel_residual": rres, "true_rel_residual": tres,
+                       "loop": "one CUDA graph with a while node per solve"},
+                "fixed_30_iters": fixed,
                 "nufft": nufft,
                 "roofline": {"bound": "hbm", "kernel": DOMINANT, "achieved": achieved, "peak": peak,
                              "peak_source": peak_src, "unit": "GB/s",
                              "frac": (achieved / peak) if achieved else None,
                              "traffic": traffic, "alg_bytes": alg_bytes,
-                             "avg_launch_us": k_avg_s * 1e6, "launches": kn.value},
+                             "avg_launch_us": k_avg_s * 1e6, "launches": kn.value,
+                             "timing": "CUDA events per launch over the same steps, CG loop host-launched "
+                                       "for the solve's iteration count"},
                 "clocks": clk.summary()}
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(traj, sens, ksp)
+            line["cpu_baseline"] = cpu_baseline(traj, sens, ksp, iters)
         print(json.dumps(line), flush=True)
 
     if world > 1:

@@ -142,6 +142,13 @@ int bnufft_pics_normal(bnufft_pics_t pics, void* dst, const void* src, void* str
  * ||r||/||A^H y||, scaling used. Synchronises the stream. */
 int bnufft_pics_stats(bnufft_pics_t pics, int* iters, double* rel_resid, float* scaling, void* stream);
 
+/* Kernels the last run executed on the device: the ones launched from the
+ * host plus those of the CG loop graph (its body once per iteration run).
+ * Synchronises the stream. The CG loop runs as one CUDA graph with a while
+ * node unless the environment sets BNUFFT_CG_GRAPH=0 (host loop, same
+ * kernels and bit-identical results). */
+int bnufft_pics_kernels(bnufft_pics_t pics, long* kernels, void* stream);
+
 void bnufft_pics_free(bnufft_pics_t pics);
 
 /* Message of the last failure on this thread ("" if none). */

@@ -1,5 +1,7 @@
 """GPU CG-SENSE (pics -l2) through the C ABI against the reference and the oracle."""
 
+import os
+
 import numpy as np
 import pytest
 
@@ -85,3 +87,31 @@ def test_pics_deterministic_mode_bit_identical():
     assert st1 == st2
     x5, _ = _run(g, maxiter=5, scaling=1.0, deterministic=True)
     assert rel(x5, g["x5_w1"]) < 1e-5
+
+
+@pytest.mark.parametrize("tol", [0.0, 1e-4])
+def test_cg_loop_graph_matches_host_loop(tol):
+    """The CG loop as one graph (a while node over one iteration) and the
+    host-driven loop run the same kernels: identical bits in deterministic
+    mode, the same stopping iteration, and the graph runs no kernels past
+    convergence."""
+    g = golden("pics2d_n64_c4")
+    res = {}
+    for mode in ("1", "0"):
+        os.environ["BNUFFT_CG_GRAPH"] = mode
+        try:
+            p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
+                     conf=PicsConf(lam=0.01, maxiter=200 if tol else 12, tol=tol, deterministic=True))
+            x = np.asarray(p.run(g["ksp"]))
+            res[mode] = (x, p.stats(), p.kernels())
+            p.free()
+        finally:
+            os.environ.pop("BNUFFT_CG_GRAPH", None)
+    (xg, sg, kg), (xh, sh, kh) = res["1"], res["0"]
+    assert np.array_equal(xg.view(np.uint32), xh.view(np.uint32))
+    assert sg == sh
+    if tol:
+        assert 10 < sg[0] < 200 and sg[1] <= tol
+        assert kg < kh / 2      # the host loop launches all 200 iterations
+    else:
+        assert sg[0] == 12 and kg == kh + sg[0]    # plus one loop-advance kernel per iteration
