@@ -24,7 +24,7 @@ class NufftConfC(ctypes.Structure):
 class PicsConfC(ctypes.Structure):
     _fields_ = [("lambda_", ctypes.c_float), ("maxiter", ctypes.c_int), ("tol", ctypes.c_float),
                 ("scaling", ctypes.c_float), ("rescale", ctypes.c_int), ("toeplitz", ctypes.c_int),
-                ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int)]
+                ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int), ("precond", ctypes.c_int)]
 
 
 _lib = None

@@ -330,14 +330,14 @@ static int prep_kernel(K kernel, size_t smem)
 
 template <int L, int B>
 static int launch_rows_fwd_LB(const float2* img, const float2* maps, const float* ax, const float* ayz,
-		int X, long YZ, long R, float2* out, cudaStream_t st)
+		int X, long YZ, long R, float2* out, cudaStream_t st, const int* done)
 {
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
 	size_t smem = rows_smem(L, B);
 	TRY(prep_kernel(k_rows_fwd<L, B>, smem));
 	cudaEvent_t pe = prof_begin("rows_fwd", st);
-	k_rows_fwd<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(img, maps, ax, ayz, X, YZ, R, out, tw);
+	k_rows_fwd<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(img, maps, ax, ayz, X, YZ, R, out, tw, done);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
@@ -422,10 +422,10 @@ static int launch_rows_fwd_cg_LB(const float2* bvec, const float2* r, const floa
 	return fail(BNUFFT_ERR_ARG, "no FFT pass instance for L=%d B=%d", L, B);
 
 static int rows_fwd(int L, const float2* img, const float2* maps, const float* ax, const float* ayz,
-		int X, long YZ, long R, float2* out, cudaStream_t st)
+		int X, long YZ, long R, float2* out, cudaStream_t st, const int* done = nullptr)
 {
 	int B = choose_B(L, R);
-	DISPATCH_LB(L, B, (launch_rows_fwd_LB<LL, BB>(img, maps, ax, ayz, X, YZ, R, out, st)));
+	DISPATCH_LB(L, B, (launch_rows_fwd_LB<LL, BB>(img, maps, ax, ayz, X, YZ, R, out, st, done)));
 }
 
 static int cols(int L, int mode, const float2* in, long ies, long ios, int n_in, int wrap_in,
@@ -1771,6 +1771,11 @@ struct bnufft_pics_s {
 	double* pap_part = nullptr;	// p^H partial, one per final row-pass block
 	double* pp_part = nullptr;	// ||p||^2, one per first row-pass block
 	double* rs_part = nullptr;	// ||r||^2, one per CG step block
+	// flexible CG (conf.precond): z = M(r), A p kept for the next direction
+	float2 *z = nullptr, *Ap = nullptr;
+	double* zap_part = nullptr;	// <A p_prev, z>, one per preconditioner row-pass block
+	double* pr_part = nullptr;	// <p, r>, one per direction-update block
+	int nzap = 0;
 	long max_row_blocks;
 	int nparts;
 	CgScalars* scal = nullptr;
@@ -1793,6 +1798,7 @@ extern "C" void bnufft_pics_conf_defaults(struct bnufft_pics_conf* c)
 	c->toeplitz = 1;
 	c->periodic = 0;
 	c->deterministic = 0;
+	c->precond = 0;
 }
 
 // A^H A x (+ lam x), with optional per-block Re<x, out> partials
@@ -1848,6 +1854,12 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 	nc.periodic = conf.periodic;
 	nc.deterministic = conf.deterministic;
 
+	if ((conf.precond < 0) || (conf.precond > 2))
+		return fail(BNUFFT_ERR_ARG, "precond must be 0, 1 or 2");
+
+	if (conf.precond && !conf.toeplitz)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "the circulant preconditioner needs the Toeplitz normal operator");
+
 	auto ps = new bnufft_pics_s();
 	ps->conf = conf;
 	int s = bnufft_create2(&ps->nufft, N, ksp_dims, sens_dims, traj_dims, traj, nullptr, nullptr, nullptr, nullptr, &nc, stream);
@@ -1883,12 +1895,24 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 	// row-pass blocks hold at least 4 rows: bounds for the partial arrays
 	ps->max_row_blocks = (YZ + 3) / 4 * ps->C + 1;
 	ck(cudaMallocAsync(&ps->pap_part, sizeof(double) * ps->max_row_blocks, st));
-	ck(cudaMallocAsync(&ps->pp_part, sizeof(double) * ps->max_row_blocks, st));
+	// ||p||^2 partials: per first row-pass block (plain CG) or per vector block (flexible CG)
+	ck(cudaMallocAsync(&ps->pp_part, sizeof(double) * std::max<long>(ps->max_row_blocks, ps->nparts), st));
 	ck(cudaMallocAsync(&ps->rs_part, sizeof(double) * ps->nparts, st));
 	ck(cudaMallocAsync(&ps->scal, sizeof(CgScalars), st));
 
 	if (!conf.toeplitz)
 		ck(cudaMallocAsync(&ps->kbuf, sizeof(float2) * ps->M * ps->C, st));
+
+	if (conf.precond) {
+
+		ck(cudaMallocAsync(&ps->z, sizeof(float2) * ps->npix, st));
+		ck(cudaMallocAsync(&ps->Ap, sizeof(float2) * ps->npix, st));
+		ck(cudaMallocAsync(&ps->zap_part, sizeof(double) * ps->max_row_blocks, st));
+		ck(cudaMallocAsync(&ps->pr_part, sizeof(double) * ps->nparts, st));
+
+		if (BNUFFT_OK == s)
+			s = build_precond(ps->nufft, st);
+	}
 
 	if (BNUFFT_OK == s) {
 
@@ -1974,6 +1998,73 @@ static int pics_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	return BNUFFT_OK;
 }
 
+// z = M(r): the circulant preconditioner applied to one image (N-point
+// transforms, no padding); optional partials Re<pdot, z>
+static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
+		int* nblocks, cudaStream_t st)
+{
+	bnufft_plan_s* p = ps->nufft;
+	const int* done = &ps->scal->done;
+	OpCtx full;
+	full.g = p->op.g;
+
+	for (int a = 0; a < 3; a++)
+		full.g.G[a] = full.g.N[a];
+
+	full.g.gsz = full.g.npix;
+	full.kb = p->op.kb;
+	full.traj = nullptr;
+	full.w = p->op.w;	// the plan's buffers (N <= 2N), free between the operator's passes
+	const Geom& g = full.g;
+	long YZ = (long)g.N[1] * g.N[2];
+	TRY(rows_fwd(g.G[0], r, nullptr, nullptr, nullptr, g.N[0], YZ, YZ, full.w.t1, st, done));
+	TRY(op_toeplitz_cols(full, p->pinv, 1, st, done));
+	return rows_inv(g.G[0], full.w.t1, nullptr, nullptr, nullptr, g.N[0], YZ, 1, 1, z, st, pdot, dot_part, done, nblocks);
+}
+
+// One flexible-CG iteration: direction update, the normal operator's passes
+// (as in plain CG), the step, the convergence test and z = M(r).
+static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
+{
+	OpCtx& op = ps->nufft->op;
+	const Geom& g = op.g;
+	long YZ = (long)g.N[1] * g.N[2];
+	const int* done = &ps->scal->done;
+	float2* p = ps->pbuf[1];
+	unsigned nb = (unsigned)ps->nparts;
+	int npap = 0;
+
+	k_fcg_dir<<<nb, RED_THREADS, 0, st>>>(p, ps->z, ps->r, ps->npix, ps->scal, it, ps->zap_part, ps->nzap,
+			ps->pr_part, ps->pp_part);
+	LAUNCHED();
+	TRY(rows_fwd(g.G[0], p, ps->sens, nullptr, nullptr, g.N[0], YZ, YZ * ps->C, op.w.t1, st, done));
+	TRY(op_toeplitz_cols(op, ps->nufft->psf, ps->C, st, done));
+	TRY(rows_inv(g.G[0], op.w.t1, ps->sens, nullptr, nullptr, g.N[0], YZ, (int)ps->C, ps->cpg, ps->part, st,
+			p, ps->pap_part, done, &npap));
+
+	if (npap > ps->max_row_blocks)
+		return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
+
+	k_fcg_step<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, p, ps->Ap, ps->part, ps->groups, ps->npix, ps->conf.lambda,
+			ps->scal, it, ps->pap_part, npap, ps->pp_part, ps->nparts, ps->pr_part, ps->nparts, ps->rs_part);
+	LAUNCHED();
+	k_fcg_check<<<1, RED_THREADS, 0, st>>>(ps->scal, it, ps->rs_part, ps->nparts);
+	LAUNCHED();
+	int nz = 0;
+	TRY(pics_precond(ps, ps->r, ps->z, ps->Ap, ps->zap_part, &nz, st));
+
+	if (nz > ps->max_row_blocks)
+		return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
+
+	ps->nzap = nz;
+	return BNUFFT_OK;
+}
+
+static int pics_any_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
+{
+	return ps->conf.precond ? pics_fcg_iteration(ps, it, st) : pics_iteration(ps, it, st);
+}
+
 // Capture the CG loop once: a graph holding one while node whose body is an
 // iteration followed by k_cg_advance, which continues the loop until the
 // solve converged or reached maxiter. One graph launch then runs the whole
@@ -1998,7 +2089,7 @@ static int capture_cg_loop(bnufft_pics_s* ps)
 
 	CUDA_TRY(cudaStreamBeginCaptureToGraph(ps->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
 	long before = g_launches.load();
-	int s = pics_iteration(ps, -1, ps->cap);
+	int s = pics_any_iteration(ps, -1, ps->cap);
 
 	if (BNUFFT_OK == s) {
 
@@ -2082,6 +2173,13 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 
 	TRY(alloc_work(op.w, op.g, ps->C, st));
 
+	if (ps->conf.precond) {	// z0 = M(b); the first direction is p = z0
+
+		int nz = 0;
+		TRY(pics_precond(ps, ps->r, ps->z, nullptr, nullptr, &nz, st));
+		ps->nzap = nz;
+	}
+
 	if (ps->conf.maxiter > 0) {
 
 		if (cg_graph_enabled()) {
@@ -2095,7 +2193,7 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 		} else {
 
 			for (int it = 0; it < ps->conf.maxiter; it++)
-				TRY(pics_iteration(ps, it, st));
+				TRY(pics_any_iteration(ps, it, st));
 		}
 	}
 
@@ -2160,7 +2258,8 @@ extern "C" void bnufft_pics_free(bnufft_pics_t ps)
 		cudaStreamDestroy(ps->cap);
 
 	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->pbuf[0], ps->pbuf[1], ps->b, ps->kbuf, ps->mag, ps->mag_sorted,
-			 ps->sort_tmp, ps->pap_part, ps->pp_part, ps->rs_part, ps->scal };
+			 ps->sort_tmp, ps->pap_part, ps->pp_part, ps->rs_part, ps->scal, ps->z, ps->Ap, ps->zap_part,
+			 ps->pr_part };
 
 	for (void* b : bufs)
 		if (b)
@@ -2340,7 +2439,7 @@ static int na_rows(const float2* img, const float* ax, const float* ayz, int X, 
 	constexpr int B = 16;
 	size_t smem = rows_smem(L, B);
 	CUDA_TRY(cudaFuncSetAttribute(k_rows_fwd<L, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-	k_rows_fwd<L, B><<<(unsigned)((Y + B - 1) / B), B * L / 8, smem, st>>>(img, nullptr, ax, ayz, X, Y, Y, out, tw);
+	k_rows_fwd<L, B><<<(unsigned)((Y + B - 1) / B), B * L / 8, smem, st>>>(img, nullptr, ax, ayz, X, Y, Y, out, tw, nullptr);
 	LAUNCHED();
 	return BNUFFT_OK;
 }

@@ -244,6 +244,139 @@ __global__ void k_precond_from_spectrum(float2* __restrict__ pinv, const float2*
 	}
 }
 
+// Flexible CG (Notay, SIAM J. Sci. Comput. 22(4), 2000: FCG with one
+// previous direction), used with a preconditioner z = M(r) that may be
+// nonlinear (the learned one) or only approximately symmetric:
+//   p = z + beta p_prev, beta = -<z, A p_prev> / <p_prev, A p_prev>
+//   alpha = <p, r> / <p, A p>,  x += alpha p,  r -= alpha A p.
+// Direction update in place (elementwise), with the partials <p, r> and
+// ||p||^2 (lambda ||p||^2 in <p, (A^H A + lambda) p>).
+__global__ void k_fcg_dir(float2* __restrict__ p, const float2* __restrict__ z, const float2* __restrict__ r, long n,
+		const CgScalars* st, int it, const double* __restrict__ zap_part, int nzap,
+		double* __restrict__ pr_part, double* __restrict__ pp_part)
+{
+	__shared__ double sh[32];
+
+	if (st->done)
+		return;
+
+	it = cg_iter(it, st);
+	float beta = 0.f;
+
+	if (it > 0)
+		beta = (float)(-sum_partials(zap_part, nzap, sh) / st->pap);
+
+	double pr = 0., pp = 0.;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		float2 zv = z[i];
+		float2 pv = (it > 0) ? p[i] : make_float2(0.f, 0.f);
+		pv.x = fmaf(beta, pv.x, zv.x);
+		pv.y = fmaf(beta, pv.y, zv.y);
+		p[i] = pv;
+		float2 rv = r[i];
+		pr += (double)pv.x * (double)rv.x + (double)pv.y * (double)rv.y;
+		pp += (double)pv.x * (double)pv.x + (double)pv.y * (double)pv.y;
+	}
+
+	double t = block_sum(pr, sh);
+	__syncthreads();
+	double u = block_sum(pp, sh);
+
+	if (0 == threadIdx.x) {
+
+		pr_part[blockIdx.x] = t;
+		pp_part[blockIdx.x] = u;
+	}
+}
+
+// FCG step: <p, A p> (coil-sum row-pass partials + lambda ||p||^2), alpha =
+// <p, r> / <p, A p>; per element A p = sum_g part_g + lambda p (kept for the
+// next direction), x += alpha p, r -= alpha A p, partial ||r||^2.
+__global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
+		float2* __restrict__ Ap, const float2* __restrict__ part, int groups, long n, float lam, CgScalars* st, int it,
+		const double* __restrict__ pap_part, int npap, const double* __restrict__ pp_part, int npp,
+		const double* __restrict__ pr_part, int npr, double* __restrict__ rs_part)
+{
+	__shared__ double sh[32];
+
+	if (st->done)
+		return;
+
+	it = cg_iter(it, st);
+	double pAp = sum_partials(pap_part, npap, sh) + (double)lam * sum_partials(pp_part, npp, sh);
+
+	if (!(pAp > 0.)) {	// zero or not positive: breakdown
+
+		if ((0 == blockIdx.x) && (0 == threadIdx.x)) {
+
+			st->done = 1;
+			st->iters = it;
+		}
+
+		return;
+	}
+
+	float a = (float)(sum_partials(pr_part, npr, sh) / pAp);
+	double acc = 0.;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		float2 pv = p[i];
+		float2 av = part[i];
+
+		for (int g = 1; g < groups; g++)
+			av = cadd(av, part[i + n * g]);
+
+		av.x = fmaf(lam, pv.x, av.x);
+		av.y = fmaf(lam, pv.y, av.y);
+		Ap[i] = av;
+
+		float2 xv = x[i];
+		float2 rv = r[i];
+		xv.x = fmaf(a, pv.x, xv.x);
+		xv.y = fmaf(a, pv.y, xv.y);
+		rv.x = fmaf(-a, av.x, rv.x);
+		rv.y = fmaf(-a, av.y, rv.y);
+		x[i] = xv;
+		r[i] = rv;
+		acc += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
+	}
+
+	double s = block_sum(acc, sh);
+
+	if (0 == threadIdx.x)
+		rs_part[blockIdx.x] = s;
+
+	if ((0 == blockIdx.x) && (0 == threadIdx.x))
+		st->pap = pAp;
+}
+
+// FCG convergence test after step it: ||r||^2 <= eps2 stops with it + 1
+// iterations done
+__global__ void k_fcg_check(CgScalars* st, int it, const double* __restrict__ rs_part, int nrs)
+{
+	__shared__ double sh[32];
+
+	if (st->done)
+		return;
+
+	it = cg_iter(it, st);
+	double rs = sum_partials(rs_part, nrs, sh);
+
+	if (0 == threadIdx.x) {
+
+		st->rs[(it + 1) & 1] = rs;
+
+		if (rs <= st->eps2) {
+
+			st->done = 1;
+			st->iters = it + 1;
+		}
+	}
+}
+
 // End of one CG iteration inside a graph: advance the device iteration
 // counter and continue the enclosing while node unless converged or at maxiter.
 __global__ void k_cg_advance(CgScalars* st, int maxiter, cudaGraphConditionalHandle loop)

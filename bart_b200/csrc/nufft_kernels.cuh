@@ -96,6 +96,7 @@ struct CgScalars {
 	int done;		// set once converged (or p^H A p == 0)
 	int iters;		// iterations completed
 	int it;			// iteration being run (device-driven loop)
+	double pap;		// <p, (A^H A + lambda) p> of the last step (flexible CG)
 	float scale;		// data scaling used
 	float inv_scale;	// float(1 / scale)
 };
@@ -226,13 +227,16 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 template <int L, int B>
 __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_rows_fwd(const float2* __restrict__ img, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
-		int X, long YZ, long R, float2* __restrict__ out, const float2* __restrict__ twg)
+		int X, long YZ, long R, float2* __restrict__ out, const float2* __restrict__ twg, const int* done)
 {
 	using LAY = RowLayout<L, B>;
 	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
 	float2* s = smem;
 	float2* tw = smem + LAY::SMEM;
+
+	if (done && *done)
+		return;
 
 	for (int i = threadIdx.x; i < L; i += NT)
 		tw[i] = twg[i];
@@ -387,6 +391,8 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 	for (int m = 0; m < 8; m++)
 		acc[m] = make_float2(0.f, 0.f);
 
+	double dot = 0.;
+
 	for (int c = c0; c < c1; c++) {
 
 		float2 v[8];
@@ -410,17 +416,25 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 				if (ax)
 					w = cscale(w, ax[x] * ayz[yz]);
 
-				if (maps)
+				if (maps) {
+
 					acc[m] = cadd(acc[m], cmulc(w, maps[x + X * yz + X * YZ * c]));
-				else
+
+				} else {
+
 					out[x + X * yz + X * YZ * c] = w;
+
+					if (pdot) {	// Re<pdot, out> per coil
+
+						float2 pv = pdot[x + X * yz + X * YZ * c];
+						dot += (double)pv.x * (double)w.x + (double)pv.y * (double)w.y;
+					}
+				}
 			}
 		}
 	}
 
 	if (maps) {
-
-		double dot = 0.;
 
 		if (valid) {
 #pragma unroll
@@ -440,14 +454,14 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 				}
 			}
 		}
+	}
 
-		if (pdot) {
+	if (pdot) {
 
-			double t = block_sum_d(dot, red);
+		double t = block_sum_d(dot, red);
 
-			if (0 == threadIdx.x)
-				dot_part[blockIdx.x + gridDim.x * blockIdx.y] = t;
-		}
+		if (0 == threadIdx.x)
+			dot_part[blockIdx.x + gridDim.x * blockIdx.y] = t;
 	}
 }
 

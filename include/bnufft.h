@@ -117,6 +117,12 @@ struct bnufft_pics_conf {
 	int toeplitz;		/* default 1 (src/pics.c:90-91); 0 = --no-toeplitz */
 	int periodic;
 	int deterministic;
+	int precond;		/* 0: plain CG (the reference's pics); 1: flexible CG with
+				   the circulant preconditioner of the NUFFT's PSF
+				   (nufft_precond_create, src/noncart/precond.c:48-164);
+				   2: flexible CG with the circulant preconditioner plus
+				   the learned correction (bnufft_pics_set_precnet).
+				   1 and 2 need the Toeplitz normal operator. */
 };
 
 typedef struct bnufft_pics_s* bnufft_pics_t;

@@ -115,3 +115,36 @@ def test_cg_loop_graph_matches_host_loop(tol):
         assert kg < kh / 2      # the host loop launches all 200 iterations
     else:
         assert sg[0] == 12 and kg == kh + sg[0]    # plus one loop-advance kernel per iteration
+
+
+def test_fcg_circulant_converges_faster():
+    """Flexible CG with the circulant PSF preconditioner reaches the same
+    tolerance in fewer iterations than plain CG, to the same solution (the
+    FP64 oracle's), with a true normal-equation residual at the tolerance;
+    graph and host loops agree bit for bit in deterministic mode."""
+    g = golden("pics2d_n64_c4")
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    C = g["sens"].shape[3]
+    A = orc.SenseOracle(traj, g["sens"])
+    b = A.adjoint(g["ksp"].reshape(-1, C, order="F"))
+    xo, _ = orc.conjgrad(A.normal, b, 0.01, 500, tol=1e-10)
+    out = {}
+    for pc in (0, 1):
+        for mode in ("1", "0"):
+            os.environ["BNUFFT_CG_GRAPH"] = mode
+            try:
+                p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
+                         conf=PicsConf(lam=0.01, maxiter=400, tol=1e-6, scaling=1.0, precond=pc, deterministic=True))
+                x = np.asarray(p.run(g["ksp"]))
+                out[pc, mode] = (x, p.stats())
+                p.free()
+            finally:
+                os.environ.pop("BNUFFT_CG_GRAPH", None)
+    for pc in (0, 1):
+        assert np.array_equal(out[pc, "1"][0].view(np.uint32), out[pc, "0"][0].view(np.uint32))
+        assert out[pc, "1"][1] == out[pc, "0"][1]
+    it_cg, it_fcg = out[0, "1"][1][0], out[1, "1"][1][0]
+    assert it_fcg < it_cg, (it_fcg, it_cg)
+    x = out[1, "1"][0].reshape(xo.shape, order="F")
+    assert orc.normal_residual(A, x, b, 0.01) < 1e-5
+    assert rel(x, xo) < 5e-4      # the problem's float32 sensitivity (see the converged test)
