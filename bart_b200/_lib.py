@@ -64,6 +64,18 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         ctypes.POINTER(ctypes.c_float), vp)
     sig("bnufft_pics_kernels", i, vp, ctypes.POINTER(ctypes.c_long), vp)
     sig("bnufft_pics_free", None, vp)
+    sig("bnufft_pics_rhs", i, vp, vp, vp, vp)
+    sig("bnufft_pics_precond", i, vp, vp, vp, vp)
+    sig("bnufft_pics_set_precnet", i, vp, vp, vp)
+    fp = ctypes.POINTER(ctypes.c_float)
+    sig("bnufft_precnet_nparams", i)
+    sig("bnufft_precnet_create", i, ctypes.POINTER(vp), vp, vp)
+    sig("bnufft_precnet_set_params", i, vp, vp, vp)
+    sig("bnufft_precnet_get_params", i, vp, fp, vp)
+    sig("bnufft_precnet_forward", i, vp, vp, vp, ctypes.c_long, ctypes.c_long, ctypes.c_long, vp)
+    sig("bnufft_precnet_train_step", i, vp, vp, vp, ctypes.c_long, ctypes.c_long, ctypes.c_long, ctypes.c_float,
+        ctypes.POINTER(ctypes.c_double), vp, vp)
+    sig("bnufft_precnet_free", None, vp)
     sig("bnufft_last_error", ctypes.c_char_p)
     sig("bnufft_launch_count", ctypes.c_long)
     sig("bnufft_prof_start", i, ctypes.c_char_p)

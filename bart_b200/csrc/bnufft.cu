@@ -21,6 +21,7 @@
 #include "nufft_kernels.cuh"
 #include "cg_kernels.cuh"
 #include "gridding.cuh"
+#include "precnet.cuh"
 
 using namespace bn;
 
@@ -1753,6 +1754,303 @@ extern "C" int bnufft_nufft_inverse(bnufft_plan_t p, void* img, const void* ksp,
 // CG-SENSE (C ABI)
 // ----------------------------------------------------------------------------
 
+// ----------------------------------------------------------------------------
+// learned preconditioner network (C ABI: bnufft_precnet_*)
+// ----------------------------------------------------------------------------
+
+struct bnufft_precnet_s {
+
+	float* params = nullptr;	// float32 master parameters
+	float* pr = nullptr;		// working copy: weights rounded to bf16, biases float
+	bf16* wf = nullptr;		// layers 2-5 forward weights [4][32][9][32]
+	bf16* wt = nullptr;		// layers 2-5 transposed, tap-flipped [4][32][9][32]
+	float *m = nullptr, *v = nullptr, *grad = nullptr;	// Adam moments, gradient
+	int step = 0;
+	// training workspace, sized for P pixels and nblk tiles
+	long ws_P = 0, ws_nblk = 0;
+	bf16* act[5] = { nullptr, nullptr, nullptr, nullptr, nullptr };
+	bf16 *gu0 = nullptr, *gu1 = nullptr;
+	float2 *out = nullptr, *gout = nullptr;
+	float* part = nullptr;
+	double* loss_part = nullptr;
+	double* loss_host = nullptr;	// pinned
+};
+
+static const int NET_N = NetLayout::total();
+enum { NET_LOSS_BLOCKS = 256 };
+
+static int net_pack(bnufft_precnet_s* n, cudaStream_t st)
+{
+	k_net_pack<<<(NET_N + 255) / 256, 256, 0, st>>>(n->params, n->pr, n->wf, n->wt);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+static dim3 net_tiles(int X, int Y, long nimg)
+{
+	return dim3((unsigned)((X + NET_TILE_X - 1) / NET_TILE_X), (unsigned)((Y + NET_TILE_Y - 1) / NET_TILE_Y), (unsigned)nimg);
+}
+
+// Forward through all six layers: act[0..4] (layer 1-5 outputs, bf16) and
+// out = zc + scale_out * net(scale_in * in). acts may alias in pairs for
+// inference (acts[i] != acts[i - 1]).
+static int net_forward(const bnufft_precnet_s* n, const float2* in, int X, int Y, long nimg, bf16* const acts[5],
+		const float* scale_in, const float* scale_out, const float2* zc, float2* out, const float2* pdot,
+		double* dot_part, int* nblocks, const int* done, const int* net_off, cudaStream_t st)
+{
+	const long P = (long)X * Y * nimg;
+	const unsigned pb = (unsigned)((P + NET_THREADS - 1) / NET_THREADS);
+	const float* pr = n->pr;
+
+	k_net_in<<<pb, NET_THREADS, 0, st>>>(in, X, Y, P, pr + NetLayout::woff(0), pr + NetLayout::boff(0), scale_in, acts[0], done);
+	LAUNCHED();
+
+	for (int l = 1; l <= 4; l++) {
+
+		TRY(prep_kernel(k_conv32<0>, NET_CONV_SMEM));
+		k_conv32<0><<<net_tiles(X, Y, nimg), NET_THREADS, NET_CONV_SMEM, st>>>(acts[l - 1], n->wf + (l - 1) * 9216,
+				pr + NetLayout::boff(l), nullptr, acts[l], X, Y, done);
+		LAUNCHED();
+	}
+
+	k_net_out<<<pb, NET_THREADS, 0, st>>>(acts[4], X, Y, P, pr + NetLayout::woff(5), pr + NetLayout::boff(5), scale_out, zc,
+			out, pdot, dot_part, done, net_off);
+	LAUNCHED();
+
+	if (nblocks)
+		*nblocks = (int)pb;
+
+	return BNUFFT_OK;
+}
+
+static void net_free_ws(bnufft_precnet_s* n)
+{
+	void* bufs[] = { n->act[0], n->act[1], n->act[2], n->act[3], n->act[4], n->gu0, n->gu1, n->out, n->gout, n->part,
+			 n->loss_part };
+
+	for (void* b : bufs)
+		if (b)
+			cudaFree(b);
+
+	for (auto& a : n->act)
+		a = nullptr;
+
+	n->gu0 = n->gu1 = nullptr;
+	n->out = n->gout = nullptr;
+	n->part = nullptr;
+	n->loss_part = nullptr;
+	n->ws_P = n->ws_nblk = 0;
+}
+
+static int net_ensure_ws(bnufft_precnet_s* n, long P, long nblk)
+{
+	if ((P <= n->ws_P) && (nblk <= n->ws_nblk))
+		return BNUFFT_OK;
+
+	CUDA_TRY(cudaDeviceSynchronize());	// buffers may be in use by earlier steps
+	net_free_ws(n);
+	size_t ab = sizeof(bf16) * NET_C * P;
+
+	for (auto& a : n->act)
+		CUDA_TRY(cudaMalloc(&a, ab));
+
+	CUDA_TRY(cudaMalloc(&n->gu0, ab));
+	CUDA_TRY(cudaMalloc(&n->gu1, ab));
+	CUDA_TRY(cudaMalloc(&n->out, sizeof(float2) * P));
+	CUDA_TRY(cudaMalloc(&n->gout, sizeof(float2) * P));
+	CUDA_TRY(cudaMalloc(&n->part, sizeof(float) * nblk * NetLayout::size(1)));
+	CUDA_TRY(cudaMalloc(&n->loss_part, sizeof(double) * NET_LOSS_BLOCKS));
+	n->ws_P = P;
+	n->ws_nblk = nblk;
+	return BNUFFT_OK;
+}
+
+// weight and bias gradients of layer l into grad
+template <int CIN, int COUT, typename AT, typename GT>
+static int net_wgrad(bnufft_precnet_s* n, int l, const AT* a, const GT* g, int X, int Y, long nimg, cudaStream_t st)
+{
+	size_t smem = sizeof(float) * (NET_HALO_Y * NET_HALO_X * CIN + NET_TILE_Y * NET_TILE_X * COUT);
+	dim3 grid = net_tiles(X, Y, nimg);
+	long nblk = (long)grid.x * grid.y * grid.z;
+	const int O = COUT * 9 * CIN + COUT;
+	TRY(prep_kernel(k_wgrad<CIN, COUT, AT, GT>, smem));
+	k_wgrad<CIN, COUT, AT, GT><<<grid, NET_THREADS, smem, st>>>(a, g, X, Y, n->part);
+	LAUNCHED();
+	k_wgrad_reduce<<<(O + 255) / 256, 256, 0, st>>>(n->part, nblk, O, n->grad + NetLayout::woff(l));
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_precnet_nparams(void) { return NET_N; }
+
+extern "C" int bnufft_precnet_set_params(bnufft_precnet_t n, const float* params, void* stream)
+{
+	cudaStream_t st = S(stream);
+	CUDA_TRY(cudaMemcpyAsync(n->params, params, sizeof(float) * NET_N, cudaMemcpyDefault, st));
+	CUDA_TRY(cudaMemsetAsync(n->m, 0, sizeof(float) * NET_N, st));
+	CUDA_TRY(cudaMemsetAsync(n->v, 0, sizeof(float) * NET_N, st));
+	n->step = 0;
+	return net_pack(n, st);
+}
+
+extern "C" int bnufft_precnet_get_params(bnufft_precnet_t n, float* params, void* stream)
+{
+	cudaStream_t st = S(stream);
+	CUDA_TRY(cudaMemcpyAsync(params, n->params, sizeof(float) * NET_N, cudaMemcpyDefault, st));
+	CUDA_TRY(cudaStreamSynchronize(st));
+	return BNUFFT_OK;
+}
+
+extern "C" void bnufft_precnet_free(bnufft_precnet_t n)
+{
+	if (!n)
+		return;
+
+	cudaDeviceSynchronize();
+	net_free_ws(n);
+	void* bufs[] = { n->params, n->pr, n->wf, n->wt, n->m, n->v, n->grad };
+
+	for (void* b : bufs)
+		if (b)
+			cudaFree(b);
+
+	if (n->loss_host)
+		cudaFreeHost(n->loss_host);
+
+	delete n;
+}
+
+extern "C" int bnufft_precnet_create(bnufft_precnet_t* out, const float* params, void* stream)
+{
+	if (!out || !params)
+		return fail(BNUFFT_ERR_ARG, "null argument");
+
+	auto n = new bnufft_precnet_s();
+	cudaError_t e = cudaSuccess;
+	auto al = [&](void** p, size_t b) { if (cudaSuccess == e) e = cudaMalloc(p, b); };
+	al((void**)&n->params, sizeof(float) * NET_N);
+	al((void**)&n->pr, sizeof(float) * NET_N);
+	al((void**)&n->m, sizeof(float) * NET_N);
+	al((void**)&n->v, sizeof(float) * NET_N);
+	al((void**)&n->grad, sizeof(float) * NET_N);
+	al((void**)&n->wf, sizeof(bf16) * 4 * 9216);
+	al((void**)&n->wt, sizeof(bf16) * 4 * 9216);
+
+	if (cudaSuccess == e)
+		e = cudaMallocHost((void**)&n->loss_host, sizeof(double) * NET_LOSS_BLOCKS);
+
+	if (cudaSuccess != e) {
+
+		bnufft_precnet_free(n);
+		return fail(BNUFFT_ERR_NOMEM, "precnet buffers: %s", cudaGetErrorString(e));
+	}
+
+	int s = bnufft_precnet_set_params(n, params, stream);
+
+	if (BNUFFT_OK != s) {
+
+		bnufft_precnet_free(n);
+		return s;
+	}
+
+	*out = n;
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_precnet_forward(bnufft_precnet_t n, void* out, const void* in, long X, long Y, long nimg, void* stream)
+{
+	cudaStream_t st = S(stream);
+
+	if (!n || (X < 1) || (Y < 1) || (nimg < 1) || (X > (1 << 20)) || (Y > 65535 * NET_TILE_Y) || (nimg > 65535))
+		return fail(BNUFFT_ERR_ARG, "bad precnet image size");
+
+	const long P = X * Y * nimg;
+	dim3 grid = net_tiles((int)X, (int)Y, nimg);
+	TRY(net_ensure_ws(n, P, (long)grid.x * grid.y * grid.z));
+	size_t b = sizeof(float2) * P;
+	Staged i, o;
+	TRY(stage_in(i, in, b, st));
+	TRY(stage_out_alloc(o, out, b, st));
+	TRY(net_forward(n, (const float2*)i.dev, (int)X, (int)Y, nimg, n->act, nullptr, nullptr, nullptr, (float2*)o.dev,
+			nullptr, nullptr, nullptr, nullptr, nullptr, st));
+	return stage_out_copy(o, out, b, st);
+}
+
+extern "C" int bnufft_precnet_train_step(bnufft_precnet_t n, const void* in, const void* target, long X, long Y,
+		long nimg, float lr, double* loss, float* grads, void* stream)
+{
+	cudaStream_t st = S(stream);
+
+	if (!n || (X < 1) || (Y < 1) || (nimg < 1) || (X > (1 << 20)) || (Y > 65535 * NET_TILE_Y) || (nimg > 65535))
+		return fail(BNUFFT_ERR_ARG, "bad precnet image size");
+
+	const long P = X * Y * nimg;
+	const int x = (int)X, y = (int)Y;
+	dim3 grid = net_tiles(x, y, nimg);
+	TRY(net_ensure_ws(n, P, (long)grid.x * grid.y * grid.z));
+	size_t b = sizeof(float2) * P;
+	Staged si, stg;
+	TRY(stage_in(si, in, b, st));
+	TRY(stage_in(stg, target, b, st));
+	const float2* inp = (const float2*)si.dev;
+	const unsigned pb = (unsigned)((P + NET_THREADS - 1) / NET_THREADS);
+
+	// forward, keeping every layer's activation
+	TRY(net_forward(n, inp, x, y, nimg, n->act, nullptr, nullptr, nullptr, n->out, nullptr, nullptr, nullptr, nullptr,
+			nullptr, st));
+
+	// loss = (1 / nimg) sum |out - target|^2, gout = dloss / dout
+	k_net_loss<<<NET_LOSS_BLOCKS, 256, 0, st>>>(n->out, (const float2*)stg.dev, P, 2.f / (float)nimg, n->gout, n->loss_part);
+	LAUNCHED();
+
+	// backward: layer 6, then 5..2 on the tensor cores, then layer 1
+	TRY((net_wgrad<NET_C, 2, bf16, float>(n, 5, n->act[4], (const float*)n->gout, x, y, nimg, st)));
+	k_net_out_bwd<<<pb, NET_THREADS, 0, st>>>(n->gout, n->act[4], x, y, P, n->pr + NetLayout::woff(5), n->gu0);
+	LAUNCHED();
+	bf16* gu = n->gu0;
+	bf16* gn = n->gu1;
+
+	for (int l = 4; l >= 1; l--) {
+
+		TRY((net_wgrad<NET_C, NET_C, bf16, bf16>(n, l, n->act[l - 1], gu, x, y, nimg, st)));
+		TRY(prep_kernel(k_conv32<1>, NET_CONV_SMEM));
+		k_conv32<1><<<grid, NET_THREADS, NET_CONV_SMEM, st>>>(gu, n->wt + (l - 1) * 9216, nullptr, n->act[l - 1], gn,
+				x, y, nullptr);
+		LAUNCHED();
+		std::swap(gu, gn);
+	}
+
+	TRY((net_wgrad<2, NET_C, float, bf16>(n, 0, (const float*)inp, gu, x, y, nimg, st)));
+
+	if (grads)
+		CUDA_TRY(cudaMemcpyAsync(grads, n->grad, sizeof(float) * NET_N, cudaMemcpyDefault, st));
+
+	if (lr > 0.f) {
+
+		n->step++;
+		const float b1 = 0.9f, b2 = 0.999f;
+		float c1 = (float)(1. / (1. - pow((double)b1, n->step)));
+		float c2 = (float)(1. / (1. - pow((double)b2, n->step)));
+		k_adam<<<(NET_N + 255) / 256, 256, 0, st>>>(n->params, n->grad, n->m, n->v, NET_N, lr, b1, b2, 1e-8f, c1, c2);
+		LAUNCHED();
+		TRY(net_pack(n, st));
+	}
+
+	if (loss) {
+
+		CUDA_TRY(cudaMemcpyAsync(n->loss_host, n->loss_part, sizeof(double) * NET_LOSS_BLOCKS, cudaMemcpyDeviceToHost, st));
+		CUDA_TRY(cudaStreamSynchronize(st));
+		double acc = 0.;
+
+		for (int i = 0; i < NET_LOSS_BLOCKS; i++)
+			acc += n->loss_host[i];
+
+		*loss = acc / (double)nimg;
+	}
+
+	return BNUFFT_OK;
+}
+
 struct bnufft_pics_s {
 
 	bnufft_plan_t nufft;
@@ -1776,6 +2074,8 @@ struct bnufft_pics_s {
 	double* zap_part = nullptr;	// <A p_prev, z>, one per preconditioner row-pass block
 	double* pr_part = nullptr;	// <p, r>, one per direction-update block
 	int nzap = 0;
+	bnufft_precnet_t net = nullptr;	// learned correction (conf.precond == 2), not owned
+	bf16* nact[2] = { nullptr, nullptr };	// its activations, ping-pong [npix][32]
 	long max_row_blocks;
 	int nparts;
 	CgScalars* scal = nullptr;
@@ -1951,6 +2251,36 @@ extern "C" int bnufft_pics_normal(bnufft_pics_t ps, void* dst, const void* src, 
 	return stage_out_copy(o, dst, b, st);
 }
 
+// b = A^H y / scale into ps->b: adjoint (coil-sum partials, then combine) and
+// the data scaling of src/pics.c:499-530 (y /= scale  <=>  A^H y /= scale)
+static int pics_prologue(bnufft_pics_s* ps, const float2* ksp, cudaStream_t st)
+{
+	OpCtx& op = ps->nufft->op;
+	unsigned nb = (unsigned)ps->nparts;
+	TRY(op_adjoint(op, ksp, ps->sens, ps->C, ps->cpg, ps->part, st));
+	k_combine<<<nb, RED_THREADS, 0, st>>>(ps->b, ps->part, ps->groups, ps->npix, nullptr, 0.f, nullptr, nullptr);
+	LAUNCHED();
+
+	if (0.f == ps->conf.scaling) {
+
+		k_abs<<<nb, RED_THREADS, 0, st>>>(ps->mag, ps->b, ps->npix);
+		LAUNCHED();
+		CUDA_TRY(cub::DeviceRadixSort::SortKeys(ps->sort_tmp, ps->sort_tmp_bytes, ps->mag, ps->mag_sorted, (int)ps->npix, 0, 32, st));
+		g_launches.fetch_add(1, std::memory_order_relaxed);
+		k_scaling_from_sorted<<<1, 1, 0, st>>>(ps->mag_sorted, ps->npix, ps->scal);
+		LAUNCHED();
+
+	} else {
+
+		k_set_scaling<<<1, 1, 0, st>>>(ps->scal, ps->conf.scaling);
+		LAUNCHED();
+	}
+
+	k_scale_dev<<<nb, RED_THREADS, 0, st>>>(ps->b, ps->b, ps->npix, &ps->scal->inv_scale);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
 // One CG iteration on (A^H A + lambda) x = b in four passes: the direction
 // update fused into the first row pass, the normal operator's column passes,
 // the final row pass with the p^H A p partials, and the x / r step with the
@@ -1998,9 +2328,32 @@ static int pics_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	return BNUFFT_OK;
 }
 
-// z = M(r): the circulant preconditioner applied to one image (N-point
-// transforms, no padding); optional partials Re<pdot, z>
+static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
+		int* nblocks, cudaStream_t st);
+
+// z = M(r): the circulant preconditioner, plus (precond 2) the learned
+// correction ||r|| net(r / ||r||) with ||r|| from the solve's scalars;
+// optional partials Re<pdot, z>
 static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
+		int* nblocks, cudaStream_t st)
+{
+	if (2 != ps->conf.precond)
+		return pics_precond_circ(ps, r, z, pdot, dot_part, nblocks, st);
+
+	if (!ps->net)
+		return fail(BNUFFT_ERR_ARG, "precond 2 needs a network (bnufft_pics_set_precnet)");
+
+	TRY(pics_precond_circ(ps, r, z, nullptr, nullptr, nullptr, st));
+	const Geom& g = ps->nufft->op.g;
+	bf16* acts[5] = { ps->nact[0], ps->nact[1], ps->nact[0], ps->nact[1], ps->nact[0] };
+	CgScalars* sc = ps->scal;
+	return net_forward(ps->net, r, g.N[0], g.N[1], 1, acts, &sc->rinv, &sc->rnorm, z, z, pdot, dot_part, nblocks,
+			&sc->done, &sc->net_off, st);
+}
+
+// the circulant preconditioner applied to one image (N-point transforms, no
+// padding)
+static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
 		int* nblocks, cudaStream_t st)
 {
 	bnufft_plan_s* p = ps->nufft;
@@ -2140,30 +2493,7 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 	unsigned nb = (unsigned)ps->nparts;
 	long launches0 = g_launches.load();
 	ps->last_graph = false;
-
-	// adjoint of the data: A^H y (coil-sum partials, then combine)
-	TRY(op_adjoint(op, (const float2*)ki.dev, ps->sens, ps->C, ps->cpg, ps->part, st));
-	k_combine<<<nb, RED_THREADS, 0, st>>>(ps->b, ps->part, ps->groups, ps->npix, nullptr, 0.f, nullptr, nullptr);
-	LAUNCHED();
-
-	// data scaling (src/pics.c:499-530): y /= scale  <=>  A^H y /= scale
-	if (0.f == ps->conf.scaling) {
-
-		k_abs<<<nb, RED_THREADS, 0, st>>>(ps->mag, ps->b, ps->npix);
-		LAUNCHED();
-		CUDA_TRY(cub::DeviceRadixSort::SortKeys(ps->sort_tmp, ps->sort_tmp_bytes, ps->mag, ps->mag_sorted, (int)ps->npix, 0, 32, st));
-		g_launches.fetch_add(1, std::memory_order_relaxed);
-		k_scaling_from_sorted<<<1, 1, 0, st>>>(ps->mag_sorted, ps->npix, ps->scal);
-		LAUNCHED();
-
-	} else {
-
-		k_set_scaling<<<1, 1, 0, st>>>(ps->scal, ps->conf.scaling);
-		LAUNCHED();
-	}
-
-	k_scale_dev<<<nb, RED_THREADS, 0, st>>>(ps->b, ps->b, ps->npix, &ps->scal->inv_scale);
-	LAUNCHED();
+	TRY(pics_prologue(ps, (const float2*)ki.dev, st));
 
 	// CG from zero (conjgrad, src/iter/italgos.c:497-572)
 	k_cg_init<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, ps->pbuf[1], ps->b, ps->npix, ps->rs_part);
@@ -2214,6 +2544,59 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 	return stage_out_copy(io, img, ib, st);
 }
 
+extern "C" int bnufft_pics_set_precnet(bnufft_pics_t ps, bnufft_precnet_t net, void* stream)
+{
+	cudaStream_t st = S(stream);
+
+	if (!ps || (2 != ps->conf.precond))
+		return fail(BNUFFT_ERR_ARG, "the model was not created with precond 2");
+
+	if (ps->nufft->op.g.N[2] > 1)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "the learned preconditioner is 2D");
+
+	ps->net = net;
+
+	for (auto& a : ps->nact)
+		if (!a)
+			CUDA_TRY(cudaMallocAsync(&a, sizeof(bf16) * NET_C * ps->npix, st));
+
+	return BNUFFT_OK;
+}
+
+// b = A^H y / scale (the right-hand side the solve uses)
+extern "C" int bnufft_pics_rhs(bnufft_pics_t ps, void* b, const void* ksp, void* stream)
+{
+	cudaStream_t st = S(stream);
+	size_t kb = sizeof(float2) * ps->M * ps->C;
+	size_t ib = sizeof(float2) * ps->npix;
+	Staged ki, bo;
+	TRY(stage_in(ki, ksp, kb, st));
+	TRY(stage_out_alloc(bo, b, ib, st));
+	TRY(pics_prologue(ps, (const float2*)ki.dev, st));
+	CUDA_TRY(cudaMemcpyAsync(bo.dev, ps->b, ib, cudaMemcpyDeviceToDevice, st));
+	return stage_out_copy(bo, b, ib, st);
+}
+
+// z = M(r) with the model's preconditioner (precond 1 or 2)
+extern "C" int bnufft_pics_precond(bnufft_pics_t ps, void* z, const void* r, void* stream)
+{
+	cudaStream_t st = S(stream);
+
+	if (!ps->conf.precond)
+		return fail(BNUFFT_ERR_ARG, "the model has no preconditioner");
+
+	size_t ib = sizeof(float2) * ps->npix;
+	Staged ri, zo;
+	TRY(stage_in(ri, r, ib, st));
+	TRY(stage_out_alloc(zo, z, ib, st));
+	OpCtx& op = ps->nufft->op;
+	TRY(alloc_work(op.w, op.g, ps->C, st));
+	k_norm_scalars<<<1, RED_THREADS, 0, st>>>((const float2*)ri.dev, ps->npix, ps->scal);
+	LAUNCHED();
+	TRY(pics_precond(ps, (const float2*)ri.dev, (float2*)zo.dev, nullptr, nullptr, nullptr, st));
+	return stage_out_copy(zo, z, ib, st);
+}
+
 extern "C" int bnufft_pics_kernels(bnufft_pics_t ps, long* kernels, void* stream)
 {
 	CgScalars h;
@@ -2259,7 +2642,7 @@ extern "C" void bnufft_pics_free(bnufft_pics_t ps)
 
 	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->pbuf[0], ps->pbuf[1], ps->b, ps->kbuf, ps->mag, ps->mag_sorted,
 			 ps->sort_tmp, ps->pap_part, ps->pp_part, ps->rs_part, ps->scal, ps->z, ps->Ap, ps->zap_part,
-			 ps->pr_part };
+			 ps->pr_part, ps->nact[0], ps->nact[1] };
 
 	for (void* b : bufs)
 		if (b)

@@ -125,6 +125,11 @@ __global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float 
 		st->iters = 0;
 		st->it = 0;
 		st->done = (0. == b2);
+		st->best_rs = b2;
+		st->best_it = 0;
+		st->net_off = 0;
+		st->rnorm = (float)sqrt(b2);
+		st->rinv = (b2 > 0.) ? (float)(1. / sqrt(b2)) : 0.f;
 	}
 }
 
@@ -368,12 +373,47 @@ __global__ void k_fcg_check(CgScalars* st, int it, const double* __restrict__ rs
 	if (0 == threadIdx.x) {
 
 		st->rs[(it + 1) & 1] = rs;
+		st->rnorm = (float)sqrt(rs);
+		st->rinv = (rs > 0.) ? (float)(1. / sqrt(rs)) : 0.f;
 
 		if (rs <= st->eps2) {
 
 			st->done = 1;
 			st->iters = it + 1;
 		}
+
+		// stall: no new smallest residual for 3 iterations switches the
+		// learned part of the preconditioner off for the rest of the solve
+		if (rs < st->best_rs) {
+
+			st->best_rs = rs;
+			st->best_it = it + 1;
+
+		} else if (it + 1 - st->best_it >= 3) {
+
+			st->net_off = 1;
+		}
+	}
+}
+
+// ||v|| into the scalars (rnorm, rinv) for a preconditioner applied outside
+// a solve; clears done and the stall flag
+__global__ void k_norm_scalars(const float2* __restrict__ v, long n, CgScalars* st)
+{
+	__shared__ double sh[32];
+	double acc = 0.;
+
+	for (long i = threadIdx.x; i < n; i += blockDim.x)
+		acc += (double)v[i].x * v[i].x + (double)v[i].y * v[i].y;
+
+	double s = block_sum(acc, sh);
+
+	if (0 == threadIdx.x) {
+
+		st->rnorm = (float)sqrt(s);
+		st->rinv = (s > 0.) ? (float)(1. / sqrt(s)) : 0.f;
+		st->done = 0;
+		st->net_off = 0;
 	}
 }
 

@@ -97,6 +97,11 @@ struct CgScalars {
 	int iters;		// iterations completed
 	int it;			// iteration being run (device-driven loop)
 	double pap;		// <p, (A^H A + lambda) p> of the last step (flexible CG)
+	double best_rs;		// smallest ||r||^2 so far (flexible CG stall test)
+	int best_it;		// iteration count at best_rs
+	int net_off;		// learned preconditioner switched off (stall fallback)
+	float rnorm;		// ||r|| of the current residual
+	float rinv;		// 1 / ||r|| (0 for r = 0)
 	float scale;		// data scaling used
 	float inv_scale;	// float(1 / scale)
 };

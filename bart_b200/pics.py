@@ -87,6 +87,32 @@ class Pics:
                                                  ctypes.byref(sc), stream))
         return it.value, res.value, sc.value
 
+    def rhs(self, ksp, out=None):
+        """b = A^H y / scale, the right-hand side of the solve."""
+        n_in = int(np.prod(self.ksp_dims))
+        n_out = int(np.prod(self.img_dims))
+        if out is None:
+            out = _alloc_like(ksp, self.img_dims)
+        pk, keep = _ptr_in(ksp, n_in)
+        _lib.check(_lib.load().bnufft_pics_rhs(self._h, _ptr_out(out, n_out), pk, _stream_of(ksp, out)))
+        del keep
+        return out
+
+    def precond(self, r, out=None):
+        """z = M(r) with the model's preconditioner (precond 1 or 2)."""
+        n = int(np.prod(self.img_dims))
+        if out is None:
+            out = _alloc_like(r, self.img_dims)
+        pr, keep = _ptr_in(r, n)
+        _lib.check(_lib.load().bnufft_pics_precond(self._h, _ptr_out(out, n), pr, _stream_of(r, out)))
+        del keep
+        return out
+
+    def set_precnet(self, net):
+        """Attach a learned preconditioner (a PrecNet) to a precond=2 model."""
+        _lib.check(_lib.load().bnufft_pics_set_precnet(self._h, net.handle, None))
+        self._net = net     # keep it alive while attached
+
     def kernels(self, stream=None):
         """Kernels the last run executed on the device (host launches plus the
         CG loop graph's body once per iteration it ran)."""

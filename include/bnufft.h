@@ -157,6 +157,42 @@ int bnufft_pics_kernels(bnufft_pics_t pics, long* kernels, void* stream);
 
 void bnufft_pics_free(bnufft_pics_t pics);
 
+/* b = A^H y / scale, the right-hand side the solve uses (scaling as in
+ * bnufft_pics_run). img-sized output. */
+int bnufft_pics_rhs(bnufft_pics_t pics, void* b, const void* ksp, void* stream);
+
+/* z = M(r), the model's preconditioner (precond 1 or 2) on one image. */
+int bnufft_pics_precond(bnufft_pics_t pics, void* z, const void* r, void* stream);
+
+/* Learned preconditioner (no counterpart in the reference; the reference's
+ * plug-in point is the preconditioner operator of lsqr2_create,
+ * src/iter/lsqr.c:126-143). A 6-layer 3x3 convolutional network,
+ * 2 -> 32 -> 32 -> 32 -> 32 -> 32 -> 2 channels (complex image as 2
+ * channels), ReLU after layers 1-5, bf16 weights and activations, float32
+ * accumulation. Parameters: float32, per layer W[cout][3 ky + kx][cin] then
+ * b[cout]; bnufft_precnet_nparams() values in all. Used by flexible CG as
+ * z = M_circ(r) + ||r|| net(r / ||r||). */
+typedef struct bnufft_precnet_s* bnufft_precnet_t;
+
+int bnufft_precnet_nparams(void);
+int bnufft_precnet_create(bnufft_precnet_t* net, const float* params, void* stream);
+int bnufft_precnet_set_params(bnufft_precnet_t net, const float* params, void* stream);
+int bnufft_precnet_get_params(bnufft_precnet_t net, float* params, void* stream);
+
+/* out = net(in) for nimg complex images [X, Y] (no scaling). */
+int bnufft_precnet_forward(bnufft_precnet_t net, void* out, const void* in, long X, long Y, long nimg, void* stream);
+
+/* One training step on a batch: loss = (1/nimg) sum |net(in) - target|^2,
+ * its gradient (copied to grads if not null), then an Adam step with
+ * learning rate lr (none if lr <= 0). loss (if not null) synchronises. */
+int bnufft_precnet_train_step(bnufft_precnet_t net, const void* in, const void* target, long X, long Y, long nimg,
+		float lr, double* loss, float* grads, void* stream);
+
+void bnufft_precnet_free(bnufft_precnet_t net);
+
+/* Attach a network to a model created with precond 2 (not owned). */
+int bnufft_pics_set_precnet(bnufft_pics_t pics, bnufft_precnet_t net, void* stream);
+
 /* Message of the last failure on this thread ("" if none). */
 const char* bnufft_last_error(void);
 

@@ -1,0 +1,135 @@
+"""GPU learned preconditioner: the network's forward pass and gradients
+through the C ABI against the CPU oracle, Adam training, and its use inside
+flexible CG."""
+
+import os
+
+import numpy as np
+import pytest
+
+from bart_b200 import precnet
+from bart_b200.pics import Pics, PicsConf
+from conftest import golden, rel
+from oracle import nufft_oracle as orc
+from oracle import precnet_oracle as po
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(rng, last=0.1):
+    p = po.init_params(rng)
+    wo = po.offsets()[5][0]
+    p[wo:] = (rng.standard_normal(po.NPARAMS - wo) * last).astype(np.float32)
+    for (_, bo, e) in po.offsets():
+        p[bo:e] = (rng.standard_normal(e - bo) * 0.05).astype(np.float32)
+    return p
+
+
+def _img(rng, X, Y, n):
+    return (rng.standard_normal((X, Y, n)) + 1j * rng.standard_normal((X, Y, n))).astype(np.complex64, order="F")
+
+
+@pytest.mark.parametrize("X,Y,n", [(40, 24, 2), (64, 64, 1), (33, 17, 3)])
+def test_forward_vs_oracle(X, Y, n):
+    rng = np.random.default_rng(X + Y)
+    p = _params(rng)
+    x = _img(rng, X, Y, n)
+    net = precnet.PrecNet(p)
+    out = np.asarray(net.forward(x, X, Y, n)).reshape(X, Y, n, order="F")
+    net.free()
+    ref, _ = po.forward(p, po.to_channels(x), bf16_mode=True)
+    assert rel(out, po.from_channels(ref)) < 3e-3
+
+
+def test_gradients_vs_oracle():
+    rng = np.random.default_rng(5)
+    X, Y, n = 40, 24, 2
+    p = _params(rng)
+    x, t = _img(rng, X, Y, n), _img(rng, X, Y, n)
+    net = precnet.PrecNet(p)
+    g = np.zeros(po.NPARAMS, dtype=np.float32)
+    loss = net.train_step(x, t, X, Y, n, 0.0, grads=g)
+    assert np.array_equal(net.params(), p)      # lr 0: no update
+    net.free()
+    lo, go = po.loss_and_grad(p, po.to_channels(x), po.to_channels(t), bf16_mode=True)
+    assert abs(loss - lo) <= 1e-4 * lo
+    for li, (wo, bo, e) in enumerate(po.offsets()):
+        assert rel(g[wo:bo], go[wo:bo]) < 1e-2, li
+        assert rel(g[bo:e], go[bo:e]) < 1e-2, li
+
+
+def test_gradients_bit_reproducible():
+    rng = np.random.default_rng(6)
+    p = _params(rng)
+    x, t = _img(rng, 64, 32, 2), _img(rng, 64, 32, 2)
+    net = precnet.PrecNet(p)
+    g1 = np.zeros(po.NPARAMS, dtype=np.float32)
+    g2 = np.zeros(po.NPARAMS, dtype=np.float32)
+    net.train_step(x, t, 64, 32, 2, 0.0, grads=g1)
+    net.train_step(x, t, 64, 32, 2, 0.0, grads=g2)
+    net.free()
+    assert np.array_equal(g1.view(np.uint32), g2.view(np.uint32))
+
+
+def test_adam_training_reduces_loss():
+    """Fit a fixed linear map (a 3x3 smoothing of the input) on one batch."""
+    rng = np.random.default_rng(7)
+    X, Y, n = 32, 32, 4
+    x = _img(rng, X, Y, n)
+    k = np.array([[1, 2, 1], [2, 4, 2], [1, 2, 1]], dtype=np.float32) / 16
+    xp = np.pad(x, ((1, 1), (1, 1), (0, 0)))
+    t = sum(k[i, j] * xp[i:i + X, j:j + Y] for i in range(3) for j in range(3)).astype(np.complex64, order="F")
+    net = precnet.PrecNet(precnet.init_params(1))
+    l0 = net.train_step(x, t, X, Y, n, 0.0)
+    for _ in range(200):
+        net.train_step(x, t, X, Y, n, 3e-3, want_loss=False)
+    l1 = net.train_step(x, t, X, Y, n, 0.0)
+    net.free()
+    assert l1 < 0.2 * l0, (l0, l1)
+
+
+def test_learned_fcg_zero_network_equals_circulant():
+    """An all-zero last layer adds nothing: precond 2 iterates exactly like
+    precond 1 (bit-identical in deterministic mode)."""
+    g = golden("pics2d_n64_c4")
+    net = precnet.PrecNet(precnet.init_params(3))
+    out = {}
+    for pc in (1, 2):
+        p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
+                 conf=PicsConf(lam=0.01, maxiter=100, tol=1e-5, scaling=1.0, precond=pc, deterministic=True))
+        if pc == 2:
+            p.set_precnet(net)
+        out[pc] = (np.asarray(p.run(g["ksp"])), p.stats())
+        p.free()
+    net.free()
+    assert np.array_equal(out[1][0].view(np.uint32), out[2][0].view(np.uint32))
+    assert out[1][1] == out[2][1]
+
+
+def test_learned_fcg_random_network_still_converges():
+    """A random (untrained) correction can only slow the solve down; the
+    stall fallback and the flexible CG still reach the FP64 solution."""
+    g = golden("pics2d_n64_c4")
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    C = g["sens"].shape[3]
+    A = orc.SenseOracle(traj, g["sens"])
+    b = A.adjoint(g["ksp"].reshape(-1, C, order="F"))
+    xo, _ = orc.conjgrad(A.normal, b, 0.01, 500, tol=1e-10)
+    net = precnet.PrecNet(_params(np.random.default_rng(9), last=0.02))
+    res = {}
+    for mode in ("1", "0"):
+        os.environ["BNUFFT_CG_GRAPH"] = mode
+        try:
+            p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
+                     conf=PicsConf(lam=0.01, maxiter=400, tol=1e-6, scaling=1.0, precond=2, deterministic=True))
+            p.set_precnet(net)
+            res[mode] = (np.asarray(p.run(g["ksp"])), p.stats())
+            p.free()
+        finally:
+            os.environ.pop("BNUFFT_CG_GRAPH", None)
+    net.free()
+    assert np.array_equal(res["1"][0].view(np.uint32), res["0"][0].view(np.uint32))
+    x = res["1"][0].reshape(xo.shape, order="F")
+    assert res["1"][1][1] <= 1e-6
+    assert orc.normal_residual(A, x, b, 0.01) < 1e-5
+    assert rel(x, xo) < 5e-4
