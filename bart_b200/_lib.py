@@ -65,6 +65,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     sig("bnufft_pics_kernels", i, vp, ctypes.POINTER(ctypes.c_long), vp)
     sig("bnufft_pics_free", None, vp)
     sig("bnufft_pics_rhs", i, vp, vp, vp, vp)
+    sig("bnufft_pics_set_iter", i, vp, i, ctypes.c_float)
     sig("bnufft_pics_precond", i, vp, vp, vp, vp)
     sig("bnufft_pics_set_precnet", i, vp, vp, vp)
     fp = ctypes.POINTER(ctypes.c_float)
@@ -75,6 +76,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     sig("bnufft_precnet_forward", i, vp, vp, vp, ctypes.c_long, ctypes.c_long, ctypes.c_long, vp)
     sig("bnufft_precnet_train_step", i, vp, vp, vp, ctypes.c_long, ctypes.c_long, ctypes.c_long, ctypes.c_float,
         ctypes.POINTER(ctypes.c_double), vp, vp)
+    sig("bnufft_precnet_backward", i, vp, vp, vp, ctypes.c_long, ctypes.c_long, ctypes.c_long, ctypes.c_float, vp, vp)
     sig("bnufft_precnet_free", None, vp)
     sig("bnufft_last_error", ctypes.c_char_p)
     sig("bnufft_launch_count", ctypes.c_long)

@@ -1709,7 +1709,7 @@ extern "C" int bnufft_nufft_inverse(bnufft_plan_t p, void* img, const void* ksp,
 
 	k_cg_init<<<nb, RED_THREADS, 0, st>>>(x, r, pv, Ap, n, rsp);
 	LAUNCHED();
-	k_cg_start<<<1, RED_THREADS, 0, st>>>(sc, rsp, (int)nb, 0.f);
+	k_cg_start<<<1, RED_THREADS, 0, st>>>(sc, rsp, (int)nb, 0.f, maxiter);
 	LAUNCHED();
 
 	for (int it = 0; it < maxiter; it++) {
@@ -1795,8 +1795,9 @@ static dim3 net_tiles(int X, int Y, long nimg)
 // out = zc + scale_out * net(scale_in * in). acts may alias in pairs for
 // inference (acts[i] != acts[i - 1]).
 static int net_forward(const bnufft_precnet_s* n, const float2* in, int X, int Y, long nimg, bf16* const acts[5],
-		const float* scale_in, const float* scale_out, const float2* zc, float2* out, const float2* pdot,
-		double* dot_part, int* nblocks, const int* done, const int* net_off, cudaStream_t st)
+		const float* scale_in, const float* scale_out, const double* norm_part, int nnorm, const float2* zc,
+		float2* out, const float2* pdot, double* dot_part, int* nblocks, const int* done, const int* net_off,
+		cudaStream_t st)
 {
 	const long P = (long)X * Y * nimg;
 	const unsigned pb = (unsigned)((P + NET_THREADS - 1) / NET_THREADS);
@@ -1813,8 +1814,8 @@ static int net_forward(const bnufft_precnet_s* n, const float2* in, int X, int Y
 		LAUNCHED();
 	}
 
-	k_net_out<<<pb, NET_THREADS, 0, st>>>(acts[4], X, Y, P, pr + NetLayout::woff(5), pr + NetLayout::boff(5), scale_out, zc,
-			out, pdot, dot_part, done, net_off);
+	k_net_out<<<pb, NET_THREADS, 0, st>>>(acts[4], X, Y, P, pr + NetLayout::woff(5), pr + NetLayout::boff(5), scale_out,
+			norm_part, nnorm, zc, out, pdot, dot_part, done, net_off);
 	LAUNCHED();
 
 	if (nblocks)
@@ -1971,15 +1972,31 @@ extern "C" int bnufft_precnet_forward(bnufft_precnet_t n, void* out, const void*
 	Staged i, o;
 	TRY(stage_in(i, in, b, st));
 	TRY(stage_out_alloc(o, out, b, st));
-	TRY(net_forward(n, (const float2*)i.dev, (int)X, (int)Y, nimg, n->act, nullptr, nullptr, nullptr, (float2*)o.dev,
-			nullptr, nullptr, nullptr, nullptr, nullptr, st));
+	TRY(net_forward(n, (const float2*)i.dev, (int)X, (int)Y, nimg, n->act, nullptr, nullptr, nullptr, 0, nullptr,
+			(float2*)o.dev, nullptr, nullptr, nullptr, nullptr, nullptr, st));
 	return stage_out_copy(o, out, b, st);
 }
+
+static int net_train(bnufft_precnet_t n, const void* in, const void* target, const void* gout_in, long X, long Y,
+		long nimg, float lr, double* loss, float* grads, cudaStream_t st);
 
 extern "C" int bnufft_precnet_train_step(bnufft_precnet_t n, const void* in, const void* target, long X, long Y,
 		long nimg, float lr, double* loss, float* grads, void* stream)
 {
-	cudaStream_t st = S(stream);
+	return net_train(n, in, target, nullptr, X, Y, nimg, lr, loss, grads, S(stream));
+}
+
+extern "C" int bnufft_precnet_backward(bnufft_precnet_t n, const void* in, const void* gout, long X, long Y,
+		long nimg, float lr, float* grads, void* stream)
+{
+	return net_train(n, in, nullptr, gout, X, Y, nimg, lr, nullptr, grads, S(stream));
+}
+
+// forward with all activations, then the gradient of the loss (MSE against
+// target) or the given output gradient gout_in, backward, optional Adam step
+static int net_train(bnufft_precnet_t n, const void* in, const void* target, const void* gout_in, long X, long Y,
+		long nimg, float lr, double* loss, float* grads, cudaStream_t st)
+{
 
 	if (!n || (X < 1) || (Y < 1) || (nimg < 1) || (X > (1 << 20)) || (Y > 65535 * NET_TILE_Y) || (nimg > 65535))
 		return fail(BNUFFT_ERR_ARG, "bad precnet image size");
@@ -1991,17 +2008,25 @@ extern "C" int bnufft_precnet_train_step(bnufft_precnet_t n, const void* in, con
 	size_t b = sizeof(float2) * P;
 	Staged si, stg;
 	TRY(stage_in(si, in, b, st));
-	TRY(stage_in(stg, target, b, st));
+	TRY(stage_in(stg, target ? target : gout_in, b, st));
 	const float2* inp = (const float2*)si.dev;
 	const unsigned pb = (unsigned)((P + NET_THREADS - 1) / NET_THREADS);
 
 	// forward, keeping every layer's activation
-	TRY(net_forward(n, inp, x, y, nimg, n->act, nullptr, nullptr, nullptr, n->out, nullptr, nullptr, nullptr, nullptr,
-			nullptr, st));
+	TRY(net_forward(n, inp, x, y, nimg, n->act, nullptr, nullptr, nullptr, 0, nullptr, n->out, nullptr, nullptr, nullptr,
+			nullptr, nullptr, st));
 
 	// loss = (1 / nimg) sum |out - target|^2, gout = dloss / dout
-	k_net_loss<<<NET_LOSS_BLOCKS, 256, 0, st>>>(n->out, (const float2*)stg.dev, P, 2.f / (float)nimg, n->gout, n->loss_part);
-	LAUNCHED();
+	if (target) {
+
+		k_net_loss<<<NET_LOSS_BLOCKS, 256, 0, st>>>(n->out, (const float2*)stg.dev, P, 2.f / (float)nimg, n->gout, n->loss_part);
+		LAUNCHED();
+
+	} else {
+
+		CUDA_TRY(cudaMemcpyAsync(n->gout, stg.dev, b, cudaMemcpyDeviceToDevice, st));
+		loss = nullptr;
+	}
 
 	// backward: layer 6, then 5..2 on the tensor cores, then layer 1
 	TRY((net_wgrad<NET_C, 2, bf16, float>(n, 5, n->act[4], (const float*)n->gout, x, y, nimg, st)));
@@ -2069,12 +2094,14 @@ struct bnufft_pics_s {
 	double* pap_part = nullptr;	// p^H partial, one per final row-pass block
 	double* pp_part = nullptr;	// ||p||^2, one per first row-pass block
 	double* rs_part = nullptr;	// ||r||^2, one per CG step block
-	// flexible CG (conf.precond): z = M(r), A p kept for the next direction
-	float2 *z = nullptr, *Ap = nullptr;
-	double* zap_part = nullptr;	// <A p_prev, z>, one per preconditioner row-pass block
+	// flexible CG (conf.precond): z = M(r); the last directions and their A p
+	float2* z = nullptr;
+	float2 *p_ring = nullptr, *ap_ring = nullptr;	// [FCG_RING][npix]
+	double* dots_part = nullptr;	// <z, A p_j> partials [FCG_MAX_M][nparts]
 	double* pr_part = nullptr;	// <p, r>, one per direction-update block
-	int nzap = 0;
+	int fcg_m = 1;			// truncation: directions orthogonalised against
 	bnufft_precnet_t net = nullptr;	// learned correction (conf.precond == 2), not owned
+	double* mcn_part = nullptr;	// ||M_circ(r)||^2 partials
 	bf16* nact[2] = { nullptr, nullptr };	// its activations, ping-pong [npix][32]
 	long max_row_blocks;
 	int nparts;
@@ -2205,9 +2232,17 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 
 	if (conf.precond) {
 
+		// the circulant preconditioner is linear (flexible CG keeps one
+		// direction, as PCG); the learned one is not: keep FCG_MAX_M
+		ps->fcg_m = (2 == conf.precond) ? (int)FCG_MAX_M : 1;
+
+		if (const char* e = getenv("BNUFFT_FCG_M"))
+			ps->fcg_m = std::max(1, std::min((int)FCG_MAX_M, atoi(e)));
+
 		ck(cudaMallocAsync(&ps->z, sizeof(float2) * ps->npix, st));
-		ck(cudaMallocAsync(&ps->Ap, sizeof(float2) * ps->npix, st));
-		ck(cudaMallocAsync(&ps->zap_part, sizeof(double) * ps->max_row_blocks, st));
+		ck(cudaMallocAsync(&ps->p_ring, sizeof(float2) * ps->npix * FCG_RING, st));
+		ck(cudaMallocAsync(&ps->ap_ring, sizeof(float2) * ps->npix * FCG_RING, st));
+		ck(cudaMallocAsync(&ps->dots_part, sizeof(double) * ps->nparts * FCG_MAX_M, st));
 		ck(cudaMallocAsync(&ps->pr_part, sizeof(double) * ps->nparts, st));
 
 		if (BNUFFT_OK == s)
@@ -2332,8 +2367,8 @@ static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, cons
 		int* nblocks, cudaStream_t st);
 
 // z = M(r): the circulant preconditioner, plus (precond 2) the learned
-// correction ||r|| net(r / ||r||) with ||r|| from the solve's scalars;
-// optional partials Re<pdot, z>
+// correction ||M_circ(r)|| net(r / ||r||) (1 / ||r|| from the solve's
+// scalars); optional partials Re<pdot, z>
 static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
 		int* nblocks, cudaStream_t st)
 {
@@ -2343,12 +2378,20 @@ static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const flo
 	if (!ps->net)
 		return fail(BNUFFT_ERR_ARG, "precond 2 needs a network (bnufft_pics_set_precnet)");
 
-	TRY(pics_precond_circ(ps, r, z, nullptr, nullptr, nullptr, st));
+	// z = M_circ(r) with the partials of ||z||^2, then z += ||z|| net(r / ||r||):
+	// flexible CG is invariant to a positive scale of z per iteration, so the
+	// network learns a scale-free correction of the circulant direction
+	int nmc = 0;
+	TRY(pics_precond_circ(ps, r, z, z, ps->mcn_part, &nmc, st));
+
+	if (nmc > ps->max_row_blocks)
+		return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
+
 	const Geom& g = ps->nufft->op.g;
 	bf16* acts[5] = { ps->nact[0], ps->nact[1], ps->nact[0], ps->nact[1], ps->nact[0] };
 	CgScalars* sc = ps->scal;
-	return net_forward(ps->net, r, g.N[0], g.N[1], 1, acts, &sc->rinv, &sc->rnorm, z, z, pdot, dot_part, nblocks,
-			&sc->done, &sc->net_off, st);
+	return net_forward(ps->net, r, g.N[0], g.N[1], 1, acts, &sc->rinv, nullptr, ps->mcn_part, nmc, z, z, pdot,
+			dot_part, nblocks, &sc->done, &sc->net_off, st);
 }
 
 // the circulant preconditioner applied to one image (N-point transforms, no
@@ -2375,8 +2418,9 @@ static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, cons
 	return rows_inv(g.G[0], full.w.t1, nullptr, nullptr, nullptr, g.N[0], YZ, 1, 1, z, st, pdot, dot_part, done, nblocks);
 }
 
-// One flexible-CG iteration: direction update, the normal operator's passes
-// (as in plain CG), the step, the convergence test and z = M(r).
+// One flexible-CG iteration: <z, A p_j> over the kept directions, the
+// direction update, the normal operator's passes (as in plain CG), the step,
+// the convergence test and z = M(r) for the next iteration.
 static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 {
 	OpCtx& op = ps->nufft->op;
@@ -2387,8 +2431,10 @@ static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	unsigned nb = (unsigned)ps->nparts;
 	int npap = 0;
 
-	k_fcg_dir<<<nb, RED_THREADS, 0, st>>>(p, ps->z, ps->r, ps->npix, ps->scal, it, ps->zap_part, ps->nzap,
-			ps->pr_part, ps->pp_part);
+	k_fcgm_dots<<<nb, RED_THREADS, 0, st>>>(ps->z, ps->ap_ring, ps->npix, ps->scal, it, ps->fcg_m, ps->dots_part);
+	LAUNCHED();
+	k_fcgm_dir<<<nb, RED_THREADS, 0, st>>>(p, ps->p_ring, ps->z, ps->r, ps->npix, ps->scal, it, ps->fcg_m,
+			ps->dots_part, ps->nparts, ps->pr_part, ps->pp_part);
 	LAUNCHED();
 	TRY(rows_fwd(g.G[0], p, ps->sens, nullptr, nullptr, g.N[0], YZ, YZ * ps->C, op.w.t1, st, done));
 	TRY(op_toeplitz_cols(op, ps->nufft->psf, ps->C, st, done));
@@ -2398,19 +2444,13 @@ static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	if (npap > ps->max_row_blocks)
 		return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
 
-	k_fcg_step<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, p, ps->Ap, ps->part, ps->groups, ps->npix, ps->conf.lambda,
-			ps->scal, it, ps->pap_part, npap, ps->pp_part, ps->nparts, ps->pr_part, ps->nparts, ps->rs_part);
+	k_fcg_step<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, p, ps->ap_ring, ps->part, ps->groups, ps->npix,
+			ps->conf.lambda, ps->scal, it, ps->pap_part, npap, ps->pp_part, ps->nparts, ps->pr_part, ps->nparts,
+			ps->rs_part);
 	LAUNCHED();
 	k_fcg_check<<<1, RED_THREADS, 0, st>>>(ps->scal, it, ps->rs_part, ps->nparts);
 	LAUNCHED();
-	int nz = 0;
-	TRY(pics_precond(ps, ps->r, ps->z, ps->Ap, ps->zap_part, &nz, st));
-
-	if (nz > ps->max_row_blocks)
-		return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
-
-	ps->nzap = nz;
-	return BNUFFT_OK;
+	return pics_precond(ps, ps->r, ps->z, nullptr, nullptr, nullptr, st);
 }
 
 static int pics_any_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
@@ -2446,7 +2486,7 @@ static int capture_cg_loop(bnufft_pics_s* ps)
 
 	if (BNUFFT_OK == s) {
 
-		k_cg_advance<<<1, 1, 0, ps->cap>>>(ps->scal, ps->conf.maxiter, loop);
+		k_cg_advance<<<1, 1, 0, ps->cap>>>(ps->scal, loop);
 		cudaError_t e = cudaGetLastError();
 
 		if (cudaSuccess != e)
@@ -2498,17 +2538,13 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 	// CG from zero (conjgrad, src/iter/italgos.c:497-572)
 	k_cg_init<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, ps->pbuf[1], ps->b, ps->npix, ps->rs_part);
 	LAUNCHED();
-	k_cg_start<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->rs_part, ps->nparts, ps->conf.tol);
+	k_cg_start<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->rs_part, ps->nparts, ps->conf.tol, ps->conf.maxiter);
 	LAUNCHED();
 
 	TRY(alloc_work(op.w, op.g, ps->C, st));
 
-	if (ps->conf.precond) {	// z0 = M(b); the first direction is p = z0
-
-		int nz = 0;
-		TRY(pics_precond(ps, ps->r, ps->z, nullptr, nullptr, &nz, st));
-		ps->nzap = nz;
-	}
+	if (ps->conf.precond)	// z0 = M(b); the first direction is p = z0
+		TRY(pics_precond(ps, ps->r, ps->z, nullptr, nullptr, nullptr, st));
 
 	if (ps->conf.maxiter > 0) {
 
@@ -2560,6 +2596,19 @@ extern "C" int bnufft_pics_set_precnet(bnufft_pics_t ps, bnufft_precnet_t net, v
 		if (!a)
 			CUDA_TRY(cudaMallocAsync(&a, sizeof(bf16) * NET_C * ps->npix, st));
 
+	if (!ps->mcn_part)
+		CUDA_TRY(cudaMallocAsync(&ps->mcn_part, sizeof(double) * ps->max_row_blocks, st));
+
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_pics_set_iter(bnufft_pics_t ps, int maxiter, float tol)
+{
+	if (!ps || (maxiter < 0) || !(tol >= 0.f))
+		return fail(BNUFFT_ERR_ARG, "bad iteration limit or tolerance");
+
+	ps->conf.maxiter = maxiter;
+	ps->conf.tol = tol;
 	return BNUFFT_OK;
 }
 
@@ -2641,8 +2690,8 @@ extern "C" void bnufft_pics_free(bnufft_pics_t ps)
 		cudaStreamDestroy(ps->cap);
 
 	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->pbuf[0], ps->pbuf[1], ps->b, ps->kbuf, ps->mag, ps->mag_sorted,
-			 ps->sort_tmp, ps->pap_part, ps->pp_part, ps->rs_part, ps->scal, ps->z, ps->Ap, ps->zap_part,
-			 ps->pr_part, ps->nact[0], ps->nact[1] };
+			 ps->sort_tmp, ps->pap_part, ps->pp_part, ps->rs_part, ps->scal, ps->z, ps->p_ring, ps->ap_ring,
+			 ps->dots_part, ps->pr_part, ps->nact[0], ps->nact[1], ps->mcn_part };
 
 	for (void* b : bufs)
 		if (b)

@@ -111,7 +111,7 @@ __global__ void k_cg_init(float2* __restrict__ x, float2* __restrict__ r, float2
 }
 
 // rs[0] = ||b||^2 = b2, eps2 = (tol*||b||)^2, iters = 0, done = (b2 == 0)
-__global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float tol)
+__global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float tol, int maxiter)
 {
 	__shared__ double sh[32];
 	double b2 = sum_partials(part, nparts, sh);
@@ -124,8 +124,10 @@ __global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float 
 		st->eps2 = eps * eps;
 		st->iters = 0;
 		st->it = 0;
+		st->maxiter = maxiter;
 		st->done = (0. == b2);
 		st->best_rs = b2;
+		st->best_hist[0] = b2;
 		st->best_it = 0;
 		st->net_off = 0;
 		st->rnorm = (float)sqrt(b2);
@@ -249,16 +251,18 @@ __global__ void k_precond_from_spectrum(float2* __restrict__ pinv, const float2*
 	}
 }
 
-// Flexible CG (Notay, SIAM J. Sci. Comput. 22(4), 2000: FCG with one
-// previous direction), used with a preconditioner z = M(r) that may be
-// nonlinear (the learned one) or only approximately symmetric:
-//   p = z + beta p_prev, beta = -<z, A p_prev> / <p_prev, A p_prev>
-//   alpha = <p, r> / <p, A p>,  x += alpha p,  r -= alpha A p.
-// Direction update in place (elementwise), with the partials <p, r> and
-// ||p||^2 (lambda ||p||^2 in <p, (A^H A + lambda) p>).
-__global__ void k_fcg_dir(float2* __restrict__ p, const float2* __restrict__ z, const float2* __restrict__ r, long n,
-		const CgScalars* st, int it, const double* __restrict__ zap_part, int nzap,
-		double* __restrict__ pr_part, double* __restrict__ pp_part)
+// Flexible CG (Notay, SIAM J. Sci. Comput. 22(4), 2000) with truncation m:
+// the preconditioner z = M(r) may be nonlinear (the learned one), so each new
+// direction is made A-orthogonal to the last m directions,
+//   p_k = z_k - sum_{j = k-m}^{k-1} (<z_k, A p_j> / <p_j, A p_j>) p_j,
+//   alpha = <p_k, r_k> / <p_k, A p_k>,  x += alpha p_k,  r -= alpha A p_k.
+// The last FCG_RING directions and their A p live in ring buffers
+// [FCG_RING][n], slot j % FCG_RING, indexed from the device iteration counter.
+
+// partials of <z, A p_j> for the window j = it - w .. it - 1, w = min(it, m):
+// part[q * gridDim.x + block], q = j - (it - w)
+__global__ void k_fcgm_dots(const float2* __restrict__ z, const float2* __restrict__ ap_ring, long n,
+		const CgScalars* st, int it, int m, double* __restrict__ part)
 {
 	__shared__ double sh[32];
 
@@ -266,20 +270,82 @@ __global__ void k_fcg_dir(float2* __restrict__ p, const float2* __restrict__ z, 
 		return;
 
 	it = cg_iter(it, st);
-	float beta = 0.f;
-
-	if (it > 0)
-		beta = (float)(-sum_partials(zap_part, nzap, sh) / st->pap);
-
-	double pr = 0., pp = 0.;
+	const int w = min(it, m);
+	double acc[FCG_MAX_M];
+#pragma unroll
+	for (int q = 0; q < FCG_MAX_M; q++)
+		acc[q] = 0.;
 
 	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
 
 		float2 zv = z[i];
-		float2 pv = (it > 0) ? p[i] : make_float2(0.f, 0.f);
-		pv.x = fmaf(beta, pv.x, zv.x);
-		pv.y = fmaf(beta, pv.y, zv.y);
-		p[i] = pv;
+#pragma unroll
+		for (int q = 0; q < FCG_MAX_M; q++) {
+
+			if (q < w) {
+
+				float2 a = ap_ring[(long)((it - w + q) % FCG_RING) * n + i];
+				acc[q] += (double)zv.x * (double)a.x + (double)zv.y * (double)a.y;
+			}
+		}
+	}
+
+#pragma unroll
+	for (int q = 0; q < FCG_MAX_M; q++) {
+
+		if (q < w) {
+
+			double t = block_sum(acc[q], sh);
+
+			if (0 == threadIdx.x)
+				part[q * gridDim.x + blockIdx.x] = t;
+
+			__syncthreads();
+		}
+	}
+}
+
+// direction: p = z - sum_q beta_q p_{it-w+q}; p into p_cur and ring slot
+// it % FCG_RING; partials <p, r> and ||p||^2 (lambda ||p||^2 in <p, A p>)
+__global__ void k_fcgm_dir(float2* __restrict__ p_cur, float2* __restrict__ p_ring, const float2* __restrict__ z,
+		const float2* __restrict__ r, long n, const CgScalars* st, int it, int m, const double* __restrict__ dots,
+		int ndots, double* __restrict__ pr_part, double* __restrict__ pp_part)
+{
+	__shared__ double sh[32];
+	__shared__ float beta[FCG_MAX_M];
+
+	if (st->done)
+		return;
+
+	it = cg_iter(it, st);
+	const int w = min(it, m);
+
+	for (int q = 0; q < w; q++) {
+
+		double d = sum_partials(dots + q * ndots, ndots, sh);
+
+		if (0 == threadIdx.x)
+			beta[q] = (float)(d / st->pap_hist[(it - w + q) % FCG_RING]);
+	}
+
+	__syncthreads();
+
+	float2* p_slot = p_ring + (long)(it % FCG_RING) * n;
+	double pr = 0., pp = 0.;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		float2 pv = z[i];
+
+		for (int q = 0; q < w; q++) {
+
+			float2 o = p_ring[(long)((it - w + q) % FCG_RING) * n + i];
+			pv.x = fmaf(-beta[q], o.x, pv.x);
+			pv.y = fmaf(-beta[q], o.y, pv.y);
+		}
+
+		p_cur[i] = pv;
+		p_slot[i] = pv;
 		float2 rv = r[i];
 		pr += (double)pv.x * (double)rv.x + (double)pv.y * (double)rv.y;
 		pp += (double)pv.x * (double)pv.x + (double)pv.y * (double)pv.y;
@@ -297,10 +363,10 @@ __global__ void k_fcg_dir(float2* __restrict__ p, const float2* __restrict__ z, 
 }
 
 // FCG step: <p, A p> (coil-sum row-pass partials + lambda ||p||^2), alpha =
-// <p, r> / <p, A p>; per element A p = sum_g part_g + lambda p (kept for the
-// next direction), x += alpha p, r -= alpha A p, partial ||r||^2.
+// <p, r> / <p, A p>; per element A p = sum_g part_g + lambda p (into ring
+// slot it % FCG_RING), x += alpha p, r -= alpha A p, partial ||r||^2.
 __global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
-		float2* __restrict__ Ap, const float2* __restrict__ part, int groups, long n, float lam, CgScalars* st, int it,
+		float2* __restrict__ ap_ring, const float2* __restrict__ part, int groups, long n, float lam, CgScalars* st, int it,
 		const double* __restrict__ pap_part, int npap, const double* __restrict__ pp_part, int npp,
 		const double* __restrict__ pr_part, int npr, double* __restrict__ rs_part)
 {
@@ -324,6 +390,7 @@ __global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const
 	}
 
 	float a = (float)(sum_partials(pr_part, npr, sh) / pAp);
+	float2* Ap = ap_ring + (long)(it % FCG_RING) * n;
 	double acc = 0.;
 
 	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -355,7 +422,7 @@ __global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const
 		rs_part[blockIdx.x] = s;
 
 	if ((0 == blockIdx.x) && (0 == threadIdx.x))
-		st->pap = pAp;
+		st->pap_hist[it % FCG_RING] = pAp;
 }
 
 // FCG convergence test after step it: ||r||^2 <= eps2 stops with it + 1
@@ -382,17 +449,26 @@ __global__ void k_fcg_check(CgScalars* st, int it, const double* __restrict__ rs
 			st->iters = it + 1;
 		}
 
-		// stall: no new smallest residual for 3 iterations switches the
-		// learned part of the preconditioner off for the rest of the solve
+		// stall: no new smallest residual for 3 iterations, or less than a 4x
+		// reduction of the smallest ||r||^2 over the last 4 iterations,
+		// switches the learned part of the preconditioner off for the rest
+		// of the solve (the method falls back to its linear preconditioner)
+		const int j = it + 1;
+
 		if (rs < st->best_rs) {
 
 			st->best_rs = rs;
-			st->best_it = it + 1;
+			st->best_it = j;
 
-		} else if (it + 1 - st->best_it >= 3) {
+		} else if (j - st->best_it >= 3) {
 
 			st->net_off = 1;
 		}
+
+		if ((j >= 4) && (st->best_rs > 0.25 * st->best_hist[j % 4]))
+			st->net_off = 1;
+
+		st->best_hist[j % 4] = st->best_rs;
 	}
 }
 
@@ -419,11 +495,11 @@ __global__ void k_norm_scalars(const float2* __restrict__ v, long n, CgScalars* 
 
 // End of one CG iteration inside a graph: advance the device iteration
 // counter and continue the enclosing while node unless converged or at maxiter.
-__global__ void k_cg_advance(CgScalars* st, int maxiter, cudaGraphConditionalHandle loop)
+__global__ void k_cg_advance(CgScalars* st, cudaGraphConditionalHandle loop)
 {
 	int it = st->it + 1;
 	st->it = it;
-	cudaGraphSetConditional(loop, (!st->done && (it < maxiter)) ? 1u : 0u);
+	cudaGraphSetConditional(loop, (!st->done && (it < st->maxiter)) ? 1u : 0u);
 }
 
 // after the last iteration: ||r||^2 and the iteration count

@@ -87,6 +87,9 @@ __device__ __forceinline__ double sum_partials_d(const double* part, int n, doub
 	return r;
 }
 
+// flexible CG: largest truncation (directions kept) and ring size
+enum { FCG_MAX_M = 16, FCG_RING = FCG_MAX_M + 1 };
+
 // device-side state of the CG solve
 struct CgScalars {
 
@@ -96,8 +99,10 @@ struct CgScalars {
 	int done;		// set once converged (or p^H A p == 0)
 	int iters;		// iterations completed
 	int it;			// iteration being run (device-driven loop)
-	double pap;		// <p, (A^H A + lambda) p> of the last step (flexible CG)
+	int maxiter;		// iteration limit of the current solve
+	double pap_hist[FCG_RING];	// <p_j, (A^H A + lambda) p_j>, slot j % FCG_RING (flexible CG)
 	double best_rs;		// smallest ||r||^2 so far (flexible CG stall test)
+	double best_hist[4];	// best_rs after iteration j, slot j % 4
 	int best_it;		// iteration count at best_rs
 	int net_off;		// learned preconditioner switched off (stall fallback)
 	float rnorm;		// ||r|| of the current residual
@@ -429,9 +434,9 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 
 					out[x + X * yz + X * YZ * c] = w;
 
-					if (pdot) {	// Re<pdot, out> per coil
+					if (pdot) {	// Re<pdot, out> per coil (pdot == out: ||out||^2)
 
-						float2 pv = pdot[x + X * yz + X * YZ * c];
+						float2 pv = ((const void*)pdot == (const void*)out) ? w : pdot[x + X * yz + X * YZ * c];
 						dot += (double)pv.x * (double)w.x + (double)pv.y * (double)w.y;
 					}
 				}

@@ -293,13 +293,14 @@ __device__ __forceinline__ float2 net_out_pixel(const bf16* __restrict__ act, lo
 }
 
 // Layer 6 (32 -> 2), one thread per pixel:
-//   out = zc + s * (conv(act, w) + b)   (zc = 0 if null; s = *scale or 1),
-// or out = zc when *net_off (the stall fallback of the flexible CG). With
-// pdot: per-block partials Re<pdot, out>.
+//   out = zc + s * (conv(act, w) + b)   (zc = 0 if null),
+// s = *scale, or sqrt(sum of norm_part) (the norm of zc, from the partials
+// of the pass that wrote it), or 1; out = zc when *net_off (the stall
+// fallback of the flexible CG). With pdot: per-block partials Re<pdot, out>.
 __global__ void __launch_bounds__(NET_THREADS) k_net_out(const bf16* __restrict__ act, int X, int Y, long P,
-		const float* __restrict__ w, const float* __restrict__ b, const float* scale, const float2* zc,
-		float2* out, const float2* __restrict__ pdot, double* __restrict__ dot_part, const int* done,
-		const int* net_off)
+		const float* __restrict__ w, const float* __restrict__ b, const float* scale, const double* norm_part,
+		int nnorm, const float2* zc, float2* out, const float2* __restrict__ pdot, double* __restrict__ dot_part,
+		const int* done, const int* net_off)
 {
 	__shared__ float sw[2 * 9 * NET_C + 2];
 	__shared__ double red[32];
@@ -310,6 +311,7 @@ __global__ void __launch_bounds__(NET_THREADS) k_net_out(const bf16* __restrict_
 	for (int i = threadIdx.x; i < 2 * 9 * NET_C + 2; i += NET_THREADS)
 		sw[i] = (i < 2 * 9 * NET_C) ? w[i] : b[i - 2 * 9 * NET_C];
 
+	const float s = scale ? *scale : (norm_part ? (float)sqrt(sum_partials_d(norm_part, nnorm, red)) : 1.f);
 	__syncthreads();
 
 	const long p = (long)blockIdx.x * NET_THREADS + threadIdx.x;
@@ -324,7 +326,6 @@ __global__ void __launch_bounds__(NET_THREADS) k_net_out(const bf16* __restrict_
 		if (!off) {
 
 			float2 o = net_out_pixel(act, (p / XY) * XY, (int)(p % X), (int)((p % XY) / X), X, Y, sw);
-			const float s = scale ? *scale : 1.f;
 			v.x = fmaf(s, o.x + sw[2 * 9 * NET_C], v.x);
 			v.y = fmaf(s, o.y + sw[2 * 9 * NET_C + 1], v.y);
 		}

@@ -87,6 +87,11 @@ class Pics:
                                                  ctypes.byref(sc), stream))
         return it.value, res.value, sc.value
 
+    def set_iter(self, maxiter, tol=0.0):
+        """Iteration limit and tolerance of later runs."""
+        _lib.check(_lib.load().bnufft_pics_set_iter(self._h, int(maxiter), float(tol)))
+        self.conf.maxiter, self.conf.tol = int(maxiter), float(tol)
+
     def rhs(self, ksp, out=None):
         """b = A^H y / scale, the right-hand side of the solve."""
         n_in = int(np.prod(self.ksp_dims))

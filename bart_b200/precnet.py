@@ -5,7 +5,7 @@ channels, bf16 weights, float32 accumulation) runs and trains on the GPU
 through libbnufft's own kernels (``bnufft_precnet_*``). Inside flexible CG
 (``PicsConf(precond=2)``) the preconditioner is
 
-    z = M_circ(r) + ||r|| net(r / ||r||)
+    z = M_circ(r) + ||M_circ(r)|| net(r / ||r||)
 
 where M_circ is the reference's circulant PSF preconditioner
 (src/noncart/precond.c:48-164). With a zero last layer the network adds
@@ -14,13 +14,17 @@ stops improving for 3 iterations the solve drops the learned term.
 
 Training data come from the method itself: for each generated problem the
 library's flexible CG (circulant preconditioner) is run for k = 0, 1, 2, ...
-iterations and to convergence; with x* the converged solution, x_k the
-iterate and r_k = b - (A^H A + lambda) x_k its true residual, the pair is
+iterations and to convergence (x*); each iterate x_k gives its true
+residual r_k = b - (A^H A + lambda) x_k and exact error e_k = x* - x_k. The
+loss is what one flexible-CG step along z = M_circ(r)/||M_circ(r)|| +
+net(r/||r||) leaves of the A-norm error after an exact line search,
 
-    input  = r_k / ||r_k||,   target = (x* - x_k - M_circ(r_k)) / ||r_k||
+    L = 1 - <z, r>^2 / (<z, A z> <e, r>),    A = A^H A + lambda,
 
-i.e. the network learns the part of the exact error A^-1 r_k that the
-circulant preconditioner misses.
+scale-free in z like the solver; its gradient needs A z, applied with the
+library's Toeplitz normal operator, and enters the network's own backward
+kernels (bnufft_precnet_backward). Training is online: problems are drawn,
+turned into a residual batch, and used for a few Adam steps.
 
   python -m bart_b200.precnet train [--problems 2000] [--eval 256] [--out FILE]
   python -m bart_b200.precnet eval [--weights FILE] [--eval 256]
@@ -125,6 +129,16 @@ class PrecNet:
         del k1, k2
         return loss.value if want_loss else None
 
+    def backward(self, x, gout, X, Y, n, lr, grads=None):
+        """Backward from a given d loss / d net(x), then an Adam step (lr > 0)."""
+        from .nufft import _ptr_in, _stream_of
+        P = X * Y * n
+        px, k1 = _ptr_in(x, P)
+        pg, k2 = _ptr_in(gout, P)
+        gp = None if grads is None else ctypes.c_void_p(grads.ctypes.data)
+        _lib.check(_lib.load().bnufft_precnet_backward(self.handle, px, pg, X, Y, n, float(lr), gp, _stream_of(x, gout)))
+        del k1, k2
+
     def free(self):
         if getattr(self, "handle", None) is not None:
             _lib.load().bnufft_precnet_free(self.handle)
@@ -155,89 +169,98 @@ def _model(prob, dev, precond, maxiter, tol):
     return p, dt(ksp)
 
 
-def training_pairs(prob, dev, iters=ITERS):
-    """(inputs, targets): complex [len(iters), N*N] tensors on dev."""
+def problem_samples(prob, dev, iters=ITERS):
+    """The model (circulant preconditioner) of one problem and, for its
+    iterates k in iters, unit residuals R_k = r_k / ||r_k||, unit circulant
+    steps Mn_k = M(r_k) / ||M(r_k)|| and E_k = <e_k, r_k> / ||r_k||^2 with
+    e_k = x* - x_k = A^-1 r_k. The caller frees the model."""
     import torch
-    N = prob["sens"].shape[0]
     p, ksp = _model(prob, dev, 1, 200, 1e-7)
-    try:
-        b = p.rhs(ksp)
-        xs = p.run(ksp).clone()
-        ins, tgs = [], []
-        for k in iters:
-            if k == 0:
-                xk = torch.zeros_like(xs)
-            else:
-                q, _ = _model(prob, dev, 1, k, 0.0)
-                try:
-                    xk = q.run(ksp).clone()
-                finally:
-                    q.free()
-            r = b - (p.normal(xk) + LAM * xk)
-            nr = torch.linalg.vector_norm(r)
-            mc = p.precond(r)
-            ins.append(r / nr)
-            tgs.append((xs - xk - mc) / nr)
-        return torch.stack(ins), torch.stack(tgs)
-    finally:
-        p.free()
+    b = p.rhs(ksp)
+    xs = p.run(ksp).clone()
+    R, Mn, E = [], [], []
+    for k in iters:
+        if k == 0:
+            xk = torch.zeros_like(xs)
+        else:
+            p.set_iter(k, 0.0)
+            xk = p.run(ksp).clone()
+        r = b - (p.normal(xk) + LAM * xk)
+        nr = torch.linalg.vector_norm(r)
+        mc = p.precond(r)
+        R.append(r / nr)
+        Mn.append(mc / torch.linalg.vector_norm(mc))
+        E.append(torch.sum(torch.conj(xs - xk) * r).real / nr ** 2)
+    return p, torch.stack(R), torch.stack(Mn), torch.stack(E)
 
 
-def make_dataset(nprob, seed, dev, N=256, coils=(8, 32), spokes=(48, 128), log=None):
+def anorm_loss(p, R, Mn, E, out):
+    """Per sample, the fraction of the A-norm error that an exact line search
+    along z = Mn + out leaves, L = 1 - <z, r>^2 / (<z, A z> <A^-1 r, r>)
+    (A = A^H A + lambda; in [0, 1], scale-free in z like flexible CG), and
+    d mean(L) / d out."""
+    import torch
+    K = R.shape[0]
+    z = Mn + out.view(K, -1)
+    Az = torch.stack([p.normal(z[k].contiguous()) + LAM * z[k] for k in range(K)])
+    a = torch.sum(torch.conj(z) * R, dim=1).real
+    q = torch.sum(torch.conj(z) * Az, dim=1).real
+    L = 1 - a ** 2 / (q * E)
+    g = -(2 * a / (q * E))[:, None] * (R - (a / q)[:, None] * Az)
+    return L, (g / K).to(torch.complex64)
+
+
+def train_online(net, nprob, seed, dev, N=256, coils=(8, 32), spokes=(48, 128), steps=3, lr=1e-3, log=None):
+    """Adam on the A-norm line-search loss, problems generated on the fly;
+    `steps` updates per problem on its residual batch; cosine-decayed rate."""
     import torch
     from .problems import cgsense_problem
     rng = np.random.default_rng(seed)
-    X, T = [], []
-    t0 = time.time()
-    for i in range(nprob):
-        prob = cgsense_problem(rng, N=N, coils=coils, spokes=spokes)
-        x, t = training_pairs(prob, dev)
-        X.append(x)
-        T.append(t)
-        if log and (i + 1) % 100 == 0:
-            log(f"data {i + 1}/{nprob} ({time.time() - t0:.1f} s)")
-    return torch.cat(X), torch.cat(T)
-
-
-# ---------------------------------------------------------------------------
-# training and evaluation
-# ---------------------------------------------------------------------------
-
-def train(net, X, T, N, epochs=4, batch=8, lr=1e-3, seed=0, log=None):
-    """Adam with cosine-decayed learning rate over shuffled batches."""
-    import torch
-    n = X.shape[0]
-    steps = epochs * (n // batch)
-    g = torch.Generator(device="cpu").manual_seed(seed)
+    total = nprob * steps
     hist = []
     s = 0
     t0 = time.time()
-    for ep in range(epochs):
-        perm = torch.randperm(n, generator=g)
-        run = 0.0
-        for j in range(n // batch):
-            idx = perm[j * batch:(j + 1) * batch].to(X.device)
-            xb = X.index_select(0, idx).contiguous().view(-1)
-            tb = T.index_select(0, idx).contiguous().view(-1)
-            lr_s = 0.5 * lr * (1 + np.cos(np.pi * s / max(1, steps)))
-            want = (j % 50 == 0)
-            loss = net.train_step(xb, tb, N, N, batch, lr_s, want_loss=want)
-            if want:
-                run = loss
-                hist.append((s, loss))
-            s += 1
-        if log:
-            log(f"epoch {ep + 1}/{epochs}: loss {run:.4g} ({time.time() - t0:.1f} s)")
+    for i in range(nprob):
+        prob = cgsense_problem(rng, N=N, coils=coils, spokes=spokes)
+        p, R, Mn, E = problem_samples(prob, dev)
+        try:
+            K = R.shape[0]
+            x = R.contiguous().view(-1)
+            for j in range(steps):
+                out = net.forward(x, N, N, K)
+                L, g = anorm_loss(p, R, Mn, E, out)
+                if j == 0:
+                    L0, _ = anorm_loss(p, R, Mn, E, torch.zeros_like(out))
+                    hist.append((i, float(L0.mean()), float(L.mean())))
+                lr_s = 0.5 * lr * (1 + np.cos(np.pi * s / max(1, total)))
+                net.backward(x, g.contiguous().view(-1), N, N, K, lr_s)
+                s += 1
+        finally:
+            p.free()
+        if log and (i + 1) % 100 == 0:
+            h = np.array(hist[-100:])
+            log(f"problem {i + 1}/{nprob}: loss circulant {h[:, 1].mean():.4f} learned {h[:, 2].mean():.4f} "
+                f"({time.time() - t0:.1f} s)")
     return hist
 
 
-def dataset_loss(net, X, T, N, batch=8):
-    tot, cnt = 0.0, 0
-    for j in range(0, X.shape[0] - batch + 1, batch):
-        tot += net.train_step(X[j:j + batch].contiguous().view(-1), T[j:j + batch].contiguous().view(-1),
-                              N, N, batch, 0.0) * batch
-        cnt += batch
-    return tot / max(1, cnt)
+def heldout_loss(net, nprob, seed, dev, N=256):
+    """Mean A-norm loss of the circulant step and of the learned one."""
+    import torch
+    from .problems import cgsense_problem
+    rng = np.random.default_rng(seed)
+    lc, ll = [], []
+    for _ in range(nprob):
+        prob = cgsense_problem(rng, N=N)
+        p, R, Mn, E = problem_samples(prob, dev)
+        try:
+            K = R.shape[0]
+            out = net.forward(R.contiguous().view(-1), N, N, K)
+            lc.append(anorm_loss(p, R, Mn, E, torch.zeros_like(out))[0].mean().item())
+            ll.append(anorm_loss(p, R, Mn, E, out)[0].mean().item())
+        finally:
+            p.free()
+    return float(np.mean(lc)), float(np.mean(ll))
 
 
 def solve_stats(prob, dev, precond, net=None, tol=1e-4, maxiter=300, reps=3):
@@ -298,9 +321,8 @@ def main(argv=None):
     ap.add_argument("cmd", choices=["train", "eval"])
     ap.add_argument("--problems", type=int, default=2000)
     ap.add_argument("--eval", type=int, default=256)
-    ap.add_argument("--epochs", type=int, default=4)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--weights", default=WEIGHTS)
     ap.add_argument("--report", default=None)
@@ -314,21 +336,14 @@ def main(argv=None):
 
     report = {}
     if a.cmd == "train":
-        t0 = time.time()
-        X, T = make_dataset(a.problems, 1, dev, log=log)
-        report["data_s"] = time.time() - t0
-        report["pairs"] = int(X.shape[0])
         net = PrecNet()
-        Xh, Th = make_dataset(min(64, a.eval), 7, dev)
-        report["heldout_loss_init"] = dataset_loss(net, Xh, Th, 256)
         t0 = time.time()
-        hist = train(net, X, T, 256, epochs=a.epochs, batch=a.batch, lr=a.lr, log=log)
+        hist = train_online(net, a.problems, 1, dev, steps=a.steps, lr=a.lr, log=log)
         torch.cuda.synchronize()
         report["train_s"] = time.time() - t0
-        report["loss_history"] = hist
-        report["heldout_loss_trained"] = dataset_loss(net, Xh, Th, 256)
-        del X, T
-        net.save(a.out, problems=a.problems, epochs=a.epochs, lr=a.lr, batch=a.batch)
+        report["loss_history"] = hist[::max(1, len(hist) // 50)]
+        report["heldout_loss_circulant"], report["heldout_loss_learned"] = heldout_loss(net, 32, 7, dev)
+        net.save(a.out, problems=a.problems, steps=a.steps, lr=a.lr)
     else:
         net = PrecNet.load(a.weights)
     rows = evaluate(net, a.eval, 2, dev, log=log)

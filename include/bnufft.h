@@ -157,6 +157,10 @@ int bnufft_pics_kernels(bnufft_pics_t pics, long* kernels, void* stream);
 
 void bnufft_pics_free(bnufft_pics_t pics);
 
+/* Change the iteration limit and tolerance of later runs (the captured CG
+ * graph reads them from the device, so it is kept). */
+int bnufft_pics_set_iter(bnufft_pics_t pics, int maxiter, float tol);
+
 /* b = A^H y / scale, the right-hand side the solve uses (scaling as in
  * bnufft_pics_run). img-sized output. */
 int bnufft_pics_rhs(bnufft_pics_t pics, void* b, const void* ksp, void* stream);
@@ -171,7 +175,7 @@ int bnufft_pics_precond(bnufft_pics_t pics, void* z, const void* r, void* stream
  * channels), ReLU after layers 1-5, bf16 weights and activations, float32
  * accumulation. Parameters: float32, per layer W[cout][3 ky + kx][cin] then
  * b[cout]; bnufft_precnet_nparams() values in all. Used by flexible CG as
- * z = M_circ(r) + ||r|| net(r / ||r||). */
+ * z = M_circ(r) + ||M_circ(r)|| net(r / ||r||). */
 typedef struct bnufft_precnet_s* bnufft_precnet_t;
 
 int bnufft_precnet_nparams(void);
@@ -187,6 +191,12 @@ int bnufft_precnet_forward(bnufft_precnet_t net, void* out, const void* in, long
  * learning rate lr (none if lr <= 0). loss (if not null) synchronises. */
 int bnufft_precnet_train_step(bnufft_precnet_t net, const void* in, const void* target, long X, long Y, long nimg,
 		float lr, double* loss, float* grads, void* stream);
+
+/* The same step with the loss gradient d loss / d net(in) given by the
+ * caller (gout, complex like in): for losses that need operators outside the
+ * network. */
+int bnufft_precnet_backward(bnufft_precnet_t net, const void* in, const void* gout, long X, long Y, long nimg,
+		float lr, float* grads, void* stream);
 
 void bnufft_precnet_free(bnufft_precnet_t net);
 
