@@ -60,14 +60,19 @@ static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
 
 static std::atomic<bool> g_prof_active{false};
 
+// passes run for the preconditioner carry this class prefix ("precond_")
+static thread_local bool t_prof_precond = false;
+
 static cudaEvent_t prof_begin(const char* kind, cudaStream_t st)
 {
 	if (!g_prof_active.load(std::memory_order_relaxed))
 		return nullptr;
 
+	std::string k = t_prof_precond ? std::string("precond_") + kind : std::string(kind);
+
 	std::lock_guard<std::mutex> lock(g_prof_mutex);
 
-	if (g_prof_target.empty() || (g_prof_target != kind))
+	if (g_prof_target.empty() || (g_prof_target != k))
 		return nullptr;
 
 	cudaEvent_t a, b;
@@ -2413,9 +2418,17 @@ static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, cons
 	full.w = p->op.w;	// the plan's buffers (N <= 2N), free between the operator's passes
 	const Geom& g = full.g;
 	long YZ = (long)g.N[1] * g.N[2];
-	TRY(rows_fwd(g.G[0], r, nullptr, nullptr, nullptr, g.N[0], YZ, YZ, full.w.t1, st, done));
-	TRY(op_toeplitz_cols(full, p->pinv, 1, st, done));
-	return rows_inv(g.G[0], full.w.t1, nullptr, nullptr, nullptr, g.N[0], YZ, 1, 1, z, st, pdot, dot_part, done, nblocks);
+	t_prof_precond = true;
+	int s = rows_fwd(g.G[0], r, nullptr, nullptr, nullptr, g.N[0], YZ, YZ, full.w.t1, st, done);
+
+	if (BNUFFT_OK == s)
+		s = op_toeplitz_cols(full, p->pinv, 1, st, done);
+
+	if (BNUFFT_OK == s)
+		s = rows_inv(g.G[0], full.w.t1, nullptr, nullptr, nullptr, g.N[0], YZ, 1, 1, z, st, pdot, dot_part, done, nblocks);
+
+	t_prof_precond = false;
+	return s;
 }
 
 // One flexible-CG iteration: <z, A p_j> over the kept directions, the

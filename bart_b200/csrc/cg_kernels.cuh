@@ -130,6 +130,7 @@ __global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float 
 		st->best_hist[0] = b2;
 		st->best_it = 0;
 		st->net_off = 0;
+		st->restart_it = 0;
 		st->rnorm = (float)sqrt(b2);
 		st->rinv = (b2 > 0.) ? (float)(1. / sqrt(b2)) : 0.f;
 	}
@@ -259,7 +260,8 @@ __global__ void k_precond_from_spectrum(float2* __restrict__ pinv, const float2*
 // The last FCG_RING directions and their A p live in ring buffers
 // [FCG_RING][n], slot j % FCG_RING, indexed from the device iteration counter.
 
-// partials of <z, A p_j> for the window j = it - w .. it - 1, w = min(it, m):
+// partials of <z, A p_j> for the window j = it - w .. it - 1,
+// w = min(it - restart, m) (the history restarts when the preconditioner changes):
 // part[q * gridDim.x + block], q = j - (it - w)
 __global__ void k_fcgm_dots(const float2* __restrict__ z, const float2* __restrict__ ap_ring, long n,
 		const CgScalars* st, int it, int m, double* __restrict__ part)
@@ -270,7 +272,7 @@ __global__ void k_fcgm_dots(const float2* __restrict__ z, const float2* __restri
 		return;
 
 	it = cg_iter(it, st);
-	const int w = min(it, m);
+	const int w = min(it - st->restart_it, m);
 	double acc[FCG_MAX_M];
 #pragma unroll
 	for (int q = 0; q < FCG_MAX_M; q++)
@@ -318,7 +320,7 @@ __global__ void k_fcgm_dir(float2* __restrict__ p_cur, float2* __restrict__ p_ri
 		return;
 
 	it = cg_iter(it, st);
-	const int w = min(it, m);
+	const int w = min(it - st->restart_it, m);
 
 	for (int q = 0; q < w; q++) {
 
@@ -460,13 +462,16 @@ __global__ void k_fcg_check(CgScalars* st, int it, const double* __restrict__ rs
 			st->best_rs = rs;
 			st->best_it = j;
 
-		} else if (j - st->best_it >= 3) {
-
-			st->net_off = 1;
 		}
 
-		if ((j >= 4) && (st->best_rs > 0.25 * st->best_hist[j % 4]))
+		bool stall = (j - st->best_it >= 3) || ((j >= 4) && (st->best_rs > 0.25 * st->best_hist[j % 4]));
+
+		if (stall && !st->net_off) {
+
+			// the preconditioner changes: restart the direction history
 			st->net_off = 1;
+			st->restart_it = j;
+		}
 
 		st->best_hist[j % 4] = st->best_rs;
 	}
@@ -490,6 +495,7 @@ __global__ void k_norm_scalars(const float2* __restrict__ v, long n, CgScalars* 
 		st->rinv = (s > 0.) ? (float)(1. / sqrt(s)) : 0.f;
 		st->done = 0;
 		st->net_off = 0;
+		st->restart_it = 0;
 	}
 }
 

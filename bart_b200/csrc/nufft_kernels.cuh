@@ -105,6 +105,7 @@ struct CgScalars {
 	double best_hist[4];	// best_rs after iteration j, slot j % 4
 	int best_it;		// iteration count at best_rs
 	int net_off;		// learned preconditioner switched off (stall fallback)
+	int restart_it;		// flexible CG direction history starts here
 	float rnorm;		// ||r|| of the current residual
 	float rinv;		// 1 / ||r|| (0 for r = 0)
 	float scale;		// data scaling used

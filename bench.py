@@ -2,13 +2,15 @@
 
 Workload (default): 2D radial CG-SENSE, 256x256 image, 16 coils with smooth
 polynomial maps, 96 golden-angle spokes x 512 samples, 40 dB noise,
-lambda 0.01, Toeplitz normal operator, automatic data scaling, plain CG run
-until the relative normal-equation residual reaches 1e-4
-(``bart pics -l2 -r0.01 -t traj ksp sens out`` with the iteration count that
-reaches it). One step is one full reconstruction from device-resident
-trajectory, maps and k-space: model set-up (trajectory upload, PSF on the
-device), adjoint, scaling, CG. L2 is flushed before every timed step. The
-same solve at a fixed 30 iterations, Toeplitz on and off, is reported beside.
+lambda 0.01, Toeplitz normal operator, automatic data scaling, solved until
+the relative normal-equation residual reaches 1e-4 (the problem of
+``bart pics -l2 -r0.01 -t traj ksp sens out``). The headline solver is
+flexible CG with the circulant PSF preconditioner; plain CG (the reference's
+method) and flexible CG with the learned correction are timed beside it.
+One step is one full reconstruction from device-resident trajectory, maps
+and k-space: model set-up (trajectory upload, PSF on the device), adjoint,
+scaling, CG graph. L2 is flushed before every timed step. The config's
+fixed 30 plain-CG iterations, Toeplitz on and off, are reported beside.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -42,7 +44,8 @@ TOL, MAXITER = 1e-4, 300
 # exactly this many
 REF_ITERS_TO_TOL = 50
 METRIC = ("CG-SENSE recons/s to 1e-4 rel. normal-equation residual "
-          "(plain CG; 2D radial 256^2, 16 coils, 96 spokes x 512, lambda 0.01)")
+          "(2D radial 256^2, 16 coils, 96 spokes x 512, lambda 0.01)")
+HEADLINE = "fcg_circulant"
 WORKLOAD = "cgsense2d_256_c16_s96_tol1e-4_toeplitz"
 DOMINANT = "cols_toeplitz"
 L2_FLUSH_BYTES = 512 << 20     # > 126 MB L2
@@ -377,27 +380,43 @@ def main():
     img_d = torch.empty(N_IMG * N_IMG, dtype=torch.complex64, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
-    conf = PicsConf(lam=LAM, maxiter=MAXITER, tol=TOL, toeplitz=True)
+    from bart_b200.precnet import PrecNet
+    net = PrecNet.load()
+    # the three solvers to 1e-4: the headline is the fastest, flexible CG
+    # with the circulant PSF preconditioner; plain CG is the reference's
+    # method, the learned correction is measured beside them
+    methods = {"cg": 0, "fcg_circulant": 1, "fcg_learned": 2}
+    confs = {k: PicsConf(lam=LAM, maxiter=MAXITER, tol=TOL, toeplitz=True, precond=v) for k, v in methods.items()}
+    conf = confs[HEADLINE]
 
     def make(c):
-        return Pics(traj_d, sens_d, ksp_dims=list(ksp.shape), conf=c, traj_dims=list(traj.shape),
-                    sens_dims=list(sens.shape))
+        p = Pics(traj_d, sens_d, ksp_dims=list(ksp.shape), conf=c, traj_dims=list(traj.shape),
+                 sens_dims=list(sens.shape))
+        if c.precond == 2:
+            p.set_precnet(net)
+        return p
 
     def step(c=conf):
         p = make(c)
         p.run(ksp_d, out=img_d)
         p.free()
 
-    for _ in range(max(3, args.warmup)):
-        step()
+    def solve_info(c):
+        """iterations, residuals and device kernels of one step (untimed)"""
+        p = make(c)
+        p.run(ksp_d, out=img_d)
+        it, rr, sc = p.stats()
+        kn = p.kernels()
+        tr = true_residual(dev, p, traj_d, sens_d, ksp_d, img_d, ksp.shape, traj.shape, sc)
+        p.free()
+        return it, rr, tr, kn
 
-    # iterations, residuals and device kernels of one step (untimed)
-    p = make(conf)
-    p.run(ksp_d, out=img_d)
-    iters, rres, scale = p.stats()
-    kernels_per_step = p.kernels()
-    tres = true_residual(dev, p, traj_d, sens_d, ksp_d, img_d, ksp.shape, traj.shape, scale)
-    p.free()
+    for c in confs.values():
+        for _ in range(max(3, args.warmup)):
+            step(c)
+
+    info = {k: solve_info(c) for k, c in confs.items()}
+    iters, rres, tres, kernels_per_step = info[HEADLINE]
 
     torch.cuda.synchronize()
     if world > 1:
@@ -408,11 +427,19 @@ def main():
     if world > 1:
         dist.barrier()
 
+    # the other methods, same steps
+    method_lines = {}
+    for k, c in confs.items():
+        mms = ms if k == HEADLINE else timed_steps(lambda: step(c), args.steps, flush, stream)
+        it_k, rr_k, tr_k, _ = info[k]
+        method_lines[k] = {"recons_per_s": args.steps / (mms / 1e3), "ms_per_recon": mms / args.steps,
+                           "iterations": it_k, "recursive_rel_residual": rr_k, "true_rel_residual": tr_k}
+
     # dominant kernel: per-launch CUDA events over the same steps, run again
     # with the CG loop launched from the host (events cannot sit inside the
     # graph's while body) for exactly the iterations the solve took, so the
     # same kernels run on the same inputs
-    conf_prof = PicsConf(lam=LAM, maxiter=iters, tol=0.0, toeplitz=True)
+    conf_prof = PicsConf(lam=LAM, maxiter=iters, tol=0.0, toeplitz=True, precond=methods[HEADLINE])
     lib.bnufft_prof_start(DOMINANT.encode())
     timed_steps(lambda: step(conf_prof), args.steps, flush, stream)
     kms, kn = ctypes.c_double(), ctypes.c_long()
@@ -480,14 +507,17 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "image": N_IMG, "coils": COILS, "spokes": SPOKES, "samples": 512,
                            "tol": TOL, "maxiter": MAXITER, "lambda": LAM, "toeplitz": True,
+                           "method": "flexible CG with the circulant PSF preconditioner (same normal equations "
+                                     "and tolerance as the reference's plain-CG pics)",
                            "parallelism": f"replicas{world}",
                            "l2": "flushed before every timed step (512 MB write); inside a step the ~60 MB "
                                  "working set stays L2-resident across CG iterations"},
                 "e2e": {"value": aggregate_rate(world, e2e_steps, e2e_s), "unit": "recons/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": kernels_per_step * args.steps,
-                "cg": {"iterations": iters, "recursive_rel_residual": rres, "true_rel_residual": tres,
-                       "loop": "one CUDA graph with a while node per solve"},
+                "cg": {"method": HEADLINE, "iterations": iters, "recursive_rel_residual": rres,
+                       "true_rel_residual": tres, "loop": "one CUDA graph with a while node per solve"},
+                "methods": method_lines,
                 "fixed_30_iters": fixed,
                 "nufft": nufft,
                 "roofline": {"bound": "hbm", "kernel": DOMINANT, "achieved": achieved, "peak": peak,
@@ -499,7 +529,7 @@ def main():
                                        "for the solve's iteration count"},
                 "clocks": clk.summary()}
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(traj, sens, ksp, iters)
+            line["cpu_baseline"] = cpu_baseline(traj, sens, ksp, method_lines["cg"]["iterations"])
         print(json.dumps(line), flush=True)
 
     if world > 1:

@@ -211,7 +211,9 @@ long bnufft_launch_count(void);
 
 /* Instrumentation (no counterpart in the reference): time every launch of
  * one kernel class ("rows_fwd", "cols_fwd", "cols_inv", "cols_toeplitz",
- * "rows_inv", "degrid", "grid") with CUDA events on its stream until
+ * "rows_inv", "degrid", "grid"; the passes of the circulant preconditioner
+ * as "precond_rows_fwd", "precond_cols_toeplitz", "precond_rows_inv") with
+ * CUDA events on its stream until
  * bnufft_prof_stop(), which returns the summed device time and launch count. */
 int bnufft_prof_start(const char* kind);
 int bnufft_prof_stop(double* total_ms, long* launches);
