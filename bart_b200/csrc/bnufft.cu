@@ -1001,15 +1001,23 @@ static int build_bins(OpCtx& op, cudaStream_t st)
 	CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, counts, bin_start, (int)(nbins + 1), st));
 	g_launches.fetch_add(2, std::memory_order_relaxed);
 
-	// sub-blocks per bin: ceil(count / BIN_SUB); their start indices
-	k_bin_nsub<<<vec_blocks(nbins + 1), RED_THREADS, 0, st>>>(bin_start, (int)nbins, nsub);
+	// sub-blocks per bin: ceil(count / sub); their start indices. A
+	// sub-block is one block of the tile scatter, which clears and flushes
+	// its tile once: large sub-blocks amortise that, small ones balance the
+	// dense bins at the k-space centre
+	int sub = BIN_SUB;
+
+	if (const char* e = getenv("BNUFFT_GRID_SUB"))
+		sub = std::max(64, std::min(1 << 20, atoi(e)));
+
+	k_bin_nsub<<<vec_blocks(nbins + 1), RED_THREADS, 0, st>>>(bin_start, (int)nbins, sub, nsub);
 	LAUNCHED();
 	CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, nsub, sub_start, (int)(nbins + 1), st));
 	g_launches.fetch_add(1, std::memory_order_relaxed);
 
 	// the number of sub-blocks stays on the device (no host round trip);
 	// launches use the upper bound nbins + M / BIN_SUB and surplus blocks exit
-	long total = nbins + M / BIN_SUB + 1;
+	long total = nbins + M / sub + 1;
 	b.nsub = (int)total;
 	b.sub_start = sub_start;
 	b.nsub_dev = sub_start + nbins;
@@ -1017,7 +1025,7 @@ static int build_bins(OpCtx& op, cudaStream_t st)
 	CUDA_TRY(cudaMallocAsync(&b.sub_bin, sizeof(int) * total, st));
 	CUDA_TRY(cudaMallocAsync(&b.sub_first, sizeof(int) * total, st));
 	CUDA_TRY(cudaMallocAsync(&b.sub_count, sizeof(int) * total, st));
-	k_sub_fill<<<vec_blocks(nbins), RED_THREADS, 0, st>>>(bin_start, sub_start, (int)nbins, b.sub_bin, b.sub_first, b.sub_count);
+	k_sub_fill<<<vec_blocks(nbins), RED_THREADS, 0, st>>>(bin_start, sub_start, (int)nbins, sub, b.sub_bin, b.sub_first, b.sub_count);
 	LAUNCHED();
 	k_gather_traj<<<vec_blocks(M), RED_THREADS, 0, st>>>(b.traj, op.traj, b.perm, M);
 	LAUNCHED();

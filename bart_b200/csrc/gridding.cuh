@@ -73,16 +73,16 @@ __global__ void k_bin_keys(const float4* __restrict__ traj, long M, GridGeom g, 
 	}
 }
 
-// nsub[b] = ceil(count_b / SUB), nsub[nbins] = 0
-__global__ void k_bin_nsub(const int* __restrict__ bin_start, int nbins, int* __restrict__ nsub)
+// nsub[b] = ceil(count_b / sub), nsub[nbins] = 0
+__global__ void k_bin_nsub(const int* __restrict__ bin_start, int nbins, int sub, int* __restrict__ nsub)
 {
 	for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= nbins; b += gridDim.x * blockDim.x)
-		nsub[b] = (b < nbins) ? (bin_start[b + 1] - bin_start[b] + BIN_SUB - 1) / BIN_SUB : 0;
+		nsub[b] = (b < nbins) ? (bin_start[b + 1] - bin_start[b] + sub - 1) / sub : 0;
 }
 
 // sub-block table: for bin b with n samples starting at bin_start[b],
-// ceil(n / SUB) entries (bin, first sample, count) starting at sub_start[b]
-__global__ void k_sub_fill(const int* __restrict__ bin_start, const int* __restrict__ sub_start, int nbins,
+// ceil(n / sub) entries (bin, first sample, count) starting at sub_start[b]
+__global__ void k_sub_fill(const int* __restrict__ bin_start, const int* __restrict__ sub_start, int nbins, int sub,
 		int* __restrict__ sub_bin, int* __restrict__ sub_first, int* __restrict__ sub_count)
 {
 	for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbins; b += gridDim.x * blockDim.x) {
@@ -90,11 +90,11 @@ __global__ void k_sub_fill(const int* __restrict__ bin_start, const int* __restr
 		int n = bin_start[b + 1] - bin_start[b];
 		int s0 = sub_start[b];
 
-		for (int j = 0; j * BIN_SUB < n; j++) {
+		for (int j = 0; j * sub < n; j++) {
 
 			sub_bin[s0 + j] = b;
-			sub_first[s0 + j] = bin_start[b] + j * BIN_SUB;
-			sub_count[s0 + j] = min(BIN_SUB, n - j * BIN_SUB);
+			sub_first[s0 + j] = bin_start[b] + j * sub;
+			sub_count[s0 + j] = min(sub, n - j * sub);
 		}
 	}
 }
