@@ -8,6 +8,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <complex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -283,7 +284,9 @@ static int get_kb_table(float os, float width, const float** out)
 // FFT pass launchers
 // ----------------------------------------------------------------------------
 
-static bool supported_len(int L) { return (L >= 16) && (L <= 2048) && (0 == (L & (L - 1))); }
+// grid lengths with a DFT: powers of two up to 4096, other lengths up to 2048
+// (Bluestein on a power-of-two FFT of at most 4096)
+static bool supported_len(int L) { return (L >= 2) && ((L <= 2048) || ((L <= 4096) && (0 == (L & (L - 1))))); }
 
 // dynamic shared memory of a column pass (ColLayout) / row pass (RowLayout), twiddles included
 static size_t pass_smem(int L, int B) { return sizeof(float2) * (size_t)L * (size_t)(smem_stride(B) + 1); }
@@ -336,14 +339,14 @@ static int prep_kernel(K kernel, size_t smem)
 
 template <int L, int B>
 static int launch_rows_fwd_LB(const float2* img, const float2* maps, const float* ax, const float* ayz,
-		int X, long YZ, long R, float2* out, cudaStream_t st, const int* done)
+		int X, long YZ, long R, float2* out, cudaStream_t st, const int* done, const Dft& d)
 {
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
 	size_t smem = rows_smem(L, B);
 	TRY(prep_kernel(k_rows_fwd<L, B>, smem));
 	cudaEvent_t pe = prof_begin("rows_fwd", st);
-	k_rows_fwd<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(img, maps, ax, ayz, X, YZ, R, out, tw, done);
+	k_rows_fwd<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(img, maps, ax, ayz, X, YZ, R, out, tw, done, d);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
@@ -352,7 +355,7 @@ static int launch_rows_fwd_LB(const float2* img, const float2* maps, const float
 template <int L, int B, int MODE>
 static int launch_cols_LB(const float2* in, long ies, long ios, int n_in, int wrap_in,
 		float2* out, long oes, long oos, int n_out, int wrap_out, int W, long O,
-		const float2* psf, long pes, long pmod, long pos, const int* done, cudaStream_t st)
+		const float2* psf, long pes, long pmod, long pos, const int* done, cudaStream_t st, const Dft& d)
 {
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
@@ -365,7 +368,7 @@ static int launch_cols_LB(const float2* in, long ies, long ios, int n_in, int wr
 	dim3 grid((unsigned)((W + B - 1) / B), (unsigned)O);
 	cudaEvent_t pe = prof_begin((2 == MODE) ? "cols_toeplitz" : ((1 == MODE) ? "cols_inv" : "cols_fwd"), st);
 	k_cols<L, B, MODE><<<grid, B * L / 8, smem, st>>>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out,
-			W, psf, pes, pmod, pos, tw, done);
+			W, psf, pes, pmod, pos, tw, done, d);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
@@ -374,7 +377,7 @@ static int launch_cols_LB(const float2* in, long ies, long ios, int n_in, int wr
 template <int L, int B>
 static int launch_rows_inv_LB(const float2* in, const float2* maps, const float* ax, const float* ayz,
 		int X, long YZ, int C, int cpg, float2* out, const float2* pdot, double* dot_part, const int* done,
-		cudaStream_t st)
+		cudaStream_t st, const Dft& d)
 {
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
@@ -383,7 +386,7 @@ static int launch_rows_inv_LB(const float2* in, const float2* maps, const float*
 	TRY(prep_kernel(k_rows_inv<L, B>, smem));
 	dim3 grid((unsigned)((YZ + B - 1) / B), (unsigned)groups);
 	cudaEvent_t pe = prof_begin("rows_inv", st);
-	k_rows_inv<L, B><<<grid, B * L / 8, smem, st>>>(in, maps, ax, ayz, X, YZ, C, cpg, out, tw, pdot, dot_part, done);
+	k_rows_inv<L, B><<<grid, B * L / 8, smem, st>>>(in, maps, ax, ayz, X, YZ, C, cpg, out, tw, pdot, dot_part, done, d);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
@@ -392,7 +395,7 @@ static int launch_rows_inv_LB(const float2* in, const float2* maps, const float*
 template <int L, int B>
 static int launch_rows_fwd_cg_LB(const float2* bvec, const float2* r, const float2* p_prev, float2* p_cur,
 		const float2* maps, const float* ax, const float* ayz, int X, long YZ, long R, float2* out,
-		CgScalars* stt, int it, const double* rs_part, int nrs, double* pp_part, cudaStream_t st)
+		CgScalars* stt, int it, const double* rs_part, int nrs, double* pp_part, cudaStream_t st, const Dft& d)
 {
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
@@ -400,7 +403,7 @@ static int launch_rows_fwd_cg_LB(const float2* bvec, const float2* r, const floa
 	TRY(prep_kernel(k_rows_fwd_cg<L, B>, smem));
 	cudaEvent_t pe = prof_begin("rows_fwd", st);
 	k_rows_fwd_cg<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(bvec, r, p_prev, p_cur, maps, ax, ayz,
-			X, YZ, R, out, tw, stt, it, rs_part, nrs, pp_part);
+			X, YZ, R, out, tw, stt, it, rs_part, nrs, pp_part, d);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
@@ -417,61 +420,196 @@ static int launch_rows_fwd_cg_LB(const float2* bvec, const float2* r, const floa
 	case 512: { constexpr int LL = 512; DISPATCH_B(B, CALL) } \
 	case 1024: { constexpr int LL = 1024; DISPATCH_B(B, CALL) } \
 	case 2048: { constexpr int LL = 2048; DISPATCH_B(B, CALL) } \
-	default: return fail(BNUFFT_ERR_UNSUPPORTED, "FFT length %d (powers of two 16..2048 are built)", L); }
+	case 4096: { constexpr int LL = 4096; DISPATCH_B(B, CALL) } \
+	default: return fail(BNUFFT_ERR_UNSUPPORTED, "FFT length %d (powers of two 16..4096 are built)", L); }
 
 #define DISPATCH_B(B, CALL) \
 	switch (B) { \
+	case 2: { constexpr int BB = 2; if constexpr (LL >= 4096 && BB * LL / 8 <= 1024) return CALL; break; } \
 	case 4: { constexpr int BB = 4; if constexpr (BB * LL / 8 <= 1024 && BB * LL / 8 >= 32) return CALL; break; } \
 	case 8: { constexpr int BB = 8; if constexpr (BB * LL / 8 <= 1024 && BB * LL / 8 >= 32) return CALL; break; } \
 	case 16: { constexpr int BB = 16; if constexpr (BB * LL / 8 <= 1024 && BB * LL / 8 >= 32) return CALL; break; } \
 	} \
 	return fail(BNUFFT_ERR_ARG, "no FFT pass instance for L=%d B=%d", L, B);
 
-static int rows_fwd(int L, const float2* img, const float2* maps, const float* ax, const float* ayz,
-		int X, long YZ, long R, float2* out, cudaStream_t st, const int* done = nullptr)
+// DFT of logical length n: the power-of-two FFT of length n itself, or
+// Bluestein's algorithm on the power-of-two length P >= 2n - 1 with its
+// chirp and filter tables (computed once per device and length on the host
+// in float64: chirp exp(-i pi (j^2 mod 2n) / n), filters by a float64 FFT)
+struct DftTables {
+
+	int P = 0;
+	float2 *chirp = nullptr, *bf = nullptr, *bi = nullptr;
+};
+
+static std::mutex g_dft_mutex;
+static std::map<std::pair<int, int>, DftTables> g_dft;
+
+static void fft_host(std::vector<std::complex<double>>& a)	// in place, forward, unnormalised
 {
-	int B = choose_B(L, R);
-	DISPATCH_LB(L, B, (launch_rows_fwd_LB<LL, BB>(img, maps, ax, ayz, X, YZ, R, out, st, done)));
+	const size_t n = a.size();
+
+	for (size_t i = 1, j = 0; i < n; i++) {
+
+		size_t bit = n >> 1;
+
+		for (; j & bit; bit >>= 1)
+			j ^= bit;
+
+		j ^= bit;
+
+		if (i < j)
+			std::swap(a[i], a[j]);
+	}
+
+	for (size_t len = 2; len <= n; len <<= 1) {
+
+		for (size_t i = 0; i < n; i += len) {
+
+			for (size_t k = 0; k < len / 2; k++) {
+
+				double ang = -2. * M_PI * (double)k / (double)len;
+				std::complex<double> w(cos(ang), sin(ang));
+				std::complex<double> u = a[i + k];
+				std::complex<double> v = a[i + k + len / 2] * w;
+				a[i + k] = u + v;
+				a[i + k + len / 2] = u - v;
+			}
+		}
+	}
 }
 
-static int cols(int L, int mode, const float2* in, long ies, long ios, int n_in, int wrap_in,
+static int get_dft(int n, Dft* d, int* P)
+{
+	d->n = n;
+	d->chirp = d->bf = d->bi = nullptr;
+
+	if ((n >= 16) && (n <= 4096) && (0 == (n & (n - 1)))) {
+
+		*P = n;
+		return BNUFFT_OK;
+	}
+
+	int p = 16;
+
+	while (p < 2 * n - 1)
+		p *= 2;
+
+	if ((n < 2) || (p > 4096))
+		return fail(BNUFFT_ERR_UNSUPPORTED, "DFT length %d (powers of two up to 4096, other lengths up to 2048)", n);
+
+	int dev;
+	CUDA_TRY(cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lock(g_dft_mutex);
+	DftTables& t = g_dft[std::make_pair(dev, n)];
+
+	if (!t.P) {
+
+		std::vector<std::complex<double>> c(n), bf(p), bi(p);
+
+		for (long j = 0; j < n; j++) {
+
+			double ang = -M_PI * (double)((j * j) % (2L * n)) / (double)n;
+			c[j] = std::complex<double>(cos(ang), sin(ang));
+		}
+
+		for (long m = -(n - 1); m <= n - 1; m++) {
+
+			const std::complex<double>& cm = c[(m < 0) ? -m : m];	// c_m = c_{-m}
+			bf[(m + p) % p] = std::conj(cm);
+			bi[(m + p) % p] = cm;
+		}
+
+		fft_host(bf);
+		fft_host(bi);
+		std::vector<float2> hc(n), hf(p), hi(p);
+
+		for (int j = 0; j < n; j++)
+			hc[j] = make_float2((float)c[j].real(), (float)c[j].imag());
+
+		for (int j = 0; j < p; j++) {
+
+			hf[j] = make_float2((float)(bf[j].real() / p), (float)(bf[j].imag() / p));
+			hi[j] = make_float2((float)(bi[j].real() / p), (float)(bi[j].imag() / p));
+		}
+
+		DftTables nt;
+		CUDA_TRY(cudaMalloc(&nt.chirp, sizeof(float2) * n));
+		CUDA_TRY(cudaMalloc(&nt.bf, sizeof(float2) * p));
+		CUDA_TRY(cudaMalloc(&nt.bi, sizeof(float2) * p));
+		CUDA_TRY(cudaMemcpy(nt.chirp, hc.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+		CUDA_TRY(cudaMemcpy(nt.bf, hf.data(), sizeof(float2) * p, cudaMemcpyHostToDevice));
+		CUDA_TRY(cudaMemcpy(nt.bi, hi.data(), sizeof(float2) * p, cudaMemcpyHostToDevice));
+		nt.P = p;
+		t = nt;
+	}
+
+	d->chirp = t.chirp;
+	d->bf = t.bf;
+	d->bi = t.bi;
+	*P = t.P;
+	return BNUFFT_OK;
+}
+
+// The passes below take the logical DFT length n (the grid length) and run
+// the power-of-two FFT of length P (n itself or Bluestein's)
+static int rows_fwd(int n, const float2* img, const float2* maps, const float* ax, const float* ayz,
+		int X, long YZ, long R, float2* out, cudaStream_t st, const int* done = nullptr)
+{
+	Dft d;
+	int L;
+	TRY(get_dft(n, &d, &L));
+	int B = choose_B(L, R);
+	DISPATCH_LB(L, B, (launch_rows_fwd_LB<LL, BB>(img, maps, ax, ayz, X, YZ, R, out, st, done, d)));
+}
+
+static int cols(int n, int mode, const float2* in, long ies, long ios, int n_in, int wrap_in,
 		float2* out, long oes, long oos, int n_out, int wrap_out, int W, long O,
 		const float2* psf, long pes, long pmod, long pos, cudaStream_t st, const int* done = nullptr)
 {
+	Dft d;
+	int L;
+	TRY(get_dft(n, &d, &L));
 	int B = choose_B(L, (long)W * O);
 
 	while ((B > std::max(4, 256 / L)) && (B > W))
 		B /= 2;
 
 	if (0 == mode)
-		DISPATCH_LB(L, B, (launch_cols_LB<LL, BB, 0>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, done, st)))
+		DISPATCH_LB(L, B, (launch_cols_LB<LL, BB, 0>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, done, st, d)))
 	else if (1 == mode)
-		DISPATCH_LB(L, B, (launch_cols_LB<LL, BB, 1>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, done, st)))
+		DISPATCH_LB(L, B, (launch_cols_LB<LL, BB, 1>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, done, st, d)))
 	else
-		DISPATCH_LB(L, B, (launch_cols_LB<LL, BB, 2>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, done, st)))
+		DISPATCH_LB(L, B, (launch_cols_LB<LL, BB, 2>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, done, st, d)))
 }
 
-static int rows_inv(int L, const float2* in, const float2* maps, const float* ax, const float* ayz,
+static int rows_inv(int n, const float2* in, const float2* maps, const float* ax, const float* ayz,
 		int X, long YZ, int C, int cpg, float2* out, cudaStream_t st,
 		const float2* pdot = nullptr, double* dot_part = nullptr, const int* done = nullptr, int* nblocks = nullptr)
 {
+	Dft d;
+	int L;
+	TRY(get_dft(n, &d, &L));
 	int groups = (C + cpg - 1) / cpg;
 	int B = choose_B(L, YZ * groups);
 
 	if (nblocks)
 		*nblocks = (int)(((YZ + B - 1) / B) * groups);
 
-	DISPATCH_LB(L, B, (launch_rows_inv_LB<LL, BB>(in, maps, ax, ayz, X, YZ, C, cpg, out, pdot, dot_part, done, st)));
+	DISPATCH_LB(L, B, (launch_rows_inv_LB<LL, BB>(in, maps, ax, ayz, X, YZ, C, cpg, out, pdot, dot_part, done, st, d)));
 }
 
-static int rows_fwd_cg(int L, const float2* bvec, const float2* r, const float2* p_prev, float2* p_cur,
+static int rows_fwd_cg(int n, const float2* bvec, const float2* r, const float2* p_prev, float2* p_cur,
 		const float2* maps, const float* ax, const float* ayz, int X, long YZ, long R, float2* out,
 		CgScalars* stt, int it, const double* rs_part, int nrs, double* pp_part, int* nblocks, cudaStream_t st)
 {
+	Dft d;
+	int L;
+	TRY(get_dft(n, &d, &L));
 	int B = choose_B(L, R);
 	*nblocks = (int)((R + B - 1) / B);
 	DISPATCH_LB(L, B, (launch_rows_fwd_cg_LB<LL, BB>(bvec, r, p_prev, p_cur, maps, ax, ayz, X, YZ, R, out,
-			stt, it, rs_part, nrs, pp_part, st)));
+			stt, it, rs_part, nrs, pp_part, st, d)));
 }
 
 static unsigned vec_blocks(long n, int threads = RED_THREADS, int maxb = 4 * 148)
@@ -2892,7 +3030,7 @@ static int na_rows(const float2* img, const float* ax, const float* ayz, int X, 
 	constexpr int B = 16;
 	size_t smem = rows_smem(L, B);
 	CUDA_TRY(cudaFuncSetAttribute(k_rows_fwd<L, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-	k_rows_fwd<L, B><<<(unsigned)((Y + B - 1) / B), B * L / 8, smem, st>>>(img, nullptr, ax, ayz, X, Y, Y, out, tw, nullptr);
+	k_rows_fwd<L, B><<<(unsigned)((Y + B - 1) / B), B * L / 8, smem, st>>>(img, nullptr, ax, ayz, X, Y, Y, out, tw, nullptr, Dft{L, nullptr, nullptr, nullptr});
 	LAUNCHED();
 	return BNUFFT_OK;
 }
@@ -2905,7 +3043,7 @@ static int na_cols(const float2* t1, int G0, int Y, float2* grid, const float2* 
 	CUDA_TRY(cudaFuncSetAttribute(k_cols<L, B, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
 	dim3 grid_dim((unsigned)((G0 + B - 1) / B), 1);
 	k_cols<L, B, 0><<<grid_dim, B * L / 8, smem, st>>>(t1, G0, (long)G0 * Y, Y, 1, grid, G0, (long)G0 * L, L, 0,
-			G0, nullptr, 0, 1, 0, tw, nullptr);
+			G0, nullptr, 0, 1, 0, tw, nullptr, Dft{L, nullptr, nullptr, nullptr});
 	LAUNCHED();
 	return BNUFFT_OK;
 }

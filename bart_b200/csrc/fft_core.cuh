@@ -1,6 +1,6 @@
 // Shared-memory Stockham FFT core for sm_100a.
 //
-// A thread block transforms B sequences of length L (power of two, 16..2048).
+// A thread block transforms B sequences of length L (power of two, 16..4096).
 // Each sequence is served by T = L/8 threads (index jt). Between stages the
 // data lives in shared memory in one of two layouts (ColLayout for column
 // passes, RowLayout for row passes; see below), chosen so that both the
@@ -213,7 +213,7 @@ __device__ __forceinline__ void fft_tail(float2 (&v)[8], float2* s, int b, int j
 template <int L, typename LAY, bool INV>
 __device__ __forceinline__ void fft_regs(float2 (&v)[8], float2* s, const float2* tw)
 {
-	static_assert(L >= 16 && L <= 2048 && (L & (L - 1)) == 0, "power-of-two length 16..2048");
+	static_assert(L >= 16 && L <= 4096 && (L & (L - 1)) == 0, "power-of-two length 16..4096");
 	const int b = LAY::seq();
 	const int jt = LAY::jt();
 

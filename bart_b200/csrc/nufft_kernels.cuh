@@ -21,6 +21,59 @@ namespace bn {
 
 enum { KB_TABLE_N = 1000 };	// kb_size_max, src/noncart/grid.c:38
 
+// A DFT of logical length n run on the power-of-two FFT of the kernel's
+// template length L. n == L: the FFT itself. n < L (any n with 2n - 1 <= L):
+// Bluestein's chirp-z algorithm (IEEE Trans. Audio Electroacoust. 18(4),
+// 1970): with c_j = exp(-i pi j^2 / n), the forward DFT is
+//   X_k = c_k sum_j (x_j c_j) conj(c_{k-j}),
+// a linear convolution computed as a length-L circular one:
+//   X = c . IFFT_L(FFT_L(c . x) . bf),  bf = FFT_L(conj(c) wrapped) / L,
+// and the inverse DFT the same with conj(c) and bi = FFT_L(c wrapped) / L.
+// Positions j >= n hold zeros before and after.
+struct Dft {
+
+	int n;			// logical length
+	const float2* chirp;	// [n] c_j (Bluestein only)
+	const float2* bf;	// [L] forward filter spectrum / L
+	const float2* bi;	// [L] inverse filter spectrum / L
+};
+
+// DFT of the register set v (positions reg_pos(m), see fft_regs); for
+// Bluestein the caller has loaded zeros at positions >= d.n and gets zeros
+// there back. Same barrier contract as fft_regs.
+template <int L, typename LAY, bool INV>
+__device__ __forceinline__ void dft_regs(float2 (&v)[8], float2* s, const float2* tw, const Dft& d)
+{
+	if (d.n == L) {
+
+		fft_regs<L, LAY, INV>(v, s, tw);
+		return;
+	}
+
+#pragma unroll
+	for (int m = 0; m < 8; m++) {
+
+		int p = reg_pos<L, LAY>(m);
+		float2 c = (p < d.n) ? d.chirp[p] : make_float2(0.f, 0.f);
+		v[m] = INV ? cmulc(v[m], c) : cmul(v[m], c);
+	}
+
+	fft_regs<L, LAY, false>(v, s, tw);
+	const float2* b = INV ? d.bi : d.bf;
+#pragma unroll
+	for (int m = 0; m < 8; m++)
+		v[m] = cmul(v[m], b[reg_pos<L, LAY>(m)]);
+
+	fft_regs<L, LAY, true>(v, s, tw);
+#pragma unroll
+	for (int m = 0; m < 8; m++) {
+
+		int p = reg_pos<L, LAY>(m);
+		float2 c = (p < d.n) ? d.chirp[p] : make_float2(0.f, 0.f);
+		v[m] = INV ? cmulc(v[m], c) : cmul(v[m], c);
+	}
+}
+
 // Element layouts ------------------------------------------------------------
 
 // smem element stride for B sequences: odd, so 8-byte accesses of a
@@ -131,7 +184,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		const float2* __restrict__ p_prev, float2* __restrict__ p_cur, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
 		int X, long YZ, long R, float2* __restrict__ out, const float2* __restrict__ twg,
-		CgScalars* st, int it, const double* __restrict__ rs_part, int nrs, double* __restrict__ pp_part)
+		CgScalars* st, int it, const double* __restrict__ rs_part, int nrs, double* __restrict__ pp_part, Dft d)
 {
 	using LAY = RowLayout<L, B>;
 	constexpr int NT = B * L / 8;
@@ -182,7 +235,8 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 #pragma unroll
 	for (int m = 0; m < 8; m++) {
 
-		int n = unwrap_pos(reg_pos<L, LAY>(m), X, L);
+		int p = reg_pos<L, LAY>(m);
+		int n = (p < d.n) ? unwrap_pos(p, X, d.n) : X;
 		v[m] = make_float2(0.f, 0.f);
 
 		if (valid && (n < X)) {
@@ -218,12 +272,17 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 	if (0 == threadIdx.x)
 		pp_part[blockIdx.x] = t;
 
-	fft_regs<L, LAY, false>(v, s, tw);
+	dft_regs<L, LAY, false>(v, s, tw, d);
 
 	if (valid) {
 #pragma unroll
-		for (int m = 0; m < 8; m++)
-			out[reg_pos<L, LAY>(m) + (long)L * row] = v[m];
+		for (int m = 0; m < 8; m++) {
+
+			int p = reg_pos<L, LAY>(m);
+
+			if (p < d.n)
+				out[p + (long)d.n * row] = v[m];
+		}
 	}
 }
 
@@ -238,7 +297,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 template <int L, int B>
 __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_rows_fwd(const float2* __restrict__ img, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
-		int X, long YZ, long R, float2* __restrict__ out, const float2* __restrict__ twg, const int* done)
+		int X, long YZ, long R, float2* __restrict__ out, const float2* __restrict__ twg, const int* done, Dft d)
 {
 	using LAY = RowLayout<L, B>;
 	constexpr int NT = B * L / 8;
@@ -261,7 +320,8 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 #pragma unroll
 	for (int m = 0; m < 8; m++) {
 
-		int n = unwrap_pos(reg_pos<L, LAY>(m), X, L);
+		int p = reg_pos<L, LAY>(m);
+		int n = (p < d.n) ? unwrap_pos(p, X, d.n) : X;
 		v[m] = make_float2(0.f, 0.f);
 
 		if (valid && (n < X)) {
@@ -272,12 +332,17 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		}
 	}
 
-	fft_regs<L, LAY, false>(v, s, tw);
+	dft_regs<L, LAY, false>(v, s, tw, d);
 
 	if (valid) {
 #pragma unroll
-		for (int m = 0; m < 8; m++)
-			out[reg_pos<L, LAY>(m) + (long)L * row] = v[m];
+		for (int m = 0; m < 8; m++) {
+
+			int p = reg_pos<L, LAY>(m);
+
+			if (p < d.n)
+				out[p + (long)d.n * row] = v[m];
+		}
 	}
 }
 
@@ -297,7 +362,7 @@ template <int L, int B, int MODE>
 __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_cols(const float2* __restrict__ in, long ies, long ios, int n_in, int wrap_in,
 		float2* __restrict__ out, long oes, long oos, int n_out, int wrap_out,
 		int W, const float2* __restrict__ psf, long pes, long pmod, long pos,
-		const float2* __restrict__ twg, const int* done)
+		const float2* __restrict__ twg, const int* done, Dft d)
 {
 	using LAY = ColLayout<L, B>;
 	constexpr int NT = B * L / 8;
@@ -321,29 +386,33 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 	for (int m = 0; m < 8; m++) {
 
 		int p = reg_pos<L, LAY>(m);
-		int n = wrap_in ? unwrap_pos(p, n_in, L) : p;
+		int n = (p >= d.n) ? n_in : (wrap_in ? unwrap_pos(p, n_in, d.n) : p);
 		v[m] = (valid && (n < n_in)) ? inp[n * ies] : make_float2(0.f, 0.f);
 	}
 
 	// the twiddle table must be complete before the first stage reads it
 	if constexpr (MODE == 1) {
 
-		fft_regs<L, LAY, true>(v, s, tw);
+		dft_regs<L, LAY, true>(v, s, tw, d);
 
 	} else {
 
-		fft_regs<L, LAY, false>(v, s, tw);
+		dft_regs<L, LAY, false>(v, s, tw, d);
 	}
 
 	if constexpr (MODE == 2) {
 
 		const float2* pp = psf + (o % pmod) * pos + cx;
 #pragma unroll
-		for (int m = 0; m < 8; m++)
-			if (valid)
-				v[m] = cmul(v[m], pp[reg_pos<L, LAY>(m) * pes]);
+		for (int m = 0; m < 8; m++) {
 
-		fft_regs<L, LAY, true>(v, s, tw);
+			int p = reg_pos<L, LAY>(m);
+
+			if (valid && (p < d.n))
+				v[m] = cmul(v[m], pp[p * pes]);
+		}
+
+		dft_regs<L, LAY, true>(v, s, tw, d);
 	}
 
 	float2* outp = out + o * oos + cx;
@@ -353,7 +422,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		for (int m = 0; m < 8; m++) {
 
 			int p = reg_pos<L, LAY>(m);
-			int n = wrap_out ? unwrap_pos(p, n_out, L) : p;
+			int n = (p >= d.n) ? n_out : (wrap_out ? unwrap_pos(p, n_out, d.n) : p);
 
 			if (n < n_out)
 				outp[n * oes] = v[m];
@@ -375,7 +444,7 @@ template <int L, int B>
 __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_rows_inv(const float2* __restrict__ in, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
 		int X, long YZ, int C, int cpg, float2* __restrict__ out, const float2* __restrict__ twg,
-		const float2* __restrict__ pdot, double* __restrict__ dot_part, const int* done)
+		const float2* __restrict__ pdot, double* __restrict__ dot_part, const int* done, Dft d)
 {
 	using LAY = RowLayout<L, B>;
 	constexpr int NT = B * L / 8;
@@ -408,16 +477,20 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 
 		float2 v[8];
 #pragma unroll
-		for (int m = 0; m < 8; m++)
-			v[m] = valid ? in[reg_pos<L, LAY>(m) + (long)L * (yz + YZ * c)] : make_float2(0.f, 0.f);
+		for (int m = 0; m < 8; m++) {
 
-		fft_regs<L, LAY, true>(v, s, tw);
+			int p = reg_pos<L, LAY>(m);
+			v[m] = (valid && (p < d.n)) ? in[p + (long)d.n * (yz + YZ * c)] : make_float2(0.f, 0.f);
+		}
+
+		dft_regs<L, LAY, true>(v, s, tw, d);
 
 		if (valid) {
 #pragma unroll
 			for (int m = 0; m < 8; m++) {
 
-				int x = unwrap_pos(reg_pos<L, LAY>(m), X, L);
+				int p = reg_pos<L, LAY>(m);
+				int x = (p < d.n) ? unwrap_pos(p, X, d.n) : X;
 
 				if (x >= X)
 					continue;
@@ -451,7 +524,8 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 #pragma unroll
 			for (int m = 0; m < 8; m++) {
 
-				int x = unwrap_pos(reg_pos<L, LAY>(m), X, L);
+				int p = reg_pos<L, LAY>(m);
+				int x = (p < d.n) ? unwrap_pos(p, X, d.n) : X;
 
 				if (x >= X)
 					continue;

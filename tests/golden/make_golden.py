@@ -7,7 +7,8 @@ files next to this script. Only needed when the fixtures change; the tests
 read the .npz files and never run the reference.
 
     make -f oracle/refbuild/Makefile -j8
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # all fixtures
+    python tests/golden/make_golden.py --uneven   # only the non-power-of-two sizes
 """
 
 from __future__ import annotations
@@ -106,7 +107,22 @@ def pics_case(name, N, C, spokes, seed):
     print(name, {k: np.shape(v) for k, v in out.items()})
 
 
+def uneven_cases():
+    """Image sides that are not powers of two (grids of 2N cells)."""
+    rng = np.random.default_rng(20261204)
+    with tempfile.TemporaryDirectory() as d:
+        run("traj", "-r", "-G", "-x40", "-o2", "-y20", "t", cwd=d)
+        t40 = readcfl(os.path.join(d, "t"))
+    nufft_case("nufft2d_n40", t40, cplx(rng, (40, 40)))
+    nufft_case("nufft2d_n40_periodic", t40, cplx(rng, (40, 40)), periodic=True)
+    nufft_case("nufft3d_n12", synth.kooshball_traj(12, 64), cplx(rng, (12, 12, 12)))
+    pics_case("pics2d_n48_c3", 48, 3, 20, seed=9)
+
+
 def main():
+    if "--uneven" in sys.argv:
+        uneven_cases()
+        return
     rng = np.random.default_rng(20261203)
     with tempfile.TemporaryDirectory() as d:
         run("traj", "-r", "-G", "-x64", "-o2", "-y24", "t", cwd=d)
@@ -124,6 +140,7 @@ def main():
     pics_case("pics2d_n64_c4", 64, 4, 24, seed=7)
     g = np.load(os.path.join(HERE, "nufft2d_n32_coils3.npz"))
     inverse_case("inverse2d_n32_coils3", g["traj"], g["fwd"], (32, 32, 1))
+    uneven_cases()
 
 
 if __name__ == "__main__":

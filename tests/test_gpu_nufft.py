@@ -33,9 +33,13 @@ def _plan(g, periodic=False, toeplitz=True):
     return nufft_create2(kd, cd, td, g["traj"], wd, w, conf=NufftConf(toeplitz=toeplitz, periodic=periodic)), cd, kd
 
 
+# image sides that are not powers of two: grid DFTs by Bluestein's algorithm
+UNEVEN = [("nufft2d_n40", False), ("nufft2d_n40_periodic", True), ("nufft3d_n12", False)]
+
+
 @pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
                                            ("nufft3d_n16", False), ("nufft2d_n32_coils3", False),
-                                           ("nufft2d_n64_weights", False)])
+                                           ("nufft2d_n64_weights", False)] + UNEVEN)
 def test_forward_adjoint_vs_reference(name, periodic):
     g = golden(name)
     op, cd, kd = _plan(g, periodic, toeplitz=False)
@@ -47,7 +51,7 @@ def test_forward_adjoint_vs_reference(name, periodic):
 
 
 @pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
-                                           ("nufft3d_n16", False), ("nufft2d_n64_weights", False)])
+                                           ("nufft3d_n16", False), ("nufft2d_n64_weights", False)] + UNEVEN)
 def test_toeplitz_normal_and_psf_vs_reference(name, periodic):
     g = golden(name)
     op, cd, kd = _plan(g, periodic, toeplitz=True)
@@ -62,7 +66,8 @@ def test_toeplitz_normal_and_psf_vs_reference(name, periodic):
     op.free()
 
 
-@pytest.mark.parametrize("N,spokes,coils", [(128, 64, 1), (64, 40, 2), (256, 402, 1), (512, 100, 1)])
+@pytest.mark.parametrize("N,spokes,coils", [(128, 64, 1), (64, 40, 2), (256, 402, 1), (512, 100, 1),
+                                            (66, 30, 2), (200, 64, 1), (318, 90, 1), (320, 40, 2)])
 def test_2d_vs_oracle(N, spokes, coils):
     rng = np.random.default_rng(N + spokes)
     t = synth.radial_traj(N, spokes)

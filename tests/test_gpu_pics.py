@@ -20,8 +20,9 @@ def _run(g, **kw):
     return np.asarray(x), st
 
 
-def test_pics_5_iterations_vs_reference():
-    g = golden("pics2d_n64_c4")
+@pytest.mark.parametrize("name", ["pics2d_n64_c4", "pics2d_n48_c3"])
+def test_pics_5_iterations_vs_reference(name):
+    g = golden(name)
     x, st = _run(g, maxiter=5, scaling=1.0)
     assert st[0] == 5
     assert rel(x, g["x5_w1"]) < 1e-5
