@@ -18,13 +18,14 @@ c_long_p = ctypes.POINTER(ctypes.c_long)
 
 class NufftConfC(ctypes.Structure):
     _fields_ = [("toeplitz", ctypes.c_int), ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int),
-                ("os", ctypes.c_float), ("width", ctypes.c_float)]
+                ("os", ctypes.c_float), ("width", ctypes.c_float), ("bin", ctypes.c_int)]
 
 
 class PicsConfC(ctypes.Structure):
     _fields_ = [("lambda_", ctypes.c_float), ("maxiter", ctypes.c_int), ("tol", ctypes.c_float),
                 ("scaling", ctypes.c_float), ("rescale", ctypes.c_int), ("toeplitz", ctypes.c_int),
-                ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int), ("precond", ctypes.c_int)]
+                ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int), ("bin", ctypes.c_int),
+                ("precond", ctypes.c_int)]
 
 
 _lib = None
@@ -65,6 +66,11 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     sig("bnufft_pics_kernels", i, vp, ctypes.POINTER(ctypes.c_long), vp)
     sig("bnufft_pics_free", None, vp)
     sig("bnufft_pics_rhs", i, vp, vp, vp, vp)
+    sig("bnufft_batch_create", i, ctypes.POINTER(vp), ctypes.POINTER(vp), i, ctypes.POINTER(vp),
+        ctypes.POINTER(vp), vp)
+    sig("bnufft_batch_run", i, vp, vp)
+    sig("bnufft_batch_kernels", ctypes.c_long, vp)
+    sig("bnufft_batch_free", None, vp)
     sig("bnufft_pics_set_iter", i, vp, i, ctypes.c_float)
     sig("bnufft_pics_precond", i, vp, vp, vp, vp)
     sig("bnufft_pics_set_precnet", i, vp, vp, vp)

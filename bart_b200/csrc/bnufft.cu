@@ -669,6 +669,7 @@ struct Bins {
 struct OpCtx {
 
 	Geom g;
+	int bin_edge = 0;	// gridding bin edge (0: default)
 	const float4* traj;	// [M]
 	const float* kb;
 	float* ax = nullptr;	// [N0] roll-off along x
@@ -1090,7 +1091,7 @@ static int build_bins(OpCtx& op, cudaStream_t st)
 	const Geom& g = op.g;
 	Bins& b = op.bins;
 	BinGeom& bg = b.bg;
-	const int bs_axis = (g.G[2] > 1) ? 16 : 32;
+	const int bs_axis = op.bin_edge ? op.bin_edge : ((g.G[2] > 1) ? 16 : 32);
 	long nbins = 1;
 	bg.ncells = 1;
 
@@ -1254,9 +1255,10 @@ static int op_toeplitz(OpCtx& op, const float2* psf, const float2* x, const floa
 // psft = adjoint NUFFT of ones with trajectory 2*traj onto the 2N image,
 // periodic gridding; psf = fftuc(psft) / npix.
 static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, float2** psf_out, cudaStream_t st,
-		bool deterministic, const float2* wgt)
+		bool deterministic, const float2* wgt, int bin_edge)
 {
 	OpCtx in;
+	in.bin_edge = bin_edge;
 	long d2[3] = { g.G[0], g.G[1], g.G[2] };
 	TRY(init_geom(in.g, d2, g.M, g.os, g.width, 1));
 
@@ -1441,10 +1443,14 @@ extern "C" void bnufft_conf_defaults(struct bnufft_conf* conf)
 	conf->deterministic = 0;
 	conf->os = 2.f;
 	conf->width = 6.f;
+	conf->bin = 0;
 }
 
 static int check_conf(const bnufft_conf* conf)
 {
+	if ((0 != conf->bin) && ((conf->bin < 8) || (conf->bin > 128) || (0 != (conf->bin & (conf->bin - 1)))))
+		return fail(BNUFFT_ERR_ARG, "bin edge %d (0 or a power of two 8..128)", conf->bin);
+
 	if (2.f != conf->os)
 		return fail(BNUFFT_ERR_UNSUPPORTED, "oversampling %g (os = 2 is built; the reference chains other os)", conf->os);
 
@@ -1476,7 +1482,8 @@ static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
 			cudaFreeAsync(p->psf, st);
 
 		p->psf = nullptr;
-		TRY(compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, st, 0 != p->conf.deterministic, p->op.wgt));
+		TRY(compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, st, 0 != p->conf.deterministic, p->op.wgt,
+				p->op.bin_edge));
 	}
 
 	if (t.owned)
@@ -1537,6 +1544,7 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 
 	long M = traj_dims[1] * traj_dims[2];
 	int s = init_geom(p->op.g, cim_dims, M, conf.os, conf.width, conf.periodic);
+	p->op.bin_edge = conf.bin;
 
 	if (BNUFFT_OK == s)
 		s = get_kb_table(conf.os, conf.width, &p->op.kb);
@@ -2276,6 +2284,7 @@ extern "C" void bnufft_pics_conf_defaults(struct bnufft_pics_conf* c)
 	c->toeplitz = 1;
 	c->periodic = 0;
 	c->deterministic = 0;
+	c->bin = 0;
 	c->precond = 0;
 }
 
@@ -2331,6 +2340,7 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 	nc.toeplitz = conf.toeplitz;
 	nc.periodic = conf.periodic;
 	nc.deterministic = conf.deterministic;
+	nc.bin = conf.bin;
 
 	if ((conf.precond < 0) || (conf.precond > 2))
 		return fail(BNUFFT_ERR_ARG, "precond must be 0, 1 or 2");
@@ -2679,20 +2689,16 @@ static bool cg_graph_enabled()
 	return !(e && (0 == strcmp(e, "0")));
 }
 
-extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, void* stream)
+// One reconstruction from device k-space into a device image: data scaling,
+// CG start, the iterations (as the while-node graph, or host-launched when
+// graph is false, e.g. while the caller captures), the result.
+static int pics_solve(bnufft_pics_s* ps, const float2* ksp, float2* out, cudaStream_t st, bool graph)
 {
-	cudaStream_t st = S(stream);
-	size_t kb = sizeof(float2) * ps->M * ps->C;
-	size_t ib = sizeof(float2) * ps->npix;
-	Staged ki, io;
-	TRY(stage_in(ki, ksp, kb, st));
-	TRY(stage_out_alloc(io, img, ib, st));
-
 	OpCtx& op = ps->nufft->op;
 	unsigned nb = (unsigned)ps->nparts;
-	long launches0 = g_launches.load();
+	size_t ib = sizeof(float2) * ps->npix;
 	ps->last_graph = false;
-	TRY(pics_prologue(ps, (const float2*)ki.dev, st));
+	TRY(pics_prologue(ps, ksp, st));
 
 	// CG from zero (conjgrad, src/iter/italgos.c:497-572)
 	k_cg_init<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, ps->pbuf[1], ps->b, ps->npix, ps->rs_part);
@@ -2707,7 +2713,7 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 
 	if (ps->conf.maxiter > 0) {
 
-		if (cg_graph_enabled()) {
+		if (graph) {
 
 			if (!ps->cg_exec)
 				TRY(capture_cg_loop(ps));
@@ -2727,17 +2733,168 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 
 	if (ps->conf.rescale) {
 
-		k_scale_dev<<<nb, RED_THREADS, 0, st>>>((float2*)io.dev, ps->x, ps->npix, &ps->scal->scale);
+		k_scale_dev<<<nb, RED_THREADS, 0, st>>>(out, ps->x, ps->npix, &ps->scal->scale);
 		LAUNCHED();
 
 	} else {
 
-		CUDA_TRY(cudaMemcpyAsync(io.dev, ps->x, ib, cudaMemcpyDeviceToDevice, st));
+		CUDA_TRY(cudaMemcpyAsync(out, ps->x, ib, cudaMemcpyDeviceToDevice, st));
 	}
 
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, void* stream)
+{
+	cudaStream_t st = S(stream);
+	size_t kb = sizeof(float2) * ps->M * ps->C;
+	size_t ib = sizeof(float2) * ps->npix;
+	Staged ki, io;
+	TRY(stage_in(ki, ksp, kb, st));
+	TRY(stage_out_alloc(io, img, ib, st));
+	long launches0 = g_launches.load();
+	TRY(pics_solve(ps, (const float2*)ki.dev, (float2*)io.dev, st, cg_graph_enabled()));
 	ps->last_host_kernels = g_launches.load() - launches0;
 	return stage_out_copy(io, img, ib, st);
 }
+
+// ----------------------------------------------------------------------------
+// batches of independent reconstructions as one graph
+// ----------------------------------------------------------------------------
+
+struct bnufft_batch_s {
+
+	std::vector<bnufft_pics_t> models;
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	long kernels = 0;		// kernel nodes in the graph
+};
+
+extern "C" void bnufft_batch_free(bnufft_batch_t b)
+{
+	if (!b)
+		return;
+
+	if (b->exec)
+		cudaGraphExecDestroy(b->exec);
+
+	if (b->graph)
+		cudaGraphDestroy(b->graph);
+
+	delete b;
+}
+
+extern "C" int bnufft_batch_create(bnufft_batch_t* out, const bnufft_pics_t* models, int n, void* const* imgs,
+		const void* const* ksps, void* stream)
+{
+	cudaStream_t st = S(stream);
+
+	if (!out || !models || !imgs || !ksps || (n < 1))
+		return fail(BNUFFT_ERR_ARG, "null argument or empty batch");
+
+	for (int p = 0; p < n; p++) {
+
+		if (!models[p])
+			return fail(BNUFFT_ERR_ARG, "batch model %d is null", p);
+
+		if (!on_device(imgs[p]) || !on_device(ksps[p]))
+			return fail(BNUFFT_ERR_ARG, "batch problem %d: images and k-space must be device memory", p);
+
+		if (models[p]->conf.tol > 0.f)
+			return fail(BNUFFT_ERR_UNSUPPORTED, "batch problem %d: batches run a fixed iteration count (tol 0)", p);
+
+		OpCtx& op = models[p]->nufft->op;
+		TRY(alloc_work(op.w, op.g, models[p]->C, st));
+	}
+
+	CUDA_TRY(cudaStreamSynchronize(st));
+
+	auto b = new bnufft_batch_s();
+	b->models.assign(models, models + n);
+	cudaStream_t cap = nullptr;
+	int s = BNUFFT_OK;
+	cudaError_t e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+
+	if (cudaSuccess == e)
+		e = cudaGraphCreate(&b->graph, 0);
+
+	if (cudaSuccess != e)
+		s = fail(BNUFFT_ERR_CUDA, "batch graph: %s", cudaGetErrorString(e));
+
+	// every problem's solve is captured into its own graph and added as a
+	// child node without dependencies: the problems run concurrently
+	for (int p = 0; (p < n) && (BNUFFT_OK == s); p++) {
+
+		cudaGraph_t gp = nullptr;
+		e = cudaGraphCreate(&gp, 0);
+
+		if (cudaSuccess == e)
+			e = cudaStreamBeginCaptureToGraph(cap, gp, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+
+		if (cudaSuccess != e) {
+
+			s = fail(BNUFFT_ERR_CUDA, "batch capture %d: %s", p, cudaGetErrorString(e));
+
+			if (gp)
+				cudaGraphDestroy(gp);
+
+			break;
+		}
+
+		long before = g_launches.load();
+		s = pics_solve(models[p], (const float2*)ksps[p], (float2*)imgs[p], cap, false);
+		long k = g_launches.load() - before;
+		g_launches.fetch_sub(k);	// captured, not launched
+		b->kernels += k;
+		cudaGraph_t got = nullptr;
+		e = cudaStreamEndCapture(cap, &got);
+
+		if ((BNUFFT_OK == s) && (cudaSuccess != e))
+			s = fail(BNUFFT_ERR_CUDA, "batch capture %d: %s", p, cudaGetErrorString(e));
+
+		if (BNUFFT_OK == s) {
+
+			cudaGraphNode_t node;
+			e = cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, gp);
+
+			if (cudaSuccess != e)
+				s = fail(BNUFFT_ERR_CUDA, "batch graph node %d: %s", p, cudaGetErrorString(e));
+		}
+
+		cudaGraphDestroy(gp);	// the child node holds its own copy
+	}
+
+	if (BNUFFT_OK == s) {
+
+		e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+
+		if (cudaSuccess != e)
+			s = fail(BNUFFT_ERR_CUDA, "batch instantiate: %s", cudaGetErrorString(e));
+	}
+
+	if (cap)
+		cudaStreamDestroy(cap);
+
+	if (BNUFFT_OK != s) {
+
+		std::string msg = g_err;
+		bnufft_batch_free(b);
+		g_err = msg;
+		return s;
+	}
+
+	*out = b;
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_batch_run(bnufft_batch_t b, void* stream)
+{
+	CUDA_TRY(cudaGraphLaunch(b->exec, S(stream)));
+	g_launches.fetch_add(b->kernels, std::memory_order_relaxed);
+	return BNUFFT_OK;
+}
+
+extern "C" long bnufft_batch_kernels(bnufft_batch_t b) { return b ? b->kernels : 0; }
 
 extern "C" int bnufft_pics_set_precnet(bnufft_pics_t ps, bnufft_precnet_t net, void* stream)
 {

@@ -27,10 +27,11 @@ class NufftConf:
     deterministic: bool = False
     os: float = 2.0
     width: float = 6.0
+    bin: int = 0              # gridding bin edge (0 = default); tuning only
 
     def c(self) -> _lib.NufftConfC:
         return _lib.NufftConfC(int(self.toeplitz), int(self.periodic), int(self.deterministic),
-                               float(self.os), float(self.width))
+                               float(self.os), float(self.width), int(self.bin))
 
 
 def _is_torch(a) -> bool:

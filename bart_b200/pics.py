@@ -29,12 +29,13 @@ class PicsConf:
     toeplitz: bool = True     # --no-toeplitz clears it
     periodic: bool = False
     deterministic: bool = False
+    bin: int = 0              # gridding bin edge (0 = default); tuning only
     precond: int = 0          # 0 plain CG, 1 FCG + circulant, 2 FCG + circulant + learned
 
     def c(self) -> _lib.PicsConfC:
         return _lib.PicsConfC(float(self.lam), int(self.maxiter), float(self.tol), float(self.scaling),
                               int(self.rescale), int(self.toeplitz), int(self.periodic), int(self.deterministic),
-                              int(self.precond))
+                              int(self.bin), int(self.precond))
 
 
 class Pics:

@@ -37,6 +37,9 @@ struct bnufft_conf {
 	int deterministic;
 	float os;
 	float width;
+	int bin;		/* gridding bin edge in grid cells (a power of two 8..128);
+				   0 = default (32 in 2D, 16 in 3D). A tuning knob with no
+				   effect on results (bnufft_autotune_bins picks it). */
 };
 
 typedef struct bnufft_plan_s* bnufft_plan_t;
@@ -117,6 +120,7 @@ struct bnufft_pics_conf {
 	int toeplitz;		/* default 1 (src/pics.c:90-91); 0 = --no-toeplitz */
 	int periodic;
 	int deterministic;
+	int bin;		/* gridding bin edge of the NUFFT (bnufft_conf.bin) */
 	int precond;		/* 0: plain CG (the reference's pics); 1: flexible CG with
 				   the circulant preconditioner of the NUFFT's PSF
 				   (nufft_precond_create, src/noncart/precond.c:48-164);
@@ -160,6 +164,22 @@ void bnufft_pics_free(bnufft_pics_t pics);
 /* Change the iteration limit and tolerance of later runs (the captured CG
  * graph reads them from the device, so it is kept). */
 int bnufft_pics_set_iter(bnufft_pics_t pics, int maxiter, float tol);
+
+/* Batches (no counterpart in the reference, which runs one pics per problem,
+ * src/pics.c, or loops with bart -p/-l, src/bart.c:202-217): n independent
+ * models, each with its own size, trajectory, coil count and maps, and their
+ * device k-space and image buffers, captured once into one CUDA graph in
+ * which every problem's whole solve (scaling, CG with the model's fixed
+ * maxiter, result) is an independent child graph; bnufft_batch_run launches
+ * it, the problems run concurrently. Models and buffers must outlive the
+ * batch; models need tol = 0. */
+typedef struct bnufft_batch_s* bnufft_batch_t;
+
+int bnufft_batch_create(bnufft_batch_t* batch, const bnufft_pics_t* models, int n, void* const* imgs,
+		const void* const* ksps, void* stream);
+int bnufft_batch_run(bnufft_batch_t batch, void* stream);
+long bnufft_batch_kernels(bnufft_batch_t batch);	/* kernel nodes per launch */
+void bnufft_batch_free(bnufft_batch_t batch);
 
 /* b = A^H y / scale, the right-hand side the solve uses (scaling as in
  * bnufft_pics_run). img-sized output. */
