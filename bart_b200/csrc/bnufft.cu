@@ -1433,8 +1433,146 @@ struct bnufft_plan_s {
 	float2* psf = nullptr;	// DFT order, includes 1/npix
 	float2* wgt = nullptr;	// weights copy [M, wgt_c]
 	float2* pinv = nullptr;	// circulant preconditioner 1/pre, [N0, N1*N2] DFT order (on demand)
+	// Toeplitz normal on a power-of-two circulant embedding when 2N is not a
+	// power of two: geometry with G = E >= 2N and the PSF re-embedded there
+	bool embed = false;
+	OpCtx toe;
+	float2* psf_t = nullptr;
 	cudaStream_t st0;
 };
+
+static OpCtx& toe_ctx(bnufft_plan_s* p) { return p->embed ? p->toe : p->op; }
+static const float2* toe_psf(const bnufft_plan_s* p) { return p->embed ? p->psf_t : p->psf; }
+
+// q'[i] = scale * q[d mod L] at d = i (i < N) or i - E (i > E - N), else 0,
+// per axis: the kernel of the Toeplitz operator (|d| < N) moved from the
+// length-L circulant to the length-E one
+__global__ static void k_toe_embed(float2* __restrict__ qe, const float2* __restrict__ q, GridGeom g, int E0, int E1,
+		int E2, float scale)
+{
+	const long n = (long)E0 * E1 * E2;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		int ia[3] = { (int)(i % E0), (int)((i / E0) % E1), (int)(i / ((long)E0 * E1)) };
+		int E[3] = { E0, E1, E2 };
+		long src = 0, stride = 1;
+		bool ok = true;
+
+		for (int a = 0; a < 3; a++) {
+
+			int d = (ia[a] < g.N[a]) ? ia[a] : ((ia[a] > E[a] - g.N[a]) ? ia[a] - E[a] : INT_MIN);
+
+			if (INT_MIN == d) {
+
+				ok = false;
+				break;
+			}
+
+			int j = (d < 0) ? d + g.G[a] : d;
+			src += j * stride;
+			stride *= g.G[a];
+		}
+
+		qe[i] = ok ? cscale(q[src], scale) : make_float2(0.f, 0.f);
+	}
+}
+
+// Build p->toe / p->psf_t from p->psf (see the struct). With P the PSF on
+// the L = 2N grid, the normal operator is y = sum_m x_m L q[(n - m) mod L],
+// q = IDFT(P) / L per axis, and only |n - m| < N enters: on a length-E grid
+// the same operator has q' = (L / E) q on |d| < N, zero elsewhere, and
+// P' = DFT_E(q').
+static int build_toeplitz_embedding(bnufft_plan_s* p, cudaStream_t st)
+{
+	const Geom& g = p->op.g;
+	int E[3];
+	bool embed = false;
+
+	for (int a = 0; a < 3; a++) {
+
+		E[a] = 1;
+
+		if (g.G[a] > 1) {
+
+			int e = 16;
+
+			while (e < g.G[a])
+				e *= 2;
+
+			E[a] = e;
+			embed |= (e != g.G[a]);
+		}
+	}
+
+	if (p->psf_t)
+		cudaFreeAsync(p->psf_t, st);
+
+	p->psf_t = nullptr;
+	p->embed = false;
+
+	if (!embed || (E[0] > 4096) || (E[1] > 4096) || (E[2] > 4096))
+		return BNUFFT_OK;
+
+	const long L0 = g.G[0], L1 = g.G[1], L2 = g.G[2];
+	const long ne = (long)E[0] * E[1] * E[2];
+	float2* q = nullptr;
+	float2* qe = nullptr;
+	CUDA_TRY(cudaMallocAsync(&q, sizeof(float2) * g.gsz, st));
+	CUDA_TRY(cudaMallocAsync(&qe, sizeof(float2) * ne, st));
+
+	// rows of a [L0, rows] array as column-pass sequences (element stride 1),
+	// at most 65535 per launch
+	auto along_x = [&](int L, int mode, const float2* in, float2* out, long rows) -> int {
+
+		for (long r0 = 0; r0 < rows; r0 += 65535) {
+
+			long nr = std::min(65535L, rows - r0);
+			TRY(cols(L, mode, in + r0 * L, 1, L, L, 0, out + r0 * L, 1, L, L, 0, 1, nr, nullptr, 0, 1, 0, st));
+		}
+
+		return BNUFFT_OK;
+	};
+
+	// unnormalised inverse DFT of the PSF along every axis (in place after the first)
+	TRY(along_x((int)L0, 1, p->psf, q, L1 * L2));
+
+	if (L1 > 1)
+		TRY(cols((int)L1, 1, q, L0, L0 * L1, (int)L1, 0, q, L0, L0 * L1, (int)L1, 0, (int)L0, L2, nullptr, 0, 1, 0, st));
+
+	if (L2 > 1)
+		TRY(cols((int)L2, 1, q, L0 * L1, 0, (int)L2, 0, q, L0 * L1, 0, (int)L2, 0, (int)(L0 * L1), 1, nullptr, 0, 1, 0, st));
+
+	k_toe_embed<<<vec_blocks(ne), RED_THREADS, 0, st>>>(qe, q, grid_geom(g), E[0], E[1], E[2], (float)(1. / (double)ne));
+	LAUNCHED();
+
+	// forward DFT on the embedding grid (powers of two)
+	const long E0 = E[0], E1 = E[1], E2 = E[2];
+	TRY(along_x((int)E0, 0, qe, qe, E1 * E2));
+
+	if (E1 > 1)
+		TRY(cols((int)E1, 0, qe, E0, E0 * E1, (int)E1, 0, qe, E0, E0 * E1, (int)E1, 0, (int)E0, E2, nullptr, 0, 1, 0, st));
+
+	if (E2 > 1)
+		TRY(cols((int)E2, 0, qe, E0 * E1, 0, (int)E2, 0, qe, E0 * E1, 0, (int)E2, 0, (int)(E0 * E1), 1, nullptr, 0, 1, 0, st));
+
+	cudaFreeAsync(q, st);
+	p->psf_t = qe;
+
+	free_work(p->toe.w, st);
+	p->toe = OpCtx();
+	p->toe.g = g;
+	p->toe.g.gsz = ne;
+
+	for (int a = 0; a < 3; a++)
+		p->toe.g.G[a] = E[a];
+
+	p->toe.kb = p->op.kb;
+	p->toe.traj = nullptr;
+	p->embed = true;
+	return BNUFFT_OK;
+}
+
 
 extern "C" void bnufft_conf_defaults(struct bnufft_conf* conf)
 {
@@ -1484,6 +1622,7 @@ static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
 		p->psf = nullptr;
 		TRY(compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, st, 0 != p->conf.deterministic, p->op.wgt,
 				p->op.bin_edge));
+		TRY(build_toeplitz_embedding(p, st));
 	}
 
 	if (t.owned)
@@ -1647,7 +1786,7 @@ extern "C" int bnufft_apply_normal(bnufft_plan_t p, void* dst, const void* src, 
 
 	if (p->psf) {
 
-		TRY(op_toeplitz(p->op, p->psf, (const float2*)i.dev, nullptr, p->C, 1, (float2*)o.dev, st));
+		TRY(op_toeplitz(toe_ctx(p), toe_psf(p), (const float2*)i.dev, nullptr, p->C, 1, (float2*)o.dev, st));
 
 	} else {
 
@@ -1746,11 +1885,13 @@ extern "C" void bnufft_free(bnufft_plan_t p)
 
 	cudaStream_t st = p->st0;
 	free_work(p->op.w, st);
+	free_work(p->toe.w, st);
 	free_csr(p->op.csr, st);
 	free_bins(p->op.bins, st);
 
 	if (p->traj) cudaFreeAsync(p->traj, st);
 	if (p->psf) cudaFreeAsync(p->psf, st);
+	if (p->psf_t) cudaFreeAsync(p->psf_t, st);
 	if (p->wgt) cudaFreeAsync(p->wgt, st);
 	if (p->pinv) cudaFreeAsync(p->pinv, st);
 	if (p->op.wbuf) cudaFreeAsync(p->op.wbuf, st);
@@ -1876,7 +2017,7 @@ extern "C" int bnufft_nufft_inverse(bnufft_plan_t p, void* img, const void* ksp,
 		// Ap = P^-1 (N^H N p + lambda p); partial p^H Ap
 		if (p->psf) {
 
-			TRY(op_toeplitz(op, p->psf, pv, nullptr, C, 1, Ap, st));
+			TRY(op_toeplitz(toe_ctx(p), toe_psf(p), pv, nullptr, C, 1, Ap, st));
 
 		} else {
 
@@ -2296,7 +2437,7 @@ static int sense_normal(bnufft_pics_s* ps, const float2* x, float2* out, float l
 
 	if (ps->nufft->psf) {
 
-		TRY(op_toeplitz(op, ps->nufft->psf, x, ps->sens, ps->C, ps->cpg, ps->part, st));
+		TRY(op_toeplitz(toe_ctx(ps->nufft), toe_psf(ps->nufft), x, ps->sens, ps->C, ps->cpg, ps->part, st));
 
 	} else {
 
@@ -2484,13 +2625,13 @@ static int pics_prologue(bnufft_pics_s* ps, const float2* ksp, cudaStream_t st)
 // device counter (the loop runs inside a graph).
 static int pics_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 {
-	OpCtx& op = ps->nufft->op;
+	bool toep = (nullptr != ps->nufft->psf);
+	OpCtx& op = toep ? toe_ctx(ps->nufft) : ps->nufft->op;	// Toeplitz: its (embedding) grid
 	const Geom& g = op.g;
 	long YZ = (long)g.N[1] * g.N[2];
 	const int* done = &ps->scal->done;
 	float2* p_prev = ps->pbuf[0];
 	float2* p_cur = ps->pbuf[1];
-	bool toep = (nullptr != ps->nufft->psf);
 	int npp = 0, npap = 0;
 
 	TRY(rows_fwd_cg(g.G[0], ps->b, ps->r, p_prev, p_cur, ps->sens, toep ? nullptr : op.ax, op.ayz,
@@ -2504,7 +2645,7 @@ static int pics_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 
 	if (toep) {
 
-		TRY(op_toeplitz_cols(op, ps->nufft->psf, ps->C, st, done));
+		TRY(op_toeplitz_cols(op, toe_psf(ps->nufft), ps->C, st, done));
 		TRY(rows_inv(g.G[0], op.w.t1, ps->sens, nullptr, nullptr, g.N[0], YZ, (int)ps->C, ps->cpg, ps->part, st,
 				dh.p, dh.part, dh.done, dh.nblocks));
 
@@ -2592,7 +2733,7 @@ static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, cons
 // the convergence test and z = M(r) for the next iteration.
 static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 {
-	OpCtx& op = ps->nufft->op;
+	OpCtx& op = toe_ctx(ps->nufft);
 	const Geom& g = op.g;
 	long YZ = (long)g.N[1] * g.N[2];
 	const int* done = &ps->scal->done;
@@ -2606,7 +2747,7 @@ static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 			ps->dots_part, ps->nparts, ps->pr_part, ps->pp_part);
 	LAUNCHED();
 	TRY(rows_fwd(g.G[0], p, ps->sens, nullptr, nullptr, g.N[0], YZ, YZ * ps->C, op.w.t1, st, done));
-	TRY(op_toeplitz_cols(op, ps->nufft->psf, ps->C, st, done));
+	TRY(op_toeplitz_cols(op, toe_psf(ps->nufft), ps->C, st, done));
 	TRY(rows_inv(g.G[0], op.w.t1, ps->sens, nullptr, nullptr, g.N[0], YZ, (int)ps->C, ps->cpg, ps->part, st,
 			p, ps->pap_part, done, &npap));
 
@@ -2708,6 +2849,9 @@ static int pics_solve(bnufft_pics_s* ps, const float2* ksp, float2* out, cudaStr
 
 	TRY(alloc_work(op.w, op.g, ps->C, st));
 
+	if (ps->nufft->embed)
+		TRY(alloc_work(ps->nufft->toe.w, ps->nufft->toe.g, ps->C, st));
+
 	if (ps->conf.precond)	// z0 = M(b); the first direction is p = z0
 		TRY(pics_precond(ps, ps->r, ps->z, nullptr, nullptr, nullptr, st));
 
@@ -2805,6 +2949,9 @@ extern "C" int bnufft_batch_create(bnufft_batch_t* out, const bnufft_pics_t* mod
 
 		OpCtx& op = models[p]->nufft->op;
 		TRY(alloc_work(op.w, op.g, models[p]->C, st));
+
+		if (models[p]->nufft->embed)
+			TRY(alloc_work(models[p]->nufft->toe.w, models[p]->nufft->toe.g, models[p]->C, st));
 	}
 
 	CUDA_TRY(cudaStreamSynchronize(st));
