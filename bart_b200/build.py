@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "lib", "libbnufft.so")
 SOURCES = [os.path.join(HERE, "csrc", "bnufft.cu")]
-HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft_core.cuh", "nufft_kernels.cuh", "cg_kernels.cuh")] + \
+HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft_core.cuh", "nufft_kernels.cuh", "cg_kernels.cuh", "gridding.cuh",
+                                                   "precnet.cuh")] + \
     [os.path.join(ROOT, "include", "bnufft.h")]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -31,6 +32,8 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    from .micro import build_atomics
+    build_atomics()
     if not force and not needs_build():
         return LIB
     os.makedirs(os.path.dirname(LIB), exist_ok=True)

@@ -184,16 +184,19 @@ def timed_steps(step, steps, flush, stream):
     return sum(e0.elapsed_time(e1) for e0, e1 in ev)
 
 
-def run_nufft3d(dev, steps, warmup):
+def run_nufft3d(dev, steps, warmup, spokes=20000):
     """3D radial kooshball NUFFT: 128^3 image, 8 coils,
     20000 spokes x 256 samples on 3D golden means (5.12 M samples per coil).
     One step = forward + adjoint of all 8 coil images, device-resident, plan
-    reused. Also times a 10-iteration Toeplitz CG-SENSE solve (model reused)."""
+    reused. Also the time per kernel class (CUDA events per launch), the
+    scatter's atomic rate, and a 10-iteration Toeplitz CG-SENSE solve (model
+    reused)."""
+    import ctypes
     import torch
-    from bart_b200 import synth
+    from bart_b200 import _lib, synth
     from bart_b200.nufft import NufftConf, nufft_create2
     from bart_b200.pics import Pics, PicsConf
-    N, C, spokes, readout = 128, 8, 20000, 128
+    N, C, readout = 128, 8, 128
     rng = np.random.default_rng(3)
     t = synth.kooshball_traj(readout, spokes)
     M = t.shape[1] * t.shape[2]
@@ -218,8 +221,20 @@ def run_nufft3d(dev, steps, warmup):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
+    lib = _lib.load()
+    classes = {}
+    for kind in ("rows_fwd", "cols_fwd", "degrid", "grid", "cols_inv", "rows_inv"):
+        lib.bnufft_prof_start(kind.encode())
+        op.forward(cim, k)
+        op.adjoint(k, a)
+        kms, kn = ctypes.c_double(), ctypes.c_long()
+        lib.bnufft_prof_stop(ctypes.byref(kms), ctypes.byref(kn))
+        classes[kind] = {"ms": kms.value, "launches": kn.value}
     op.free()
     nbytes = 2 * (N ** 3 * C * 8 + M * C * 8 + M * 12)
+    # scatter: one float2 atomic add per tap (6^3 taps, weight-0 taps skipped)
+    atomics = M * C * 216
+    classes["grid"]["g_float2_atomics_per_s"] = atomics / (classes["grid"]["ms"] * 1e-3) / 1e9
     sens_d = torch.from_numpy(np.asfortranarray(sens).ravel(order="F").copy()).to(dev)
     t0 = time.perf_counter()
     p = Pics(t_d, sens_d, ksp_dims=kd, conf=PicsConf(lam=LAM, maxiter=10), traj_dims=list(t.shape), sens_dims=cd)
@@ -233,7 +248,7 @@ def run_nufft3d(dev, steps, warmup):
     torch.cuda.synchronize()
     cg_ms = e0.elapsed_time(e1)
     p.free()
-    return {"workload": "nufft3d_128_c8_kooshball_20000x256", "nufft_fwd_adj_ms": ms,
+    return {"workload": f"nufft3d_128_c8_kooshball_{spokes}x256", "nufft_fwd_adj_ms": ms, "kernel_classes": classes,
             "nufft_gbs": nbytes / (ms * 1e-3) / 1e9, "bytes_per_step": nbytes,
             "cgsense_setup_s": setup_s, "cgsense_10iter_ms": cg_ms}
 
@@ -393,6 +408,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "batch"])
+    ap.add_argument("--spokes", type=int, default=20000, help="nufft3d: kooshball spokes")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -421,7 +437,7 @@ def main():
 
     if args.workload == "nufft3d":
         if rank == 0:
-            print(json.dumps(run_nufft3d(dev, args.steps, args.warmup)), flush=True)
+            print(json.dumps(run_nufft3d(dev, args.steps, args.warmup, args.spokes)), flush=True)
         return
 
     if args.workload == "batch":
