@@ -344,9 +344,10 @@ static int launch_rows_fwd_LB(const float2* img, const float2* maps, const float
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
 	size_t smem = rows_smem(L, B);
-	TRY(prep_kernel(k_rows_fwd<L, B>, smem));
+	auto kern = (d.n == L) ? k_rows_fwd<L, B, false> : k_rows_fwd<L, B, true>;
+	TRY(prep_kernel(kern, smem));
 	cudaEvent_t pe = prof_begin("rows_fwd", st);
-	k_rows_fwd<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(img, maps, ax, ayz, X, YZ, R, out, tw, done, d);
+	kern<<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(img, maps, ax, ayz, X, YZ, R, out, tw, done, d);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
@@ -360,14 +361,15 @@ static int launch_cols_LB(const float2* in, long ies, long ios, int n_in, int wr
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
 	size_t smem = pass_smem(L, B);
-	TRY(prep_kernel(k_cols<L, B, MODE>, smem));
+	auto kern = (d.n == L) ? k_cols<L, B, MODE, false> : k_cols<L, B, MODE, true>;
+	TRY(prep_kernel(kern, smem));
 
 	if (O > 65535)
 		return fail(BNUFFT_ERR_UNSUPPORTED, "column pass with %ld outer sequences", O);
 
 	dim3 grid((unsigned)((W + B - 1) / B), (unsigned)O);
 	cudaEvent_t pe = prof_begin((2 == MODE) ? "cols_toeplitz" : ((1 == MODE) ? "cols_inv" : "cols_fwd"), st);
-	k_cols<L, B, MODE><<<grid, B * L / 8, smem, st>>>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out,
+	kern<<<grid, B * L / 8, smem, st>>>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out,
 			W, psf, pes, pmod, pos, tw, done, d);
 	prof_end(pe, st);
 	LAUNCHED();
@@ -383,10 +385,11 @@ static int launch_rows_inv_LB(const float2* in, const float2* maps, const float*
 	TRY(get_twiddles(L, &tw));
 	int groups = (C + cpg - 1) / cpg;
 	size_t smem = rows_smem(L, B);
-	TRY(prep_kernel(k_rows_inv<L, B>, smem));
+	auto kern = (d.n == L) ? k_rows_inv<L, B, false> : k_rows_inv<L, B, true>;
+	TRY(prep_kernel(kern, smem));
 	dim3 grid((unsigned)((YZ + B - 1) / B), (unsigned)groups);
 	cudaEvent_t pe = prof_begin("rows_inv", st);
-	k_rows_inv<L, B><<<grid, B * L / 8, smem, st>>>(in, maps, ax, ayz, X, YZ, C, cpg, out, tw, pdot, dot_part, done, d);
+	kern<<<grid, B * L / 8, smem, st>>>(in, maps, ax, ayz, X, YZ, C, cpg, out, tw, pdot, dot_part, done, d);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
@@ -400,9 +403,10 @@ static int launch_rows_fwd_cg_LB(const float2* bvec, const float2* r, const floa
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
 	size_t smem = rows_smem(L, B);
-	TRY(prep_kernel(k_rows_fwd_cg<L, B>, smem));
+	auto kern = (d.n == L) ? k_rows_fwd_cg<L, B, false> : k_rows_fwd_cg<L, B, true>;
+	TRY(prep_kernel(kern, smem));
 	cudaEvent_t pe = prof_begin("rows_fwd", st);
-	k_rows_fwd_cg<L, B><<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(bvec, r, p_prev, p_cur, maps, ax, ayz,
+	kern<<<(unsigned)((R + B - 1) / B), B * L / 8, smem, st>>>(bvec, r, p_prev, p_cur, maps, ax, ayz,
 			X, YZ, R, out, tw, stt, it, rs_part, nrs, pp_part, d);
 	prof_end(pe, st);
 	LAUNCHED();
@@ -3333,8 +3337,8 @@ static int na_rows(const float2* img, const float* ax, const float* ayz, int X, 
 {
 	constexpr int B = 16;
 	size_t smem = rows_smem(L, B);
-	CUDA_TRY(cudaFuncSetAttribute(k_rows_fwd<L, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-	k_rows_fwd<L, B><<<(unsigned)((Y + B - 1) / B), B * L / 8, smem, st>>>(img, nullptr, ax, ayz, X, Y, Y, out, tw, nullptr, Dft{L, nullptr, nullptr, nullptr});
+	CUDA_TRY(cudaFuncSetAttribute(k_rows_fwd<L, B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+	k_rows_fwd<L, B, false><<<(unsigned)((Y + B - 1) / B), B * L / 8, smem, st>>>(img, nullptr, ax, ayz, X, Y, Y, out, tw, nullptr, Dft{L, nullptr, nullptr, nullptr});
 	LAUNCHED();
 	return BNUFFT_OK;
 }
@@ -3344,9 +3348,9 @@ static int na_cols(const float2* t1, int G0, int Y, float2* grid, const float2* 
 {
 	constexpr int B = 16;
 	size_t smem = pass_smem(L, B);
-	CUDA_TRY(cudaFuncSetAttribute(k_cols<L, B, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+	CUDA_TRY(cudaFuncSetAttribute(k_cols<L, B, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
 	dim3 grid_dim((unsigned)((G0 + B - 1) / B), 1);
-	k_cols<L, B, 0><<<grid_dim, B * L / 8, smem, st>>>(t1, G0, (long)G0 * Y, Y, 1, grid, G0, (long)G0 * L, L, 0,
+	k_cols<L, B, 0, false><<<grid_dim, B * L / 8, smem, st>>>(t1, G0, (long)G0 * Y, Y, 1, grid, G0, (long)G0 * L, L, 0,
 			G0, nullptr, 0, 1, 0, tw, nullptr, Dft{L, nullptr, nullptr, nullptr});
 	LAUNCHED();
 	return BNUFFT_OK;

@@ -22,6 +22,7 @@
 // grid index to the tile-local index of the same cell.
 #pragma once
 
+#include <climits>
 #include <cuda_runtime.h>
 
 #include "nufft_kernels.cuh"
@@ -408,7 +409,14 @@ __global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_binned(const float4* _
 }
 
 // Gridding, width 6, without tiles: one thread per sample in bin order,
-// weights computed once for all coils, one global float2 atomic per tap.
+// weights computed once for all coils, global atomics. The scatter is bound
+// by the L2's atomic-operation rate, which is the same for 8- and 16-byte
+// vector atomics: so the six x-taps of a sample (at most 7 consecutive cells
+// of a grid row) are laid into an 8-cell window starting at an even cell,
+// and each (z, y) row takes up to 4 float4 atomics (two cells each) instead
+// of 6 float2 ones. Windows that wrap around the row fall back to one float2
+// atomic per tap. Float sums in another order than the per-tap form: the
+// result is the same up to rounding (the atomics' order is arbitrary anyway).
 template <int TZ>
 __global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_atomic(const float4* __restrict__ traj_sorted,
 		const int* __restrict__ perm, long M, GridGeom g, int C,
@@ -433,6 +441,34 @@ __global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_atomic(const float4* _
 	axis_taps6<0>(k.z, g.N[2], g.periodic, kb, 0, tz);
 	const long m = perm[i];
 
+	// the x window: taps with weight, their lowest and highest cell
+	int lo = INT_MAX, hi = INT_MIN;
+#pragma unroll
+	for (int e = 0; e < 6; e++) {
+
+		if (0.f != tx.w[e]) {
+
+			lo = min(lo, tx.cell[e]);
+			hi = max(hi, tx.cell[e]);
+		}
+	}
+
+	const int base = lo & ~1;
+	const bool vec = (lo <= hi) && (hi - base < 8);
+	float wx8[8];
+#pragma unroll
+	for (int j = 0; j < 8; j++) {
+
+		// only taps with weight: a clipped tap (weight 0) of a non-periodic
+		// grid may sit on the same cell as a valid one
+		float w = 0.f;
+#pragma unroll
+		for (int e = 0; e < 6; e++)
+			w = ((0.f != tx.w[e]) && (tx.cell[e] == base + j)) ? tx.w[e] : w;
+
+		wx8[j] = vec ? w : 0.f;
+	}
+
 	for (int c = 0; c < C; c++) {
 
 		float2 val = ksp[m + M * c];
@@ -451,13 +487,31 @@ __global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_atomic(const float4* _
 
 				float dzy = __fmul_rn(dz, ty.w[b]);
 				long oy = (oz + ty.cell[b]) * g.G[0];
+
+				if (0.f == dzy)
+					continue;
+
+				if (vec) {
 #pragma unroll
-				for (int e = 0; e < 6; e++) {
+					for (int q = 0; q < 4; q++) {
 
-					float d = __fmul_rn(dzy, tx.w[e]);
+						float d0 = __fmul_rn(dzy, wx8[2 * q]);
+						float d1 = __fmul_rn(dzy, wx8[2 * q + 1]);
 
-					if (0.f != d)
-						atomicAdd(&gc[oy + tx.cell[e]], make_float2(val.x * d, val.y * d));
+						if ((0.f != d0) || (0.f != d1))
+							atomicAdd((float4*)(gc + oy + base + 2 * q),
+								make_float4(val.x * d0, val.y * d0, val.x * d1, val.y * d1));
+					}
+
+				} else {
+#pragma unroll
+					for (int e = 0; e < 6; e++) {
+
+						float d = __fmul_rn(dzy, tx.w[e]);
+
+						if (0.f != d)
+							atomicAdd(&gc[oy + tx.cell[e]], make_float2(val.x * d, val.y * d));
+					}
 				}
 			}
 		}

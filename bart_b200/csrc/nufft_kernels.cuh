@@ -41,10 +41,10 @@ struct Dft {
 // DFT of the register set v (positions reg_pos(m), see fft_regs); for
 // Bluestein the caller has loaded zeros at positions >= d.n and gets zeros
 // there back. Same barrier contract as fft_regs.
-template <int L, typename LAY, bool INV>
+template <int L, typename LAY, bool INV, bool BLUE>
 __device__ __forceinline__ void dft_regs(float2 (&v)[8], float2* s, const float2* tw, const Dft& d)
 {
-	if (d.n == L) {
+	if constexpr (!BLUE) {
 
 		fft_regs<L, LAY, INV>(v, s, tw);
 		return;
@@ -179,7 +179,7 @@ __device__ __forceinline__ int cg_iter(int it, const CgScalars* st) { return (it
 // Rows of coil 0 write p and the partial ||p||^2 (for lambda ||p||^2 in
 // p^H (A^H A + lambda) p); every row multiplies by its coil's map and runs the
 // forward transform like k_rows_fwd.
-template <int L, int B>
+template <int L, int B, bool BLUE>
 __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_rows_fwd_cg(const float2* __restrict__ bvec, const float2* __restrict__ r,
 		const float2* __restrict__ p_prev, float2* __restrict__ p_cur, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		CgScalars* st, int it, const double* __restrict__ rs_part, int nrs, double* __restrict__ pp_part, Dft d)
 {
 	using LAY = RowLayout<L, B>;
+	const int dn = BLUE ? d.n : L;	// logical DFT length (compile-time for the FFT itself)
 	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
 	__shared__ double red[32];
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 	for (int m = 0; m < 8; m++) {
 
 		int p = reg_pos<L, LAY>(m);
-		int n = (p < d.n) ? unwrap_pos(p, X, d.n) : X;
+		int n = (p < dn) ? unwrap_pos(p, X, dn) : X;
 		v[m] = make_float2(0.f, 0.f);
 
 		if (valid && (n < X)) {
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 	if (0 == threadIdx.x)
 		pp_part[blockIdx.x] = t;
 
-	dft_regs<L, LAY, false>(v, s, tw, d);
+	dft_regs<L, LAY, false, BLUE>(v, s, tw, d);
 
 	if (valid) {
 #pragma unroll
@@ -280,8 +281,8 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 
 			int p = reg_pos<L, LAY>(m);
 
-			if (p < d.n)
-				out[p + (long)d.n * row] = v[m];
+			if (p < dn)
+				out[p + (long)dn * row] = v[m];
 		}
 	}
 }
@@ -294,12 +295,13 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 // placed at wrap_pos(x, X, L), transformed, written to out[p + L*r].
 // One block: B rows, B*L/8 threads; a warp reads and writes consecutive
 // elements of one row straight from / into the FFT's registers.
-template <int L, int B>
+template <int L, int B, bool BLUE>
 __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_rows_fwd(const float2* __restrict__ img, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
 		int X, long YZ, long R, float2* __restrict__ out, const float2* __restrict__ twg, const int* done, Dft d)
 {
 	using LAY = RowLayout<L, B>;
+	const int dn = BLUE ? d.n : L;	// logical DFT length (compile-time for the FFT itself)
 	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
 	float2* s = smem;
@@ -321,7 +323,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 	for (int m = 0; m < 8; m++) {
 
 		int p = reg_pos<L, LAY>(m);
-		int n = (p < d.n) ? unwrap_pos(p, X, d.n) : X;
+		int n = (p < dn) ? unwrap_pos(p, X, dn) : X;
 		v[m] = make_float2(0.f, 0.f);
 
 		if (valid && (n < X)) {
@@ -332,7 +334,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		}
 	}
 
-	dft_regs<L, LAY, false>(v, s, tw, d);
+	dft_regs<L, LAY, false, BLUE>(v, s, tw, d);
 
 	if (valid) {
 #pragma unroll
@@ -340,8 +342,8 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 
 			int p = reg_pos<L, LAY>(m);
 
-			if (p < d.n)
-				out[p + (long)d.n * row] = v[m];
+			if (p < dn)
+				out[p + (long)dn * row] = v[m];
 		}
 	}
 }
@@ -358,13 +360,14 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 // One block: B columns of one outer index, B*L/8 threads; grid (ceil(W/B), O).
 // Global loads go straight into the first FFT stage's registers and results
 // leave from the last stage's registers (B consecutive columns per access).
-template <int L, int B, int MODE>
+template <int L, int B, int MODE, bool BLUE>
 __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_cols(const float2* __restrict__ in, long ies, long ios, int n_in, int wrap_in,
 		float2* __restrict__ out, long oes, long oos, int n_out, int wrap_out,
 		int W, const float2* __restrict__ psf, long pes, long pmod, long pos,
 		const float2* __restrict__ twg, const int* done, Dft d)
 {
 	using LAY = ColLayout<L, B>;
+	const int dn = BLUE ? d.n : L;	// logical DFT length (compile-time for the FFT itself)
 	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
 	float2* s = smem;
@@ -386,18 +389,18 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 	for (int m = 0; m < 8; m++) {
 
 		int p = reg_pos<L, LAY>(m);
-		int n = (p >= d.n) ? n_in : (wrap_in ? unwrap_pos(p, n_in, d.n) : p);
+		int n = (p >= dn) ? n_in : (wrap_in ? unwrap_pos(p, n_in, dn) : p);
 		v[m] = (valid && (n < n_in)) ? inp[n * ies] : make_float2(0.f, 0.f);
 	}
 
 	// the twiddle table must be complete before the first stage reads it
 	if constexpr (MODE == 1) {
 
-		dft_regs<L, LAY, true>(v, s, tw, d);
+		dft_regs<L, LAY, true, BLUE>(v, s, tw, d);
 
 	} else {
 
-		dft_regs<L, LAY, false>(v, s, tw, d);
+		dft_regs<L, LAY, false, BLUE>(v, s, tw, d);
 	}
 
 	if constexpr (MODE == 2) {
@@ -408,11 +411,11 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 
 			int p = reg_pos<L, LAY>(m);
 
-			if (valid && (p < d.n))
+			if (valid && (p < dn))
 				v[m] = cmul(v[m], pp[p * pes]);
 		}
 
-		dft_regs<L, LAY, true>(v, s, tw, d);
+		dft_regs<L, LAY, true, BLUE>(v, s, tw, d);
 	}
 
 	float2* outp = out + o * oos + cx;
@@ -422,7 +425,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		for (int m = 0; m < 8; m++) {
 
 			int p = reg_pos<L, LAY>(m);
-			int n = (p >= d.n) ? n_out : (wrap_out ? unwrap_pos(p, n_out, d.n) : p);
+			int n = (p >= dn) ? n_out : (wrap_out ? unwrap_pos(p, n_out, dn) : p);
 
 			if (n < n_out)
 				outp[n * oes] = v[m];
@@ -440,13 +443,14 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 //              into out[x + X*yz + X*YZ*g] (g = blockIdx.y, partial per group)
 //   maps == 0: write out[x + X*yz + X*YZ*c] per coil.
 // grid (ceil(YZ/B), groups); coils per group cpg.
-template <int L, int B>
+template <int L, int B, bool BLUE>
 __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_rows_inv(const float2* __restrict__ in, const float2* __restrict__ maps,
 		const float* __restrict__ ax, const float* __restrict__ ayz,
 		int X, long YZ, int C, int cpg, float2* __restrict__ out, const float2* __restrict__ twg,
 		const float2* __restrict__ pdot, double* __restrict__ dot_part, const int* done, Dft d)
 {
 	using LAY = RowLayout<L, B>;
+	const int dn = BLUE ? d.n : L;	// logical DFT length (compile-time for the FFT itself)
 	constexpr int NT = B * L / 8;
 	extern __shared__ float2 smem[];
 	__shared__ double red[32];
@@ -480,17 +484,17 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		for (int m = 0; m < 8; m++) {
 
 			int p = reg_pos<L, LAY>(m);
-			v[m] = (valid && (p < d.n)) ? in[p + (long)d.n * (yz + YZ * c)] : make_float2(0.f, 0.f);
+			v[m] = (valid && (p < dn)) ? in[p + (long)dn * (yz + YZ * c)] : make_float2(0.f, 0.f);
 		}
 
-		dft_regs<L, LAY, true>(v, s, tw, d);
+		dft_regs<L, LAY, true, BLUE>(v, s, tw, d);
 
 		if (valid) {
 #pragma unroll
 			for (int m = 0; m < 8; m++) {
 
 				int p = reg_pos<L, LAY>(m);
-				int x = (p < d.n) ? unwrap_pos(p, X, d.n) : X;
+				int x = (p < dn) ? unwrap_pos(p, X, dn) : X;
 
 				if (x >= X)
 					continue;
@@ -525,7 +529,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 			for (int m = 0; m < 8; m++) {
 
 				int p = reg_pos<L, LAY>(m);
-				int x = (p < d.n) ? unwrap_pos(p, X, d.n) : X;
+				int x = (p < dn) ? unwrap_pos(p, X, dn) : X;
 
 				if (x >= X)
 					continue;
