@@ -264,6 +264,34 @@ __global__ void __launch_bounds__(BIN_THREADS, 2) k_degrid6(const float4* __rest
 	axis_taps6<0>(k.z, g.N[2], g.periodic, kb, 0, tz);
 	const long m = perm[i];
 
+	// the x taps as an 8-cell window from an even cell: each (z, y) row is
+	// read with 4 float4 loads instead of 6 float2 gathers (the gather is
+	// bound by L1 requests); windows that wrap around the row read per tap
+	int lo = INT_MAX, hi = INT_MIN;
+#pragma unroll
+	for (int e = 0; e < 6; e++) {
+
+		if (0.f != tx.w[e]) {
+
+			lo = min(lo, tx.cell[e]);
+			hi = max(hi, tx.cell[e]);
+		}
+	}
+
+	const int base = lo & ~1;
+	const bool vec = (lo <= hi) && (hi - base < 8);
+	float wx8[8];
+#pragma unroll
+	for (int j = 0; j < 8; j++) {
+
+		float w = 0.f;	// taps with weight only (see k_grid6_atomic)
+#pragma unroll
+		for (int e = 0; e < 6; e++)
+			w = ((0.f != tx.w[e]) && (tx.cell[e] == base + j)) ? tx.w[e] : w;
+
+		wx8[j] = vec ? w : 0.f;
+	}
+
 	for (int c = 0; c < C; c++) {
 
 		const float2* gc = grid + g.gsz * c;
@@ -278,13 +306,34 @@ __global__ void __launch_bounds__(BIN_THREADS, 2) k_degrid6(const float4* __rest
 
 				float dzy = __fmul_rn(dz, ty.w[b]);
 				long oy = (oz + ty.cell[b]) * g.G[0];
-#pragma unroll
-				for (int e = 0; e < 6; e++) {
 
-					float d = __fmul_rn(dzy, tx.w[e]);
-					float2 v = gc[oy + tx.cell[e]];
-					acc.x = fmaf(v.x, d, acc.x);
-					acc.y = fmaf(v.y, d, acc.y);
+				if (vec) {
+#pragma unroll
+					for (int q = 0; q < 4; q++) {
+
+						// slots past the last tap hold no weight and are not
+						// read (the window may pass the end of the row)
+						if ((0.f == wx8[2 * q]) && (0.f == wx8[2 * q + 1]))
+							continue;
+
+						float d0 = __fmul_rn(dzy, wx8[2 * q]);
+						float d1 = __fmul_rn(dzy, wx8[2 * q + 1]);
+						float4 v = *(const float4*)(gc + oy + base + 2 * q);
+						acc.x = fmaf(v.x, d0, acc.x);
+						acc.y = fmaf(v.y, d0, acc.y);
+						acc.x = fmaf(v.z, d1, acc.x);
+						acc.y = fmaf(v.w, d1, acc.y);
+					}
+
+				} else {
+#pragma unroll
+					for (int e = 0; e < 6; e++) {
+
+						float d = __fmul_rn(dzy, tx.w[e]);
+						float2 v = gc[oy + tx.cell[e]];
+						acc.x = fmaf(v.x, d, acc.x);
+						acc.y = fmaf(v.y, d, acc.y);
+					}
 				}
 			}
 		}
