@@ -45,7 +45,6 @@ TOL, MAXITER = 1e-4, 300
 REF_ITERS_TO_TOL = 50
 METRIC = ("CG-SENSE recons/s to 1e-4 rel. normal-equation residual "
           "(2D radial 256^2, 16 coils, 96 spokes x 512, lambda 0.01)")
-HEADLINE = "fcg_circulant"
 WORKLOAD = "cgsense2d_256_c16_s96_tol1e-4_toeplitz"
 DOMINANT = "cols_toeplitz"
 L2_FLUSH_BYTES = 512 << 20     # > 126 MB L2
@@ -409,6 +408,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "batch"])
     ap.add_argument("--spokes", type=int, default=20000, help="nufft3d: kooshball spokes")
+    ap.add_argument("--methods", default="fcg_circulant,cg,fcg_learned",
+                    help="solvers to time (cgsense2d); the first is the headline")
+    ap.add_argument("--lean", action="store_true",
+                    help="skip the fixed-iteration, end-to-end and NUFFT extras (for profiling runs)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -461,9 +464,13 @@ def main():
     # the three solvers to 1e-4: the headline is the fastest, flexible CG
     # with the circulant PSF preconditioner; plain CG is the reference's
     # method, the learned correction is measured beside them
-    methods = {"cg": 0, "fcg_circulant": 1, "fcg_learned": 2}
+    all_methods = {"cg": 0, "fcg_circulant": 1, "fcg_learned": 2}
+    names = [m for m in args.methods.split(",") if m]
+    assert names and all(m in all_methods for m in names), f"--methods from {list(all_methods)}"
+    headline = names[0]
+    methods = {k: all_methods[k] for k in names}
     confs = {k: PicsConf(lam=LAM, maxiter=MAXITER, tol=TOL, toeplitz=True, precond=v) for k, v in methods.items()}
-    conf = confs[HEADLINE]
+    conf = confs[headline]
 
     def make(c):
         p = Pics(traj_d, sens_d, ksp_dims=list(ksp.shape), conf=c, traj_dims=list(traj.shape),
@@ -492,7 +499,7 @@ def main():
             step(c)
 
     info = {k: solve_info(c) for k, c in confs.items()}
-    iters, rres, tres, kernels_per_step = info[HEADLINE]
+    iters, rres, tres, kernels_per_step = info[headline]
 
     torch.cuda.synchronize()
     if world > 1:
@@ -506,7 +513,7 @@ def main():
     # the other methods, same steps
     method_lines = {}
     for k, c in confs.items():
-        mms = ms if k == HEADLINE else timed_steps(lambda: step(c), args.steps, flush, stream)
+        mms = ms if k == headline else timed_steps(lambda: step(c), args.steps, flush, stream)
         it_k, rr_k, tr_k, _ = info[k]
         method_lines[k] = {"recons_per_s": args.steps / (mms / 1e3), "ms_per_recon": mms / args.steps,
                            "iterations": it_k, "recursive_rel_residual": rr_k, "true_rel_residual": tr_k}
@@ -515,7 +522,7 @@ def main():
     # with the CG loop launched from the host (events cannot sit inside the
     # graph's while body) for exactly the iterations the solve took, so the
     # same kernels run on the same inputs
-    conf_prof = PicsConf(lam=LAM, maxiter=iters, tol=0.0, toeplitz=True, precond=methods[HEADLINE])
+    conf_prof = PicsConf(lam=LAM, maxiter=iters, tol=0.0, toeplitz=True, precond=methods[headline])
     lib.bnufft_prof_start(DOMINANT.encode())
     timed_steps(lambda: step(conf_prof), args.steps, flush, stream)
     kms, kn = ctypes.c_double(), ctypes.c_long()
@@ -523,7 +530,7 @@ def main():
 
     # the same solve at a fixed 30 iterations (Toeplitz on and off)
     fixed = {}
-    for toep in (True, False):
+    for toep in (() if args.lean else (True, False)):
         c = PicsConf(lam=LAM, maxiter=ITERS, toeplitz=toep)
         step(c)
         fms = timed_steps(lambda: step(c), max(3, args.steps // 4), flush, stream)
@@ -549,7 +556,10 @@ def main():
         ph.run(ksp_h, out=img_h)       # returns after the image is on the host
         ph.free()
 
-    step_host()
+    if args.lean:
+        e2e_steps = 0
+    else:
+        step_host()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -574,7 +584,7 @@ def main():
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get(DOMINANT)
 
-    nufft = nufft_throughput(dev) if rank == 0 else None
+    nufft = nufft_throughput(dev) if (rank == 0 and not args.lean) else None
 
     if rank == 0:
         value = aggregate_rate(world, args.steps, ms_max / 1e3)
@@ -588,10 +598,10 @@ def main():
                            "parallelism": f"replicas{world}",
                            "l2": "flushed before every timed step (512 MB write); inside a step the ~60 MB "
                                  "working set stays L2-resident across CG iterations"},
-                "e2e": {"value": aggregate_rate(world, e2e_steps, e2e_s), "unit": "recons/s",
+                "e2e": {"value": aggregate_rate(world, e2e_steps, e2e_s) if e2e_steps else None, "unit": "recons/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": kernels_per_step * args.steps,
-                "cg": {"method": HEADLINE, "iterations": iters, "recursive_rel_residual": rres,
+                "cg": {"method": headline, "iterations": iters, "recursive_rel_residual": rres,
                        "true_rel_residual": tres, "loop": "one CUDA graph with a while node per solve"},
                 "methods": method_lines,
                 "fixed_30_iters": fixed,
