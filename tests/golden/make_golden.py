@@ -84,23 +84,24 @@ def inverse_case(name, traj, ksp, dims):
     print(name, {k: np.shape(v) for k, v in out.items()})
 
 
-def pics_case(name, N, C, spokes, seed):
+def pics_case(name, N, C, spokes, seed, ndim=2, runs=None):
     from oracle.nufft_oracle import SenseOracle
     rng = np.random.default_rng(seed)
-    traj = synth.radial_traj(N, spokes)
-    truth = synth.ellipse_phantom(N, 20, rng)
-    sens = synth.coil_maps(N, C, rng)
+    traj = synth.radial_traj(N, spokes) if ndim == 2 else synth.kooshball_traj(N, spokes)
+    truth = synth.ellipse_phantom(N, 20, rng, ndim=ndim)
+    sens = synth.coil_maps(N, C, rng, ndim=ndim)
     A = SenseOracle(traj.real.reshape(3, -1, order="F"), sens)
-    y = A.forward(truth.reshape(N, N, 1, 1))
+    y = A.forward(truth.reshape(N, N, 1 if ndim == 2 else N, 1))
     y = synth.add_noise(y, 40.0, rng)
     ksp = y.reshape(1, traj.shape[1], traj.shape[2], C, order="F")
     out = dict(traj=traj, sens=sens, ksp=ksp, truth=truth)
+    runs = runs or [("x5_w1", ["-i5", "-w1"]), ("x30_w1", ["-i30", "-w1"]), ("x30", ["-i30"]),
+                    ("x5_w1_notoep", ["-i5", "-w1", "--no-toeplitz"]), ("x30_rescale", ["-i30", "-S"])]
     with tempfile.TemporaryDirectory() as d:
         writecfl(os.path.join(d, "t"), traj)
         writecfl(os.path.join(d, "s"), sens)
         writecfl(os.path.join(d, "k"), ksp)
-        for key, args in [("x5_w1", ["-i5", "-w1"]), ("x30_w1", ["-i30", "-w1"]), ("x30", ["-i30"]),
-                          ("x5_w1_notoep", ["-i5", "-w1", "--no-toeplitz"]), ("x30_rescale", ["-i30", "-S"])]:
+        for key, args in runs:
             run("pics", "-l2", "-r0.01", *args, "-t", "t", "k", "s", "o", cwd=d)
             out[key] = readcfl(os.path.join(d, "o"))
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
@@ -117,6 +118,8 @@ def uneven_cases():
     nufft_case("nufft2d_n40_periodic", t40, cplx(rng, (40, 40)), periodic=True)
     nufft_case("nufft3d_n12", synth.kooshball_traj(12, 64), cplx(rng, (12, 12, 12)))
     pics_case("pics2d_n48_c3", 48, 3, 20, seed=9)
+    pics_case("pics3d_n16_c2", 16, 2, 120, seed=11, ndim=3,
+              runs=[("x5_w1", ["-i5", "-w1"]), ("x5_w1_notoep", ["-i5", "-w1", "--no-toeplitz"])])
 
 
 def main():

@@ -20,14 +20,17 @@ def _run(g, **kw):
     return np.asarray(x), st
 
 
-@pytest.mark.parametrize("name", ["pics2d_n64_c4", "pics2d_n48_c3"])
-def test_pics_5_iterations_vs_reference(name):
+# Reconstructions: the bar is 1e-4 (per operator apply 1e-5). The 2D cases
+# hold 1e-5; in 3D each sample has 216 taps and float32 atomics add them in
+# an arbitrary order, measured 1.2e-5 after 5 iterations.
+@pytest.mark.parametrize("name,tol", [("pics2d_n64_c4", 1e-5), ("pics2d_n48_c3", 1e-5), ("pics3d_n16_c2", 5e-5)])
+def test_pics_5_iterations_vs_reference(name, tol):
     g = golden(name)
     x, st = _run(g, maxiter=5, scaling=1.0)
     assert st[0] == 5
-    assert rel(x, g["x5_w1"]) < 1e-5
+    assert rel(x, g["x5_w1"]) < tol
     x, st = _run(g, maxiter=5, scaling=1.0, toeplitz=False)
-    assert rel(x, g["x5_w1_notoep"]) < 1e-5
+    assert rel(x, g["x5_w1_notoep"]) < tol
 
 
 def test_pics_30_iterations_vs_reference():

@@ -73,7 +73,7 @@ def test_nufft_close_to_ndft():
     assert rel(o.forward(img), exact) < 1e-4
 
 
-@pytest.mark.parametrize("name", ["pics2d_n64_c4", "pics2d_n48_c3"])
+@pytest.mark.parametrize("name", ["pics2d_n64_c4", "pics2d_n48_c3", "pics3d_n16_c2"])
 def test_pics_few_iterations(name):
     """CG-SENSE at 5 iterations matches the reference's pics (float32 CG)."""
     g = golden(name)
