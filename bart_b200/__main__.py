@@ -51,6 +51,7 @@ def main_nufft(argv) -> int:
     ap.add_argument("-l", dest="lam", type=float, default=0.0)
     ap.add_argument("-m", dest="iters", type=int, default=50)
     ap.add_argument("-p", dest="pattern")
+    ap.add_argument("-s", dest="dft", action="store_true", help="direct non-uniform DFT")
     ap.add_argument("traj")
     ap.add_argument("input")
     ap.add_argument("output")
@@ -64,6 +65,23 @@ def main_nufft(argv) -> int:
     conf = NufftConf(toeplitz=a.inverse and not a.no_toeplitz, periodic=a.periodic)
     inp = readcfl(a.input)
     pat = readcfl(a.pattern) if a.pattern else None
+    if a.dft:   # src/nufft.c:244, 297 (no basis, no pattern)
+        from .nufft import Nudft
+        if a.inverse or pat is not None:
+            sys.stderr.write("-s: forward and adjoint only, without -p\n")
+            return 1
+        if a.adjoint:
+            kd = list(inp.shape)
+            cd = (a.dims or estimate_im_dims(traj)) + kd[3:]
+            op = Nudft(kd, cd, tdims, traj)
+            writecfl(a.output, op.adjoint(inp).reshape(cd, order="F"))
+        else:
+            cd = list(inp.shape)
+            kd = [1, tdims[1], tdims[2]] + cd[3:]
+            op = Nudft(kd, cd, tdims, traj)
+            writecfl(a.output, op.forward(inp).reshape(kd, order="F"))
+        op.free()
+        return 0
     if a.inverse:
         kd = list(inp.shape)
         cd = (a.dims or estimate_im_dims(traj)) + kd[3:]

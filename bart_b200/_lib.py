@@ -66,6 +66,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     sig("bnufft_pics_kernels", i, vp, ctypes.POINTER(ctypes.c_long), vp)
     sig("bnufft_pics_free", None, vp)
     sig("bnufft_pics_rhs", i, vp, vp, vp, vp)
+    sig("bnufft_nudft_create", i, ctypes.POINTER(vp), i, cl, cl, cl, vp, vp)
+    sig("bnufft_nudft_apply_forward", i, vp, vp, vp, vp)
+    sig("bnufft_nudft_apply_adjoint", i, vp, vp, vp, vp)
+    sig("bnufft_nudft_free", None, vp)
     sig("bnufft_batch_create", i, ctypes.POINTER(vp), ctypes.POINTER(vp), i, ctypes.POINTER(vp),
         ctypes.POINTER(vp), vp)
     sig("bnufft_batch_run", i, vp, vp)

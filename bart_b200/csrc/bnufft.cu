@@ -23,6 +23,7 @@
 #include "cg_kernels.cuh"
 #include "gridding.cuh"
 #include "precnet.cuh"
+#include "nudft.cuh"
 
 using namespace bn;
 
@@ -2057,6 +2058,122 @@ extern "C" int bnufft_nufft_inverse(bnufft_plan_t p, void* img, const void* ksp,
 // ----------------------------------------------------------------------------
 // CG-SENSE (C ABI)
 // ----------------------------------------------------------------------------
+
+// ----------------------------------------------------------------------------
+// direct non-uniform DFT (C ABI: bnufft_nudft_*)
+// ----------------------------------------------------------------------------
+
+struct bnufft_nudft_s {
+
+	NudftGeom g;
+	float4* traj = nullptr;		// [M] (kx, ky, kz, 0)
+	cudaStream_t st0 = nullptr;
+};
+
+extern "C" void bnufft_nudft_free(bnufft_nudft_t p)
+{
+	if (!p)
+		return;
+
+	if (p->traj)
+		cudaFreeAsync(p->traj, p->st0);
+
+	delete p;
+}
+
+extern "C" int bnufft_nudft_create(bnufft_nudft_t* out, int N, const long ksp_dims[], const long cim_dims[],
+		const long traj_dims[], const void* traj, void* stream)
+{
+	cudaStream_t st = S(stream);
+
+	if (!out || !ksp_dims || !cim_dims || !traj_dims || !traj || (N < 4))
+		return fail(BNUFFT_ERR_ARG, "null argument or fewer than 4 dims");
+
+	if ((3 != traj_dims[0]) || (1 != ksp_dims[0]) || (ksp_dims[1] != traj_dims[1]) || (ksp_dims[2] != traj_dims[2]))
+		return fail(BNUFFT_ERR_ARG, "trajectory [3, Mr, Ms] and k-space [1, Mr, Ms, ...] do not match");
+
+	for (int i = 3; i < N; i++)
+		if ((i < N) && (traj_dims[i] != 1))
+			return fail(BNUFFT_ERR_UNSUPPORTED, "trajectory with dims beyond 2");
+
+	long C = prod(N - 3, cim_dims + 3);
+
+	if (prod(N - 3, ksp_dims + 3) != C)
+		return fail(BNUFFT_ERR_ARG, "k-space and image batch dims differ");
+
+	auto p = new bnufft_nudft_s();
+	p->st0 = st;
+
+	for (int a = 0; a < 3; a++)
+		p->g.N[a] = (int)cim_dims[a];
+
+	p->g.npix = (long)cim_dims[0] * cim_dims[1] * cim_dims[2];
+	p->g.M = traj_dims[1] * traj_dims[2];
+	p->g.C = C;
+	// the reference scales by all image dims, coils included (nudft_forward2,
+	// src/noncart/nudft.c:122-124)
+	p->g.scale = (float)(1. / sqrt((double)(p->g.npix * C)));
+
+	Staged t;
+	int s = stage_in(t, traj, sizeof(float2) * 3 * p->g.M, st);
+	cudaError_t e = cudaSuccess;
+
+	if (BNUFFT_OK == s)
+		e = cudaMallocAsync(&p->traj, sizeof(float4) * p->g.M, st);
+
+	if ((BNUFFT_OK == s) && (cudaSuccess != e))
+		s = fail(BNUFFT_ERR_NOMEM, "nudft trajectory: %s", cudaGetErrorString(e));
+
+	if (BNUFFT_OK == s) {
+
+		k_traj_convert<<<vec_blocks(p->g.M), RED_THREADS, 0, st>>>(p->traj, (const float2*)t.dev, p->g.M, 1.f);
+		e = cudaGetLastError();
+		g_launches.fetch_add(1, std::memory_order_relaxed);
+
+		if (cudaSuccess != e)
+			s = fail(BNUFFT_ERR_CUDA, "nudft trajectory: %s", cudaGetErrorString(e));
+	}
+
+	if ((BNUFFT_OK == s) && t.owned)
+		e = cudaStreamSynchronize(st);
+
+	if (BNUFFT_OK != s) {
+
+		std::string msg = g_err;
+		bnufft_nudft_free(p);
+		g_err = msg;
+		return s;
+	}
+
+	*out = p;
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_nudft_apply_forward(bnufft_nudft_t p, void* ksp, const void* cim, void* stream)
+{
+	cudaStream_t st = S(stream);
+	const NudftGeom& g = p->g;
+	Staged i, o;
+	TRY(stage_in(i, cim, sizeof(float2) * g.npix * g.C, st));
+	TRY(stage_out_alloc(o, ksp, sizeof(float2) * g.M * g.C, st));
+	dim3 grid((unsigned)((g.M + NUDFT_THREADS - 1) / NUDFT_THREADS), (unsigned)((g.C + NUDFT_CC - 1) / NUDFT_CC));
+	k_nudft_fwd<<<grid, NUDFT_THREADS, 0, st>>>(p->traj, g, (const float2*)i.dev, (float2*)o.dev);
+	LAUNCHED();
+	return stage_out_copy(o, ksp, sizeof(float2) * g.M * g.C, st);
+}
+
+extern "C" int bnufft_nudft_apply_adjoint(bnufft_nudft_t p, void* cim, const void* ksp, void* stream)
+{
+	cudaStream_t st = S(stream);
+	const NudftGeom& g = p->g;
+	Staged i, o;
+	TRY(stage_in(i, ksp, sizeof(float2) * g.M * g.C, st));
+	TRY(stage_out_alloc(o, cim, sizeof(float2) * g.npix * g.C, st));
+	dim3 grid((unsigned)((g.npix + NUDFT_THREADS - 1) / NUDFT_THREADS), (unsigned)((g.C + NUDFT_CC - 1) / NUDFT_CC));
+	k_nudft_adj<<<grid, NUDFT_THREADS, 0, st>>>(p->traj, g, (const float2*)i.dev, (float2*)o.dev);
+	LAUNCHED();
+	return stage_out_copy(o, cim, sizeof(float2) * g.npix * g.C, st);
+}
 
 // ----------------------------------------------------------------------------
 // learned preconditioner network (C ABI: bnufft_precnet_*)

@@ -197,3 +197,46 @@ def nufft_create(ksp_dims, cim_dims, traj_dims, traj, weights=None, conf: NufftC
     """nufft_create (src/noncart/nufft.c:1315): weights share the traj dims."""
     wd = None if weights is None else [1] + list(dims16(traj_dims))[1:]
     return nufft_create2(ksp_dims, cim_dims, traj_dims, traj, wd, weights, None, None, conf)
+
+
+class Nudft:
+    """nudft_create (src/noncart/nudft.c:331): the exact non-uniform DFT as a
+    linop (``bart nufft -s``), scaled like the reference (1/sqrt of all image
+    dims, coils included)."""
+
+    def __init__(self, ksp_dims, cim_dims, traj_dims, traj):
+        lib = _lib.load()
+        kd, cd, td = dims16(ksp_dims), dims16(cim_dims), dims16(traj_dims)
+        pt, keep = _ptr_in(traj, int(np.prod(td)))
+        h = ctypes.c_void_p()
+        _lib.check(lib.bnufft_nudft_create(ctypes.byref(h), 16, _lib.dims_array(kd), _lib.dims_array(cd),
+                                           _lib.dims_array(td), pt, _stream_of(traj)))
+        del keep
+        self._h = h
+        self.domain_dims, self.codomain_dims = cd, kd
+
+    def _call(self, fn, src, dst, in_dims, out_dims):
+        nin, nout = int(np.prod(in_dims)), int(np.prod(out_dims))
+        if dst is None:
+            dst = _alloc_like(src, out_dims)
+        ps, keep = _ptr_in(src, nin)
+        _lib.check(fn(self._h, _ptr_out(dst, nout), ps, _stream_of(src, dst)))
+        del keep
+        return dst
+
+    def forward(self, src, dst=None):
+        return self._call(_lib.load().bnufft_nudft_apply_forward, src, dst, self.domain_dims, self.codomain_dims)
+
+    def adjoint(self, src, dst=None):
+        return self._call(_lib.load().bnufft_nudft_apply_adjoint, src, dst, self.codomain_dims, self.domain_dims)
+
+    def free(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.load().bnufft_nudft_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -165,6 +165,20 @@ void bnufft_pics_free(bnufft_pics_t pics);
  * graph reads them from the device, so it is kept). */
 int bnufft_pics_set_iter(bnufft_pics_t pics, int maxiter, float tol);
 
+/* Direct non-uniform DFT, replaces nudft_create / nudft_forward2 /
+ * nudft_adjoint2 (src/noncart/nudft.c:69-348; `bart nufft -s`):
+ * ksp[m, c] = s sum_n img[n, c] exp(-2 pi i k_m . (n - N/2) / N) and its
+ * adjoint, s = 1 / sqrt(product of all image dims, coils included) as in the
+ * reference. Same dims as bnufft_create2. No field map / time map. Exact
+ * (float64-reduced phases), O(samples x pixels): for small sizes. */
+typedef struct bnufft_nudft_s* bnufft_nudft_t;
+
+int bnufft_nudft_create(bnufft_nudft_t* nudft, int N, const long ksp_dims[], const long cim_dims[],
+		const long traj_dims[], const void* traj, void* stream);
+int bnufft_nudft_apply_forward(bnufft_nudft_t nudft, void* ksp, const void* cim, void* stream);
+int bnufft_nudft_apply_adjoint(bnufft_nudft_t nudft, void* cim, const void* ksp, void* stream);
+void bnufft_nudft_free(bnufft_nudft_t nudft);
+
 /* Batches (no counterpart in the reference, which runs one pics per problem,
  * src/pics.c, or loops with bart -p/-l, src/bart.c:202-217): n independent
  * models, each with its own size, trajectory, coil count and maps, and their

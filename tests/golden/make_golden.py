@@ -70,6 +70,24 @@ def nufft_case(name, traj, img, periodic=False, normal=True, pattern=None):
     print(name, {k: np.shape(v) for k, v in out.items()})
 
 
+def nudft_case(name, traj, img):
+    """bart nufft -s (direct DFT), forward and adjoint."""
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "t"), traj)
+        writecfl(os.path.join(d, "x"), img)
+        run("nufft", "-s", "t", "x", "k", cwd=d)
+        fwd = readcfl(os.path.join(d, "k"))
+        ksp = cplx(rng, fwd.shape)
+        writecfl(os.path.join(d, "y"), ksp)
+        dims = ":".join(str(s) for s in (list(img.shape) + [1, 1])[:3])
+        run("nufft", "-s", "-a", f"-x{dims}", "t", "y", "a", cwd=d)
+        adj = readcfl(os.path.join(d, "a"))
+    out = dict(traj=traj, img=img, fwd=fwd, ksp=ksp, adj=adj)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **{k: np.asarray(v) for k, v in out.items()})
+    print(name, {k: np.shape(v) for k, v in out.items()})
+
+
 def inverse_case(name, traj, ksp, dims):
     out = dict(traj=traj, ksp=ksp)
     with tempfile.TemporaryDirectory() as d:
@@ -108,6 +126,18 @@ def pics_case(name, N, C, spokes, seed, ndim=2, runs=None):
     print(name, {k: np.shape(v) for k, v in out.items()})
 
 
+def t24_traj():
+    with tempfile.TemporaryDirectory() as d:
+        run("traj", "-r", "-G", "-x24", "-o2", "-y10", "t", cwd=d)
+        return readcfl(os.path.join(d, "t"))
+
+
+def t16_traj():
+    with tempfile.TemporaryDirectory() as d:
+        run("traj", "-r", "-G", "-x16", "-o2", "-y8", "t", cwd=d)
+        return readcfl(os.path.join(d, "t"))
+
+
 def uneven_cases():
     """Image sides that are not powers of two (grids of 2N cells)."""
     rng = np.random.default_rng(20261204)
@@ -118,6 +148,8 @@ def uneven_cases():
     nufft_case("nufft2d_n40_periodic", t40, cplx(rng, (40, 40)), periodic=True)
     nufft_case("nufft3d_n12", synth.kooshball_traj(12, 64), cplx(rng, (12, 12, 12)))
     pics_case("pics2d_n48_c3", 48, 3, 20, seed=9)
+    nudft_case("nudft2d_n24", t24_traj(), cplx(rng, (24, 24)))
+    nudft_case("nudft2d_n16_coils2", t16_traj(), cplx(rng, (16, 16, 1, 2)))
     pics_case("pics3d_n16_c2", 16, 2, 120, seed=11, ndim=3,
               runs=[("x5_w1", ["-i5", "-w1"]), ("x5_w1_notoep", ["-i5", "-w1", "--no-toeplitz"])])
 

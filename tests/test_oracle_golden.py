@@ -113,3 +113,20 @@ def test_nufft_inverse_and_circulant_precond(key, kw):
     o = orc.NufftOracle(g["traj"].real.reshape(3, -1, order="F"), (32, 32, 1))
     x = orc.nufft_inverse(o, g["ksp"].reshape(-1, 3, order="F"), **kw)
     assert rel(x, g[key].reshape(32, 32, 1, 3, order="F")) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["nudft2d_n24", "nudft2d_n16_coils2"])
+def test_ndft_vs_reference_nudft(name):
+    """The FP64 NDFT against the reference's direct DFT (bart nufft -s). The
+    reference scales by all image dims, coils included, and forms its phases
+    in float32 (linear_phase, src/num/filter.c:256-265)."""
+    g = golden(name)
+    img = g["img"]
+    while img.ndim < 4:
+        img = img[..., None]
+    C = img.shape[3]
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    s = 1.0 / np.sqrt(C)
+    assert rel(orc.ndft_forward(traj, img) * s, g["fwd"].reshape(-1, C, order="F")) < 2e-5
+    adj = orc.ndft_adjoint(traj, g["ksp"].reshape(-1, C, order="F"), img.shape[:3]) * s
+    assert rel(adj, g["adj"].reshape(adj.shape, order="F")) < 2e-5
