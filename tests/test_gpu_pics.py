@@ -152,3 +152,25 @@ def test_fcg_circulant_converges_faster():
     x = out[1, "1"][0].reshape(xo.shape, order="F")
     assert orc.normal_residual(A, x, b, 0.01) < 1e-5
     assert rel(x, xo) < 5e-4      # the problem's float32 sensitivity (see the converged test)
+
+
+@pytest.mark.parametrize("name", ["pics2d_n48_c3", "pics3d_n16_c2"])
+def test_fcg_circulant_uneven_and_3d(name):
+    """Flexible CG with the circulant preconditioner on a non-power-of-two 2D
+    size (Bluestein grid DFTs, power-of-two Toeplitz embedding) and in 3D:
+    converges to the FP64 oracle's solution in fewer iterations than CG."""
+    g = golden(name)
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    C = g["sens"].shape[3]
+    A = orc.SenseOracle(traj, g["sens"])
+    b = A.adjoint(g["ksp"].reshape(-1, C, order="F"))
+    its = {}
+    for pc in (0, 1):
+        p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
+                 conf=PicsConf(lam=0.01, maxiter=400, tol=1e-6, scaling=1.0, precond=pc))
+        x = np.asarray(p.run(g["ksp"]))
+        its[pc] = p.stats()[0]
+        p.free()
+        xr = x.reshape(b.shape, order="F")
+        assert orc.normal_residual(A, xr, b, 0.01) < 2e-5, pc
+    assert its[1] < its[0], its
