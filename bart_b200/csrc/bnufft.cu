@@ -2521,6 +2521,8 @@ struct bnufft_pics_s {
 	double* dots_part = nullptr;	// <z, A p_j> partials [FCG_MAX_M][nparts]
 	double* pr_part = nullptr;	// <p, r>, one per direction-update block
 	int fcg_m = 1;			// truncation: directions orthogonalised against
+	int ndots = 0;			// preconditioner last-pass blocks (folded <z, A p> partials)
+	bool fcg_fold = true;		// fold the dot and test launches (BNUFFT_FCG_FOLD=0: not)
 	bnufft_precnet_t net = nullptr;	// learned correction (conf.precond == 2), not owned
 	double* mcn_part = nullptr;	// ||M_circ(r)||^2 partials
 	bf16* nact[2] = { nullptr, nullptr };	// its activations, ping-pong [npix][32]
@@ -2662,10 +2664,14 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 		if (const char* e = getenv("BNUFFT_FCG_M"))
 			ps->fcg_m = std::max(1, std::min((int)FCG_MAX_M, atoi(e)));
 
+		if (const char* e = getenv("BNUFFT_FCG_FOLD"))
+			ps->fcg_fold = (0 != strcmp(e, "0"));
+
 		ck(cudaMallocAsync(&ps->z, sizeof(float2) * ps->npix, st));
 		ck(cudaMallocAsync(&ps->p_ring, sizeof(float2) * ps->npix * FCG_RING, st));
 		ck(cudaMallocAsync(&ps->ap_ring, sizeof(float2) * ps->npix * FCG_RING, st));
-		ck(cudaMallocAsync(&ps->dots_part, sizeof(double) * ps->nparts * FCG_MAX_M, st));
+		ck(cudaMallocAsync(&ps->dots_part, sizeof(double) * std::max<long>((long)ps->nparts * FCG_MAX_M,
+				ps->max_row_blocks), st));
 		ck(cudaMallocAsync(&ps->pr_part, sizeof(double) * ps->nparts, st));
 
 		if (BNUFFT_OK == s)
@@ -2851,7 +2857,10 @@ static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, cons
 
 // One flexible-CG iteration: <z, A p_j> over the kept directions, the
 // direction update, the normal operator's passes (as in plain CG), the step,
-// the convergence test and z = M(r) for the next iteration.
+// the convergence test and z = M(r) for the next iteration. With the linear
+// circulant preconditioner and one kept direction (the default of precond
+// 1) two launches are folded away: <z, A p> comes from the preconditioner's
+// last pass and the convergence test runs in the next direction update.
 static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 {
 	OpCtx& op = toe_ctx(ps->nufft);
@@ -2861,11 +2870,18 @@ static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	float2* p = ps->pbuf[1];
 	unsigned nb = (unsigned)ps->nparts;
 	int npap = 0;
+	const bool folded = (1 == ps->conf.precond) && (1 == ps->fcg_m) && ps->fcg_fold;
+	const int ring = (1 == ps->fcg_m) ? 1 : (int)FCG_RING;
 
-	k_fcgm_dots<<<nb, RED_THREADS, 0, st>>>(ps->z, ps->ap_ring, ps->npix, ps->scal, it, ps->fcg_m, ps->dots_part);
-	LAUNCHED();
-	k_fcgm_dir<<<nb, RED_THREADS, 0, st>>>(p, ps->p_ring, ps->z, ps->r, ps->npix, ps->scal, it, ps->fcg_m,
-			ps->dots_part, ps->nparts, ps->pr_part, ps->pp_part);
+	if (!folded) {
+
+		k_fcgm_dots<<<nb, RED_THREADS, 0, st>>>(ps->z, ps->ap_ring, ps->npix, ps->scal, it, ps->fcg_m, ring, ps->dots_part);
+		LAUNCHED();
+	}
+
+	k_fcgm_dir<<<nb, RED_THREADS, 0, st>>>(p, ps->p_ring, ps->z, ps->r, ps->npix, ps->scal, it, ps->fcg_m, ring,
+			ps->dots_part, folded ? ps->ndots : ps->nparts, ps->pr_part, ps->pp_part,
+			folded ? ps->rs_part : nullptr, ps->nparts);
 	LAUNCHED();
 	TRY(rows_fwd(g.G[0], p, ps->sens, nullptr, nullptr, g.N[0], YZ, YZ * ps->C, op.w.t1, st, done));
 	TRY(op_toeplitz_cols(op, toe_psf(ps->nufft), ps->C, st, done));
@@ -2875,10 +2891,22 @@ static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	if (npap > ps->max_row_blocks)
 		return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
 
-	k_fcg_step<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, p, ps->ap_ring, ps->part, ps->groups, ps->npix,
+	k_fcg_step<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, p, ps->ap_ring, ring, ps->part, ps->groups, ps->npix,
 			ps->conf.lambda, ps->scal, it, ps->pap_part, npap, ps->pp_part, ps->nparts, ps->pr_part, ps->nparts,
 			ps->rs_part);
 	LAUNCHED();
+
+	if (folded) {
+
+		int nd = 0;
+		TRY(pics_precond(ps, ps->r, ps->z, ps->ap_ring, ps->dots_part, &nd, st));
+
+		if (nd != ps->ndots)
+			return fail(BNUFFT_ERR_ARG, "internal: preconditioner block count changed");
+
+		return BNUFFT_OK;
+	}
+
 	k_fcg_check<<<1, RED_THREADS, 0, st>>>(ps->scal, it, ps->rs_part, ps->nparts);
 	LAUNCHED();
 	return pics_precond(ps, ps->r, ps->z, nullptr, nullptr, nullptr, st);
@@ -2973,8 +3001,16 @@ static int pics_solve(bnufft_pics_s* ps, const float2* ksp, float2* out, cudaStr
 	if (ps->nufft->embed)
 		TRY(alloc_work(ps->nufft->toe.w, ps->nufft->toe.g, ps->C, st));
 
-	if (ps->conf.precond)	// z0 = M(b); the first direction is p = z0
-		TRY(pics_precond(ps, ps->r, ps->z, nullptr, nullptr, nullptr, st));
+	if (ps->conf.precond) {	// z0 = M(b); the first direction is p = z0
+
+		int nd = 0;
+		TRY(pics_precond(ps, ps->r, ps->z, nullptr, nullptr, &nd, st));
+
+		if (nd > ps->max_row_blocks)
+			return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
+
+		ps->ndots = nd;		// the folded iteration's <z, A p> partials per launch
+	}
 
 	if (ps->conf.maxiter > 0) {
 

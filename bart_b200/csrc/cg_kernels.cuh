@@ -264,7 +264,7 @@ __global__ void k_precond_from_spectrum(float2* __restrict__ pinv, const float2*
 // w = min(it - restart, m) (the history restarts when the preconditioner changes):
 // part[q * gridDim.x + block], q = j - (it - w)
 __global__ void k_fcgm_dots(const float2* __restrict__ z, const float2* __restrict__ ap_ring, long n,
-		const CgScalars* st, int it, int m, double* __restrict__ part)
+		const CgScalars* st, int it, int m, int ring, double* __restrict__ part)
 {
 	__shared__ double sh[32];
 
@@ -286,7 +286,7 @@ __global__ void k_fcgm_dots(const float2* __restrict__ z, const float2* __restri
 
 			if (q < w) {
 
-				float2 a = ap_ring[(long)((it - w + q) % FCG_RING) * n + i];
+				float2 a = ap_ring[(long)((it - w + q) % ring) * n + i];
 				acc[q] += (double)zv.x * (double)a.x + (double)zv.y * (double)a.y;
 			}
 		}
@@ -310,8 +310,8 @@ __global__ void k_fcgm_dots(const float2* __restrict__ z, const float2* __restri
 // direction: p = z - sum_q beta_q p_{it-w+q}; p into p_cur and ring slot
 // it % FCG_RING; partials <p, r> and ||p||^2 (lambda ||p||^2 in <p, A p>)
 __global__ void k_fcgm_dir(float2* __restrict__ p_cur, float2* __restrict__ p_ring, const float2* __restrict__ z,
-		const float2* __restrict__ r, long n, const CgScalars* st, int it, int m, const double* __restrict__ dots,
-		int ndots, double* __restrict__ pr_part, double* __restrict__ pp_part)
+		const float2* __restrict__ r, long n, CgScalars* st, int it, int m, int ring, const double* __restrict__ dots,
+		int ndots, double* __restrict__ pr_part, double* __restrict__ pp_part, const double* __restrict__ rs_part, int nrs)
 {
 	__shared__ double sh[32];
 	__shared__ float beta[FCG_MAX_M];
@@ -320,6 +320,28 @@ __global__ void k_fcgm_dir(float2* __restrict__ p_cur, float2* __restrict__ p_ri
 		return;
 
 	it = cg_iter(it, st);
+
+	// with rs_part: the convergence test of the previous step is done here
+	// (every block reaches the same decision from the same partial sums)
+	if (rs_part && (it > 0)) {
+
+		double rs = sum_partials(rs_part, nrs, sh);
+
+		if ((0 == blockIdx.x) && (0 == threadIdx.x)) {
+
+			st->rs[it & 1] = rs;
+
+			if (rs <= st->eps2) {
+
+				st->done = 1;
+				st->iters = it;
+			}
+		}
+
+		if (rs <= st->eps2)
+			return;
+	}
+
 	const int w = min(it - st->restart_it, m);
 
 	for (int q = 0; q < w; q++) {
@@ -327,12 +349,12 @@ __global__ void k_fcgm_dir(float2* __restrict__ p_cur, float2* __restrict__ p_ri
 		double d = sum_partials(dots + q * ndots, ndots, sh);
 
 		if (0 == threadIdx.x)
-			beta[q] = (float)(d / st->pap_hist[(it - w + q) % FCG_RING]);
+			beta[q] = (float)(d / st->pap_hist[(it - w + q) % ring]);
 	}
 
 	__syncthreads();
 
-	float2* p_slot = p_ring + (long)(it % FCG_RING) * n;
+	float2* p_slot = p_ring + (long)(it % ring) * n;
 	double pr = 0., pp = 0.;
 
 	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -341,7 +363,7 @@ __global__ void k_fcgm_dir(float2* __restrict__ p_cur, float2* __restrict__ p_ri
 
 		for (int q = 0; q < w; q++) {
 
-			float2 o = p_ring[(long)((it - w + q) % FCG_RING) * n + i];
+			float2 o = p_ring[(long)((it - w + q) % ring) * n + i];
 			pv.x = fmaf(-beta[q], o.x, pv.x);
 			pv.y = fmaf(-beta[q], o.y, pv.y);
 		}
@@ -368,7 +390,7 @@ __global__ void k_fcgm_dir(float2* __restrict__ p_cur, float2* __restrict__ p_ri
 // <p, r> / <p, A p>; per element A p = sum_g part_g + lambda p (into ring
 // slot it % FCG_RING), x += alpha p, r -= alpha A p, partial ||r||^2.
 __global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const float2* __restrict__ p,
-		float2* __restrict__ ap_ring, const float2* __restrict__ part, int groups, long n, float lam, CgScalars* st, int it,
+		float2* __restrict__ ap_ring, int ring, const float2* __restrict__ part, int groups, long n, float lam, CgScalars* st, int it,
 		const double* __restrict__ pap_part, int npap, const double* __restrict__ pp_part, int npp,
 		const double* __restrict__ pr_part, int npr, double* __restrict__ rs_part)
 {
@@ -392,7 +414,7 @@ __global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const
 	}
 
 	float a = (float)(sum_partials(pr_part, npr, sh) / pAp);
-	float2* Ap = ap_ring + (long)(it % FCG_RING) * n;
+	float2* Ap = ap_ring + (long)(it % ring) * n;
 	double acc = 0.;
 
 	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -424,7 +446,7 @@ __global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const
 		rs_part[blockIdx.x] = s;
 
 	if ((0 == blockIdx.x) && (0 == threadIdx.x))
-		st->pap_hist[it % FCG_RING] = pAp;
+		st->pap_hist[it % ring] = pAp;
 }
 
 // FCG convergence test after step it: ||r||^2 <= eps2 stops with it + 1

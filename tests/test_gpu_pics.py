@@ -174,3 +174,29 @@ def test_fcg_circulant_uneven_and_3d(name):
         xr = x.reshape(b.shape, order="F")
         assert orc.normal_residual(A, xr, b, 0.01) < 2e-5, pc
     assert its[1] < its[0], its
+
+
+def test_fcg_folded_launches_match_unfolded():
+    """The folded circulant flexible CG (dot products from the
+    preconditioner's last pass, convergence test in the next direction
+    update) solves like the unfolded one: about the same iterations, the
+    same solution to the problem's float32 sensitivity at this tolerance,
+    fewer launches."""
+    g = golden("pics2d_n64_c4")
+    res = {}
+    for fold in ("1", "0"):
+        os.environ["BNUFFT_FCG_FOLD"] = fold
+        try:
+            p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
+                     conf=PicsConf(lam=0.01, maxiter=300, tol=1e-5, scaling=1.0, precond=1))
+            x = np.asarray(p.run(g["ksp"]))
+            res[fold] = (x, p.stats(), p.kernels())
+            p.free()
+        finally:
+            os.environ.pop("BNUFFT_FCG_FOLD", None)
+    (xf, sf, kf), (xu, su, ku) = res["1"], res["0"]
+    # float32 rounding in another summation order moves the stopping
+    # iteration by a few near the tolerance
+    assert abs(sf[0] - su[0]) <= max(3, su[0] // 10) and sf[1] <= 1e-5 and su[1] <= 1e-5
+    assert rel(xf, xu) < 2e-3
+    assert kf < ku

@@ -95,6 +95,7 @@ def test_learned_fcg_zero_network_equals_circulant():
     net = precnet.PrecNet(precnet.init_params(3))
     out = {}
     os.environ["BNUFFT_FCG_M"] = "1"     # the same truncation for both
+    os.environ["BNUFFT_FCG_FOLD"] = "0"  # and the same launches (no folded dot products)
     try:
         for pc in (1, 2):
             p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
@@ -105,6 +106,7 @@ def test_learned_fcg_zero_network_equals_circulant():
             p.free()
     finally:
         os.environ.pop("BNUFFT_FCG_M", None)
+        os.environ.pop("BNUFFT_FCG_FOLD", None)
     net.free()
     assert np.array_equal(out[1][0].view(np.uint32), out[2][0].view(np.uint32))
     assert out[1][1] == out[2][1]
