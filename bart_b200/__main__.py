@@ -52,6 +52,7 @@ def main_nufft(argv) -> int:
     ap.add_argument("-m", dest="iters", type=int, default=50)
     ap.add_argument("-p", dest="pattern")
     ap.add_argument("-s", dest="dft", action="store_true", help="direct non-uniform DFT")
+    ap.add_argument("--lowmem", action="store_true", help="one coil's oversampled grid at a time")
     ap.add_argument("traj")
     ap.add_argument("input")
     ap.add_argument("output")
@@ -62,7 +63,7 @@ def main_nufft(argv) -> int:
     traj = readcfl(a.traj)
     tdims = list(traj.shape)
     # the PSF is only built for the inverse (src/nufft.c:121-122); Toeplitz is on by default there
-    conf = NufftConf(toeplitz=a.inverse and not a.no_toeplitz, periodic=a.periodic)
+    conf = NufftConf(toeplitz=a.inverse and not a.no_toeplitz, periodic=a.periodic, lowmem=a.lowmem)
     inp = readcfl(a.input)
     pat = readcfl(a.pattern) if a.pattern else None
     if a.dft:   # src/nufft.c:244, 297 (no basis, no pattern)

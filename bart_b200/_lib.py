@@ -18,7 +18,7 @@ c_long_p = ctypes.POINTER(ctypes.c_long)
 
 class NufftConfC(ctypes.Structure):
     _fields_ = [("toeplitz", ctypes.c_int), ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int),
-                ("os", ctypes.c_float), ("width", ctypes.c_float), ("bin", ctypes.c_int)]
+                ("os", ctypes.c_float), ("width", ctypes.c_float), ("bin", ctypes.c_int), ("lowmem", ctypes.c_int)]
 
 
 class PicsConfC(ctypes.Structure):

@@ -1587,6 +1587,7 @@ extern "C" void bnufft_conf_defaults(struct bnufft_conf* conf)
 	conf->os = 2.f;
 	conf->width = 6.f;
 	conf->bin = 0;
+	conf->lowmem = 0;
 }
 
 static int check_conf(const bnufft_conf* conf)
@@ -1727,6 +1728,9 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 
 			p->op.wgt = p->wgt;
 			p->op.wgt_c = wc;
+
+			if ((BNUFFT_OK == s) && conf.lowmem && (wc > 1))
+				s = fail(BNUFFT_ERR_UNSUPPORTED, "--lowmem with per-coil weights");
 		}
 	}
 
@@ -1757,27 +1761,41 @@ extern "C" int bnufft_update_traj(bnufft_plan_t p, int N, const long traj_dims[]
 	return upload_traj(p, traj, S(stream));
 }
 
+// coils per apply pass: all, or one with --lowmem (the work grids then hold
+// one coil; results are the same)
+static long coil_chunk(const bnufft_plan_s* p) { return p->conf.lowmem ? 1 : p->C; }
+
 extern "C" int bnufft_apply_forward(bnufft_plan_t p, void* dst, const void* src, void* stream)
 {
 	cudaStream_t st = S(stream);
-	size_t in_b = sizeof(float2) * p->op.g.npix * p->C;
-	size_t out_b = sizeof(float2) * p->op.g.M * p->C;
+	const long npix = p->op.g.npix, M = p->op.g.M, cc = coil_chunk(p);
+	size_t in_b = sizeof(float2) * npix * p->C;
+	size_t out_b = sizeof(float2) * M * p->C;
 	Staged i, o;
 	TRY(stage_in(i, src, in_b, st));
 	TRY(stage_out_alloc(o, dst, out_b, st));
-	TRY(op_forward(p->op, (const float2*)i.dev, nullptr, p->C, (float2*)o.dev, st));
+
+	for (long c0 = 0; c0 < p->C; c0 += cc)
+		TRY(op_forward(p->op, (const float2*)i.dev + npix * c0, nullptr, std::min(cc, p->C - c0),
+				(float2*)o.dev + M * c0, st));
+
 	return stage_out_copy(o, dst, out_b, st);
 }
 
 extern "C" int bnufft_apply_adjoint(bnufft_plan_t p, void* dst, const void* src, void* stream)
 {
 	cudaStream_t st = S(stream);
-	size_t in_b = sizeof(float2) * p->op.g.M * p->C;
-	size_t out_b = sizeof(float2) * p->op.g.npix * p->C;
+	const long npix = p->op.g.npix, M = p->op.g.M, cc = coil_chunk(p);
+	size_t in_b = sizeof(float2) * M * p->C;
+	size_t out_b = sizeof(float2) * npix * p->C;
 	Staged i, o;
 	TRY(stage_in(i, src, in_b, st));
 	TRY(stage_out_alloc(o, dst, out_b, st));
-	TRY(op_adjoint(p->op, (const float2*)i.dev, nullptr, p->C, 1, (float2*)o.dev, st));
+
+	for (long c0 = 0; c0 < p->C; c0 += cc)
+		TRY(op_adjoint(p->op, (const float2*)i.dev + M * c0, nullptr, std::min(cc, p->C - c0), 1,
+				(float2*)o.dev + npix * c0, st));
+
 	return stage_out_copy(o, dst, out_b, st);
 }
 
@@ -1791,7 +1809,11 @@ extern "C" int bnufft_apply_normal(bnufft_plan_t p, void* dst, const void* src, 
 
 	if (p->psf) {
 
-		TRY(op_toeplitz(toe_ctx(p), toe_psf(p), (const float2*)i.dev, nullptr, p->C, 1, (float2*)o.dev, st));
+		const long npix = p->op.g.npix, cc = coil_chunk(p);
+
+		for (long c0 = 0; c0 < p->C; c0 += cc)
+			TRY(op_toeplitz(toe_ctx(p), toe_psf(p), (const float2*)i.dev + npix * c0, nullptr, std::min(cc, p->C - c0),
+					1, (float2*)o.dev + npix * c0, st));
 
 	} else {
 

@@ -28,10 +28,11 @@ class NufftConf:
     os: float = 2.0
     width: float = 6.0
     bin: int = 0              # gridding bin edge (0 = default); tuning only
+    lowmem: bool = False      # --lowmem: one coil's grid at a time
 
     def c(self) -> _lib.NufftConfC:
         return _lib.NufftConfC(int(self.toeplitz), int(self.periodic), int(self.deterministic),
-                               float(self.os), float(self.width), int(self.bin))
+                               float(self.os), float(self.width), int(self.bin), int(self.lowmem))
 
 
 def _is_torch(a) -> bool:

@@ -40,6 +40,10 @@ struct bnufft_conf {
 	int bin;		/* gridding bin edge in grid cells (a power of two 8..128);
 				   0 = default (32 in 2D, 16 in 3D). A tuning knob with no
 				   effect on results (bnufft_autotune_bins picks it). */
+	int lowmem;		/* --lowmem (nufft_conf_s.lowmem): the apply calls hold
+				   the oversampled grid of one coil at a time (same
+				   results, coil passes one after another); not with
+				   per-coil weights */
 };
 
 typedef struct bnufft_plan_s* bnufft_plan_t;

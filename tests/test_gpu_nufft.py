@@ -194,3 +194,21 @@ def test_nufft_inverse_30_iterations_precond():
     x = op.inverse(g["ksp"].reshape(kd, order="F"), maxiter=30, precond=True)
     op.free()
     assert rel(x, g["inv_m30_c"]) < 1e-3
+
+
+def test_lowmem_matches_default():
+    """--lowmem (one coil's grid at a time) gives the default's results
+    (deterministic gridding: identical bits)."""
+    rng = np.random.default_rng(21)
+    N, C = 48, 3
+    t = synth.radial_traj(N, 20)
+    img = (rng.standard_normal((N, N, 1, C)) + 1j * rng.standard_normal((N, N, 1, C))).astype(np.complex64)
+    cd, kd = [N, N, 1, C], [1, t.shape[1], t.shape[2], C]
+    out = {}
+    for low in (False, True):
+        op = nufft_create2(kd, cd, list(t.shape), t, conf=NufftConf(toeplitz=True, lowmem=low, deterministic=True))
+        k = np.asarray(op.forward(img))
+        out[low] = (k, np.asarray(op.adjoint(k.reshape(kd, order="F"))), np.asarray(op.normal(img)))
+        op.free()
+    for a, b in zip(out[False], out[True]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
