@@ -267,6 +267,90 @@ def run_nufft3d(dev, steps, warmup, spokes=20000):
             "cgsense_setup_s": setup_s, "cgsense_10iter_ms": cg_ms, "cgsense_to_1e-4": to_tol}
 
 
+def toeplitz_normal_torch(x_yx, maps_cyx, P_yx):
+    """S^H F^H P F S x with torch.fft (cuFFT on a GPU): x [Y, X], maps
+    [C, Y, X], P the 2N x 2N PSF in DFT order, [y][x], scaled 1/npix. Pixel
+    n sits at (n - N/2) mod 2N of the zero-padded grid, as in the library."""
+    import torch
+    C, N = maps_cyx.shape[0], x_yx.shape[0]
+    h = N // 2
+    cim = maps_cyx * x_yx.unsqueeze(0)
+    pad = torch.zeros(C, 2 * N, 2 * N, dtype=cim.dtype, device=cim.device)
+    pad[:, :h, :h] = cim[:, h:, h:]
+    pad[:, :h, -h:] = cim[:, h:, :h]
+    pad[:, -h:, :h] = cim[:, :h, h:]
+    pad[:, -h:, -h:] = cim[:, :h, :h]
+    g = torch.fft.ifft2(torch.fft.fft2(pad) * P_yx.unsqueeze(0), norm="forward")
+    out = torch.empty_like(cim)
+    out[:, h:, h:] = g[:, :h, :h]
+    out[:, h:, :h] = g[:, :h, -h:]
+    out[:, :h, h:] = g[:, -h:, :h]
+    out[:, :h, :h] = g[:, -h:, -h:]
+    return (torch.conj(maps_cyx) * out).sum(0)
+
+
+def psf_grid_yx(psf_ref, N):
+    """The reference's decomposed PSF [X, Y, 1, 4] (sub-grid s = sx + 2 sy,
+    centred cell 2w + s per axis) as the 2N x 2N DFT-order grid [y][x] / npix."""
+    import torch
+    sub = torch.from_numpy(np.ascontiguousarray(psf_ref.reshape(N, N, 4, order="F")))
+    Pc = torch.zeros(2 * N, 2 * N, dtype=torch.complex64)   # [cx][cy]
+    for s_ in range(4):
+        Pc[s_ & 1::2, s_ >> 1::2] = sub[:, :, s_]
+    return torch.roll(Pc, shifts=(N, N), dims=(0, 1)).t().contiguous() / (N * N)
+
+
+def fft_vs_cufft(dev, traj, sens, reps=50):
+    """The Toeplitz normal operator S^H F^H P F S x of the bench problem
+    (256^2, 16 coils, 512^2 grid), once with this library's fused FFT passes
+    (Pics.normal) and once with cuFFT (torch.fft: zero-pad, 2D FFT, PSF
+    multiply, inverse 2D FFT, crop, coil sum): CUDA-event time per
+    application and the relative difference of the results."""
+    import torch
+    from bart_b200.nufft import NufftConf, nufft_create2
+    from bart_b200.pics import Pics, PicsConf
+    N, C = N_IMG, COILS
+    td = torch.from_numpy(np.asfortranarray(traj).ravel(order="F").copy()).to(dev)
+    sd = torch.from_numpy(np.asfortranarray(sens).ravel(order="F").copy()).to(dev)
+    kd = [1, traj.shape[1], traj.shape[2], C]
+    p = Pics(td, sd, ksp_dims=kd, conf=PicsConf(lam=0.0), traj_dims=list(traj.shape), sens_dims=list(sens.shape))
+    op = nufft_create2([1, traj.shape[1], traj.shape[2], 1], [N, N, 1, 1], list(traj.shape), td,
+                       conf=NufftConf(toeplitz=True))
+    P = psf_grid_yx(op.psf(), N).to(dev)
+    op.free()
+    x = torch.randn(N * N, dtype=torch.complex64, device=dev)
+    maps = sd.reshape(C, N, N)           # [c][y][x]
+    res, ys = {}, {}
+    for name, fn in (("bnufft", lambda: p.normal(x)), ("cufft", lambda: toeplitz_normal_torch(x.reshape(N, N), maps, P))):
+        for _ in range(5):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            y = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        res[name + "_us"] = e0.elapsed_time(e1) / reps * 1e3
+        ys[name] = y.reshape(N, N)
+    # cuFFT's transforms alone (forward + inverse 2D FFT of the 16 padded grids)
+    pad = torch.randn(C, 2 * N, 2 * N, dtype=torch.complex64, device=dev)
+    for _ in range(5):
+        torch.fft.ifft2(torch.fft.fft2(pad), norm="forward")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        torch.fft.ifft2(torch.fft.fft2(pad), norm="forward")
+    e1.record()
+    torch.cuda.synchronize()
+    res["cufft_fft_pair_only_us"] = e0.elapsed_time(e1) / reps * 1e3
+    res["rel_diff"] = float(torch.linalg.vector_norm(ys["bnufft"] - ys["cufft"]) / torch.linalg.vector_norm(ys["cufft"]))
+    res["speedup_vs_cufft"] = res["cufft_us"] / res["bnufft_us"]
+    p.free()
+    return res
+
+
 def run_batch(dev, steps, warmup, nprob=512, seed=4):
     """Batched uneven 2D reconstructions: nprob problems,
     N ~ U{64..320} even, spokes ~ U{16..256} x 2N samples, coils ~ U{4..32},
@@ -600,6 +684,7 @@ def main():
         traffic = json.load(open(tpath)).get(DOMINANT)
 
     nufft = nufft_throughput(dev) if (rank == 0 and not args.lean) else None
+    vs_cufft = fft_vs_cufft(dev, traj, sens) if (rank == 0 and not args.lean) else None
 
     if rank == 0:
         value = aggregate_rate(world, args.steps, ms_max / 1e3)
@@ -621,6 +706,7 @@ def main():
                 "methods": method_lines,
                 "fixed_30_iters": fixed,
                 "nufft": nufft,
+                "toeplitz_normal_vs_cufft": vs_cufft,
                 "roofline": {"bound": "hbm", "kernel": DOMINANT, "achieved": achieved, "peak": peak,
                              "peak_source": peak_src, "unit": "GB/s",
                              "frac": (achieved / peak) if achieved else None,
