@@ -102,20 +102,28 @@ __device__ __forceinline__ void butterfly(float2* v)
 		dft2<INV>(v);
 }
 
-// twiddle v[i] *= w^(i*k), w = exp(-+2 pi i / (Ns*R)), from tw[m] = exp(-2 pi i m / L)
+// twiddle v[i] *= w^(i*k), w = exp(-+2 pi i / (Ns*R)): w^k from the table
+// tw[m] = exp(-2 pi i m / L), its powers by complex multiplication (one
+// shared-memory load per stage instead of R - 1; the products add a few
+// float32 roundings, well below the transforms' own error)
 template <int L, int Ns, int R, bool INV>
 __device__ __forceinline__ void twiddle(float2* v, int k, const float2* tw)
 {
 	if constexpr (Ns > 1) {
+
+		float2 w1 = tw[k * (L / (Ns * R))];
+
+		if (INV)
+			w1.y = -w1.y;
+
+		float2 w = w1;
 #pragma unroll
 		for (int i = 1; i < R; i++) {
 
-			float2 w = tw[i * k * (L / (Ns * R))];
-
-			if (INV)
-				w.y = -w.y;
-
 			v[i] = cmul(v[i], w);
+
+			if (i + 1 < R)
+				w = cmul(w, w1);
 		}
 	}
 }
