@@ -2552,13 +2552,87 @@ struct bnufft_pics_s {
 	int nparts;
 	CgScalars* scal = nullptr;
 	// the CG iterations as one graph: a while node whose body is one iteration
-	cudaStream_t cap = nullptr;	// capture stream
 	cudaGraph_t cg_graph = nullptr;
+	cudaGraph_t cg_body = nullptr;
+	cudaGraphConditionalHandle cg_loop = 0;
 	cudaGraphExec_t cg_exec = nullptr;
+	int cg_dev = -1;
 	int body_kernels = 0;
 	long last_host_kernels = 0;	// launched from the host by the last run
 	bool last_graph = false;	// last run's CG loop ran as the graph
+	cudaEvent_t run_done = nullptr;	// recorded after each run on its stream
 };
+
+// The CG loop graph of a model (a while node whose body is one iteration)
+// and, once its model is freed, the event of its last launch.
+struct LoopGraph {
+
+	int dev;
+	cudaGraph_t graph;
+	cudaGraph_t body;
+	cudaGraphConditionalHandle loop;
+	cudaGraphExec_t exec;
+	cudaEvent_t done;
+};
+
+// Loop graphs of freed models, for reuse. Instantiating and destroying an
+// executable per model costs the host hundreds of microseconds, and
+// destroying one whose launch still runs can wait for the device. A new model
+// instead clears a pooled graph's body, captures its own iteration into it
+// (same graph, same conditional handle) and updates the executable in place
+// (cudaGraphExecUpdate); an update applies to later launches only, so the
+// freed model's last solve may still be running. When the topology differs
+// (another solver or size) the update fails and the model instantiates its
+// own graph.
+enum { LOOP_POOL_MAX = 8 };
+static std::mutex g_loop_mutex;
+static std::vector<LoopGraph> g_loop_pool;
+
+// Loop graphs that could not be reused, destroyed once their last launch has
+// completed (checked without waiting on every create and free).
+struct GraphGrave {
+
+	cudaEvent_t done;
+	cudaGraphExec_t exec;
+	cudaGraph_t graph;
+};
+
+static std::mutex g_grave_mutex;
+static std::vector<GraphGrave> g_grave;
+
+static void bury(const LoopGraph& lg)
+{
+	std::lock_guard<std::mutex> lock(g_grave_mutex);
+	g_grave.push_back(GraphGrave{ lg.done, lg.exec, lg.graph });
+}
+
+static void reap_graves()
+{
+	std::lock_guard<std::mutex> lock(g_grave_mutex);
+	size_t k = 0;
+
+	for (size_t i = 0; i < g_grave.size(); i++) {
+
+		GraphGrave& g = g_grave[i];
+		cudaError_t e = cudaEventQuery(g.done);
+
+		if (cudaErrorNotReady == e) {
+
+			cudaGetLastError();	// not an error: clear it
+			g_grave[k++] = g;
+			continue;
+		}
+
+		cudaGraphExecDestroy(g.exec);
+
+		if (g.graph)
+			cudaGraphDestroy(g.graph);
+
+		cudaEventDestroy(g.done);
+	}
+
+	g_grave.resize(k);
+}
 
 extern "C" void bnufft_pics_conf_defaults(struct bnufft_pics_conf* c)
 {
@@ -2602,6 +2676,7 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 	*out = nullptr;
 	cudaStream_t st = S(stream);
 	bnufft_pics_conf conf;
+	reap_graves();
 
 	if (conf_in)
 		conf = *conf_in;
@@ -2939,35 +3014,34 @@ static int pics_any_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	return ps->conf.precond ? pics_fcg_iteration(ps, it, st) : pics_iteration(ps, it, st);
 }
 
-// Capture the CG loop once: a graph holding one while node whose body is an
-// iteration followed by k_cg_advance, which continues the loop until the
-// solve converged or reached maxiter. One graph launch then runs the whole
-// loop with no host round trip and no launches past convergence.
-static int capture_cg_loop(bnufft_pics_s* ps)
+// per thread and device: the stream the loop graphs are captured on
+static cudaStream_t capture_stream(int dev)
 {
-	if (!ps->cap)
-		CUDA_TRY(cudaStreamCreateWithFlags(&ps->cap, cudaStreamNonBlocking));
+	static thread_local std::map<int, cudaStream_t> streams;
+	auto it = streams.find(dev);
 
-	CUDA_TRY(cudaGraphCreate(&ps->cg_graph, 0));
-	cudaGraphConditionalHandle loop;
-	CUDA_TRY(cudaGraphConditionalHandleCreate(&loop, ps->cg_graph, 1, cudaGraphCondAssignDefault));
+	if (it != streams.end())
+		return it->second;
 
-	cudaGraphNodeParams np = {};
-	np.type = cudaGraphNodeTypeConditional;
-	np.conditional.handle = loop;
-	np.conditional.type = cudaGraphCondTypeWhile;
-	np.conditional.size = 1;
-	cudaGraphNode_t node;
-	CUDA_TRY(cudaGraphAddNode(&node, ps->cg_graph, nullptr, 0, &np));
-	cudaGraph_t body = np.conditional.phGraph_out[0];
+	cudaStream_t s = nullptr;
 
-	CUDA_TRY(cudaStreamBeginCaptureToGraph(ps->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+	if (cudaSuccess != cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking))
+		return nullptr;
+
+	streams[dev] = s;
+	return s;
+}
+
+// one iteration and k_cg_advance, captured into the (empty) loop body
+static int capture_body(bnufft_pics_s* ps, cudaStream_t cap, cudaGraph_t body, cudaGraphConditionalHandle loop)
+{
+	CUDA_TRY(cudaStreamBeginCaptureToGraph(cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
 	long before = g_launches.load();
-	int s = pics_any_iteration(ps, -1, ps->cap);
+	int s = pics_any_iteration(ps, -1, cap);
 
 	if (BNUFFT_OK == s) {
 
-		k_cg_advance<<<1, 1, 0, ps->cap>>>(ps->scal, loop);
+		k_cg_advance<<<1, 1, 0, cap>>>(ps->scal, loop);
 		cudaError_t e = cudaGetLastError();
 
 		if (cudaSuccess != e)
@@ -2981,12 +3055,102 @@ static int capture_cg_loop(bnufft_pics_s* ps)
 	g_launches.fetch_sub(ps->body_kernels);
 
 	cudaGraph_t captured = nullptr;
-	cudaError_t e = cudaStreamEndCapture(ps->cap, &captured);
+	cudaError_t e = cudaStreamEndCapture(cap, &captured);
 
 	if (BNUFFT_OK != s)
 		return s;
 
 	CUDA_TRY(e);
+	return BNUFFT_OK;
+}
+
+// a pooled loop graph of this device updated to this model's iteration
+static bool reuse_loop_graph(bnufft_pics_s* ps, cudaStream_t cap, int dev)
+{
+	LoopGraph lg;
+	bool found = false;
+
+	{
+		std::lock_guard<std::mutex> lock(g_loop_mutex);
+
+		for (size_t i = 0; i < g_loop_pool.size(); i++) {
+
+			if (g_loop_pool[i].dev == dev) {
+
+				lg = g_loop_pool[i];
+				g_loop_pool.erase(g_loop_pool.begin() + i);
+				found = true;
+				break;
+			}
+		}
+	}
+
+	if (!found)
+		return false;
+
+	size_t n = 0;
+	cudaError_t e = cudaGraphGetNodes(lg.body, nullptr, &n);
+	std::vector<cudaGraphNode_t> nodes(n);
+
+	if ((cudaSuccess == e) && (n > 0))
+		e = cudaGraphGetNodes(lg.body, nodes.data(), &n);
+
+	for (size_t i = 0; (cudaSuccess == e) && (i < n); i++)
+		e = cudaGraphDestroyNode(nodes[i]);
+
+	if ((cudaSuccess == e) && (BNUFFT_OK == capture_body(ps, cap, lg.body, lg.loop))) {
+
+		cudaGraphExecUpdateResultInfo info;
+		e = cudaGraphExecUpdate(lg.exec, lg.graph, &info);
+
+		if (cudaSuccess == e) {
+
+			ps->cg_graph = lg.graph;
+			ps->cg_body = lg.body;
+			ps->cg_loop = lg.loop;
+			ps->cg_exec = lg.exec;
+			ps->cg_dev = dev;
+			cudaEventDestroy(lg.done);
+			return true;
+		}
+	}
+
+	// not reusable (the executable is unchanged): destroyed once idle
+	cudaGetLastError();
+	g_err.clear();
+	bury(lg);
+	return false;
+}
+
+// Capture the CG loop once: a graph holding one while node whose body is an
+// iteration followed by k_cg_advance, which continues the loop until the
+// solve converged or reached maxiter. One graph launch then runs the whole
+// loop with no host round trip and no launches past convergence.
+static int capture_cg_loop(bnufft_pics_s* ps)
+{
+	int dev;
+	CUDA_TRY(cudaGetDevice(&dev));
+	cudaStream_t cap = capture_stream(dev);
+
+	if (!cap)
+		return fail(BNUFFT_ERR_CUDA, "capture stream");
+
+	if (reuse_loop_graph(ps, cap, dev))
+		return BNUFFT_OK;
+
+	CUDA_TRY(cudaGraphCreate(&ps->cg_graph, 0));
+	CUDA_TRY(cudaGraphConditionalHandleCreate(&ps->cg_loop, ps->cg_graph, 1, cudaGraphCondAssignDefault));
+
+	cudaGraphNodeParams np = {};
+	np.type = cudaGraphNodeTypeConditional;
+	np.conditional.handle = ps->cg_loop;
+	np.conditional.type = cudaGraphCondTypeWhile;
+	np.conditional.size = 1;
+	cudaGraphNode_t node;
+	CUDA_TRY(cudaGraphAddNode(&node, ps->cg_graph, nullptr, 0, &np));
+	ps->cg_body = np.conditional.phGraph_out[0];
+	ps->cg_dev = dev;
+	TRY(capture_body(ps, cap, ps->cg_body, ps->cg_loop));
 	CUDA_TRY(cudaGraphInstantiate(&ps->cg_exec, ps->cg_graph, 0));
 	return BNUFFT_OK;
 }
@@ -3078,6 +3242,11 @@ extern "C" int bnufft_pics_run(bnufft_pics_t ps, void* img, const void* ksp, voi
 	long launches0 = g_launches.load();
 	TRY(pics_solve(ps, (const float2*)ki.dev, (float2*)io.dev, st, cg_graph_enabled()));
 	ps->last_host_kernels = g_launches.load() - launches0;
+
+	if (!ps->run_done)
+		CUDA_TRY(cudaEventCreateWithFlags(&ps->run_done, cudaEventDisableTiming));
+
+	CUDA_TRY(cudaEventRecord(ps->run_done, st));
 	return stage_out_copy(io, img, ib, st);
 }
 
@@ -3321,15 +3490,42 @@ extern "C" void bnufft_pics_free(bnufft_pics_t ps)
 		return;
 
 	cudaStream_t st = ps->nufft ? ps->nufft->st0 : nullptr;
+	reap_graves();
 
-	if (ps->cg_exec)
-		cudaGraphExecDestroy(ps->cg_exec);
+	// the stream-ordered frees below follow the last run, on whatever stream it was
+	if (ps->run_done)
+		cudaStreamWaitEvent(st, ps->run_done, 0);
 
-	if (ps->cg_graph)
-		cudaGraphDestroy(ps->cg_graph);
+	if (ps->cg_exec && ps->run_done) {
 
-	if (ps->cap)
-		cudaStreamDestroy(ps->cap);
+		LoopGraph lg = { ps->cg_dev, ps->cg_graph, ps->cg_body, ps->cg_loop, ps->cg_exec, ps->run_done };
+		bool kept = false;
+		ps->run_done = nullptr;
+
+		{
+			std::lock_guard<std::mutex> lock(g_loop_mutex);
+
+			if (g_loop_pool.size() < LOOP_POOL_MAX) {
+
+				g_loop_pool.push_back(lg);
+				kept = true;
+			}
+		}
+
+		if (!kept)
+			bury(lg);
+
+	} else {
+
+		if (ps->cg_exec)
+			cudaGraphExecDestroy(ps->cg_exec);
+
+		if (ps->cg_graph)
+			cudaGraphDestroy(ps->cg_graph);
+	}
+
+	if (ps->run_done)
+		cudaEventDestroy(ps->run_done);
 
 	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->pbuf[0], ps->pbuf[1], ps->b, ps->kbuf, ps->mag, ps->mag_sorted,
 			 ps->sort_tmp, ps->pap_part, ps->pp_part, ps->rs_part, ps->scal, ps->z, ps->p_ring, ps->ap_ring,

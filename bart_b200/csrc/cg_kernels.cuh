@@ -146,14 +146,14 @@ __global__ void k_cg_step(float2* __restrict__ x, float2* __restrict__ r, const 
 		const double* __restrict__ pap_part, int npap, const double* __restrict__ pp_part, int npp,
 		double* __restrict__ rs_part, float2* __restrict__ p_keep)
 {
-	__shared__ double sh[32];
+	__shared__ double sh[96];
 
 	if (st->done)
 		return;
 
 	it = cg_iter(it, st);
-
-	double pAp = sum_partials(pap_part, npap, sh) + (double)lam * sum_partials(pp_part, npp, sh);
+	const double3 sums = sum_partials3_d(pap_part, npap, pp_part, npp, nullptr, 0, sh);
+	double pAp = sums.x + (double)lam * sums.y;
 
 	if (0. == pAp) {
 
@@ -313,19 +313,23 @@ __global__ void k_fcgm_dir(float2* __restrict__ p_cur, float2* __restrict__ p_ri
 		const float2* __restrict__ r, long n, CgScalars* st, int it, int m, int ring, const double* __restrict__ dots,
 		int ndots, double* __restrict__ pr_part, double* __restrict__ pp_part, const double* __restrict__ rs_part, int nrs)
 {
-	__shared__ double sh[32];
+	__shared__ double sh[96];
 	__shared__ float beta[FCG_MAX_M];
 
 	if (st->done)
 		return;
 
 	it = cg_iter(it, st);
+	const int w = min(it - st->restart_it, m);
+	const bool check = rs_part && (it > 0);
+	// ||r||^2 and the first <z, A p_j> in one reduction
+	const double3 s3 = sum_partials3_d(rs_part, check ? nrs : 0, dots, (w > 0) ? ndots : 0, nullptr, 0, sh);
 
 	// with rs_part: the convergence test of the previous step is done here
 	// (every block reaches the same decision from the same partial sums)
-	if (rs_part && (it > 0)) {
+	if (check) {
 
-		double rs = sum_partials(rs_part, nrs, sh);
+		double rs = s3.x;
 
 		if ((0 == blockIdx.x) && (0 == threadIdx.x)) {
 
@@ -342,11 +346,9 @@ __global__ void k_fcgm_dir(float2* __restrict__ p_cur, float2* __restrict__ p_ri
 			return;
 	}
 
-	const int w = min(it - st->restart_it, m);
-
 	for (int q = 0; q < w; q++) {
 
-		double d = sum_partials(dots + q * ndots, ndots, sh);
+		double d = (0 == q) ? s3.y : sum_partials(dots + q * ndots, ndots, sh);
 
 		if (0 == threadIdx.x)
 			beta[q] = (float)(d / st->pap_hist[(it - w + q) % ring]);
@@ -394,13 +396,14 @@ __global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const
 		const double* __restrict__ pap_part, int npap, const double* __restrict__ pp_part, int npp,
 		const double* __restrict__ pr_part, int npr, double* __restrict__ rs_part)
 {
-	__shared__ double sh[32];
+	__shared__ double sh[96];
 
 	if (st->done)
 		return;
 
 	it = cg_iter(it, st);
-	double pAp = sum_partials(pap_part, npap, sh) + (double)lam * sum_partials(pp_part, npp, sh);
+	const double3 sums = sum_partials3_d(pap_part, npap, pp_part, npp, pr_part, npr, sh);
+	double pAp = sums.x + (double)lam * sums.y;
 
 	if (!(pAp > 0.)) {	// zero or not positive: breakdown
 
@@ -413,7 +416,7 @@ __global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const
 		return;
 	}
 
-	float a = (float)(sum_partials(pr_part, npr, sh) / pAp);
+	float a = (float)(sums.z / pAp);
 	float2* Ap = ap_ring + (long)(it % ring) * n;
 	double acc = 0.;
 
@@ -422,6 +425,7 @@ __global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const
 		float2 pv = p[i];
 		float2 av = part[i];
 
+#pragma unroll 4
 		for (int g = 1; g < groups; g++)
 			av = cadd(av, part[i + n * g]);
 

@@ -169,6 +169,56 @@ struct CgScalars {
 // loop runs inside a graph (it < 0)
 __device__ __forceinline__ int cg_iter(int it, const CgScalars* st) { return (it < 0) ? st->it : it; }
 
+// three fixed-order float64 sums of partials in one block reduction, the
+// same values in every thread (sh: 3 doubles per warp)
+__device__ __forceinline__ double3 sum_partials3_d(const double* a, int na, const double* b, int nb,
+		const double* c, int nc, double* sh)
+{
+	double3 v = make_double3(0., 0., 0.);
+	const int n = max(na, max(nb, nc));
+
+	for (int i = threadIdx.x; i < n; i += blockDim.x) {
+
+		if (i < na)
+			v.x += a[i];
+
+		if (i < nb)
+			v.y += b[i];
+
+		if (i < nc)
+			v.z += c[i];
+	}
+
+	for (int o = 16; o > 0; o >>= 1) {
+
+		v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+		v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+		v.z += __shfl_down_sync(0xffffffffu, v.z, o);
+	}
+
+	__syncthreads();
+
+	if (0 == threadIdx.x % 32) {
+
+		sh[3 * (threadIdx.x / 32) + 0] = v.x;
+		sh[3 * (threadIdx.x / 32) + 1] = v.y;
+		sh[3 * (threadIdx.x / 32) + 2] = v.z;
+	}
+
+	__syncthreads();
+	double3 r = make_double3(0., 0., 0.);
+
+	for (int w = 0; w < (int)(blockDim.x / 32); w++) {
+
+		r.x += sh[3 * w + 0];
+		r.y += sh[3 * w + 1];
+		r.z += sh[3 * w + 2];
+	}
+
+	__syncthreads();
+	return r;
+}
+
 // Row pass, forward, first step of a CG iteration (conjgrad,
 // src/iter/italgos.c:538-566, reordered so that the direction update of the
 // previous iteration happens while loading):

@@ -121,6 +121,35 @@ def test_cg_loop_graph_matches_host_loop(tol):
         assert sg[0] == 12 and kg == kh + sg[0]    # plus one loop-advance kernel per iteration
 
 
+def test_cg_loop_graph_reused_across_models():
+    """A freed model hands its loop graph to the next one, which captures its
+    own iteration into it and updates the executable in place (or, when that
+    fails, instantiates its own): a chain of models of two sizes and two
+    solvers, each built after the last was freed, solves bit-identically to
+    the host-driven loop."""
+    gs = {"a": golden("pics2d_n64_c4"), "b": golden("pics2d_n48_c3")}
+
+    def solve(name, pc, graph):
+        g = gs[name]
+        os.environ["BNUFFT_CG_GRAPH"] = graph
+        try:
+            p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
+                     conf=PicsConf(lam=0.01, maxiter=60, tol=1e-6, scaling=1.0, precond=pc, deterministic=True))
+            x = np.asarray(p.run(g["ksp"]))
+            st = p.stats()
+            p.free()
+        finally:
+            os.environ.pop("BNUFFT_CG_GRAPH", None)
+        return x, st
+
+    chain = [("a", 0), ("a", 0), ("b", 0), ("a", 1), ("a", 1), ("b", 1), ("b", 1), ("a", 0)]
+    ref = {k: solve(*k, "0") for k in set(chain)}
+    for k in chain:
+        x, st = solve(*k, "1")
+        assert np.array_equal(x.view(np.uint32), ref[k][0].view(np.uint32)), k
+        assert st == ref[k][1], k
+
+
 def test_fcg_circulant_converges_faster():
     """Flexible CG with the circulant PSF preconditioner reaches the same
     tolerance in fewer iterations than plain CG, to the same solution (the
