@@ -24,6 +24,7 @@
 #include "gridding.cuh"
 #include "precnet.cuh"
 #include "nudft.cuh"
+#include "precond_cluster.cuh"
 
 using namespace bn;
 
@@ -2920,6 +2921,104 @@ static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const flo
 			dot_part, nblocks, &sc->done, &sc->net_off, st);
 }
 
+// the one-launch cluster form of the circulant preconditioner (square 2D
+// images of 64, 128 or 256 pixels a side; BNUFFT_PRECOND_CLUSTER=0: the
+// three-pass form): one cluster of CL CTAs
+template <int N, int CL>
+static int launch_precond_cluster(const float2* r, const float2* pinv, float2* z, const float2* pdot,
+		double* dot_part, const int* done, cudaStream_t st)
+{
+	using Sh = PrecondClusterShape<N, CL>;
+	const float2* tw;
+	TRY(get_twiddles(N, &tw));
+	cudaLaunchConfig_t cfg = {};
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeClusterDimension;
+	at[0].val.clusterDim.x = CL;
+	at[0].val.clusterDim.y = 1;
+	at[0].val.clusterDim.z = 1;
+	cfg.gridDim = dim3(CL);
+	cfg.blockDim = dim3(Sh::NT);
+	cfg.dynamicSmemBytes = Sh::SMEM;
+	cfg.stream = st;
+	cfg.attrs = at;
+	cfg.numAttrs = 1;
+	cudaEvent_t pe = prof_begin("cluster", st);
+	cudaError_t e = cudaLaunchKernelEx(&cfg, k_precond_cluster<N, CL>, r, pinv, z, tw, pdot, dot_part, done);
+	prof_end(pe, st);
+	g_launches.fetch_add(1, std::memory_order_relaxed);
+
+	if (cudaSuccess != e)
+		return fail(BNUFFT_ERR_CUDA, "preconditioner cluster launch: %s", cudaGetErrorString(e));
+
+	return BNUFFT_OK;
+}
+
+// whether one cluster of CL CTAs with their shared memory fits this device
+// (16 is a non-portable cluster size), once per size and device
+template <int N, int CL>
+static bool precond_cluster_fits()
+{
+	static std::mutex m;
+	static std::map<int, bool> fits;
+	int dev = 0;
+
+	if (cudaSuccess != cudaGetDevice(&dev))
+		return false;
+
+	std::lock_guard<std::mutex> lock(m);
+	auto it = fits.find(dev);
+
+	if (it != fits.end())
+		return it->second;
+
+	using Sh = PrecondClusterShape<N, CL>;
+	auto kern = k_precond_cluster<N, CL>;
+	bool ok = (cudaSuccess == cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::SMEM));
+
+	if (ok && (CL > 8))
+		ok = (cudaSuccess == cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+
+	if (ok) {
+
+		cudaLaunchConfig_t cfg = {};
+		cudaLaunchAttribute at[1];
+		at[0].id = cudaLaunchAttributeClusterDimension;
+		at[0].val.clusterDim.x = CL;
+		at[0].val.clusterDim.y = 1;
+		at[0].val.clusterDim.z = 1;
+		cfg.gridDim = dim3(CL);
+		cfg.blockDim = dim3(Sh::NT);
+		cfg.dynamicSmemBytes = Sh::SMEM;
+		cfg.attrs = at;
+		cfg.numAttrs = 1;
+		int nc = 0;
+		ok = (cudaSuccess == cudaOccupancyMaxActiveClusters(&nc, kern, &cfg)) && (nc > 0);
+	}
+
+	cudaGetLastError();
+	fits[dev] = ok;
+	return ok;
+}
+
+// the cluster size for this image (0: use the three-pass form)
+static int precond_cluster_size(const Geom& g)
+{
+	if (const char* e = getenv("BNUFFT_PRECOND_CLUSTER"))
+		if (0 == strcmp(e, "0"))
+			return 0;
+
+	if ((1 != g.N[2]) || (g.N[0] != g.N[1]))
+		return 0;
+
+	switch (g.N[0]) {
+	case 64: return precond_cluster_fits<64, 16>() ? 16 : (precond_cluster_fits<64, 8>() ? 8 : 0);
+	case 128: return precond_cluster_fits<128, 16>() ? 16 : (precond_cluster_fits<128, 8>() ? 8 : 0);
+	case 256: return precond_cluster_fits<256, 16>() ? 16 : (precond_cluster_fits<256, 8>() ? 8 : 0);
+	default: return 0;
+	}
+}
+
 // the circulant preconditioner applied to one image (N-point transforms, no
 // padding)
 static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
@@ -2927,6 +3026,29 @@ static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, cons
 {
 	bnufft_plan_s* p = ps->nufft;
 	const int* done = &ps->scal->done;
+
+	if (const int cl = precond_cluster_size(p->op.g)) {
+
+		int s = BNUFFT_OK;
+		const int n = p->op.g.N[0];
+		t_prof_precond = true;
+
+		if (16 == cl)
+			s = (64 == n) ? launch_precond_cluster<64, 16>(r, p->pinv, z, pdot, dot_part, done, st)
+				: (128 == n) ? launch_precond_cluster<128, 16>(r, p->pinv, z, pdot, dot_part, done, st)
+				: launch_precond_cluster<256, 16>(r, p->pinv, z, pdot, dot_part, done, st);
+		else
+			s = (64 == n) ? launch_precond_cluster<64, 8>(r, p->pinv, z, pdot, dot_part, done, st)
+				: (128 == n) ? launch_precond_cluster<128, 8>(r, p->pinv, z, pdot, dot_part, done, st)
+				: launch_precond_cluster<256, 8>(r, p->pinv, z, pdot, dot_part, done, st);
+
+		t_prof_precond = false;
+
+		if (nblocks)
+			*nblocks = cl;
+
+		return s;
+	}
 	OpCtx full;
 	full.g = p->op.g;
 

@@ -205,6 +205,34 @@ def test_fcg_circulant_uneven_and_3d(name):
     assert its[1] < its[0], its
 
 
+@pytest.mark.parametrize("N", [64, 128, 256])
+def test_precond_cluster_matches_three_passes(N):
+    """The circulant preconditioner in one launch on a thread-block cluster
+    (square 2D images of 64, 128, 256 pixels) runs the three-pass form's
+    arithmetic: z bit-identical, and a solve stops at the same iteration."""
+    from bart_b200.problems import cgsense_problem
+    prob = cgsense_problem(np.random.default_rng(N), N=N, coils=4, spokes=max(16, N // 4))
+    r = (np.random.default_rng(1).standard_normal((N, N)) + 1j * np.random.default_rng(2).standard_normal((N, N)))
+    r = np.asfortranarray(r.astype(np.complex64))
+    out = {}
+    for mode in ("1", "0"):
+        os.environ["BNUFFT_PRECOND_CLUSTER"] = mode
+        try:
+            p = Pics(prob["traj"], prob["sens"], ksp_dims=list(prob["ksp"].shape),
+                     conf=PicsConf(lam=0.01, maxiter=100, tol=1e-5, scaling=1.0, precond=1, deterministic=True))
+            z = np.asarray(p.precond(r))
+            p.run(prob["ksp"])
+            out[mode] = (z, p.stats())
+            p.free()
+        finally:
+            os.environ.pop("BNUFFT_PRECOND_CLUSTER", None)
+    assert np.array_equal(out["1"][0].view(np.uint32), out["0"][0].view(np.uint32))
+    assert np.abs(out["1"][0]).max() > 0
+    # the <A p, z> partials are summed in another grouping: the stopping
+    # iteration may move by one near the tolerance
+    assert abs(out["1"][1][0] - out["0"][1][0]) <= 1 and out["1"][1][1] <= 1e-5
+
+
 def test_fcg_folded_launches_match_unfolded():
     """The folded circulant flexible CG (dot products from the
     preconditioner's last pass, convergence test in the next direction
