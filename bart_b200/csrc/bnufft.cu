@@ -1605,32 +1605,96 @@ static int check_conf(const bnufft_conf* conf)
 	return BNUFFT_OK;
 }
 
+// per thread and device: an auxiliary stream and a fork / join event pair
+struct AuxStream {
+
+	cudaStream_t st = nullptr;
+	cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+static const AuxStream* aux_stream(int dev)
+{
+	static thread_local std::map<int, AuxStream> aux;
+	auto it = aux.find(dev);
+
+	if (it != aux.end())
+		return &it->second;
+
+	AuxStream a;
+
+	if ((cudaSuccess != cudaStreamCreateWithFlags(&a.st, cudaStreamNonBlocking))
+	    || (cudaSuccess != cudaEventCreateWithFlags(&a.fork, cudaEventDisableTiming))
+	    || (cudaSuccess != cudaEventCreateWithFlags(&a.join, cudaEventDisableTiming))) {
+
+		cudaGetLastError();
+		return nullptr;
+	}
+
+	return &(aux[dev] = a);
+}
+
+// Trajectory upload: converted trajectory and sample bins on st; with the
+// Toeplitz normal the PSF chain (its own binning on the 4N grid, gridding,
+// transforms, embedding) runs meanwhile on an auxiliary stream (the two are
+// independent chains of small kernels), joined back into st before return.
 static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
 {
 	Staged t;
 	TRY(stage_in(t, traj, sizeof(float2) * 3 * p->op.g.M, st));
-	k_traj_convert<<<vec_blocks(p->op.g.M), RED_THREADS, 0, st>>>(p->traj, (const float2*)t.dev, p->op.g.M, 1.f);
-	LAUNCHED();
-
-	free_bins(p->op.bins, st);
-	TRY(build_bins(p->op, st));
-
-	if (p->conf.deterministic) {
-
-		free_csr(p->op.csr, st);
-		TRY(build_csr(p->op, st));
-	}
+	int dev = 0;
+	CUDA_TRY(cudaGetDevice(&dev));
+	const AuxStream* aux = p->conf.toeplitz ? aux_stream(dev) : nullptr;
+	cudaStream_t pst = aux ? aux->st : st;
+	int s_psf = BNUFFT_OK;
 
 	if (p->conf.toeplitz) {
 
 		if (p->psf)
 			cudaFreeAsync(p->psf, st);
 
+		if (p->pinv)	// the preconditioner follows the PSF
+			cudaFreeAsync(p->pinv, st);
+
 		p->psf = nullptr;
-		TRY(compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, st, 0 != p->conf.deterministic, p->op.wgt,
-				p->op.bin_edge));
-		TRY(build_toeplitz_embedding(p, st));
+		p->pinv = nullptr;
+
+		if (aux) {
+
+			CUDA_TRY(cudaEventRecord(aux->fork, st));
+			CUDA_TRY(cudaStreamWaitEvent(pst, aux->fork, 0));
+		}
+
+		s_psf = compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, pst, 0 != p->conf.deterministic,
+				p->op.wgt, p->op.bin_edge);
+
+		if (BNUFFT_OK == s_psf)
+			s_psf = build_toeplitz_embedding(p, pst);
 	}
+
+	k_traj_convert<<<vec_blocks(p->op.g.M), RED_THREADS, 0, st>>>(p->traj, (const float2*)t.dev, p->op.g.M, 1.f);
+	cudaError_t e = cudaGetLastError();
+	g_launches.fetch_add(1, std::memory_order_relaxed);
+	int s = (cudaSuccess == e) ? BNUFFT_OK : fail(BNUFFT_ERR_CUDA, "trajectory: %s", cudaGetErrorString(e));
+	free_bins(p->op.bins, st);
+
+	if (BNUFFT_OK == s)
+		s = build_bins(p->op, st);
+
+	if ((BNUFFT_OK == s) && p->conf.deterministic) {
+
+		free_csr(p->op.csr, st);
+		s = build_csr(p->op, st);
+	}
+
+	// joined whatever happened, so that nothing outlives its inputs
+	if (aux) {
+
+		cudaEventRecord(aux->join, pst);
+		cudaStreamWaitEvent(st, aux->join, 0);
+	}
+
+	TRY(s_psf);
+	TRY(s);
 
 	if (t.owned)
 		CUDA_TRY(cudaStreamSynchronize(st));
