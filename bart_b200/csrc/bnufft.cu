@@ -2596,9 +2596,7 @@ struct bnufft_pics_s {
 	float2* pbuf[2] = { nullptr, nullptr };	// search direction, alternating by iteration
 	float2* kbuf = nullptr;		// [M, C] (non-Toeplitz normal)
 	float* mag = nullptr;		// [npix] |adj|
-	float* mag_sorted = nullptr;
-	void* sort_tmp = nullptr;
-	size_t sort_tmp_bytes = 0;
+	SelectState* sel = nullptr;	// radix select of the scaling's order statistics
 	double* pap_part = nullptr;	// p^H partial, one per final row-pass block
 	double* pp_part = nullptr;	// ||p||^2, one per first row-pass block
 	double* rs_part = nullptr;	// ||r||^2, one per CG step block
@@ -2805,7 +2803,10 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 	ck(cudaMallocAsync(&ps->pbuf[1], sizeof(float2) * ps->npix, st));
 	ck(cudaMallocAsync(&ps->b, sizeof(float2) * ps->npix, st));
 	ck(cudaMallocAsync(&ps->mag, sizeof(float) * ps->npix, st));
-	ck(cudaMallocAsync(&ps->mag_sorted, sizeof(float) * ps->npix, st));
+	ck(cudaMallocAsync(&ps->sel, sizeof(SelectState), st));
+
+	if (ps->sel)
+		ck(cudaMemsetAsync(ps->sel, 0, sizeof(SelectState), st));
 	// row-pass blocks hold at least 4 rows: bounds for the partial arrays
 	ps->max_row_blocks = (YZ + 3) / 4 * ps->C + 1;
 	ck(cudaMallocAsync(&ps->pap_part, sizeof(double) * ps->max_row_blocks, st));
@@ -2838,12 +2839,6 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 
 		if (BNUFFT_OK == s)
 			s = build_precond(ps->nufft, st);
-	}
-
-	if (BNUFFT_OK == s) {
-
-		cub::DeviceRadixSort::SortKeys(nullptr, ps->sort_tmp_bytes, ps->mag, ps->mag_sorted, (int)ps->npix, 0, 32, st);
-		ck(cudaMallocAsync(&ps->sort_tmp, ps->sort_tmp_bytes, st));
 	}
 
 	if (BNUFFT_OK == s) {
@@ -2889,11 +2884,13 @@ static int pics_prologue(bnufft_pics_s* ps, const float2* ksp, cudaStream_t st)
 
 	if (0.f == ps->conf.scaling) {
 
-		k_abs<<<nb, RED_THREADS, 0, st>>>(ps->mag, ps->b, ps->npix);
+		// three order statistics of |b| by radix select (estimate_scaling_norm)
+		const unsigned sb = (unsigned)std::max(1L, std::min<long>((ps->npix + 4 * SEL_THREADS - 1) / (4 * SEL_THREADS), 2 * 148));
+		k_select_pass<0><<<sb, SEL_THREADS, 0, st>>>(ps->b, ps->mag, ps->npix, ps->sel, ps->scal);
 		LAUNCHED();
-		CUDA_TRY(cub::DeviceRadixSort::SortKeys(ps->sort_tmp, ps->sort_tmp_bytes, ps->mag, ps->mag_sorted, (int)ps->npix, 0, 32, st));
-		g_launches.fetch_add(1, std::memory_order_relaxed);
-		k_scaling_from_sorted<<<1, 1, 0, st>>>(ps->mag_sorted, ps->npix, ps->scal);
+		k_select_pass<1><<<sb, SEL_THREADS, 0, st>>>(ps->b, ps->mag, ps->npix, ps->sel, ps->scal);
+		LAUNCHED();
+		k_select_pass<2><<<sb, SEL_THREADS, 0, st>>>(ps->b, ps->mag, ps->npix, ps->sel, ps->scal);
 		LAUNCHED();
 
 	} else {
@@ -3713,8 +3710,8 @@ extern "C" void bnufft_pics_free(bnufft_pics_t ps)
 	if (ps->run_done)
 		cudaEventDestroy(ps->run_done);
 
-	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->pbuf[0], ps->pbuf[1], ps->b, ps->kbuf, ps->mag, ps->mag_sorted,
-			 ps->sort_tmp, ps->pap_part, ps->pp_part, ps->rs_part, ps->scal, ps->z, ps->p_ring, ps->ap_ring,
+	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->pbuf[0], ps->pbuf[1], ps->b, ps->kbuf, ps->mag, ps->sel,
+			 ps->pap_part, ps->pp_part, ps->rs_part, ps->scal, ps->z, ps->p_ring, ps->ap_ring,
 			 ps->dots_part, ps->pr_part, ps->nact[0], ps->nact[1], ps->mcn_part };
 
 	for (void* b : bufs)

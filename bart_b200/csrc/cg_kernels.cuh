@@ -566,29 +566,176 @@ __global__ void k_scale(float2* __restrict__ dst, const float2* __restrict__ src
 		dst[i] = cscale(src[i], f);
 }
 
-__global__ void k_abs(float* __restrict__ dst, const float2* __restrict__ src, long n)
+// estimate_scaling_norm (src/sense/optcom.c:74-109): of the magnitudes |b|
+// sorted ascending, p90 unless (max - p90) >= 2 (p90 - median), then max;
+// 0 -> 1. The three order statistics (ranks n/2, trunc(0.9 n), n - 1) come
+// without sorting from a radix select over the magnitudes' bit
+// patterns (non-negative floats order like their unsigned bits) in three
+// passes of 11, 11 and 10 bits. Each pass histograms the digit of the
+// elements whose higher bits match a rank's prefix so far (one shared
+// histogram in the first pass), the counts are added into the state with
+// integer atomics (exact, order-free), and the last block to finish picks
+// each rank's digit and resets the histograms. The third pass ends with the
+// three values, exactly the sorted array's entries.
+enum { SEL_BINS = 2048, SEL_THREADS = 256 };
+
+struct SelectState {
+
+	unsigned prefix[3];	// key bits chosen so far per rank
+	long long rank[3];	// rank left within the chosen prefix
+	unsigned blocks_done;
+	unsigned hist[3][SEL_BINS];
+};
+
+template <int P>
+struct SelDigit {
+
+	static constexpr int SHIFT = (0 == P) ? 21 : ((1 == P) ? 10 : 0);
+	static constexpr int W = (2 == P) ? 10 : 11;
+};
+
+template <int P>
+__global__ void __launch_bounds__(SEL_THREADS) k_select_pass(const float2* __restrict__ b, float* __restrict__ mag,
+		long n, SelectState* ss, CgScalars* st)
 {
+	constexpr int SHIFT = SelDigit<P>::SHIFT;
+	constexpr int W = SelDigit<P>::W;
+	constexpr int NB = 1 << W;
+	constexpr int NH = (0 == P) ? 1 : 3;
+	__shared__ unsigned h[NH * NB];
+	__shared__ unsigned pre[3];
+	__shared__ int last;
+
+	for (int i = threadIdx.x; i < NH * NB; i += blockDim.x)
+		h[i] = 0u;
+
+	if (threadIdx.x < 3)
+		pre[threadIdx.x] = ss->prefix[threadIdx.x];
+
+	__syncthreads();
+
 	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
 
-		float2 v = src[i];
-		dst[i] = hypotf(v.x, v.y);	// cabsf
+		float m;
+
+		if (0 == P) {
+
+			float2 v = b[i];
+			m = hypotf(v.x, v.y);	// cabsf
+			mag[i] = m;
+
+		} else {
+
+			m = mag[i];
+		}
+
+		const unsigned key = __float_as_uint(m);
+		const unsigned d = (key >> SHIFT) & (NB - 1);
+
+		if (0 == P) {
+
+			atomicAdd(&h[d], 1u);
+
+		} else {
+#pragma unroll
+			for (int j = 0; j < 3; j++)
+				if ((key >> (SHIFT + W)) == (pre[j] >> (SHIFT + W)))
+					atomicAdd(&h[j * NB + d], 1u);
+		}
 	}
-}
 
-// estimate_scaling_norm (src/sense/optcom.c:74-109) on magnitudes sorted
-// ascending: p90 unless (max - p90) >= 2 (p90 - median), then max; 0 -> 1.
-__global__ void k_scaling_from_sorted(const float* sorted, long n, CgScalars* st)
-{
-	float median = sorted[n / 2];
-	float p90 = sorted[(long)trunc(n * 0.9)];
-	float mx = sorted[n - 1];
-	float scale = ((mx - p90) < 2 * (p90 - median)) ? p90 : mx;
+	__syncthreads();
 
-	if (0.f == scale)
-		scale = 1.f;
+	for (int i = threadIdx.x; i < NH * NB; i += blockDim.x)
+		if (h[i])
+			atomicAdd(&ss->hist[0][0] + i, h[i]);
 
-	st->scale = scale;
-	st->inv_scale = (float)(1. / scale);
+	__threadfence();
+	__syncthreads();
+
+	if (0 == threadIdx.x)
+		last = (atomicAdd(&ss->blocks_done, 1u) == gridDim.x - 1);
+
+	__syncthreads();
+
+	if (!last)
+		return;
+
+	__threadfence();
+	const int warp = threadIdx.x / 32;
+	const int lane = threadIdx.x % 32;
+
+	if (warp < 3) {	// one warp per rank: the digit holding it
+
+		const unsigned* hg = &ss->hist[0][0] + ((0 == P) ? 0 : warp * NB);
+		long long rank = (0 == P) ? ((0 == warp) ? n / 2 : ((1 == warp) ? (long long)trunc(n * 0.9) : n - 1))
+					  : ss->rank[warp];
+		constexpr int PER = NB / 32;
+		unsigned tot = 0u;
+
+		for (int k = 0; k < PER; k++)
+			tot += __ldcg(hg + lane * PER + k);
+
+		unsigned incl = tot;
+
+		for (int o = 1; o < 32; o <<= 1) {
+
+			unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+
+			if (lane >= o)
+				incl += t;
+		}
+
+		const long long excl = (long long)incl - tot;
+		const bool mine = (excl <= rank) && (rank < (long long)incl);
+
+		if (mine) {
+
+			long long before = excl;
+			int dsel = lane * PER;
+
+			for (int k = 0; k < PER; k++) {
+
+				unsigned c = __ldcg(hg + lane * PER + k);
+
+				if (rank < before + (long long)c) {
+
+					dsel = lane * PER + k;
+					break;
+				}
+
+				before += c;
+			}
+
+			const unsigned base = (0 == P) ? 0u : pre[warp];
+			ss->prefix[warp] = base | ((unsigned)dsel << SHIFT);
+			ss->rank[warp] = rank - before;
+		}
+	}
+
+	__syncthreads();
+
+	for (int i = threadIdx.x; i < NH * NB; i += blockDim.x)
+		(&ss->hist[0][0])[i] = 0u;
+
+	if (0 == threadIdx.x) {
+
+		ss->blocks_done = 0u;
+
+		if (2 == P) {	// estimate_scaling_norm
+
+			float median = __uint_as_float(ss->prefix[0]);
+			float p90 = __uint_as_float(ss->prefix[1]);
+			float mx = __uint_as_float(ss->prefix[2]);
+			float scale = ((mx - p90) < 2 * (p90 - median)) ? p90 : mx;
+
+			if (0.f == scale)
+				scale = 1.f;
+
+			st->scale = scale;
+			st->inv_scale = (float)(1. / scale);
+		}
+	}
 }
 
 __global__ void k_set_scaling(CgScalars* st, float scale)
