@@ -15,6 +15,27 @@
 
 namespace bn {
 
+// sum of the coil-group partials part[i + n g], g = 0..groups-1, in order;
+// the loads of eight groups at a time are issued together
+__device__ __forceinline__ float2 group_sum(const float2* __restrict__ part, long i, long n, int groups)
+{
+	float2 v = part[i];
+
+	for (int g0 = 1; g0 < groups; g0 += 8) {
+
+		float2 t[8];
+#pragma unroll
+		for (int k = 0; k < 8; k++)
+			t[k] = (g0 + k < groups) ? part[i + n * (g0 + k)] : make_float2(0.f, 0.f);
+#pragma unroll
+		for (int k = 0; k < 8; k++)
+			if (g0 + k < groups)
+				v = cadd(v, t[k]);
+	}
+
+	return v;
+}
+
 enum { RED_THREADS = 256 };
 
 template <typename T>
@@ -63,10 +84,7 @@ __global__ void k_combine(float2* __restrict__ dst, const float2* __restrict__ p
 
 	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
 
-		float2 v = part[i];
-
-		for (int g = 1; g < groups; g++)
-			v = cadd(v, part[i + n * g]);
+		float2 v = group_sum(part, i, n, groups);
 
 		if (x) {
 
@@ -172,13 +190,10 @@ __global__ void k_cg_step(float2* __restrict__ x, float2* __restrict__ r, const 
 	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
 
 		float2 pv = p[i];
-		float2 av = part[i];
+		float2 av = group_sum(part, i, n, groups);
 
 		if (p_keep)
 			p_keep[i] = pv;
-
-		for (int g = 1; g < groups; g++)
-			av = cadd(av, part[i + n * g]);
 
 		av.x = fmaf(lam, pv.x, av.x);
 		av.y = fmaf(lam, pv.y, av.y);
@@ -423,11 +438,7 @@ __global__ void k_fcg_step(float2* __restrict__ x, float2* __restrict__ r, const
 	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
 
 		float2 pv = p[i];
-		float2 av = part[i];
-
-#pragma unroll 4
-		for (int g = 1; g < groups; g++)
-			av = cadd(av, part[i + n * g]);
+		float2 av = group_sum(part, i, n, groups);
 
 		av.x = fmaf(lam, pv.x, av.x);
 		av.y = fmaf(lam, pv.y, av.y);
@@ -581,10 +592,10 @@ enum { SEL_BINS = 2048, SEL_THREADS = 256 };
 
 struct SelectState {
 
+	alignas(16) unsigned hist[3][SEL_BINS];	// first: 16-byte vector access
 	unsigned prefix[3];	// key bits chosen so far per rank
 	long long rank[3];	// rank left within the chosen prefix
 	unsigned blocks_done;
-	unsigned hist[3][SEL_BINS];
 };
 
 template <int P>
@@ -602,7 +613,7 @@ __global__ void __launch_bounds__(SEL_THREADS) k_select_pass(const float2* __res
 	constexpr int W = SelDigit<P>::W;
 	constexpr int NB = 1 << W;
 	constexpr int NH = (0 == P) ? 1 : 3;
-	__shared__ unsigned h[NH * NB];
+	__shared__ __align__(16) unsigned h[NH * NB];
 	__shared__ unsigned pre[3];
 	__shared__ int last;
 
@@ -662,19 +673,25 @@ __global__ void __launch_bounds__(SEL_THREADS) k_select_pass(const float2* __res
 		return;
 
 	__threadfence();
+
+	// the global histograms into shared memory (16-byte loads from L2)
+	for (int i = threadIdx.x; i < NH * NB / 4; i += blockDim.x)
+		reinterpret_cast<uint4*>(h)[i] = __ldcg(reinterpret_cast<const uint4*>(&ss->hist[0][0]) + i);
+
+	__syncthreads();
 	const int warp = threadIdx.x / 32;
 	const int lane = threadIdx.x % 32;
 
 	if (warp < 3) {	// one warp per rank: the digit holding it
 
-		const unsigned* hg = &ss->hist[0][0] + ((0 == P) ? 0 : warp * NB);
+		const unsigned* hg = h + ((0 == P) ? 0 : warp * NB);
 		long long rank = (0 == P) ? ((0 == warp) ? n / 2 : ((1 == warp) ? (long long)trunc(n * 0.9) : n - 1))
 					  : ss->rank[warp];
 		constexpr int PER = NB / 32;
 		unsigned tot = 0u;
 
 		for (int k = 0; k < PER; k++)
-			tot += __ldcg(hg + lane * PER + k);
+			tot += hg[lane * PER + k];
 
 		unsigned incl = tot;
 
@@ -696,7 +713,7 @@ __global__ void __launch_bounds__(SEL_THREADS) k_select_pass(const float2* __res
 
 			for (int k = 0; k < PER; k++) {
 
-				unsigned c = __ldcg(hg + lane * PER + k);
+				unsigned c = hg[lane * PER + k];
 
 				if (rank < before + (long long)c) {
 
@@ -715,8 +732,8 @@ __global__ void __launch_bounds__(SEL_THREADS) k_select_pass(const float2* __res
 
 	__syncthreads();
 
-	for (int i = threadIdx.x; i < NH * NB; i += blockDim.x)
-		(&ss->hist[0][0])[i] = 0u;
+	for (int i = threadIdx.x; i < NH * NB / 4; i += blockDim.x)
+		reinterpret_cast<uint4*>(&ss->hist[0][0])[i] = make_uint4(0u, 0u, 0u, 0u);
 
 	if (0 == threadIdx.x) {
 
