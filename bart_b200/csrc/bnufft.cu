@@ -2786,11 +2786,15 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 	ps->npix = ps->nufft->op.g.npix;
 	ps->M = ps->nufft->op.g.M;
 
-	// coil groups: enough blocks in the final row pass, few partials to combine
+	// coil groups of the coil-summing row pass: the fewest coils per block
+	// whose blocks all fit one wave of resident blocks (two per SM), so no
+	// partial second wave idles the SMs, and fewer partials to combine
+	// (256^2, 16 coils: 2 coils per block, 3.6% faster solve than 1)
 	long YZ = (long)ps->nufft->op.g.N[1] * ps->nufft->op.g.N[2];
 	int Brow = choose_B(ps->nufft->op.g.G[0], YZ * ps->C);
 	long rowblocks = (YZ + Brow - 1) / Brow;
-	ps->cpg = (int)std::max<long>(1, std::min<long>(ps->C, (rowblocks * ps->C) / (2 * 148)));
+	const long slots = 2 * 148;
+	ps->cpg = (int)std::max<long>(1, std::min<long>(ps->C, (rowblocks * ps->C + slots - 1) / slots));
 	ps->groups = (int)((ps->C + ps->cpg - 1) / ps->cpg);
 	ps->nparts = (int)vec_blocks(ps->npix);
 
