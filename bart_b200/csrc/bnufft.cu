@@ -2608,6 +2608,9 @@ struct bnufft_pics_s {
 	int fcg_m = 1;			// truncation: directions orthogonalised against
 	int ndots = 0;			// preconditioner last-pass blocks (folded <z, A p> partials)
 	bool fcg_fold = true;		// fold the dot and test launches (BNUFFT_FCG_FOLD=0: not)
+	bool fcg_fused = false;		// folded, and the direction update runs in the cluster
+					// preconditioner (BNUFFT_FCG_FUSE=0: not)
+	int ndir = 0;			// its <p, r> and ||p||^2 partials per launch
 	bnufft_precnet_t net = nullptr;	// learned correction (conf.precond == 2), not owned
 	double* mcn_part = nullptr;	// ||M_circ(r)||^2 partials
 	bf16* nact[2] = { nullptr, nullptr };	// its activations, ping-pong [npix][32]
@@ -2956,7 +2959,7 @@ static int pics_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 }
 
 static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
-		int* nblocks, cudaStream_t st);
+		int* nblocks, cudaStream_t st, const PcDir* dir = nullptr);
 
 // z = M(r): the circulant preconditioner, plus (precond 2) the learned
 // correction ||M_circ(r)|| net(r / ||r||) (1 / ||r|| from the solve's
@@ -2991,7 +2994,7 @@ static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const flo
 // three-pass form): one cluster of CL CTAs
 template <int N, int CL>
 static int launch_precond_cluster(const float2* r, const float2* pinv, float2* z, const float2* pdot,
-		double* dot_part, const int* done, cudaStream_t st)
+		double* dot_part, const int* done, const PcDir& dir, cudaStream_t st)
 {
 	using Sh = PrecondClusterShape<N, CL>;
 	const float2* tw;
@@ -3009,7 +3012,7 @@ static int launch_precond_cluster(const float2* r, const float2* pinv, float2* z
 	cfg.attrs = at;
 	cfg.numAttrs = 1;
 	cudaEvent_t pe = prof_begin("cluster", st);
-	cudaError_t e = cudaLaunchKernelEx(&cfg, k_precond_cluster<N, CL>, r, pinv, z, tw, pdot, dot_part, done);
+	cudaError_t e = cudaLaunchKernelEx(&cfg, k_precond_cluster<N, CL>, r, pinv, z, tw, pdot, dot_part, done, dir);
 	prof_end(pe, st);
 	g_launches.fetch_add(1, std::memory_order_relaxed);
 
@@ -3086,11 +3089,15 @@ static int precond_cluster_size(const Geom& g)
 
 // the circulant preconditioner applied to one image (N-point transforms, no
 // padding)
+// dir: the flexible-CG direction update fused into the cluster form (only
+// where precond_cluster_size is nonzero)
 static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
-		int* nblocks, cudaStream_t st)
+		int* nblocks, cudaStream_t st, const PcDir* dir)
 {
 	bnufft_plan_s* p = ps->nufft;
 	const int* done = &ps->scal->done;
+	PcDir nodir = {};
+	const PcDir& d = dir ? *dir : nodir;
 
 	if (const int cl = precond_cluster_size(p->op.g)) {
 
@@ -3099,13 +3106,13 @@ static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, cons
 		t_prof_precond = true;
 
 		if (16 == cl)
-			s = (64 == n) ? launch_precond_cluster<64, 16>(r, p->pinv, z, pdot, dot_part, done, st)
-				: (128 == n) ? launch_precond_cluster<128, 16>(r, p->pinv, z, pdot, dot_part, done, st)
-				: launch_precond_cluster<256, 16>(r, p->pinv, z, pdot, dot_part, done, st);
+			s = (64 == n) ? launch_precond_cluster<64, 16>(r, p->pinv, z, pdot, dot_part, done, d, st)
+				: (128 == n) ? launch_precond_cluster<128, 16>(r, p->pinv, z, pdot, dot_part, done, d, st)
+				: launch_precond_cluster<256, 16>(r, p->pinv, z, pdot, dot_part, done, d, st);
 		else
-			s = (64 == n) ? launch_precond_cluster<64, 8>(r, p->pinv, z, pdot, dot_part, done, st)
-				: (128 == n) ? launch_precond_cluster<128, 8>(r, p->pinv, z, pdot, dot_part, done, st)
-				: launch_precond_cluster<256, 8>(r, p->pinv, z, pdot, dot_part, done, st);
+			s = (64 == n) ? launch_precond_cluster<64, 8>(r, p->pinv, z, pdot, dot_part, done, d, st)
+				: (128 == n) ? launch_precond_cluster<128, 8>(r, p->pinv, z, pdot, dot_part, done, d, st)
+				: launch_precond_cluster<256, 8>(r, p->pinv, z, pdot, dot_part, done, d, st);
 
 		t_prof_precond = false;
 
@@ -3114,6 +3121,9 @@ static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, cons
 
 		return s;
 	}
+
+	if (dir)
+		return fail(BNUFFT_ERR_ARG, "internal: fused direction without the cluster preconditioner");
 	OpCtx full;
 	full.g = p->op.g;
 
@@ -3156,6 +3166,30 @@ static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	int npap = 0;
 	const bool folded = (1 == ps->conf.precond) && (1 == ps->fcg_m) && ps->fcg_fold;
 	const int ring = (1 == ps->fcg_m) ? 1 : (int)FCG_RING;
+
+	if (folded && ps->fcg_fused) {	// five launches: the normal's passes, the step, the
+					// cluster preconditioner with the next direction
+		TRY(rows_fwd(g.G[0], p, ps->sens, nullptr, nullptr, g.N[0], YZ, YZ * ps->C, op.w.t1, st, done));
+		TRY(op_toeplitz_cols(op, toe_psf(ps->nufft), ps->C, st, done));
+		TRY(rows_inv(g.G[0], op.w.t1, ps->sens, nullptr, nullptr, g.N[0], YZ, (int)ps->C, ps->cpg, ps->part, st,
+				p, ps->pap_part, done, &npap));
+
+		if (npap > ps->max_row_blocks)
+			return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
+
+		k_fcg_step<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, p, ps->ap_ring, 1, ps->part, ps->groups, ps->npix,
+				ps->conf.lambda, ps->scal, it, ps->pap_part, npap, ps->pp_part, ps->ndir, ps->pr_part, ps->ndir,
+				ps->rs_part);
+		LAUNCHED();
+		PcDir d = { ps->scal, it, 0, ps->rs_part, ps->nparts, p, ps->r, ps->pr_part, ps->pp_part };
+		int nd = 0;
+		TRY(pics_precond_circ(ps, ps->r, ps->z, ps->ap_ring, nullptr, &nd, st, &d));
+
+		if (nd != ps->ndir)
+			return fail(BNUFFT_ERR_ARG, "internal: preconditioner block count changed");
+
+		return BNUFFT_OK;
+	}
 
 	if (!folded) {
 
@@ -3377,7 +3411,20 @@ static int pics_solve(bnufft_pics_s* ps, const float2* ksp, float2* out, cudaStr
 	if (ps->conf.precond) {	// z0 = M(b); the first direction is p = z0
 
 		int nd = 0;
-		TRY(pics_precond(ps, ps->r, ps->z, nullptr, nullptr, &nd, st));
+		const char* e = getenv("BNUFFT_FCG_FUSE");
+		ps->fcg_fused = (1 == ps->conf.precond) && (1 == ps->fcg_m) && ps->fcg_fold
+				&& (0 != precond_cluster_size(ps->nufft->op.g)) && !(e && (0 == strcmp(e, "0")));
+
+		if (ps->fcg_fused) {	// p0 = z0 and its partials, from the cluster preconditioner
+
+			PcDir d = { ps->scal, 0, 1, ps->rs_part, ps->nparts, ps->pbuf[1], ps->r, ps->pr_part, ps->pp_part };
+			TRY(pics_precond_circ(ps, ps->r, ps->z, nullptr, nullptr, &nd, st, &d));
+			ps->ndir = nd;
+
+		} else {
+
+			TRY(pics_precond(ps, ps->r, ps->z, nullptr, nullptr, &nd, st));
+		}
 
 		if (nd > ps->max_row_blocks)
 			return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");

@@ -21,6 +21,14 @@
 //      the partial <pdot, z> of the CTA (flexible CG's next beta).
 // After the second barrier no CTA touches another's shared memory, so CTAs
 // may exit independently.
+//
+// With PcDir (flexible CG with one kept direction) the kernel also ends the
+// CG iteration: before the transforms, the convergence test of the step
+// just taken (||r||^2 partials; every CTA reaches the same decision, so all
+// return together); after them, <A p, z> is summed over the CTAs through
+// distributed shared memory in a fixed order, beta = <A p, z> / <p, A p>,
+// p = z - beta p in place (p = z for the first direction), and per CTA the
+// partials <p, r> and ||p||^2 of the next step. z itself is not stored.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -30,6 +38,19 @@
 #include "nufft_kernels.cuh"
 
 namespace bn {
+
+struct PcDir {
+
+	CgScalars* st;		// nullptr: plain application
+	int it;			// the step just taken (< 0: the device counter)
+	int start;		// first direction: p = z, no test
+	const double* rs_part;	// ||r||^2 partials of the step
+	int nrs;
+	float2* p;		// the direction, updated in place
+	const float2* r;	// the residual
+	double* pr_part;	// [CL] partials <p, r>
+	double* pp_part;	// [CL] partials ||p||^2
+};
 
 template <int N, int CL>
 struct PrecondClusterShape {
@@ -48,7 +69,8 @@ struct PrecondClusterShape {
 template <int N, int CL>
 __global__ void __launch_bounds__(PrecondClusterShape<N, CL>::NT, 1)
 k_precond_cluster(const float2* __restrict__ r, const float2* __restrict__ pinv, float2* z,
-		const float2* __restrict__ twg, const float2* pdot, double* __restrict__ dot_part, const int* done)
+		const float2* __restrict__ twg, const float2* pdot, double* __restrict__ dot_part, const int* done,
+		PcDir dir)
 {
 	using S = PrecondClusterShape<N, CL>;
 	constexpr int R = S::R;
@@ -57,6 +79,7 @@ k_precond_cluster(const float2* __restrict__ r, const float2* __restrict__ pinv,
 	using CLY = typename S::CLY;
 	extern __shared__ float2 smem[];
 	__shared__ double red[32];
+	__shared__ double cdot;
 	float2* rowbuf = smem;			// [R][N] this CTA's rows
 	float2* s = smem + R * N;		// FFT scratch
 	float2* tw = s + S::SCR;
@@ -68,6 +91,28 @@ k_precond_cluster(const float2* __restrict__ r, const float2* __restrict__ pinv,
 	namespace cgr = cooperative_groups;
 	cgr::cluster_group cluster = cgr::this_cluster();
 	const int c = (int)cluster.block_rank();
+	const bool fuse = (nullptr != dir.st);
+	const int it = fuse ? cg_iter(dir.it, dir.st) : 0;
+
+	if (fuse && !dir.start) {	// convergence test of the step just taken
+
+		const double rs = sum_partials_d(dir.rs_part, dir.nrs, red);
+		const bool stop = (rs <= dir.st->eps2);
+
+		if ((0 == c) && (0 == threadIdx.x)) {
+
+			dir.st->rs[(it + 1) & 1] = rs;
+
+			if (stop) {
+
+				dir.st->done = 1;
+				dir.st->iters = it + 1;
+			}
+		}
+
+		if (stop)
+			return;
+	}
 
 	for (int i = threadIdx.x; i < N; i += S::NT)
 		tw[i] = twg[i];
@@ -135,7 +180,9 @@ k_precond_cluster(const float2* __restrict__ r, const float2* __restrict__ pinv,
 		for (int m = 0; m < 8; m++) {
 
 			const long i = unwrap_pos(jt + T * m, N, N) + N * y;
-			z[i] = v[m];
+
+			if (!fuse)
+				z[i] = v[m];
 
 			if (pdot) {	// Re<pdot, z> (pdot == z: ||z||^2)
 
@@ -144,12 +191,65 @@ k_precond_cluster(const float2* __restrict__ r, const float2* __restrict__ pinv,
 			}
 		}
 
-		if (pdot) {
+		if (pdot && !fuse) {
 
 			double t = block_sum_d(dot, red);
 
 			if (0 == threadIdx.x)
 				dot_part[c] = t;
+		}
+
+		if (fuse) {
+
+			float beta = 0.f;
+
+			if (!dir.start) {	// <A p, z> over the cluster, fixed order
+
+				double t = block_sum_d(dot, red);
+
+				if (0 == threadIdx.x)
+					cdot = t;
+
+				cluster.sync();
+				double dsum = 0.;
+
+				for (int k = 0; k < CL; k++)
+					dsum += *cluster.map_shared_rank(&cdot, k);
+
+				cluster.sync();	// no CTA leaves while its cdot is read
+				beta = (float)(dsum / dir.st->pap_hist[0]);
+			}
+
+			double pr = 0., pp = 0.;
+#pragma unroll
+			for (int m = 0; m < 8; m++) {
+
+				const long i = unwrap_pos(jt + T * m, N, N) + N * y;
+				float2 pn = v[m];
+
+				if (!dir.start) {
+
+					float2 po = dir.p[i];
+					pn.x = fmaf(-beta, po.x, pn.x);
+					pn.y = fmaf(-beta, po.y, pn.y);
+				}
+
+				dir.p[i] = pn;
+				float2 rv = dir.r[i];
+				pr += (double)pn.x * (double)rv.x + (double)pn.y * (double)rv.y;
+				pp += (double)pn.x * (double)pn.x + (double)pn.y * (double)pn.y;
+			}
+
+			double t = block_sum_d(pr, red);
+
+			if (0 == threadIdx.x)
+				dir.pr_part[c] = t;
+
+			__syncthreads();
+			t = block_sum_d(pp, red);
+
+			if (0 == threadIdx.x)
+				dir.pp_part[c] = t;
 		}
 	}
 }
