@@ -1370,6 +1370,88 @@ static bool on_device(const void* p)
 	return (cudaMemoryTypeDevice == a.type) || (cudaMemoryTypeManaged == a.type);
 }
 
+// per thread and device: an auxiliary compute stream with a fork / join
+// event pair, and a copy stream with its event
+struct AuxStream {
+
+	cudaStream_t st = nullptr;
+	cudaEvent_t fork = nullptr, join = nullptr;
+	cudaStream_t cp = nullptr;
+	cudaEvent_t copied = nullptr;
+};
+
+static const AuxStream* aux_stream(int dev)
+{
+	static thread_local std::map<int, AuxStream> aux;
+	auto it = aux.find(dev);
+
+	if (it != aux.end())
+		return &it->second;
+
+	AuxStream a;
+
+	if ((cudaSuccess != cudaStreamCreateWithFlags(&a.st, cudaStreamNonBlocking))
+	    || (cudaSuccess != cudaEventCreateWithFlags(&a.fork, cudaEventDisableTiming))
+	    || (cudaSuccess != cudaEventCreateWithFlags(&a.join, cudaEventDisableTiming))
+	    || (cudaSuccess != cudaStreamCreateWithFlags(&a.cp, cudaStreamNonBlocking))
+	    || (cudaSuccess != cudaEventCreateWithFlags(&a.copied, cudaEventDisableTiming))) {
+
+		cudaGetLastError();
+		return nullptr;
+	}
+
+	// the library allocates and frees stream-ordered per model: keep the
+	// device's default pool from returning its memory at every host
+	// synchronisation (it would map it again for the next model)
+	cudaMemPool_t pool;
+
+	if (cudaSuccess == cudaDeviceGetDefaultMemPool(&pool, dev)) {
+
+		uint64_t keep = UINT64_MAX;
+		cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+	}
+
+	cudaGetLastError();
+	return &(aux[dev] = a);
+}
+
+// the copy stream of this thread and device (nullptr: none)
+static cudaStream_t copy_stream()
+{
+	int dev = 0;
+
+	if (cudaSuccess != cudaGetDevice(&dev))
+		return nullptr;
+
+	const AuxStream* aux = aux_stream(dev);
+	return aux ? aux->cp : nullptr;
+}
+
+// host-to-device copy of a host array on the copy stream: st waits for it,
+// and the call returns once the copy has read the host array (not after
+// earlier work queued on st). dst must be allocated in the copy stream's
+// order (copy_stream()), so that a block still in use by earlier work on
+// st is never handed out for it.
+static int copy_in(void* dst, const void* src, size_t bytes, cudaStream_t st)
+{
+	int dev = 0;
+	CUDA_TRY(cudaGetDevice(&dev));
+	const AuxStream* aux = aux_stream(dev);
+
+	if (!aux) {
+
+		CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+		CUDA_TRY(cudaStreamSynchronize(st));
+		return BNUFFT_OK;
+	}
+
+	CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, aux->cp));
+	CUDA_TRY(cudaEventRecord(aux->copied, aux->cp));
+	CUDA_TRY(cudaStreamWaitEvent(st, aux->copied, 0));
+	CUDA_TRY(cudaEventSynchronize(aux->copied));
+	return BNUFFT_OK;
+}
+
 // staging of host data through device buffers (the e2e path)
 // Staging buffers come from the stream-ordered pool (cudaMallocAsync) and go
 // back to it in stream order, so host-pointer calls neither synchronise the
@@ -1393,11 +1475,11 @@ static int stage_in(Staged& s, const void* p, size_t bytes, cudaStream_t st)
 		return BNUFFT_OK;
 	}
 
-	CUDA_TRY(cudaMallocAsync(&s.dev, bytes, st));
+	cudaStream_t cs = copy_stream();
+	CUDA_TRY(cudaMallocAsync(&s.dev, bytes, cs ? cs : st));
 	s.owned = true;
 	s.st = st;
-	CUDA_TRY(cudaMemcpyAsync(s.dev, p, bytes, cudaMemcpyHostToDevice, st));
-	return BNUFFT_OK;
+	return copy_in(s.dev, p, bytes, st);
 }
 
 static int stage_out_alloc(Staged& s, void* p, size_t bytes, cudaStream_t st = nullptr)
@@ -1605,34 +1687,6 @@ static int check_conf(const bnufft_conf* conf)
 	return BNUFFT_OK;
 }
 
-// per thread and device: an auxiliary stream and a fork / join event pair
-struct AuxStream {
-
-	cudaStream_t st = nullptr;
-	cudaEvent_t fork = nullptr, join = nullptr;
-};
-
-static const AuxStream* aux_stream(int dev)
-{
-	static thread_local std::map<int, AuxStream> aux;
-	auto it = aux.find(dev);
-
-	if (it != aux.end())
-		return &it->second;
-
-	AuxStream a;
-
-	if ((cudaSuccess != cudaStreamCreateWithFlags(&a.st, cudaStreamNonBlocking))
-	    || (cudaSuccess != cudaEventCreateWithFlags(&a.fork, cudaEventDisableTiming))
-	    || (cudaSuccess != cudaEventCreateWithFlags(&a.join, cudaEventDisableTiming))) {
-
-		cudaGetLastError();
-		return nullptr;
-	}
-
-	return &(aux[dev] = a);
-}
-
 // Trajectory upload: converted trajectory and sample bins on st; with the
 // Toeplitz normal the PSF chain (its own binning on the 4N grid, gridding,
 // transforms, embedding) runs meanwhile on an auxiliary stream (the two are
@@ -1695,9 +1749,6 @@ static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
 
 	TRY(s_psf);
 	TRY(s);
-
-	if (t.owned)
-		CUDA_TRY(cudaStreamSynchronize(st));
 
 	return BNUFFT_OK;
 }
@@ -2802,7 +2853,9 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 	ps->nparts = (int)vec_blocks(ps->npix);
 
 	auto ck = [&](cudaError_t e) { if (cudaSuccess != e && BNUFFT_OK == s) s = fail(BNUFFT_ERR_NOMEM, "pics buffers: %s", cudaGetErrorString(e)); };
-	ck(cudaMallocAsync(&ps->sens, sizeof(float2) * ps->npix * ps->C, st));
+	// maps from the host are copied on the copy stream: allocated in its order
+	cudaStream_t mst = on_device(sens) ? st : copy_stream();
+	ck(cudaMallocAsync(&ps->sens, sizeof(float2) * ps->npix * ps->C, mst ? mst : st));
 	ck(cudaMallocAsync(&ps->part, sizeof(float2) * ps->npix * ps->groups, st));
 	ck(cudaMallocAsync(&ps->x, sizeof(float2) * ps->npix, st));
 	ck(cudaMallocAsync(&ps->r, sizeof(float2) * ps->npix, st));
@@ -2850,10 +2903,19 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 
 	if (BNUFFT_OK == s) {
 
-		cudaError_t e = cudaMemcpyAsync(ps->sens, sens, sizeof(float2) * ps->npix * ps->C, cudaMemcpyDefault, st);
+		const size_t mb = sizeof(float2) * ps->npix * ps->C;
 
-		if (cudaSuccess != e)
-			s = fail(BNUFFT_ERR_CUDA, "maps upload: %s", cudaGetErrorString(e));
+		if (on_device(sens)) {
+
+			cudaError_t e = cudaMemcpyAsync(ps->sens, sens, mb, cudaMemcpyDeviceToDevice, st);
+
+			if (cudaSuccess != e)
+				s = fail(BNUFFT_ERR_CUDA, "maps upload: %s", cudaGetErrorString(e));
+
+		} else {	// returns once the host array has been read
+
+			s = copy_in(ps->sens, sens, mb, st);
+		}
 	}
 
 	if (BNUFFT_OK != s) {
