@@ -91,6 +91,37 @@ __device__ __forceinline__ void dft8(float2* v)
 	v[7] = csub(e3, t3);
 }
 
+// dft8 of (v0, v1, 0, 0, 0, 0, v6, v7): the first stage of a transform whose
+// input is zero-padded to twice its length with the centred placement (the
+// nonzero half at positions < L/4 and >= 3L/4, i.e. registers 0, 1, 6, 7).
+// The same operations as dft8 minus those on the known zeros, so the same
+// results (up to the sign of exact zeros).
+template <bool INV>
+__device__ __forceinline__ void dft8_half(float2* v)
+{
+	// dft4 of (a, 0, 0, b): (a + b, a + rot(-b), a - b, a - rot(-b))
+	const float2 e0 = cadd(v[0], v[6]), e2 = csub(v[0], v[6]);
+	const float2 eb = rot90<INV>(make_float2(-v[6].x, -v[6].y));
+	const float2 e1 = cadd(v[0], eb), e3 = csub(v[0], eb);
+	const float2 o0 = cadd(v[1], v[7]), o2 = csub(v[1], v[7]);
+	const float2 ob = rot90<INV>(make_float2(-v[7].x, -v[7].y));
+	const float2 o1 = cadd(v[1], ob), o3 = csub(v[1], ob);
+	const float c = 0.70710678118654752440f;
+	float2 t1 = INV ? make_float2(c * (o1.x - o1.y), c * (o1.x + o1.y))
+			: make_float2(c * (o1.x + o1.y), c * (o1.y - o1.x));
+	float2 t2 = rot90<INV>(o2);
+	float2 t3 = INV ? make_float2(-c * (o3.x + o3.y), c * (o3.x - o3.y))
+			: make_float2(c * (o3.y - o3.x), -c * (o3.x + o3.y));
+	v[0] = cadd(e0, o0);
+	v[4] = csub(e0, o0);
+	v[1] = cadd(e1, t1);
+	v[5] = csub(e1, t1);
+	v[2] = cadd(e2, t2);
+	v[6] = csub(e2, t2);
+	v[3] = cadd(e3, t3);
+	v[7] = csub(e3, t3);
+}
+
 template <int R, bool INV>
 __device__ __forceinline__ void butterfly(float2* v)
 {
@@ -218,15 +249,19 @@ __device__ __forceinline__ void fft_tail(float2 (&v)[8], float2* s, int b, int j
 // Full transform of the register set v (positions jt + (L/8)*m in, same
 // out). Begins with a barrier, so the caller may have been reading s just
 // before; the caller must barrier before writing s after it returns.
+// half_in: registers 2..5 are known zeros (input of length L/2, centred).
 template <int L, typename LAY, bool INV>
-__device__ __forceinline__ void fft_regs(float2 (&v)[8], float2* s, const float2* tw)
+__device__ __forceinline__ void fft_regs(float2 (&v)[8], float2* s, const float2* tw, bool half_in = false)
 {
 	static_assert(L >= 16 && L <= 4096 && (L & (L - 1)) == 0, "power-of-two length 16..4096");
 	const int b = LAY::seq();
 	const int jt = LAY::jt();
 
 	// stage 1 (Ns = 1, radix 8, no twiddles): registers -> smem at 8*jt + i
-	butterfly<8, INV>(v);
+	if (half_in)
+		dft8_half<INV>(v);
+	else
+		butterfly<8, INV>(v);
 	__syncthreads();
 #pragma unroll
 	for (int i = 0; i < 8; i++)

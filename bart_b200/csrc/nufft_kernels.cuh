@@ -42,11 +42,12 @@ struct Dft {
 // Bluestein the caller has loaded zeros at positions >= d.n and gets zeros
 // there back. Same barrier contract as fft_regs.
 template <int L, typename LAY, bool INV, bool BLUE>
-__device__ __forceinline__ void dft_regs(float2 (&v)[8], float2* s, const float2* tw, const Dft& d)
+__device__ __forceinline__ void dft_regs(float2 (&v)[8], float2* s, const float2* tw, const Dft& d,
+		bool half_in = false)
 {
 	if constexpr (!BLUE) {
 
-		fft_regs<L, LAY, INV>(v, s, tw);
+		fft_regs<L, LAY, INV>(v, s, tw, half_in);
 		return;
 	}
 
@@ -323,7 +324,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 	if (0 == threadIdx.x)
 		pp_part[blockIdx.x] = t;
 
-	dft_regs<L, LAY, false, BLUE>(v, s, tw, d);
+	dft_regs<L, LAY, false, BLUE>(v, s, tw, d, 2 * X == L);
 
 	if (valid) {
 #pragma unroll
@@ -384,7 +385,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		}
 	}
 
-	dft_regs<L, LAY, false, BLUE>(v, s, tw, d);
+	dft_regs<L, LAY, false, BLUE>(v, s, tw, d, 2 * X == L);
 
 	if (valid) {
 #pragma unroll
@@ -450,7 +451,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 
 	} else {
 
-		dft_regs<L, LAY, false, BLUE>(v, s, tw, d);
+		dft_regs<L, LAY, false, BLUE>(v, s, tw, d, wrap_in && (2 * n_in == L));
 	}
 
 	if constexpr (MODE == 2) {
