@@ -139,7 +139,10 @@ void bnufft_pics_conf_defaults(struct bnufft_pics_conf* conf);
 
 /* Builds the SENSE model A = NUFFT o maps (sense_nc_init,
  * src/sense/modelnc.c:28-67; maps2_create src/sense/model.c:93) for
- * ksp_dims [1, Mr, Ms, C], sens_dims [X, Y, Z, C], traj_dims [3, Mr, Ms]. */
+ * ksp_dims [1, Mr, Ms, C], sens_dims [X, Y, Z, C], traj_dims [3, Mr, Ms].
+ * Host arrays are copied on the library's per-thread copy stream; the call
+ * returns once they have been read (the caller may reuse them), while the
+ * model's set-up kernels may still run on the stream. */
 int bnufft_pics_create(bnufft_pics_t* pics, int N, const long ksp_dims[], const long sens_dims[],
 		const long traj_dims[], const void* traj, const void* sens,
 		const struct bnufft_pics_conf* conf, void* stream);
@@ -163,6 +166,9 @@ int bnufft_pics_stats(bnufft_pics_t pics, int* iters, double* rel_resid, float* 
  * kernels and bit-identical results). */
 int bnufft_pics_kernels(bnufft_pics_t pics, long* kernels, void* stream);
 
+/* Releases the model without waiting for the device: its buffers are freed
+ * in stream order after its last run, and its CG loop graph is kept for
+ * the next model to reuse (or destroyed once that run has completed). */
 void bnufft_pics_free(bnufft_pics_t pics);
 
 /* Change the iteration limit and tolerance of later runs (the captured CG
