@@ -4,6 +4,11 @@
                             [-p pattern] traj input output
   python -m bart_b200 pics -l2 -r lambda [-i iter] -t traj [-w scale] [-S]
                            [--no-toeplitz] ksp sens output
+  python -m bart_b200 -l flags pics ...   (or -p flags: the same here)
+
+With -l / -p (src/bart.c:202-217) pics runs once per index of the flagged
+dims (e.g. 8192 = slices, dim 13); all those problems run as one batched
+graph launch and the images are joined along the flagged dims.
 
 Options follow src/nufft.c:75-101 and src/pics.c:137-199; options of the
 reference that are not built here are rejected with an error.
@@ -104,7 +109,8 @@ def main_nufft(argv) -> int:
     return 0
 
 
-def main_pics(argv) -> int:
+def parse_pics(argv):
+    """pics options and its three input arrays"""
     ap = argparse.ArgumentParser(prog="pics")
     ap.add_argument("-l", dest="reg", choices=["2"], help="only -l2 (CG) is built")
     ap.add_argument("-r", dest="lam", type=float, default=0.0)
@@ -118,23 +124,44 @@ def main_pics(argv) -> int:
     ap.add_argument("sens")
     ap.add_argument("output")
     a = ap.parse_args(argv)
-    traj = readcfl(a.traj)
-    ksp = readcfl(a.ksp)
-    sens = readcfl(a.sens)
-    conf = PicsConf(lam=a.lam, maxiter=a.iters, scaling=a.scaling, rescale=a.rescale, toeplitz=not a.no_toeplitz)
-    p = Pics(traj, sens, ksp_dims=list(ksp.shape), conf=conf)
-    img = p.run(ksp)
+    a.traj_name = a.traj
+    a.traj = readcfl(a.traj_name)
+    a.ksp = readcfl(a.ksp)
+    a.sens = readcfl(a.sens)
+    a.toeplitz = not a.no_toeplitz
+    return a
+
+
+def main_pics(argv, loop_flags: int = 0) -> int:
+    a = parse_pics(argv)
+    if loop_flags:
+        from .loop import loop_pics
+        writecfl(a.output, loop_pics(loop_flags, a))
+        return 0
+    conf = PicsConf(lam=a.lam, maxiter=a.iters, scaling=a.scaling, rescale=a.rescale, toeplitz=a.toeplitz)
+    p = Pics(a.traj, a.sens, ksp_dims=list(a.ksp.shape), conf=conf)
+    img = p.run(a.ksp)
     p.free()
-    writecfl(a.output, img.reshape(list(sens.shape[:3]), order="F"))
+    sd = list(a.sens.shape) + [1] * 3
+    writecfl(a.output, img.reshape(sd[:3], order="F"))
     return 0
 
 
 def main(argv=None) -> int:
     argv = list(sys.argv[1:] if argv is None else argv)
-    if not argv or argv[0] not in ("nufft", "pics"):
+    flags = 0
+    while argv and argv[0] in ("-l", "-p", "--loop", "--parallel-loop"):	# bart -l / -p flags
+        if len(argv) < 2:
+            sys.stderr.write(__doc__)
+            return 2
+        flags |= int(argv[1])
+        argv = argv[2:]
+    if not argv or argv[0] not in ("nufft", "pics") or (flags and argv[0] != "pics"):
         sys.stderr.write(__doc__)
         return 2
-    return {"nufft": main_nufft, "pics": main_pics}[argv[0]](argv[1:])
+    if "pics" == argv[0]:
+        return main_pics(argv[1:], flags)
+    return main_nufft(argv[1:])
 
 
 if __name__ == "__main__":

@@ -52,12 +52,13 @@ class BatchRecon:
         for prob in problems:
             traj, sens, ksp = prob["traj"], prob["sens"], prob["ksp"]
             N = sens.shape[0]
+            npix = int(np.prod(sens.shape[:3]))
             conf = PicsConf(lam=lam, maxiter=maxiter, toeplitz=True, bin=pick_bin(bins, N), **conf_kw)
             td, sd = _dev(traj, dev), _dev(sens, dev)
             p = Pics(td, sd, ksp_dims=list(ksp.shape), conf=conf, traj_dims=list(traj.shape), sens_dims=list(sens.shape))
             self.models.append(p)
             self.ksp.append(_dev(ksp, dev))
-            self.img.append(torch.empty(N * N, dtype=torch.complex64, device=dev))
+            self.img.append(torch.empty(npix, dtype=torch.complex64, device=dev))
         self.batch = None
 
     def build(self):

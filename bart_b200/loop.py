@@ -1,0 +1,118 @@
+"""``bart -l flags`` / ``bart -p flags``: one tool run over the slices of its
+files (src/bart.c:202-217, 568-600).
+
+The reference runs the tool once per index of the flagged dimensions: every
+input file is read at that index along each flagged dimension it has (a
+file of size 1 there is used for every index), and the outputs are joined
+along those dimensions. Here the per-index problems of ``pics`` are not run
+one after another: each becomes its own SENSE model, and all of them run as
+one batched graph launch (``bnufft_batch_create``: every problem's whole
+solve an independent child graph), which the GPU overlaps. The results are
+those of the loop of single runs up to float32 summation order.
+"""
+
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+
+from .cfl import DIMS, dims16
+
+
+def loop_dims(flags: int) -> list:
+    """The dimensions selected by a BART loop bitmask."""
+    if flags < 0 or flags >= (1 << DIMS):
+        raise ValueError(f"loop flags {flags} outside the 16 dims")
+    return [d for d in range(DIMS) if flags & (1 << d)]
+
+
+def loop_sizes(shapes, dims) -> list:
+    """Loop length per flagged dim: the files' sizes there must be 1 or one
+    common value (as the reference's cfl loop requires)."""
+    sizes = []
+    for d in dims:
+        vals = {dims16(s)[d] for s in shapes} - {1}
+        if len(vals) > 1:
+            raise ValueError(f"files disagree along looped dim {d}: sizes {sorted(vals)}")
+        sizes.append(vals.pop() if vals else 1)
+    return sizes
+
+
+def loop_indices(sizes) -> list:
+    """All index tuples, the first flagged dim fastest (the reference's
+    default order)."""
+    return [tuple(reversed(t)) for t in itertools.product(*[range(n) for n in reversed(sizes)])]
+
+
+def slice_at(a: np.ndarray, dims, idx) -> np.ndarray:
+    """``a`` at index idx along the flagged dims it has (size-1 dims are
+    kept as they are), as an F-ordered array of the same rank."""
+    a16 = a.reshape(dims16(a.shape), order="F")
+    sl = [slice(None)] * DIMS
+    for d, i in zip(dims, idx):
+        if a16.shape[d] > 1:
+            sl[d] = slice(i, i + 1)
+    return np.asfortranarray(a16[tuple(sl)])
+
+
+def place_at(out: np.ndarray, dims, idx, block: np.ndarray) -> None:
+    """Write one index's result into the joined output."""
+    sl = [slice(None)] * DIMS
+    for d, i in zip(dims, idx):
+        sl[d] = slice(i, i + 1)
+    out[tuple(sl)] = block.reshape(out[tuple(sl)].shape, order="F")
+
+
+def loop_pics(flags: int, a, dev=None) -> np.ndarray:
+    """``bart -l flags pics ...``: every index of the flagged dims as one
+    problem, all problems as one batched launch; returns the joined image
+    (X, Y, Z and the flagged dims). ``a`` holds the parsed pics options and
+    arrays (traj, ksp, sens). The looped dims must lie outside the ones the
+    problem itself uses (0-3: readout / phase / partition, coils)."""
+    import torch
+    from .batch import BatchRecon
+    from .pics import Pics, PicsConf
+
+    dims = loop_dims(flags)
+    if any(d < 4 for d in dims):
+        raise ValueError("pics: looped dims must be >= 4 (dims 0-3 are the image and coil axes)")
+    shapes = [a.traj.shape, a.ksp.shape, a.sens.shape]
+    sizes = loop_sizes(shapes, dims)
+    idxs = loop_indices(sizes)
+    img_dims = list(dims16(a.sens.shape)[:3])
+    out_dims = img_dims + [1] * (DIMS - 3)
+    for d, n in zip(dims, sizes):
+        out_dims[d] = n
+    out = np.zeros(out_dims, dtype=np.complex64, order="F")
+
+    def problem(idx):
+        traj = slice_at(a.traj, dims, idx).reshape(dims16(a.traj.shape)[:3], order="F")
+        ksp = slice_at(a.ksp, dims, idx)
+        ksp = ksp.reshape(dims16(ksp.shape)[:4], order="F")
+        sens = slice_at(a.sens, dims, idx)
+        sens = sens.reshape(dims16(sens.shape)[:4], order="F")
+        return {"traj": traj, "sens": sens, "ksp": ksp}
+
+    probs = [problem(i) for i in idxs]
+    dev = dev or torch.device("cuda", torch.cuda.current_device())
+
+    if a.toeplitz:	# one graph launch for all problems
+        br = BatchRecon(probs, dev, lam=a.lam, maxiter=a.iters, scaling=a.scaling, rescale=a.rescale).build()
+        try:
+            br.run()
+            torch.cuda.synchronize(dev)
+            imgs = [t.cpu().numpy() for t in br.img]
+        finally:
+            br.free()
+    else:		# the non-Toeplitz normal: one solve after another
+        imgs = []
+        for pr in probs:
+            conf = PicsConf(lam=a.lam, maxiter=a.iters, scaling=a.scaling, rescale=a.rescale, toeplitz=False)
+            p = Pics(pr["traj"], pr["sens"], ksp_dims=list(pr["ksp"].shape), conf=conf)
+            imgs.append(np.asarray(p.run(pr["ksp"])))
+            p.free()
+
+    for idx, im in zip(idxs, imgs):
+        place_at(out, dims, idx, im)
+    return out

@@ -46,3 +46,55 @@ def test_autotuner_returns_candidates(cuda):
     table, detail = autotune_bins(cuda, sizes=(64, 96), candidates=(16, 32), coils=2, spokes=16, reps=1)
     assert set(table) == {64, 96} and all(v in (16, 32) for v in table.values())
     assert all(len(d) == 2 for d in detail.values())
+
+
+@pytest.mark.parametrize("traj_per_slice", [False, True])
+def test_cli_loop_over_slices_matches_single_runs(cuda, tmp_path, traj_per_slice):
+    """python -m bart_b200 -l 8192 pics (slices along dim 13, the reference's
+    bart -l): all slices in one batched launch, joined along dim 13, equal to
+    running pics on each slice's own files (up to the atomics' summation
+    order of the adjoint). The trajectory is shared (size 1 along dim 13) or
+    one per slice."""
+    from bart_b200 import __main__ as cli
+    from bart_b200.cfl import readcfl, writecfl
+    from bart_b200.problems import cgsense_problem, simulate_ksp
+
+    S = 3
+    base = cgsense_problem(np.random.default_rng(10), N=64, coils=4, spokes=24)
+    probs = []
+    for sl in range(S):
+        p = cgsense_problem(np.random.default_rng(20 + sl), N=64, coils=4, spokes=24)
+        t = base["traj"].copy()
+        if traj_per_slice:	# each slice's spokes rotated by its own angle
+            c, sn = np.cos(0.3 * sl), np.sin(0.3 * sl)
+            x, y = t[0].real.copy(), t[1].real.copy()
+            t[0], t[1] = c * x - sn * y, sn * x + c * y
+        p["traj"] = t.astype(np.complex64)
+        p["ksp"] = simulate_ksp(p["traj"], p["truth"], p["sens"], 40.0, np.random.default_rng(30 + sl))
+        probs.append(p)
+
+    def stack(key):
+        arrs = [np.asarray(p[key]) for p in probs]
+        a16 = [a.reshape(list(a.shape) + [1] * (16 - a.ndim), order="F") for a in arrs]
+        return np.concatenate(a16, axis=13)
+
+    ksp, sens = stack("ksp"), stack("sens")
+    traj = stack("traj") if traj_per_slice else probs[0]["traj"]
+    d = str(tmp_path)
+    writecfl(d + "/traj", traj)
+    writecfl(d + "/ksp", ksp)
+    writecfl(d + "/sens", sens)
+    opts = ["-r", "0.01", "-i", "15"]
+    assert 0 == cli.main(["-l", "8192", "pics"] + opts + ["-t", d + "/traj", d + "/ksp", d + "/sens", d + "/out"])
+    out = readcfl(d + "/out")
+    assert out.shape[13] == S and out.shape[:3] == (64, 64, 1)
+    for s in range(S):
+        p = probs[s]
+        writecfl(d + f"/t{s}", p["traj"])
+        writecfl(d + f"/k{s}", p["ksp"])
+        writecfl(d + f"/s{s}", p["sens"])
+        assert 0 == cli.main(["pics"] + opts + ["-t", d + f"/t{s}", d + f"/k{s}", d + f"/s{s}", d + f"/o{s}"])
+        single = readcfl(d + f"/o{s}").reshape(64, 64, order="F")
+        joined = out[..., s, :, :].reshape(64, 64, order="F")
+        assert np.linalg.norm(single) > 0
+        assert rel(joined, single) < 1e-4, (s, rel(joined, single))

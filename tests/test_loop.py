@@ -1,0 +1,43 @@
+"""The bart -l / -p loop front-end (src/bart.c:202-217): slicing, joining and
+index order, on the CPU."""
+
+import numpy as np
+import pytest
+
+from bart_b200 import __main__ as cli
+from bart_b200.loop import loop_dims, loop_indices, loop_sizes, place_at, slice_at
+
+
+def test_loop_dims_and_sizes():
+    assert loop_dims(8192) == [13]
+    assert loop_dims((1 << 10) | (1 << 13)) == [10, 13]
+    assert loop_sizes([[3, 64, 8] + [1] * 10 + [1], [1, 64, 8, 4] + [1] * 9 + [5]], [13]) == [5]
+    with pytest.raises(ValueError):
+        loop_sizes([[1] * 13 + [3], [1] * 13 + [5]], [13])
+    with pytest.raises(ValueError):
+        loop_dims(1 << 16)
+
+
+def test_loop_indices_first_dim_fastest():
+    assert loop_indices([2, 3]) == [(0, 0), (1, 0), (0, 1), (1, 1), (0, 2), (1, 2)]
+    assert loop_indices([1]) == [(0,)]
+
+
+def test_slice_and_place_round_trip():
+    rng = np.random.default_rng(0)
+    a = (rng.standard_normal((4, 3, 1, 2) + (1,) * 9 + (5, 1, 1)) + 0j).astype(np.complex64)
+    out = np.zeros_like(a, order="F")
+    for idx in loop_indices([5]):
+        s = slice_at(a, [13], idx)
+        assert s.shape[13] == 1
+        np.testing.assert_array_equal(s[..., 0, :, :], a[..., idx[0]:idx[0] + 1, :, :][..., 0, :, :])
+        place_at(out, [13], idx, s)
+    np.testing.assert_array_equal(out, a)
+    # a file of size 1 along the looped dim is used for every index
+    b = a[..., :1, :, :]
+    np.testing.assert_array_equal(slice_at(b, [13], (3,)), b)
+
+
+def test_cli_rejects_loop_for_other_tools(capsys):
+    assert 2 == cli.main(["-l", "8192", "nufft", "t", "i", "o"])
+    assert 2 == cli.main(["-l"])
