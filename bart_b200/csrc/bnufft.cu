@@ -1527,10 +1527,46 @@ struct bnufft_plan_s {
 	OpCtx toe;
 	float2* psf_t = nullptr;
 	cudaStream_t st0;
+	// the PSF chain (and a pics model's preconditioner spectrum) runs on the
+	// auxiliary stream; this event is recorded after it
+	cudaEvent_t psf_ev = nullptr;
 };
 
+// A stream about to use the PSF, its embedding or the preconditioner
+// spectrum first waits for the auxiliary stream's work that builds them, so
+// the model's other set-up and the solve's adjoint run meanwhile. Skipped
+// while the stream captures a graph (captures of whole solves are preceded
+// by a host wait for that work; the CG loop graph is launched after a wait).
+static void psf_wait(const bnufft_plan_s* p, cudaStream_t st)
+{
+	if (!p->psf_ev)
+		return;
+
+	cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+
+	if (cudaSuccess != cudaStreamIsCapturing(st, &cs)) {
+
+		cudaGetLastError();
+		return;
+	}
+
+	if (cudaStreamCaptureStatusNone == cs)
+		cudaStreamWaitEvent(st, p->psf_ev, 0);
+}
+
 static OpCtx& toe_ctx(bnufft_plan_s* p) { return p->embed ? p->toe : p->op; }
-static const float2* toe_psf(const bnufft_plan_s* p) { return p->embed ? p->psf_t : p->psf; }
+
+static const float2* toe_psf(const bnufft_plan_s* p, cudaStream_t st)
+{
+	psf_wait(p, st);
+	return p->embed ? p->psf_t : p->psf;
+}
+
+static const float2* precond_spec(const bnufft_plan_s* p, cudaStream_t st)
+{
+	psf_wait(p, st);
+	return p->pinv;
+}
 
 // q'[i] = scale * q[d mod L] at d = i (i < N) or i - E (i > E - N), else 0,
 // per axis: the kernel of the Toeplitz operator (|d| < N) moved from the
@@ -1690,16 +1726,19 @@ static int check_conf(const bnufft_conf* conf)
 // Trajectory upload: converted trajectory and sample bins on st; with the
 // Toeplitz normal the PSF chain (its own binning on the 4N grid, gridding,
 // transforms, embedding) runs meanwhile on an auxiliary stream (the two are
-// independent chains of small kernels), joined back into st before return.
+// independent chains of small kernels). It is not joined here: p->psf_ev is
+// recorded after it, and every later use of the PSF waits for that event
+// (psf_wait), so work that does not need the PSF proceeds.
 static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
 {
 	Staged t;
 	TRY(stage_in(t, traj, sizeof(float2) * 3 * p->op.g.M, st));
 	int dev = 0;
 	CUDA_TRY(cudaGetDevice(&dev));
-	const AuxStream* aux = p->conf.toeplitz ? aux_stream(dev) : nullptr;
+	const AuxStream* aux = (p->conf.toeplitz && p->psf_ev) ? aux_stream(dev) : nullptr;
 	cudaStream_t pst = aux ? aux->st : st;
 	int s_psf = BNUFFT_OK;
+	psf_wait(p, st);	// an earlier PSF chain of this plan is done before its buffers go
 
 	if (p->conf.toeplitz) {
 
@@ -1740,11 +1779,22 @@ static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
 		s = build_csr(p->op, st);
 	}
 
-	// joined whatever happened, so that nothing outlives its inputs
-	if (aux) {
+	if (p->conf.toeplitz) {	// whatever happened, so that nothing outlives its inputs
 
-		cudaEventRecord(aux->join, pst);
-		cudaStreamWaitEvent(st, aux->join, 0);
+		if (p->psf_ev)
+			cudaEventRecord(p->psf_ev, pst);
+
+		if (aux) {	// the staged trajectory is freed after both streams' uses
+
+			cudaEventRecord(aux->join, st);
+			cudaStreamWaitEvent(pst, aux->join, 0);
+
+			if (t.owned) {
+
+				cudaFreeAsync(t.dev, pst);
+				t.owned = false;
+			}
+		}
 	}
 
 	TRY(s_psf);
@@ -1795,6 +1845,13 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 	}
 
 	auto p = new bnufft_plan_s();
+
+	if (cudaSuccess != cudaEventCreateWithFlags(&p->psf_ev, cudaEventDisableTiming)) {
+
+		cudaGetLastError();
+		p->psf_ev = nullptr;	// no event: the PSF is then built on the caller's stream
+	}
+
 	p->N = N;
 	p->ksp_dims.assign(ksp_dims, ksp_dims + N);
 	p->cim_dims.assign(cim_dims, cim_dims + N);
@@ -1928,7 +1985,7 @@ extern "C" int bnufft_apply_normal(bnufft_plan_t p, void* dst, const void* src, 
 		const long npix = p->op.g.npix, cc = coil_chunk(p);
 
 		for (long c0 = 0; c0 < p->C; c0 += cc)
-			TRY(op_toeplitz(toe_ctx(p), toe_psf(p), (const float2*)i.dev + npix * c0, nullptr, std::min(cc, p->C - c0),
+			TRY(op_toeplitz(toe_ctx(p), toe_psf(p, st), (const float2*)i.dev + npix * c0, nullptr, std::min(cc, p->C - c0),
 					1, (float2*)o.dev + npix * c0, st));
 
 	} else {
@@ -2016,6 +2073,7 @@ extern "C" int bnufft_get_psf(bnufft_plan_t p, int ND, const long psf_dims[], vo
 	size_t b = sizeof(float2) * p->op.g.gsz;
 	Staged o;
 	TRY(stage_out_alloc(o, psf, b, st));
+	psf_wait(p, st);
 	k_psf_decompose<<<vec_blocks(p->op.g.gsz), RED_THREADS, 0, st>>>((float2*)o.dev, p->psf, grid_geom(p->op.g), (float)p->op.g.npix);
 	LAUNCHED();
 	return stage_out_copy(o, psf, b, st);
@@ -2027,6 +2085,7 @@ extern "C" void bnufft_free(bnufft_plan_t p)
 		return;
 
 	cudaStream_t st = p->st0;
+	psf_wait(p, st);	// the frees follow the auxiliary stream's work on the PSF
 	free_work(p->op.w, st);
 	free_work(p->toe.w, st);
 	free_csr(p->op.csr, st);
@@ -2038,6 +2097,9 @@ extern "C" void bnufft_free(bnufft_plan_t p)
 	if (p->wgt) cudaFreeAsync(p->wgt, st);
 	if (p->pinv) cudaFreeAsync(p->pinv, st);
 	if (p->op.wbuf) cudaFreeAsync(p->op.wbuf, st);
+
+	if (p->psf_ev)
+		cudaEventDestroy(p->psf_ev);
 
 	delete p;	// device frees are stream-ordered; host state can go now
 }
@@ -2062,7 +2124,11 @@ static int build_precond(bnufft_plan_s* p, cudaStream_t st)
 	if (!p->psf)
 		return fail(BNUFFT_ERR_ARG, "the circulant preconditioner needs the Toeplitz PSF");
 
-	OpCtx& op = p->op;
+	psf_wait(p, st);
+	// work buffers of its own: it may run on the auxiliary stream while the
+	// plan's buffers serve the solve on another stream
+	OpCtx op = p->op;
+	op.w = Work{};
 	const Geom& g = op.g;
 	TRY(alloc_work(op.w, g, 1, st));
 	float2* crop = nullptr;
@@ -2087,6 +2153,7 @@ static int build_precond(bnufft_plan_s* p, cudaStream_t st)
 	k_precond_from_spectrum<<<vec_blocks(g.npix), RED_THREADS, 0, st>>>(p->pinv, F, g.npix, (float)(1. / sqrt((double)g.npix)));
 	LAUNCHED();
 	free_work(full.w, st);
+	free_work(op.w, st);
 	cudaFreeAsync(crop, st);
 	cudaFreeAsync(F, st);
 	return BNUFFT_OK;
@@ -2108,7 +2175,7 @@ static int apply_precond(bnufft_plan_s* p, float2* v, long C, cudaStream_t st)
 	const Geom& g = full.g;
 	long YZ = (long)g.N[1] * g.N[2];
 	TRY(rows_fwd(g.G[0], v, nullptr, nullptr, nullptr, g.N[0], YZ, YZ * C, full.w.t1, st));
-	TRY(op_toeplitz_cols(full, p->pinv, C, st));
+	TRY(op_toeplitz_cols(full, precond_spec(p, st), C, st));
 	return rows_inv(g.G[0], full.w.t1, nullptr, nullptr, nullptr, g.N[0], YZ, (int)C, 1, v, st);
 }
 
@@ -2160,7 +2227,7 @@ extern "C" int bnufft_nufft_inverse(bnufft_plan_t p, void* img, const void* ksp,
 		// Ap = P^-1 (N^H N p + lambda p); partial p^H Ap
 		if (p->psf) {
 
-			TRY(op_toeplitz(toe_ctx(p), toe_psf(p), pv, nullptr, C, 1, Ap, st));
+			TRY(op_toeplitz(toe_ctx(p), toe_psf(p, st), pv, nullptr, C, 1, Ap, st));
 
 		} else {
 
@@ -2773,7 +2840,7 @@ static int sense_normal(bnufft_pics_s* ps, const float2* x, float2* out, float l
 
 	if (ps->nufft->psf) {
 
-		TRY(op_toeplitz(toe_ctx(ps->nufft), toe_psf(ps->nufft), x, ps->sens, ps->C, ps->cpg, ps->part, st));
+		TRY(op_toeplitz(toe_ctx(ps->nufft), toe_psf(ps->nufft, st), x, ps->sens, ps->C, ps->cpg, ps->part, st));
 
 	} else {
 
@@ -2897,8 +2964,16 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 				ps->max_row_blocks), st));
 		ck(cudaMallocAsync(&ps->pr_part, sizeof(double) * ps->nparts, st));
 
-		if (BNUFFT_OK == s)
-			s = build_precond(ps->nufft, st);
+		if (BNUFFT_OK == s) {	// after the PSF, on the stream that builds it
+
+			int dev = 0;
+			const AuxStream* aux = (ps->nufft->psf_ev && (cudaSuccess == cudaGetDevice(&dev))) ? aux_stream(dev) : nullptr;
+			cudaStream_t pst = aux ? aux->st : st;
+			s = build_precond(ps->nufft, pst);
+
+			if (ps->nufft->psf_ev)
+				cudaEventRecord(ps->nufft->psf_ev, pst);
+		}
 	}
 
 	if (BNUFFT_OK == s) {
@@ -3000,7 +3075,7 @@ static int pics_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 
 	if (toep) {
 
-		TRY(op_toeplitz_cols(op, toe_psf(ps->nufft), ps->C, st, done));
+		TRY(op_toeplitz_cols(op, toe_psf(ps->nufft, st), ps->C, st, done));
 		TRY(rows_inv(g.G[0], op.w.t1, ps->sens, nullptr, nullptr, g.N[0], YZ, (int)ps->C, ps->cpg, ps->part, st,
 				dh.p, dh.part, dh.done, dh.nblocks));
 
@@ -3168,13 +3243,13 @@ static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, cons
 		t_prof_precond = true;
 
 		if (16 == cl)
-			s = (64 == n) ? launch_precond_cluster<64, 16>(r, p->pinv, z, pdot, dot_part, done, d, st)
-				: (128 == n) ? launch_precond_cluster<128, 16>(r, p->pinv, z, pdot, dot_part, done, d, st)
-				: launch_precond_cluster<256, 16>(r, p->pinv, z, pdot, dot_part, done, d, st);
+			s = (64 == n) ? launch_precond_cluster<64, 16>(r, precond_spec(p, st), z, pdot, dot_part, done, d, st)
+				: (128 == n) ? launch_precond_cluster<128, 16>(r, precond_spec(p, st), z, pdot, dot_part, done, d, st)
+				: launch_precond_cluster<256, 16>(r, precond_spec(p, st), z, pdot, dot_part, done, d, st);
 		else
-			s = (64 == n) ? launch_precond_cluster<64, 8>(r, p->pinv, z, pdot, dot_part, done, d, st)
-				: (128 == n) ? launch_precond_cluster<128, 8>(r, p->pinv, z, pdot, dot_part, done, d, st)
-				: launch_precond_cluster<256, 8>(r, p->pinv, z, pdot, dot_part, done, d, st);
+			s = (64 == n) ? launch_precond_cluster<64, 8>(r, precond_spec(p, st), z, pdot, dot_part, done, d, st)
+				: (128 == n) ? launch_precond_cluster<128, 8>(r, precond_spec(p, st), z, pdot, dot_part, done, d, st)
+				: launch_precond_cluster<256, 8>(r, precond_spec(p, st), z, pdot, dot_part, done, d, st);
 
 		t_prof_precond = false;
 
@@ -3202,7 +3277,7 @@ static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, cons
 	int s = rows_fwd(g.G[0], r, nullptr, nullptr, nullptr, g.N[0], YZ, YZ, full.w.t1, st, done);
 
 	if (BNUFFT_OK == s)
-		s = op_toeplitz_cols(full, p->pinv, 1, st, done);
+		s = op_toeplitz_cols(full, precond_spec(p, st), 1, st, done);
 
 	if (BNUFFT_OK == s)
 		s = rows_inv(g.G[0], full.w.t1, nullptr, nullptr, nullptr, g.N[0], YZ, 1, 1, z, st, pdot, dot_part, done, nblocks);
@@ -3232,7 +3307,7 @@ static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	if (folded && ps->fcg_fused) {	// five launches: the normal's passes, the step, the
 					// cluster preconditioner with the next direction
 		TRY(rows_fwd(g.G[0], p, ps->sens, nullptr, nullptr, g.N[0], YZ, YZ * ps->C, op.w.t1, st, done));
-		TRY(op_toeplitz_cols(op, toe_psf(ps->nufft), ps->C, st, done));
+		TRY(op_toeplitz_cols(op, toe_psf(ps->nufft, st), ps->C, st, done));
 		TRY(rows_inv(g.G[0], op.w.t1, ps->sens, nullptr, nullptr, g.N[0], YZ, (int)ps->C, ps->cpg, ps->part, st,
 				p, ps->pap_part, done, &npap));
 
@@ -3264,7 +3339,7 @@ static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 			folded ? ps->rs_part : nullptr, ps->nparts);
 	LAUNCHED();
 	TRY(rows_fwd(g.G[0], p, ps->sens, nullptr, nullptr, g.N[0], YZ, YZ * ps->C, op.w.t1, st, done));
-	TRY(op_toeplitz_cols(op, toe_psf(ps->nufft), ps->C, st, done));
+	TRY(op_toeplitz_cols(op, toe_psf(ps->nufft, st), ps->C, st, done));
 	TRY(rows_inv(g.G[0], op.w.t1, ps->sens, nullptr, nullptr, g.N[0], YZ, (int)ps->C, ps->cpg, ps->part, st,
 			p, ps->pap_part, done, &npap));
 
@@ -3470,6 +3545,11 @@ static int pics_solve(bnufft_pics_s* ps, const float2* ksp, float2* out, cudaStr
 	if (ps->nufft->embed)
 		TRY(alloc_work(ps->nufft->toe.w, ps->nufft->toe.g, ps->C, st));
 
+	// the adjoint and the scaling above ran while the auxiliary stream built
+	// the PSF (and the preconditioner); the iterations need them (the loop
+	// graph's capture does not wait, so the stream waits here)
+	psf_wait(ps->nufft, st);
+
 	if (ps->conf.precond) {	// z0 = M(b); the first direction is p = z0
 
 		int nd = 0;
@@ -3596,6 +3676,10 @@ extern "C" int bnufft_batch_create(bnufft_batch_t* out, const bnufft_pics_t* mod
 
 		if (models[p]->nufft->embed)
 			TRY(alloc_work(models[p]->nufft->toe.w, models[p]->nufft->toe.g, models[p]->C, st));
+
+		// the captured solves do not wait for the PSF's stream: it is done first
+		if (models[p]->nufft->psf_ev)
+			CUDA_TRY(cudaEventSynchronize(models[p]->nufft->psf_ev));
 	}
 
 	CUDA_TRY(cudaStreamSynchronize(st));
