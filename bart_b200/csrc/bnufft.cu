@@ -2730,6 +2730,7 @@ struct bnufft_pics_s {
 					// preconditioner (BNUFFT_FCG_FUSE=0: not)
 	int ndir = 0;			// its <p, r> and ||p||^2 partials per launch
 	bnufft_precnet_t net = nullptr;	// learned correction (conf.precond == 2), not owned
+	float2* pinv_pad = nullptr;	// padded-circulant spectrum (conf.precond == 3), Toeplitz grid
 	double* mcn_part = nullptr;	// ||M_circ(r)||^2 partials
 	bf16* nact[2] = { nullptr, nullptr };	// its activations, ping-pong [npix][32]
 	long max_row_blocks;
@@ -2853,6 +2854,8 @@ static int sense_normal(bnufft_pics_s* ps, const float2* x, float2* out, float l
 	return BNUFFT_OK;
 }
 
+static int build_precond_pad(bnufft_pics_s* ps, cudaStream_t st);
+
 extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims[], const long sens_dims[],
 		const long traj_dims[], const void* traj, const void* sens,
 		const struct bnufft_pics_conf* conf_in, void* stream)
@@ -2887,7 +2890,7 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 	nc.deterministic = conf.deterministic;
 	nc.bin = conf.bin;
 
-	if ((conf.precond < 0) || (conf.precond > 2))
+	if ((conf.precond < 0) || (conf.precond > 3))
 		return fail(BNUFFT_ERR_ARG, "precond must be 0, 1 or 2");
 
 	if (conf.precond && !conf.toeplitz)
@@ -2969,7 +2972,11 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 			int dev = 0;
 			const AuxStream* aux = (ps->nufft->psf_ev && (cudaSuccess == cudaGetDevice(&dev))) ? aux_stream(dev) : nullptr;
 			cudaStream_t pst = aux ? aux->st : st;
-			s = build_precond(ps->nufft, pst);
+
+			if (3 == conf.precond)
+				s = build_precond_pad(ps, pst);
+			else
+				s = build_precond(ps->nufft, pst);
 
 			if (ps->nufft->psf_ev)
 				cudaEventRecord(ps->nufft->psf_ev, pst);
@@ -3098,12 +3105,58 @@ static int pics_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 static int pics_precond_circ(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
 		int* nblocks, cudaStream_t st, const PcDir* dir = nullptr);
 
+// the padded-circulant spectrum 1/(|P| + mu) on the Toeplitz grid (precond 3,
+// k_precond_pad_spectrum), built after the PSF on the stream that builds it
+static int build_precond_pad(bnufft_pics_s* ps, cudaStream_t st)
+{
+	bnufft_plan_s* p = ps->nufft;
+
+	if (!p->psf)
+		return fail(BNUFFT_ERR_ARG, "the padded preconditioner needs the Toeplitz PSF");
+
+	const Geom& g = toe_ctx(p).g;
+	const float mu_lam = (float)(2.5 * ps->conf.lambda * std::pow(4., (double)g.nd) / (double)g.gsz);
+	CUDA_TRY(cudaMallocAsync(&ps->pinv_pad, sizeof(float2) * g.gsz, st));
+	k_precond_pad_spectrum<<<vec_blocks(g.gsz), RED_THREADS, 0, st>>>(ps->pinv_pad, toe_psf(p, st), g.gsz, mu_lam);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+// z = crop F^-1 (|P| + mu)^-1 F pad r: the Toeplitz passes on one image with
+// the padded-circulant spectrum in place of the PSF (the plan's buffers,
+// free between the normal operator's passes); optional partials Re<pdot, z>
+static int pics_precond_pad(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
+		int* nblocks, cudaStream_t st)
+{
+	bnufft_plan_s* p = ps->nufft;
+	OpCtx& op = toe_ctx(p);
+	const Geom& g = op.g;
+	const int* done = &ps->scal->done;
+	long YZ = (long)g.N[1] * g.N[2];
+	psf_wait(p, st);
+	TRY(alloc_work(op.w, g, 1, st));	// allocates only outside a solve (which sizes it first)
+	t_prof_precond = true;
+	int s = rows_fwd(g.G[0], r, nullptr, nullptr, nullptr, g.N[0], YZ, YZ, op.w.t1, st, done);
+
+	if (BNUFFT_OK == s)
+		s = op_toeplitz_cols(op, ps->pinv_pad, 1, st, done);
+
+	if (BNUFFT_OK == s)
+		s = rows_inv(g.G[0], op.w.t1, nullptr, nullptr, nullptr, g.N[0], YZ, 1, 1, z, st, pdot, dot_part, done, nblocks);
+
+	t_prof_precond = false;
+	return s;
+}
+
 // z = M(r): the circulant preconditioner, plus (precond 2) the learned
 // correction ||M_circ(r)|| net(r / ||r||) (1 / ||r|| from the solve's
 // scalars); optional partials Re<pdot, z>
 static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
 		int* nblocks, cudaStream_t st)
 {
+	if (3 == ps->conf.precond)
+		return pics_precond_pad(ps, r, z, pdot, dot_part, nblocks, st);
+
 	if (2 != ps->conf.precond)
 		return pics_precond_circ(ps, r, z, pdot, dot_part, nblocks, st);
 
@@ -3301,7 +3354,7 @@ static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	float2* p = ps->pbuf[1];
 	unsigned nb = (unsigned)ps->nparts;
 	int npap = 0;
-	const bool folded = (1 == ps->conf.precond) && (1 == ps->fcg_m) && ps->fcg_fold;
+	const bool folded = ((1 == ps->conf.precond) || (3 == ps->conf.precond)) && (1 == ps->fcg_m) && ps->fcg_fold;
 	const int ring = (1 == ps->fcg_m) ? 1 : (int)FCG_RING;
 
 	if (folded && ps->fcg_fused) {	// five launches: the normal's passes, the step, the
@@ -3909,7 +3962,7 @@ extern "C" void bnufft_pics_free(bnufft_pics_t ps)
 
 	void* bufs[] = { ps->sens, ps->part, ps->x, ps->r, ps->pbuf[0], ps->pbuf[1], ps->b, ps->kbuf, ps->mag, ps->sel,
 			 ps->pap_part, ps->pp_part, ps->rs_part, ps->scal, ps->z, ps->p_ring, ps->ap_ring,
-			 ps->dots_part, ps->pr_part, ps->nact[0], ps->nact[1], ps->mcn_part };
+			 ps->dots_part, ps->pr_part, ps->nact[0], ps->nact[1], ps->mcn_part, ps->pinv_pad };
 
 	for (void* b : bufs)
 		if (b)

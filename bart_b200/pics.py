@@ -30,7 +30,7 @@ class PicsConf:
     periodic: bool = False
     deterministic: bool = False
     bin: int = 0              # gridding bin edge (0 = default); tuning only
-    precond: int = 0          # 0 plain CG, 1 FCG + circulant, 2 FCG + circulant + learned
+    precond: int = 0          # 0 plain CG, 1 FCG + circulant, 2 FCG + circulant + learned, 3 FCG + padded circulant
 
     def c(self) -> _lib.PicsConfC:
         return _lib.PicsConfC(float(self.lam), int(self.maxiter), float(self.tol), float(self.scaling),

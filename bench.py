@@ -507,7 +507,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "batch"])
     ap.add_argument("--spokes", type=int, default=20000, help="nufft3d: kooshball spokes")
-    ap.add_argument("--methods", default="fcg_circulant,cg,fcg_learned",
+    ap.add_argument("--methods", default="fcg_padded,fcg_circulant,cg,fcg_learned",
                     help="solvers to time (cgsense2d); the first is the headline")
     ap.add_argument("--lean", action="store_true",
                     help="skip the fixed-iteration, end-to-end and NUFFT extras (for profiling runs)")
@@ -563,7 +563,7 @@ def main():
     # the three solvers to 1e-4: the headline is the fastest, flexible CG
     # with the circulant PSF preconditioner; plain CG is the reference's
     # method, the learned correction is measured beside them
-    all_methods = {"cg": 0, "fcg_circulant": 1, "fcg_learned": 2}
+    all_methods = {"cg": 0, "fcg_circulant": 1, "fcg_learned": 2, "fcg_padded": 3}
     names = [m for m in args.methods.split(",") if m]
     assert names and all(m in all_methods for m in names), f"--methods from {list(all_methods)}"
     headline = names[0]

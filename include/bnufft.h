@@ -129,8 +129,12 @@ struct bnufft_pics_conf {
 				   the circulant preconditioner of the NUFFT's PSF
 				   (nufft_precond_create, src/noncart/precond.c:48-164);
 				   2: flexible CG with the circulant preconditioner plus
-				   the learned correction (bnufft_pics_set_precnet).
-				   1 and 2 need the Toeplitz normal operator. */
+				   the learned correction (bnufft_pics_set_precnet);
+				   3: flexible CG with the padded-circulant preconditioner
+				   (no counterpart in the reference): the Toeplitz
+				   operator's own 2N (or embedding) circulant inverted,
+				   crop F^-1 (|P| + mu)^-1 F pad, mu from lambda.
+				   1, 2 and 3 need the Toeplitz normal operator. */
 };
 
 typedef struct bnufft_pics_s* bnufft_pics_t;
@@ -209,7 +213,7 @@ void bnufft_batch_free(bnufft_batch_t batch);
  * bnufft_pics_run). img-sized output. */
 int bnufft_pics_rhs(bnufft_pics_t pics, void* b, const void* ksp, void* stream);
 
-/* z = M(r), the model's preconditioner (precond 1 or 2) on one image. */
+/* z = M(r), the model's preconditioner (precond 1, 2 or 3) on one image. */
 int bnufft_pics_precond(bnufft_pics_t pics, void* z, const void* r, void* stream);
 
 /* Learned preconditioner (no counterpart in the reference; the reference's
