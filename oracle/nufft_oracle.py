@@ -429,6 +429,49 @@ def circulant_precond(op: "NufftOracle") -> np.ndarray:
     return np.abs(_fftuc(pre, axes)) + 1e-3
 
 
+def padded_precond(op: "NufftOracle", lam: float, beta: float = 2.5):
+    """The library's padded-circulant preconditioner (precond 3; no
+    counterpart in the reference): the Toeplitz product's own circulant
+    inverted on the zero-padded image, M^-1 v = S^H (|P| + mu)^-1 S v with
+    S = spectrum (S^H S = 2^d here), mu = beta lam 2^d, floored at
+    1e-3 |P| at DC. The device kernel uses the same operator with its
+    unnormalised FFTs and P / npix: its z is npix^2 times this one."""
+    dims3 = op.dims3
+    d = len(_axes(dims3))
+    P = np.abs(op.psf())
+    dc = P[tuple(n // 2 for n in P.shape)]
+    mu = max(beta * lam * 2.0 ** d, 1e-3 * float(dc))
+    Pm = (P + mu)[..., None]
+
+    def apply(v):
+        return spectrum_adjoint(spectrum(_as4(v)) / Pm, dims3)
+
+    return apply
+
+
+def pcg(normal, b, lam, M, tol=1e-4, maxiter=300):
+    """Preconditioned CG on (normal + lam I) x = b with the preconditioner
+    M (float64); stops when ||r|| <= tol ||b||. Returns (x, iterations)."""
+    x = np.zeros_like(b)
+    r = b.copy()
+    z = M(r)
+    p = z.copy()
+    rz = float(np.vdot(r, z).real)
+    nb = math.sqrt(float(np.vdot(b, b).real))
+    for it in range(1, maxiter + 1):
+        Ap = normal(p) + lam * p
+        a = rz / float(np.vdot(p, Ap).real)
+        x = x + a * p
+        r = r - a * Ap
+        if math.sqrt(float(np.vdot(r, r).real)) <= tol * nb:
+            return x, it
+        z = M(r)
+        rz2 = float(np.vdot(r, z).real)
+        p = z + (rz2 / rz) * p
+        rz = rz2
+    return x, maxiter
+
+
 def nufft_inverse(op: "NufftOracle", ksp, lam=0.0, maxiter=50, precond=False):
     """``bart nufft -i [-c] -l lam -m maxiter`` (src/nufft.c:250-263): CG
     (l2lambda 0) on P^-1 (N^H N + lam) x = P^-1 N^H y over all coil images

@@ -264,6 +264,23 @@ def test_fcg_padded_precond(name):
     assert its[3, "1"] < its[0, "1"] and its[3, "1"] <= its[1, "1"], its
 
 
+def test_padded_precond_matches_oracle():
+    """z = M(r) of precond 3 on the device equals the FP64 oracle's
+    padded-circulant preconditioner (its npix^2 normalisation, see
+    oracle.padded_precond) on a power-of-two problem."""
+    g = golden("pics2d_n64_c4")
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    N = g["sens"].shape[0]
+    A = orc.SenseOracle(traj, g["sens"])
+    p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape), conf=PicsConf(lam=0.01, precond=3))
+    rng = np.random.default_rng(3)
+    r = (rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))).astype(np.complex64)
+    z = np.asarray(p.precond(np.asfortranarray(r))).reshape(N, N, order="F")
+    p.free()
+    zo = orc.padded_precond(A.nufft, 0.01)(r.astype(np.complex128).reshape(N, N, 1, 1))[:, :, 0, 0]
+    assert rel(z, (N * N) ** 2 * zo) < 1e-5
+
+
 def test_fcg_folded_launches_match_unfolded():
     """The folded circulant flexible CG (dot products from the
     preconditioner's last pass, convergence test in the next direction
