@@ -5,8 +5,10 @@ polynomial maps, 96 golden-angle spokes x 512 samples, 40 dB noise,
 lambda 0.01, Toeplitz normal operator, automatic data scaling, solved until
 the relative normal-equation residual reaches 1e-4 (the problem of
 ``bart pics -l2 -r0.01 -t traj ksp sens out``). The headline solver is
-flexible CG with the circulant PSF preconditioner; plain CG (the reference's
-method) and flexible CG with the learned correction are timed beside it.
+PCG with the padded-circulant preconditioner (the Toeplitz operator's own
+circulant inverted on the padded image); flexible CG with the reference's
+Strang circulant preconditioner, plain CG (the reference's method) and
+flexible CG with the learned correction are timed beside it.
 One step is one full reconstruction from device-resident trajectory, maps
 and k-space: model set-up (trajectory upload, PSF on the device), adjoint,
 scaling, CG graph. L2 is flushed before every timed step. The config's
@@ -247,10 +249,11 @@ def run_nufft3d(dev, steps, warmup, spokes=20000):
     torch.cuda.synchronize()
     cg_ms = e0.elapsed_time(e1)
     p.free()
-    # to the 1e-4 tolerance: plain CG and flexible CG with the circulant
-    # preconditioner (model reused, one solve each after a warm-up)
+    # to the 1e-4 tolerance: plain CG, flexible CG with the circulant
+    # preconditioner, PCG with the padded one (model reused, one solve each
+    # after a warm-up)
     to_tol = {}
-    for name, pc in (("cg", 0), ("fcg_circulant", 1)):
+    for name, pc in (("cg", 0), ("fcg_circulant", 1), ("fcg_padded", 3)):
         p = Pics(t_d, sens_d, ksp_dims=kd, conf=PicsConf(lam=LAM, maxiter=200, tol=TOL, precond=pc),
                  traj_dims=list(t.shape), sens_dims=cd)
         x = p.run(k)
@@ -560,9 +563,10 @@ def main():
     stream = torch.cuda.current_stream(dev)
     from bart_b200.precnet import PrecNet
     net = PrecNet.load()
-    # the three solvers to 1e-4: the headline is the fastest, flexible CG
-    # with the circulant PSF preconditioner; plain CG is the reference's
-    # method, the learned correction is measured beside them
+    # the solvers to 1e-4: the headline is the fastest, PCG with the
+    # padded-circulant preconditioner; flexible CG with the reference's
+    # circulant preconditioner, plain CG (the reference's method) and the
+    # learned correction are measured beside it
     all_methods = {"cg": 0, "fcg_circulant": 1, "fcg_learned": 2, "fcg_padded": 3}
     names = [m for m in args.methods.split(",") if m]
     assert names and all(m in all_methods for m in names), f"--methods from {list(all_methods)}"
@@ -693,8 +697,11 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "image": N_IMG, "coils": COILS, "spokes": SPOKES, "samples": 512,
                            "tol": TOL, "maxiter": MAXITER, "lambda": LAM, "toeplitz": True,
-                           "method": "flexible CG with the circulant PSF preconditioner (same normal equations "
-                                     "and tolerance as the reference's plain-CG pics)",
+                           "method": {"cg": "plain CG (the reference's pics)",
+                                      "fcg_circulant": "flexible CG with the reference's circulant PSF preconditioner",
+                                      "fcg_learned": "flexible CG with the circulant preconditioner and the learned correction",
+                                      "fcg_padded": "PCG with the padded-circulant preconditioner"}[headline]
+                                     + " (same normal equations and tolerance as the reference's plain-CG pics)",
                            "parallelism": f"replicas{world}",
                            "l2": "flushed before every timed step (512 MB write); inside a step the ~60 MB "
                                  "working set stays L2-resident across CG iterations"},
