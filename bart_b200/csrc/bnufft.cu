@@ -3925,9 +3925,14 @@ extern "C" void bnufft_pics_free(bnufft_pics_t ps)
 	cudaStream_t st = ps->nufft ? ps->nufft->st0 : nullptr;
 	reap_graves();
 
-	// the stream-ordered frees below follow the last run, on whatever stream it was
+	// the stream-ordered frees below follow the last run, on whatever stream
+	// it was, and the auxiliary stream's set-up work (the preconditioner
+	// spectrum is written there)
 	if (ps->run_done)
 		cudaStreamWaitEvent(st, ps->run_done, 0);
+
+	if (ps->nufft)
+		psf_wait(ps->nufft, st);
 
 	if (ps->cg_exec && ps->run_done) {
 
