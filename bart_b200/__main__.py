@@ -6,6 +6,11 @@
                            [--no-toeplitz] ksp sens output
   python -m bart_b200 -l flags pics ...   (or -p flags: the same here)
 
+pics also takes two options the reference does not have: --precond 1|3
+(flexible CG with the reference's circulant preconditioner / PCG with the
+padded-circulant one; default 0, the reference's plain CG) and --tol t
+(stop at ||r|| <= t ||A^H y||; default 0, run -i iterations).
+
 With -l / -p (src/bart.c:202-217) pics runs once per index of the flagged
 dims (e.g. 8192 = slices, dim 13); all those problems run as one batched
 graph launch and the images are joined along the flagged dims.
@@ -120,10 +125,17 @@ def parse_pics(argv):
     ap.add_argument("-S", dest="rescale", action="store_true")
     ap.add_argument("-g", dest="gpu", action="store_true")
     ap.add_argument("--no-toeplitz", dest="no_toeplitz", action="store_true")
+    # not in the reference: the library's preconditioned solvers and a CG
+    # tolerance (defaults keep the reference's plain CG for -i iterations)
+    ap.add_argument("--precond", type=int, choices=[0, 1, 3], default=0,
+                    help="0 plain CG, 1 flexible CG + circulant, 3 PCG + padded circulant")
+    ap.add_argument("--tol", type=float, default=0.0, help="stop at ||r|| <= tol ||A^H y|| (0: run -i iterations)")
     ap.add_argument("ksp")
     ap.add_argument("sens")
     ap.add_argument("output")
     a = ap.parse_args(argv)
+    if a.precond and a.no_toeplitz:
+        ap.error("--precond needs the Toeplitz normal operator")
     a.traj_name = a.traj
     a.traj = readcfl(a.traj_name)
     a.ksp = readcfl(a.ksp)
@@ -138,7 +150,8 @@ def main_pics(argv, loop_flags: int = 0) -> int:
         from .loop import loop_pics
         writecfl(a.output, loop_pics(loop_flags, a))
         return 0
-    conf = PicsConf(lam=a.lam, maxiter=a.iters, scaling=a.scaling, rescale=a.rescale, toeplitz=a.toeplitz)
+    conf = PicsConf(lam=a.lam, maxiter=a.iters, tol=a.tol, scaling=a.scaling, rescale=a.rescale, toeplitz=a.toeplitz,
+                    precond=a.precond)
     p = Pics(a.traj, a.sens, ksp_dims=list(a.ksp.shape), conf=conf)
     img = p.run(a.ksp)
     p.free()

@@ -97,18 +97,22 @@ def loop_pics(flags: int, a, dev=None) -> np.ndarray:
     probs = [problem(i) for i in idxs]
     dev = dev or torch.device("cuda", torch.cuda.current_device())
 
-    if a.toeplitz:	# one graph launch for all problems
-        br = BatchRecon(probs, dev, lam=a.lam, maxiter=a.iters, scaling=a.scaling, rescale=a.rescale).build()
+    precond = getattr(a, "precond", 0)
+    tol = getattr(a, "tol", 0.0)
+    if a.toeplitz and tol == 0.0:	# one graph launch for all problems (fixed iteration count)
+        br = BatchRecon(probs, dev, lam=a.lam, maxiter=a.iters, scaling=a.scaling, rescale=a.rescale,
+                        precond=precond).build()
         try:
             br.run()
             torch.cuda.synchronize(dev)
             imgs = [t.cpu().numpy() for t in br.img]
         finally:
             br.free()
-    else:		# the non-Toeplitz normal: one solve after another
+    else:		# non-Toeplitz normal or a tolerance: one solve after another
         imgs = []
         for pr in probs:
-            conf = PicsConf(lam=a.lam, maxiter=a.iters, scaling=a.scaling, rescale=a.rescale, toeplitz=False)
+            conf = PicsConf(lam=a.lam, maxiter=a.iters, tol=tol, scaling=a.scaling, rescale=a.rescale,
+                            toeplitz=a.toeplitz, precond=precond)
             p = Pics(pr["traj"], pr["sens"], ksp_dims=list(pr["ksp"].shape), conf=conf)
             imgs.append(np.asarray(p.run(pr["ksp"])))
             p.free()

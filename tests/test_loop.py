@@ -41,3 +41,18 @@ def test_slice_and_place_round_trip():
 def test_cli_rejects_loop_for_other_tools(capsys):
     assert 2 == cli.main(["-l", "8192", "nufft", "t", "i", "o"])
     assert 2 == cli.main(["-l"])
+
+
+def test_pics_cli_options_parse(tmp_path):
+    """pics command-line options: the reference's defaults (plain CG, -i
+    iterations) and the library's opt-in --precond / --tol."""
+    from bart_b200.cfl import writecfl
+    d = str(tmp_path)
+    for name in ("t", "k", "s"):
+        writecfl(d + "/" + name, np.zeros((2, 2), dtype=np.complex64))
+    a = cli.parse_pics(["-r", "0.01", "-i", "7", "-t", d + "/t", d + "/k", d + "/s", d + "/o"])
+    assert (a.precond, a.tol, a.iters, a.lam, a.toeplitz) == (0, 0.0, 7, 0.01, True)
+    a = cli.parse_pics(["--precond", "3", "--tol", "1e-4", "-t", d + "/t", d + "/k", d + "/s", d + "/o"])
+    assert (a.precond, a.tol) == (3, 1e-4)
+    with pytest.raises(SystemExit):
+        cli.parse_pics(["--precond", "3", "--no-toeplitz", "-t", d + "/t", d + "/k", d + "/s", d + "/o"])
