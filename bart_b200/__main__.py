@@ -13,7 +13,9 @@ padded-circulant one; default 0, the reference's plain CG) and --tol t
 
 With -l / -p (src/bart.c:202-217) pics runs once per index of the flagged
 dims (e.g. 8192 = slices, dim 13); all those problems run as one batched
-graph launch and the images are joined along the flagged dims.
+graph launch and the images are joined along the flagged dims. Launched by
+torchrun with several ranks (one per GPU), the problems are split over the
+ranks by their cost and rank 0 gathers the images and writes the output.
 
 Options follow src/nufft.c:75-101 and src/pics.c:137-199; options of the
 reference that are not built here are rejected with an error.
@@ -22,6 +24,7 @@ reference that are not built here are rejected with an error.
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 
 import numpy as np
@@ -146,9 +149,30 @@ def parse_pics(argv):
 
 def main_pics(argv, loop_flags: int = 0) -> int:
     a = parse_pics(argv)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     if loop_flags:
         from .loop import loop_pics
-        writecfl(a.output, loop_pics(loop_flags, a))
+        if world == 1:
+            writecfl(a.output, loop_pics(loop_flags, a))
+            return 0
+        # one rank per GPU (device = local rank mod GPU count, as the
+        # reference's MPI ranks pick theirs, src/num/gpuops.c:169-187); the
+        # ranks exchange only the finished images, on the host
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")) % torch.cuda.device_count())
+        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+        try:
+            out = loop_pics(loop_flags, a)
+            if rank == 0:
+                writecfl(a.output, out)
+            dist.barrier()
+        finally:
+            dist.destroy_process_group()
+        return 0
+    if rank != 0:	# one problem: rank 0 solves it, the others have nothing to do
         return 0
     conf = PicsConf(lam=a.lam, maxiter=a.iters, tol=a.tol, scaling=a.scaling, rescale=a.rescale, toeplitz=a.toeplitz,
                     precond=a.precond)

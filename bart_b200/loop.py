@@ -69,9 +69,16 @@ def loop_pics(flags: int, a, dev=None) -> np.ndarray:
     problem, all problems as one batched launch; returns the joined image
     (X, Y, Z and the flagged dims). ``a`` holds the parsed pics options and
     arrays (traj, ksp, sens). The looped dims must lie outside the ones the
-    problem itself uses (0-3: readout / phase / partition, coils)."""
+    problem itself uses (0-3: readout / phase / partition, coils).
+
+    Inside a process group of several ranks (one per GPU, as the reference's
+    MPI slice loop, src/bart.c:361-409), every rank solves the share of the
+    problems that the cost-model split gives it, with no exchange while it
+    solves, and the images are gathered to rank 0, which returns the joined
+    image; the other ranks return None."""
     import torch
     from .batch import BatchRecon
+    from .dist import gather_to_root, partition, problem_cost, world_rank
     from .pics import Pics, PicsConf
 
     dims = loop_dims(flags)
@@ -94,12 +101,19 @@ def loop_pics(flags: int, a, dev=None) -> np.ndarray:
         sens = sens.reshape(dims16(sens.shape)[:4], order="F")
         return {"traj": traj, "sens": sens, "ksp": ksp}
 
-    probs = [problem(i) for i in idxs]
+    rank, world = world_rank()
+    mine = list(range(len(idxs)))
+    if world > 1:
+        costs = [problem_cost(problem(i), a.iters, a.toeplitz) for i in idxs]
+        mine = partition(costs, world)[rank]
+    probs = [problem(idxs[k]) for k in mine]
     dev = dev or torch.device("cuda", torch.cuda.current_device())
 
     precond = getattr(a, "precond", 0)
     tol = getattr(a, "tol", 0.0)
-    if a.toeplitz and tol == 0.0:	# one graph launch for all problems (fixed iteration count)
+    if not probs:
+        imgs = []
+    elif a.toeplitz and tol == 0.0:	# one graph launch for all problems (fixed iteration count)
         br = BatchRecon(probs, dev, lam=a.lam, maxiter=a.iters, scaling=a.scaling, rescale=a.rescale,
                         precond=precond).build()
         try:
@@ -117,6 +131,11 @@ def loop_pics(flags: int, a, dev=None) -> np.ndarray:
             imgs.append(np.asarray(p.run(pr["ksp"])))
             p.free()
 
-    for idx, im in zip(idxs, imgs):
-        place_at(out, dims, idx, im)
+    got = dict(zip(mine, imgs))
+    if world > 1:
+        got = gather_to_root(got)
+        if got is None:
+            return None
+    for k, idx in enumerate(idxs):
+        place_at(out, dims, idx, got[k])
     return out

@@ -354,22 +354,35 @@ def fft_vs_cufft(dev, traj, sens, reps=50):
     return res
 
 
-def run_batch(dev, steps, warmup, nprob=512, seed=4):
+def run_batch(dev, steps, warmup, nprob=512, seed=4, rank=0, world=1):
     """Batched uneven 2D reconstructions: nprob problems,
     N ~ U{64..320} even, spokes ~ U{16..256} x 2N samples, coils ~ U{4..32},
     ellipse phantoms, polynomial maps, 20 plain-CG iterations each, lambda
     0.01, Toeplitz. One step = all reconstructions, one graph launch (the
     problems run as independent child graphs); the baseline is a loop of
     single solves on the same GPU. Gridding bins from the autotuner. The
-    batch's inputs (several GB) exceed L2."""
+    batch's inputs (several GB) exceed L2.
+
+    With several ranks every rank draws the same problem list and takes the
+    share that the cost-model split gives it (no exchange while solving);
+    the time is the slowest rank's and the rate is all problems over it
+    (strong scaling: the total work is fixed)."""
     import torch
+    import torch.distributed as dist
     from bart_b200.batch import BatchRecon, autotune_bins, uneven_problems
+    from bart_b200.dist import partition, problem_cost, reduce_max, reduce_sum
+    iters = 20
     t0 = time.time()
     probs = uneven_problems(nprob, seed)
     gen_s = time.time() - t0
+    costs = [problem_cost(p, iters) for p in probs]
+    shards = partition(costs, world)
+    loads = [sum(costs[i] for i in s) for s in shards]
+    Ns = [p["sens"].shape[0] for p in probs]
+    probs = [probs[i] for i in shards[rank]]
     table, detail = autotune_bins(dev, reps=2)
     t0 = time.time()
-    br = BatchRecon(probs, dev, maxiter=20, bins=table)
+    br = BatchRecon(probs, dev, maxiter=iters, bins=table)
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     br.build()
@@ -377,34 +390,43 @@ def run_batch(dev, steps, warmup, nprob=512, seed=4):
         br.run()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(0) as clk:
+    with ClockSampler(dev.index or 0) as clk:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
         e0.record()
         for _ in range(steps):
             br.run()
         e1.record()
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    xb = [x.clone() for x in br.img]
-    br.run_loop()
-    torch.cuda.synchronize()
-    e0.record()
-    br.run_loop()
-    e1.record()
-    torch.cuda.synchronize()
-    ms_loop = e0.elapsed_time(e1)
-    diff = max(float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) for a, b in zip(xb, br.img))
-    kernels = br.kernels()
+        if world > 1:
+            dist.barrier()
+    ms = reduce_max(e0.elapsed_time(e1) / steps, dev)
+    launches = int(reduce_sum(br.kernels() * steps, dev))
+    loop = None
+    diff = None
+    if world == 1:	# the loop of single solves on the same GPU, for comparison
+        xb = [x.clone() for x in br.img]
+        br.run_loop()
+        torch.cuda.synchronize()
+        e0.record()
+        br.run_loop()
+        e1.record()
+        torch.cuda.synchronize()
+        ms_loop = e0.elapsed_time(e1)
+        diff = max(float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) for a, b in zip(xb, br.img))
+        loop = {"ms": ms_loop, "recons_per_s": nprob / (ms_loop / 1e3), "batch_speedup": ms_loop / ms}
     br.free()
-    Ns = [p["sens"].shape[0] for p in probs]
     return {"metric": "batched uneven CG-SENSE recons/s (20 CG iterations each)", "value": nprob / (ms / 1e3),
-            "unit": "recons/s", "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": ms,
-            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "unit": "recons/s", "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"batch{nprob}_uneven_2d_i20", "problems": nprob, "N_range": [min(Ns), max(Ns)],
-                       "spokes": [16, 256], "coils": [4, 32], "iters": 20, "lambda": 0.01,
-                       "l2": "batch inputs (GBs) exceed L2"},
-            "loop_of_single_solves": {"ms": ms_loop, "recons_per_s": nprob / (ms_loop / 1e3),
-                                      "batch_speedup": ms_loop / ms},
-            "max_rel_diff_batch_vs_loop": diff, "gpu_launches": kernels * steps,
+                       "spokes": [16, 256], "coils": [4, 32], "iters": iters, "lambda": 0.01,
+                       "l2": "batch inputs (GBs) exceed L2",
+                       "split": "cost model C (G log G + M taps) iters, LPT" if world > 1 else "one GPU",
+                       "predicted_load_max_over_mean": max(loads) / (sum(loads) / world)},
+            "loop_of_single_solves": loop,
+            "max_rel_diff_batch_vs_loop": diff, "gpu_launches": launches,
             "autotuned_bins": table, "autotune_ms": detail, "gen_s": gen_s, "setup_s": setup_s,
             "clocks": clk.summary()}
 
@@ -546,8 +568,11 @@ def main():
         return
 
     if args.workload == "batch":
+        out = run_batch(dev, args.steps, args.warmup, rank=rank, world=world)
         if rank == 0:
-            print(json.dumps(run_batch(dev, args.steps, args.warmup)), flush=True)
+            print(json.dumps(out), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
         return
 
     from bart_b200.dist import aggregate_rate, rank_seed, reduce_max
