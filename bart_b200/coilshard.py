@@ -1,0 +1,126 @@
+"""CG-SENSE on one problem with its coils split over ranks (one per GPU).
+
+The SENSE normal operator is a sum over coils, A^H A = sum_c S_c^H F^H F S_c,
+so rank r holding coils [c0, c1) (their maps and k-space) computes its share
+of A^H A p with the library's own normal operator (a ``Pics`` model built on
+those coils) and one all-reduce (sum) of that image-sized vector per
+iteration completes it. The CG vectors x, r, p are image-sized and
+replicated: after the reduction every rank holds the same A^H A p, so the
+dot products need no further exchange. This is the reference's
+``--md-split-mpi-dims`` on the coil dim with ``mpi_reduce_zsum`` after each
+normal application (src/pics.c:245-251, src/num/mpi_ops.c:680-735), with
+the CG of src/iter/italgos.c:497-572.
+
+The right-hand side is reduced the same way (one all-reduce of A_r^H y_r)
+before the data scaling is estimated on it, so the scaling is the one the
+whole problem would get (src/sense/optcom.c:74-109).
+"""
+
+from __future__ import annotations
+
+
+def coil_range(coils: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous coils [c0, c1) of ``rank``; shares differ by at most one."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("coil_range: need 0 <= rank < world")
+    base, extra = divmod(int(coils), int(world))
+    c0 = rank * base + min(rank, extra)
+    return c0, c0 + base + (1 if rank < extra else 0)
+
+
+def scaling_from_adjoint(adj) -> float:
+    """Data scaling of ``pics`` from the adjoint image A^H y
+    (estimate_scaling_norm, src/sense/optcom.c:74-109): the 90th percentile
+    of the magnitudes, or their maximum when the tail above it is longer
+    than twice the median-to-p90 gap; 1 when it comes out zero."""
+    import torch
+    mag = torch.sort(adj.reshape(-1).abs().to(torch.float32)).values
+    n = mag.numel()
+    median, p90, mx = (float(mag[i]) for i in (n // 2, int(n * 0.9), n - 1))
+    s = p90 if (mx - p90) < 2 * (p90 - median) else mx
+    return s if s != 0.0 else 1.0
+
+
+def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, reduce=None):
+    """CG from zero on (sum over ranks of normal_local + lam I) x = b.
+
+    ``normal_local(p)`` returns this rank's share of A^H A p; ``reduce(t)``
+    sums a tensor over the ranks in place (None: one rank). ``b`` is the
+    already-reduced right-hand side, the same on every rank. One reduction
+    per iteration; the dots are float64 and local (the vectors are
+    replicated). Stops after ``maxiter`` iterations or when
+    ||r|| <= tol ||b|| (tol > 0 reads the residual on the host each
+    iteration). Returns (x, iterations run)."""
+    import torch
+    x = torch.zeros_like(b)
+    r = b.clone()
+    p = r.clone()
+
+    def dot(u, v):
+        return torch.sum((u.conj() * v).real.to(torch.float64))
+
+    rsold = dot(r, r)
+    eps2 = (tol ** 2) * float(rsold) if tol > 0 else 0.0
+    if float(rsold) == 0.0:
+        return x, 0
+    it = 0
+    for it in range(1, maxiter + 1):
+        q = normal_local(p)
+        if reduce is not None:
+            reduce(q)
+        q = q + lam * p
+        pq = dot(p, q)
+        alpha = (rsold / pq).to(torch.float32)
+        x = x + alpha * p
+        r = r - alpha * q
+        rsnew = dot(r, r)
+        beta = (rsnew / rsold).to(torch.float32)
+        rsold = rsnew
+        if tol > 0 and float(rsnew) <= eps2:
+            break
+        p = beta * p + r
+    return x, it
+
+
+def allreduce_sum(t) -> None:
+    """In-place sum over the process group of a complex or real tensor."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return
+    dist.all_reduce(torch.view_as_real(t) if t.is_complex() else t, op=dist.ReduceOp.SUM)
+
+
+class CoilShardedPics:
+    """``pics -l2 -r lam -i iters -t`` on one problem whose coils are split
+    over the ranks of the process group: this rank's ``traj``, its coils'
+    ``sens`` (X, Y, Z, C_r) and ``ksp`` (1, R, S, C_r) as CUDA tensors or
+    arrays. ``run`` returns the image on every rank."""
+
+    def __init__(self, traj, sens_local, ksp_dims, lam=0.01, maxiter=30, tol=0.0, scaling=0.0,
+                 rescale=False, toeplitz=True, traj_dims=None, sens_dims=None):
+        from .pics import Pics, PicsConf
+        self.lam, self.maxiter, self.tol = float(lam), int(maxiter), float(tol)
+        self.scaling, self.rescale = float(scaling), bool(rescale)
+        # scaling 1: rhs() returns this rank's A_r^H y unscaled; the scale is
+        # estimated on the reduced sum
+        conf = PicsConf(lam=lam, maxiter=maxiter, scaling=1.0, toeplitz=toeplitz)
+        self.model = Pics(traj, sens_local, ksp_dims=list(ksp_dims), conf=conf, traj_dims=traj_dims,
+                          sens_dims=sens_dims)
+        self.iters = 0
+        self.scale = None
+
+    def run(self, ksp_local):
+        import torch
+        b = self.model.rhs(ksp_local)
+        if not torch.is_tensor(b):
+            raise TypeError("CoilShardedPics.run: give CUDA tensors (k-space on this rank's device)")
+        allreduce_sum(b)
+        scale = self.scaling if self.scaling != 0.0 else scaling_from_adjoint(b)
+        b = b / scale
+        x, self.iters = sharded_cg(self.model.normal, b, self.lam, self.maxiter, self.tol, allreduce_sum)
+        self.scale = scale
+        return x * scale if self.rescale else x
+
+    def free(self):
+        self.model.free()
