@@ -56,3 +56,30 @@ def test_pics_cli_options_parse(tmp_path):
     assert (a.precond, a.tol) == (3, 1e-4)
     with pytest.raises(SystemExit):
         cli.parse_pics(["--precond", "3", "--no-toeplitz", "-t", d + "/t", d + "/k", d + "/s", d + "/o"])
+
+
+def test_pics_cli_single_problem_runs_on_rank_0_only(tmp_path, monkeypatch):
+    """Under torchrun without -l/-p there is one problem: ranks other than 0
+    return at once, write nothing and touch no GPU."""
+    from bart_b200.cfl import writecfl
+    d = str(tmp_path)
+    for name in ("t", "k", "s"):
+        writecfl(d + "/" + name, np.zeros((2, 2), dtype=np.complex64))
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    monkeypatch.setenv("RANK", "1")
+    assert 0 == cli.main(["pics", "-r", "0.01", "-t", d + "/t", d + "/k", d + "/s", d + "/o"])
+    import os
+    assert not os.path.exists(d + "/o.cfl")
+
+
+def test_loop_split_follows_the_cost_model():
+    """The slices a rank of the -l loop takes: the cost-model split of the
+    loop indices, disjoint over ranks, all of them together."""
+    from bart_b200.dist import partition, problem_cost
+    sizes = [64, 64, 128, 256, 64, 32]
+    probs = [{"sens": np.zeros((n, n, 1, 4), np.complex64), "ksp": np.zeros((1, 2 * n, 32, 4), np.complex64)}
+             for n in sizes]
+    costs = [problem_cost(p, 10) for p in probs]
+    shards = partition(costs, 2)
+    assert 3 in shards[0] and 2 in shards[1]      # the two largest on different ranks
+    assert sorted(shards[0] + shards[1]) == list(range(len(sizes)))
