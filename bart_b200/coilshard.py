@@ -47,7 +47,7 @@ def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, redu
     ``normal_local(p)`` returns this rank's share of A^H A p; ``reduce(t)``
     sums a tensor over the ranks in place (None: one rank). ``b`` is the
     already-reduced right-hand side, the same on every rank. One reduction
-    per iteration; the dots are float64 and local (the vectors are
+    per iteration; the dots sum in float64 and are local (the vectors are
     replicated). Stops after ``maxiter`` iterations or when
     ||r|| <= tol ||b|| (tol > 0 reads the residual on the host each
     iteration). Returns (x, iterations run)."""
@@ -70,11 +70,14 @@ def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, redu
             reduce(q)
         q = q + lam * p
         pq = dot(p, q)
-        alpha = (rsold / pq).to(torch.float32)
+        # where the reference stops (<p, A p> = 0: r reached exactly zero),
+        # alpha and beta are 0 here, so x and r stay as they are without a
+        # host read of the scalars
+        alpha = torch.where(pq != 0, rsold / pq, torch.zeros_like(pq)).to(torch.float32)
         x = x + alpha * p
         r = r - alpha * q
         rsnew = dot(r, r)
-        beta = (rsnew / rsold).to(torch.float32)
+        beta = torch.where(rsold != 0, rsnew / rsold, torch.zeros_like(rsold)).to(torch.float32)
         rsold = rsnew
         if tol > 0 and float(rsnew) <= eps2:
             break
@@ -94,8 +97,9 @@ def allreduce_sum(t) -> None:
 class CoilShardedPics:
     """``pics -l2 -r lam -i iters -t`` on one problem whose coils are split
     over the ranks of the process group: this rank's ``traj``, its coils'
-    ``sens`` (X, Y, Z, C_r) and ``ksp`` (1, R, S, C_r) as CUDA tensors or
-    arrays. ``run`` returns the image on every rank."""
+    ``sens`` (X, Y, Z, C_r) and ``ksp`` (1, R, S, C_r), the k-space as a
+    CUDA tensor on this rank's device. ``run`` returns the image (a flat
+    complex64 CUDA tensor) on every rank."""
 
     def __init__(self, traj, sens_local, ksp_dims, lam=0.01, maxiter=30, tol=0.0, scaling=0.0,
                  rescale=False, toeplitz=True, traj_dims=None, sens_dims=None):

@@ -104,3 +104,16 @@ def test_two_ranks_match_reference_and_one_rank():
         # and beta, as the reference rounds them, 30 unconverged iterations
         # stay within 1.3e-4 of it (the float64 oracle drifts to 1e-2)
         assert rel(xs, g["x30"].reshape(xs.shape, order="F")) < 5e-4
+
+
+def test_exact_convergence_keeps_the_solution():
+    """A normal operator that CG solves exactly in one step (a multiple of
+    the identity): later iterations keep x (the reference stops at
+    <p, A p> = 0) instead of dividing by zero."""
+    import torch
+    from bart_b200.coilshard import sharded_cg
+    b = torch.tensor([1.0 + 2.0j, -0.5j, 3.0], dtype=torch.complex128)
+    x, it = sharded_cg(lambda p: 3.0 * p, b, 1.0, 5)
+    assert it == 5
+    assert torch.allclose(x, b / 4.0)
+    assert torch.isfinite(torch.view_as_real(x)).all()
