@@ -121,7 +121,7 @@ class ClockSampler:
 
 
 def nufft_throughput(dev, steps=50, warmup=5):
-    """NUFFT GB/s on the 2D single-coil workload (BASELINE config 1): 256^2
+    """NUFFT GB/s on the 2D single-coil workload: 256^2
     i.i.d. complex Gaussian image, 402 golden-angle spokes x 512 samples,
     os 2, width 6. One step = forward + adjoint on device-resident data with
     the plan reused; bytes = compulsory I/O of both directions (image, k-space,
@@ -186,7 +186,7 @@ def timed_steps(step, steps, flush, stream):
 
 
 def run_nufft3d(dev, steps, warmup, spokes=20000):
-    """3D radial kooshball NUFFT (BASELINE config 3): 128^3 image, 8 coils,
+    """3D radial kooshball NUFFT: 128^3 image, 8 coils,
     20000 spokes x 256 samples on 3D golden means (5.12 M samples per coil).
     One step = forward + adjoint of all 8 coil images, device-resident, plan
     reused. Also the time per kernel class (CUDA events per launch), the
@@ -355,7 +355,7 @@ def fft_vs_cufft(dev, traj, sens, reps=50):
 
 
 def run_batch(dev, steps, warmup, nprob=512, seed=4, rank=0, world=1):
-    """Batched uneven 2D reconstructions (BASELINE config 4): nprob problems,
+    """Batched uneven 2D reconstructions: nprob problems,
     N ~ U{64..320} even, spokes ~ U{16..256} x 2N samples, coils ~ U{4..32},
     ellipse phantoms, polynomial maps, 20 plain-CG iterations each, lambda
     0.01, Toeplitz. One step = all reconstructions, one graph launch (the
