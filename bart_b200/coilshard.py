@@ -41,7 +41,7 @@ def scaling_from_adjoint(adj) -> float:
     return s if s != 0.0 else 1.0
 
 
-def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, reduce=None):
+def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, reduce=None, precond=None):
     """CG from zero on (sum over ranks of normal_local + lam I) x = b.
 
     ``normal_local(p)`` returns this rank's share of A^H A p; ``reduce(t)``
@@ -50,18 +50,34 @@ def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, redu
     per iteration; the dots sum in float64 and are local (the vectors are
     replicated). Stops after ``maxiter`` iterations or when
     ||r|| <= tol ||b|| (tol > 0 reads the residual on the host each
-    iteration). Returns (x, iterations run)."""
+    iteration). Returns (x, iterations run).
+
+    Without ``precond`` this is the reference's CG, alpha and beta rounded
+    to float32 as it stores them. With ``precond(r)`` (the same operator on
+    every rank, e.g. the padded-circulant one, which depends only on the
+    trajectory's PSF and lambda) it is preconditioned CG with float64
+    scalars, the library's precond-3 solve."""
     import torch
     x = torch.zeros_like(b)
     r = b.clone()
-    p = r.clone()
+    z = precond(r) if precond is not None else r
+    p = z.clone()
+    f32 = precond is None
 
     def dot(u, v):
         return torch.sum((u.conj() * v).real.to(torch.float64))
 
-    rsold = dot(r, r)
-    eps2 = (tol ** 2) * float(rsold) if tol > 0 else 0.0
-    if float(rsold) == 0.0:
+    def ratio(num, den):
+        # where the reference stops (a zero denominator: r reached exactly
+        # zero) the ratio is 0, so x and r stay as they are without a host
+        # read of the scalars
+        q = torch.where(den != 0, num / den, torch.zeros_like(den))
+        return q.to(torch.float32) if f32 else q
+
+    rr = dot(r, r)
+    rz = rr if precond is None else dot(r, z)
+    eps2 = (tol ** 2) * float(rr) if tol > 0 else 0.0
+    if float(rr) == 0.0:
         return x, 0
     it = 0
     for it in range(1, maxiter + 1):
@@ -69,19 +85,22 @@ def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, redu
         if reduce is not None:
             reduce(q)
         q = q + lam * p
-        pq = dot(p, q)
-        # where the reference stops (<p, A p> = 0: r reached exactly zero),
-        # alpha and beta are 0 here, so x and r stay as they are without a
-        # host read of the scalars
-        alpha = torch.where(pq != 0, rsold / pq, torch.zeros_like(pq)).to(torch.float32)
+        alpha = ratio(rz, dot(p, q))
         x = x + alpha * p
         r = r - alpha * q
-        rsnew = dot(r, r)
-        beta = torch.where(rsold != 0, rsnew / rsold, torch.zeros_like(rsold)).to(torch.float32)
-        rsold = rsnew
-        if tol > 0 and float(rsnew) <= eps2:
+        if precond is None:
+            rz_new = dot(r, r)
+            rr = rz_new
+        else:
+            if tol > 0:
+                rr = dot(r, r)
+            z = precond(r)
+            rz_new = dot(r, z)
+        beta = ratio(rz_new, rz)
+        rz = rz_new
+        if tol > 0 and float(rr) <= eps2:
             break
-        p = beta * p + r
+        p = beta * p + (r if precond is None else z)
     return x, it
 
 
@@ -102,13 +121,17 @@ class CoilShardedPics:
     complex64 CUDA tensor) on every rank."""
 
     def __init__(self, traj, sens_local, ksp_dims, lam=0.01, maxiter=30, tol=0.0, scaling=0.0,
-                 rescale=False, toeplitz=True, traj_dims=None, sens_dims=None):
+                 rescale=False, toeplitz=True, traj_dims=None, sens_dims=None, precond=0):
         from .pics import Pics, PicsConf
+        if precond not in (0, 3) or (precond == 3 and not toeplitz):
+            raise ValueError("CoilShardedPics: precond 0 (CG) or 3 (padded-circulant PCG, Toeplitz only)")
         self.lam, self.maxiter, self.tol = float(lam), int(maxiter), float(tol)
-        self.scaling, self.rescale = float(scaling), bool(rescale)
+        self.scaling, self.rescale, self.precond = float(scaling), bool(rescale), int(precond)
         # scaling 1: rhs() returns this rank's A_r^H y unscaled; the scale is
-        # estimated on the reduced sum
-        conf = PicsConf(lam=lam, maxiter=maxiter, scaling=1.0, toeplitz=toeplitz)
+        # estimated on the reduced sum. The padded-circulant preconditioner
+        # depends only on the trajectory and lambda, so every rank's model
+        # applies the same one.
+        conf = PicsConf(lam=lam, maxiter=maxiter, scaling=1.0, toeplitz=toeplitz, precond=precond)
         self.model = Pics(traj, sens_local, ksp_dims=list(ksp_dims), conf=conf, traj_dims=traj_dims,
                           sens_dims=sens_dims)
         self.iters = 0
@@ -122,7 +145,8 @@ class CoilShardedPics:
         allreduce_sum(b)
         scale = self.scaling if self.scaling != 0.0 else scaling_from_adjoint(b)
         b = b / scale
-        x, self.iters = sharded_cg(self.model.normal, b, self.lam, self.maxiter, self.tol, allreduce_sum)
+        x, self.iters = sharded_cg(self.model.normal, b, self.lam, self.maxiter, self.tol, allreduce_sum,
+                                   precond=self.model.precond if self.precond else None)
         self.scale = scale
         return x * scale if self.rescale else x
 

@@ -105,7 +105,7 @@ class Pics:
         return out
 
     def precond(self, r, out=None):
-        """z = M(r) with the model's preconditioner (precond 1 or 2)."""
+        """z = M(r) with the model's preconditioner (precond 1, 2 or 3)."""
         n = int(np.prod(self.img_dims))
         if out is None:
             out = _alloc_like(r, self.img_dims)

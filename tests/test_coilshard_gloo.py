@@ -59,6 +59,26 @@ def _solve(name, rank, world, maxiter, scaling):
     return x.numpy(), scale, it
 
 
+def _solve_pcg(name, rank, world, tol=1e-4):
+    """PCG with the padded-circulant preconditioner (the trajectory's PSF and
+    lambda only, so the same operator on every rank)."""
+    import torch
+    from bart_b200.coilshard import allreduce_sum, coil_range, sharded_cg
+    from oracle import nufft_oracle as orc
+    g = golden(name)
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    C = g["sens"].shape[3]
+    y = g["ksp"].reshape(-1, C, order="F").astype(np.complex128)
+    c0, c1 = coil_range(C, rank, world)
+    A = orc.SenseOracle(traj, g["sens"][..., c0:c1])
+    M = orc.padded_precond(A.nufft, 0.01)
+    b = torch.from_numpy(A.adjoint(y[:, c0:c1]))
+    allreduce_sum(b)
+    x, it = sharded_cg(lambda p: torch.from_numpy(A.normal(p.numpy())), b, 0.01, 100, tol, allreduce_sum,
+                       precond=lambda r: torch.from_numpy(M(r.numpy())))
+    return x.numpy(), b.numpy(), it
+
+
 def _worker(rank, world, port, q):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -69,6 +89,7 @@ def _worker(rank, world, port, q):
         for name in ("pics2d_n64_c4", "pics2d_n48_c3"):	# 2 + 2 and 2 + 1 coils
             out[name, 5] = _solve(name, rank, world, 5, 1.0)
             out[name, 30] = _solve(name, rank, world, 30, 0.0)
+            out[name, "pcg"] = _solve_pcg(name, rank, world)
         q.put((rank, out))
     finally:
         dist.destroy_process_group()
@@ -104,6 +125,13 @@ def test_two_ranks_match_reference_and_one_rank():
         # and beta, as the reference rounds them, 30 unconverged iterations
         # stay within 1.3e-4 of it (the float64 oracle drifts to 1e-2)
         assert rel(xs, g["x30"].reshape(xs.shape, order="F")) < 5e-4
+        # PCG to 1e-4: the oracle's PCG on all coils, iteration for iteration
+        xp, b, itp = res[0][name, "pcg"]
+        A = orc.SenseOracle(traj, g["sens"])
+        xo, ito = orc.pcg(A.normal, b, 0.01, orc.padded_precond(A.nufft, 0.01), tol=1e-4, maxiter=100)
+        assert itp == ito < 100
+        assert rel(xp, xo) < 1e-9
+        assert np.array_equal(xp, res[1][name, "pcg"][0])
 
 
 def test_exact_convergence_keeps_the_solution():
@@ -117,3 +145,12 @@ def test_exact_convergence_keeps_the_solution():
     assert it == 5
     assert torch.allclose(x, b / 4.0)
     assert torch.isfinite(torch.view_as_real(x)).all()
+
+
+def test_sharded_model_rejects_other_preconditioners():
+    """The sharded solve runs CG or the padded-circulant PCG (Toeplitz); the
+    flexible-CG preconditioners are refused before any device work."""
+    from bart_b200.coilshard import CoilShardedPics
+    for kw in (dict(precond=1), dict(precond=2), dict(precond=3, toeplitz=False)):
+        with pytest.raises(ValueError):
+            CoilShardedPics(None, None, [1, 2, 2, 1], **kw)
