@@ -35,6 +35,7 @@ def test_scaling_rule_matches_the_oracle():
         a.flat[7] *= tail
         want = orc.estimate_scaling_norm(a)
         assert scaling_from_adjoint(torch.from_numpy(a)) == pytest.approx(want, rel=1e-6)
+    assert scaling_from_adjoint(torch.zeros(16, dtype=torch.complex64)) == 1.0	# as pics: a zero scale is 1
 
 
 def _solve(name, rank, world, maxiter, scaling):
