@@ -25,14 +25,16 @@ from .pics import Pics, PicsConf
 from .problems import cgsense_problem
 
 
-def uneven_problems(n, seed, sizes=(64, 320), spokes=(16, 256), coils=(4, 32), snr_db=40.0):
-    """n problems: N ~ U{even sizes}, spokes ~ U, 2N samples per spoke, coils ~ U."""
+def uneven_problems(n, seed, sizes=(64, 320), spokes=(16, 256), coils=(4, 32), snr_db=40.0, forward=None):
+    """n problems: N ~ U{even sizes}, spokes ~ U, 2N samples per spoke, coils ~ U.
+    The first k problems of any n are the same (one random stream, drawn in
+    order); ``forward`` as in problems.simulate_ksp."""
     rng = np.random.default_rng(seed)
     evens = np.arange(sizes[0], sizes[1] + 1, 2)
     out = []
     for _ in range(n):
         N = int(rng.choice(evens))
-        out.append(cgsense_problem(rng, N=N, coils=coils, spokes=spokes, snr_db=snr_db))
+        out.append(cgsense_problem(rng, N=N, coils=coils, spokes=spokes, snr_db=snr_db, forward=forward))
     return out
 
 

@@ -354,7 +354,7 @@ def fft_vs_cufft(dev, traj, sens, reps=50):
     return res
 
 
-def run_batch(dev, steps, warmup, nprob=512, seed=4, rank=0, world=1):
+def run_batch(dev, steps, warmup, nprob=512, seed=4, rank=0, world=1, cpu_base=True):
     """Batched uneven 2D reconstructions: nprob problems,
     N ~ U{64..320} even, spokes ~ U{16..256} x 2N samples, coils ~ U{4..32},
     ellipse phantoms, polynomial maps, 20 plain-CG iterations each, lambda
@@ -428,7 +428,8 @@ def run_batch(dev, steps, warmup, nprob=512, seed=4, rank=0, world=1):
             "loop_of_single_solves": loop,
             "max_rel_diff_batch_vs_loop": diff, "gpu_launches": launches,
             "autotuned_bins": table, "autotune_ms": detail, "gen_s": gen_s, "setup_s": setup_s,
-            "clocks": clk.summary()}
+            "clocks": clk.summary(),
+            "cpu_baseline": batch_cpu_baseline() if (cpu_base and rank == 0 and world == 1) else None}
 
 
 def reference_pics_seconds(traj, sens, ksp, iters=REF_ITERS_TO_TOL, threads=None, out=None):
@@ -474,9 +475,87 @@ def cpu_baseline(traj, sens, ksp, iters):
             "sample": f"1 full recon of {iters} CG iterations with the NumPy oracle (float64)"}
 
 
+def oracle_forward(traj, cim, kd):
+    """Noiseless SENSE k-space on the host (the oracle's NUFFT), for the
+    reference arm, which runs no GPU code."""
+    from oracle import nufft_oracle as orc
+    op = orc.NufftOracle(traj.real.reshape(3, -1, order="F"), cim.shape[:3])
+    return op.forward(cim).reshape(kd, order="F")
+
+
+BATCH_REF_SAMPLE = 6	# problems of the 512-problem batch the reference solves per step
+
+
+def batch_reference_sample(k=BATCH_REF_SAMPLE, seed=4):
+    """The first k problems of the uneven batch (the same random stream as
+    the batch), k-space from the oracle's NUFFT on the host."""
+    from bart_b200.batch import uneven_problems
+    return uneven_problems(k, seed, forward=oracle_forward)
+
+
+def batch_reference_seconds(probs, iters=20):
+    """Wall time of the reference's CPU pics -i20 on ``probs``, one after
+    another as its slice loop runs them; (seconds, kind, sample)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "bin", "pics")
+    t = 0.0
+    for p in probs:
+        if os.path.exists(exe):
+            t += reference_pics_seconds(p["traj"], p["sens"], p["ksp"], iters=iters)
+        else:
+            from oracle import nufft_oracle as orc
+            C = p["sens"].shape[3]
+            t0 = time.perf_counter()
+            orc.pics_l2(p["traj"].real.reshape(3, -1, order="F"), p["ksp"].reshape(-1, C, order="F"), p["sens"],
+                        lam=LAM, maxiter=iters)
+            t += time.perf_counter() - t0
+    Ns = [p["sens"].shape[0] for p in probs]
+    Cs = [p["sens"].shape[3] for p in probs]
+    kind = "reference" if os.path.exists(exe) else "port"
+    sample = (f"first {len(probs)} of the 512 uneven problems (N {Ns}, coils {Cs}), pics -l2 -r{LAM} "
+              f"-i{iters} -t each, "
+              + ("the reference's CPU pics (OpenMP), wall incl. .cfl I/O" if kind == "reference"
+                 else "the NumPy oracle (float64, 1 core)"))
+    return t, kind, sample
+
+
+def batch_cpu_baseline():
+    """cpu_baseline of the batch line: the reference on the bounded sample."""
+    probs = batch_reference_sample()
+    dt, kind, sample = batch_reference_seconds(probs)
+    return {"value": len(probs) / dt, "unit": "recons/s", "cores": os.cpu_count() if kind == "reference" else 1,
+            "kind": kind, "sample": sample}
+
+
+def run_reference_batch(args):
+    """--impl reference --workload batch: recons/s of the reference's CPU pics
+    over a bounded sample of the uneven batch."""
+    probs = batch_reference_sample()
+    times = []
+    for i in range(args.warmup + args.steps):
+        dt, kind, sample = batch_reference_seconds(probs)
+        if i >= args.warmup:
+            times.append(dt)
+    tot = sum(times)
+    value = len(probs) * len(times) / tot
+    cores = os.cpu_count() if kind == "reference" else 1
+    print(json.dumps({"metric": "batched uneven CG-SENSE recons/s (20 CG iterations each)", "impl": "reference",
+                      "value": value, "unit": "recons/s", "n_gpus": 0, "steps": args.steps,
+                      "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True,
+                      "scaling": "strong", "dtype": "f32", "data": "synthetic",
+                      "config": {"workload": "batch512_uneven_2d_i20", "problems": 512, "iters": 20,
+                                 "lambda": LAM, "sampled_problems": len(probs)},
+                      "cpu_baseline": {"value": value, "unit": "recons/s", "cores": cores, "kind": kind,
+                                       "sample": sample},
+                      "e2e": {"value": value, "unit": "recons/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU path on the host cores."""
     if rank != 0:
+        return
+    if args.workload == "batch":
+        run_reference_batch(args)
         return
     traj, truth, sens, rng = make_problem(1000)
     # k-space from the oracle's forward model (CPU; this arm uses no GPU code)
@@ -568,7 +647,7 @@ def main():
         return
 
     if args.workload == "batch":
-        out = run_batch(dev, args.steps, args.warmup, rank=rank, world=world)
+        out = run_batch(dev, args.steps, args.warmup, rank=rank, world=world, cpu_base=not args.no_cpu_baseline)
         if rank == 0:
             print(json.dumps(out), flush=True)
         if world > 1:
