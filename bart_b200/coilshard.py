@@ -41,7 +41,8 @@ def scaling_from_adjoint(adj) -> float:
     return s if s != 0.0 else 1.0
 
 
-def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, reduce=None, precond=None):
+def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, reduce=None, precond=None,
+               f32_scalars: bool = False):
     """CG from zero on (sum over ranks of normal_local + lam I) x = b.
 
     ``normal_local(p)`` returns this rank's share of A^H A p; ``reduce(t)``
@@ -52,17 +53,19 @@ def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, redu
     ||r|| <= tol ||b|| (tol > 0 reads the residual on the host each
     iteration). Returns (x, iterations run).
 
-    Without ``precond`` this is the reference's CG, alpha and beta rounded
-    to float32 as it stores them. With ``precond(r)`` (the same operator on
-    every rank, e.g. the padded-circulant one, which depends only on the
-    trajectory's PSF and lambda) it is preconditioned CG with float64
-    scalars, the library's precond-3 solve."""
+    Without ``precond`` this is the reference's CG with float64 alpha and
+    beta, as the library's single-GPU CG keeps them; ``f32_scalars`` rounds
+    them to float32 as the reference stores them, which reproduces its
+    unconverged iterates more closely. With ``precond(r)`` (the same
+    operator on every rank, e.g. the padded-circulant one, which depends
+    only on the trajectory's PSF and lambda) it is preconditioned CG with
+    float64 scalars, the library's precond-3 solve."""
     import torch
     x = torch.zeros_like(b)
     r = b.clone()
     z = precond(r) if precond is not None else r
     p = z.clone()
-    f32 = precond is None
+    f32 = f32_scalars and precond is None
 
     def dot(u, v):
         return torch.sum((u.conj() * v).real.to(torch.float64))
