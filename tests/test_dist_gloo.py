@@ -117,3 +117,19 @@ def test_two_ranks_shard_and_gather_to_root():
     assert not set(mine0) & set(mine1)
     for i, (tag, idx, r) in got0.items():
         assert tag == "img" and idx == i and i in (mine0 if r == 0 else mine1)
+
+
+def test_gather_to_root_refuses_a_problem_from_two_ranks(monkeypatch):
+    """A split that gave one problem to two ranks is an error on the root,
+    not a silent overwrite (the gather itself is faked here)."""
+    import torch.distributed as dist
+    from bart_b200 import dist as bd
+    monkeypatch.setattr(bd, "world_rank", lambda: (0, 2))
+
+    def fake_gather(obj, parts, dst=0):
+        parts[0], parts[1] = obj, {1: "b", 2: "c"}
+
+    monkeypatch.setattr(dist, "gather_object", fake_gather)
+    assert bd.gather_to_root({0: "a"}) == {0: "a", 1: "b", 2: "c"}
+    with pytest.raises(RuntimeError):
+        bd.gather_to_root({2: "a"})
