@@ -92,6 +92,7 @@ def _worker(rank, world, port, q):
             out[name, 30] = _solve(name, rank, world, 30, 0.0)
             out[name, "30f32"] = _solve(name, rank, world, 30, 0.0, f32_scalars=True)
             out[name, "pcg"] = _solve_pcg(name, rank, world)
+        out["pics3d_n16_c2", 5] = _solve("pics3d_n16_c2", rank, world, 5, 1.0)	# 3D, 1 + 1 coils
         q.put((rank, out))
     finally:
         dist.destroy_process_group()
@@ -107,6 +108,9 @@ def test_two_ranks_match_reference_and_one_rank():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
+    g = golden("pics3d_n16_c2")
+    x3 = res[0]["pics3d_n16_c2", 5][0]
+    assert rel(x3, g["x5_w1"].reshape(x3.shape, order="F")) < 1e-5
     for name in ("pics2d_n64_c4", "pics2d_n48_c3"):
         g = golden(name)
         x0, _, it0 = res[0][name, 5]
