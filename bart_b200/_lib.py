@@ -25,7 +25,7 @@ class PicsConfC(ctypes.Structure):
     _fields_ = [("lambda_", ctypes.c_float), ("maxiter", ctypes.c_int), ("tol", ctypes.c_float),
                 ("scaling", ctypes.c_float), ("rescale", ctypes.c_int), ("toeplitz", ctypes.c_int),
                 ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int), ("bin", ctypes.c_int),
-                ("precond", ctypes.c_int)]
+                ("precond", ctypes.c_int), ("ref_scalars", ctypes.c_int)]
 
 
 _lib = None
@@ -88,6 +88,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         ctypes.POINTER(ctypes.c_double), vp, vp)
     sig("bnufft_precnet_backward", i, vp, vp, vp, ctypes.c_long, ctypes.c_long, ctypes.c_long, ctypes.c_float, vp, vp)
     sig("bnufft_precnet_free", None, vp)
+    sig("bnufft_calc_beta", ctypes.c_double, ctypes.c_float, ctypes.c_float)
+    sig("bnufft_kb_precompute", i, ctypes.c_double, i, fp)
+    sig("bnufft_rolloff_axis", i, ctypes.c_float, ctypes.c_float, ctypes.c_long, ctypes.POINTER(ctypes.c_double))
     sig("bnufft_last_error", ctypes.c_char_p)
     sig("bnufft_launch_count", ctypes.c_long)
     sig("bnufft_prof_start", i, ctypes.c_char_p)

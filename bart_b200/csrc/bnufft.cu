@@ -191,6 +191,33 @@ static double rolloff_axis(int d, int i, float os, float width, double beta, dou
 	return 1. / ftkb(beta, (double)p * (double)width, i0b) / (double)width;
 }
 
+// host-only views of the tables above (no device work), for checking them
+// against the reference's calc_beta / kb_precompute / rolloff
+extern "C" double bnufft_calc_beta(float os, float width) { return calc_beta(os, width); }
+
+extern "C" int bnufft_kb_precompute(double beta, int n, float* table)
+{
+	if ((n < 2) || !table)
+		return fail(BNUFFT_ERR_ARG, "kb_precompute: n >= 2 and a table are needed");
+
+	kb_precompute(beta, n, table);
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_rolloff_axis(float os, float width, long n, double* roll)
+{
+	if ((n < 1) || !roll)
+		return fail(BNUFFT_ERR_ARG, "rolloff: n >= 1 and an output are needed");
+
+	double beta = kernel_beta(os, width);
+	double i0b = bessel_i0(beta);
+
+	for (long i = 0; i < n; i++)
+		roll[i] = rolloff_axis((int)n, (int)i, os, width, beta, i0b);
+
+	return BNUFFT_OK;
+}
+
 // ----------------------------------------------------------------------------
 // per-device constant tables
 // ----------------------------------------------------------------------------
@@ -206,6 +233,16 @@ static std::map<int, DevTables> g_tabs;
 
 // lock-free lookup of tables already built: [device][log2 L]
 static std::atomic<const float2*> g_tw_fast[64][16];
+
+// exp(-2 pi i m / L), m = 0..L-1, in float64 then float32
+static void twiddles_host(int L, float2* h)
+{
+	for (int m = 0; m < L; m++) {
+
+		double a = -2. * M_PI * (double)m / (double)L;
+		h[m] = make_float2((float)cos(a), (float)sin(a));
+	}
+}
 
 static int get_twiddles(int L, const float2** out)
 {
@@ -238,13 +275,7 @@ static int get_twiddles(int L, const float2** out)
 	}
 
 	std::vector<float2> h(L);
-
-	for (int m = 0; m < L; m++) {
-
-		double a = -2. * M_PI * (double)m / (double)L;
-		h[m] = make_float2((float)cos(a), (float)sin(a));
-	}
-
+	twiddles_host(L, h.data());
 	float2* d = nullptr;
 	CUDA_TRY(cudaMalloc(&d, sizeof(float2) * L));
 	CUDA_TRY(cudaMemcpy(d, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
@@ -804,6 +835,23 @@ struct RollKey {
 
 static std::map<std::pair<int, RollKey>, std::pair<float*, float*>> g_roll;
 
+// separable roll-off of an N[0] x N[1] x N[2] image: ax[x] and
+// ayz[y + N[1] z] (the latter with the unitary 1/sqrt(npix) folded in)
+static void rolloff_host(const int N[3], float os, float width, float* ax, float* ayz)
+{
+	double beta = kernel_beta(os, width);
+	double i0b = bessel_i0(beta);
+	double sc = 1. / sqrt((double)N[0] * (double)N[1] * (double)N[2]);
+
+	for (int x = 0; x < N[0]; x++)
+		ax[x] = (float)rolloff_axis(N[0], x, os, width, beta, i0b);
+
+	for (int z = 0; z < N[2]; z++)
+		for (int y = 0; y < N[1]; y++)
+			ayz[y + (size_t)N[1] * z] = (float)(rolloff_axis(N[1], y, os, width, beta, i0b)
+						* rolloff_axis(N[2], z, os, width, beta, i0b) * sc);
+}
+
 static int init_rolloff(OpCtx& op, cudaStream_t st)
 {
 	const Geom& g = op.g;
@@ -828,20 +876,9 @@ static int init_rolloff(OpCtx& op, cudaStream_t st)
 		return BNUFFT_OK;
 	}
 
-	double beta = kernel_beta(g.os, g.width);
-	double i0b = bessel_i0(beta);
 	std::vector<float> ax(g.N[0]);
 	std::vector<float> ayz((size_t)g.N[1] * g.N[2]);
-	double sc = 1. / sqrt((double)g.npix);
-
-	for (int x = 0; x < g.N[0]; x++)
-		ax[x] = (float)rolloff_axis(g.N[0], x, g.os, g.width, beta, i0b);
-
-	for (int z = 0; z < g.N[2]; z++)
-		for (int y = 0; y < g.N[1]; y++)
-			ayz[y + (size_t)g.N[1] * z] = (float)(rolloff_axis(g.N[1], y, g.os, g.width, beta, i0b)
-						* rolloff_axis(g.N[2], z, g.os, g.width, beta, i0b) * sc);
-
+	rolloff_host(g.N, g.os, g.width, ax.data(), ayz.data());
 	float* dax = nullptr;
 	float* dayz = nullptr;
 	CUDA_TRY(cudaMalloc(&dax, sizeof(float) * ax.size()));
@@ -2219,7 +2256,7 @@ extern "C" int bnufft_nufft_inverse(bnufft_plan_t p, void* img, const void* ksp,
 
 	k_cg_init<<<nb, RED_THREADS, 0, st>>>(x, r, pv, Ap, n, rsp);
 	LAUNCHED();
-	k_cg_start<<<1, RED_THREADS, 0, st>>>(sc, rsp, (int)nb, 0.f, maxiter);
+	k_cg_start<<<1, RED_THREADS, 0, st>>>(sc, rsp, (int)nb, 0.f, maxiter, 1);
 	LAUNCHED();
 
 	for (int it = 0; it < maxiter; it++) {
@@ -2831,6 +2868,7 @@ extern "C" void bnufft_pics_conf_defaults(struct bnufft_pics_conf* c)
 	c->deterministic = 0;
 	c->bin = 0;
 	c->precond = 0;
+	c->ref_scalars = 1;
 }
 
 // A^H A x (+ lam x), with optional per-block Re<x, out> partials
@@ -3590,7 +3628,8 @@ static int pics_solve(bnufft_pics_s* ps, const float2* ksp, float2* out, cudaStr
 	// CG from zero (conjgrad, src/iter/italgos.c:497-572)
 	k_cg_init<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, ps->pbuf[1], ps->b, ps->npix, ps->rs_part);
 	LAUNCHED();
-	k_cg_start<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->rs_part, ps->nparts, ps->conf.tol, ps->conf.maxiter);
+	k_cg_start<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->rs_part, ps->nparts, ps->conf.tol, ps->conf.maxiter,
+			(0 == ps->conf.precond) && ps->conf.ref_scalars);
 	LAUNCHED();
 
 	TRY(alloc_work(op.w, op.g, ps->C, st));
@@ -4046,28 +4085,34 @@ extern "C" long bnufft_launch_count(void) { return g_launches.load(); }
 //
 // The first call on a device does the set-up: it takes the array's device
 // address with cudaGetSymbolAddress (the array's name in host code is only a
-// host-side stand-in), fills the Kaiser-Bessel and twiddle tables and
-// synchronises the caller's stream once. Make that first call before any
-// stream capture.
+// host-side stand-in), copies in the Kaiser-Bessel, twiddle and roll-off
+// tables, built on the host by the same functions as a plan's (kb_precompute,
+// twiddles_host, rolloff_host), and synchronises the caller's stream once.
+// Make that first call before any stream capture. A cudaDeviceReset between
+// calls is not supported: it would drop the tables without this library
+// noticing.
 //
 // All calls share the one array and every call overwrites the regions it
-// uses (trajectory copy, row-transformed buffer, grid, roll-off tables), so
-// nothing needs clearing between calls; calls whose work overlaps on the GPU
-// (different streams, or another thread) race on the array and must be
-// serialised by the caller.
+// uses (trajectory copy, row-transformed buffer, grid); the tables are only
+// read. So nothing needs clearing between calls; calls whose work overlaps
+// on the GPU (different streams, or another thread) race on the array and
+// must be serialised by the caller.
 
 enum : long {
 
+	NA_MIN_N = 8,
 	NA_MAX_N = 256,
+	NA_NSIDES = 6,							// 8, 16, ..., 256
+	NA_ROLL_N = 512,						// floats per roll-off table set
 	NA_MAX_M = 262144,
 	NA_TRAJ_OFF = 0,						// float4[NA_MAX_M]
 	NA_T1_OFF = NA_TRAJ_OFF + 16L * NA_MAX_M,			// float2[2N x N]
 	NA_GRID_OFF = NA_T1_OFF + 8L * (2 * NA_MAX_N) * NA_MAX_N,	// float2[2N x 2N]
 	NA_TW_OFF = NA_GRID_OFF + 8L * (2 * NA_MAX_N) * (2 * NA_MAX_N),	// float2[1024]: L = 16..512 back to back
 	NA_KB_OFF = NA_TW_OFF + 8L * 1024,				// float[1024]
-	NA_AX_OFF = NA_KB_OFF + 4L * 1024,				// float[NA_MAX_N]
-	NA_AYZ_OFF = NA_AX_OFF + 4L * NA_MAX_N,				// float[NA_MAX_N]
-	NA_BYTES = NA_AYZ_OFF + 4L * NA_MAX_N,
+	NA_AX_OFF = NA_KB_OFF + 4L * 1024,				// float[NA_ROLL_N]: ax of X = 8..256 back to back
+	NA_AYZ_OFF = NA_AX_OFF + 4L * NA_ROLL_N,			// float[NA_NSIDES][NA_ROLL_N]: ayz of (X, Y)
+	NA_BYTES = NA_AYZ_OFF + 4L * NA_NSIDES * NA_ROLL_N,
 };
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
@@ -4078,66 +4123,18 @@ static unsigned char* g_na_base[64];
 // twiddle table of length L (power of two, 16..512) inside the scratch table block
 static long na_tw_offset(int L) { return L - 16; }
 
-__device__ static double na_bessel_i0(double x)
+// roll-off tables of an image side n (power of two, 8..256): ax at
+// na_roll_offset(X), ayz of (X, Y) in the table set of X at na_roll_offset(Y)
+static long na_roll_offset(long n) { return n - NA_MIN_N; }
+
+static int na_log2(long n)
 {
-	x = fabs(x);
-	double q = 0.25 * x * x, term = 1., sum = 1.;
+	int k = 0;
 
-	for (int k = 1; k < 500; k++) {
+	while ((1L << k) < n)
+		k++;
 
-		term *= q / ((double)k * (double)k);
-		sum += term;
-
-		if (term < 1e-18 * sum)
-			break;
-	}
-
-	return sum;
-}
-
-// Kaiser-Bessel table (kb_precompute, src/noncart/grid.c:86-97) and the
-// twiddle tables exp(-2 pi i m / L), L = 16..512, in float64 then float32
-__global__ static void k_na_tables(float2* tw, float* kb, double beta)
-{
-	double i0b = na_bessel_i0(beta);
-
-	for (int i = threadIdx.x; i <= KB_TABLE_N; i += blockDim.x) {
-
-		double x = (double)i / (double)(KB_TABLE_N - 1) / 2.;
-		kb[i] = (fabs(x) >= 0.5) ? 0.f : (float)(na_bessel_i0(beta * sqrt(1. - pow(2. * x, 2.))) / i0b);
-	}
-
-	for (int L = 16; L <= 512; L *= 2)
-		for (int m = threadIdx.x; m < L; m += blockDim.x) {
-
-			double a = -2. * M_PI * (double)m / (double)L;
-			tw[L - 16 + m] = make_float2((float)cos(a), (float)sin(a));
-		}
-}
-
-__device__ static double na_rolloff(int d, int i, double beta, double i0b)
-{
-	// rolloff() / pos() of src/noncart/grid.c:114-117, 522-533 for os = 2, width = 6
-	int od = 2 * d;
-	int oi = i + (od / 2 - d / 2);
-	float p = ((float)oi - (float)(od / 2)) / (float)od;
-	double x = (double)p * 6.;
-	double a = beta * beta - pow(M_PI * x, 2.);
-	double ft = (0. == a) ? 1. / i0b : ((a > 0) ? (sinh(sqrt(a)) / sqrt(a)) / i0b : (sin(sqrt(-a)) / sqrt(-a)) / i0b);
-	return 1. / ft / 6.;
-}
-
-// roll-off tables of an X x Y image: ax[x], ayz[y] (with 1/sqrt(X*Y))
-__global__ static void k_na_rolloff(float* ax, float* ayz, int X, int Y, double beta)
-{
-	double i0b = na_bessel_i0(beta);
-	double sc = 1. / sqrt((double)X * (double)Y);
-
-	for (int i = threadIdx.x; i < X; i += blockDim.x)
-		ax[i] = (float)na_rolloff(X, i, beta, i0b);
-
-	for (int i = threadIdx.x; i < Y; i += blockDim.x)
-		ayz[i] = (float)(na_rolloff(Y, i, beta, i0b) * sc);
+	return k;
 }
 
 template <int L>
@@ -4146,7 +4143,7 @@ static int na_rows(const float2* img, const float* ax, const float* ayz, int X, 
 {
 	constexpr int B = 16;
 	size_t smem = rows_smem(L, B);
-	CUDA_TRY(cudaFuncSetAttribute(k_rows_fwd<L, B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+	TRY(prep_kernel(k_rows_fwd<L, B, false>, smem));
 	k_rows_fwd<L, B, false><<<(unsigned)((Y + B - 1) / B), B * L / 8, smem, st>>>(img, nullptr, ax, ayz, X, Y, Y, out, tw, nullptr, Dft{L, nullptr, nullptr, nullptr});
 	LAUNCHED();
 	return BNUFFT_OK;
@@ -4157,7 +4154,7 @@ static int na_cols(const float2* t1, int G0, int Y, float2* grid, const float2* 
 {
 	constexpr int B = 16;
 	size_t smem = pass_smem(L, B);
-	CUDA_TRY(cudaFuncSetAttribute(k_cols<L, B, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+	TRY(prep_kernel(k_cols<L, B, 0, false>, smem));
 	dim3 grid_dim((unsigned)((G0 + B - 1) / B), 1);
 	k_cols<L, B, 0, false><<<grid_dim, B * L / 8, smem, st>>>(t1, G0, (long)G0 * Y, Y, 1, grid, G0, (long)G0 * L, L, 0,
 			G0, nullptr, 0, 1, 0, tw, nullptr, Dft{L, nullptr, nullptr, nullptr});
@@ -4197,10 +4194,29 @@ static int na_setup(unsigned char** base, cudaStream_t st)
 	if ((cudaSuccess != e) || (nullptr == p))
 		return fail(BNUFFT_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
 
+	// the tables a plan would build, on the host, into one host block that
+	// mirrors the scratch's table region [NA_TW_OFF, NA_BYTES)
+	std::vector<unsigned char> h(NA_BYTES - NA_TW_OFF, 0);
+	auto at = [&](long off) { return h.data() + (off - NA_TW_OFF); };	// scratch offset -> host block
+
+	for (int L = 16; L <= 512; L *= 2)
+		twiddles_host(L, (float2*)at(NA_TW_OFF) + na_tw_offset(L));
+
+	kb_precompute(kernel_beta(2.f, 6.f), KB_TABLE_N, (float*)at(NA_KB_OFF));
+
+	for (long X = NA_MIN_N; X <= NA_MAX_N; X *= 2)
+		for (long Y = NA_MIN_N; Y <= NA_MAX_N; Y *= 2) {
+
+			const int n[3] = { (int)X, (int)Y, 1 };
+			float* ayz = (float*)at(NA_AYZ_OFF) + NA_ROLL_N * (na_log2(X) - na_log2(NA_MIN_N)) + na_roll_offset(Y);
+			std::vector<float> ax(X);
+			rolloff_host(n, 2.f, 6.f, ax.data(), ayz);
+			std::memcpy((float*)at(NA_AX_OFF) + na_roll_offset(X), ax.data(), sizeof(float) * X);
+		}
+
 	unsigned char* b = (unsigned char*)p;
-	k_na_tables<<<1, 256, 0, st>>>((float2*)(b + NA_TW_OFF), (float*)(b + NA_KB_OFF), kernel_beta(2.f, 6.f));
-	LAUNCHED();
-	CUDA_TRY(cudaStreamSynchronize(st));	// tables ready before any other stream uses them
+	CUDA_TRY(cudaMemcpyAsync(b + NA_TW_OFF, h.data(), h.size(), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaStreamSynchronize(st));	// tables ready before any other stream uses them (and h is freed)
 	g_na_base[dev] = b;
 	*base = b;
 	return BNUFFT_OK;
@@ -4211,8 +4227,9 @@ extern "C" int bnufft_forward2d_noalloc(long X, long Y, long M, const void* traj
 	cudaStream_t st = S(stream);
 
 	for (long n : { X, Y })
-		if ((n < 8) || (n > NA_MAX_N) || (0 != (n & (n - 1))))
-			return fail(BNUFFT_ERR_ARG, "allocation-free NUFFT: image side %ld (powers of two 8..%ld)", n, (long)NA_MAX_N);
+		if ((n < NA_MIN_N) || (n > NA_MAX_N) || (0 != (n & (n - 1))))
+			return fail(BNUFFT_ERR_ARG, "allocation-free NUFFT: image side %ld (powers of two %ld..%ld)", n,
+					(long)NA_MIN_N, (long)NA_MAX_N);
 
 	if ((M < 1) || (M > NA_MAX_M))
 		return fail(BNUFFT_ERR_ARG, "allocation-free NUFFT: %ld samples (at most %ld)", M, (long)NA_MAX_M);
@@ -4228,13 +4245,11 @@ extern "C" int bnufft_forward2d_noalloc(long X, long Y, long M, const void* traj
 	float2* grid = (float2*)(base + NA_GRID_OFF);
 	const float2* tw = (const float2*)(base + NA_TW_OFF);
 	const float* kb = (const float*)(base + NA_KB_OFF);
-	float* ax = (float*)(base + NA_AX_OFF);
-	float* ayz = (float*)(base + NA_AYZ_OFF);
+	const float* ax = (const float*)(base + NA_AX_OFF) + na_roll_offset(X);
+	const float* ayz = (const float*)(base + NA_AYZ_OFF) + NA_ROLL_N * (na_log2(X) - na_log2(NA_MIN_N)) + na_roll_offset(Y);
 
 	const int G0 = (int)(2 * X), G1 = (int)(2 * Y);
 
-	k_na_rolloff<<<1, 256, 0, st>>>(ax, ayz, (int)X, (int)Y, kernel_beta(2.f, 6.f));
-	LAUNCHED();
 	k_traj_convert<<<vec_blocks(M), RED_THREADS, 0, st>>>(ntraj, (const float2*)traj, M, 1.f);
 	LAUNCHED();
 

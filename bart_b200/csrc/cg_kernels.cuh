@@ -128,18 +128,32 @@ __global__ void k_cg_init(float2* __restrict__ x, float2* __restrict__ r, float2
 		part[blockIdx.x] = s;
 }
 
-// rs[0] = ||b||^2 = b2, eps2 = (tol*||b||)^2, iters = 0, done = (b2 == 0)
-__global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float tol, int maxiter)
+// rs[0] = ||b||^2 = b2, eps2 = (tol*||b||)^2, iters = 0, done = (b2 == 0).
+// f32: the plain CG's scalars in float32 as the reference keeps them:
+// eps = float(||b||) * tol and eps2 = float(eps^2) (iter2_conjgrad,
+// src/iter/iter2.c:249-254; conjgrad, src/iter/italgos.c:518-523).
+__global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float tol, int maxiter, int f32)
 {
 	__shared__ double sh[32];
 	double b2 = sum_partials(part, nparts, sh);
 
 	if (0 == threadIdx.x) {
 
+		st->f32 = f32;
 		st->b2 = b2;
-		st->rs[0] = b2;
-		double eps = (double)tol * sqrt(b2);
-		st->eps2 = eps * eps;
+		st->rs[0] = cg_keep(st, b2);
+
+		if (f32) {
+
+			float eps = __fmul_rn((float)sqrt(b2), tol);
+			st->eps2 = (double)(float)((double)eps * (double)eps);
+
+		} else {
+
+			double eps = (double)tol * sqrt(b2);
+			st->eps2 = eps * eps;
+		}
+
 		st->iters = 0;
 		st->it = 0;
 		st->maxiter = maxiter;
@@ -171,7 +185,7 @@ __global__ void k_cg_step(float2* __restrict__ x, float2* __restrict__ r, const 
 
 	it = cg_iter(it, st);
 	const double3 sums = sum_partials3_d(pap_part, npap, pp_part, npp, nullptr, 0, sh);
-	double pAp = sums.x + (double)lam * sums.y;
+	double pAp = cg_keep(st, sums.x + (double)lam * sums.y);
 
 	if (0. == pAp) {
 
@@ -184,7 +198,7 @@ __global__ void k_cg_step(float2* __restrict__ x, float2* __restrict__ r, const 
 		return;
 	}
 
-	float a = (float)(st->rs[it & 1] / pAp);
+	float a = cg_ratio(st, st->rs[it & 1], pAp);
 	double acc = 0.;
 
 	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
@@ -226,13 +240,13 @@ __global__ void k_cg_dir(float2* __restrict__ p, const float2* __restrict__ r, l
 	if (st->done)
 		return;
 
-	double rs_new = sum_partials(rs_part, nrs, sh);
+	double rs_new = cg_keep(st, sum_partials(rs_part, nrs, sh));
 	double rs_old = st->rs[it & 1];
 	bool stop = (rs_new <= st->eps2);
 
 	if (!stop) {
 
-		float beta = (float)(rs_new / rs_old);
+		float beta = cg_ratio(st, rs_new, rs_old);
 
 		for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
 

@@ -15,7 +15,7 @@
 // sub-block, accumulates its samples' taps into a zeroed shared-memory tile
 // (bin plus HALO cells per side, a chunk of coils) with shared-memory atomics
 // and flushes touched cells with one global atomic each; on B200 it measured
-// slower for radial and kooshball data (profiles/gridding_scatter_variants.md).
+// slower for radial and kooshball data.
 //
 // Taps and weights are those of axis_taps (bit-identical to the reference's,
 // src/noncart/grid.c:403-465); only the cell index changes from the DFT-order

@@ -164,11 +164,27 @@ struct CgScalars {
 	float rinv;		// 1 / ||r|| (0 for r = 0)
 	float scale;		// data scaling used
 	float inv_scale;	// float(1 / scale)
+	int f32;		// plain CG keeps ||r||^2, p^H A p, alpha and beta in float32
 };
 
 // iteration index of a CG pass: the host's, or the device counter when the
 // loop runs inside a graph (it < 0)
 __device__ __forceinline__ int cg_iter(int it, const CgScalars* st) { return (it < 0) ? st->it : it; }
+
+// Plain-CG scalars in the reference's precision when st->f32 is set:
+// conjgrad (src/iter/italgos.c:518-554) sums its dot products in float64
+// but stores rsold, rsnew, pAp, alpha and beta as float, and divides in
+// float. cg_keep rounds a float64 sum as the reference stores it; cg_ratio
+// is alpha = rsold / pAp or beta = rsnew / rsold.
+__device__ __forceinline__ double cg_keep(const CgScalars* st, double v)
+{
+	return st->f32 ? (double)(float)v : v;
+}
+
+__device__ __forceinline__ float cg_ratio(const CgScalars* st, double num, double den)
+{
+	return st->f32 ? __fdiv_rn((float)num, (float)den) : (float)(num / den);
+}
 
 // three fixed-order float64 sums of partials in one block reduction, the
 // same values in every thread (sh: 3 doubles per warp)
@@ -253,7 +269,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 
 	if (it > 0) {
 
-		double rs = sum_partials_d(rs_part, nrs, red);
+		double rs = cg_keep(st, sum_partials_d(rs_part, nrs, red));
 		double rs_prev = st->rs[(it - 1) & 1];
 		bool stop = (rs <= st->eps2);
 
@@ -271,7 +287,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		if (stop)
 			return;
 
-		beta = (float)(rs / rs_prev);
+		beta = cg_ratio(st, rs, rs_prev);
 	}
 
 	for (int i = threadIdx.x; i < L; i += NT)

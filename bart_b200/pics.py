@@ -31,11 +31,12 @@ class PicsConf:
     deterministic: bool = False
     bin: int = 0              # gridding bin edge (0 = default); tuning only
     precond: int = 0          # 0 plain CG, 1 FCG + circulant, 2 FCG + circulant + learned, 3 FCG + padded circulant
+    ref_scalars: bool = True  # plain CG keeps its scalars in float32 as the reference's conjgrad does
 
     def c(self) -> _lib.PicsConfC:
         return _lib.PicsConfC(float(self.lam), int(self.maxiter), float(self.tol), float(self.scaling),
                               int(self.rescale), int(self.toeplitz), int(self.periodic), int(self.deterministic),
-                              int(self.bin), int(self.precond))
+                              int(self.bin), int(self.precond), int(self.ref_scalars))
 
 
 class Pics:

@@ -49,6 +49,9 @@ METRIC = ("CG-SENSE recons/s to 1e-4 rel. normal-equation residual "
           "(2D radial 256^2, 16 coils, 96 spokes x 512, lambda 0.01)")
 WORKLOAD = "cgsense2d_256_c16_s96_tol1e-4_toeplitz"
 DOMINANT = "cols_toeplitz"
+# the ncu summary of the dominant kernel on this workload; its table carries
+# the DRAM bytes (read + write) of one launch
+DOMINANT_PROFILE = os.path.join(ROOT, "profiles", "k_cols_toeplitz_512_cgsense2d.md")
 L2_FLUSH_BYTES = 512 << 20     # > 126 MB L2
 
 
@@ -62,8 +65,28 @@ def make_problem(seed: int):
     return traj, truth, sens, rng
 
 
+def workload_config():
+    """The workload both arms measure (the same dict in both JSON lines)."""
+    return {"workload": WORKLOAD, "image": N_IMG, "coils": COILS, "spokes": SPOKES, "samples": 512,
+            "tol": TOL, "lambda": LAM, "toeplitz": True}
+
+
+def inputs_record(traj, sens, ksp):
+    """Checksums of the inputs a step reconstructs: both arms print them, so
+    equal digests show the arms solved byte-identical problems."""
+    import hashlib
+
+    def h(a):
+        return hashlib.sha256(np.ascontiguousarray(np.asfortranarray(a).ravel(order="F")).tobytes()).hexdigest()[:16]
+    return {"traj_sha256": h(traj), "sens_sha256": h(sens), "ksp_sha256": h(ksp),
+            "ksp_generator": "the library's forward NUFFT (GPU) of the seeded phantom times the maps, "
+                             "plus seeded 40 dB noise, outside the timed region"}
+
+
 def simulate_ksp(traj, truth, sens, rng):
-    """k-space of the SENSE model on the GPU (NUFFT of truth * maps) + noise."""
+    """k-space of the SENSE model on the GPU (NUFFT of truth * maps) + noise.
+    Both arms of the bench simulate their input this way, so they read
+    byte-identical k-space."""
     from bart_b200.nufft import NufftConf, nufft_create2
     cim = (truth.reshape(N_IMG, N_IMG, 1, 1) * sens).astype(np.complex64)
     kd = [1, traj.shape[1], traj.shape[2], COILS]
@@ -558,12 +581,19 @@ def run_reference(args, rank, world):
         run_reference_batch(args)
         return
     traj, truth, sens, rng = make_problem(1000)
-    # k-space from the oracle's forward model (CPU; this arm uses no GPU code)
+    # the same input bytes as the other arm: its k-space simulation (the
+    # library's forward NUFFT on the GPU, outside the timed region); the timed
+    # path below is the reference's own pics alone
     from oracle import nufft_oracle as orc
     A = orc.SenseOracle(traj.real.reshape(3, -1, order="F"), sens)
-    from bart_b200 import synth
-    y = A.forward(truth.reshape(N_IMG, N_IMG, 1, 1))
-    ksp = synth.add_noise(y, SNR_DB, rng).reshape(1, traj.shape[1], traj.shape[2], COILS, order="F")
+    try:
+        ksp = simulate_ksp(traj, truth, sens, rng)
+        inputs = inputs_record(traj, sens, ksp)
+    except Exception as e:      # no usable GPU here: the oracle's forward model instead
+        y = A.forward(truth.reshape(N_IMG, N_IMG, 1, 1))
+        from bart_b200 import synth
+        ksp = synth.add_noise(y, SNR_DB, rng).reshape(1, traj.shape[1], traj.shape[2], COILS, order="F")
+        inputs = dict(inputs_record(traj, sens, ksp), ksp_generator=f"the oracle's forward model ({e})")
     kind = "reference" if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "bin", "pics")) else "port"
     outs = []
     run = (lambda: reference_pics_seconds(traj, sens, ksp, out=outs)) if kind == "reference" else \
@@ -585,14 +615,26 @@ def run_reference(args, rank, world):
             "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOAD, "image": N_IMG, "coils": COILS, "spokes": SPOKES, "samples": 512,
-                       "tol": TOL, "iters": REF_ITERS_TO_TOL, "lambda": LAM, "toeplitz": True},
+            "config": workload_config(),
+            "solver": {"method": "the reference's pics: plain CG", "iters": REF_ITERS_TO_TOL,
+                       "why": "pics has no tolerance option; this many iterations reach the 1e-4 residual"},
+            "inputs": inputs,
             "true_rel_residual": true_res,
             "cpu_baseline": {"value": value, "unit": "recons/s", "cores": os.cpu_count() if kind == "reference" else 1,
                              "kind": kind, "sample": f"full recon per step (pics -l2 -r{LAM} -i{REF_ITERS_TO_TOL}), "
                                                      "wall time incl. .cfl I/O"},
             "e2e": {"value": value, "unit": "recons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def profiled_traffic(path):
+    """DRAM bytes (read + write) of one launch from a committed ncu summary
+    (its '| dram bytes per launch (read + write) | N |' row), or None."""
+    import re
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"\|\s*dram bytes per launch \(read \+ write\)\s*\|\s*(\d+)\s*\|", open(path).read())
+    return int(m.group(1)) if m else None
 
 
 def peak_hbm():
@@ -786,10 +828,7 @@ def main():
     k_avg_s = (kms.value / 1e3) / max(1, kn.value)
     peak, peak_src = peak_hbm()
     achieved = alg_bytes / k_avg_s / 1e9 if k_avg_s > 0 else None
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(DOMINANT)
+    traffic = profiled_traffic(DOMINANT_PROFILE)
 
     nufft = nufft_throughput(dev) if (rank == 0 and not args.lean) else None
     vs_cufft = fft_vs_cufft(dev, traj, sens) if (rank == 0 and not args.lean) else None
@@ -799,16 +838,17 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "recons/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "image": N_IMG, "coils": COILS, "spokes": SPOKES, "samples": 512,
-                           "tol": TOL, "maxiter": MAXITER, "lambda": LAM, "toeplitz": True,
-                           "method": {"cg": "plain CG (the reference's pics)",
+                "config": workload_config(),
+                "solver": {"method": {"cg": "plain CG (the reference's pics)",
                                       "fcg_circulant": "flexible CG with the reference's circulant PSF preconditioner",
                                       "fcg_learned": "flexible CG with the circulant preconditioner and the learned correction",
                                       "fcg_padded": "PCG with the padded-circulant preconditioner"}[headline]
                                      + " (same normal equations and tolerance as the reference's plain-CG pics)",
-                           "parallelism": f"replicas{world}",
-                           "l2": "flushed before every timed step (512 MB write); inside a step the ~60 MB "
-                                 "working set stays L2-resident across CG iterations"},
+                           "maxiter": MAXITER},
+                "parallelism": f"replicas{world}",
+                "l2": "flushed before every timed step (512 MB write); inside a step the ~60 MB "
+                      "working set stays L2-resident across CG iterations",
+                "inputs": inputs_record(traj, sens, ksp),
                 "e2e": {"value": aggregate_rate(world, e2e_steps, e2e_s) if e2e_steps else None, "unit": "recons/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": kernels_per_step * args.steps,

@@ -53,9 +53,14 @@ void bnufft_conf_defaults(struct bnufft_conf* conf);
 
 /* Replaces nufft_create2() (src/noncart/nufft.h:48-57, src/noncart/nufft.c:1174).
  * ksp_dims [1, Mr, Ms, C, ...], cim_dims [X, Y, Z, C, ...], traj_dims
- * [3, Mr, Ms, 1, ...], traj complex float (real parts used). Weights and
- * basis must be NULL here (BNUFFT_ERR_UNSUPPORTED otherwise). The plan
- * copies the trajectory (the caller keeps its buffer) and, with
+ * [3, Mr, Ms, 1, ...], traj complex float (real parts used). weights
+ * (density weights or the -p sampling pattern, nufft_set_traj
+ * src/noncart/nufft.c:1041-1049) may be NULL, [1, Mr, Ms] or match the
+ * k-space dims (per coil; not with the Toeplitz PSF or --lowmem): the
+ * forward multiplies its k-space by them, the adjoint its input by their
+ * conjugate (src/noncart/nufft.c:1457, 1477).
+ * basis must be NULL (BNUFFT_ERR_UNSUPPORTED otherwise). The plan copies
+ * the trajectory and weights (the caller keeps its buffers) and, with
  * conf->toeplitz, computes the PSF on the device (compute_psf2,
  * src/noncart/nufft.c:727-776). */
 int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[], const long cim_dims[],
@@ -80,7 +85,11 @@ int bnufft_get_psf_dims(bnufft_plan_t plan, int ND, long psf_dims[]);
 int bnufft_get_psf(bnufft_plan_t plan, int ND, const long psf_dims[], void* psf, void* stream);
 
 /* Replaces nufft_update_traj (src/noncart/nufft.c:2041-2054) for a
- * trajectory of unchanged dims (weights / basis must be NULL). */
+ * trajectory of unchanged dims. The plan keeps its weights, as the
+ * reference does when its weights argument is NULL; the sample bins (and
+ * the CSR of the deterministic mode) and, with Toeplitz, the PSF are
+ * rebuilt for the new trajectory, so the plan then equals one created with
+ * it. */
 int bnufft_update_traj(bnufft_plan_t plan, int N, const long traj_dims[], const void* traj, void* stream);
 
 /* bart nufft -i [-c] -l lambda -m maxiter (src/nufft.c:250-263): CG
@@ -135,6 +144,10 @@ struct bnufft_pics_conf {
 				   operator's own 2N (or embedding) circulant inverted,
 				   crop F^-1 (|P| + mu)^-1 F pad, mu from lambda.
 				   1, 2 and 3 need the Toeplitz normal operator. */
+	int ref_scalars;	/* plain CG (precond 0) keeps ||r||^2, p^H A p, alpha and
+				   beta in float32 as conjgrad stores them
+				   (src/iter/italgos.c:518-554), so unconverged iterates
+				   follow the reference's; 0 = float64 scalars. Default 1. */
 };
 
 typedef struct bnufft_pics_s* bnufft_pics_t;
@@ -250,6 +263,20 @@ void bnufft_precnet_free(bnufft_precnet_t net);
 
 /* Attach a network to a model created with precond 2 (not owned). */
 int bnufft_pics_set_precnet(bnufft_pics_t pics, bnufft_precnet_t net, void* stream);
+
+/* Host-only views of the library's interpolation tables (no device work,
+ * usable without a GPU), built in float64 exactly as the plans build them:
+ * bnufft_calc_beta replaces calc_beta (src/noncart/grid.c:516-519);
+ * bnufft_kb_precompute replaces kb_precompute (src/noncart/grid.c:86-97,
+ * table[i] = I0(beta sqrt(1 - (2x)^2)) / I0(beta), x = i / (n - 1) / 2, n + 1
+ * floats; plans use n = 1000 and beta = float(calc_beta(os, width)), as
+ * the reference's kb_init receives it from rolloff_correction);
+ * bnufft_rolloff_axis gives the roll-off of one n-point image axis in
+ * float64, rolloff(pos(n, i, os), beta, width) of src/noncart/grid.c:114-117,
+ * 522-533. */
+double bnufft_calc_beta(float os, float width);
+int bnufft_kb_precompute(double beta, int n, float* table);
+int bnufft_rolloff_axis(float os, float width, long n, double* roll);
 
 /* Message of the last failure on this thread ("" if none). */
 const char* bnufft_last_error(void);

@@ -9,6 +9,8 @@ read the .npz files and never run the reference.
     make -f oracle/refbuild/Makefile -j8
     python tests/golden/make_golden.py            # all fixtures
     python tests/golden/make_golden.py --uneven   # only the non-power-of-two sizes
+    python tests/golden/make_golden.py --kb       # only the KB table and roll-off
+    python tests/golden/make_golden.py --fullsize # only the C1 / C2 full-size cases
 """
 
 from __future__ import annotations
@@ -31,8 +33,9 @@ from bart_b200.cfl import readcfl, writecfl  # noqa: E402
 BIN = os.path.join(ROOT, "oracle", "_ref", "bin")
 
 
-def run(*args, cwd):
-    r = subprocess.run([os.path.join(BIN, args[0])] + list(args[1:]), cwd=cwd, capture_output=True, text=True)
+def run(*args, cwd, env=None):
+    r = subprocess.run([os.path.join(BIN, args[0])] + list(args[1:]), cwd=cwd, capture_output=True, text=True,
+                       env=env)
     if r.returncode != 0:
         raise RuntimeError(f"{args}: {r.stderr}")
 
@@ -102,7 +105,10 @@ def inverse_case(name, traj, ksp, dims):
     print(name, {k: np.shape(v) for k, v in out.items()})
 
 
-def pics_case(name, N, C, spokes, seed, ndim=2, runs=None):
+def sense_problem(N, C, spokes, seed, ndim=2):
+    """Seeded CG-SENSE problem: trajectory, ellipse phantom, polynomial maps,
+    k-space simulated by the oracle's SENSE forward model plus 40 dB noise.
+    Deterministic: the full-size tests regenerate it from the seed."""
     from oracle.nufft_oracle import SenseOracle
     rng = np.random.default_rng(seed)
     traj = synth.radial_traj(N, spokes) if ndim == 2 else synth.kooshball_traj(N, spokes)
@@ -112,7 +118,23 @@ def pics_case(name, N, C, spokes, seed, ndim=2, runs=None):
     y = A.forward(truth.reshape(N, N, 1 if ndim == 2 else N, 1))
     y = synth.add_noise(y, 40.0, rng)
     ksp = y.reshape(1, traj.shape[1], traj.shape[2], C, order="F")
-    out = dict(traj=traj, sens=sens, ksp=ksp, truth=truth)
+    return traj, truth, sens, ksp
+
+
+def sha256(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes(order="F")).hexdigest()
+
+
+def pics_case(name, N, C, spokes, seed, ndim=2, runs=None, store_inputs=True, spread=()):
+    """Reference pics outputs on a seeded problem. store_inputs=False keeps
+    only the seed and a checksum of the k-space (full-size cases); spread
+    lists runs repeated with one OpenMP thread, whose difference to the
+    all-thread run measures the reference's own run-to-run spread (its
+    gridding adds with OpenMP atomics)."""
+    traj, truth, sens, ksp = sense_problem(N, C, spokes, seed, ndim)
+    out = dict(traj=traj, sens=sens, ksp=ksp, truth=truth) if store_inputs else \
+        dict(seed=np.int64(seed), N=np.int64(N), C=np.int64(C), spokes=np.int64(spokes), ksp_sha256=sha256(ksp))
     runs = runs or [("x5_w1", ["-i5", "-w1"]), ("x30_w1", ["-i30", "-w1"]), ("x30", ["-i30"]),
                     ("x5_w1_notoep", ["-i5", "-w1", "--no-toeplitz"]), ("x30_rescale", ["-i30", "-S"])]
     with tempfile.TemporaryDirectory() as d:
@@ -122,6 +144,63 @@ def pics_case(name, N, C, spokes, seed, ndim=2, runs=None):
         for key, args in runs:
             run("pics", "-l2", "-r0.01", *args, "-t", "t", "k", "s", "o", cwd=d)
             out[key] = readcfl(os.path.join(d, "o"))
+            if key in spread:
+                run("pics", "-l2", "-r0.01", *args, "-t", "t", "k", "s", "o1", cwd=d,
+                    env=dict(os.environ, OMP_NUM_THREADS="1"))
+                o1 = readcfl(os.path.join(d, "o1"))
+                out[key + "_spread"] = np.float64(np.linalg.norm((o1 - out[key]).ravel()) /
+                                                  np.linalg.norm(out[key].ravel()))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, {k: (np.shape(v) if np.ndim(v) else v) for k, v in out.items()})
+
+
+def fullsize_cases():
+    """The configs' own sizes. C1: 256^2 image, 402 golden-angle spokes x 512
+    samples, forward then adjoint of the forward's output. C2: 256^2, 16
+    coils, 96 spokes x 512, pics -l2 -r0.01 at 30 iterations (automatic and
+    unit scaling) and 5 iterations. Inputs regenerate from the seeds."""
+    seed = 20261205
+    rng = np.random.default_rng(seed)
+    traj = synth.radial_traj(256, 402)
+    img = cplx(rng, (256, 256))
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "t"), traj)
+        writecfl(os.path.join(d, "x"), img)
+        run("nufft", "t", "x", "k", cwd=d)
+        fwd = readcfl(os.path.join(d, "k"))
+        run("nufft", "-a", "-x256:256:1", "t", "k", "a", cwd=d)
+        adj = readcfl(os.path.join(d, "a"))
+    out = dict(seed=np.int64(seed), spokes=np.int64(402), img_sha256=sha256(img), fwd=fwd, adj=adj)
+    np.savez_compressed(os.path.join(HERE, "nufft2d_c1_n256.npz"), **out)
+    print("nufft2d_c1_n256", {k: np.shape(v) for k, v in out.items()})
+    pics_case("pics2d_c2_n256_c16", 256, 16, 96, seed=1000, store_inputs=False,
+              runs=[("x5_w1", ["-i5", "-w1"]), ("x30_w1", ["-i30", "-w1"]), ("x30", ["-i30"])],
+              spread=("x30_w1", "x30"))
+
+
+ROLL_SIDES = (8, 12, 16, 40, 48, 64, 128, 256, 512)
+
+
+def kb_case(name="kb_table"):
+    """The reference's KB table, I0(beta) and per-axis roll-off (kbtable tool)."""
+    r = subprocess.run([os.path.join(BIN, "kbtable"), "2", "6"] + [str(n) for n in ROLL_SIDES],
+                       capture_output=True, text=True, check=True)
+    kb, roll, out = {}, {}, {}
+    for line in r.stdout.split("\n"):
+        f = line.split()
+        if not f:
+            continue
+        if f[0] == "beta":
+            out["beta"] = np.float64(float.fromhex(f[1]))
+        elif f[0] == "i0beta":
+            out["i0beta"] = np.float64(float.fromhex(f[1]))
+        elif f[0] == "kb":
+            kb[int(f[1])] = float.fromhex(f[2])
+        elif f[0] == "roll":
+            roll.setdefault(int(f[1]), {})[int(f[2])] = float.fromhex(f[3])
+    out["kb"] = np.array([kb[i] for i in range(len(kb))], dtype=np.float32)
+    for n, v in roll.items():
+        out[f"roll_{n}"] = np.array([v[i] for i in range(n)], dtype=np.float32)
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print(name, {k: np.shape(v) for k, v in out.items()})
 
@@ -158,6 +237,12 @@ def main():
     if "--uneven" in sys.argv:
         uneven_cases()
         return
+    if "--kb" in sys.argv:
+        kb_case()
+        return
+    if "--fullsize" in sys.argv:
+        fullsize_cases()
+        return
     rng = np.random.default_rng(20261203)
     with tempfile.TemporaryDirectory() as d:
         run("traj", "-r", "-G", "-x64", "-o2", "-y24", "t", cwd=d)
@@ -176,6 +261,8 @@ def main():
     g = np.load(os.path.join(HERE, "nufft2d_n32_coils3.npz"))
     inverse_case("inverse2d_n32_coils3", g["traj"], g["fwd"], (32, 32, 1))
     uneven_cases()
+    kb_case()
+    fullsize_cases()
 
 
 if __name__ == "__main__":

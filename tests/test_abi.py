@@ -46,3 +46,26 @@ def test_argument_errors_without_device():
     assert "trajectory" in lib.bnufft_last_error().decode()
     with pytest.raises(_lib.BnufftError):
         _lib.check(st)
+
+
+def test_kb_table_bitwise_library():
+    """The library's own table builder (the one every plan and the
+    allocation-free entry point upload) gives the reference's 1001 floats
+    bit for bit, and its float64 roll-off rounds to the reference's float
+    roll-off (kb_precompute / rolloff_correction, src/noncart/grid.c:86-97,
+    536-556). Host-only calls: no GPU needed."""
+    import numpy as np
+    from bart_b200 import _lib
+    from conftest import golden
+    lib = _lib.load()
+    g = golden("kb_table")
+    beta = lib.bnufft_calc_beta(2.0, 6.0)
+    assert beta == float(g["beta"])
+    t = np.zeros(1001, dtype=np.float32)
+    kb_beta = float(np.float32(beta))     # rolloff_correction passes beta as float to kb_init
+    _lib.check(lib.bnufft_kb_precompute(kb_beta, 1000, t.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+    assert np.array_equal(t.view(np.uint32), g["kb"].view(np.uint32))
+    for n in (8, 12, 16, 40, 48, 64, 128, 256, 512):
+        r = np.zeros(n, dtype=np.float64)
+        _lib.check(lib.bnufft_rolloff_axis(2.0, 6.0, n, r.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        assert np.array_equal(r.astype(np.float32).view(np.uint32), g[f"roll_{n}"].view(np.uint32)), n

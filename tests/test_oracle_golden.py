@@ -177,3 +177,22 @@ def test_padded_precond_beats_strang_on_the_oracle():
     x1, it1 = orc.pcg(A.normal, b, 0.01, strang)
     assert orc.normal_residual(A, x3, b, 0.01) < 1.5e-4
     assert it3 < it1, (it3, it1)
+
+
+ROLL_SIDES = (8, 12, 16, 40, 48, 64, 128, 256, 512)
+
+
+def test_kb_table_bitwise():
+    """The oracle's Kaiser-Bessel table (1001 floats) and per-axis roll-off
+    are bit-identical to the reference's (kbtable tool: kb_init through
+    rolloff_correction, src/noncart/grid.c:45-97, 536-556)."""
+    g = golden("kb_table")
+    assert orc.calc_beta(2.0, 6.0) == float(g["beta"])
+    beta = orc.kernel_beta(2.0, 6.0)
+    t = orc.kb_table(beta)
+    assert t.shape == g["kb"].shape == (1001,)
+    assert np.array_equal(t.view(np.uint32), g["kb"].view(np.uint32))
+    assert abs(orc.bessel_i0(beta) / float(g["i0beta"]) - 1.0) < 2e-15   # a few float64 ulp
+    for n in ROLL_SIDES:
+        r = orc.rolloff_axis(n, 2.0, 6.0, beta).astype(np.float32)
+        assert np.array_equal(r.view(np.uint32), g[f"roll_{n}"].view(np.uint32)), n
