@@ -11,6 +11,7 @@ read the .npz files and never run the reference.
     python tests/golden/make_golden.py --uneven   # only the non-power-of-two sizes
     python tests/golden/make_golden.py --kb       # only the KB table and roll-off
     python tests/golden/make_golden.py --fullsize # only the C1 / C2 full-size cases
+    python tests/golden/make_golden.py --gpu-gridding  # the reference's GPU-gridding test inputs
 """
 
 from __future__ import annotations
@@ -129,9 +130,9 @@ def sha256(a):
 def pics_case(name, N, C, spokes, seed, ndim=2, runs=None, store_inputs=True, spread=()):
     """Reference pics outputs on a seeded problem. store_inputs=False keeps
     only the seed and a checksum of the k-space (full-size cases); spread
-    lists runs repeated with one OpenMP thread, whose difference to the
-    all-thread run measures the reference's own run-to-run spread (its
-    gridding adds with OpenMP atomics)."""
+    lists runs repeated with 1, 2, 4 and 8 OpenMP threads, whose largest
+    difference to the stored run measures the reference's own run-to-run
+    spread (its gridding adds with OpenMP atomics in thread order)."""
     traj, truth, sens, ksp = sense_problem(N, C, spokes, seed, ndim)
     out = dict(traj=traj, sens=sens, ksp=ksp, truth=truth) if store_inputs else \
         dict(seed=np.int64(seed), N=np.int64(N), C=np.int64(C), spokes=np.int64(spokes), ksp_sha256=sha256(ksp))
@@ -145,11 +146,37 @@ def pics_case(name, N, C, spokes, seed, ndim=2, runs=None, store_inputs=True, sp
             run("pics", "-l2", "-r0.01", *args, "-t", "t", "k", "s", "o", cwd=d)
             out[key] = readcfl(os.path.join(d, "o"))
             if key in spread:
-                run("pics", "-l2", "-r0.01", *args, "-t", "t", "k", "s", "o1", cwd=d,
-                    env=dict(os.environ, OMP_NUM_THREADS="1"))
-                o1 = readcfl(os.path.join(d, "o1"))
-                out[key + "_spread"] = np.float64(np.linalg.norm((o1 - out[key]).ravel()) /
-                                                  np.linalg.norm(out[key].ravel()))
+                sp = 0.0
+                for th in ("1", "2", "4", "8"):
+                    run("pics", "-l2", "-r0.01", *args, "-t", "t", "k", "s", "o1", cwd=d,
+                        env=dict(os.environ, OMP_NUM_THREADS=th))
+                    o1 = readcfl(os.path.join(d, "o1"))
+                    sp = max(sp, np.linalg.norm((o1 - out[key]).ravel()) / np.linalg.norm(out[key].ravel()))
+                out[key + "_spread"] = np.float64(sp)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, {k: (np.shape(v) if np.ndim(v) else v) for k, v in out.items()})
+
+
+def gpu_gridding_case(name="pics2d_gpu_gridding_n128"):
+    """The inputs of the reference's own GPU-gridding test
+    (tests/gpu.mk:27-37, test-pics-gpu-noncart-gridding): radial trajectory
+    256 x 64 scaled by 0.5, the analytic Shepp-Logan k-space on it, a
+    128 x 128 map of ones; the reference's CPU pics -S -r0.001 (30
+    iterations) is the result its GPU gridding must match to nrmse 0.007.
+    Also stored: the spread of that output between 1 and all OpenMP threads."""
+    with tempfile.TemporaryDirectory() as d:
+        run("traj", "-r", "-x256", "-y64", "traj", cwd=d)
+        run("scale", "0.5", "traj", "traj2", cwd=d)
+        run("phantom", "-t", "traj2", "ksp", cwd=d)
+        run("ones", "3", "128", "128", "1", "o", cwd=d)
+        run("pics", "-S", "-r0.001", "-t", "traj2", "ksp", "o", "reco1", cwd=d)
+        run("pics", "-S", "-r0.001", "-t", "traj2", "ksp", "o", "reco1t1", cwd=d,
+            env=dict(os.environ, OMP_NUM_THREADS="1"))
+        traj, ksp, reco = readcfl(os.path.join(d, "traj2")), readcfl(os.path.join(d, "ksp")), \
+            readcfl(os.path.join(d, "reco1"))
+        t1 = readcfl(os.path.join(d, "reco1t1"))
+    spread = np.float64(np.linalg.norm((t1 - reco).ravel()) / np.linalg.norm(reco.ravel()))
+    out = dict(traj=traj, ksp=ksp, reco=reco, spread=spread)
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print(name, {k: (np.shape(v) if np.ndim(v) else v) for k, v in out.items()})
 
@@ -174,8 +201,10 @@ def fullsize_cases():
     np.savez_compressed(os.path.join(HERE, "nufft2d_c1_n256.npz"), **out)
     print("nufft2d_c1_n256", {k: np.shape(v) for k, v in out.items()})
     pics_case("pics2d_c2_n256_c16", 256, 16, 96, seed=1000, store_inputs=False,
-              runs=[("x5_w1", ["-i5", "-w1"]), ("x30_w1", ["-i30", "-w1"]), ("x30", ["-i30"])],
-              spread=("x30_w1", "x30"))
+              runs=[("x5_w1", ["-i5", "-w1"]), ("x30_w1", ["-i30", "-w1"]), ("x30", ["-i30"]),
+                    ("x30_w1_notoep", ["-i30", "-w1", "--no-toeplitz"]), ("x30_notoep", ["-i30", "--no-toeplitz"]),
+                    ("x300_w1", ["-i300", "-w1"]), ("x300", ["-i300"])],
+              spread=("x30_w1", "x30", "x300_w1", "x300"))
 
 
 ROLL_SIDES = (8, 12, 16, 40, 48, 64, 128, 256, 512)
@@ -243,6 +272,9 @@ def main():
     if "--fullsize" in sys.argv:
         fullsize_cases()
         return
+    if "--gpu-gridding" in sys.argv:
+        gpu_gridding_case()
+        return
     rng = np.random.default_rng(20261203)
     with tempfile.TemporaryDirectory() as d:
         run("traj", "-r", "-G", "-x64", "-o2", "-y24", "t", cwd=d)
@@ -263,6 +295,7 @@ def main():
     uneven_cases()
     kb_case()
     fullsize_cases()
+    gpu_gridding_case()
 
 
 if __name__ == "__main__":

@@ -34,15 +34,22 @@ def test_pics_5_iterations_vs_reference(name, tol):
 
 
 def test_pics_30_iterations_vs_reference():
-    """Unconverged float32 CG drifts with rounding; the reference itself moves
-    by ~1e-4..1e-2 between float32 orderings. Scaling must match exactly."""
+    """30 unconverged iterations at 64^2 (4 coils) stay within the 1e-4
+    reconstruction bar of the reference's pics (measured 4.9e-5; the
+    reference's own runs at 1..8 threads differ by ~2.5e-5). Scaling must
+    match to the last bit of the adjoint's order statistics."""
     g = golden("pics2d_n64_c4")
     x, st = _run(g, maxiter=30)
-    assert rel(x, g["x30"]) < 2e-2
+    xw, _ = _run(g, maxiter=30, scaling=1.0)
+    x64, _ = _run(g, maxiter=30, ref_scalars=False)
+    print(f"30 it: float32 scalars {rel(x, g['x30']):.2e} (w1 {rel(xw, g['x30_w1']):.2e}), "
+          f"float64 scalars {rel(x64, g['x30']):.2e}")
+    assert rel(x, g["x30"]) < 1e-4
+    assert rel(xw, g["x30_w1"]) < 1e-4
     xs, st2 = _run(g, maxiter=30, rescale=True)
     # gridding adds with atomics, so the adjoint's p90 moves in the last bit
     assert abs(st2[2] - st[2]) <= 1e-6 * st[2]
-    assert rel(xs, g["x30_rescale"]) < 2e-2
+    assert rel(xs, g["x30_rescale"]) < 1e-4
 
 
 @pytest.mark.parametrize("lam,tol", [(0.1, 1e-4), (0.01, 5e-4)])
@@ -305,3 +312,22 @@ def test_fcg_folded_launches_match_unfolded():
     assert abs(sf[0] - su[0]) <= max(3, su[0] // 10) and sf[1] <= 1e-5 and su[1] <= 1e-5
     assert rel(xf, xu) < 2e-3
     assert kf < ku
+
+
+def test_pics_gpu_gridding_case_vs_reference():
+    """Counterpart of the reference's GPU-gridding test (tests/gpu.mk:27-37,
+    test-pics-gpu-noncart-gridding): the reference's own traj / scale /
+    phantom -t / ones inputs and its CPU pics -S -r0.001 (30 iterations) as
+    the fixture. The reference accepts its GPU gridding within nrmse 0.007 of
+    its CPU result; here all gridding runs on the GPU, and with the
+    reference's float32 CG scalars the result lies within the reference's own
+    1-vs-all-thread spread (stored in the fixture) of its CPU output."""
+    g = golden("pics2d_gpu_gridding_n128")
+    traj, ksp = g["traj"], g["ksp"]
+    sens = np.ones((128, 128, 1, 1), dtype=np.complex64)
+    p = Pics(traj, sens, ksp_dims=list(ksp.shape), conf=PicsConf(lam=0.001, maxiter=30, rescale=True))
+    x = np.asarray(p.run(ksp))
+    p.free()
+    e = rel(x, g["reco"])
+    print(f"GPU-gridding case: {e:.2e} (reference spread {float(g['spread']):.2e})")
+    assert e < 0.007
