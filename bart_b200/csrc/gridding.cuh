@@ -567,4 +567,503 @@ __global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_atomic(const float4* _
 	}
 }
 
+// Gridding, width 6, output-stationary (the default scatter) ------------------
+//
+// The grid is cut into tiles that are the sample bins (TX x LY x LZ cells of
+// the centred oversampled grid). One warp job owns one tile and a group of
+// coils: lane (line, grp) holds the TX x-cells of tile line (y, z) = line
+// for CT coils in registers, so it accumulates without atomics. A sample's
+// taps lie within 3 cells of its centred position 2k + N on every axis
+// (cells 2w + s, |w - pos_s| <= 1.5), so the samples that reach a tile are
+// in the tile's bin and its 3^d - 1 neighbours: the warp scans those bins'
+// sorted samples 32 at a time, keeps the ones whose footprint meets the tile
+// (ballot + compaction into shared memory, with their weights and coil
+// values), and adds each kept sample to its lanes' cells. The x offset of a
+// sample is the same for the whole warp, so a switch on it selects a fully
+// unrolled update of exactly the taps inside the tile; lanes whose line is
+// outside the sample's y/z window skip it.
+//
+// Work items: a tile's candidates (the samples of its neighbourhood, in a
+// fixed bin order) are cut into chunks of TG_CAND; tiles with one chunk
+// write their cells with plain stores (empty tiles write zeros, so the grid
+// needs no clearing), tiles with several chunks (the dense k-space centre)
+// add their chunks with atomics into cells that k_zero_tiles cleared.
+// Weights are those of axis_taps6 (bit-identical to the reference's
+// grid_point_gen, src/noncart/grid.c:403-465) and the combined weight the
+// same float32 product ((1 * wz) * wy) * wx.
+
+enum { TG_CAND = 512, TG_WARPS = 4 };
+
+struct TileWork {
+
+	const int* bin_start;		// [nbins + 1] sorted sample range of each bin
+	const int* work_tile;		// [nwork] tile of a work item
+	const int* work_chunk;		// [nwork] chunk of the tile's candidates
+	const int* nwork_dev;		// number of work items
+	const unsigned char* multi;	// [ntiles] 1 if the tile has several work items
+	const float4* foot;		// [M][FOOT_F4] footprints of the sorted samples
+};
+
+// Footprint record of a sorted sample (built once per trajectory by
+// k_foot): float4 0 holds the centred start cells lo of the x, y, z taps
+// (as int bits); float4s 1..5 the weights of cells lo .. lo + 5 per axis,
+// x then y then z (6 each, the last two slots zero). A singleton axis has
+// lo = 0 and the one weight intlookup(0).
+enum { FOOT_F4 = 6 };
+
+// Footprint of one axis: the six taps of a sample (two sub-grids x three)
+// lie on the centred cells lo .. lo + 5 (2w + s); w7[t] is the weight of
+// cell lo + t (0 where a non-periodic grid clips the tap). Singleton axis:
+// one tap at 0 with weight intlookup(0).
+__device__ __forceinline__ int foot6_lo(float k, int N)
+{
+	if (1 == N)
+		return 0;
+
+	const float half = (float)(N / 2);
+	int lo = INT_MAX;
+#pragma unroll
+	for (int s = 0; s < 2; s++) {
+
+		float pos = __fadd_rn(__fadd_rn(k, s ? -0.5f : -0.0f), half);
+		double l = (double)pos - 1.5;
+		int sti = (int)ceil(l);
+
+		if ((double)sti == l)
+			sti += 1;
+
+		lo = min(lo, 2 * sti + s);
+	}
+
+	return lo;
+}
+
+__device__ __forceinline__ void foot6_w(float k, int N, int periodic, const float* kb, int lo, float* w7)
+{
+#pragma unroll
+	for (int t = 0; t < 7; t++)
+		w7[t] = 0.f;
+
+	if (1 == N) {
+
+		w7[0] = kb_lookup(kb, 0.f);
+		return;
+	}
+
+	const float half = (float)(N / 2);
+#pragma unroll
+	for (int s = 0; s < 2; s++) {
+
+		float pos = __fadd_rn(__fadd_rn(k, s ? -0.5f : -0.0f), half);
+		double l = (double)pos - 1.5;
+		int sti = (int)ceil(l);
+
+		if ((double)sti == l)
+			sti += 1;
+#pragma unroll
+		for (int q = 0; q < 3; q++) {
+
+			int w = sti + q;
+			float frac = fabsf(__fsub_rn((float)w, pos));
+			float val = kb_lookup(kb, __fdiv_rn(frac, 3.0f));
+			bool valid = periodic || ((w >= 0) && (w <= N - 1));
+			int t = 2 * w + s - lo;
+
+			if ((t >= 0) && (t < 7))
+				w7[t] = valid ? val : 0.f;
+		}
+	}
+}
+
+// footprints of all sorted samples (the weights as axis_taps6 computes them:
+// the same kb_lookup of the same float32 distances)
+__global__ void k_foot(const float4* __restrict__ traj_sorted, long M, GridGeom g, const float* __restrict__ kbg,
+		float4* __restrict__ foot)
+{
+	__shared__ float kb[KB_TABLE_N + 1];
+
+	for (int i = threadIdx.x; i <= KB_TABLE_N; i += blockDim.x)
+		kb[i] = kbg[i];
+
+	__syncthreads();
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += (long)gridDim.x * blockDim.x) {
+
+		const float4 k = traj_sorted[i];
+		const float kk[3] = { k.x, k.y, k.z };
+		float w[24];
+		int lo[3];
+#pragma unroll
+		for (int a = 0; a < 3; a++) {
+
+			float w7[7];
+			lo[a] = foot6_lo(kk[a], g.N[a]);
+			foot6_w(kk[a], g.N[a], g.periodic, kb, lo[a], w7);
+#pragma unroll
+			for (int t = 0; t < 6; t++)
+				w[6 * a + t] = w7[t];
+		}
+
+		w[18] = w[19] = w[20] = w[21] = w[22] = w[23] = 0.f;
+		float4* f = foot + i * FOOT_F4;
+		f[0] = make_float4(__int_as_float(lo[0]), __int_as_float(lo[1]), __int_as_float(lo[2]), 0.f);
+#pragma unroll
+		for (int q = 0; q < 5; q++)
+			f[1 + q] = make_float4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+	}
+}
+
+// offset of a footprint start relative to a tile origin, along an axis of
+// G cells: periodic grids take the representative nearest to the tile
+__device__ __forceinline__ int foot_rel(int lo, int origin, int G, int periodic)
+{
+	int r = lo - origin;
+
+	if (periodic) {
+
+		r %= G;
+
+		if (r > G / 2)
+			r -= G;
+		else if (r < -G / 2)
+			r += G;
+	}
+
+	return r;
+}
+
+// DFT-order index of centred cell c of an axis (G = 2N cells; 0 for singletons)
+__device__ __forceinline__ int dft_index(int c, int N, int G)
+{
+	if (1 == G)
+		return 0;
+
+	c += N;
+	return (c >= G) ? c - G : c;
+}
+
+// one staged sample of a warp job
+template <int CW>
+struct __align__(16) TgSample {
+
+	float w[24];		// x, y, z weights of cells lo .. lo + 5 (6 each)
+	int rx, ry, rz, pad;
+	float2 v[CW];
+};
+
+// acc[i][c] += (wyz * wx[t]) * v[c] for the taps t whose cell i = RX + t is
+// inside the tile (RX a compile-time offset)
+template <int TX, int CT, int RX>
+__device__ __forceinline__ void tg_accum_x(float2 (&acc)[TX][CT], const float* wx, float wyz, const float2* v)
+{
+#pragma unroll
+	for (int t = 0; t < 6; t++) {
+
+		if ((RX + t >= 0) && (RX + t < TX)) {
+
+			float d = __fmul_rn(wyz, wx[t]);
+#pragma unroll
+			for (int c = 0; c < CT; c++) {
+
+				acc[RX + t][c].x = fmaf(v[c].x, d, acc[RX + t][c].x);
+				acc[RX + t][c].y = fmaf(v[c].y, d, acc[RX + t][c].y);
+			}
+		}
+	}
+}
+
+// the update for a sample at x offset rx (-5 .. TX - 1, at most 15)
+#define BN_TG_CASE(R) case R: tg_accum_x<TX, CT, R>(acc, wx, wyz, v); break;
+
+template <int TX, int CT>
+__device__ __forceinline__ void tg_switch(int rx, float2 (&acc)[TX][CT], const float* wx, float wyz, const float2* v)
+{
+	static_assert(TX <= 16, "x offsets up to 15");
+
+	switch (rx) {
+	BN_TG_CASE(-5) BN_TG_CASE(-4) BN_TG_CASE(-3) BN_TG_CASE(-2) BN_TG_CASE(-1)
+	BN_TG_CASE(0) BN_TG_CASE(1) BN_TG_CASE(2) BN_TG_CASE(3) BN_TG_CASE(4) BN_TG_CASE(5) BN_TG_CASE(6)
+	BN_TG_CASE(7) BN_TG_CASE(8) BN_TG_CASE(9) BN_TG_CASE(10) BN_TG_CASE(11) BN_TG_CASE(12) BN_TG_CASE(13)
+	BN_TG_CASE(14) BN_TG_CASE(15)
+	default: break;
+	}
+}
+
+#undef BN_TG_CASE
+
+// grid cells of the tiles that several work items add into: zeroed first
+__global__ void k_zero_tiles(float2* __restrict__ grid, GridGeom g, BinGeom bg, const unsigned char* __restrict__ multi,
+		long ntiles, int C)
+{
+	const long per = (long)bg.bs[0] * bg.bs[1] * bg.bs[2];
+
+	for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+
+		if (!multi[t])
+			continue;
+
+		const int bx = (int)(t % bg.nb[0]), by = (int)((t / bg.nb[0]) % bg.nb[1]), bz = (int)(t / ((long)bg.nb[0] * bg.nb[1]));
+
+		for (long e = threadIdx.x; e < per * C; e += blockDim.x) {
+
+			const int c = (int)(e / per);
+			const long l = e - (long)c * per;
+			const int cx = bx * bg.bs[0] + (int)(l % bg.bs[0]);
+			const int cy = by * bg.bs[1] + (int)((l / bg.bs[0]) % bg.bs[1]);
+			const int cz = bz * bg.bs[2] + (int)(l / ((long)bg.bs[0] * bg.bs[1]));
+
+			if ((cx >= g.G[0]) || (cy >= g.G[1]) || (cz >= g.G[2]))
+				continue;
+
+			const long cell = dft_index(cx, g.N[0], g.G[0]) + (long)g.G[0] * (dft_index(cy, g.N[1], g.G[1])
+					+ (long)g.G[1] * dft_index(cz, g.N[2], g.G[2]));
+			grid[cell + g.gsz * c] = make_float2(0.f, 0.f);
+		}
+	}
+}
+
+// candidates of tile (tx, ty, tz): the neighbour bins in the order dz, dy,
+// dx = -1..1 (singleton axes: 0 only; non-periodic edges skipped)
+__device__ __forceinline__ int tg_neighbour(int b, int d, int nb, int periodic)
+{
+	int n = b + d;
+
+	if (periodic)
+		return (n < 0) ? n + nb : ((n >= nb) ? n - nb : n);
+
+	return ((n < 0) || (n >= nb)) ? -1 : n;
+}
+
+// candidates per tile and the work items (chunks of TG_CAND) per tile
+__global__ void k_tile_cand(const int* __restrict__ bin_start, BinGeom bg, int periodic, long ntiles,
+		int* __restrict__ nwork, unsigned char* __restrict__ multi)
+{
+	for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += (long)gridDim.x * blockDim.x) {
+
+		const int bx = (int)(t % bg.nb[0]), by = (int)((t / bg.nb[0]) % bg.nb[1]), bz = (int)(t / ((long)bg.nb[0] * bg.nb[1]));
+		const int rz = (bg.nb[2] > 1) ? 1 : 0, ry = (bg.nb[1] > 1) ? 1 : 0;
+		long n = 0;
+
+		for (int dz = -rz; dz <= rz; dz++) {
+
+			const int z = tg_neighbour(bz, dz, bg.nb[2], periodic);
+
+			if (z < 0)
+				continue;
+
+			for (int dy = -ry; dy <= ry; dy++) {
+
+				const int y = tg_neighbour(by, dy, bg.nb[1], periodic);
+
+				if (y < 0)
+					continue;
+
+				for (int dx = -1; dx <= 1; dx++) {
+
+					const int x = tg_neighbour(bx, dx, bg.nb[0], periodic);
+
+					if (x < 0)
+						continue;
+
+					const long b = x + (long)bg.nb[0] * (y + (long)bg.nb[1] * z);
+					n += bin_start[b + 1] - bin_start[b];
+				}
+			}
+		}
+
+		const long w = (n + TG_CAND - 1) / TG_CAND;
+		nwork[t] = (int)((w < 1) ? 1 : w);
+		multi[t] = (w > 1) ? 1 : 0;
+	}
+}
+
+// work item table: tile t owns items work_start[t] .. work_start[t + 1] - 1
+__global__ void k_work_fill(const int* __restrict__ work_start, long ntiles, int* __restrict__ work_tile,
+		int* __restrict__ work_chunk)
+{
+	for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += (long)gridDim.x * blockDim.x)
+		for (int w = work_start[t]; w < work_start[t + 1]; w++) {
+
+			work_tile[w] = (int)t;
+			work_chunk[w] = w - work_start[t];
+		}
+}
+
+// TX x-cells per lane, LY x LZ lines per tile (LY * LZ divides 32), CT coils
+// per lane: a warp job covers CW = (32 / (LY * LZ)) * CT coils. ksp_sorted:
+// ksp is in bin order (sample i of the sorted trajectory at ksp[i + M c]),
+// else in the caller's order (ksp[perm[i] + M c]).
+template <int TX, int LY, int LZ, int CT>
+__global__ void __launch_bounds__(32 * TG_WARPS, 4) k_grid6_tiles(const int* __restrict__ perm, long M, GridGeom g,
+		BinGeom bg, TileWork tw, int C, const float2* __restrict__ ksp, int ksp_sorted, float2* __restrict__ grid)
+{
+	constexpr int NL = LY * LZ;
+	constexpr int GPW = 32 / NL;
+	constexpr int CW = GPW * CT;
+	static_assert(NL * GPW == 32, "lines per tile must divide 32");
+	__shared__ TgSample<CW> stage[TG_WARPS][32];
+
+	const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+	const int ncq = (C + CW - 1) / CW;	// coil chunks
+	const long job = (long)blockIdx.x * TG_WARPS + warp;
+	const long wi = job / ncq;
+	const int cq = (int)(job % ncq);
+
+	if (wi >= *tw.nwork_dev)	// warp-uniform; the warps share no barrier
+		return;
+
+	const int tile = tw.work_tile[wi];
+	const int chunk = tw.work_chunk[wi];
+	const int bx = tile % bg.nb[0], by = (tile / bg.nb[0]) % bg.nb[1], bz = tile / (bg.nb[0] * bg.nb[1]);
+	const int ox = bx * TX, oy = by * LY, oz = bz * LZ;
+	const int j = lane % LY, k = (lane / LY) % LZ, grp = lane / NL;
+	const int cw0 = cq * CW;		// first coil of the job
+	const int c0 = cw0 + grp * CT;		// first coil of this lane
+	TgSample<CW>* sg = stage[warp];
+
+	float2 acc[TX][CT];
+#pragma unroll
+	for (int i = 0; i < TX; i++)
+#pragma unroll
+		for (int c = 0; c < CT; c++)
+			acc[i][c] = make_float2(0.f, 0.f);
+
+	const long cand0 = (long)chunk * TG_CAND, cand1 = cand0 + TG_CAND;
+	const int rz = (bg.nb[2] > 1) ? 1 : 0, ry = (bg.nb[1] > 1) ? 1 : 0;
+	long off = 0;
+
+	for (int dz = -rz; (dz <= rz) && (off < cand1); dz++) {
+
+		const int nz = tg_neighbour(bz, dz, bg.nb[2], g.periodic);
+
+		if (nz < 0)
+			continue;
+
+		for (int dy = -ry; (dy <= ry) && (off < cand1); dy++) {
+
+			const int ny = tg_neighbour(by, dy, bg.nb[1], g.periodic);
+
+			if (ny < 0)
+				continue;
+
+			for (int dx = -1; (dx <= 1) && (off < cand1); dx++) {
+
+				const int nx = tg_neighbour(bx, dx, bg.nb[0], g.periodic);
+
+				if (nx < 0)
+					continue;
+
+				const long b = nx + (long)bg.nb[0] * (ny + (long)bg.nb[1] * nz);
+				const int s0 = tw.bin_start[b], s1 = tw.bin_start[b + 1];
+				const long a = max(off, cand0), e = min(off + (long)(s1 - s0), cand1);
+				const int i0 = s0 + (int)(a - off), i1 = s0 + (int)(e - off);
+				off += s1 - s0;
+
+				for (int base = i0; base < i1; base += 32) {
+
+					const int i = base + lane;
+					bool hit = false;
+					int lx = 0, ly = 0, lz = 0;
+
+					if (i < i1) {
+
+						const float4 f0 = tw.foot[(long)i * FOOT_F4];
+						lx = foot_rel(__float_as_int(f0.x), ox, g.G[0], g.periodic);
+						ly = foot_rel(__float_as_int(f0.y), oy, g.G[1], g.periodic);
+						lz = foot_rel(__float_as_int(f0.z), oz, g.G[2], g.periodic);
+						hit = (lx > -6) && (lx < TX) && (ly > -6) && (ly < LY) && (lz > -6) && (lz < LZ);
+					}
+
+					const unsigned mask = __ballot_sync(0xffffffffu, hit);
+					const int n = __popc(mask);
+
+					if (hit) {
+
+						TgSample<CW>& d = sg[__popc(mask & ((1u << lane) - 1u))];
+						const float4* f = tw.foot + (long)i * FOOT_F4;
+#pragma unroll
+						for (int q = 0; q < 5; q++)
+							*(float4*)(d.w + 4 * q) = f[1 + q];
+						d.rx = lx;
+						d.ry = ly;
+						d.rz = lz;
+						const long m = ksp_sorted ? (long)i : (long)perm[i];
+#pragma unroll
+						for (int c = 0; c < CW; c++)
+							d.v[c] = (cw0 + c < C) ? ksp[m + M * (cw0 + c)] : make_float2(0.f, 0.f);
+					}
+
+					__syncwarp();
+
+					for (int q = 0; q < n; q++) {
+
+						const TgSample<CW>& d = sg[q];
+						const int ty = j - d.ry, tz = k - d.rz;
+
+						if ((ty < 0) || (ty >= 6) || (tz < 0) || (tz >= 6))
+							continue;
+
+						const float wyz = __fmul_rn(d.w[12 + tz], d.w[6 + ty]);
+
+						if (0.f == wyz)
+							continue;
+
+						float2 v[CT];
+#pragma unroll
+						for (int c = 0; c < CT; c++)
+							v[c] = d.v[grp * CT + c];
+
+						tg_switch<TX, CT>(d.rx, acc, d.w, wyz, v);
+					}
+
+					__syncwarp();
+				}
+			}
+		}
+	}
+
+	// this lane's line: TX cells from ox along x, at (oy + j, oz + k)
+	const int cy = oy + j, cz = oz + k;
+
+	if ((cy >= g.G[1]) || (cz >= g.G[2]))
+		return;
+
+	const bool add = tw.multi[tile];
+	const long row = (long)g.G[0] * (dft_index(cy, g.N[1], g.G[1]) + (long)g.G[1] * dft_index(cz, g.N[2], g.G[2]));
+#pragma unroll
+	for (int i = 0; i < TX; i++) {
+
+		const int cx = ox + i;
+
+		if (cx >= g.G[0])
+			break;
+
+		const long cell = row + dft_index(cx, g.N[0], g.G[0]);
+#pragma unroll
+		for (int c = 0; c < CT; c++) {
+
+			if (c0 + c >= C)
+				break;
+
+			float2* dst = grid + cell + g.gsz * (c0 + c);
+
+			if (add)
+				atomicAdd(dst, acc[i][c]);
+			else
+				*dst = acc[i][c];
+		}
+	}
+}
+
+// ksp [M, C] into bin order: dst[i + M c] = src[perm[i] + M c]
+__global__ void k_permute_ksp(float2* __restrict__ dst, const float2* __restrict__ src, const int* __restrict__ perm,
+		long M, int C)
+{
+	for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < M * C; e += (long)gridDim.x * blockDim.x) {
+
+		const long c = e / M, i = e - c * M;
+		dst[e] = src[perm[i] + M * c];
+	}
+}
+
 } // namespace bn
