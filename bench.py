@@ -288,8 +288,25 @@ def run_nufft3d(dev, steps, warmup, spokes=20000):
         it, rr, _ = p.stats()
         to_tol[name] = {"ms": e0.elapsed_time(e1), "iterations": it, "recursive_rel_residual": rr}
         p.free()
+    # roofline of the fwd+adj step: compulsory bytes (coil images in and out,
+    # k-space out and in, trajectory twice), the oversampled grid's round
+    # trips (written and read once per direction), and the interpolation's
+    # FP32 work (a complex multiply-add per tap, sample and coil, both
+    # directions) against the nominal FP32 rate at the sampled SM clock
+    peak, peak_src = peak_hbm()
+    G3 = (2 * N) ** 3
+    grid_bytes = 2 * 2 * G3 * C * 8
+    tap_flop = 2 * 4 * 216 * M * C
+    fp32_peak = 148 * 128 * 2 * 1.965e9
     return {"workload": f"nufft3d_128_c8_kooshball_{spokes}x256", "nufft_fwd_adj_ms": ms, "kernel_classes": classes,
             "nufft_gbs": nbytes / (ms * 1e-3) / 1e9, "bytes_per_step": nbytes,
+            "roofline": {"hbm_peak_gbs": peak, "peak_source": peak_src,
+                         "compulsory_frac": nbytes / (ms * 1e-3) / 1e9 / peak,
+                         "with_grid_roundtrip_frac": (nbytes + grid_bytes) / (ms * 1e-3) / 1e9 / peak,
+                         "grid_roundtrip_bytes": grid_bytes,
+                         "tap_tflops": tap_flop / (ms * 1e-3) / 1e12,
+                         "tap_fp32_frac": tap_flop / (ms * 1e-3) / fp32_peak,
+                         "fp32_peak_note": "nominal 148 SMs x 128 FP32 lanes x 2 x 1.965 GHz = 74.4 TFLOP/s"},
             "cgsense_setup_s": setup_s, "cgsense_10iter_ms": cg_ms, "cgsense_to_1e-4": to_tol}
 
 
@@ -868,6 +885,13 @@ def main():
                 "clocks": clk.summary()}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(traj, sens, ksp, method_lines["cg"]["iterations"])
+        if world == 1 and not args.lean:
+            # the other configs' workloads, timed in the same run: 3D
+            # kooshball NUFFT + CG-SENSE, and the batch of 512 uneven problems
+            torch.cuda.empty_cache()
+            line["kooshball3d"] = run_nufft3d(dev, 3, 2)
+            torch.cuda.empty_cache()
+            line["batch512"] = run_batch(dev, 2, 3, cpu_base=not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
 
     if world > 1:

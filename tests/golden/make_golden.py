@@ -12,6 +12,7 @@ read the .npz files and never run the reference.
     python tests/golden/make_golden.py --kb       # only the KB table and roll-off
     python tests/golden/make_golden.py --fullsize # only the C1 / C2 full-size cases
     python tests/golden/make_golden.py --gpu-gridding  # the reference's GPU-gridding test inputs
+    python tests/golden/make_golden.py --kooshball     # 3D kooshball at 32^3, 2 coils
 """
 
 from __future__ import annotations
@@ -181,6 +182,30 @@ def gpu_gridding_case(name="pics2d_gpu_gridding_n128"):
     print(name, {k: (np.shape(v) if np.ndim(v) else v) for k, v in out.items()})
 
 
+def kooshball_case(name="nufft3d_n32_c2"):
+    """3D golden-means kooshball at 32^3 (400 spokes x 64 samples), 2 coils:
+    the reference's nufft forward, adjoint, and its Toeplitz normal with the
+    PSF. Inputs regenerate from the seed (image) and the trajectory
+    generator; only outputs and checksums are stored."""
+    seed = 20261206
+    rng = np.random.default_rng(seed)
+    traj = synth.kooshball_traj(32, 400)
+    img = cplx(rng, (32, 32, 32, 2))
+    ksp = cplx(rng, (1, traj.shape[1], traj.shape[2], 2))
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "t"), traj)
+        writecfl(os.path.join(d, "x"), img)
+        writecfl(os.path.join(d, "y"), ksp)
+        run("nufft", "t", "x", "k", cwd=d)
+        run("nufft", "-a", "-x32:32:32", "t", "y", "a", cwd=d)
+        run("refnormal", "t", "x", "n", "p", cwd=d)
+        out = dict(seed=np.int64(seed), img_sha256=sha256(img), ksp_sha256=sha256(ksp),
+                   fwd=readcfl(os.path.join(d, "k")), adj=readcfl(os.path.join(d, "a")),
+                   normal=readcfl(os.path.join(d, "n")))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, {k: np.shape(v) for k, v in out.items()})
+
+
 def fullsize_cases():
     """The configs' own sizes. C1: 256^2 image, 402 golden-angle spokes x 512
     samples, forward then adjoint of the forward's output. C2: 256^2, 16
@@ -275,6 +300,9 @@ def main():
     if "--gpu-gridding" in sys.argv:
         gpu_gridding_case()
         return
+    if "--kooshball" in sys.argv:
+        kooshball_case()
+        return
     rng = np.random.default_rng(20261203)
     with tempfile.TemporaryDirectory() as d:
         run("traj", "-r", "-G", "-x64", "-o2", "-y24", "t", cwd=d)
@@ -296,6 +324,7 @@ def main():
     kb_case()
     fullsize_cases()
     gpu_gridding_case()
+    kooshball_case()
 
 
 if __name__ == "__main__":

@@ -196,3 +196,22 @@ def test_kb_table_bitwise():
     for n in ROLL_SIDES:
         r = orc.rolloff_axis(n, 2.0, 6.0, beta).astype(np.float32)
         assert np.array_equal(r.view(np.uint32), g[f"roll_{n}"].view(np.uint32)), n
+
+
+def test_kooshball_32_two_coils():
+    """The 3D golden-means kooshball (32^3, 400 x 64, 2 coils): oracle forward,
+    adjoint and Toeplitz normal against the reference's nufft / refnormal
+    (inputs regenerated from the fixture's seed and checked by checksum)."""
+    import hashlib
+    from bart_b200 import synth
+    g = golden("nufft3d_n32_c2")
+    rng = np.random.default_rng(int(g["seed"]))
+    traj = synth.kooshball_traj(32, 400)
+    img = (rng.standard_normal((32, 32, 32, 2)) + 1j * rng.standard_normal((32, 32, 32, 2))).astype(np.complex64)
+    ksp = (rng.standard_normal((1, 64, 400, 2)) + 1j * rng.standard_normal((1, 64, 400, 2))).astype(np.complex64)
+    for a, key in ((img, "img_sha256"), (ksp, "ksp_sha256")):
+        assert hashlib.sha256(np.ascontiguousarray(a).tobytes(order="F")).hexdigest() == str(g[key])
+    o = orc.NufftOracle(traj.real.reshape(3, -1, order="F"), (32, 32, 32))
+    assert rel(o.forward(img), g["fwd"].reshape(-1, 2, order="F")) < OPS_TOL
+    assert rel(o.adjoint(ksp.reshape(-1, 2, order="F")), g["adj"].reshape(32, 32, 32, 2, order="F")) < OPS_TOL
+    assert rel(o.normal_toeplitz(img), g["normal"].reshape(32, 32, 32, 2, order="F")) < OPS_TOL
