@@ -400,6 +400,10 @@ static int launch_cols_LB(const float2* in, long ies, long ios, int n_in, int wr
 	const float2* tw;
 	TRY(get_twiddles(L, &tw));
 	size_t smem = pass_smem(L, B);
+
+	if ((d.n == L) && cols_double_buffered(MODE, false, L, B))
+		smem += sizeof(float2) * (size_t)L * (size_t)smem_stride(B);	// the second exchange buffer
+
 	auto kern = (d.n == L) ? k_cols<L, B, MODE, false> : k_cols<L, B, MODE, true>;
 	TRY(prep_kernel(kern, smem));
 
@@ -617,6 +621,19 @@ static int cols(int n, int mode, const float2* in, long ies, long ios, int n_in,
 
 	while ((B > std::max(4, 256 / L)) && (B > W))
 		B /= 2;
+
+	// the double-buffered Toeplitz pass: two blocks of 8 sequences per SM
+	// overlap one another's barriers (measured faster than one block of 16)
+	if ((2 == mode) && (B > 8) && (d.n == L) && cols_double_buffered(2, false, L, 8))
+		B = 8;
+
+	if (const char* e = getenv("BNUFFT_COLS_B")) {	// tuning knob: sequences per block (4, 8, 16)
+
+		int b = atoi(e);
+
+		if (((4 == b) || (8 == b) || (16 == b)) && (b * L / 8 <= 1024) && (b * L / 8 >= 32))
+			B = b;
+	}
 
 	if (0 == mode)
 		DISPATCH_LB(L, B, (launch_cols_LB<LL, BB, 0>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out, wrap_out, W, O, psf, pes, pmod, pos, done, st, d)))

@@ -271,6 +271,83 @@ __device__ __forceinline__ void fft_regs(float2 (&v)[8], float2* s, const float2
 	fft_tail<L, LAY, 8, INV>(v, s, b, jt, tw);
 }
 
+// Double-buffered form for transforms of three stages (L = 128, 256, 512):
+// stage 1 writes s, stage 2 reads s and writes s2, stage 3 reads s2. Each
+// stage writes a buffer that no thread reads any more (the other one was
+// read in the stage before, which every thread finished before the last
+// barrier), so one barrier per exchange suffices and the transform needs no
+// barrier on entry: two transforms in a row (forward, then inverse) are
+// safe, since the second one's stage 1 writes s, last read in the first
+// one's stage 2. Same arithmetic as fft_regs, so the same results.
+template <int L, typename LAY, int Ns, bool INV>
+__device__ __forceinline__ void fft_tail_db(float2 (&v)[8], const float2* sr, float2* sw, int b, int jt,
+		const float2* tw)
+{
+	constexpr int REM = L / Ns;
+	constexpr int R = (REM >= 8) ? 8 : REM;
+	constexpr int NB = L / R;
+	constexpr int T = L / 8;
+	constexpr int PER = NB / T;
+	constexpr bool LAST = (Ns * R == L);
+
+	float2 u[PER][R];
+
+#pragma unroll
+	for (int q = 0; q < PER; q++) {
+#pragma unroll
+		for (int i = 0; i < R; i++)
+			u[q][i] = sr[LAY::idx(jt + q * T + i * NB, b)];
+	}
+
+#pragma unroll
+	for (int q = 0; q < PER; q++) {
+
+		int j = jt + q * T;
+		int k = j % Ns;
+		twiddle<L, Ns, R, INV>(u[q], k, tw);
+		butterfly<R, INV>(u[q]);
+
+		if constexpr (LAST) {
+#pragma unroll
+			for (int i = 0; i < R; i++)
+				v[q + PER * i] = u[q][i];
+
+		} else {
+
+			int idxD = (j / Ns) * Ns * R + k;
+#pragma unroll
+			for (int i = 0; i < R; i++)
+				sw[LAY::idx(idxD + i * Ns, b)] = u[q][i];
+		}
+	}
+
+	if constexpr (!LAST) {
+
+		__syncthreads();
+		fft_tail_db<L, LAY, Ns * R, INV>(v, sw, const_cast<float2*>(sr), b, jt, tw);
+	}
+}
+
+template <int L, typename LAY, bool INV>
+__device__ __forceinline__ void fft_regs_db(float2 (&v)[8], float2* s, float2* s2, const float2* tw,
+		bool half_in = false)
+{
+	static_assert((L >= 128) && (L <= 512), "three-stage lengths only");
+	const int b = LAY::seq();
+	const int jt = LAY::jt();
+
+	if (half_in)
+		dft8_half<INV>(v);
+	else
+		butterfly<8, INV>(v);
+#pragma unroll
+	for (int i = 0; i < 8; i++)
+		s[LAY::idx(8 * jt + i, b)] = v[i];
+	__syncthreads();
+
+	fft_tail_db<L, LAY, 8, INV>(v, s, s2, b, jt, tw);
+}
+
 // stage-1 position of register m for this thread
 template <int L, typename LAY>
 __device__ __forceinline__ int reg_pos(int m) { return LAY::jt() + (L / 8) * m; }

@@ -427,6 +427,14 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 // One block: B columns of one outer index, B*L/8 threads; grid (ceil(W/B), O).
 // Global loads go straight into the first FFT stage's registers and results
 // leave from the last stage's registers (B consecutive columns per access).
+// the Toeplitz column pass of three-stage power-of-two lengths keeps two
+// exchange buffers when they fit (fft_regs_db)
+__host__ __device__ constexpr bool cols_double_buffered(int MODE, bool BLUE, int L, int B)
+{
+	return (2 == MODE) && !BLUE && (L >= 128) && (L <= 512)
+		&& ((2 * L * (B | 1) + L) * 8 <= 200 * 1024);
+}
+
 template <int L, int B, int MODE, bool BLUE>
 __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (B * L / 8) : 1) k_cols(const float2* __restrict__ in, long ies, long ios, int n_in, int wrap_in,
 		float2* __restrict__ out, long oes, long oos, int n_out, int wrap_out,
@@ -436,9 +444,10 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 	using LAY = ColLayout<L, B>;
 	const int dn = BLUE ? d.n : L;	// logical DFT length (compile-time for the FFT itself)
 	constexpr int NT = B * L / 8;
+	constexpr bool DB = cols_double_buffered(MODE, BLUE, L, B);
 	extern __shared__ float2 smem[];
 	float2* s = smem;
-	float2* tw = smem + LAY::SMEM;
+	float2* tw = smem + (DB ? 2 : 1) * LAY::SMEM;
 
 	if (done && *done)
 		return;
@@ -460,8 +469,22 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		v[m] = (valid && (n < n_in)) ? inp[n * ies] : make_float2(0.f, 0.f);
 	}
 
-	// the twiddle table must be complete before the first stage reads it
-	if constexpr (MODE == 1) {
+	if constexpr (DB) {	// Toeplitz with double-buffered exchanges; the PSF column loads first
+
+		const float2* pp = psf + (o % pmod) * pos + cx;
+		float2 pv[8];
+#pragma unroll
+		for (int m = 0; m < 8; m++)
+			pv[m] = valid ? pp[reg_pos<L, LAY>(m) * pes] : make_float2(0.f, 0.f);
+
+		fft_regs_db<L, LAY, false>(v, s, s + LAY::SMEM, tw, wrap_in && (2 * n_in == L));
+#pragma unroll
+		for (int m = 0; m < 8; m++)
+			v[m] = cmul(v[m], pv[m]);
+
+		fft_regs_db<L, LAY, true>(v, s, s + LAY::SMEM, tw);
+
+	} else if constexpr (MODE == 1) {	// the twiddle table must be complete before the first stage reads it
 
 		dft_regs<L, LAY, true, BLUE>(v, s, tw, d);
 
@@ -470,7 +493,7 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 		dft_regs<L, LAY, false, BLUE>(v, s, tw, d, wrap_in && (2 * n_in == L));
 	}
 
-	if constexpr (MODE == 2) {
+	if constexpr ((MODE == 2) && !DB) {
 
 		const float2* pp = psf + (o % pmod) * pos + cx;
 #pragma unroll
