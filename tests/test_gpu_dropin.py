@@ -1,0 +1,81 @@
+"""The drop-in, compiled: the reference's own `nufft` and `pics` tools built
+from its sources with their nufft_create2() call sites bound to the adapter
+(oracle/refbuild/nufft_bnufft.c), which builds the reference's linop on the
+library's C ABI. The reference's host code (option parsing, .cfl I/O, the
+maps chain, data scaling, its CPU CG) then drives the GPU NUFFT through
+lop_fun_t callbacks. Outputs are compared with the reference's own CPU
+results on the golden fixtures: 1e-5 per operator apply, 1e-4 for
+reconstructions.
+
+The binaries (oracle/_ref/bin/{nufft,pics}_bnufft) are built by
+`make -f oracle/refbuild/Makefile` after `python -m bart_b200.build`.
+"""
+
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from bart_b200.cfl import readcfl, writecfl
+from conftest import ROOT, golden, rel
+
+pytestmark = pytest.mark.gpu
+
+BIN = os.path.join(ROOT, "oracle", "_ref", "bin")
+
+
+def _tool(name):
+    exe = os.path.join(BIN, name)
+    if not os.path.exists(exe):
+        pytest.skip(f"{name} not built (make -f oracle/refbuild/Makefile)")
+    return exe
+
+
+def _run(d, exe, *args):
+    r = subprocess.run([exe] + list(args), cwd=d, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    return r
+
+
+def test_dropin_nufft_forward_adjoint():
+    exe = _tool("nufft_bnufft")
+    g = golden("nufft2d_n64")
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "t"), g["traj"])
+        writecfl(os.path.join(d, "x"), g["img"])
+        writecfl(os.path.join(d, "y"), g["ksp"])
+        _run(d, exe, "t", "x", "k")
+        _run(d, exe, "-a", "-x64:64:1", "t", "y", "a")
+        assert rel(readcfl(os.path.join(d, "k")), g["fwd"]) < 1e-5
+        assert rel(readcfl(os.path.join(d, "a")), g["adj"]) < 1e-5
+
+
+def test_dropin_nufft_inverse():
+    """bart nufft -i: the reference's lsqr/CG on the library's Toeplitz normal."""
+    exe = _tool("nufft_bnufft")
+    g = golden("inverse2d_n32_coils3")
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "t"), g["traj"])
+        writecfl(os.path.join(d, "k"), g["ksp"])
+        for key, args in [("inv_m5", ["-m5"]), ("inv_m5_l", ["-m5", "-l0.1"])]:
+            _run(d, exe, "-i", "-x32:32:1", *args, "t", "k", "o")
+            assert rel(readcfl(os.path.join(d, "o")), g[key]) < 1e-5, key
+
+
+@pytest.mark.parametrize("key,args,tol", [("x5_w1", ["-i5", "-w1"], 1e-5),
+                                          ("x5_w1_notoep", ["-i5", "-w1", "--no-toeplitz"], 1e-5),
+                                          ("x30", ["-i30"], 1e-4)])
+def test_dropin_pics(key, args, tol):
+    """bart pics -l2 -r0.01 -t: SENSE model, scaling and CG of the reference
+    on the library's NUFFT linop (Toeplitz normal or forward/adjoint)."""
+    exe = _tool("pics_bnufft")
+    g = golden("pics2d_n64_c4")
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "t"), g["traj"])
+        writecfl(os.path.join(d, "s"), g["sens"])
+        writecfl(os.path.join(d, "k"), g["ksp"])
+        r = _run(d, exe, "-d4", "-l2", "-r0.01", *args, "-t", "t", "k", "s", "o")
+        assert "libbnufft" in r.stderr + r.stdout      # the adapter built the NUFFT
+        assert rel(readcfl(os.path.join(d, "o")), g[key]) < tol
