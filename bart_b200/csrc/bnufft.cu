@@ -733,6 +733,7 @@ struct Bins {
 	int* work_start = nullptr;	// [ntiles + 1]; work_start[ntiles] = work items
 	unsigned char* multi = nullptr;	// [ntiles]
 	long nwork_max = 0;		// upper bound of work items (launch size)
+	int cand = 512;			// candidates per work item
 	float4* foot = nullptr;		// [M][FOOT_F4] footprints of the sorted samples
 	float2* kperm = nullptr;	// [M][kperm_c] k-space in bin order (large problems)
 	long kperm_c = 0;
@@ -1061,14 +1062,14 @@ static int grid_adj(OpCtx& op, const float2* ksp, long C, float2* grid, cudaStre
 
 		Bins& b = op.bins;
 		const GridGeom gg = grid_geom(op.g);
-		TileWork tw = { b.bin_start, b.work_tile, b.work_chunk, b.work_start + b.ntiles, b.multi, b.foot };
+		TileWork tw = { b.bin_start, b.work_tile, b.work_chunk, b.work_start + b.ntiles, b.multi, b.foot, b.cand };
 		int sorted = 0;
 
-		// k-space that does not stay in L2: one pass into bin order, so the
-		// tiles read their samples' values coalesced
-		if ((long)sizeof(float2) * op.g.M * C > (64L << 20)) {
+		// k-space in bin order (one pass), so the tiles read their samples'
+		// values coalesced
+		if (C > 1) {
 
-			if (b.kperm_c < C) {
+			if (b.kperm_c < C) {	// more channels than the plan was made for (not while capturing)
 
 				if (b.kperm)
 					cudaFreeAsync(b.kperm, st);
@@ -1252,11 +1253,12 @@ static int build_bins(OpCtx& op, cudaStream_t st)
 	// and, on periodic grids, room for an unambiguous footprint offset
 	b.tg_cfg = -1;
 
-	// measured on B200: it wins for 3D multi-channel problems (8-coil 128^3
-	// kooshball: 10.2 against 28.3 ms), while single-channel and 2D problems
-	// (little work per candidate sample) are faster with the global-atomic
-	// scatter; BNUFFT_GRIDDING=lines selects it everywhere
-	const bool tg_want = (2 == gridding_kind()) ? ((g.G[2] > 1) && (op.coils >= 2)) : (3 == gridding_kind());
+	// measured on B200: it wins for multi-channel problems (8-coil 128^3
+	// kooshball: 10.5 against 28.2 ms; 16-coil 256^2 radial: 122 against
+	// 144 us), while single-channel problems (little work per candidate
+	// sample) are faster with the global-atomic scatter (256^2, 402 spokes:
+	// 55 against 122 us); BNUFFT_GRIDDING=lines selects it everywhere
+	const bool tg_want = (2 == gridding_kind()) ? (op.coils >= 2) : (3 == gridding_kind());
 
 	if ((6.f == g.width) && (0 == op.bin_edge) && tg_want && (g.G[0] > 1) && (g.G[1] > 1)) {
 
@@ -1358,7 +1360,7 @@ static int build_bins(OpCtx& op, cudaStream_t st)
 	b.cc = (int)std::max(1L, std::min(8L, (110L * 1024) / (long)(sizeof(float2) * bg.ncells)));
 
 	// work items of the output-stationary scatter: each tile's candidates
-	// (the samples of its neighbour bins) in chunks of TG_CAND
+	// (the samples of its neighbour bins) in chunks of b.cand
 	if (b.tg_cfg >= 0) {
 
 		const long nt = nbins;
@@ -1369,7 +1371,12 @@ static int build_bins(OpCtx& op, cudaStream_t st)
 		b.ntiles = nt;
 		b.bin_start = bin_start;
 		bin_start = nullptr;	// kept by the plan
-		b.nwork_max = nt + (M * nneigh + TG_CAND - 1) / TG_CAND;
+		b.cand = (g.G[2] > 1) ? 1024 : 256;	// measured best (256..1024 tried)
+
+		if (const char* e = getenv("BNUFFT_GRID_CAND"))	// tuning knob: candidates per work item
+			b.cand = std::max(64, std::min(4096, atoi(e)));
+
+		b.nwork_max = nt + (M * nneigh + b.cand - 1) / b.cand;
 
 		if (b.nwork_max >= (1L << 31))
 			return fail(BNUFFT_ERR_UNSUPPORTED, "gridding: %ld work items", b.nwork_max);
@@ -1380,7 +1387,7 @@ static int build_bins(OpCtx& op, cudaStream_t st)
 		CUDA_TRY(cudaMallocAsync(&b.work_tile, sizeof(int) * b.nwork_max, st));
 		CUDA_TRY(cudaMallocAsync(&b.work_chunk, sizeof(int) * b.nwork_max, st));
 		CUDA_TRY(cudaMemsetAsync(nwork + nt, 0, sizeof(int), st));
-		k_tile_cand<<<vec_blocks(nt), RED_THREADS, 0, st>>>(b.bin_start, bg, g.periodic, nt, nwork, b.multi);
+		k_tile_cand<<<vec_blocks(nt), RED_THREADS, 0, st>>>(b.bin_start, bg, g.periodic, nt, b.cand, nwork, b.multi);
 		LAUNCHED();
 		CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, wtmp_bytes, nwork, b.work_start, (int)(nt + 1), st));
 		CUDA_TRY(cudaMallocAsync(&wtmp, wtmp_bytes, st));
@@ -1397,6 +1404,15 @@ static int build_bins(OpCtx& op, cudaStream_t st)
 		CUDA_TRY(cudaMallocAsync(&b.foot, sizeof(float4) * FOOT_F4 * M, st));
 		k_foot<<<vec_blocks(M, 128, 8 * 148), 128, 0, st>>>(b.traj, M, grid_geom(g), op.kb, b.foot);
 		LAUNCHED();
+
+		// the bin-ordered k-space of the applies, allocated here so that
+		// applies allocate nothing (their solves can then be captured into
+		// graphs and nested as child graphs)
+		if (op.coils > 1) {
+
+			CUDA_TRY(cudaMallocAsync(&b.kperm, sizeof(float2) * M * op.coils, st));
+			b.kperm_c = op.coils;
+		}
 	}
 
 	void* frees[] = { keys, keys2, vals, counts, bin_start, nsub, tmp };

@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_atomic(const float4* _
 // outside the sample's y/z window skip it.
 //
 // Work items: a tile's candidates (the samples of its neighbourhood, in a
-// fixed bin order) are cut into chunks of TG_CAND; tiles with one chunk
+// fixed bin order) are cut into chunks (TileWork.cand); tiles with one chunk
 // write their cells with plain stores (empty tiles write zeros, so the grid
 // needs no clearing), tiles with several chunks (the dense k-space centre)
 // add their chunks with atomics into cells that k_zero_tiles cleared.
@@ -592,7 +592,7 @@ __global__ void __launch_bounds__(BIN_THREADS, 2) k_grid6_atomic(const float4* _
 // grid_point_gen, src/noncart/grid.c:403-465) and the combined weight the
 // same float32 product ((1 * wz) * wy) * wx.
 
-enum { TG_CAND = 512, TG_WARPS = 4 };
+enum { TG_WARPS = 4 };
 
 struct TileWork {
 
@@ -602,6 +602,7 @@ struct TileWork {
 	const int* nwork_dev;		// number of work items
 	const unsigned char* multi;	// [ntiles] 1 if the tile has several work items
 	const float4* foot;		// [M][FOOT_F4] footprints of the sorted samples
+	int cand;			// candidates per work item
 };
 
 // Footprint record of a sorted sample (built once per trajectory by
@@ -834,8 +835,8 @@ __device__ __forceinline__ int tg_neighbour(int b, int d, int nb, int periodic)
 	return ((n < 0) || (n >= nb)) ? -1 : n;
 }
 
-// candidates per tile and the work items (chunks of TG_CAND) per tile
-__global__ void k_tile_cand(const int* __restrict__ bin_start, BinGeom bg, int periodic, long ntiles,
+// candidates per tile and the work items (chunks of cand) per tile
+__global__ void k_tile_cand(const int* __restrict__ bin_start, BinGeom bg, int periodic, long ntiles, int cand,
 		int* __restrict__ nwork, unsigned char* __restrict__ multi)
 {
 	for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += (long)gridDim.x * blockDim.x) {
@@ -871,7 +872,7 @@ __global__ void k_tile_cand(const int* __restrict__ bin_start, BinGeom bg, int p
 			}
 		}
 
-		const long w = (n + TG_CAND - 1) / TG_CAND;
+		const long w = (n + cand - 1) / cand;
 		nwork[t] = (int)((w < 1) ? 1 : w);
 		multi[t] = (w > 1) ? 1 : 0;
 	}
@@ -928,7 +929,7 @@ __global__ void __launch_bounds__(32 * TG_WARPS, 4) k_grid6_tiles(const int* __r
 		for (int c = 0; c < CT; c++)
 			acc[i][c] = make_float2(0.f, 0.f);
 
-	const long cand0 = (long)chunk * TG_CAND, cand1 = cand0 + TG_CAND;
+	const long cand0 = (long)chunk * tw.cand, cand1 = cand0 + tw.cand;
 	const int rz = (bg.nb[2] > 1) ? 1 : 0, ry = (bg.nb[1] > 1) ? 1 : 0;
 	long off = 0;
 
@@ -959,15 +960,39 @@ __global__ void __launch_bounds__(32 * TG_WARPS, 4) k_grid6_tiles(const int* __r
 				const int i0 = s0 + (int)(a - off), i1 = s0 + (int)(e - off);
 				off += s1 - s0;
 
+				// rounds of 32 candidates; the next round's footprint start
+				// and coil values are loaded while this round accumulates
+				float4 f0n = make_float4(0.f, 0.f, 0.f, 0.f);
+				float2 vn[CW];
+
+				auto fetch = [&](int i) {
+					if (i < i1) {
+
+						f0n = tw.foot[(long)i * FOOT_F4];
+						const long m = ksp_sorted ? (long)i : (long)perm[i];
+#pragma unroll
+						for (int c = 0; c < CW; c++)
+							vn[c] = (cw0 + c < C) ? ksp[m + M * (cw0 + c)] : make_float2(0.f, 0.f);
+					}
+				};
+
+				fetch(i0 + lane);
+
 				for (int base = i0; base < i1; base += 32) {
 
 					const int i = base + lane;
+					const float4 f0 = f0n;
+					float2 vc[CW];
+#pragma unroll
+					for (int c = 0; c < CW; c++)
+						vc[c] = vn[c];
+
+					fetch(i + 32);
 					bool hit = false;
 					int lx = 0, ly = 0, lz = 0;
 
 					if (i < i1) {
 
-						const float4 f0 = tw.foot[(long)i * FOOT_F4];
 						lx = foot_rel(__float_as_int(f0.x), ox, g.G[0], g.periodic);
 						ly = foot_rel(__float_as_int(f0.y), oy, g.G[1], g.periodic);
 						lz = foot_rel(__float_as_int(f0.z), oz, g.G[2], g.periodic);
@@ -987,10 +1012,9 @@ __global__ void __launch_bounds__(32 * TG_WARPS, 4) k_grid6_tiles(const int* __r
 						d.rx = lx;
 						d.ry = ly;
 						d.rz = lz;
-						const long m = ksp_sorted ? (long)i : (long)perm[i];
 #pragma unroll
 						for (int c = 0; c < CW; c++)
-							d.v[c] = (cw0 + c < C) ? ksp[m + M * (cw0 + c)] : make_float2(0.f, 0.f);
+							d.v[c] = vc[c];
 					}
 
 					__syncwarp();
