@@ -310,6 +310,50 @@ def run_nufft3d(dev, steps, warmup, spokes=20000):
             "cgsense_setup_s": setup_s, "cgsense_10iter_ms": cg_ms, "cgsense_to_1e-4": to_tol}
 
 
+def run_scatter(dev, steps=5, warmup=3):
+    """Adjoint gridding (the scatter) alone, per kernel variant in force
+    (BNUFFT_GRIDDING: default, lines, atomic, tiles), CUDA-event time per
+    launch of the "grid" class on four problems: 256^2 with 16 coils and 96
+    spokes x 512 (the CG-SENSE bench problem), 256^2 single-coil with 402
+    spokes (config 1), the 2D PSF's periodic 1024^2 grid (2 x trajectory, one
+    channel), and the 8-coil 128^3 kooshball with 20000 spokes x 256."""
+    import ctypes
+    import torch
+    from bart_b200 import _lib, synth
+    from bart_b200.nufft import NufftConf, nufft_create2
+    lib = _lib.load()
+
+    def d(a):
+        return torch.from_numpy(np.asfortranarray(a).ravel(order="F").copy()).to(dev)
+
+    out = {"workload": "scatter", "variant": os.environ.get("BNUFFT_GRIDDING", "default"), "unit": "us per launch"}
+    for name, N, sp, C, nd, per in (("cgsense2d_256_c16_s96", 256, 96, 16, 2, 0), ("nufft2d_256_c1_s402", 256, 402, 1, 2, 0),
+                                    ("psf2d_1024_periodic", 512, 96, 1, 2, 1),
+                                    ("kooshball3d_128_c8_s20000", 128, 20000, 8, 3, 0)):
+        t = synth.radial_traj(N, sp) if nd == 2 else synth.kooshball_traj(N, sp)
+        if per:
+            t = t * 2
+        M = t.shape[1] * t.shape[2]
+        cd = [N, N, 1 if nd == 2 else N, C]
+        kd = [1, t.shape[1], t.shape[2], C]
+        op = nufft_create2(kd, cd, list(t.shape), d(t), conf=NufftConf(toeplitz=False, periodic=bool(per)))
+        y = torch.randn(M * C, dtype=torch.complex64, device=dev)
+        a = torch.empty(int(np.prod(cd)), dtype=torch.complex64, device=dev)
+        for _ in range(warmup):
+            op.adjoint(y, a)
+        torch.cuda.synchronize()
+        lib.bnufft_prof_start(b"grid")
+        for _ in range(steps):
+            op.adjoint(y, a)
+        ms, n = ctypes.c_double(), ctypes.c_long()
+        lib.bnufft_prof_stop(ctypes.byref(ms), ctypes.byref(n))
+        out[name] = ms.value * 1e3 / max(1, n.value)
+        op.free()
+        del y, a
+        torch.cuda.empty_cache()
+    return out
+
+
 def toeplitz_normal_torch(x_yx, maps_cyx, P_yx):
     """S^H F^H P F S x with torch.fft (cuFFT on a GPU): x [Y, X], maps
     [C, Y, X], P the 2N x 2N PSF in DFT order, [y][x], scaled 1/npix. Pixel
@@ -668,7 +712,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "batch"])
+    ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "batch", "scatter"])
     ap.add_argument("--spokes", type=int, default=20000, help="nufft3d: kooshball spokes")
     ap.add_argument("--methods", default="fcg_padded,fcg_circulant,cg,fcg_learned",
                     help="solvers to time (cgsense2d); the first is the headline")
@@ -703,6 +747,11 @@ def main():
     if args.workload == "nufft3d":
         if rank == 0:
             print(json.dumps(run_nufft3d(dev, args.steps, args.warmup, args.spokes)), flush=True)
+        return
+
+    if args.workload == "scatter":
+        if rank == 0:
+            print(json.dumps(run_scatter(dev, args.steps, args.warmup)), flush=True)
         return
 
     if args.workload == "batch":
