@@ -25,7 +25,8 @@ class PicsConfC(ctypes.Structure):
     _fields_ = [("lambda_", ctypes.c_float), ("maxiter", ctypes.c_int), ("tol", ctypes.c_float),
                 ("scaling", ctypes.c_float), ("rescale", ctypes.c_int), ("toeplitz", ctypes.c_int),
                 ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int), ("bin", ctypes.c_int),
-                ("precond", ctypes.c_int), ("ref_scalars", ctypes.c_int)]
+                ("precond", ctypes.c_int), ("ref_scalars", ctypes.c_int),
+                ("net_iters", ctypes.c_int)]
 
 
 _lib = None
@@ -87,6 +88,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     sig("bnufft_precnet_train_step", i, vp, vp, vp, ctypes.c_long, ctypes.c_long, ctypes.c_long, ctypes.c_float,
         ctypes.POINTER(ctypes.c_double), vp, vp)
     sig("bnufft_precnet_backward", i, vp, vp, vp, ctypes.c_long, ctypes.c_long, ctypes.c_long, ctypes.c_float, vp, vp)
+    sig("bnufft_precnet_status", i, vp, ctypes.POINTER(i), vp)
     sig("bnufft_precnet_free", None, vp)
     sig("bnufft_calc_beta", ctypes.c_double, ctypes.c_float, ctypes.c_float)
     sig("bnufft_kb_precompute", i, ctypes.c_double, i, fp)

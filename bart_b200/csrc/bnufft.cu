@@ -25,6 +25,9 @@
 #include "precnet.cuh"
 #include "nudft.cuh"
 #include "precond_cluster.cuh"
+#include "precnet_tc.cuh"
+
+#include <cudaTypedefs.h>
 
 using namespace bn;
 
@@ -633,6 +636,31 @@ static int cols(int n, int mode, const float2* in, long ies, long ios, int n_in,
 
 		if (((4 == b) || (8 == b) || (16 == b)) && (b * L / 8 <= 1024) && (b * L / 8 >= 32))
 			B = b;
+	}
+
+	// 512-point Toeplitz columns of several images (coils): the two-stage
+	// transform kernel, 16 threads per column (BNUFFT_TOE512=0 keeps the
+	// three-stage k_cols, whose 64 threads per column suit the single-image
+	// passes better: 30.7 vs 28.5 us per 16-coil launch, but a slower solve
+	// when the preconditioner's one image also takes the new kernel)
+	if ((2 == mode) && (512 == L) && (d.n == L) && (O >= 4) && (O <= 65535)) {
+
+		const char* e = getenv("BNUFFT_TOE512");
+
+		if (!(e && (0 == strcmp(e, "0")))) {
+
+			const float2* tw;
+			TRY(get_twiddles(L, &tw));
+			const size_t smem = sizeof(float2) * (size_t)L * (TOE512_B + 1);
+			TRY(prep_kernel(k_cols_toe512, smem));
+			dim3 grid((unsigned)((W + TOE512_B - 1) / TOE512_B), (unsigned)O);
+			cudaEvent_t pe = prof_begin("cols_toeplitz", st);
+			k_cols_toe512<<<grid, TOE512_B * 16, smem, st>>>(in, ies, ios, n_in, wrap_in, out, oes, oos, n_out,
+					wrap_out, W, psf, pes, pmod, pos, tw, done);
+			prof_end(pe, st);
+			LAUNCHED();
+			return BNUFFT_OK;
+		}
 	}
 
 	if (0 == mode)
@@ -2639,6 +2667,9 @@ struct bnufft_precnet_s {
 	float* part = nullptr;
 	double* loss_part = nullptr;
 	double* loss_host = nullptr;	// pinned
+	int* tc_status = nullptr;	// tensor-core conv error word (1: a wait ran out)
+	bf16* wf_tc = nullptr;		// wf and wt in the tensor-core kernel's B-plane order
+	bf16* wt_tc = nullptr;
 };
 
 static const int NET_N = NetLayout::total();
@@ -2648,12 +2679,88 @@ static int net_pack(bnufft_precnet_s* n, cudaStream_t st)
 {
 	k_net_pack<<<(NET_N + 255) / 256, 256, 0, st>>>(n->params, n->pr, n->wf, n->wt);
 	LAUNCHED();
+	k_net_pack_tc<<<(4 * 9216 + 255) / 256, 256, 0, st>>>(n->wf, n->wf_tc);
+	LAUNCHED();
+	k_net_pack_tc<<<(4 * 9216 + 255) / 256, 256, 0, st>>>(n->wt, n->wt_tc);
+	LAUNCHED();
 	return BNUFFT_OK;
 }
 
 static dim3 net_tiles(int X, int Y, long nimg)
 {
 	return dim3((unsigned)((X + NET_TILE_X - 1) / NET_TILE_X), (unsigned)((Y + NET_TILE_Y - 1) / NET_TILE_Y), (unsigned)nimg);
+}
+
+// cuTensorMapEncodeTiled from the driver (no link against libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+	static std::once_flag once;
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	std::call_once(once, [] {
+		void* p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+
+		if ((cudaSuccess == cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q))
+				&& (cudaDriverEntryPointSuccess == q))
+			fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+	});
+	return fn;
+}
+
+static int sm_count()
+{
+	int dev, n = 0;
+	CUDA_TRY(cudaGetDevice(&dev));
+	CUDA_TRY(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+	return n;
+}
+
+// One 32 -> 32 layer: the tcgen05 kernel (default; work tiles of two rows
+// of 128 pixels) or the mma.sync kernel (BNUFFT_NET_TC=0). wtc: the layer's
+// weights in the tensor-core kernel's plane order; w: the same in the
+// mma.sync kernel's order.
+template <int MODE>
+static int launch_conv32(const bnufft_precnet_s* n, const bf16* in, const bf16* w, const bf16* wtc,
+		const float* bias, const bf16* mask, bf16* out, int X, int Y, long nimg, const int* done, cudaStream_t st)
+{
+	const char* e = getenv("BNUFFT_NET_TC");
+	constexpr int R = 2;
+
+	if (!(e && (0 == strcmp(e, "0")))) {
+
+		auto enc = tensor_map_encoder();
+
+		if (!enc)
+			return fail(BNUFFT_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+
+		// activations [nimg][Y][X][32] bf16; box {8 channels, 130 pixels, R + 2 rows, 1 image}
+		CUtensorMap map;
+		const cuuint64_t gdim[4] = { (cuuint64_t)NET_C, (cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)nimg };
+		const cuuint64_t gstr[3] = { (cuuint64_t)NET_C * 2, (cuuint64_t)NET_C * 2 * X, (cuuint64_t)NET_C * 2 * X * Y };
+		const cuuint32_t box[4] = { 8, TC_HX, R + 2, 1 };
+		const cuuint32_t estr[4] = { 1, 1, 1, 1 };
+		CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void*)in, gdim, gstr, box, estr,
+				CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+				CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+
+		if (CUDA_SUCCESS != r)
+			return fail(BNUFFT_ERR_CUDA, "cuTensorMapEncodeTiled: error %d", (int)r);
+
+		const size_t smem = conv_tc_smem(R);
+		TRY(prep_kernel(k_conv32_tc<MODE, R>, smem));
+		const long tiles = (long)((X + TC_M - 1) / TC_M) * ((Y + R - 1) / R) * nimg;
+		const int per_sm = (int)std::max<size_t>(1, (227 * 1024) / (smem + 1024));
+		const long blocks = std::min<long>(tiles, (long)sm_count() * std::min(per_sm, 4));
+		k_conv32_tc<MODE, R><<<(unsigned)blocks, 128, smem, st>>>(map, wtc, bias, mask, out, X, Y, (int)nimg, done,
+				n->tc_status);
+		LAUNCHED();
+		return BNUFFT_OK;
+	}
+
+	TRY(prep_kernel(k_conv32<MODE>, NET_CONV_SMEM));
+	k_conv32<MODE><<<net_tiles(X, Y, nimg), NET_THREADS, NET_CONV_SMEM, st>>>(in, w, bias, mask, out, X, Y, done);
+	LAUNCHED();
+	return BNUFFT_OK;
 }
 
 // Forward through all six layers: act[0..4] (layer 1-5 outputs, bf16) and
@@ -2673,10 +2780,8 @@ static int net_forward(const bnufft_precnet_s* n, const float2* in, int X, int Y
 
 	for (int l = 1; l <= 4; l++) {
 
-		TRY(prep_kernel(k_conv32<0>, NET_CONV_SMEM));
-		k_conv32<0><<<net_tiles(X, Y, nimg), NET_THREADS, NET_CONV_SMEM, st>>>(acts[l - 1], n->wf + (l - 1) * 9216,
-				pr + NetLayout::boff(l), nullptr, acts[l], X, Y, done);
-		LAUNCHED();
+		TRY(launch_conv32<0>(n, acts[l - 1], n->wf + (l - 1) * 9216, n->wf_tc + (l - 1) * 9216, pr + NetLayout::boff(l),
+				nullptr, acts[l], X, Y, nimg, done, st));
 	}
 
 	k_net_out<<<pb, NET_THREADS, 0, st>>>(acts[4], X, Y, P, pr + NetLayout::woff(5), pr + NetLayout::boff(5), scale_out,
@@ -2767,6 +2872,17 @@ extern "C" int bnufft_precnet_get_params(bnufft_precnet_t n, float* params, void
 	return BNUFFT_OK;
 }
 
+extern "C" int bnufft_precnet_status(bnufft_precnet_t n, int* status, void* stream)
+{
+	if (!n || !status)
+		return fail(BNUFFT_ERR_ARG, "null argument");
+
+	cudaStream_t st = S(stream);
+	CUDA_TRY(cudaMemcpyAsync(status, n->tc_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+	CUDA_TRY(cudaStreamSynchronize(st));
+	return BNUFFT_OK;
+}
+
 extern "C" void bnufft_precnet_free(bnufft_precnet_t n)
 {
 	if (!n)
@@ -2774,7 +2890,7 @@ extern "C" void bnufft_precnet_free(bnufft_precnet_t n)
 
 	cudaDeviceSynchronize();
 	net_free_ws(n);
-	void* bufs[] = { n->params, n->pr, n->wf, n->wt, n->m, n->v, n->grad };
+	void* bufs[] = { n->params, n->pr, n->wf, n->wt, n->m, n->v, n->grad, n->tc_status, n->wf_tc, n->wt_tc };
 
 	for (void* b : bufs)
 		if (b)
@@ -2801,6 +2917,12 @@ extern "C" int bnufft_precnet_create(bnufft_precnet_t* out, const float* params,
 	al((void**)&n->grad, sizeof(float) * NET_N);
 	al((void**)&n->wf, sizeof(bf16) * 4 * 9216);
 	al((void**)&n->wt, sizeof(bf16) * 4 * 9216);
+	al((void**)&n->tc_status, sizeof(int));
+	al((void**)&n->wf_tc, sizeof(bf16) * 4 * 9216);
+	al((void**)&n->wt_tc, sizeof(bf16) * 4 * 9216);
+
+	if (cudaSuccess == e)
+		e = cudaMemset(n->tc_status, 0, sizeof(int));
 
 	if (cudaSuccess == e)
 		e = cudaMallocHost((void**)&n->loss_host, sizeof(double) * NET_LOSS_BLOCKS);
@@ -2903,10 +3025,8 @@ static int net_train(bnufft_precnet_t n, const void* in, const void* target, con
 	for (int l = 4; l >= 1; l--) {
 
 		TRY((net_wgrad<NET_C, NET_C, bf16, bf16>(n, l, n->act[l - 1], gu, x, y, nimg, st)));
-		TRY(prep_kernel(k_conv32<1>, NET_CONV_SMEM));
-		k_conv32<1><<<grid, NET_THREADS, NET_CONV_SMEM, st>>>(gu, n->wt + (l - 1) * 9216, nullptr, n->act[l - 1], gn,
-				x, y, nullptr);
-		LAUNCHED();
+		TRY(launch_conv32<1>(n, gu, n->wt + (l - 1) * 9216, n->wt_tc + (l - 1) * 9216, nullptr, n->act[l - 1], gn, x,
+				y, nimg, nullptr, st));
 		std::swap(gu, gn);
 	}
 
@@ -3071,6 +3191,7 @@ extern "C" void bnufft_pics_conf_defaults(struct bnufft_pics_conf* c)
 	c->bin = 0;
 	c->precond = 0;
 	c->ref_scalars = 1;
+	c->net_iters = 0;
 }
 
 // A^H A x (+ lam x), with optional per-block Re<x, out> partials
@@ -3131,7 +3252,7 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 	nc.bin = conf.bin;
 
 	if ((conf.precond < 0) || (conf.precond > 3))
-		return fail(BNUFFT_ERR_ARG, "precond must be 0, 1 or 2");
+		return fail(BNUFFT_ERR_ARG, "precond must be 0, 1, 2 or 3");
 
 	if (conf.precond && !conf.toeplitz)
 		return fail(BNUFFT_ERR_UNSUPPORTED, "the circulant preconditioner needs the Toeplitz normal operator");
@@ -3213,7 +3334,7 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 			const AuxStream* aux = (ps->nufft->psf_ev && (cudaSuccess == cudaGetDevice(&dev))) ? aux_stream(dev) : nullptr;
 			cudaStream_t pst = aux ? aux->st : st;
 
-			if (3 == conf.precond)
+			if ((2 == conf.precond) || (3 == conf.precond))
 				s = build_precond_pad(ps, pst);
 			else
 				s = build_precond(ps->nufft, pst);
@@ -3388,8 +3509,9 @@ static int pics_precond_pad(bnufft_pics_s* ps, const float2* r, float2* z, const
 	return s;
 }
 
-// z = M(r): the circulant preconditioner, plus (precond 2) the learned
-// correction ||M_circ(r)|| net(r / ||r||) (1 / ||r|| from the solve's
+// z = M(r): the circulant preconditioner (precond 1), the padded one
+// (precond 3), or the padded one plus the learned correction
+// ||M_pad(r)|| net(r / ||r||) (precond 2; 1 / ||r|| from the solve's
 // scalars); optional partials Re<pdot, z>
 static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
 		int* nblocks, cudaStream_t st)
@@ -3403,11 +3525,11 @@ static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const flo
 	if (!ps->net)
 		return fail(BNUFFT_ERR_ARG, "precond 2 needs a network (bnufft_pics_set_precnet)");
 
-	// z = M_circ(r) with the partials of ||z||^2, then z += ||z|| net(r / ||r||):
+	// z = M_pad(r) with the partials of ||z||^2, then z += ||z|| net(r / ||r||):
 	// flexible CG is invariant to a positive scale of z per iteration, so the
-	// network learns a scale-free correction of the circulant direction
+	// network learns a scale-free correction of the padded-circulant direction
 	int nmc = 0;
-	TRY(pics_precond_circ(ps, r, z, z, ps->mcn_part, &nmc, st));
+	TRY(pics_precond_pad(ps, r, z, z, ps->mcn_part, &nmc, st));
 
 	if (nmc > ps->max_row_blocks)
 		return fail(BNUFFT_ERR_ARG, "internal: partial arrays too small");
@@ -3831,7 +3953,7 @@ static int pics_solve(bnufft_pics_s* ps, const float2* ksp, float2* out, cudaStr
 	k_cg_init<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, ps->pbuf[1], ps->b, ps->npix, ps->rs_part);
 	LAUNCHED();
 	k_cg_start<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->rs_part, ps->nparts, ps->conf.tol, ps->conf.maxiter,
-			(0 == ps->conf.precond) && ps->conf.ref_scalars);
+			(0 == ps->conf.precond) && ps->conf.ref_scalars, ps->conf.net_iters);
 	LAUNCHED();
 
 	TRY(alloc_work(op.w, op.g, ps->C, st));

@@ -132,7 +132,8 @@ __global__ void k_cg_init(float2* __restrict__ x, float2* __restrict__ r, float2
 // f32: the plain CG's scalars in float32 as the reference keeps them:
 // eps = float(||b||) * tol and eps2 = float(eps^2) (iter2_conjgrad,
 // src/iter/iter2.c:249-254; conjgrad, src/iter/italgos.c:518-523).
-__global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float tol, int maxiter, int f32)
+__global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float tol, int maxiter, int f32,
+		int net_iters = 0)
 {
 	__shared__ double sh[32];
 	double b2 = sum_partials(part, nparts, sh);
@@ -162,6 +163,7 @@ __global__ void k_cg_start(CgScalars* st, const double* part, int nparts, float 
 		st->best_hist[0] = b2;
 		st->best_it = 0;
 		st->net_off = 0;
+		st->net_iters = net_iters;
 		st->restart_it = 0;
 		st->rnorm = (float)sqrt(b2);
 		st->rinv = (b2 > 0.) ? (float)(1. / sqrt(b2)) : 0.f;
@@ -536,6 +538,11 @@ __global__ void k_fcg_check(CgScalars* st, int it, const double* __restrict__ rs
 		}
 
 		bool stall = (j - st->best_it >= 3) || ((j >= 4) && (st->best_rs > 0.25 * st->best_hist[j % 4]));
+
+		// the learned part's iteration budget: switched off without a
+		// restart (flexible CG keeps the directions it has)
+		if ((st->net_iters > 0) && (j >= st->net_iters))
+			st->net_off = 1;
 
 		if (stall && !st->net_off) {
 

@@ -16,6 +16,7 @@
 #include <stdint.h>
 
 #include "fft_core.cuh"
+#include "fft512.cuh"
 
 namespace bn {
 
@@ -160,6 +161,7 @@ struct CgScalars {
 	int best_it;		// iteration count at best_rs
 	int net_off;		// learned preconditioner switched off (stall fallback)
 	int restart_it;		// flexible CG direction history starts here
+	int net_iters;		// learned preconditioner used in iterations < net_iters (0: no limit)
 	float rnorm;		// ||r|| of the current residual
 	float rinv;		// 1 / ||r|| (0 for r = 0)
 	float scale;		// data scaling used
@@ -520,6 +522,75 @@ __global__ void __launch_bounds__(B * L / 8, (1024 / (B * L / 8)) > 0 ? 1024 / (
 			if (n < n_out)
 				outp[n * oes] = v[m];
 		}
+	}
+}
+
+// Toeplitz column pass for 512-point columns in two-stage transforms
+// (fft512_regs): sixteen columns per block, sixteen threads per column, 32
+// elements per thread. The same positions, PSF product and crop as k_cols
+// MODE 2; one shared-memory exchange and one barrier per transform, plus the
+// barrier for the twiddle table and the one between the two transforms.
+enum { TOE512_B = 16 };
+
+__global__ void __launch_bounds__(TOE512_B * 16, 2) k_cols_toe512(const float2* __restrict__ in, long ies, long ios,
+		int n_in, int wrap_in, float2* __restrict__ out, long oes, long oos, int n_out, int wrap_out,
+		int W, const float2* __restrict__ psf, long pes, long pmod, long pos,
+		const float2* __restrict__ twg, const int* done)
+{
+	constexpr int L = 512, SB = TOE512_B;
+	extern __shared__ float2 smem[];
+	float2* s = smem;
+	float2* tw = smem + L * SB;
+
+	if (done && *done)
+		return;
+
+	for (int i = threadIdx.x; i < L; i += blockDim.x)
+		tw[i] = twg[i];
+
+	const int b = threadIdx.x % TOE512_B, t = threadIdx.x / TOE512_B;
+	const int cx = blockIdx.x * TOE512_B + b;
+	const bool valid = (cx < W);
+	const long o = blockIdx.y;
+	const float2* inp = in + o * ios + cx;
+
+	float2 v[32];
+#pragma unroll
+	for (int m = 0; m < 32; m++) {
+
+		const int p = t + 16 * m;
+		const int n = wrap_in ? unwrap_pos(p, n_in, L) : p;
+		v[m] = (valid && (n < n_in)) ? inp[n * ies] : make_float2(0.f, 0.f);
+	}
+
+	__syncthreads();	// the twiddle table is complete
+
+	if (wrap_in && (2 * n_in == L))
+		fft512_regs<false, true, SB>(v, s, tw, t, b);
+	else
+		fft512_regs<false, false, SB>(v, s, tw, t, b);
+
+	const float2* pp = psf + (o % pmod) * pos + cx;
+#pragma unroll
+	for (int m = 0; m < 32; m++)
+		if (valid)
+			v[m] = cmul(v[m], pp[(t + 16 * m) * pes]);
+
+	__syncthreads();	// every thread's stage-2 loads are done before s is rewritten
+	fft512_regs<true, false, SB>(v, s, tw, t, b);
+
+	if (!valid)
+		return;
+
+	float2* outp = out + o * oos + cx;
+#pragma unroll
+	for (int m = 0; m < 32; m++) {
+
+		const int p = t + 16 * m;
+		const int n = wrap_out ? unwrap_pos(p, n_out, L) : p;
+
+		if (n < n_out)
+			outp[n * oes] = v[m];
 	}
 }
 

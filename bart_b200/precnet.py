@@ -5,19 +5,22 @@ channels, bf16 weights, float32 accumulation) runs and trains on the GPU
 through libbnufft's own kernels (``bnufft_precnet_*``). Inside flexible CG
 (``PicsConf(precond=2)``) the preconditioner is
 
-    z = M_circ(r) + ||M_circ(r)|| net(r / ||r||)
+    z = M(r) + ||M(r)|| net(r / ||r||)
 
-where M_circ is the reference's circulant PSF preconditioner
-(src/noncart/precond.c:48-164). With a zero last layer the network adds
-nothing and the method is flexible CG with M_circ alone; if the residual
-stops improving for 3 iterations the solve drops the learned term.
+where M is the padded-circulant preconditioner (the Toeplitz operator's own
+circulant inverted on the zero-padded image, precond 3; the reference's
+circulant PSF preconditioner, src/noncart/precond.c:48-164, is the weaker
+Strang form of it). With a zero last layer the network adds nothing and the
+method is flexible CG with M alone; the learned term is used in the first
+``net_iters`` iterations (PicsConf.net_iters; 0 = all) and dropped for good
+if the residual stops improving for 3 iterations.
 
 Training data come from the method itself: for each generated problem the
-library's flexible CG (circulant preconditioner) is run for k = 0, 1, 2, ...
-iterations and to convergence (x*); each iterate x_k gives its true
+library's flexible CG (padded-circulant preconditioner) is run for k = 0, 1,
+2, ... iterations and to convergence (x*); each iterate x_k gives its true
 residual r_k = b - (A^H A + lambda) x_k and exact error e_k = x* - x_k. The
-loss is what one flexible-CG step along z = M_circ(r)/||M_circ(r)|| +
-net(r/||r||) leaves of the A-norm error after an exact line search,
+loss is what one flexible-CG step along z = M(r)/||M(r)|| + net(r/||r||)
+leaves of the A-norm error after an exact line search,
 
     L = 1 - <z, r>^2 / (<z, A z> <e, r>),    A = A^H A + lambda,
 
@@ -48,7 +51,8 @@ WEIGHTS = os.path.join(HERE, "precnet_weights.npz")
 CIN = [2, 32, 32, 32, 32, 32]
 COUT = [32, 32, 32, 32, 32, 2]
 LAM = 0.01
-ITERS = (0, 1, 2, 4, 6, 9, 13)       # iterates whose residuals become training pairs
+ITERS = (0, 1, 2, 3, 5, 7, 10)      # iterates whose residuals become training pairs
+BASE = 3                              # the preconditioner the network corrects (padded circulant)
 
 
 def layer_offsets():
@@ -139,6 +143,12 @@ class PrecNet:
         _lib.check(_lib.load().bnufft_precnet_backward(self.handle, px, pg, X, Y, n, float(lr), gp, _stream_of(x, gout)))
         del k1, k2
 
+    def status(self):
+        """0, or 1 if a tensor-core layer's bounded wait ran out (synchronises)."""
+        st = ctypes.c_int(-1)
+        _lib.check(_lib.load().bnufft_precnet_status(self.handle, ctypes.byref(st), None))
+        return st.value
+
     def free(self):
         if getattr(self, "handle", None) is not None:
             _lib.load().bnufft_precnet_free(self.handle)
@@ -155,7 +165,7 @@ class PrecNet:
 # training data from the method itself
 # ---------------------------------------------------------------------------
 
-def _model(prob, dev, precond, maxiter, tol):
+def _model(prob, dev, precond, maxiter, tol, net_iters=0):
     import torch
     from .pics import Pics, PicsConf
 
@@ -164,18 +174,18 @@ def _model(prob, dev, precond, maxiter, tol):
 
     traj, sens, ksp = prob["traj"], prob["sens"], prob["ksp"]
     p = Pics(dt(traj), dt(sens), ksp_dims=list(ksp.shape),
-             conf=PicsConf(lam=LAM, maxiter=maxiter, tol=tol, precond=precond),
+             conf=PicsConf(lam=LAM, maxiter=maxiter, tol=tol, precond=precond, net_iters=net_iters),
              traj_dims=list(traj.shape), sens_dims=list(sens.shape))
     return p, dt(ksp)
 
 
 def problem_samples(prob, dev, iters=ITERS):
-    """The model (circulant preconditioner) of one problem and, for its
-    iterates k in iters, unit residuals R_k = r_k / ||r_k||, unit circulant
-    steps Mn_k = M(r_k) / ||M(r_k)|| and E_k = <e_k, r_k> / ||r_k||^2 with
-    e_k = x* - x_k = A^-1 r_k. The caller frees the model."""
+    """The model (padded-circulant preconditioner) of one problem and, for
+    its iterates k in iters, unit residuals R_k = r_k / ||r_k||, unit
+    preconditioned steps Mn_k = M(r_k) / ||M(r_k)|| and E_k = <e_k, r_k> /
+    ||r_k||^2 with e_k = x* - x_k = A^-1 r_k. The caller frees the model."""
     import torch
-    p, ksp = _model(prob, dev, 1, 200, 1e-7)
+    p, ksp = _model(prob, dev, BASE, 200, 1e-7)
     b = p.rhs(ksp)
     xs = p.run(ksp).clone()
     R, Mn, E = [], [], []
@@ -239,13 +249,13 @@ def train_online(net, nprob, seed, dev, N=256, coils=(8, 32), spokes=(48, 128), 
             p.free()
         if log and (i + 1) % 100 == 0:
             h = np.array(hist[-100:])
-            log(f"problem {i + 1}/{nprob}: loss circulant {h[:, 1].mean():.4f} learned {h[:, 2].mean():.4f} "
+            log(f"problem {i + 1}/{nprob}: loss base {h[:, 1].mean():.4f} learned {h[:, 2].mean():.4f} "
                 f"({time.time() - t0:.1f} s)")
     return hist
 
 
 def heldout_loss(net, nprob, seed, dev, N=256):
-    """Mean A-norm loss of the circulant step and of the learned one."""
+    """Mean A-norm loss of the padded-circulant step and of the learned one."""
     import torch
     from .problems import cgsense_problem
     rng = np.random.default_rng(seed)
@@ -263,10 +273,10 @@ def heldout_loss(net, nprob, seed, dev, N=256):
     return float(np.mean(lc)), float(np.mean(ll))
 
 
-def solve_stats(prob, dev, precond, net=None, tol=1e-4, maxiter=300, reps=3):
+def solve_stats(prob, dev, precond, net=None, tol=1e-4, maxiter=300, reps=3, net_iters=0):
     """Iterations, ms per solve (model reused, CUDA events) and true residual."""
     import torch
-    p, ksp = _model(prob, dev, precond, maxiter, tol)
+    p, ksp = _model(prob, dev, precond, maxiter, tol, net_iters)
     try:
         if net is not None:
             p.set_precnet(net)
@@ -287,7 +297,10 @@ def solve_stats(prob, dev, precond, net=None, tol=1e-4, maxiter=300, reps=3):
         p.free()
 
 
-def evaluate(net, nprob, seed, dev, N=256, coils=(8, 32), spokes=(48, 128), log=None):
+def evaluate(net, nprob, seed, dev, N=256, coils=(8, 32), spokes=(48, 128), log=None, net_iters=(0,)):
+    """Per problem: plain CG, FCG with the reference's circulant and with the
+    padded-circulant preconditioner, and the learned method at each
+    net_iters budget ("fcg_learned" = the first budget)."""
     from .problems import cgsense_problem
     rng = np.random.default_rng(seed)
     rows = []
@@ -295,7 +308,9 @@ def evaluate(net, nprob, seed, dev, N=256, coils=(8, 32), spokes=(48, 128), log=
         prob = cgsense_problem(rng, N=N, coils=coils, spokes=spokes)
         row = {"coils": prob["coils"], "spokes": prob["spokes"],
                "cg": solve_stats(prob, dev, 0), "fcg_circ": solve_stats(prob, dev, 1),
-               "fcg_learned": solve_stats(prob, dev, 2, net)}
+               "fcg_padded": solve_stats(prob, dev, 3)}
+        for j, k in enumerate(net_iters):
+            row["fcg_learned" if j == 0 else f"fcg_learned_k{k}"] = solve_stats(prob, dev, 2, net, net_iters=k)
         rows.append(row)
         if log and (i + 1) % 32 == 0:
             log(f"eval {i + 1}/{nprob}")
@@ -304,7 +319,7 @@ def evaluate(net, nprob, seed, dev, N=256, coils=(8, 32), spokes=(48, 128), log=
 
 def summarize(rows):
     out = {}
-    for k in ("cg", "fcg_circ", "fcg_learned"):
+    for k in [k for k in rows[0] if k.startswith(("cg", "fcg"))]:
         its = np.array([r[k]["iters"] for r in rows], dtype=float)
         ms = np.array([r[k]["ms"] for r in rows])
         tr = np.array([r[k]["true_res"] for r in rows])
@@ -312,6 +327,7 @@ def summarize(rows):
                   "converged_frac": float(np.mean(tr <= 1.05e-4))}
     out["speedup_learned_vs_cg"] = out["cg"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
     out["speedup_learned_vs_circ"] = out["fcg_circ"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
+    out["speedup_learned_vs_padded"] = out["fcg_padded"]["ms_mean"] / out["fcg_learned"]["ms_mean"]
     out["speedup_circ_vs_cg"] = out["cg"]["ms_mean"] / out["fcg_circ"]["ms_mean"]
     return out
 
@@ -326,6 +342,7 @@ def main(argv=None):
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--weights", default=WEIGHTS)
     ap.add_argument("--report", default=None)
+    ap.add_argument("--net-iters", default="0", help="comma list of learned-iteration budgets to evaluate")
     a = ap.parse_args(argv)
 
     import torch
@@ -346,7 +363,7 @@ def main(argv=None):
         net.save(a.out, problems=a.problems, steps=a.steps, lr=a.lr)
     else:
         net = PrecNet.load(a.weights)
-    rows = evaluate(net, a.eval, 2, dev, log=log)
+    rows = evaluate(net, a.eval, 2, dev, log=log, net_iters=tuple(int(v) for v in a.net_iters.split(",")))
     report["eval"] = summarize(rows)
     report["eval_problems"] = a.eval
     line = json.dumps(report)

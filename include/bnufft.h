@@ -10,6 +10,10 @@
  * staged through device buffers. "stream" is a cudaStream_t (NULL: default
  * stream). There is no CPU fallback: without a usable CUDA device every
  * call fails with BNUFFT_ERR_CUDA.
+ * The library keeps per-device tables (FFT twiddles, the allocation-free
+ * entry point's scratch contents) for the life of the process: a
+ * cudaDeviceReset() while it is loaded destroys them without its knowledge
+ * and is not supported.
  */
 #ifndef BNUFFT_H
 #define BNUFFT_H
@@ -137,8 +141,9 @@ struct bnufft_pics_conf {
 	int precond;		/* 0: plain CG (the reference's pics); 1: flexible CG with
 				   the circulant preconditioner of the NUFFT's PSF
 				   (nufft_precond_create, src/noncart/precond.c:48-164);
-				   2: flexible CG with the circulant preconditioner plus
-				   the learned correction (bnufft_pics_set_precnet);
+				   2: flexible CG with the padded-circulant preconditioner
+				   (as 3) plus the learned correction
+				   (bnufft_pics_set_precnet);
 				   3: flexible CG with the padded-circulant preconditioner
 				   (no counterpart in the reference): the Toeplitz
 				   operator's own 2N (or embedding) circulant inverted,
@@ -148,6 +153,9 @@ struct bnufft_pics_conf {
 				   beta in float32 as conjgrad stores them
 				   (src/iter/italgos.c:518-554), so unconverged iterates
 				   follow the reference's; 0 = float64 scalars. Default 1. */
+	int net_iters;		/* precond 2: the learned correction is used in the first
+				   net_iters iterations only (0 = until the stall test
+				   switches it off); the kept directions stay. */
 };
 
 typedef struct bnufft_pics_s* bnufft_pics_t;
@@ -258,6 +266,12 @@ int bnufft_precnet_train_step(bnufft_precnet_t net, const void* in, const void* 
  * network. */
 int bnufft_precnet_backward(bnufft_precnet_t net, const void* in, const void* gout, long X, long Y, long nimg,
 		float lr, float* grads, void* stream);
+
+/* The network's 32 -> 32 layers run on the tcgen05 tensor cores; their
+ * waits for the tensor core are bounded. *status (synchronises): 0, or 1 if
+ * a wait ran out since the network was created (the layer's output was then
+ * not written). */
+int bnufft_precnet_status(bnufft_precnet_t net, int* status, void* stream);
 
 void bnufft_precnet_free(bnufft_precnet_t net);
 

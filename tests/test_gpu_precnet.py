@@ -41,6 +41,31 @@ def test_forward_vs_oracle(X, Y, n):
     assert rel(out, po.from_channels(ref)) < 3e-3
 
 
+@pytest.mark.parametrize("X,Y,n", [(256, 256, 1), (200, 131, 2), (128, 9, 1)])
+def test_tensor_core_layers_match_mma_sync(X, Y, n, monkeypatch):
+    """The tcgen05 layers (default) against the mma.sync ones: both sum the
+    same exact bf16 products in float32, in another order, so outputs and
+    gradients differ only where an activation rounds to the other bf16
+    neighbour. Covers partial 128-pixel tiles, an odd row count and a batch."""
+    rng = np.random.default_rng(X * Y + n)
+    p = _params(rng)
+    x, t = _img(rng, X, Y, n), _img(rng, X, Y, n)
+    net = precnet.PrecNet(p)
+    res = {}
+    for tc in ("0", "1"):
+        monkeypatch.setenv("BNUFFT_NET_TC", tc)
+        out = np.asarray(net.forward(x, X, Y, n)).reshape(X, Y, n, order="F")
+        g = np.zeros(po.NPARAMS, dtype=np.float32)
+        net.train_step(x, t, X, Y, n, 0.0, grads=g)
+        res[tc] = (out, g)
+    status = net.status()
+    net.free()
+    assert status == 0
+    assert rel(res["1"][0], res["0"][0]) < 2e-3
+    for li, (wo, bo, e) in enumerate(po.offsets()):
+        assert rel(res["1"][1][wo:bo], res["0"][1][wo:bo]) < 1e-2, li
+
+
 def test_gradients_vs_oracle():
     rng = np.random.default_rng(5)
     X, Y, n = 40, 24, 2
@@ -88,16 +113,17 @@ def test_adam_training_reduces_loss():
     assert l1 < 0.2 * l0, (l0, l1)
 
 
-def test_learned_fcg_zero_network_equals_circulant():
+def test_learned_fcg_zero_network_equals_padded():
     """An all-zero last layer adds nothing: precond 2 iterates exactly like
-    precond 1 (bit-identical in deterministic mode)."""
+    precond 3, its padded-circulant base (bit-identical in deterministic
+    mode)."""
     g = golden("pics2d_n64_c4")
     net = precnet.PrecNet(precnet.init_params(3))
     out = {}
     os.environ["BNUFFT_FCG_M"] = "1"     # the same truncation for both
     os.environ["BNUFFT_FCG_FOLD"] = "0"  # and the same launches (no folded dot products)
     try:
-        for pc in (1, 2):
+        for pc in (3, 2):
             p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
                      conf=PicsConf(lam=0.01, maxiter=100, tol=1e-5, scaling=1.0, precond=pc, deterministic=True))
             if pc == 2:
@@ -108,8 +134,8 @@ def test_learned_fcg_zero_network_equals_circulant():
         os.environ.pop("BNUFFT_FCG_M", None)
         os.environ.pop("BNUFFT_FCG_FOLD", None)
     net.free()
-    assert np.array_equal(out[1][0].view(np.uint32), out[2][0].view(np.uint32))
-    assert out[1][1] == out[2][1]
+    assert np.array_equal(out[3][0].view(np.uint32), out[2][0].view(np.uint32))
+    assert out[3][1] == out[2][1]
 
 
 def test_learned_fcg_random_network_still_converges():
