@@ -2721,7 +2721,8 @@ static int sm_count()
 // mma.sync kernel's order.
 template <int MODE>
 static int launch_conv32(const bnufft_precnet_s* n, const bf16* in, const bf16* w, const bf16* wtc,
-		const float* bias, const bf16* mask, bf16* out, int X, int Y, long nimg, const int* done, cudaStream_t st)
+		const float* bias, const bf16* mask, bf16* out, int X, int Y, long nimg, const int* done, const int* skip,
+		cudaStream_t st)
 {
 	const char* e = getenv("BNUFFT_NET_TC");
 	constexpr int R = 2;
@@ -2752,36 +2753,40 @@ static int launch_conv32(const bnufft_precnet_s* n, const bf16* in, const bf16* 
 		const int per_sm = (int)std::max<size_t>(1, (227 * 1024) / (smem + 1024));
 		const long blocks = std::min<long>(tiles, (long)sm_count() * std::min(per_sm, 4));
 		k_conv32_tc<MODE, R><<<(unsigned)blocks, 128, smem, st>>>(map, wtc, bias, mask, out, X, Y, (int)nimg, done,
-				n->tc_status);
+				skip, n->tc_status);
 		LAUNCHED();
 		return BNUFFT_OK;
 	}
 
 	TRY(prep_kernel(k_conv32<MODE>, NET_CONV_SMEM));
-	k_conv32<MODE><<<net_tiles(X, Y, nimg), NET_THREADS, NET_CONV_SMEM, st>>>(in, w, bias, mask, out, X, Y, done);
+	k_conv32<MODE><<<net_tiles(X, Y, nimg), NET_THREADS, NET_CONV_SMEM, st>>>(in, w, bias, mask, out, X, Y, done,
+			skip);
 	LAUNCHED();
 	return BNUFFT_OK;
 }
 
 // Forward through all six layers: act[0..4] (layer 1-5 outputs, bf16) and
 // out = zc + scale_out * net(scale_in * in). acts may alias in pairs for
-// inference (acts[i] != acts[i - 1]).
+// inference (acts[i] != acts[i - 1]). scale_in null: the input's own norm
+// from in_norm_part (if given); scale_out null: the norm of zc from
+// norm_part. With *net_off the layers do nothing and out = zc.
 static int net_forward(const bnufft_precnet_s* n, const float2* in, int X, int Y, long nimg, bf16* const acts[5],
 		const float* scale_in, const float* scale_out, const double* norm_part, int nnorm, const float2* zc,
 		float2* out, const float2* pdot, double* dot_part, int* nblocks, const int* done, const int* net_off,
-		cudaStream_t st)
+		cudaStream_t st, const double* in_norm_part = nullptr, int in_nnorm = 0)
 {
 	const long P = (long)X * Y * nimg;
 	const unsigned pb = (unsigned)((P + NET_THREADS - 1) / NET_THREADS);
 	const float* pr = n->pr;
 
-	k_net_in<<<pb, NET_THREADS, 0, st>>>(in, X, Y, P, pr + NetLayout::woff(0), pr + NetLayout::boff(0), scale_in, acts[0], done);
+	k_net_in<<<pb, NET_THREADS, 0, st>>>(in, X, Y, P, pr + NetLayout::woff(0), pr + NetLayout::boff(0), scale_in,
+			in_norm_part, in_nnorm, acts[0], done, net_off);
 	LAUNCHED();
 
 	for (int l = 1; l <= 4; l++) {
 
 		TRY(launch_conv32<0>(n, acts[l - 1], n->wf + (l - 1) * 9216, n->wf_tc + (l - 1) * 9216, pr + NetLayout::boff(l),
-				nullptr, acts[l], X, Y, nimg, done, st));
+				nullptr, acts[l], X, Y, nimg, done, net_off, st));
 	}
 
 	k_net_out<<<pb, NET_THREADS, 0, st>>>(acts[4], X, Y, P, pr + NetLayout::woff(5), pr + NetLayout::boff(5), scale_out,
@@ -3026,7 +3031,7 @@ static int net_train(bnufft_precnet_t n, const void* in, const void* target, con
 
 		TRY((net_wgrad<NET_C, NET_C, bf16, bf16>(n, l, n->act[l - 1], gu, x, y, nimg, st)));
 		TRY(launch_conv32<1>(n, gu, n->wt + (l - 1) * 9216, n->wt_tc + (l - 1) * 9216, nullptr, n->act[l - 1], gn, x,
-				y, nimg, nullptr, st));
+				y, nimg, nullptr, nullptr, st));
 		std::swap(gu, gn);
 	}
 
@@ -3511,8 +3516,8 @@ static int pics_precond_pad(bnufft_pics_s* ps, const float2* r, float2* z, const
 
 // z = M(r): the circulant preconditioner (precond 1), the padded one
 // (precond 3), or the padded one plus the learned correction
-// ||M_pad(r)|| net(r / ||r||) (precond 2; 1 / ||r|| from the solve's
-// scalars); optional partials Re<pdot, z>
+// ||M_pad(r)|| net(M_pad(r) / ||M_pad(r)||) (precond 2; the norm from the
+// partials of the pass that wrote M_pad(r)); optional partials Re<pdot, z>
 static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const float2* pdot, double* dot_part,
 		int* nblocks, cudaStream_t st)
 {
@@ -3525,9 +3530,10 @@ static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const flo
 	if (!ps->net)
 		return fail(BNUFFT_ERR_ARG, "precond 2 needs a network (bnufft_pics_set_precnet)");
 
-	// z = M_pad(r) with the partials of ||z||^2, then z += ||z|| net(r / ||r||):
+	// z = M_pad(r) with the partials of ||z||^2, then z += ||z|| net(z / ||z||):
 	// flexible CG is invariant to a positive scale of z per iteration, so the
-	// network learns a scale-free correction of the padded-circulant direction
+	// network learns a scale-free correction of the padded-circulant step
+	// from the step itself
 	int nmc = 0;
 	TRY(pics_precond_pad(ps, r, z, z, ps->mcn_part, &nmc, st));
 
@@ -3537,8 +3543,8 @@ static int pics_precond(bnufft_pics_s* ps, const float2* r, float2* z, const flo
 	const Geom& g = ps->nufft->op.g;
 	bf16* acts[5] = { ps->nact[0], ps->nact[1], ps->nact[0], ps->nact[1], ps->nact[0] };
 	CgScalars* sc = ps->scal;
-	return net_forward(ps->net, r, g.N[0], g.N[1], 1, acts, &sc->rinv, nullptr, ps->mcn_part, nmc, z, z, pdot,
-			dot_part, nblocks, &sc->done, &sc->net_off, st);
+	return net_forward(ps->net, z, g.N[0], g.N[1], 1, acts, nullptr, nullptr, ps->mcn_part, nmc, z, z, pdot,
+			dot_part, nblocks, &sc->done, &sc->net_off, st, ps->mcn_part, nmc);
 }
 
 // the one-launch cluster form of the circulant preconditioner (square 2D

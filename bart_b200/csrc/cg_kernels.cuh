@@ -539,10 +539,14 @@ __global__ void k_fcg_check(CgScalars* st, int it, const double* __restrict__ rs
 
 		bool stall = (j - st->best_it >= 3) || ((j >= 4) && (st->best_rs > 0.25 * st->best_hist[j % 4]));
 
-		// the learned part's iteration budget: switched off without a
-		// restart (flexible CG keeps the directions it has)
-		if ((st->net_iters > 0) && (j >= st->net_iters))
+		// the learned part's iteration budget: once it is spent the
+		// preconditioner is the linear one, and the direction history
+		// restarts (one kept direction from here on, as PCG)
+		if ((st->net_iters > 0) && (j >= st->net_iters) && !st->net_off) {
+
 			st->net_off = 1;
+			st->restart_it = j;
+		}
 
 		if (stall && !st->net_off) {
 

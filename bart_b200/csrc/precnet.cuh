@@ -72,13 +72,13 @@ __device__ __forceinline__ uint32_t lds32(const bf16* p) { return *(const uint32
 template <int MODE>
 __global__ void __launch_bounds__(NET_THREADS) k_conv32(const bf16* __restrict__ in, const bf16* __restrict__ w,
 		const float* __restrict__ bias, const bf16* __restrict__ mask, bf16* __restrict__ out, int X, int Y,
-		const int* done)
+		const int* done, const int* skip = nullptr)
 {
 	extern __shared__ __align__(16) unsigned char net_smem[];
 	bf16* sA = (bf16*)net_smem;
 	bf16* sW = sA + NET_HALO_X * NET_HALO_Y * NET_SA_STRIDE;
 
-	if (done && *done)
+	if ((done && *done) || (skip && *skip))
 		return;
 
 	const int x0 = blockIdx.x * NET_TILE_X;
@@ -197,19 +197,34 @@ __global__ void __launch_bounds__(NET_THREADS) k_conv32(const bf16* __restrict__
 }
 
 // Layer 1 (2 -> 32), one thread per pixel: act = bf16(relu(conv(s * in) + b)),
-// in complex [nimg][Y][X], s = *scale (1 if null). w: float [32][9][2]
-// (values already rounded to bf16), b: [32].
+// in complex [nimg][Y][X], s = *scale, or 1 / sqrt(sum of norm_part) (the
+// input's norm from the partials of the pass that wrote it), or 1. w: float
+// [32][9][2] (values already rounded to bf16), b: [32]. Nothing is done when
+// *done or *skip (the learned term switched off).
 __global__ void __launch_bounds__(NET_THREADS) k_net_in(const float2* __restrict__ in, int X, int Y, long P,
-		const float* __restrict__ w, const float* __restrict__ b, const float* scale, bf16* __restrict__ out,
-		const int* done)
+		const float* __restrict__ w, const float* __restrict__ b, const float* scale, const double* norm_part,
+		int nnorm, bf16* __restrict__ out, const int* done, const int* skip)
 {
 	__shared__ float sw[NET_C * 18 + NET_C];
+	__shared__ double red[32];
 
-	if (done && *done)
+	if ((done && *done) || (skip && *skip))
 		return;
 
 	for (int i = threadIdx.x; i < NET_C * 18 + NET_C; i += NET_THREADS)
 		sw[i] = (i < NET_C * 18) ? w[i] : b[i - NET_C * 18];
+
+	float s = 1.f;
+
+	if (scale) {
+
+		s = *scale;
+
+	} else if (norm_part) {
+
+		const double n2 = sum_partials_d(norm_part, nnorm, red);
+		s = (n2 > 0.) ? (float)(1. / sqrt(n2)) : 0.f;
+	}
 
 	__syncthreads();
 
@@ -222,7 +237,6 @@ __global__ void __launch_bounds__(NET_THREADS) k_net_in(const float2* __restrict
 	const long base = (p / XY) * XY;
 	const int y = (int)((p % XY) / X);
 	const int x = (int)(p % X);
-	const float s = scale ? *scale : 1.f;
 	float v[18];
 #pragma unroll
 	for (int tap = 0; tap < 9; tap++) {
@@ -238,8 +252,9 @@ __global__ void __launch_bounds__(NET_THREADS) k_net_in(const float2* __restrict
 		v[2 * tap + 1] = u.y * s;
 	}
 
-	bf162* o = (bf162*)(out + p * NET_C);
-#pragma unroll 4
+	// the pixel's 32 channels leave as four 16-byte stores
+	uint32_t pk[16];
+#pragma unroll
 	for (int co = 0; co < NET_C; co += 2) {
 
 		float a0 = sw[NET_C * 18 + co];
@@ -251,8 +266,14 @@ __global__ void __launch_bounds__(NET_THREADS) k_net_in(const float2* __restrict
 			a1 = fmaf(sw[(co + 1) * 18 + k], v[k], a1);
 		}
 
-		o[co / 2] = __floats2bfloat162_rn(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
+		const bf162 h = __floats2bfloat162_rn(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
+		pk[co / 2] = *(const uint32_t*)&h;
 	}
+
+	uint4* o = (uint4*)(out + p * NET_C);
+#pragma unroll
+	for (int q = 0; q < 4; q++)
+		o[q] = make_uint4(pk[4 * q], pk[4 * q + 1], pk[4 * q + 2], pk[4 * q + 3]);
 }
 
 // sum over the 3x3 neighbourhood of a 32-channel bf16 activation with

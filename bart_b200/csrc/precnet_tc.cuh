@@ -154,7 +154,7 @@ __global__ void k_net_pack_tc(const bf16* __restrict__ w, bf16* __restrict__ wp)
 template <int MODE, int R>
 __global__ void __launch_bounds__(128) k_conv32_tc(const __grid_constant__ CUtensorMap in, const bf16* __restrict__ wp,
 		const float* __restrict__ bias, const bf16* __restrict__ mask, bf16* __restrict__ out, int X, int Y,
-		int nimg, const int* done, int* status)
+		int nimg, const int* done, const int* skip, int* status)
 {
 	constexpr uint32_t PLANE = conv_tc_plane(R);
 	constexpr uint32_t NCOL = conv_tc_cols(R);
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(128) k_conv32_tc(const __grid_constant__ CUten
 	uint64_t* bars = (uint64_t*)(sB + TC_W_BYTES);		// [0] loads, [1] MMAs
 	uint32_t* tslot = (uint32_t*)(bars + 2);
 
-	if (done && *done)
+	if ((done && *done) || (skip && *skip))
 		return;
 
 	const int tid = threadIdx.x;

@@ -5,7 +5,7 @@ channels, bf16 weights, float32 accumulation) runs and trains on the GPU
 through libbnufft's own kernels (``bnufft_precnet_*``). Inside flexible CG
 (``PicsConf(precond=2)``) the preconditioner is
 
-    z = M(r) + ||M(r)|| net(r / ||r||)
+    z = M(r) + ||M(r)|| net(M(r) / ||M(r)||)
 
 where M is the padded-circulant preconditioner (the Toeplitz operator's own
 circulant inverted on the zero-padded image, precond 3; the reference's
@@ -19,7 +19,7 @@ Training data come from the method itself: for each generated problem the
 library's flexible CG (padded-circulant preconditioner) is run for k = 0, 1,
 2, ... iterations and to convergence (x*); each iterate x_k gives its true
 residual r_k = b - (A^H A + lambda) x_k and exact error e_k = x* - x_k. The
-loss is what one flexible-CG step along z = M(r)/||M(r)|| + net(r/||r||)
+loss is what one flexible-CG step along z = Mn + net(Mn), Mn = M(r)/||M(r)||,
 leaves of the A-norm error after an exact line search,
 
     L = 1 - <z, r>^2 / (<z, A z> <e, r>),    A = A^H A + lambda,
@@ -235,7 +235,7 @@ def train_online(net, nprob, seed, dev, N=256, coils=(8, 32), spokes=(48, 128), 
         p, R, Mn, E = problem_samples(prob, dev)
         try:
             K = R.shape[0]
-            x = R.contiguous().view(-1)
+            x = Mn.contiguous().view(-1)
             for j in range(steps):
                 out = net.forward(x, N, N, K)
                 L, g = anorm_loss(p, R, Mn, E, out)
@@ -265,7 +265,7 @@ def heldout_loss(net, nprob, seed, dev, N=256):
         p, R, Mn, E = problem_samples(prob, dev)
         try:
             K = R.shape[0]
-            out = net.forward(R.contiguous().view(-1), N, N, K)
+            out = net.forward(Mn.contiguous().view(-1), N, N, K)
             lc.append(anorm_loss(p, R, Mn, E, torch.zeros_like(out))[0].mean().item())
             ll.append(anorm_loss(p, R, Mn, E, out)[0].mean().item())
         finally:

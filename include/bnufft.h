@@ -155,7 +155,8 @@ struct bnufft_pics_conf {
 				   follow the reference's; 0 = float64 scalars. Default 1. */
 	int net_iters;		/* precond 2: the learned correction is used in the first
 				   net_iters iterations only (0 = until the stall test
-				   switches it off); the kept directions stay. */
+				   switches it off); the direction history then
+				   restarts. */
 };
 
 typedef struct bnufft_pics_s* bnufft_pics_t;
@@ -244,7 +245,8 @@ int bnufft_pics_precond(bnufft_pics_t pics, void* z, const void* r, void* stream
  * channels), ReLU after layers 1-5, bf16 weights and activations, float32
  * accumulation. Parameters: float32, per layer W[cout][3 ky + kx][cin] then
  * b[cout]; bnufft_precnet_nparams() values in all. Used by flexible CG as
- * z = M_circ(r) + ||M_circ(r)|| net(r / ||r||). */
+ * z = M(r) + ||M(r)|| net(M(r) / ||M(r)||), M the padded-circulant
+ * preconditioner. */
 typedef struct bnufft_precnet_s* bnufft_precnet_t;
 
 int bnufft_precnet_nparams(void);
