@@ -3196,7 +3196,7 @@ extern "C" void bnufft_pics_conf_defaults(struct bnufft_pics_conf* c)
 	c->bin = 0;
 	c->precond = 0;
 	c->ref_scalars = 1;
-	c->net_iters = 0;
+	c->net_iters = 1;
 }
 
 // A^H A x (+ lam x), with optional per-block Re<x, out> partials
@@ -3316,9 +3316,10 @@ extern "C" int bnufft_pics_create(bnufft_pics_t* out, int N, const long ksp_dims
 
 	if (conf.precond) {
 
-		// the circulant preconditioner is linear (flexible CG keeps one
-		// direction, as PCG); the learned one is not: keep FCG_MAX_M
-		ps->fcg_m = (2 == conf.precond) ? (int)FCG_MAX_M : 1;
+		// the circulant preconditioners are linear (flexible CG keeps one
+		// direction, as PCG); the learned one is not: keep FCG_MAX_M, or
+		// one direction when it is used in the first iterations only
+		ps->fcg_m = ((2 == conf.precond) && (conf.net_iters <= 0)) ? (int)FCG_MAX_M : 1;
 
 		if (const char* e = getenv("BNUFFT_FCG_M"))
 			ps->fcg_m = std::max(1, std::min((int)FCG_MAX_M, atoi(e)));
@@ -3722,7 +3723,7 @@ static int pics_fcg_iteration(bnufft_pics_s* ps, int it, cudaStream_t st)
 	float2* p = ps->pbuf[1];
 	unsigned nb = (unsigned)ps->nparts;
 	int npap = 0;
-	const bool folded = ((1 == ps->conf.precond) || (3 == ps->conf.precond)) && (1 == ps->fcg_m) && ps->fcg_fold;
+	const bool folded = (1 == ps->fcg_m) && ps->fcg_fold;
 	const int ring = (1 == ps->fcg_m) ? 1 : (int)FCG_RING;
 
 	if (folded && ps->fcg_fused) {	// five launches: the normal's passes, the step, the

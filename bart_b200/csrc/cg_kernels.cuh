@@ -371,8 +371,18 @@ __global__ void k_fcgm_dir(float2* __restrict__ p_cur, float2* __restrict__ p_ri
 		return;
 
 	it = cg_iter(it, st);
-	const int w = min(it - st->restart_it, m);
+	// the learned term's iteration budget: z of iterations < net_iters
+	// carries it, and the first direction after it restarts (p = z, PCG
+	// from there on; a short recurrence across the switch converges slower).
+	// Every block derives the restart from it alone; net_off is only read
+	// by the preconditioner pass at the end of this iteration (z for
+	// iteration it + 1).
+	const bool restart = (st->net_iters > 0) && (it == st->net_iters);
+	const int w = restart ? 0 : min(it - st->restart_it, m);
 	const bool check = rs_part && (it > 0);
+
+	if ((0 == blockIdx.x) && (0 == threadIdx.x) && (st->net_iters > 0) && (it + 1 >= st->net_iters))
+		st->net_off = 1;
 	// ||r||^2 and the first <z, A p_j> in one reduction
 	const double3 s3 = sum_partials3_d(rs_part, check ? nrs : 0, dots, (w > 0) ? ndots : 0, nullptr, 0, sh);
 

@@ -32,7 +32,7 @@ class PicsConf:
     bin: int = 0              # gridding bin edge (0 = default); tuning only
     precond: int = 0          # 0 plain CG, 1 FCG + circulant, 2 FCG + padded circulant + learned, 3 FCG + padded circulant
     ref_scalars: bool = True  # plain CG keeps its scalars in float32 as the reference's conjgrad does
-    net_iters: int = 0        # precond 2: iterations that use the learned term (0 = until it stalls)
+    net_iters: int = 1        # precond 2: iterations that use the learned term (0 = until it stalls)
 
     def c(self) -> _lib.PicsConfC:
         return _lib.PicsConfC(float(self.lam), int(self.maxiter), float(self.tol), float(self.scaling),

@@ -165,7 +165,7 @@ class PrecNet:
 # training data from the method itself
 # ---------------------------------------------------------------------------
 
-def _model(prob, dev, precond, maxiter, tol, net_iters=0):
+def _model(prob, dev, precond, maxiter, tol, net_iters=None):
     import torch
     from .pics import Pics, PicsConf
 
@@ -174,7 +174,8 @@ def _model(prob, dev, precond, maxiter, tol, net_iters=0):
 
     traj, sens, ksp = prob["traj"], prob["sens"], prob["ksp"]
     p = Pics(dt(traj), dt(sens), ksp_dims=list(ksp.shape),
-             conf=PicsConf(lam=LAM, maxiter=maxiter, tol=tol, precond=precond, net_iters=net_iters),
+             conf=PicsConf(lam=LAM, maxiter=maxiter, tol=tol, precond=precond,
+                           **({} if net_iters is None else {"net_iters": net_iters})),
              traj_dims=list(traj.shape), sens_dims=list(sens.shape))
     return p, dt(ksp)
 
@@ -273,7 +274,7 @@ def heldout_loss(net, nprob, seed, dev, N=256):
     return float(np.mean(lc)), float(np.mean(ll))
 
 
-def solve_stats(prob, dev, precond, net=None, tol=1e-4, maxiter=300, reps=3, net_iters=0):
+def solve_stats(prob, dev, precond, net=None, tol=1e-4, maxiter=300, reps=3, net_iters=None):
     """Iterations, ms per solve (model reused, CUDA events) and true residual."""
     import torch
     p, ksp = _model(prob, dev, precond, maxiter, tol, net_iters)
@@ -297,7 +298,7 @@ def solve_stats(prob, dev, precond, net=None, tol=1e-4, maxiter=300, reps=3, net
         p.free()
 
 
-def evaluate(net, nprob, seed, dev, N=256, coils=(8, 32), spokes=(48, 128), log=None, net_iters=(0,)):
+def evaluate(net, nprob, seed, dev, N=256, coils=(8, 32), spokes=(48, 128), log=None, net_iters=(1,)):
     """Per problem: plain CG, FCG with the reference's circulant and with the
     padded-circulant preconditioner, and the learned method at each
     net_iters budget ("fcg_learned" = the first budget)."""
@@ -332,9 +333,41 @@ def summarize(rows):
     return out
 
 
+def time_forward(net, dev, N=256, reps=50):
+    """Mean device time of one network forward on an N x N image with the
+    tcgen05 layers and with the mma.sync layers (BNUFFT_NET_TC=0), CUDA
+    events, after 3 warm-up passes; and whether the two outputs agree."""
+    import torch
+    x = torch.randn(N * N, dtype=torch.complex64, device=dev)
+    res, outs = {}, {}
+    old = os.environ.get("BNUFFT_NET_TC")
+    try:
+        for tc in ("1", "0"):
+            os.environ["BNUFFT_NET_TC"] = tc
+            for _ in range(3):
+                net.forward(x, N, N, 1)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                net.forward(x, N, N, 1)
+            e1.record()
+            torch.cuda.synchronize()
+            res["tcgen05_us" if tc == "1" else "mma_sync_us"] = e0.elapsed_time(e1) * 1e3 / max(1, reps)
+            outs[tc] = net.forward(x, N, N, 1)
+    finally:
+        if old is None:
+            os.environ.pop("BNUFFT_NET_TC", None)
+        else:
+            os.environ["BNUFFT_NET_TC"] = old
+    res["max_abs_diff"] = float((outs["1"] - outs["0"]).abs().max())
+    res["status"] = net.status()
+    return res
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m bart_b200.precnet")
-    ap.add_argument("cmd", choices=["train", "eval"])
+    ap.add_argument("cmd", choices=["train", "eval", "time"])
     ap.add_argument("--problems", type=int, default=2000)
     ap.add_argument("--eval", type=int, default=256)
     ap.add_argument("--steps", type=int, default=3)
@@ -342,7 +375,8 @@ def main(argv=None):
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--weights", default=WEIGHTS)
     ap.add_argument("--report", default=None)
-    ap.add_argument("--net-iters", default="0", help="comma list of learned-iteration budgets to evaluate")
+    ap.add_argument("--reps", type=int, default=50, help="time: forward passes per layer kernel")
+    ap.add_argument("--net-iters", default="1", help="comma list of learned-iteration budgets to evaluate")
     a = ap.parse_args(argv)
 
     import torch
@@ -352,6 +386,9 @@ def main(argv=None):
         print(m, file=sys.stderr, flush=True)
 
     report = {}
+    if a.cmd == "time":
+        print(json.dumps(time_forward(PrecNet.load(a.weights), dev, reps=a.reps)), flush=True)
+        return
     if a.cmd == "train":
         net = PrecNet()
         t0 = time.time()

@@ -915,7 +915,7 @@ def main():
                 "config": workload_config(),
                 "solver": {"method": {"cg": "plain CG (the reference's pics)",
                                       "fcg_circulant": "flexible CG with the reference's circulant PSF preconditioner",
-                                      "fcg_learned": "flexible CG with the circulant preconditioner and the learned correction",
+                                      "fcg_learned": "flexible CG with the padded-circulant preconditioner and the learned correction (first iteration), then PCG",
                                       "fcg_padded": "PCG with the padded-circulant preconditioner"}[headline]
                                      + " (same normal equations and tolerance as the reference's plain-CG pics)",
                            "maxiter": MAXITER},

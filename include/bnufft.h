@@ -155,8 +155,8 @@ struct bnufft_pics_conf {
 				   follow the reference's; 0 = float64 scalars. Default 1. */
 	int net_iters;		/* precond 2: the learned correction is used in the first
 				   net_iters iterations only (0 = until the stall test
-				   switches it off); the direction history then
-				   restarts. */
+				   switches it off). With a budget flexible CG keeps
+				   one direction (short recurrence). Default 1. */
 };
 
 typedef struct bnufft_pics_s* bnufft_pics_t;

@@ -170,11 +170,11 @@ def test_learned_fcg_random_network_still_converges():
 def test_trained_network_gain():
     """The committed network on held-out 256x256 problems (seeds not used in
     training): each learned step removes more of the A-norm error than the
-    circulant step alone (the network's gain), and learned flexible CG reaches
-    the 1e-4 tolerance (true residual) in fewer iterations than plain CG.
-    Against circulant flexible CG alone it needs more iterations (the
-    nonlinear correction costs PCG's Krylov optimality); the measured
-    numbers are in profiles/precnet_fcg_eval_256.md."""
+    padded-circulant step alone (the network's gain, 0.41 -> 0.31 in
+    training), and learned flexible CG reaches the 1e-4 tolerance (true
+    residual) in fewer iterations than plain CG. Against the padded-circulant
+    PCG alone it needs more iterations: a greedy one-step gain is not a
+    Krylov gain."""
     import torch
     from bart_b200.problems import cgsense_problem
     dev = torch.device("cuda", 0)
