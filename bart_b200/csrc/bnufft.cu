@@ -3960,7 +3960,7 @@ static int pics_solve(bnufft_pics_s* ps, const float2* ksp, float2* out, cudaStr
 	k_cg_init<<<nb, RED_THREADS, 0, st>>>(ps->x, ps->r, ps->pbuf[1], ps->b, ps->npix, ps->rs_part);
 	LAUNCHED();
 	k_cg_start<<<1, RED_THREADS, 0, st>>>(ps->scal, ps->rs_part, ps->nparts, ps->conf.tol, ps->conf.maxiter,
-			(0 == ps->conf.precond) && ps->conf.ref_scalars, ps->conf.net_iters);
+			(0 == ps->conf.precond) && ps->conf.ref_scalars, (2 == ps->conf.precond) ? ps->conf.net_iters : 0);
 	LAUNCHED();
 
 	TRY(alloc_work(op.w, op.g, ps->C, st));

@@ -123,9 +123,10 @@ def test_learned_fcg_zero_network_equals_padded():
     os.environ["BNUFFT_FCG_M"] = "1"     # the same truncation for both
     os.environ["BNUFFT_FCG_FOLD"] = "0"  # and the same launches (no folded dot products)
     try:
-        for pc in (3, 2):
+        for pc in (3, 2):   # no iteration budget: no restart when the learned term stops
             p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
-                     conf=PicsConf(lam=0.01, maxiter=100, tol=1e-5, scaling=1.0, precond=pc, deterministic=True))
+                     conf=PicsConf(lam=0.01, maxiter=100, tol=1e-5, scaling=1.0, precond=pc, deterministic=True,
+                                   net_iters=0))
             if pc == 2:
                 p.set_precnet(net)
             out[pc] = (np.asarray(p.run(g["ksp"])), p.stats())
@@ -136,6 +137,23 @@ def test_learned_fcg_zero_network_equals_padded():
     net.free()
     assert np.array_equal(out[3][0].view(np.uint32), out[2][0].view(np.uint32))
     assert out[3][1] == out[2][1]
+
+
+@pytest.mark.parametrize("pc", [1, 3])
+def test_learned_budget_leaves_linear_methods_alone(pc):
+    """net_iters belongs to the learned method: the linear preconditioners
+    iterate bit for bit the same whatever it is set to."""
+    g = golden("pics2d_n64_c4")
+    out = []
+    for k in (0, 1, 3):
+        p = Pics(g["traj"], g["sens"], ksp_dims=list(g["ksp"].shape),
+                 conf=PicsConf(lam=0.01, maxiter=100, tol=1e-5, scaling=1.0, precond=pc, deterministic=True,
+                               net_iters=k))
+        out.append((np.asarray(p.run(g["ksp"])), p.stats()))
+        p.free()
+    for x, st in out[1:]:
+        assert np.array_equal(x.view(np.uint32), out[0][0].view(np.uint32))
+        assert st == out[0][1]
 
 
 def test_learned_fcg_random_network_still_converges():
