@@ -1522,30 +1522,79 @@ static int op_toeplitz(OpCtx& op, const float2* psf, const float2* x, const floa
 	return rows_inv(g.G[0], op.w.t1, maps, nullptr, nullptr, g.N[0], YZ, (int)C, maps ? cpg : 1, out, st);
 }
 
+// Toeplitz normal with a subspace basis (toeplitz_mult with the block PSF,
+// src/noncart/nufft.c:1546-1625): the full 2N spectra of all Cc K channels,
+// per cell and coil the K x K product with the block PSF (k_basis_mix), and
+// back; the same unnormalised transforms as the single-PSF column pass.
+static int op_toeplitz_basis(OpCtx& op, const float2* psfb, const float2* x, long Cc, int K, float2* out,
+		cudaStream_t st)
+{
+	const Geom& g = op.g;
+	const long C = Cc * K;
+	long YZ = (long)g.N[1] * g.N[2];
+	TRY(alloc_work(op.w, g, C, st));
+	TRY(rows_fwd(g.G[0], x, nullptr, nullptr, nullptr, g.N[0], YZ, YZ * C, op.w.t1, st));
+	float2* spec = op.w.grid;
+
+	if (1 == g.G[2]) {
+
+		TRY(cols(g.G[1], 0, op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1,
+				spec, g.G[0], g.gsz, g.G[1], 0, g.G[0], C, nullptr, 0, 1, 0, st));
+		k_basis_mix<<<vec_blocks(g.gsz * Cc), RED_THREADS, 0, st>>>(spec, psfb, g.gsz, Cc, K);
+		LAUNCHED();
+		TRY(cols(g.G[1], 1, spec, g.G[0], g.gsz, g.G[1], 0,
+				op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1, g.G[0], C, nullptr, 0, 1, 0, st));
+
+	} else {
+
+		long plane = (long)g.G[0] * g.G[1];
+		TRY(cols(g.G[1], 0, op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1,
+				op.w.t2, g.G[0], plane, g.G[1], 0, g.G[0], (long)g.N[2] * C, nullptr, 0, 1, 0, st));
+		TRY(cols(g.G[2], 0, op.w.t2, plane, plane * g.N[2], g.N[2], 1,
+				spec, plane, g.gsz, g.G[2], 0, (int)plane, C, nullptr, 0, 1, 0, st));
+		k_basis_mix<<<vec_blocks(g.gsz * Cc), RED_THREADS, 0, st>>>(spec, psfb, g.gsz, Cc, K);
+		LAUNCHED();
+		TRY(cols(g.G[2], 1, spec, plane, g.gsz, g.G[2], 0,
+				op.w.t2, plane, plane * g.N[2], g.N[2], 1, (int)plane, C, nullptr, 0, 1, 0, st));
+		TRY(cols(g.G[1], 1, op.w.t2, g.G[0], plane, g.G[1], 0,
+				op.w.t1, g.G[0], (long)g.G[0] * g.N[1], g.N[1], 1, g.G[0], (long)g.N[2] * C, nullptr, 0, 1, 0, st));
+	}
+
+	return rows_inv(g.G[0], op.w.t1, nullptr, nullptr, nullptr, g.N[0], YZ, (int)C, 1, out, st);
+}
+
 // PSF on the 2N grid in DFT order, scaled by 1/npix so that the Toeplitz
 // product needs no further normalisation (compute_psf2, src/noncart/nufft.c:727-776):
 // psft = adjoint NUFFT of ones with trajectory 2*traj onto the 2N image,
 // periodic gridding; psf = fftuc(psft) / npix.
+// With a subspace basis (K coefficients over T frames of MrMs samples) the
+// "ones" are the K^2 channels conj(B[t, k]) B[t, k'] |w|^2 and the result is
+// the block PSF [K^2][gsz], pair k + K k' (compute_square_basis,
+// src/noncart/nufft.c:470-505).
 static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, float2** psf_out, cudaStream_t st,
-		bool deterministic, const float2* wgt, int bin_edge)
+		bool deterministic, const float2* wgt, int bin_edge, const float2* basis = nullptr, int K = 1, int T = 1,
+		long MrMs = 0)
 {
 	OpCtx in;
 	in.bin_edge = bin_edge;
 	long d2[3] = { g.G[0], g.G[1], g.G[2] };
 	TRY(init_geom(in.g, d2, g.M, g.os, g.width, 1));
+	const long nch = basis ? (long)K * K : 1;
 
 	float4* t2 = nullptr;
 	float2* ones = nullptr;
 	float2* psft = nullptr;
 	float2* psf = nullptr;
 	CUDA_TRY(cudaMallocAsync(&t2, sizeof(float4) * g.M, st));
-	CUDA_TRY(cudaMallocAsync(&ones, sizeof(float2) * g.M, st));
-	CUDA_TRY(cudaMallocAsync(&psft, sizeof(float2) * in.g.npix, st));
-	CUDA_TRY(cudaMallocAsync(&psf, sizeof(float2) * g.gsz, st));
+	CUDA_TRY(cudaMallocAsync(&ones, sizeof(float2) * g.M * nch, st));
+	CUDA_TRY(cudaMallocAsync(&psft, sizeof(float2) * in.g.npix * nch, st));
+	CUDA_TRY(cudaMallocAsync(&psf, sizeof(float2) * g.gsz * nch, st));
 
 	k_traj_convert<<<vec_blocks(g.M), RED_THREADS, 0, st>>>(t2, traj_c, g.M, 2.f);
 	LAUNCHED();
-	if (wgt)	// compute_square_weights (src/noncart/nufft.c:509-518)
+	if (basis)
+		k_basis_psf_weights<<<vec_blocks(g.M * nch), RED_THREADS, 0, st>>>(ones, basis, wgt, MrMs, T, K);
+	else if (wgt)	// compute_square_weights (src/noncart/nufft.c:509-518)
 		k_weight_sq<<<vec_blocks(g.M), RED_THREADS, 0, st>>>(ones, wgt, g.M);
 	else
 		k_fill<<<vec_blocks(g.M), RED_THREADS, 0, st>>>(ones, g.M, make_float2(1.f, 0.f));
@@ -1561,7 +1610,7 @@ static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, flo
 	if (deterministic)
 		TRY(build_csr(in, st));
 
-	TRY(op_adjoint(in, ones, nullptr, 1, 1, psft, st));
+	TRY(op_adjoint(in, ones, nullptr, nch, 1, psft, st));
 	free_csr(in.csr, st);
 	free_bins(in.bins, st);
 
@@ -1575,28 +1624,28 @@ static int compute_psf(const Geom& g, const float2* traj_c, const float* kb, flo
 		full.g.N[i] = g.G[i];	// input length L on every axis
 
 	full.g.npix = g.gsz;
-	TRY(alloc_work(full.w, full.g, 1, st));
+	TRY(alloc_work(full.w, full.g, nch, st));
 
 	long YZ = (long)g.G[1] * g.G[2];
-	TRY(rows_fwd(g.G[0], psft, nullptr, nullptr, nullptr, g.G[0], YZ, YZ, full.w.t1, st));
+	TRY(rows_fwd(g.G[0], psft, nullptr, nullptr, nullptr, g.G[0], YZ, YZ * nch, full.w.t1, st));
 
 	if (1 == g.G[2]) {
 
 		TRY(cols(g.G[1], 0, full.w.t1, g.G[0], (long)g.G[0] * g.G[1], g.G[1], 1,
-				psf, g.G[0], (long)g.G[0] * g.G[1], g.G[1], 0, g.G[0], 1, nullptr, 0, 1, 0, st));
+				psf, g.G[0], (long)g.G[0] * g.G[1], g.G[1], 0, g.G[0], nch, nullptr, 0, 1, 0, st));
 
 	} else {
 
 		long plane = (long)g.G[0] * g.G[1];
 
 		TRY(cols(g.G[1], 0, full.w.t1, g.G[0], plane, g.G[1], 1,
-				full.w.t2, g.G[0], plane, g.G[1], 0, g.G[0], (long)g.G[2], nullptr, 0, 1, 0, st));
+				full.w.t2, g.G[0], plane, g.G[1], 0, g.G[0], (long)g.G[2] * nch, nullptr, 0, 1, 0, st));
 		TRY(cols(g.G[2], 0, full.w.t2, plane, plane * g.G[2], g.G[2], 1,
-				psf, plane, plane * g.G[2], g.G[2], 0, (int)plane, 1, nullptr, 0, 1, 0, st));
+				psf, plane, plane * g.G[2], g.G[2], 0, (int)plane, nch, nullptr, 0, 1, 0, st));
 	}
 
 	double sc = 1. / sqrt((double)g.gsz) / (double)g.npix;
-	k_scale<<<vec_blocks(g.gsz), RED_THREADS, 0, st>>>(psf, psf, g.gsz, (float)sc);
+	k_scale<<<vec_blocks(g.gsz * nch), RED_THREADS, 0, st>>>(psf, psf, g.gsz * nch, (float)sc);
 	LAUNCHED();
 
 	free_work(full.w, st);
@@ -1784,8 +1833,16 @@ struct bnufft_plan_s {
 	long C;			// batch (product of cim dims >= 3)
 	OpCtx op;
 	float4* traj = nullptr;
-	float2* psf = nullptr;	// DFT order, includes 1/npix
+	float2* psf = nullptr;	// DFT order, includes 1/npix ([K^2][gsz] with a basis)
 	float2* wgt = nullptr;	// weights copy [M, wgt_c]
+	// subspace basis: K = nb coefficients over T frames of MrMs samples each
+	// (nb = 0 without one); the op's samples are all frames' (M = MrMs T),
+	// its channels (coil c, coefficient k) at c + Cc k
+	int nb = 0;
+	int T = 1;
+	long Cc = 1;
+	long MrMs = 0;
+	float2* basis = nullptr;	// [T, K], element t + T k
 	float2* pinv = nullptr;	// circulant preconditioner 1/pre, [N0, N1*N2] DFT order (on demand)
 	// Toeplitz normal on a power-of-two circulant embedding when 2N is not a
 	// power of two: geometry with G = E >= 2N and the PSF re-embedded there
@@ -1995,10 +2052,16 @@ static int check_conf(const bnufft_conf* conf)
 // independent chains of small kernels). It is not joined here: p->psf_ev is
 // recorded after it, and every later use of the PSF waits for that event
 // (psf_wait), so work that does not need the PSF proceeds.
-static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
+static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st, bool own = false)
 {
 	Staged t;
 	TRY(stage_in(t, traj, sizeof(float2) * 3 * p->op.g.M, st));
+
+	if (own) {	// a device buffer of the caller's, freed here like a staged copy
+
+		t.owned = true;
+		t.st = st;
+	}
 	int dev = 0;
 	CUDA_TRY(cudaGetDevice(&dev));
 	const AuxStream* aux = (p->conf.toeplitz && p->psf_ev) ? aux_stream(dev) : nullptr;
@@ -2024,9 +2087,11 @@ static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st)
 		}
 
 		s_psf = compute_psf(p->op.g, (const float2*)t.dev, p->op.kb, &p->psf, pst, 0 != p->conf.deterministic,
-				p->op.wgt, p->op.bin_edge);
+				p->op.wgt, p->op.bin_edge, p->basis, p->nb, p->T, p->MrMs);
 
-		if (BNUFFT_OK == s_psf)
+		// the block PSF of a basis stays on the 2N grid (Bluestein transforms
+		// where 2N is not a power of two)
+		if ((BNUFFT_OK == s_psf) && !p->nb)
 			s_psf = build_toeplitz_embedding(p, pst);
 	}
 
@@ -2075,16 +2140,42 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 		const long bas_dims[], const void* basis,
 		const struct bnufft_conf* conf_in, void* stream)
 {
-	(void)wgh_dims;
-	(void)bas_dims;
 	*plan = nullptr;
 	cudaStream_t st = S(stream);
 
 	if ((N < 4) || (nullptr == traj))
 		return fail(BNUFFT_ERR_ARG, "need N >= 4 dims and a trajectory");
 
-	if (basis)
-		return fail(BNUFFT_ERR_UNSUPPORTED, "subspace basis is not built yet");
+	// subspace basis [1, 1, 1, 1, 1, T, K] (nufft_set_traj,
+	// src/noncart/nufft.c:1018-1042): cim [X, Y, Z, ..., 1 (TE), K (COEFF)],
+	// ksp [1, Mr, Ms, ..., T, 1], trajectory per frame or shared
+	int nb = 0, T = 1;
+
+	if (basis) {
+
+		if (!bas_dims || (N < 7))
+			return fail(BNUFFT_ERR_ARG, "a basis needs its dims and N >= 7");
+
+		for (int i = 0; i < N; i++)
+			if ((5 != i) && (6 != i) && (1 != bas_dims[i]))
+				return fail(BNUFFT_ERR_ARG, "basis dims must be [1, 1, 1, 1, 1, T, K]");
+
+		T = (int)bas_dims[5];
+		nb = (int)bas_dims[6];
+
+		if ((T < 1) || (nb < 1) || (nb > BASIS_MAX_K))
+			return fail(BNUFFT_ERR_UNSUPPORTED, "basis with %d coefficients (at most %d)", nb, (int)BASIS_MAX_K);
+
+		// ksp dim 6 may name the coefficients (the SENSE model passes them,
+		// src/sense/modelnc.c:41-43); the k-space itself has none (out_dims,
+		// src/noncart/nufft.c:1018-1022)
+		if ((ksp_dims[5] != T) || ((1 != ksp_dims[6]) && (nb != ksp_dims[6])) || (1 != cim_dims[5])
+				|| (cim_dims[6] != nb))
+			return fail(BNUFFT_ERR_ARG, "with a basis: ksp dims 5/6 must be T/(1 or K) and image dims 5/6 1/K");
+
+		if ((1 != traj_dims[5]) && (T != traj_dims[5]))
+			return fail(BNUFFT_ERR_ARG, "trajectory frames (dim 5) must be 1 or the basis' T");
+	}
 
 	bnufft_conf conf;
 
@@ -2103,12 +2194,18 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 
 	for (int i = 3; i < N; i++) {
 
+		if (nb && ((5 == i) || (6 == i)))
+			continue;
+
 		if (ksp_dims[i] != cim_dims[i])
 			return fail(BNUFFT_ERR_UNSUPPORTED, "ksp/cim dim %d differ (%ld, %ld)", i, ksp_dims[i], cim_dims[i]);
 
 		if (1 != traj_dims[i])
 			return fail(BNUFFT_ERR_UNSUPPORTED, "trajectory varying along dim %d", i);
 	}
+
+	if (nb && conf.lowmem)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "--lowmem with a basis");
 
 	auto p = new bnufft_plan_s();
 
@@ -2125,8 +2222,12 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 	p->conf = conf;
 	p->C = prod(N - 3, cim_dims + 3);
 	p->st0 = st;
+	p->nb = nb;
+	p->T = T;
+	p->Cc = p->C / std::max(1, nb);
+	p->MrMs = traj_dims[1] * traj_dims[2];
 
-	long M = traj_dims[1] * traj_dims[2];
+	long M = p->MrMs * T;	// all frames' samples
 	int s = init_geom(p->op.g, cim_dims, M, conf.os, conf.width, conf.periodic);
 	p->op.bin_edge = conf.bin;
 	p->op.coils = conf.lowmem ? 1 : (int)std::min<long>(p->C, 1 << 20);
@@ -2141,6 +2242,52 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 		s = fail(BNUFFT_ERR_NOMEM, "trajectory buffer");
 
 	p->op.traj = p->traj;
+
+	if ((BNUFFT_OK == s) && nb) {	// the basis; weights [1, Mr, Ms, 1, 1, T or 1] over all frames' samples
+
+		Staged bs;
+		s = stage_in(bs, basis, sizeof(float2) * T * nb, st);
+
+		if ((BNUFFT_OK == s) && (cudaSuccess != cudaMallocAsync(&p->basis, sizeof(float2) * T * nb, st)))
+			s = fail(BNUFFT_ERR_NOMEM, "basis buffer");
+
+		if ((BNUFFT_OK == s) && (cudaSuccess != cudaMemcpyAsync(p->basis, bs.dev, sizeof(float2) * T * nb, cudaMemcpyDeviceToDevice, st)))
+			s = fail(BNUFFT_ERR_CUDA, "basis copy");
+
+		if (weights && (BNUFFT_OK == s)) {
+
+			bool ok = wgh_dims && (1 == wgh_dims[0]) && (wgh_dims[1] == ksp_dims[1]) && (wgh_dims[2] == ksp_dims[2])
+				&& ((1 == wgh_dims[5]) || (T == wgh_dims[5]));
+
+			for (int i = 3; ok && (i < N); i++)
+				ok = (5 == i) || (1 == wgh_dims[i]);
+
+			if (!ok)
+				s = fail(BNUFFT_ERR_UNSUPPORTED, "with a basis, weights must be [1, Mr, Ms, 1, 1, T or 1]");
+
+			const long wf = ok ? wgh_dims[5] : 1;	// frames the weights hold
+			Staged ws;
+
+			if (BNUFFT_OK == s)
+				s = stage_in(ws, weights, sizeof(float2) * p->MrMs * wf, st);
+
+			if ((BNUFFT_OK == s) && (cudaSuccess != cudaMallocAsync(&p->wgt, sizeof(float2) * M, st)))
+				s = fail(BNUFFT_ERR_NOMEM, "weights buffer");
+
+			for (long t = 0; (BNUFFT_OK == s) && (t < T); t++)
+				if (cudaSuccess != cudaMemcpyAsync(p->wgt + p->MrMs * t, (const float2*)ws.dev + p->MrMs * (t % wf),
+						sizeof(float2) * p->MrMs, cudaMemcpyDeviceToDevice, st))
+					s = fail(BNUFFT_ERR_CUDA, "weights copy");
+
+			p->op.wgt = p->wgt;
+			p->op.wgt_c = 1;
+		}
+
+		if (BNUFFT_OK == s)
+			cudaStreamSynchronize(st);	// the staged inputs are read before they go
+
+		weights = nullptr;	// handled
+	}
 
 	// weights [1, Mr, Ms, 1 or C, 1...] (nufft_set_traj, src/noncart/nufft.c:1041-1049)
 	if ((BNUFFT_OK == s) && weights) {
@@ -2174,8 +2321,29 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 		}
 	}
 
-	if (BNUFFT_OK == s)
+	if ((BNUFFT_OK == s) && nb && (1 == traj_dims[5]) && (T > 1)) {	// one trajectory for all frames
+
+		float2* rep = nullptr;
+		Staged ts;
+		s = stage_in(ts, traj, sizeof(float2) * 3 * p->MrMs, st);
+
+		if ((BNUFFT_OK == s) && (cudaSuccess != cudaMallocAsync(&rep, sizeof(float2) * 3 * M, st)))
+			s = fail(BNUFFT_ERR_NOMEM, "trajectory frames");
+
+		for (long t = 0; (BNUFFT_OK == s) && (t < T); t++)
+			if (cudaSuccess != cudaMemcpyAsync(rep + 3 * p->MrMs * t, ts.dev, sizeof(float2) * 3 * p->MrMs,
+					cudaMemcpyDeviceToDevice, st))
+				s = fail(BNUFFT_ERR_CUDA, "trajectory frames");
+
+		if (BNUFFT_OK == s)
+			s = upload_traj(p, rep, st, true);
+		else if (rep)
+			cudaFreeAsync(rep, st);
+
+	} else if (BNUFFT_OK == s) {
+
 		s = upload_traj(p, traj, st);
+	}
 
 	if (BNUFFT_OK != s) {
 
@@ -2194,6 +2362,9 @@ extern "C" int bnufft_update_traj(bnufft_plan_t p, int N, const long traj_dims[]
 	if (!p || (N != p->N))
 		return fail(BNUFFT_ERR_ARG, "bad plan or dims");
 
+	if (p->nb)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "trajectory update of a plan with a basis");
+
 	for (int i = 0; i < N; i++)
 		if (traj_dims[i] != p->trj_dims[i])
 			return fail(BNUFFT_ERR_ARG, "trajectory dims changed (dim %d)", i);
@@ -2205,15 +2376,58 @@ extern "C" int bnufft_update_traj(bnufft_plan_t p, int N, const long traj_dims[]
 // one coil; results are the same)
 static long coil_chunk(const bnufft_plan_s* p) { return p->conf.lowmem ? 1 : p->C; }
 
+// forward / adjoint with a subspace basis: the NUFFT of every (coil,
+// coefficient) channel at all frames' samples, then the basis contraction
+// over the coefficients (nufft_apply_forward, src/noncart/nufft.c:1443-1453;
+// the adjoint expands with conj(B) first, :1483-1487)
+static int basis_forward(bnufft_plan_s* p, const float2* x, float2* y, cudaStream_t st)
+{
+	const long M = p->op.g.M;
+	float2* tmp = nullptr;
+	CUDA_TRY(cudaMallocAsync(&tmp, sizeof(float2) * M * p->C, st));
+	int s = op_forward(p->op, x, nullptr, p->C, tmp, st);
+
+	if (BNUFFT_OK == s) {
+
+		k_basis_contract<<<vec_blocks(M * p->Cc), RED_THREADS, 0, st>>>(y, tmp, p->basis, p->MrMs, p->T, p->Cc, p->nb);
+		cudaError_t e = cudaGetLastError();
+		g_launches.fetch_add(1, std::memory_order_relaxed);
+		s = (cudaSuccess == e) ? BNUFFT_OK : fail(BNUFFT_ERR_CUDA, "basis contraction: %s", cudaGetErrorString(e));
+	}
+
+	cudaFreeAsync(tmp, st);
+	return s;
+}
+
+static int basis_adjoint(bnufft_plan_s* p, const float2* y, float2* x, cudaStream_t st)
+{
+	const long M = p->op.g.M;
+	float2* tmp = nullptr;
+	CUDA_TRY(cudaMallocAsync(&tmp, sizeof(float2) * M * p->C, st));
+	k_basis_expand<<<vec_blocks(M * p->C), RED_THREADS, 0, st>>>(tmp, y, p->basis, p->MrMs, p->T, p->Cc, p->nb);
+	cudaError_t e = cudaGetLastError();
+	g_launches.fetch_add(1, std::memory_order_relaxed);
+	int s = (cudaSuccess == e) ? op_adjoint(p->op, tmp, nullptr, p->C, 1, x, st)
+				: fail(BNUFFT_ERR_CUDA, "basis expansion: %s", cudaGetErrorString(e));
+	cudaFreeAsync(tmp, st);
+	return s;
+}
+
 extern "C" int bnufft_apply_forward(bnufft_plan_t p, void* dst, const void* src, void* stream)
 {
 	cudaStream_t st = S(stream);
 	const long npix = p->op.g.npix, M = p->op.g.M, cc = coil_chunk(p);
 	size_t in_b = sizeof(float2) * npix * p->C;
-	size_t out_b = sizeof(float2) * M * p->C;
+	size_t out_b = sizeof(float2) * M * (p->nb ? p->Cc : p->C);
 	Staged i, o;
 	TRY(stage_in(i, src, in_b, st));
 	TRY(stage_out_alloc(o, dst, out_b, st));
+
+	if (p->nb) {
+
+		TRY(basis_forward(p, (const float2*)i.dev, (float2*)o.dev, st));
+		return stage_out_copy(o, dst, out_b, st);
+	}
 
 	for (long c0 = 0; c0 < p->C; c0 += cc)
 		TRY(op_forward(p->op, (const float2*)i.dev + npix * c0, nullptr, std::min(cc, p->C - c0),
@@ -2226,11 +2440,17 @@ extern "C" int bnufft_apply_adjoint(bnufft_plan_t p, void* dst, const void* src,
 {
 	cudaStream_t st = S(stream);
 	const long npix = p->op.g.npix, M = p->op.g.M, cc = coil_chunk(p);
-	size_t in_b = sizeof(float2) * M * p->C;
+	size_t in_b = sizeof(float2) * M * (p->nb ? p->Cc : p->C);
 	size_t out_b = sizeof(float2) * npix * p->C;
 	Staged i, o;
 	TRY(stage_in(i, src, in_b, st));
 	TRY(stage_out_alloc(o, dst, out_b, st));
+
+	if (p->nb) {
+
+		TRY(basis_adjoint(p, (const float2*)i.dev, (float2*)o.dev, st));
+		return stage_out_copy(o, dst, out_b, st);
+	}
 
 	for (long c0 = 0; c0 < p->C; c0 += cc)
 		TRY(op_adjoint(p->op, (const float2*)i.dev + M * c0, nullptr, std::min(cc, p->C - c0), 1,
@@ -2246,6 +2466,29 @@ extern "C" int bnufft_apply_normal(bnufft_plan_t p, void* dst, const void* src, 
 	Staged i, o;
 	TRY(stage_in(i, src, b, st));
 	TRY(stage_out_alloc(o, dst, b, st));
+
+	if (p->nb) {	// block-Toeplitz, or the adjoint of the forward
+
+		if (p->psf) {
+
+			psf_wait(p, st);
+			TRY(op_toeplitz_basis(p->op, p->psf, (const float2*)i.dev, p->Cc, p->nb, (float2*)o.dev, st));
+
+		} else {
+
+			float2* k = nullptr;
+			CUDA_TRY(cudaMallocAsync(&k, sizeof(float2) * p->op.g.M * p->Cc, st));
+			int s = basis_forward(p, (const float2*)i.dev, k, st);
+
+			if (BNUFFT_OK == s)
+				s = basis_adjoint(p, k, (float2*)o.dev, st);
+
+			cudaFreeAsync(k, st);
+			TRY(s);
+		}
+
+		return stage_out_copy(o, dst, b, st);
+	}
 
 	if (p->psf) {
 
@@ -2271,6 +2514,9 @@ extern "C" int bnufft_get_psf_dims(bnufft_plan_t p, int ND, long psf_dims[])
 {
 	if (!p || !p->psf)
 		return fail(BNUFFT_ERR_ARG, "plan has no PSF");
+
+	if (p->nb)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "the block PSF of a basis in the decomposed layout");
 
 	if (ND != p->N + 1)
 		return fail(BNUFFT_ERR_ARG, "PSF has N+1 = %d dims", p->N + 1);
@@ -2364,6 +2610,7 @@ extern "C" void bnufft_free(bnufft_plan_t p)
 	if (p->wgt) cudaFreeAsync(p->wgt, st);
 	if (p->pinv) cudaFreeAsync(p->pinv, st);
 	if (p->op.wbuf) cudaFreeAsync(p->op.wbuf, st);
+	if (p->basis) cudaFreeAsync(p->basis, st);
 
 	if (p->psf_ev)
 		cudaEventDestroy(p->psf_ev);
@@ -2453,6 +2700,9 @@ extern "C" int bnufft_nufft_inverse(bnufft_plan_t p, void* img, const void* ksp,
 
 	if (!p || (maxiter < 0))
 		return fail(BNUFFT_ERR_ARG, "bad plan or iteration count");
+
+	if (p->nb)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "nufft -i with a basis");
 
 	OpCtx& op = p->op;
 	const long C = p->C;

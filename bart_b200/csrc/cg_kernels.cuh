@@ -855,4 +855,120 @@ __global__ void k_traj_convert(float4* __restrict__ dst, const float2* __restric
 		dst[i] = make_float4(src[3 * i + 0].x * factor, src[3 * i + 1].x * factor, src[3 * i + 2].x * factor, 0.f);
 }
 
+// Subspace basis (nufft_create2 with a basis, src/noncart/nufft.c:1427-1491,
+// 1546-1625). Samples of all T frames form one list of Mt = MrMs * T samples
+// (frame t at [t MrMs, (t + 1) MrMs)); the NUFFT's channels are (c, k), c <
+// Cc coils, k < K coefficients, channel c + Cc k; k-space is the
+// reference's [1, Mr, Ms, Cc, 1, T] array, element m + MrMs (c + Cc t); the
+// basis [1, 1, 1, 1, 1, T, K], element t + T k.
+
+// forward: ksp[m, c, t] = sum_k B[t, k] tmp[t MrMs + m, c + Cc k]
+// (md_ztenmul over COEFF, :1450-1453)
+__global__ void k_basis_contract(float2* __restrict__ ksp, const float2* __restrict__ tmp, const float2* __restrict__ B,
+		long MrMs, int T, long Cc, int K)
+{
+	const long Mt = MrMs * T;
+	const long n = Mt * Cc;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		const long m = i % MrMs;
+		const long c = (i / MrMs) % Cc;
+		const int t = (int)(i / (MrMs * Cc));
+		float2 acc = make_float2(0.f, 0.f);
+
+		for (int k = 0; k < K; k++) {
+
+			const float2 v = tmp[t * MrMs + m + Mt * (c + Cc * k)];
+			const float2 b = B[t + (long)T * k];
+			acc.x = fmaf(b.x, v.x, fmaf(-b.y, v.y, acc.x));
+			acc.y = fmaf(b.x, v.y, fmaf(b.y, v.x, acc.y));
+		}
+
+		ksp[i] = acc;
+	}
+}
+
+// adjoint: tmp[t MrMs + m, c + Cc k] = conj(B[t, k]) ksp[m, c, t]
+// (md_ztenmulc, :1483-1487)
+__global__ void k_basis_expand(float2* __restrict__ tmp, const float2* __restrict__ ksp, const float2* __restrict__ B,
+		long MrMs, int T, long Cc, int K)
+{
+	const long Mt = MrMs * T;
+	const long n = Mt * Cc * K;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		const long mt = i % Mt;			// t MrMs + m
+		const long ch = i / Mt;			// c + Cc k
+		const long c = ch % Cc;
+		const int k = (int)(ch / Cc);
+		const int t = (int)(mt / MrMs);
+		const long m = mt % MrMs;
+		tmp[i] = cmulc(ksp[m + MrMs * (c + Cc * t)], B[t + (long)T * k]);
+	}
+}
+
+// the PSF's k-space for coefficient pair j = k + K k' (compute_square_basis
+// and the adjoint's conjugate, :470-505, 535-586):
+// w[s, j] = conj(B[t(s), k]) B[t(s), k'] |wgt[s]|^2 (wgt: Mt sample weights or null)
+__global__ void k_basis_psf_weights(float2* __restrict__ w, const float2* __restrict__ B,
+		const float2* __restrict__ wgt, long MrMs, int T, int K)
+{
+	const long Mt = MrMs * T;
+	const long n = Mt * K * K;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		const long s = i % Mt;
+		const int j = (int)(i / Mt);
+		const int k = j % K, kp = j / K;
+		const int t = (int)(s / MrMs);
+		float2 v = cmulc(B[t + (long)T * kp], B[t + (long)T * k]);
+
+		if (wgt) {
+
+			const float2 u = wgt[s];
+			const float a = u.x * u.x + u.y * u.y;
+			v = make_float2(v.x * a, v.y * a);
+		}
+
+		w[i] = v;
+	}
+}
+
+enum { BASIS_MAX_K = 32 };
+
+// the block-Toeplitz product on the spectrum (md_ztenmul with the psf
+// [K (out)][K (in)], :1586-1592): spec[g, c + Cc k] <- sum_k'
+// P[g, k + K k'] spec[g, c + Cc k'], for every cell g < gsz and coil c
+__global__ void k_basis_mix(float2* __restrict__ spec, const float2* __restrict__ P, long gsz, long Cc, int K)
+{
+	const long n = gsz * Cc;
+
+	for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		const long g = i % gsz;
+		const long c = i / gsz;
+		float2 x[BASIS_MAX_K];
+
+		for (int k = 0; k < K; k++)
+			x[k] = spec[g + gsz * (c + Cc * k)];
+
+		for (int k = 0; k < K; k++) {
+
+			float2 acc = make_float2(0.f, 0.f);
+
+			for (int kp = 0; kp < K; kp++) {
+
+				const float2 pv = P[g + gsz * (k + (long)K * kp)];
+				acc.x = fmaf(pv.x, x[kp].x, fmaf(-pv.y, x[kp].y, acc.x));
+				acc.y = fmaf(pv.x, x[kp].y, fmaf(pv.y, x[kp].x, acc.y));
+			}
+
+			spec[g + gsz * (c + Cc * k)] = acc;
+		}
+	}
+}
+
 } // namespace bn

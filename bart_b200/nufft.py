@@ -169,8 +169,10 @@ def nufft_create2(ksp_dims, cim_dims, traj_dims, traj, wgh_dims=None, weights=No
     ``traj`` is the reference's [3, Mr, Ms] complex64 trajectory (numpy, or a
     torch tensor on the device). ``weights`` (density compensation / sampling
     pattern, ``bart nufft -p``) is [1, Mr, Ms] or [1, Mr, Ms, C]; with the
-    Toeplitz PSF it must be shared by all channels. A subspace basis is not
-    built yet.
+    Toeplitz PSF it must be shared by all channels. ``basis`` (``bart nufft
+    -B``) is [1, 1, 1, 1, 1, T, K]: then cim_dims has K coefficients in dim 6,
+    ksp_dims T frames in dim 5, the trajectory 1 or T frames in dim 5 and the
+    weights [1, Mr, Ms, 1, 1, T or 1].
     """
     lib = _lib.load()
     conf = conf or NufftConf()
@@ -181,14 +183,20 @@ def nufft_create2(ksp_dims, cim_dims, traj_dims, traj, wgh_dims=None, weights=No
         wd = dims16(wgh_dims if wgh_dims is not None else np.shape(weights))
         wd_arr = _lib.dims_array(wd)
         pw, keep_w = _ptr_in(weights, int(np.prod(wd)))
+    bd_arr, pb, keep_b = None, None, None
     if basis is not None:
-        raise _lib.BnufftError(2, "subspace basis is not built yet")
+        bd = dims16(bas_dims if bas_dims is not None else np.shape(basis))
+        bd_arr = _lib.dims_array(bd)
+        pb, keep_b = _ptr_in(basis, int(np.prod(bd)))
     h = ctypes.c_void_p()
     cc = conf.c()
     _lib.check(lib.bnufft_create2(ctypes.byref(h), 16, _lib.dims_array(kd), _lib.dims_array(cd),
-                                  _lib.dims_array(td), pt, wd_arr, pw, None, None, ctypes.byref(cc),
+                                  _lib.dims_array(td), pt, wd_arr, pw, bd_arr, pb, ctypes.byref(cc),
                                   _stream_of(traj)))
-    del keep, keep_w
+    del keep, keep_w, keep_b
+    if basis is not None:   # the k-space has the basis' frames and no coefficient dim
+        kd = list(kd)
+        kd[5], kd[6] = bd[5], 1
     op = Linop(h, cd, kd, has_normal=True)
     op._traj_dims = td
     return op

@@ -63,7 +63,15 @@ void bnufft_conf_defaults(struct bnufft_conf* conf);
  * k-space dims (per coil; not with the Toeplitz PSF or --lowmem): the
  * forward multiplies its k-space by them, the adjoint its input by their
  * conjugate (src/noncart/nufft.c:1457, 1477).
- * basis must be NULL (BNUFFT_ERR_UNSUPPORTED otherwise). The plan copies
+ * basis (bart nufft/pics -B, the subspace basis of nufft_set_traj,
+ * src/noncart/nufft.c:1018-1042) may be NULL or [1, 1, 1, 1, 1, T, K]
+ * with K <= 32: then cim_dims has the K coefficients in dim 6 (dim 5 = 1),
+ * ksp_dims the T frames in dim 5 (dim 6 = 1), traj_dims 1 or T frames in
+ * dim 5, and weights are [1, Mr, Ms, 1, 1, T or 1]. The forward is
+ * y_t = sum_k B[t, k] NUFFT_t(x_k) (:1443-1453), the normal with Toeplitz
+ * the block PSF P[k, k'] = sum_t conj(B[t, k]) B[t, k'] PSF_t (:470-505,
+ * 1546-1625). Not with --lowmem, trajectory updates, nufft -i or
+ * bnufft_get_psf. The plan copies
  * the trajectory and weights (the caller keeps its buffers) and, with
  * conf->toeplitz, computes the PSF on the device (compute_psf2,
  * src/noncart/nufft.c:727-776). */

@@ -504,6 +504,59 @@ def _as4(a):
 
 
 # ---------------------------------------------------------------------------
+# Subspace basis (nufft_create2 with a basis, src/noncart/nufft.c:1018-1042,
+# 1427-1491, 1546-1625, 470-505)
+# ---------------------------------------------------------------------------
+
+class BasisNufftOracle:
+    """NUFFT with a temporal basis B [T, K]: frame t has its own trajectory
+    (or the shared one) and optional sampling weights w_t;
+    y_t = w_t * sum_k B[t, k] NUFFT_t(x_k), adjoint x_k = sum_t conj(B[t, k])
+    NUFFT_t^H(conj(w_t) y_t). Images [X, Y, Z, C, K] (coils C), k-space
+    [M, C, T] (M samples of one frame)."""
+
+    def __init__(self, trajs, dims, basis, weights=None):
+        self.B = np.asarray(basis, dtype=np.complex128).reshape(-1, np.shape(basis)[-1], order="F")  # [T, K]
+        self.T, self.K = self.B.shape
+        self.ops = [NufftOracle(trajs[t if len(trajs) > 1 else 0], dims) for t in range(self.T)]
+        self.w = None if weights is None else [np.asarray(weights[t]).reshape(-1).astype(np.complex128)
+                                               for t in range(self.T)]
+
+    def forward(self, x):
+        x = np.asarray(x, dtype=np.complex128)      # [X, Y, Z, C, K]
+        out = []
+        for t, op in enumerate(self.ops):
+            y = sum(self.B[t, k] * op.forward(x[..., k]) for k in range(self.K))
+            out.append(y if self.w is None else y * self.w[t][:, None])
+        return np.stack(out, axis=-1)               # [M, C, T]
+
+    def adjoint(self, y):
+        y = np.asarray(y, dtype=np.complex128)      # [M, C, T]
+        acc = None
+        for t, op in enumerate(self.ops):
+            yt = y[..., t] if self.w is None else y[..., t] * np.conj(self.w[t])[:, None]
+            a = op.adjoint(yt)                      # [X, Y, Z, C]
+            v = np.stack([np.conj(self.B[t, k]) * a for k in range(self.K)], axis=-1)
+            acc = v if acc is None else acc + v
+        return acc
+
+    def normal_toeplitz(self, x):
+        """sum_t conj(B[t, k]) B[t, k'] applied to each frame's Toeplitz
+        normal (with |w_t|^2 weights): the block-Toeplitz product."""
+        x = np.asarray(x, dtype=np.complex128)
+        out = np.zeros_like(x)
+        for t, op in enumerate(self.ops):
+            if self.w is not None and op.weights is None:
+                op.weights = self.w[t].astype(np.complex64)
+                op._psf = None
+            for kp in range(self.K):
+                n = op.normal_toeplitz(x[..., kp])
+                for k in range(self.K):
+                    out[..., k] += np.conj(self.B[t, k]) * self.B[t, kp] * n
+        return out
+
+
+# ---------------------------------------------------------------------------
 # SENSE model, data scaling and CG (pics -l2 -r lambda -t ...)
 # ---------------------------------------------------------------------------
 

@@ -88,6 +88,19 @@ struct linop_s* nufft_create2_bnufft(int N, const long ksp_dims[N], const long c
 
 	debug_printf(DP_DEBUG1, "NUFFT: libbnufft (GPU)%s\n", conf.toeplitz ? ", Toeplitz" : "");
 
-	return linop_create(N, ksp_dims, N, cim_dims, CAST_UP(PTR_PASS(data)),
+	// the k-space the linop maps to: with a basis it has the basis' frames
+	// and no coefficient dim (out_dims, src/noncart/nufft.c:1018-1022, 1260)
+	long out_dims[N];
+
+	for (int i = 0; i < N; i++)
+		out_dims[i] = ksp_dims[i];
+
+	if (basis) {
+
+		out_dims[5] = bas_dims[5];
+		out_dims[6] = 1;
+	}
+
+	return linop_create(N, out_dims, N, cim_dims, CAST_UP(PTR_PASS(data)),
 			bn_forward, bn_adjoint, conf.toeplitz ? bn_normal : NULL, NULL, bn_free);
 }

@@ -3,7 +3,7 @@
  * normal operator and the PSF, which the reference's command-line tools do
  * not print directly. Test infrastructure only.
  *
- *   refnormal [-P] [--no-toeplitz] [-p pattern] traj img out [psf_out]
+ *   refnormal [-P] [--no-toeplitz] [-p pattern] [-B basis] traj img out [psf_out]
  *
  * out = N^H N img, with N = nufft_create2(..., conf) and conf.toeplitz set
  * (src/noncart/nufft.c:1174-1276, normal at :1740 -> toeplitz_mult :1546).
@@ -29,6 +29,7 @@ int main(int argc, char* argv[])
 	bool periodic = false;
 	bool toeplitz = true;
 	const char* pattern_file = NULL;
+	const char* basis_file = NULL;
 	int a = 1;
 
 	while ((a < argc) && ('-' == argv[a][0])) {
@@ -39,6 +40,8 @@ int main(int argc, char* argv[])
 			toeplitz = false;
 		else if ((0 == strcmp(argv[a], "-p")) && (a + 1 < argc))
 			pattern_file = argv[++a];
+		else if ((0 == strcmp(argv[a], "-B")) && (a + 1 < argc))
+			basis_file = argv[++a];
 		else
 			error("unknown option %s\n", argv[a]);
 		a++;
@@ -65,7 +68,17 @@ int main(int argc, char* argv[])
 	long pat_dims[DIMS];
 	complex float* pattern = (NULL != pattern_file) ? load_cfl(pattern_file, DIMS, pat_dims) : NULL;
 
-	const struct linop_s* op = nufft_create2(DIMS, ksp_dims, img_dims, trj_dims, traj, pat_dims, pattern, NULL, NULL, conf);
+	long bas_dims[DIMS];
+	complex float* basis = (NULL != basis_file) ? load_cfl(basis_file, DIMS, bas_dims) : NULL;
+
+	if (NULL != basis) {	// as the nufft tool's forward (src/nufft.c:284-288)
+
+		ksp_dims[TE_DIM] = bas_dims[TE_DIM];
+		ksp_dims[COEFF_DIM] = 1;
+	}
+
+	const struct linop_s* op = nufft_create2(DIMS, ksp_dims, img_dims, trj_dims, traj, pat_dims, pattern,
+			bas_dims, basis, conf);
 
 	complex float* out = create_cfl(argv[a + 2], DIMS, img_dims);
 
@@ -81,7 +94,7 @@ int main(int argc, char* argv[])
 		md_free(ksp);
 	}
 
-	if (toeplitz && ((argc - a) > 3)) {
+	if (toeplitz && (NULL == basis) && ((argc - a) > 3)) {
 
 		long psf_dims[DIMS + 1];
 		int ND = nufft_get_psf_dims(op, DIMS + 1, psf_dims);

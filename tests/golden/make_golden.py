@@ -13,6 +13,7 @@ read the .npz files and never run the reference.
     python tests/golden/make_golden.py --fullsize # only the C1 / C2 full-size cases
     python tests/golden/make_golden.py --gpu-gridding  # the reference's GPU-gridding test inputs
     python tests/golden/make_golden.py --kooshball     # 3D kooshball at 32^3, 2 coils
+    python tests/golden/make_golden.py --basis         # subspace basis (nufft / pics -B)
 """
 
 from __future__ import annotations
@@ -287,7 +288,99 @@ def uneven_cases():
               runs=[("x5_w1", ["-i5", "-w1"]), ("x5_w1_notoep", ["-i5", "-w1", "--no-toeplitz"])])
 
 
+def basis_nufft_case(name, traj, img, basis, pattern=None):
+    """nufft -B (forward, adjoint) and the Toeplitz / explicit normal with
+    the basis: img [X, Y, 1, C, 1, 1, K], basis [1, 1, 1, 1, 1, T, K],
+    traj [3, Mr, Ms(, 1, 1, T)], pattern [1, Mr, Ms, 1, 1, T]."""
+    with tempfile.TemporaryDirectory() as d:
+        rng = np.random.default_rng(zlib.crc32(name.encode()))
+        writecfl(os.path.join(d, "t"), traj)
+        writecfl(os.path.join(d, "x"), img)
+        writecfl(os.path.join(d, "b"), basis)
+        P = ["-B", "b"]
+        if pattern is not None:
+            writecfl(os.path.join(d, "w"), pattern)
+            P += ["-p", "w"]
+        run("nufft", *P, "t", "x", "k", cwd=d)
+        fwd = readcfl(os.path.join(d, "k"))
+        ksp = cplx(rng, fwd.shape)
+        writecfl(os.path.join(d, "y"), ksp)
+        dims = ":".join(str(s) for s in (list(img.shape) + [1, 1])[:3])
+        run("nufft", *P, "-a", f"-x{dims}", "t", "y", "a", cwd=d)
+        adj = readcfl(os.path.join(d, "a"))
+        run("refnormal", *P, "t", "x", "n", cwd=d)
+        nrm = readcfl(os.path.join(d, "n"))
+        run("refnormal", *P, "--no-toeplitz", "t", "x", "ne", cwd=d)
+        nre = readcfl(os.path.join(d, "ne"))
+    out = dict(traj=traj, img=img, basis=basis, fwd=fwd, ksp=ksp, adj=adj, normal=nrm, normal_explicit=nre)
+    if pattern is not None:
+        out["pattern"] = pattern
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **{k: np.asarray(v) for k, v in out.items()})
+    print(name, {k: np.shape(v) for k, v in out.items()})
+
+
+def basis_pics_case(name, traj, ksp, sens, basis, pattern, iters=10):
+    """pics -B with a sampling pattern (tests/pics.mk test-pics-basis-noncart
+    style): -l2 -r0.01 -i iters, automatic scaling, Toeplitz. Also stores the
+    reference's own spread: its Toeplitz against its explicit normal
+    (--no-toeplitz), the float32 sensitivity of these unconverged iterates."""
+    with tempfile.TemporaryDirectory() as d:
+        for n, a in (("t", traj), ("k", ksp), ("s", sens), ("b", basis), ("w", pattern)):
+            writecfl(os.path.join(d, n), a)
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        run("pics", "-l2", "-r0.01", f"-i{iters}", "-B", "b", "-p", "w", "-t", "t", "k", "s", "o", cwd=d, env=env)
+        out = readcfl(os.path.join(d, "o"))
+        run("pics", "-l2", "-r0.01", f"-i{iters}", "-B", "b", "-p", "w", "--no-toeplitz", "-t", "t", "k", "s", "e",
+            cwd=d, env=env)
+        spread = float(np.linalg.norm(readcfl(os.path.join(d, "e")) - out) / np.linalg.norm(out))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), traj=traj, ksp=ksp, sens=sens, basis=basis,
+                        pattern=pattern, out=out, iters=iters, spread=spread)
+    print(name, out.shape, "reference spread", spread)
+
+
+def basis_cases():
+    rng = np.random.default_rng(555)
+    T, K = 4, 3
+    with tempfile.TemporaryDirectory() as d:
+        run("traj", "-r", "-G", "-x32", "-o2", "-y48", "t", cwd=d)
+        t48 = readcfl(os.path.join(d, "t"))            # [3, 64, 48]
+    # frame t: spokes t, t + 4, ... (interleaved golden-angle frames)
+    tf = np.stack([t48[:, :, f::T] for f in range(T)], axis=-1).reshape(3, 64, 12, 1, 1, T, order="F")
+    basis = cplx(rng, (1, 1, 1, 1, 1, T, K)) / np.float32(2.0)
+    img = cplx(rng, (32, 32, 1, 2, 1, 1, K))
+    basis_nufft_case("nufft2d_n32_basis", tf, img, basis)
+    # one trajectory shared by all frames, a sampling pattern per frame
+    pat = np.zeros((1, 64, 12, 1, 1, T), dtype=np.complex64)
+    for f in range(T):
+        pat[0, :, f::T, 0, 0, f] = 1.0                 # frame f keeps spokes f, f + 4, ... of the shared 12
+    basis_nufft_case("nufft2d_n32_basis_shared", t48[:, :, :12], img, basis, pattern=pat)
+    # pics -B on a sampled phantom: an orthonormal basis (as a subspace
+    # basis from an SVD is), 24 spokes per frame, coil maps from the SENSE
+    # generator
+    with tempfile.TemporaryDirectory() as d:
+        run("traj", "-r", "-G", "-x32", "-o2", "-y96", "t", cwd=d)
+        t96 = readcfl(os.path.join(d, "t"))
+    tf = np.stack([t96[:, :, f::T] for f in range(T)], axis=-1).reshape(3, 64, 24, 1, 1, T, order="F")
+    q, _ = np.linalg.qr(rng.standard_normal((T, K)) + 1j * rng.standard_normal((T, K)))
+    basis = q.astype(np.complex64).reshape(1, 1, 1, 1, 1, T, K, order="F")
+    N, C = 32, 4
+    sens = synth.coil_maps(N, C, rng)
+    truth = np.stack([synth.ellipse_phantom(N, 8, rng) for _ in range(K)], axis=-1).reshape(N, N, 1, 1, 1, 1, K)
+    from oracle import nufft_oracle as orc
+    ksp = np.zeros((1, 64, 24, C, 1, T), dtype=np.complex64)
+    for f in range(T):
+        A = orc.SenseOracle(tf[..., 0, 0, f].real.reshape(3, -1, order="F"), sens)
+        xf = sum(basis[0, 0, 0, 0, 0, f, k] * truth[..., 0, 0, k].reshape(N, N, 1, 1) for k in range(K))
+        ksp[:, :, :, :, 0, f] = A.forward(xf).reshape(1, 64, 24, C, order="F").astype(np.complex64)
+    ksp = synth.add_noise(ksp, 40.0, rng)
+    pat2 = np.ones((1, 64, 24, 1, 1, T), dtype=np.complex64)
+    basis_pics_case("pics2d_n32_basis", tf, ksp, sens.astype(np.complex64), basis, pat2)
+
+
 def main():
+    if "--basis" in sys.argv:
+        basis_cases()
+        return
     if "--uneven" in sys.argv:
         uneven_cases()
         return

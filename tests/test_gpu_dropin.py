@@ -79,3 +79,33 @@ def test_dropin_pics(key, args, tol):
         r = _run(d, exe, "-d4", "-l2", "-r0.01", *args, "-t", "t", "k", "s", "o")
         assert "libbnufft" in r.stderr + r.stdout      # the adapter built the NUFFT
         assert rel(readcfl(os.path.join(d, "o")), g[key]) < tol
+
+
+def test_dropin_nufft_basis():
+    """bart nufft -B (forward and adjoint with a temporal basis) on the
+    library's NUFFT."""
+    exe = _tool("nufft_bnufft")
+    g = golden("nufft2d_n32_basis")
+    with tempfile.TemporaryDirectory() as d:
+        for n in ("traj", "img", "ksp", "basis"):
+            writecfl(os.path.join(d, n), g[n])
+        _run(d, exe, "-B", "basis", "traj", "img", "k")
+        _run(d, exe, "-a", "-B", "basis", "-x32:32:1", "traj", "ksp", "a")
+        assert rel(readcfl(os.path.join(d, "k")), g["fwd"]) < 1e-5
+        assert rel(readcfl(os.path.join(d, "a")), g["adj"]) < 1e-5
+
+
+def test_dropin_pics_basis():
+    """bart pics -B (subspace reconstruction, tests/pics.mk's basis cases):
+    the reference's SENSE model with the basis and its CG on the library's
+    block-Toeplitz NUFFT, against its CPU output (orthonormal basis of 3
+    over 4 frames, 10 iterations, automatic scaling; measured 2.4e-6)."""
+    exe = _tool("pics_bnufft")
+    g = golden("pics2d_n32_basis")
+    with tempfile.TemporaryDirectory() as d:
+        for n, k in (("t", "traj"), ("k", "ksp"), ("s", "sens"), ("b", "basis"), ("w", "pattern")):
+            writecfl(os.path.join(d, n), g[k])
+        r = _run(d, exe, "-d4", "-l2", "-r0.01", f"-i{int(g['iters'])}", "-B", "b", "-p", "w", "-t", "t",
+                 "k", "s", "o")
+        assert "libbnufft" in r.stderr + r.stdout
+        assert rel(readcfl(os.path.join(d, "o")), g["out"]) < 1e-4

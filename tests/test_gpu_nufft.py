@@ -66,6 +66,55 @@ def test_toeplitz_normal_and_psf_vs_reference(name, periodic):
     op.free()
 
 
+def _basis_plan(g, toeplitz):
+    w = g.get("pattern")
+    return nufft_create2(list(g["fwd"].shape), list(g["img"].shape), list(g["traj"].shape), g["traj"],
+                         None if w is None else list(w.shape), w, list(g["basis"].shape), g["basis"],
+                         conf=NufftConf(toeplitz=toeplitz))
+
+
+@pytest.mark.parametrize("name", ["nufft2d_n32_basis", "nufft2d_n32_basis_shared"])
+def test_basis_vs_reference(name):
+    """Subspace basis (nufft -B): forward, adjoint, block-Toeplitz normal and
+    the explicit normal against the reference's outputs; frames with their
+    own trajectories, or one trajectory with a per-frame sampling pattern."""
+    g = golden(name)
+    op = _basis_plan(g, toeplitz=True)
+    cd, kd = list(g["img"].shape), list(g["fwd"].shape)
+    assert rel(op.forward(g["img"]), g["fwd"]) < TOL
+    assert rel(op.adjoint(g["ksp"].reshape(kd, order="F")), g["adj"]) < TOL
+    assert rel(op.normal(g["img"]), g["normal"]) < TOL
+    op.free()
+    op = _basis_plan(g, toeplitz=False)
+    assert rel(op.normal(g["img"].reshape(cd, order="F")), g["normal_explicit"]) < TOL
+    op.free()
+
+
+def test_basis_uneven_size_and_3d_vs_oracle():
+    """The basis on a non-power-of-two side (Bluestein spectra, block PSF on
+    the 2N grid) and in 3D, against the oracle."""
+    rng = np.random.default_rng(41)
+    T, K, C = 3, 2, 2
+    for N, ndim, spokes in ((40, 2, 30), (12, 3, 60)):
+        t = synth.radial_traj(N, spokes) if ndim == 2 else synth.kooshball_traj(N, spokes)
+        S = t.shape[2] // T
+        tf = np.stack([t[:, :, f * S:(f + 1) * S] for f in range(T)], axis=-1).reshape(3, t.shape[1], S, 1, 1, T,
+                                                                                    order="F")
+        B = (rng.standard_normal((1, 1, 1, 1, 1, T, K)) + 1j * rng.standard_normal((1, 1, 1, 1, 1, T, K))).astype(
+            np.complex64)
+        Z = N if ndim == 3 else 1
+        cd = [N, N, Z, C, 1, 1, K]
+        kd = [1, t.shape[1], S, C, 1, T]
+        x = (rng.standard_normal(cd) + 1j * rng.standard_normal(cd)).astype(np.complex64)
+        op = nufft_create2(kd, cd, list(tf.shape), tf, None, None, list(B.shape), B, conf=NufftConf(toeplitz=True))
+        o = orc.BasisNufftOracle([tf[..., 0, 0, f].real.reshape(3, -1, order="F") for f in range(T)], (N, N, Z),
+                                 B.reshape(T, K, order="F"))
+        xo = x.reshape(N, N, Z, C, K, order="F")
+        assert rel(op.forward(x), o.forward(xo)) < TOL, (N, ndim)
+        assert rel(op.normal(x), o.normal_toeplitz(xo)) < TOL, (N, ndim)
+        op.free()
+
+
 @pytest.mark.parametrize("N,spokes,coils", [(128, 64, 1), (64, 40, 2), (256, 402, 1), (512, 100, 1),
                                             (66, 30, 2), (200, 64, 1), (318, 90, 1), (320, 40, 2)])
 def test_2d_vs_oracle(N, spokes, coils):

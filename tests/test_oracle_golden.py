@@ -215,3 +215,33 @@ def test_kooshball_32_two_coils():
     assert rel(o.forward(img), g["fwd"].reshape(-1, 2, order="F")) < OPS_TOL
     assert rel(o.adjoint(ksp.reshape(-1, 2, order="F")), g["adj"].reshape(32, 32, 32, 2, order="F")) < OPS_TOL
     assert rel(o.normal_toeplitz(img), g["normal"].reshape(32, 32, 32, 2, order="F")) < OPS_TOL
+
+
+def _basis_oracle(g):
+    """BasisNufftOracle of a basis fixture and its image [X, Y, 1, C, K]."""
+    tr = g["traj"].real
+    T, K = g["basis"].shape[5], g["basis"].shape[6]
+    if tr.ndim >= 6 and tr.shape[5] == T:
+        trajs = [tr[..., 0, 0, t].reshape(3, -1, order="F") for t in range(T)]
+    else:
+        trajs = [tr.reshape(3, -1, order="F")]
+    w = None
+    if "pattern" in g:
+        w = [g["pattern"][0, :, :, 0, 0, t].reshape(-1, order="F") for t in range(T)]
+    img = g["img"]
+    X, Y, C = img.shape[0], img.shape[1], img.shape[3]
+    op = orc.BasisNufftOracle(trajs, (X, Y, 1), g["basis"].reshape(T, K, order="F"), w)
+    return op, img.reshape(X, Y, 1, C, K, order="F"), (X, Y, C, K, T)
+
+
+@pytest.mark.parametrize("name", ["nufft2d_n32_basis", "nufft2d_n32_basis_shared"])
+def test_basis_forward_adjoint_normal(name):
+    """nufft -B: forward, adjoint, Toeplitz and explicit normal with a
+    temporal basis (per-frame trajectories; or a shared trajectory with a
+    per-frame sampling pattern) against the reference."""
+    g = golden(name)
+    op, x, (X, Y, C, K, T) = _basis_oracle(g)
+    assert rel(op.forward(x), g["fwd"].reshape(-1, C, T, order="F")) < OPS_TOL
+    assert rel(op.adjoint(g["ksp"].reshape(-1, C, T, order="F")), g["adj"].reshape(x.shape, order="F")) < OPS_TOL
+    assert rel(op.normal_toeplitz(x), g["normal"].reshape(x.shape, order="F")) < OPS_TOL
+    assert rel(op.adjoint(op.forward(x)), g["normal_explicit"].reshape(x.shape, order="F")) < OPS_TOL
