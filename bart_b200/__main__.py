@@ -1,7 +1,7 @@
 """Command line mirror of ``bart nufft`` and ``bart pics -t`` with .cfl I/O.
 
   python -m bart_b200 nufft [-a|-i [-c] [-l lambda] [-m iter]] [-x X:Y:Z] [-P] [-r|-t]
-                            [-p pattern] traj input output
+                            [-p pattern] [-B basis] traj input output
   python -m bart_b200 pics -l2 -r lambda [-i iter] -t traj [-w scale] [-S]
                            [--no-toeplitz] ksp sens output
   python -m bart_b200 -l flags pics ...   (or -p flags: the same here)
@@ -64,8 +64,13 @@ def main_nufft(argv) -> int:
     ap.add_argument("-l", dest="lam", type=float, default=0.0)
     ap.add_argument("-m", dest="iters", type=int, default=50)
     ap.add_argument("-p", dest="pattern")
+    ap.add_argument("-B", dest="basis", help="temporal (or other) basis [1,1,1,1,1,T,K]")
     ap.add_argument("-s", dest="dft", action="store_true", help="direct non-uniform DFT")
     ap.add_argument("--lowmem", action="store_true", help="one coil's oversampled grid at a time")
+    # the reference's other memory modes change what it holds, not its results;
+    # the library precomputes no linear phases or fftmod tables, so they are accepted as they are
+    ap.add_argument("--zero-mem", action="store_true", help="accepted (the reference's zero-overhead mode)")
+    ap.add_argument("--no-precomp", action="store_true", help="accepted (no precomputed tables)")
     ap.add_argument("traj")
     ap.add_argument("input")
     ap.add_argument("output")
@@ -79,6 +84,31 @@ def main_nufft(argv) -> int:
     conf = NufftConf(toeplitz=a.inverse and not a.no_toeplitz, periodic=a.periodic, lowmem=a.lowmem)
     inp = readcfl(a.input)
     pat = readcfl(a.pattern) if a.pattern else None
+    bas = readcfl(a.basis) if a.basis else None
+    bd = None if bas is None else (list(bas.shape) + [1] * 16)[:16]
+    pd = None if pat is None else list(pat.shape)
+
+    def create(kd, cd):
+        return nufft_create2(kd, cd, tdims, traj, pd, pat, bd, bas, conf=conf)
+
+    if bas is not None:     # src/nufft.c:169-176, 208-211, 284-288
+        if a.dft or a.inverse:
+            sys.stderr.write("-B: forward and adjoint only here\n")
+            return 1
+        if a.adjoint:
+            kd = (list(inp.shape) + [1] * 16)[:16]
+            cd = (a.dims or estimate_im_dims(traj)) + kd[3:]
+            cd[5], cd[6] = 1, bd[6]
+            op = create(kd, cd)
+            writecfl(a.output, op.adjoint(inp).reshape(cd, order="F"))
+        else:
+            cd = (list(inp.shape) + [1] * 16)[:16]
+            kd = [1, tdims[1], tdims[2]] + cd[3:]
+            kd[5], kd[6] = bd[5], 1
+            op = create(kd, cd)
+            writecfl(a.output, op.forward(inp).reshape(kd, order="F"))
+        op.free()
+        return 0
     if a.dft:   # src/nufft.c:244, 297 (no basis, no pattern)
         from .nufft import Nudft
         if a.inverse or pat is not None:

@@ -109,3 +109,36 @@ def test_dropin_pics_basis():
                  "k", "s", "o")
         assert "libbnufft" in r.stderr + r.stdout
         assert rel(readcfl(os.path.join(d, "o")), g["out"]) < 1e-4
+
+
+@pytest.mark.parametrize("opts", [["--zero-mem"], ["--no-precomp"], ["--lowmem"]])
+def test_dropin_nufft_memory_modes(opts):
+    """The reference's memory options of `bart nufft` (zero-overhead mode, no
+    precomputed tables, low-mem mode) change how much it holds, not its
+    results; on the library they give the same forward and adjoint."""
+    exe = _tool("nufft_bnufft")
+    g = golden("nufft2d_n64")
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "t"), g["traj"])
+        writecfl(os.path.join(d, "x"), g["img"])
+        writecfl(os.path.join(d, "y"), g["ksp"])
+        _run(d, exe, *opts, "t", "x", "k")
+        _run(d, exe, *opts, "-a", "-x64:64:1", "t", "y", "a")
+        assert rel(readcfl(os.path.join(d, "k")), g["fwd"]) < 1e-5
+        assert rel(readcfl(os.path.join(d, "a")), g["adj"]) < 1e-5
+
+
+@pytest.mark.parametrize("conf", ["real-psf,upper-triag-psf,compress-psf", "real-psf", "upper-triag-psf",
+                                  "compress-psf", "decomposed-psf"])
+def test_dropin_pics_basis_psf_storage(conf):
+    """tests/linsub.mk:90-97: pics -B with the reference's PSF storage options
+    (real part only, upper triangle of the coefficient pairs, compressed to
+    the sampled cells, decomposed) reconstructs the same image."""
+    exe = _tool("pics_bnufft")
+    g = golden("pics2d_n32_basis")
+    with tempfile.TemporaryDirectory() as d:
+        for n, k in (("t", "traj"), ("k", "ksp"), ("s", "sens"), ("b", "basis"), ("w", "pattern")):
+            writecfl(os.path.join(d, n), g[k])
+        _run(d, exe, "-l2", "-r0.01", f"-i{int(g['iters'])}", "--nufft-conf", conf, "-B", "b", "-p", "w", "-t", "t",
+             "k", "s", "o")
+        assert rel(readcfl(os.path.join(d, "o")), g["out"]) < 1e-4

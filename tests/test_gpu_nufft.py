@@ -327,3 +327,18 @@ def test_tiled_scatter_matches_atomic(N, spokes, coils, nd, periodic, monkeypatc
     o = orc.NufftOracle(t.real.reshape(3, -1, order="F"), tuple(cd[:3]), periodic=periodic)
     want = o.adjoint(y.reshape(-1, coils, order="F"))
     assert rel(outs[0], want.reshape(cd, order="F")) < TOL
+
+
+def test_cli_nufft_basis(tmp_path):
+    """python -m bart_b200 nufft -B (forward, then adjoint with -x) on the
+    basis fixture, as the reference's `bart nufft -B`."""
+    from bart_b200.__main__ import main_nufft
+    from bart_b200.cfl import readcfl, writecfl
+    g = golden("nufft2d_n32_basis")
+    for n in ("traj", "img", "ksp", "basis"):
+        writecfl(str(tmp_path / n), g[n])
+    p = lambda n: str(tmp_path / n)     # noqa: E731
+    assert 0 == main_nufft(["-B", p("basis"), p("traj"), p("img"), p("k")])
+    assert rel(readcfl(p("k")), g["fwd"]) < TOL
+    assert 0 == main_nufft(["-a", "-B", p("basis"), "-x", "32:32:1", p("traj"), p("ksp"), p("a")])
+    assert rel(readcfl(p("a")), g["adj"]) < TOL
