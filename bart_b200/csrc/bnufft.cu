@@ -713,13 +713,14 @@ static unsigned vec_blocks(long n, int threads = RED_THREADS, int maxb = 4 * 148
 struct Geom {
 
 	int N[3];	// image dims
-	int G[3];	// oversampled dims (2N or 1)
+	int G[3];	// oversampled dims (2N, lround(os N) when chain, or 1)
 	int nd;		// number of transformed (non-singleton) axes
 	long npix;	// N0*N1*N2
 	long gsz;	// G0*G1*G2
 	long M;		// samples
 	float os, width;
 	int periodic;
+	int chain = 0;	// os != 2: the reference's chained NUFFT (src/noncart/nufft_chain.c)
 };
 
 struct Work {
@@ -828,6 +829,9 @@ static GridGeom grid_geom(const Geom& g)
 	gg.gsz = g.gsz;
 	gg.hw = g.width / 2.f;
 	gg.periodic = g.periodic;
+	gg.chain = g.chain;
+	gg.os = g.os;
+	gg.wg = g.width;
 	return gg;
 }
 
@@ -865,10 +869,14 @@ static int init_geom(Geom& g, const long dims3[3], long M, float os, float width
 	g.npix = 1;
 	g.gsz = 1;
 
+	g.chain = (2.f != os);
+
 	for (int i = 0; i < 3; i++) {
 
 		g.N[i] = (int)dims3[i];
-		g.G[i] = (dims3[i] > 1) ? (int)(2 * dims3[i]) : 1;
+		// os != 2: the grid of lround(os N) cells of nufft_create_chain
+		// (src/noncart/nufft_chain.c:205-208)
+		g.G[i] = (dims3[i] > 1) ? (g.chain ? (int)std::lround((double)os * (double)dims3[i]) : (int)(2 * dims3[i])) : 1;
 
 		if (dims3[i] > 1) {
 
@@ -876,6 +884,10 @@ static int init_geom(Geom& g, const long dims3[3], long M, float os, float width
 
 			if (0 != dims3[i] % 2)
 				return fail(BNUFFT_ERR_UNSUPPORTED, "odd image size %ld (even sizes are built)", dims3[i]);
+
+			if (g.chain && ((0 != g.G[i] % 2) || (g.G[i] <= g.N[i])))
+				return fail(BNUFFT_ERR_UNSUPPORTED, "oversampled grid of %d cells for %ld pixels (an even grid larger than the image is built)",
+						g.G[i], dims3[i]);
 
 			if (!supported_len(g.G[i]))
 				return fail(BNUFFT_ERR_UNSUPPORTED, "grid length %d on axis %d", g.G[i], i);
@@ -919,6 +931,21 @@ static void rolloff_host(const int N[3], float os, float width, float* ax, float
 	double beta = kernel_beta(os, width);
 	double i0b = bessel_i0(beta);
 	double sc = 1. / sqrt((double)N[0] * (double)N[1] * (double)N[2]);
+
+	if (2.f != os) {	// the chain: unitary centred FFT on the lround(os N) grid, times os^(d/2)
+
+		double gs = 1.;
+		int nd = 0;
+
+		for (int i = 0; i < 3; i++)
+			if (N[i] > 1) {
+
+				gs *= (double)std::lround((double)os * (double)N[i]);
+				nd++;
+			}
+
+		sc = pow((double)os, 0.5 * nd) / sqrt(gs);
+	}
 
 	for (int x = 0; x < N[0]; x++)
 		ax[x] = (float)rolloff_axis(N[0], x, os, width, beta, i0b);
@@ -2037,8 +2064,8 @@ static int check_conf(const bnufft_conf* conf)
 	if ((0 != conf->bin) && ((conf->bin < 8) || (conf->bin > 128) || (0 != (conf->bin & (conf->bin - 1)))))
 		return fail(BNUFFT_ERR_ARG, "bin edge %d (0 or a power of two 8..128)", conf->bin);
 
-	if (2.f != conf->os)
-		return fail(BNUFFT_ERR_UNSUPPORTED, "oversampling %g (os = 2 is built; the reference chains other os)", conf->os);
+	if (!(conf->os > 1.f) || (conf->os > 4.f))
+		return fail(BNUFFT_ERR_UNSUPPORTED, "oversampling %g (1 < os <= 4 is built)", conf->os);
 
 	if ((conf->width <= 0.f) || (conf->width > 8.f))
 		return fail(BNUFFT_ERR_UNSUPPORTED, "kernel width %g", conf->width);
@@ -2101,7 +2128,8 @@ static int upload_traj(bnufft_plan_s* p, const void* traj, cudaStream_t st, bool
 	int s = (cudaSuccess == e) ? BNUFFT_OK : fail(BNUFFT_ERR_CUDA, "trajectory: %s", cudaGetErrorString(e));
 	free_bins(p->op.bins, st);
 
-	if (BNUFFT_OK == s)
+	// the chained NUFFT (os != 2) grids with the generic per-sample kernels
+	if ((BNUFFT_OK == s) && !p->op.g.chain)
 		s = build_bins(p->op, st);
 
 	if ((BNUFFT_OK == s) && p->conf.deterministic) {
@@ -2185,6 +2213,17 @@ extern "C" int bnufft_create2(bnufft_plan_t* plan, int N, const long ksp_dims[],
 		bnufft_conf_defaults(&conf);
 
 	TRY(check_conf(&conf));
+
+	if (2.f != conf.os) {	// the chained NUFFT (src/noncart/nufft.c:1185-1198, nufft_chain.c)
+
+		if (basis)
+			return fail(BNUFFT_ERR_UNSUPPORTED, "a basis with os != 2");
+
+		if (conf.deterministic)
+			return fail(BNUFFT_ERR_UNSUPPORTED, "deterministic gridding with os != 2");
+
+		conf.toeplitz = 0;	// the chain has no Toeplitz normal: adjoint(forward)
+	}
 
 	if (3 != traj_dims[0] || 1 != ksp_dims[0])
 		return fail(BNUFFT_ERR_ARG, "traj dims[0] must be 3 and ksp dims[0] 1");

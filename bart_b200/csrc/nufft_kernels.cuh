@@ -799,11 +799,70 @@ __device__ __forceinline__ void axis_taps(float k, int N, float hw, int periodic
 struct GridGeom {
 
 	int N[3];	// image size per axis
-	int G[3];	// grid size per axis (2N, or 1)
+	int G[3];	// grid size per axis (2N, lround(os N) for the chain, or 1)
 	long gsz;	// cells per channel
 	float hw;	// kernel width on the N-grid (conf.width / 2)
 	int periodic;
+	// (defaults: the os = 2 gridding, for geometries built field by field)
+	int chain = 0;	// os != 2: the chained NUFFT's plain gridding on the G grid
+	float os = 2.f;	// its oversampling
+	float wg = 6.f;	// its kernel width on the G grid (conf.width)
 };
+
+// Taps of one axis of the chained NUFFT (os != 2; nufft_create_chain,
+// src/noncart/nufft_chain.c:190-244, gridding by gridH / grid_point_gen,
+// src/noncart/grid.c:150-199, 403-465):
+//   pos = float(os * k) + float(G/2)   (the centred grid of G cells)
+//   taps t = ceil(pos - w/2) .. floor(pos + w/2)  (float64 bounds)
+//   weight = intlookup(|t - pos| / w)
+//   cell: centred t -> DFT order (t + G/2) mod G (G even)
+// Non-periodic: taps clipped to [0, G-1]; periodic: t mod G.
+__device__ __forceinline__ void chain_taps(float k, int G, float os, float w, int periodic, const float* kb,
+		AxisTaps& t)
+{
+	t.n = 0;
+
+	if (1 == G) {
+
+		t.cell[0] = 0;
+		t.w[0] = kb_lookup(kb, 0.f);
+		t.n = 1;
+		return;
+	}
+
+	const float pos = __fadd_rn(__fmul_rn(os, k), (float)(G / 2));
+	int sti = (int)ceil((double)pos - 0.5 * (double)w);
+	int eni = (int)floor((double)pos + 0.5 * (double)w);
+
+	if (!periodic) {
+
+		sti = max(sti, 0);
+		eni = min(eni, G - 1);
+	}
+
+	for (int c = sti; (c <= eni) && (t.n < MAX_AXIS_TAPS); c++) {
+
+		const float frac = fabsf(__fsub_rn((float)c, pos));
+		const int cm = periodic ? (((c % G) + G) % G) : c;
+		int j = cm + G / 2;
+
+		if (j >= G)
+			j -= G;
+
+		t.cell[t.n] = j;
+		t.w[t.n] = kb_lookup(kb, __fdiv_rn(frac, w));
+		t.n++;
+	}
+}
+
+// the taps of axis a for either gridding
+__device__ __forceinline__ void geom_taps(const GridGeom& g, int a, float k, const float* kb, AxisTaps& t)
+{
+	if (g.chain)
+		chain_taps(k, g.G[a], g.os, g.wg, g.periodic, kb, t);
+	else
+		axis_taps(k, g.N[a], g.hw, g.periodic, kb, t);
+}
 
 // Degridding (forward interpolation), one thread per sample, coils
 // [blockIdx.y*cpc, ...). ksp[m + M*c] = sum_taps w * grid[cell + gsz*c].
@@ -825,9 +884,9 @@ __global__ void k_degrid(const float4* __restrict__ traj, long M, GridGeom g, in
 
 	float4 k = traj[m];
 	AxisTaps tx, ty, tz;
-	axis_taps(k.x, g.N[0], g.hw, g.periodic, kb, tx);
-	axis_taps(k.y, g.N[1], g.hw, g.periodic, kb, ty);
-	axis_taps(k.z, g.N[2], g.hw, g.periodic, kb, tz);
+	geom_taps(g, 0, k.x, kb, tx);
+	geom_taps(g, 1, k.y, kb, ty);
+	geom_taps(g, 2, k.z, kb, tz);
 
 	const int c0 = blockIdx.y * cpc;
 	const int c1 = min(C, c0 + cpc);
@@ -880,9 +939,9 @@ __global__ void k_grid_atomic(const float4* __restrict__ traj, long M, GridGeom 
 
 	float4 k = traj[m];
 	AxisTaps tx, ty, tz;
-	axis_taps(k.x, g.N[0], g.hw, g.periodic, kb, tx);
-	axis_taps(k.y, g.N[1], g.hw, g.periodic, kb, ty);
-	axis_taps(k.z, g.N[2], g.hw, g.periodic, kb, tz);
+	geom_taps(g, 0, k.x, kb, tx);
+	geom_taps(g, 1, k.y, kb, ty);
+	geom_taps(g, 2, k.z, kb, tz);
 
 	const int c0 = blockIdx.y * cpc;
 	const int c1 = min(C, c0 + cpc);
@@ -946,9 +1005,9 @@ __global__ void k_csr_keys(const float4* __restrict__ traj, long M, GridGeom g, 
 
 	float4 k = traj[m];
 	AxisTaps tx, ty, tz;
-	axis_taps(k.x, g.N[0], g.hw, g.periodic, kb, tx);
-	axis_taps(k.y, g.N[1], g.hw, g.periodic, kb, ty);
-	axis_taps(k.z, g.N[2], g.hw, g.periodic, kb, tz);
+	geom_taps(g, 0, k.x, kb, tx);
+	geom_taps(g, 1, k.y, kb, ty);
+	geom_taps(g, 2, k.z, kb, tz);
 
 	const int slots = CSR_TAPS_AXIS * CSR_TAPS_AXIS * slots_z;
 	unsigned long long* kp = keys + m * slots;

@@ -39,7 +39,10 @@ struct bnufft_conf {
 	int toeplitz;
 	int periodic;
 	int deterministic;
-	float os;
+	float os;		/* 2, or in (1, 4] with an even lround(os N): the
+				   reference's chained NUFFT (src/noncart/nufft_chain.c),
+				   which has no Toeplitz normal (toeplitz is then ignored;
+				   the normal is adjoint(forward)) */
 	float width;
 	int bin;		/* gridding bin edge in grid cells (a power of two 8..128);
 				   0 = default (32 in 2D, 16 in 3D). A tuning knob with no

@@ -504,6 +504,115 @@ def _as4(a):
 
 
 # ---------------------------------------------------------------------------
+# Chained NUFFT for os != 2 (nufft_create2 -> nufft_create_chain,
+# src/noncart/nufft.c:1185-1198, src/noncart/nufft_chain.c:190-244)
+# ---------------------------------------------------------------------------
+
+class ChainNufftOracle:
+    """roll-off (os) -> centred in the G = lround(os N) grid -> unitary
+    centred FFT -> KB gridding on that grid (width w, beta(os, w)) -> times
+    os^(d/2) (and the weights); the adjoint in reverse. float64 except the
+    taps, which follow gridH / grid_point_gen in float32 (src/noncart/grid.c:
+    150-199, 403-465): pos = float(os k) + float(G/2), taps ceil(pos - w/2) ..
+    floor(pos + w/2) in float64, weight ((1 wz) wy) wx with
+    w* = intlookup(|t - pos| / w)."""
+
+    def __init__(self, traj, dims, os, width=6.0, periodic=False, weights=None):
+        self.dims3 = tuple(int(d) for d in dims)
+        self.os, self.width = float(os), float(width)
+        # lround: halves away from zero (Python's round() would round them to even)
+        self.G = tuple(int(math.floor(float(os) * d + 0.5)) if d > 1 else 1 for d in self.dims3)
+        self.nd = sum(1 for d in self.dims3 if d > 1)
+        beta = kernel_beta(os, width)
+        self.roll = rolloff_table(self.dims3, os, width).astype(np.float64)
+        self.scale = self.os ** (0.5 * self.nd) / math.sqrt(float(np.prod(self.G)))
+        self.weights = None if weights is None else np.asarray(weights).reshape(-1, order="F").astype(np.complex128)
+        table = kb_table(beta)
+        traj = np.asarray(traj, dtype=F32).reshape(3, -1)
+        self.M = M = traj.shape[1]
+        w = F32(width)
+        per_axis = []
+        for ax in range(3):
+            G = self.G[ax]
+            if G == 1:
+                per_axis.append(([np.zeros(M, dtype=np.int64)],
+                                 [np.full(M, intlookup(table, np.zeros(1, dtype=F32))[0], dtype=F32)],
+                                 [np.ones(M, dtype=bool)]))
+                continue
+            pos = (F32(os) * traj[ax]).astype(F32)
+            pos = (pos + F32(G // 2)).astype(F32)
+            sti = np.ceil(pos.astype(np.float64) - 0.5 * float(w)).astype(np.int64)
+            eni = np.floor(pos.astype(np.float64) + 0.5 * float(w)).astype(np.int64)
+            idxs, wts, valid = [], [], []
+            for o in range(int((eni - sti).max()) + 1 if M else 0):
+                t = sti + o
+                ok = t <= eni
+                if periodic:
+                    ti = np.mod(t, G)
+                else:
+                    ok &= (t >= 0) & (t <= G - 1)
+                    ti = t
+                frac = np.where(ok, np.abs(t.astype(F32) - pos), F32(0.0)).astype(F32)
+                wts.append(intlookup(table, (frac / w).astype(F32)))
+                idxs.append(np.clip(ti, 0, G - 1))
+                valid.append(ok)
+            per_axis.append((idxs, wts, valid))
+        (ix, wx, vx), (iy, wy, vy), (iz, wz, vz) = per_axis
+        samp, cell, wgt = [], [], []
+        for a in range(len(iz)):
+            for b in range(len(iy)):
+                dzy = ((F32(1.0) * wz[a]).astype(F32) * wy[b]).astype(F32)
+                for c in range(len(ix)):
+                    ok = vz[a] & vy[b] & vx[c]
+                    d = (dzy * wx[c]).astype(F32)
+                    sel = np.nonzero(ok)[0]
+                    samp.append(sel)
+                    cell.append((ix[c] + self.G[0] * (iy[b] + self.G[1] * iz[a]))[sel])
+                    wgt.append(d[sel])
+        self.samp, self.cell = np.concatenate(samp), np.concatenate(cell)
+        self.wgt = np.concatenate(wgt).astype(np.float64)
+
+    def _axes(self):
+        return tuple(i for i in range(3) if self.G[i] > 1)
+
+    def forward(self, img):
+        img = _as4(img)
+        C = img.shape[3]
+        x = img * self.roll[..., None]
+        xg = np.zeros(self.G + (C,), dtype=np.complex128)
+        sl = tuple(slice(g // 2 - n // 2, g // 2 - n // 2 + n) for g, n in zip(self.G, self.dims3))
+        xg[sl] = x
+        ax = self._axes()
+        spec = np.fft.fftshift(np.fft.fftn(np.fft.ifftshift(xg, axes=ax), axes=ax), axes=ax) * self.scale
+        gf = spec.reshape(-1, C, order="F")
+        out = np.zeros((self.M, C), dtype=np.complex128)
+        for c in range(C):
+            v = gf[self.cell, c] * self.wgt
+            out[:, c] = (np.bincount(self.samp, weights=v.real, minlength=self.M)
+                         + 1j * np.bincount(self.samp, weights=v.imag, minlength=self.M))
+        if self.weights is not None:
+            out = out * self.weights[:, None]
+        return out
+
+    def adjoint(self, ksp):
+        ksp = np.asarray(ksp).reshape(self.M, -1).astype(np.complex128)
+        if self.weights is not None:
+            ksp = ksp * np.conj(self.weights)[:, None]
+        C = ksp.shape[1]
+        n = int(np.prod(self.G))
+        g = np.zeros((n, C), dtype=np.complex128)
+        for c in range(C):
+            v = ksp[self.samp, c] * self.wgt
+            g[:, c] = (np.bincount(self.cell, weights=v.real, minlength=n)
+                       + 1j * np.bincount(self.cell, weights=v.imag, minlength=n))
+        g = g.reshape(self.G + (C,), order="F")
+        ax = self._axes()
+        xg = np.fft.fftshift(np.fft.ifftn(np.fft.ifftshift(g, axes=ax), axes=ax), axes=ax) * (self.scale * n)
+        sl = tuple(slice(gg // 2 - nn // 2, gg // 2 - nn // 2 + nn) for gg, nn in zip(self.G, self.dims3))
+        return xg[sl] * self.roll[..., None]
+
+
+# ---------------------------------------------------------------------------
 # Subspace basis (nufft_create2 with a basis, src/noncart/nufft.c:1018-1042,
 # 1427-1491, 1546-1625, 470-505)
 # ---------------------------------------------------------------------------

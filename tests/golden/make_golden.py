@@ -14,6 +14,7 @@ read the .npz files and never run the reference.
     python tests/golden/make_golden.py --gpu-gridding  # the reference's GPU-gridding test inputs
     python tests/golden/make_golden.py --kooshball     # 3D kooshball at 32^3, 2 coils
     python tests/golden/make_golden.py --basis         # subspace basis (nufft / pics -B)
+    python tests/golden/make_golden.py --chain         # oversampling other than 2 (nufft -o)
 """
 
 from __future__ import annotations
@@ -338,6 +339,45 @@ def basis_pics_case(name, traj, ksp, sens, basis, pattern, iters=10):
     print(name, out.shape, "reference spread", spread)
 
 
+def chain_case(name, traj, img, oss, pattern=None):
+    """nufft -o os (the reference's chained NUFFT) forward and adjoint for
+    each oversampling factor in oss."""
+    out = dict(traj=traj, img=img, oss=np.asarray(oss, dtype=np.float64))
+    with tempfile.TemporaryDirectory() as d:
+        rng = np.random.default_rng(zlib.crc32(name.encode()))
+        writecfl(os.path.join(d, "t"), traj)
+        writecfl(os.path.join(d, "x"), img)
+        P = []
+        if pattern is not None:
+            writecfl(os.path.join(d, "w"), pattern)
+            P = ["-p", "w"]
+            out["pattern"] = pattern
+        dims = ":".join(str(s) for s in (list(img.shape) + [1, 1])[:3])
+        for i, o in enumerate(oss):
+            run("nufft", *P, "-o", str(o), "t", "x", "k", cwd=d)
+            fwd = readcfl(os.path.join(d, "k"))
+            if i == 0:
+                out["ksp"] = cplx(rng, fwd.shape)
+                writecfl(os.path.join(d, "y"), out["ksp"])
+            run("nufft", *P, "-o", str(o), "-a", f"-x{dims}", "t", "y", "a", cwd=d)
+            out[f"fwd_{i}"] = fwd
+            out[f"adj_{i}"] = readcfl(os.path.join(d, "a"))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **{k: np.asarray(v) for k, v in out.items()})
+    print(name, {k: np.shape(v) for k, v in out.items()})
+
+
+def chain_cases():
+    rng = np.random.default_rng(2468)
+    with tempfile.TemporaryDirectory() as d:
+        run("traj", "-r", "-G", "-x64", "-o2", "-y24", "t", cwd=d)
+        t64 = readcfl(os.path.join(d, "t"))
+    img = cplx(rng, (64, 64, 1, 2))
+    chain_case("nufft2d_n64_chain", t64, img, [1.5, 1.25, 2.5])
+    w = (0.2 + rng.random((1,) + t64.shape[1:3])).astype(np.complex64)
+    chain_case("nufft2d_n64_chain_weights", t64, img[..., :1], [1.5], pattern=w)
+    chain_case("nufft3d_n16_chain", synth.kooshball_traj(16, 64), cplx(rng, (16, 16, 16)), [1.5])
+
+
 def basis_cases():
     rng = np.random.default_rng(555)
     T, K = 4, 3
@@ -380,6 +420,9 @@ def basis_cases():
 def main():
     if "--basis" in sys.argv:
         basis_cases()
+        return
+    if "--chain" in sys.argv:
+        chain_cases()
         return
     if "--uneven" in sys.argv:
         uneven_cases()

@@ -142,3 +142,19 @@ def test_dropin_pics_basis_psf_storage(conf):
         _run(d, exe, "-l2", "-r0.01", f"-i{int(g['iters'])}", "--nufft-conf", conf, "-B", "b", "-p", "w", "-t", "t",
              "k", "s", "o")
         assert rel(readcfl(os.path.join(d, "o")), g["out"]) < 1e-4
+
+
+def test_dropin_nufft_oversampling():
+    """bart nufft -o 1.5 / 1.25 (the reference's chained NUFFT for os != 2)
+    through the adapter, which passes conf.os on."""
+    exe = _tool("nufft_bnufft")
+    g = golden("nufft2d_n64_chain")
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "t"), g["traj"])
+        writecfl(os.path.join(d, "x"), g["img"])
+        writecfl(os.path.join(d, "y"), g["ksp"])
+        for i, o in enumerate(g["oss"]):
+            _run(d, exe, "-o", str(o), "t", "x", "k")
+            _run(d, exe, "-o", str(o), "-a", "-x64:64:1", "t", "y", "a")
+            assert rel(readcfl(os.path.join(d, "k")), g[f"fwd_{i}"]) < 1e-5, o
+            assert rel(readcfl(os.path.join(d, "a")), g[f"adj_{i}"]) < 1e-5, o

@@ -179,12 +179,20 @@ def test_adjointness_full_size():
 
 
 def test_unsupported_options_fail_loudly():
+    """Options outside what is built are refused with a status, not run: an
+    oversampled grid of odd length (os 1.25 on 34 pixels: 42.5 -> 42 is even,
+    on 30: 37.5 -> 38 even, on 26: 32.5 -> 33 odd), os beyond 4, odd image
+    sides, deterministic gridding with os != 2."""
     from bart_b200._lib import BnufftError
     t = synth.radial_traj(32, 8)
     with pytest.raises(BnufftError):
-        nufft_create2([1, 64, 8, 1], [32, 32, 1, 1], list(t.shape), t, conf=NufftConf(os=1.5))
+        nufft_create2([1, 64, 8, 1], [26, 26, 1, 1], list(t.shape), t, conf=NufftConf(os=1.25))
+    with pytest.raises(BnufftError):
+        nufft_create2([1, 64, 8, 1], [32, 32, 1, 1], list(t.shape), t, conf=NufftConf(os=5.0))
     with pytest.raises(BnufftError):
         nufft_create2([1, 64, 8, 1], [33, 33, 1, 1], list(t.shape), t)
+    with pytest.raises(BnufftError):
+        nufft_create2([1, 64, 8, 1], [32, 32, 1, 1], list(t.shape), t, conf=NufftConf(os=1.5, deterministic=True))
 
 
 @pytest.mark.parametrize("name,periodic", [("nufft2d_n64", False), ("nufft2d_n64_periodic", True),
@@ -327,6 +335,28 @@ def test_tiled_scatter_matches_atomic(N, spokes, coils, nd, periodic, monkeypatc
     o = orc.NufftOracle(t.real.reshape(3, -1, order="F"), tuple(cd[:3]), periodic=periodic)
     want = o.adjoint(y.reshape(-1, coils, order="F"))
     assert rel(outs[0], want.reshape(cd, order="F")) < TOL
+
+
+@pytest.mark.parametrize("name", ["nufft2d_n64_chain", "nufft2d_n64_chain_weights", "nufft3d_n16_chain"])
+def test_chain_vs_reference(name):
+    """Oversampling other than 2 (nufft -o 1.25 / 1.5 / 2.5: the reference's
+    chained NUFFT on a grid of lround(os N) cells, Bluestein transforms):
+    forward, adjoint and the normal (adjoint of the forward, as the chain
+    has no Toeplitz form) against the reference's outputs."""
+    g = golden(name)
+    cd = _dims(g["img"].shape)
+    td = list(g["traj"].shape)
+    kd = [1, td[1], td[2], cd[3]]
+    w = g.get("pattern")
+    for i, os_ in enumerate(g["oss"]):
+        op = nufft_create2(kd, cd, td, g["traj"], None if w is None else list(w.shape), w,
+                           conf=NufftConf(toeplitz=True, os=float(os_)))
+        img = g["img"].reshape(cd, order="F")
+        assert rel(op.forward(img), g[f"fwd_{i}"]) < TOL, os_
+        assert rel(op.adjoint(g["ksp"].reshape(kd, order="F")), g[f"adj_{i}"]) < TOL, os_
+        o = orc.ChainNufftOracle(g["traj"].real.reshape(3, -1, order="F"), cd[:3], float(os_), weights=w)
+        assert rel(op.normal(img), o.adjoint(o.forward(img))) < TOL, os_
+        op.free()
 
 
 def test_cli_nufft_basis(tmp_path):

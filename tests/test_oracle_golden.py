@@ -245,3 +245,22 @@ def test_basis_forward_adjoint_normal(name):
     assert rel(op.adjoint(g["ksp"].reshape(-1, C, T, order="F")), g["adj"].reshape(x.shape, order="F")) < OPS_TOL
     assert rel(op.normal_toeplitz(x), g["normal"].reshape(x.shape, order="F")) < OPS_TOL
     assert rel(op.adjoint(op.forward(x)), g["normal_explicit"].reshape(x.shape, order="F")) < OPS_TOL
+
+
+@pytest.mark.parametrize("name", ["nufft2d_n64_chain", "nufft2d_n64_chain_weights", "nufft3d_n16_chain"])
+def test_chain_forward_adjoint(name):
+    """nufft -o os (os != 2: the reference's chained NUFFT on a grid of
+    lround(os N) cells) against the reference, for every os of the fixture.
+    Bar 3e-6: the reference's float32 FFTs of the 80-, 96- and 24-point grids
+    round more than its power-of-two ones (measured 1.0-1.1e-6)."""
+    g = golden(name)
+    img = g["img"]
+    while img.ndim < 4:
+        img = img[..., None]
+    traj = g["traj"].real.reshape(3, -1, order="F")
+    for i, os_ in enumerate(g["oss"]):
+        op = orc.ChainNufftOracle(traj, img.shape[:3], float(os_), weights=g.get("pattern"))
+        C = img.shape[3]
+        assert rel(op.forward(img), g[f"fwd_{i}"].reshape(-1, C, order="F")) < 3e-6, os_
+        assert rel(op.adjoint(g["ksp"].reshape(-1, C, order="F")), g[f"adj_{i}"].reshape(img.shape, order="F")) \
+            < 3e-6, os_
