@@ -1,7 +1,7 @@
 """Command line mirror of ``bart nufft`` and ``bart pics -t`` with .cfl I/O.
 
   python -m bart_b200 nufft [-a|-i [-c] [-l lambda] [-m iter]] [-x X:Y:Z] [-P] [-r|-t]
-                            [-p pattern] [-B basis] traj input output
+                            [-p pattern] [-B basis] [-o os] traj input output
   python -m bart_b200 pics -l2 -r lambda [-i iter] -t traj [-w scale] [-S]
                            [--no-toeplitz] ksp sens output
   python -m bart_b200 -l flags pics ...   (or -p flags: the same here)
@@ -65,6 +65,8 @@ def main_nufft(argv) -> int:
     ap.add_argument("-m", dest="iters", type=int, default=50)
     ap.add_argument("-p", dest="pattern")
     ap.add_argument("-B", dest="basis", help="temporal (or other) basis [1,1,1,1,1,T,K]")
+    ap.add_argument("-o", "--oversampling", dest="os", type=float, default=2.0,
+                    help="oversampling (default 2; other values: the reference's chained NUFFT, no Toeplitz)")
     ap.add_argument("-s", dest="dft", action="store_true", help="direct non-uniform DFT")
     ap.add_argument("--lowmem", action="store_true", help="one coil's oversampled grid at a time")
     # the reference's other memory modes change what it holds, not its results;
@@ -81,7 +83,7 @@ def main_nufft(argv) -> int:
     traj = readcfl(a.traj)
     tdims = list(traj.shape)
     # the PSF is only built for the inverse (src/nufft.c:121-122); Toeplitz is on by default there
-    conf = NufftConf(toeplitz=a.inverse and not a.no_toeplitz, periodic=a.periodic, lowmem=a.lowmem)
+    conf = NufftConf(toeplitz=a.inverse and not a.no_toeplitz, periodic=a.periodic, lowmem=a.lowmem, os=a.os)
     inp = readcfl(a.input)
     pat = readcfl(a.pattern) if a.pattern else None
     bas = readcfl(a.basis) if a.basis else None

@@ -51,7 +51,10 @@ WORKLOAD = "cgsense2d_256_c16_s96_tol1e-4_toeplitz"
 DOMINANT = "cols_toeplitz"
 # the ncu summary of the dominant kernel on this workload; its table carries
 # the DRAM bytes (read + write) of one launch
-DOMINANT_PROFILE = os.path.join(ROOT, "profiles", "k_cols_toeplitz_512_cgsense2d.md")
+DOMINANT_PROFILE = os.path.join(ROOT, "profiles", "k_cols_toe512_cgsense2d.md")
+# FP32 peak of the CUDA cores (no measured figure exists for it): 148 SMs x
+# 128 lanes x 2 flop (FMA) x the max SM clock 1.965 GHz
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 L2_FLUSH_BYTES = 512 << 20     # > 126 MB L2
 
 
@@ -903,6 +906,10 @@ def main():
     peak, peak_src = peak_hbm()
     achieved = alg_bytes / k_avg_s / 1e9 if k_avg_s > 0 else None
     traffic = profiled_traffic(DOMINANT_PROFILE)
+    # its FFT work: a forward and an inverse G1-point transform per column
+    # (G0 columns x COILS), 5 n log2 n flop each
+    fft_flop = 2 * G0 * COILS * 5 * G1 * np.log2(G1)
+    fft_tflops = fft_flop / k_avg_s / 1e12 if k_avg_s > 0 else None
 
     nufft = nufft_throughput(dev) if (rank == 0 and not args.lean) else None
     vs_cufft = fft_vs_cufft(dev, traj, sens) if (rank == 0 and not args.lean) else None
@@ -937,6 +944,10 @@ def main():
                              "frac": (achieved / peak) if achieved else None,
                              "traffic": traffic, "alg_bytes": alg_bytes,
                              "avg_launch_us": k_avg_s * 1e6, "launches": kn.value,
+                             "fft_flop": fft_flop, "fp32_tflops": fft_tflops,
+                             "fp32_peak_tflops": FP32_PEAK_TFLOPS,
+                             "fp32_frac": (fft_tflops / FP32_PEAK_TFLOPS) if fft_tflops else None,
+                             "fp32_peak_source": "nominal: 148 SMs x 128 lanes x 2 x 1.965 GHz",
                              "timing": "CUDA events per launch over the same steps, CG loop host-launched "
                                        "for the solve's iteration count"},
                 "clocks": clk.summary()}
