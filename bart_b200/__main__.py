@@ -6,6 +6,11 @@
                            [--no-toeplitz] ksp sens output
   python -m bart_b200 -l flags pics ...   (or -p flags: the same here)
 
+The k-space argument of pics may be "-": a stream of the reference's
+(src/misc/stream.c, e.g. from `copy --stream flags -- ksp -`) on stdin.
+With -l flags along the streamed dims every slice is reconstructed as soon
+as it has arrived; without, the whole stream is read first.
+
 pics also takes two options the reference does not have: --precond 1|3
 (flexible CG with the reference's circulant preconditioner / PCG with the
 padded-circulant one; default 0, the reference's plain CG) and --tol t
@@ -173,7 +178,11 @@ def parse_pics(argv):
         ap.error("--precond needs the Toeplitz normal operator")
     a.traj_name = a.traj
     a.traj = readcfl(a.traj_name)
-    a.ksp = readcfl(a.ksp)
+    if a.ksp == "-":	# a stream on stdin (src/misc/stream.c): read as it arrives
+        from .stream import StreamReader
+        a.ksp = StreamReader(sys.stdin.buffer)
+    else:
+        a.ksp = readcfl(a.ksp)
     a.sens = readcfl(a.sens)
     a.toeplitz = not a.no_toeplitz
     return a
@@ -183,6 +192,20 @@ def main_pics(argv, loop_flags: int = 0) -> int:
     a = parse_pics(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    from .stream import StreamReader
+    if isinstance(a.ksp, StreamReader):
+        if loop_flags and world == 1:	# each slice reconstructed as it arrives
+            from .loop import stream_pics
+            writecfl(a.output, stream_pics(loop_flags, a))
+            return 0
+        # without a loop: the whole stream is the k-space
+        full = np.zeros(a.ksp.dims, dtype=np.complex64, order="F")
+        for _, pos, block in a.ksp:
+            sl = [slice(None)] * 16
+            for d, p in zip(a.ksp.sdims, pos):
+                sl[d] = slice(p, p + 1)
+            full[tuple(sl)] = block
+        a.ksp = full
     if loop_flags:
         from .loop import loop_pics
         if world == 1:

@@ -139,3 +139,38 @@ def loop_pics(flags: int, a, dev=None) -> np.ndarray:
     for k, idx in enumerate(idxs):
         place_at(out, dims, idx, got[k])
     return out
+
+
+def stream_pics(flags: int, a) -> np.ndarray:
+    """``bart -l flags pics ... - sens out`` with the k-space arriving as a
+    stream (``a.ksp`` a bart_b200.stream.StreamReader) along the looped dims:
+    each slice is reconstructed as soon as it has arrived (its own SENSE
+    model and solve), and the images are joined along those dims."""
+    from .pics import Pics, PicsConf
+
+    r = a.ksp
+    dims = loop_dims(flags)
+    if any(d < 4 for d in dims):
+        raise ValueError("pics: looped dims must be >= 4 (dims 0-3 are the image and coil axes)")
+    if sorted(r.sdims) != dims:
+        raise ValueError(f"the k-space stream runs along dims {r.sdims}, the loop along {dims}")
+    sizes = loop_sizes([a.traj.shape, r.dims, a.sens.shape], dims)
+    img_dims = list(dims16(a.sens.shape)[:3])
+    out_dims = img_dims + [1] * (DIMS - 3)
+    for d, n in zip(dims, sizes):
+        out_dims[d] = n
+    out = np.zeros(out_dims, dtype=np.complex64, order="F")
+    conf = PicsConf(lam=a.lam, maxiter=a.iters, tol=getattr(a, "tol", 0.0), scaling=a.scaling, rescale=a.rescale,
+                    toeplitz=a.toeplitz, precond=getattr(a, "precond", 0))
+    for _, pos, block in r:
+        idx = tuple(pos[r.sdims.index(d)] for d in dims)
+        traj = slice_at(a.traj, dims, idx).reshape(dims16(a.traj.shape)[:3], order="F")
+        sens = slice_at(a.sens, dims, idx)
+        sens = sens.reshape(dims16(sens.shape)[:4], order="F")
+        ksp = block.reshape(dims16(block.shape)[:4], order="F")
+        p = Pics(traj, sens, ksp_dims=list(ksp.shape), conf=conf)
+        try:
+            place_at(out, dims, idx, np.asarray(p.run(ksp)))
+        finally:
+            p.free()
+    return out

@@ -15,6 +15,7 @@ read the .npz files and never run the reference.
     python tests/golden/make_golden.py --kooshball     # 3D kooshball at 32^3, 2 coils
     python tests/golden/make_golden.py --basis         # subspace basis (nufft / pics -B)
     python tests/golden/make_golden.py --chain         # oversampling other than 2 (nufft -o)
+    python tests/golden/make_golden.py --stream        # a k-space stream (copy --stream | tee -b)
 """
 
 from __future__ import annotations
@@ -378,6 +379,26 @@ def chain_cases():
     chain_case("nufft3d_n16_chain", synth.kooshball_traj(16, 64), cplx(rng, (16, 16, 16)), [1.5])
 
 
+def stream_case(name="stream_ksp_c4_s3"):
+    """Three k-space slices (dim 13) of the pics2d_n64_c4 problem, scaled
+    differently, as the reference writes them into a pipe: `copy --stream
+    8192 -- k - | tee -b` (tee -b: the data inline, a binary stream). Stores
+    the array and the stream's bytes."""
+    g = np.load(os.path.join(HERE, "pics2d_n64_c4.npz"))
+    k = g["ksp"].reshape(list(g["ksp"].shape[:4]) + [1] * 9 + [1], order="F")
+    ksp = np.concatenate([k * np.complex64(s) for s in (1.0, 0.5, 2.0)], axis=13).astype(np.complex64)
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "k"), ksp)
+        r = subprocess.run(f"{os.path.join(BIN, 'copy')} --stream 8192 -- k - | {os.path.join(BIN, 'tee')} -b",
+                           shell=True, cwd=d, capture_output=True)
+        if r.returncode != 0:
+            raise RuntimeError(r.stderr.decode())
+        stream = r.stdout
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), ksp=ksp,
+                        stream=np.frombuffer(stream, dtype=np.uint8))
+    print(name, ksp.shape, len(stream), "stream bytes")
+
+
 def basis_cases():
     rng = np.random.default_rng(555)
     T, K = 4, 3
@@ -423,6 +444,9 @@ def main():
         return
     if "--chain" in sys.argv:
         chain_cases()
+        return
+    if "--stream" in sys.argv:
+        stream_case()
         return
     if "--uneven" in sys.argv:
         uneven_cases()

@@ -158,3 +158,29 @@ def test_cli_loop_two_ranks_split_by_cost(cuda, tmp_path):
         assert rel(b, a) < 1.5e-2, (s, rel(b, a))
         others = [rel(b, one[..., t, :, :]) for t in range(S) if t != s]
         assert min(others) > 10 * rel(b, a), (s, others)
+
+
+def test_cli_pics_from_a_reference_stream(cuda, tmp_path, monkeypatch):
+    """python -m bart_b200 -l 8192 pics ... - sens out with the k-space on
+    stdin as the reference streams it (copy --stream 8192 | tee -b): every
+    slice is reconstructed as it arrives, and the images equal those of the
+    same loop over the k-space file (there one batched launch, so equal up
+    to the atomics' float32 summation order: 30 iterations, where two runs
+    of the same slice agree to 2e-5; at 10 they differ by up to 6e-3)."""
+    import io
+    import sys
+    import bart_b200.__main__ as cli
+    from bart_b200.cfl import readcfl, writecfl
+    g = golden("pics2d_n64_c4")
+    s = golden("stream_ksp_c4_s3")
+    d = str(tmp_path)
+    writecfl(d + "/traj", g["traj"])
+    writecfl(d + "/sens", g["sens"])
+    writecfl(d + "/ksp", s["ksp"])
+    opts = ["-l2", "-r0.01", "-i30"]
+    monkeypatch.setattr(sys, "stdin", type("Stdin", (), {"buffer": io.BytesIO(s["stream"].tobytes())})())
+    assert 0 == cli.main(["-l", "8192", "pics"] + opts + ["-t", d + "/traj", "-", d + "/sens", d + "/out_stream"])
+    assert 0 == cli.main(["-l", "8192", "pics"] + opts + ["-t", d + "/traj", d + "/ksp", d + "/sens", d + "/out_file"])
+    a, b = readcfl(d + "/out_stream"), readcfl(d + "/out_file")
+    assert a.shape == b.shape and a.shape[13] == 3
+    assert rel(a, b) < 1e-4

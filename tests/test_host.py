@@ -44,3 +44,21 @@ def test_kooshball_directions_are_unit():
 def test_estimate_im_dims():
     t = synth.radial_traj(64, 8)
     assert estimate_im_dims(t) == [2 * int(np.ceil(np.abs(t.real[0]).max())), 2 * int(np.ceil(np.abs(t.real[1]).max())), 1]
+
+
+def test_stream_reader_on_the_reference_stream():
+    """bart_b200.stream reads a stream the reference wrote (copy --stream
+    8192 | tee -b: header, settings, then index / raw / break per slice):
+    every slice arrives once, at its position, with the array's values."""
+    import io
+    from bart_b200.stream import StreamReader
+    from conftest import golden
+    g = golden("stream_ksp_c4_s3")
+    r = StreamReader(io.BytesIO(g["stream"].tobytes()))
+    assert r.binary and r.flags == 8192 and r.dims[13] == 3
+    seen = []
+    for index, pos, block in r:
+        seen.append(index)
+        assert np.array_equal(block[..., 0, 0].reshape(block.shape[:4], order="F"),
+                              g["ksp"][..., pos[0]].reshape(block.shape[:4], order="F"))
+    assert seen == [0, 1, 2]
