@@ -211,6 +211,62 @@ def timed_steps(step, steps, flush, stream):
     return sum(e0.elapsed_time(e1) for e0, e1 in ev)
 
 
+def run_normal3d(dev, steps, warmup, coils=8, N=128, spokes=2000):
+    """The 3D SENSE normal operator of the CG iterations (Toeplitz; 128^3,
+    `coils` coils, kooshball PSF): device time per apply and per pass class
+    (CUDA events per launch), against the HBM bytes of its five passes:
+    rows (x + maps in, [2N, N, N, C] out), y forward ([2N, 2N, N, C] out),
+    z Toeplitz (in place on it, + the (2N)^3 PSF), y inverse, rows (maps in,
+    the coil-group sums out)."""
+    import ctypes
+    import torch
+    from bart_b200 import _lib, synth
+    from bart_b200.pics import Pics, PicsConf
+    rng = np.random.default_rng(7)
+    t = synth.kooshball_traj(N, spokes)
+    sens = synth.coil_maps(N, coils, rng, ndim=3)
+    cd = [N, N, N, coils]
+    kd = [1, t.shape[1], t.shape[2], coils]
+    t_d = torch.from_numpy(np.asfortranarray(t).ravel(order="F").copy()).to(dev)
+    sens_d = torch.from_numpy(np.asfortranarray(sens).ravel(order="F").copy()).to(dev)
+    p = Pics(t_d, sens_d, ksp_dims=kd, conf=PicsConf(lam=LAM, maxiter=10), traj_dims=list(t.shape), sens_dims=cd)
+    x = torch.randn(N ** 3, dtype=torch.complex64, device=dev)
+    y = torch.empty_like(x)
+    for _ in range(max(1, warmup)):
+        p.normal(x, y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        p.normal(x, y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    lib = _lib.load()
+    passes = {}
+    for kind in ("rows_fwd", "cols_fwd", "cols_toeplitz", "cols_inv", "rows_inv"):
+        lib.bnufft_prof_start(kind.encode())
+        p.normal(x, y)
+        kms, kn = ctypes.c_double(), ctypes.c_long()
+        lib.bnufft_prof_stop(ctypes.byref(kms), ctypes.byref(kn))
+        passes[kind] = {"ms": kms.value, "launches": kn.value}
+    p.free()
+    img, G = N ** 3 * 8, 2 * N
+    t1, t2 = G * N * N * coils * 8, G * G * N * coils * 8
+    maps = img * coils
+    pass_bytes = {"rows_fwd": img + maps + t1, "cols_fwd": t1 + t2, "cols_toeplitz": 2 * t2 + G ** 3 * 8,
+                  "cols_inv": t2 + t1, "rows_inv": t1 + maps + img}
+    peak, peak_src = peak_hbm()
+    for k, b in pass_bytes.items():
+        if passes[k]["ms"] > 0:
+            passes[k]["gbs"] = b / (passes[k]["ms"] * 1e-3) / 1e9
+            passes[k]["hbm_frac"] = passes[k]["gbs"] / peak
+    total = sum(pass_bytes.values())
+    return {"workload": f"normal3d_{N}_c{coils}", "ms_per_apply": ms, "hbm_bytes_per_apply": total,
+            "gbs": total / (ms * 1e-3) / 1e9, "hbm_frac": total / (ms * 1e-3) / 1e9 / peak,
+            "hbm_peak_gbs": peak, "peak_source": peak_src, "passes": passes}
+
+
 def run_nufft3d(dev, steps, warmup, spokes=20000):
     """3D radial kooshball NUFFT: 128^3 image, 8 coils,
     20000 spokes x 256 samples on 3D golden means (5.12 M samples per coil).
@@ -723,7 +779,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "batch", "scatter"])
+    ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "normal3d", "batch", "scatter"])
+    ap.add_argument("--coils", type=int, default=8, help="normal3d: coils")
     ap.add_argument("--spokes", type=int, default=20000, help="nufft3d: kooshball spokes")
     ap.add_argument("--methods", default="fcg_padded,fcg_circulant,cg,fcg_learned",
                     help="solvers to time (cgsense2d); the first is the headline")
@@ -758,6 +815,11 @@ def main():
     if args.workload == "nufft3d":
         if rank == 0:
             print(json.dumps(run_nufft3d(dev, args.steps, args.warmup, args.spokes)), flush=True)
+        return
+
+    if args.workload == "normal3d":
+        if rank == 0:
+            print(json.dumps(run_normal3d(dev, args.steps, args.warmup, args.coils)), flush=True)
         return
 
     if args.workload == "scatter":
@@ -958,6 +1020,8 @@ def main():
             # kooshball NUFFT + CG-SENSE, and the batch of 512 uneven problems
             torch.cuda.empty_cache()
             line["kooshball3d"] = run_nufft3d(dev, 3, 2)
+            torch.cuda.empty_cache()
+            line["kooshball3d"]["normal3d"] = run_normal3d(dev, 5, 3)
             torch.cuda.empty_cache()
             line["batch512"] = run_batch(dev, 2, 3, cpu_base=not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
