@@ -497,7 +497,57 @@ def fft_vs_cufft(dev, traj, sens, reps=50):
     return res
 
 
-def run_batch(dev, steps, warmup, nprob=512, seed=4, rank=0, world=1, cpu_base=True):
+def batch_analysis(br, probs, dev):
+    """Where the batch's time goes: the same single solves spread over 4, 8
+    and 16 streams (any concurrency, without the graph), and each solve
+    timed alone, summed per Toeplitz embedding size E (next power of two
+    >= 2N)."""
+    import torch
+    main = torch.cuda.current_stream(dev)
+    ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))   # noqa: E731
+    out = {}
+    for S in (4, 8, 16):
+        streams = [torch.cuda.Stream(dev) for _ in range(S)]
+
+        def spread():
+            e = torch.cuda.Event()
+            e.record(main)
+            for s in streams:
+                s.wait_event(e)
+            for i, (p, k, x) in enumerate(zip(br.models, br.ksp, br.img)):
+                with torch.cuda.stream(streams[i % S]):
+                    p.run(k, out=x)
+            for s in streams:
+                e2 = torch.cuda.Event()
+                e2.record(s)
+                main.wait_event(e2)
+
+        spread()
+        torch.cuda.synchronize()
+        e0, e1 = ev()
+        e0.record()
+        spread()
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"streams{S}_ms"] = e0.elapsed_time(e1)
+    per = {}
+    for p, k, x, pr in zip(br.models, br.ksp, br.img, probs):
+        E = 1 << int(np.ceil(np.log2(2 * pr["sens"].shape[0])))
+        torch.cuda.synchronize()
+        e0, e1 = ev()
+        e0.record()
+        p.run(k, out=x)
+        e1.record()
+        torch.cuda.synchronize()
+        d = per.setdefault(str(E), {"problems": 0, "ms": 0.0})
+        d["problems"] += 1
+        d["ms"] += e0.elapsed_time(e1)
+    out["alone_per_embedding"] = per
+    out["alone_sum_ms"] = sum(d["ms"] for d in per.values())
+    return out
+
+
+def run_batch(dev, steps, warmup, nprob=512, seed=4, rank=0, world=1, cpu_base=True, analysis=False):
     """Batched uneven 2D reconstructions: nprob problems,
     N ~ U{64..320} even, spokes ~ U{16..256} x 2N samples, coils ~ U{4..32},
     ellipse phantoms, polynomial maps, 20 plain-CG iterations each, lambda
@@ -559,6 +609,7 @@ def run_batch(dev, steps, warmup, nprob=512, seed=4, rank=0, world=1, cpu_base=T
         ms_loop = e0.elapsed_time(e1)
         diff = max(float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) for a, b in zip(xb, br.img))
         loop = {"ms": ms_loop, "recons_per_s": nprob / (ms_loop / 1e3), "batch_speedup": ms_loop / ms}
+    extra = batch_analysis(br, probs, dev) if (analysis and world == 1) else None
     br.free()
     return {"metric": "batched uneven CG-SENSE recons/s (20 CG iterations each)", "value": nprob / (ms / 1e3),
             "unit": "recons/s", "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms,
@@ -569,6 +620,7 @@ def run_batch(dev, steps, warmup, nprob=512, seed=4, rank=0, world=1, cpu_base=T
                        "split": "cost model C (G log G + M taps) iters, LPT" if world > 1 else "one GPU",
                        "predicted_load_max_over_mean": max(loads) / (sum(loads) / world)},
             "loop_of_single_solves": loop,
+            "analysis": extra,
             "max_rel_diff_batch_vs_loop": diff, "gpu_launches": launches,
             "autotuned_bins": table, "autotune_ms": detail, "gen_s": gen_s, "setup_s": setup_s,
             "clocks": clk.summary(),
@@ -781,6 +833,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "normal3d", "batch", "scatter"])
     ap.add_argument("--coils", type=int, default=8, help="normal3d: coils")
+    ap.add_argument("--analysis", action="store_true",
+                    help="batch: also the solves spread over streams and timed alone per embedding size")
     ap.add_argument("--spokes", type=int, default=20000, help="nufft3d: kooshball spokes")
     ap.add_argument("--methods", default="fcg_padded,fcg_circulant,cg,fcg_learned",
                     help="solvers to time (cgsense2d); the first is the headline")
@@ -828,7 +882,8 @@ def main():
         return
 
     if args.workload == "batch":
-        out = run_batch(dev, args.steps, args.warmup, rank=rank, world=world, cpu_base=not args.no_cpu_baseline)
+        out = run_batch(dev, args.steps, args.warmup, rank=rank, world=world, cpu_base=not args.no_cpu_baseline,
+                        analysis=args.analysis)
         if rank == 0:
             print(json.dumps(out), flush=True)
         if world > 1:
