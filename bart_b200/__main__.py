@@ -1,10 +1,12 @@
-"""Command line mirror of ``bart nufft`` and ``bart pics -t`` with .cfl I/O.
+"""Command line mirror of ``bart nufft``, ``bart pics -t`` and ``bart ecalib`` with .cfl I/O.
 
   python -m bart_b200 nufft [-a|-i [-c] [-l lambda] [-m iter]] [-x X:Y:Z] [-P] [-r|-t]
                             [-p pattern] [-B basis] [-o os] traj input output
   python -m bart_b200 pics -l2 -r lambda [-i iter] -t traj [-w scale] [-S]
                            [--no-toeplitz] ksp sens output
   python -m bart_b200 -l flags pics ...   (or -p flags: the same here)
+  python -m bart_b200 ecalib [-k k] [-r cal] [-m maps] [-t thr] [-c crop] [-S] [-P]
+                             [-n numsv] [-p percent] [-V] kspace sens [emaps]
 
 The k-space argument of pics may be "-": a stream of the reference's
 (src/misc/stream.c, e.g. from `copy --stream flags -- ksp -`) on stdin.
@@ -22,8 +24,8 @@ graph launch and the images are joined along the flagged dims. Launched by
 torchrun with several ranks (one per GPU), the problems are split over the
 ranks by their cost and rank 0 gathers the images and writes the output.
 
-Options follow src/nufft.c:75-101 and src/pics.c:137-199; options of the
-reference that are not built here are rejected with an error.
+Options follow src/nufft.c:75-101, src/pics.c:137-199 and src/ecalib.c:64-97;
+options of the reference that are not built here are rejected with an error.
 """
 
 from __future__ import annotations
@@ -239,6 +241,65 @@ def main_pics(argv, loop_flags: int = 0) -> int:
     return 0
 
 
+def _vec3_or_one(s: str):
+    """opt_vec3 (src/misc/opts.c:1075-1096): "x:y:z" or one value for all three."""
+    v = s.split(":")
+    if len(v) == 3:
+        return [int(x) for x in v]
+    return [int(v[0])] * 3
+
+
+def main_ecalib(argv) -> int:
+    """bart ecalib (src/ecalib.c:46-262)."""
+    from .espirit import EcalibConf, ecalib
+    ap = argparse.ArgumentParser(prog="ecalib")
+    ap.add_argument("-t", dest="threshold", type=float, default=0.001)
+    ap.add_argument("-c", dest="crop", type=float, default=0.8)
+    ap.add_argument("-k", "-K", dest="kdims", type=_vec3_or_one, default=[6, 6, 6])
+    ap.add_argument("-r", "-R", dest="calsize", type=_vec3_or_one, default=[24, 24, 24])
+    ap.add_argument("-m", dest="maps", type=int, default=2)
+    ap.add_argument("-S", dest="softcrop", action="store_true")
+    ap.add_argument("-W", dest="weighting", action="store_true")
+    ap.add_argument("-I", dest="intensity", action="store_true")
+    ap.add_argument("-1", dest="one", action="store_true")
+    ap.add_argument("-P", dest="norotphase", action="store_true")
+    ap.add_argument("-N", dest="phase_normalize", action="store_true")
+    ap.add_argument("-A", dest="nystroem", action="store_true")
+    ap.add_argument("-O", dest="no_orthiter", action="store_true")
+    ap.add_argument("-i", "--orthiter", dest="num_orthiter", type=int, default=30)
+    ap.add_argument("-p", dest="percentsv", type=float, default=-1.0)
+    ap.add_argument("-n", dest="numsv", type=int, default=-1)
+    ap.add_argument("-a", dest="automate", action="store_true")
+    ap.add_argument("-v", dest="var", type=float, default=-1.0)
+    ap.add_argument("-V", dest="print_svals", action="store_true")
+    ap.add_argument("-d", dest="debug", type=int, default=0)
+    ap.add_argument("kspace")
+    ap.add_argument("sens")
+    ap.add_argument("emaps", nargs="?")
+    a = ap.parse_args(argv)
+    if a.one:
+        sys.stderr.write("ecalib: -1 (first part only) is not built\n")
+        return 1
+    conf = EcalibConf(kdims=tuple(a.kdims), calsize=tuple(a.calsize), maps=a.maps, threshold=a.threshold,
+                      numsv=a.numsv, percentsv=a.percentsv, crop=a.crop, softcrop=a.softcrop,
+                      rotphase=not a.norotphase, num_orthiter=a.num_orthiter, intensity=a.intensity,
+                      phase_normalize=a.phase_normalize, nystroem=a.nystroem, orthiter=not a.no_orthiter)
+    if a.automate:				# src/ecalib.c:109-113
+        conf.crop = -1.0
+        conf.weighting = True
+    if a.weighting:
+        conf.weighting = True
+    ksp = readcfl(a.kspace)
+    sens, ev, info = ecalib(ksp, conf, emaps=a.emaps is not None)
+    writecfl(a.sens, sens)
+    if a.emaps is not None:
+        writecfl(a.emaps, ev)
+    if a.print_svals:
+        for i, v in enumerate(info["svals"]):
+            print(f"SVALS {i} {v:f}")
+    return 0
+
+
 def main(argv=None) -> int:
     argv = list(sys.argv[1:] if argv is None else argv)
     flags = 0
@@ -248,9 +309,11 @@ def main(argv=None) -> int:
             return 2
         flags |= int(argv[1])
         argv = argv[2:]
-    if not argv or argv[0] not in ("nufft", "pics") or (flags and argv[0] != "pics"):
+    if not argv or argv[0] not in ("nufft", "pics", "ecalib") or (flags and argv[0] != "pics"):
         sys.stderr.write(__doc__)
         return 2
+    if "ecalib" == argv[0]:
+        return main_ecalib(argv[1:])
     if "pics" == argv[0]:
         return main_pics(argv[1:], flags)
     return main_nufft(argv[1:])

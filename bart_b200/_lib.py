@@ -1,4 +1,5 @@
-"""ctypes binding of the C ABI in include/bnufft.h (``bart_b200/lib/libbnufft.so``).
+"""ctypes binding of the C ABI in include/bnufft.h and include/bespirit.h
+(``bart_b200/lib/libbnufft.so``).
 
 The library is the product; this module only declares its signatures. There
 is no fallback: if the shared library or a CUDA device is missing, loading or
@@ -27,6 +28,14 @@ class PicsConfC(ctypes.Structure):
                 ("periodic", ctypes.c_int), ("deterministic", ctypes.c_int), ("bin", ctypes.c_int),
                 ("precond", ctypes.c_int), ("ref_scalars", ctypes.c_int),
                 ("net_iters", ctypes.c_int)]
+
+
+class EcalibConfC(ctypes.Structure):
+    _fields_ = [("kdims", ctypes.c_long * 3), ("calsize", ctypes.c_long * 3), ("maps", ctypes.c_int),
+                ("threshold", ctypes.c_float), ("numsv", ctypes.c_int), ("percentsv", ctypes.c_float),
+                ("crop", ctypes.c_float), ("softcrop", ctypes.c_int), ("rotphase", ctypes.c_int),
+                ("orthiter", ctypes.c_int), ("num_orthiter", ctypes.c_int), ("weighting", ctypes.c_int),
+                ("intensity", ctypes.c_int), ("phase_normalize", ctypes.c_int), ("nystroem", ctypes.c_int)]
 
 
 _lib = None
@@ -93,6 +102,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     sig("bnufft_calc_beta", ctypes.c_double, ctypes.c_float, ctypes.c_float)
     sig("bnufft_kb_precompute", i, ctypes.c_double, i, fp)
     sig("bnufft_rolloff_axis", i, ctypes.c_float, ctypes.c_float, ctypes.c_long, ctypes.POINTER(ctypes.c_double))
+    sig("bnufft_ecalib_defaults", None, ctypes.POINTER(EcalibConfC))
+    sig("bnufft_ecalib_dims", i, ctypes.POINTER(EcalibConfC), i, cl, cl, cl)
+    sig("bnufft_ecalib", i, ctypes.POINTER(EcalibConfC), i, cl, vp, vp, vp, fp, cl, cl, vp)
     sig("bnufft_last_error", ctypes.c_char_p)
     sig("bnufft_launch_count", ctypes.c_long)
     sig("bnufft_prof_start", i, ctypes.c_char_p)

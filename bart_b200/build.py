@@ -1,7 +1,8 @@
 """Build the sm_100a shared library ``bart_b200/lib/libbnufft.so`` in-tree.
 
 ``python -m bart_b200.build`` (or ``build()``) runs nvcc directly; the
-library has a plain C ABI (include/bnufft.h) and links only the CUDA runtime.
+library has a plain C ABI (include/bnufft.h, include/bespirit.h) and links only the CUDA
+runtime; the ESPIRiT calibration loads cuSOLVER on first use.
 """
 
 from __future__ import annotations
@@ -16,8 +17,8 @@ LIB = os.path.join(HERE, "lib", "libbnufft.so")
 SOURCES = [os.path.join(HERE, "csrc", "bnufft.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft_core.cuh", "nufft_kernels.cuh", "cg_kernels.cuh", "gridding.cuh",
                                                    "precnet.cuh", "nudft.cuh", "precond_cluster.cuh", "fft512.cuh",
-                                                   "precnet_tc.cuh")] + \
-    [os.path.join(ROOT, "include", "bnufft.h")]
+                                                   "precnet_tc.cuh", "espirit.cuh")] + \
+    [os.path.join(ROOT, "include", f) for f in ("bnufft.h", "bespirit.h")]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

@@ -4893,3 +4893,6 @@ extern "C" int bnufft_forward2d_noalloc(long X, long Y, long M, const void* traj
 	LAUNCHED();
 	return BNUFFT_OK;
 }
+
+// ESPIRiT calibration (include/bespirit.h)
+#include "espirit.cuh"

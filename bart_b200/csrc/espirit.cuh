@@ -1,0 +1,1158 @@
+// ESPIRiT calibration (bart ecalib) on the GPU: the reference's default
+// path (src/ecalib.c:46-262, src/calib/calib.c) as
+//
+//   calibration region (host search over the centre block's pattern)
+//   -> Casorati matrix of the region's kernel-sized patches
+//   -> Gram matrix (tiled complex GEMM)
+//   -> Hermitian eigen-decomposition (cuSOLVER cheevd, the one library
+//      call: the reference calls LAPACK cheev here)
+//   -> kernel images on the (2k)^d grid (DFT as a complex GEMM) and their
+//      packed C x C Gram matrix per low-resolution pixel
+//   -> sinc interpolation along y and z to every image row
+//   -> one fused pass per image pixel: sinc interpolation along x, the
+//      orthogonal iteration, eigenvalue crop and phase alignment, written
+//      straight to the maps [X, Y, Z, C, maps].
+//
+// This file is included into bnufft.cu and uses its error and launch
+// helpers (fail, CUDA_TRY, LAUNCHED, TRY, on_device).
+
+#include <dlfcn.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <type_traits>
+
+#include "../../include/bespirit.h"
+
+namespace bn {
+
+// ---------------------------------------------------------------------------
+// device kernels
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float2 ec_cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ float2 ec_cmulc(float2 a, float2 b) { return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }	// a conj(b)
+__device__ __forceinline__ float2 ec_conj(float2 a) { return make_float2(a.x, -a.y); }
+
+// dst[bx, by, bz, C] (contiguous) = src[ox + x, oy + y, oz + z, c] of a
+// [X, Y, Z, C] array.
+__global__ void k_ec_gather(const float2* __restrict__ src, long X, long Y, long Z, int C, int ox, int oy, int oz,
+			    int bx, int by, int bz, float2* __restrict__ dst)
+{
+	const long n = (long)bx * by * bz * C;
+
+	for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		long t = i;
+		const int x = (int)(t % bx); t /= bx;
+		const int y = (int)(t % by); t /= by;
+		const int z = (int)(t % bz);
+		const int c = (int)(t / bz);
+		dst[i] = src[(ox + x) + X * ((oy + y) + Y * ((oz + z) + Z * (long)c))];
+	}
+}
+
+// Casorati matrix A [P][Ncol] (row-major): A[p][j] = cal[p + k_j, c_j] with
+// j = kx_i + kx (ky_i + ky (kz_i + kz c)) (src/num/casorati.c:34-65).
+__global__ void k_ec_casorati(const float2* __restrict__ cal, int cx, int cy, int cz, int kx, int ky, int kz, int C,
+			      float2* __restrict__ A)
+{
+	const int px = cx - kx + 1, py = cy - ky + 1, pz = cz - kz + 1;
+	const long P = (long)px * py * pz;
+	const long ncol = (long)kx * ky * kz * C;
+
+	for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < P * ncol; i += (long)gridDim.x * blockDim.x) {
+
+		const long p = i / ncol;
+		long j = i % ncol;
+		const int jx = (int)(j % kx); j /= kx;
+		const int jy = (int)(j % ky); j /= ky;
+		const int jz = (int)(j % kz);
+		const int c = (int)(j / kz);
+		const int x = (int)(p % px), y = (int)((p / px) % py), z = (int)(p / ((long)px * py));
+		A[i] = cal[(x + jx) + (long)cx * ((y + jy) + (long)cy * ((z + jz) + (long)cz * c))];
+	}
+}
+
+// C [M][N] = op(A) [M][K] * B [K][N], row-major complex float, 64 x 64
+// tiles, 4 x 4 outputs per thread. CONJ_A: op(A) = A^H with A stored
+// [K][M]; else A stored [M][K].
+template <bool CONJ_A>
+__global__ void __launch_bounds__(256) k_ec_cgemm(int M, int N, int K, const float2* __restrict__ A, long lda,
+						  const float2* __restrict__ B, long ldb, float2* __restrict__ Cm, long ldc)
+{
+	__shared__ float2 As[16][64 + 1];
+	__shared__ float2 Bs[16][64 + 1];
+
+	const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+	const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+
+	float2 acc[4][4];
+
+	for (int i = 0; i < 4; i++)
+		for (int j = 0; j < 4; j++)
+			acc[i][j] = make_float2(0.f, 0.f);
+
+	for (int k0 = 0; k0 < K; k0 += 16) {
+
+		for (int e = threadIdx.x; e < 1024; e += 256) {
+
+			int kk, mm;
+
+			if (CONJ_A) {
+
+				kk = e / 64;
+				mm = e % 64;
+
+			} else {
+
+				mm = e / 16;
+				kk = e % 16;
+			}
+
+			const int gm = m0 + mm, gk = k0 + kk;
+			float2 a = make_float2(0.f, 0.f);
+
+			if (gm < M && gk < K)
+				a = CONJ_A ? ec_conj(A[gk * lda + gm]) : A[gm * lda + gk];
+
+			As[kk][mm] = a;
+
+			const int nn = e % 64, kb = e / 64, gn = n0 + nn, gkb = k0 + kb;
+			Bs[kb][nn] = (gn < N && gkb < K) ? B[gkb * ldb + gn] : make_float2(0.f, 0.f);
+		}
+
+		__syncthreads();
+
+#pragma unroll
+		for (int kk = 0; kk < 16; kk++) {
+
+			float2 a[4], b[4];
+
+			for (int i = 0; i < 4; i++)
+				a[i] = As[kk][ty * 4 + i];
+
+			for (int j = 0; j < 4; j++)
+				b[j] = Bs[kk][tx * 4 + j];
+
+			for (int i = 0; i < 4; i++)
+				for (int j = 0; j < 4; j++) {
+
+					acc[i][j].x = fmaf(a[i].x, b[j].x, fmaf(-a[i].y, b[j].y, acc[i][j].x));
+					acc[i][j].y = fmaf(a[i].x, b[j].y, fmaf(a[i].y, b[j].x, acc[i][j].y));
+				}
+		}
+
+		__syncthreads();
+	}
+
+	for (int i = 0; i < 4; i++)
+		for (int j = 0; j < 4; j++) {
+
+			const int gm = m0 + ty * 4 + i, gn = n0 + tx * 4 + j;
+
+			if (gm < M && gn < N)
+				Cm[gm * ldc + gn] = acc[i][j];
+		}
+}
+
+// Kernels in descending eigenvalue order, arranged for the kernel-image
+// GEMM: KT[u][c n + i] = E[N - 1 - i][u + kd c] (E row-major: row r is the
+// eigenvector of the r-th smallest eigenvalue, as LAPACK returns them).
+__global__ void k_ec_kern_perm(const float2* __restrict__ E, int Ncol, int kd, int C, int n, float2* __restrict__ KT)
+{
+	const long tot = (long)kd * C * n;
+
+	for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
+
+		const int u = (int)(t / ((long)C * n));
+		const int r = (int)(t % ((long)C * n));
+		const int c = r / n, i = r % n;
+		KT[t] = E[(long)(Ncol - 1 - i) * Ncol + u + (long)kd * c];
+	}
+}
+
+// Packed lower-triangular Gram matrix of the kernel images per
+// low-resolution pixel: cov[x][l(a, b)] = sum_i conj(K[x][a n + i])
+// K[x][b n + i] * scale, l(a, b) = a (a + 1) / 2 + b, b <= a
+// (src/calib/calib.c:1072-1088, src/num/linalg.c:642-664, 1211-1232).
+__global__ void k_ec_pixgram(const float2* __restrict__ Kimg, int C, int n, float scale, float2* __restrict__ cov)
+{
+	const int x = blockIdx.x;
+	const int L = C * (C + 1) / 2;
+	const float2* K = Kimg + (long)x * C * n;
+
+	for (int l = threadIdx.x; l < L; l += blockDim.x) {
+
+		int a = (int)((sqrtf(8.f * l + 1.f) - 1.f) * 0.5f);
+
+		while (a * (a + 1) / 2 > l)
+			a--;
+
+		while ((a + 1) * (a + 2) / 2 <= l)
+			a++;
+
+		const int b = l - a * (a + 1) / 2;
+		const float2* ka = K + (long)a * n;
+		const float2* kb = K + (long)b * n;
+		float sr = 0.f, si = 0.f;
+
+		for (int i = 0; i < n; i++) {
+
+			const float2 p = ka[i], q = kb[i];	// conj(p) q
+			sr = fmaf(p.x, q.x, fmaf(p.y, q.y, sr));
+			si = fmaf(p.x, q.y, fmaf(-p.y, q.x, si));
+		}
+
+		cov[(long)x * L + l] = make_float2(sr * scale, si * scale);
+	}
+}
+
+// sinc interpolation along y and z (the reference's sinc_zeropad,
+// src/misc/resize.c:234-292, written as its per-axis linear maps):
+// T[(z Y + y)][u][l] = sum_{v, w} Ry[y][v] Rz[z][w] cov[(w yh + v) xh + u][l].
+__global__ void k_ec_interp_yz(const float2* __restrict__ cov, int xh, int yh, int zh, int L, int Y,
+			       const float2* __restrict__ Ry, const float2* __restrict__ Rz, float2* __restrict__ T)
+{
+	const int row = blockIdx.x;
+	const int y = row % Y, z = row / Y;
+	const int n = xh * L;
+
+	for (int t = threadIdx.x; t < n; t += blockDim.x) {
+
+		const int u = t / L, l = t % L;
+		float2 s = make_float2(0.f, 0.f);
+
+		for (int w = 0; w < zh; w++) {
+
+			const float2 rz = Rz[(long)z * zh + w];
+
+			for (int v = 0; v < yh; v++) {
+
+				const float2 r = ec_cmul(Ry[(long)y * yh + v], rz);
+				const float2 c = cov[((long)(w * yh + v) * xh + u) * L + l];
+				s.x = fmaf(r.x, c.x, fmaf(-r.y, c.y, s.x));
+				s.y = fmaf(r.x, c.y, fmaf(r.y, c.x, s.y));
+			}
+		}
+
+		T[(long)row * n + t] = s;
+	}
+}
+
+template <int W>
+__device__ __forceinline__ float ec_group_sum(float v)
+{
+#pragma unroll
+	for (int o = W / 2; o > 0; o >>= 1)
+		v += __shfl_xor_sync(0xffffffffu, v, o);
+
+	return v;
+}
+
+// One pass per image pixel: W lanes per pixel (lane c = coil c, W >= C,
+// 32 / W pixels per warp), PX = 8 * 32 / W consecutive pixels of one image
+// row per block.
+//   1. lane c builds column c of the pixel's C x C Hermitian matrix from
+//      the row's y/z-interpolated packed covariance (shared memory) and
+//      the x-interpolation row Rx[x] (the upper triangle is the conjugate
+//      of the lower, src/calib/calib.c:73-86);
+//   2. iters steps of orthogonal iteration: rows v_m <- v_m H, then
+//      Gram-Schmidt from the last row to the first (src/num/linalg.c
+//      :1235-1313); the last row is the principal eigenvector;
+//   3. map u = row M-1-u with eigenvalue = that row's last norm
+//      (src/calib/calib.c:474-483); weight 0/1 for |e| >= crop, or the
+//      reference's soft s-curve (src/calib/calib.c:88-134);
+//   4. phase: times conj of the phase of sum_c map[c] conj(rot[c])
+//      (src/misc/utils.c:148-174);
+//   5. staged through shared memory and written coalesced along x.
+template <int W, int MMAX>
+__global__ void __launch_bounds__(256) k_ec_eigen(int X, int Y, int Z, int C, int M, int xh, int L,
+						  const float2* __restrict__ T, const float2* __restrict__ Rx,
+						  const float2* __restrict__ rot, int iters, float crop, int soft,
+						  float2* __restrict__ sens, float2* __restrict__ ev)
+{
+	constexpr int PX = 8 * 32 / W;
+	extern __shared__ float2 ec_smem[];
+	float2* sT = ec_smem;				// [xh][L]
+	float2* sR = sT + (long)xh * L;			// [PX][xh]
+	float2* sO = sR + PX * xh;			// [PX][M][C]
+	float* sE = (float*)(sO + PX * M * C);		// [PX][M]
+
+	const int row = blockIdx.x;
+	const int y = row % Y, z = row / Y;
+	const int x0 = blockIdx.y * PX;
+	const float2* Trow = T + (long)row * xh * L;
+
+	for (int t = threadIdx.x; t < xh * L; t += blockDim.x)
+		sT[t] = Trow[t];
+
+	for (int t = threadIdx.x; t < PX * xh; t += blockDim.x) {
+
+		const int px = t / xh, u = t % xh;
+		sR[t] = (x0 + px < X) ? Rx[(long)(x0 + px) * xh + u] : make_float2(0.f, 0.f);
+	}
+
+	__syncthreads();
+
+	const int lane = threadIdx.x % 32;
+	const int c = lane % W;
+	const int px = (threadIdx.x / 32) * (32 / W) + lane / W;
+	const bool act = c < C;
+	const float2* rx = sR + px * xh;
+
+	float2 Hc[W];
+
+#pragma unroll
+	for (int k = 0; k < W; k++) {
+
+		float2 s = make_float2(0.f, 0.f);
+
+		if (act && k < C) {
+
+			const bool lo = c <= k;
+			const int l = lo ? k * (k + 1) / 2 + c : c * (c + 1) / 2 + k;
+
+			for (int u = 0; u < xh; u++) {
+
+				const float2 r = rx[u], v = sT[u * L + l];
+				s.x = fmaf(r.x, v.x, fmaf(-r.y, v.y, s.x));
+				s.y = fmaf(r.x, v.y, fmaf(r.y, v.x, s.y));
+			}
+
+			if (!lo)
+				s.y = -s.y;
+		}
+
+		Hc[k] = s;
+	}
+
+	float2 v[MMAX];
+	float val[MMAX];
+
+#pragma unroll
+	for (int m = 0; m < MMAX; m++) {
+
+		v[m] = make_float2((m < M && c == m) ? 1.f : 0.f, 0.f);
+		val[m] = 0.f;
+	}
+
+	for (int it = 0; it < iters; it++) {
+
+#pragma unroll
+		for (int m = 0; m < MMAX; m++) {
+
+			if (m >= M)
+				continue;
+
+			float2 s = make_float2(0.f, 0.f);
+
+#pragma unroll
+			for (int k = 0; k < W; k++) {
+
+				const float2 a = make_float2(__shfl_sync(0xffffffffu, v[m].x, k, W), __shfl_sync(0xffffffffu, v[m].y, k, W));
+				s.x = fmaf(a.x, Hc[k].x, fmaf(-a.y, Hc[k].y, s.x));
+				s.y = fmaf(a.x, Hc[k].y, fmaf(a.y, Hc[k].x, s.y));
+			}
+
+			v[m] = s;
+		}
+
+#pragma unroll
+		for (int m = MMAX - 1; m >= 0; m--) {
+
+			if (m >= M)
+				continue;
+
+#pragma unroll
+			for (int j = m + 1; j < MMAX; j++) {
+
+				if (j >= M)
+					continue;
+
+				const float2 p = ec_cmulc(v[m], v[j]);
+				const float sr = ec_group_sum<W>(p.x), si = ec_group_sum<W>(p.y);
+				v[m].x -= sr * v[j].x - si * v[j].y;
+				v[m].y -= sr * v[j].y + si * v[j].x;
+			}
+
+			const float nrm = sqrtf(ec_group_sum<W>(v[m].x * v[m].x + v[m].y * v[m].y));
+			val[m] = nrm;
+			const float inv = (nrm > 0.f) ? 1.f / nrm : 0.f;
+			v[m].x *= inv;
+			v[m].y *= inv;
+		}
+	}
+
+#pragma unroll
+	for (int u = 0; u < MMAX; u++) {
+
+		if (u >= M)
+			continue;
+
+		const int r = M - 1 - u;
+		float2 mv = make_float2(0.f, 0.f);
+		float e = 0.f;
+
+#pragma unroll
+		for (int q = 0; q < MMAX; q++)
+			if (q == r) {
+
+				mv = v[q];
+				e = val[q];
+			}
+
+		float w;
+
+		if (soft) {
+
+			const float t = (sqrtf(fabsf(e)) - crop) / (1.f - crop);
+			w = ((t >= 1.f) ? 1.f : 0.f) + ((t >= -1.f) ? (t / (t * t + 1.f) + 0.5f) : 0.f);
+
+		} else {
+
+			w = (fabsf(e) >= crop) ? 1.f : 0.f;
+		}
+
+		mv.x *= w;
+		mv.y *= w;
+
+		const float2 rc = act ? rot[c] : make_float2(0.f, 0.f);
+		const float2 p = ec_cmulc(mv, rc);
+		const float sr = ec_group_sum<W>(p.x), si = ec_group_sum<W>(p.y);
+		const float a = sqrtf(sr * sr + si * si);
+		const float2 ph = (a == 0.f) ? make_float2(1.f, 0.f) : make_float2(sr / a, si / a);
+		const float2 o = ec_cmulc(mv, ph);
+
+		if (act)
+			sO[(px * M + u) * C + c] = o;
+
+		if (0 == c)
+			sE[px * M + u] = e;
+	}
+
+	__syncthreads();
+
+	const long npix = (long)X * Y * Z;
+	const long base = (long)x0 + (long)X * (y + (long)Y * z);
+	const int nx = min(PX, X - x0);
+
+	for (int t = threadIdx.x; t < PX * M * C; t += blockDim.x) {
+
+		const int p = t % PX, cu = t / PX;
+		const int cc = cu % C, u = cu / C;
+
+		if (p < nx)
+			sens[base + p + npix * (cc + (long)C * u)] = sO[(p * M + u) * C + cc];
+	}
+
+	if (nullptr != ev)
+		for (int t = threadIdx.x; t < PX * M; t += blockDim.x) {
+
+			const int p = t % PX, u = t / PX;
+
+			if (p < nx)
+				ev[base + p + npix * u] = make_float2(sE[p * M + u], 0.f);
+		}
+}
+
+// coil covariance of the calibration data, row-major [C][C]:
+// Gc[i][j] = sum_p conj(d_i[p]) d_j[p] (src/calib/cc.c:56-57,
+// src/num/linalg.c:642-654)
+__global__ void k_ec_coilcov(const float2* __restrict__ cal, long csize, int C, float2* __restrict__ Gc)
+{
+	const int i = blockIdx.x / C, j = blockIdx.x % C;
+	const float2* a = cal + csize * i;
+	const float2* b = cal + csize * j;
+	double sr = 0., si = 0.;
+
+	for (long p = threadIdx.x; p < csize; p += blockDim.x) {
+
+		const float2 x = a[p], y = b[p];
+		sr += (double)x.x * y.x + (double)x.y * y.y;
+		si += (double)x.x * y.y - (double)x.y * y.x;
+	}
+
+	__shared__ double rr[256], ri[256];
+	rr[threadIdx.x] = sr;
+	ri[threadIdx.x] = si;
+	__syncthreads();
+
+	for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+
+		if ((int)threadIdx.x < o) {
+
+			rr[threadIdx.x] += rr[threadIdx.x + o];
+			ri[threadIdx.x] += ri[threadIdx.x + o];
+		}
+
+		__syncthreads();
+	}
+
+	if (0 == threadIdx.x)
+		Gc[blockIdx.x] = make_float2((float)rr[0], (float)ri[0]);
+}
+
+}	// namespace bn
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+// cuSOLVER, loaded on first use so that the NUFFT / CG entry points keep
+// depending on the CUDA runtime alone.
+struct EcSolver {
+
+	cusolverStatus_t (*create)(cusolverDnHandle_t*);
+	cusolverStatus_t (*destroy)(cusolverDnHandle_t);
+	cusolverStatus_t (*set_stream)(cusolverDnHandle_t, cudaStream_t);
+	cusolverStatus_t (*heevd_size)(cusolverDnHandle_t, cusolverEigMode_t, cublasFillMode_t, int, const cuComplex*, int, const float*, int*);
+	cusolverStatus_t (*heevd)(cusolverDnHandle_t, cusolverEigMode_t, cublasFillMode_t, int, cuComplex*, int, float*, cuComplex*, int, int*);
+};
+
+static int ec_solver(const EcSolver** out)
+{
+	static EcSolver api;
+	static int state = 0;	// 0 unloaded, 1 ok, 2 failed
+	static std::mutex mu;
+	std::lock_guard<std::mutex> lock(mu);
+
+	if (0 == state) {
+
+		void* h = dlopen("libcusolver.so.11", RTLD_NOW | RTLD_LOCAL);
+
+		if (nullptr == h)
+			h = dlopen("libcusolver.so", RTLD_NOW | RTLD_LOCAL);
+
+		state = 2;
+
+		if (nullptr != h) {
+
+			api.create = (decltype(api.create))dlsym(h, "cusolverDnCreate");
+			api.destroy = (decltype(api.destroy))dlsym(h, "cusolverDnDestroy");
+			api.set_stream = (decltype(api.set_stream))dlsym(h, "cusolverDnSetStream");
+			api.heevd_size = (decltype(api.heevd_size))dlsym(h, "cusolverDnCheevd_bufferSize");
+			api.heevd = (decltype(api.heevd))dlsym(h, "cusolverDnCheevd");
+
+			if (api.create && api.destroy && api.set_stream && api.heevd_size && api.heevd)
+				state = 1;
+		}
+	}
+
+	if (1 != state)
+		return fail(BNUFFT_ERR_CUDA, "ecalib: cuSOLVER (libcusolver.so.11) not available");
+
+	*out = &api;
+	return BNUFFT_OK;
+}
+
+// Hermitian eigen-decomposition of the n x n matrix that the column-major
+// view of A shows (for a row-major Hermitian G that is conj(G), what the
+// reference hands LAPACK): eigenvalues ascending in w, eigenvector i in
+// column i (= row i of the row-major array).
+static int ec_heevd(int n, float2* A, float* w, cudaStream_t st)
+{
+	const EcSolver* api = nullptr;
+	TRY(ec_solver(&api));
+
+	cusolverDnHandle_t h = nullptr;
+
+	if (CUSOLVER_STATUS_SUCCESS != api->create(&h))
+		return fail(BNUFFT_ERR_CUDA, "ecalib: cusolverDnCreate failed");
+
+	int status = BNUFFT_OK;
+	int lwork = 0;
+	cuComplex* work = nullptr;
+	int* info = nullptr;
+	int hinfo = 0;
+
+	if (CUSOLVER_STATUS_SUCCESS != api->set_stream(h, st)
+	    || CUSOLVER_STATUS_SUCCESS != api->heevd_size(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, (const cuComplex*)A, n, w, &lwork)) {
+
+		status = fail(BNUFFT_ERR_CUDA, "ecalib: cheevd workspace query failed");
+
+	} else if (cudaSuccess != cudaMalloc(&work, sizeof(cuComplex) * (size_t)std::max(lwork, 1))
+		   || cudaSuccess != cudaMalloc(&info, sizeof(int))) {
+
+		status = fail(BNUFFT_ERR_NOMEM, "ecalib: cheevd workspace (%d) allocation failed", lwork);
+
+	} else if (CUSOLVER_STATUS_SUCCESS != api->heevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, (cuComplex*)A, n, w, work, lwork, info)
+		   || cudaSuccess != cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, st)
+		   || cudaSuccess != cudaStreamSynchronize(st)) {
+
+		status = fail(BNUFFT_ERR_CUDA, "ecalib: cheevd failed");
+
+	} else if (0 != hinfo) {
+
+		status = fail(BNUFFT_ERR_CUDA, "ecalib: cheevd info %d", hinfo);
+	}
+
+	cudaFree(work);
+	cudaFree(info);
+	api->destroy(h);
+	return status;
+}
+
+// fftmod phase of index j on an axis of length n (src/num/fft.c:62-90)
+static std::complex<double> ec_fftmod(long n, long j, bool inv)
+{
+	const long c = n / 2;
+	const double ph = ((double)j - (double)c / 2.) * ((double)c / (double)n);
+	const double rem = ph - std::floor(ph);
+	const double sg = inv ? -1. : 1.;
+
+	if (0. == rem)
+		return 1.;
+
+	if (0.5 == rem)
+		return -1.;
+
+	if (0.25 == rem)
+		return std::complex<double>(0., sg);
+
+	if (0.75 == rem)
+		return std::complex<double>(0., -sg);
+
+	return std::polar(1., 2. * M_PI * sg * rem);
+}
+
+// The linear map of the reference's sinc_resize along one axis from n to m
+// points (src/misc/resize.c:234-261: fftmod, FFT, fftmod, centred
+// zero-padding, ifftmod, unnormalised inverse FFT, ifftmod), [m][n]
+// row-major.
+static std::vector<float2> ec_sinc_matrix(long n, long m)
+{
+	std::vector<float2> R((size_t)(m * n));
+
+	if (n == m) {
+
+		for (long i = 0; i < n; i++)
+			R[(size_t)(i * n + i)] = make_float2(1.f, 0.f);
+
+		return R;
+	}
+
+	const long p = m / 2 - n / 2;
+
+	for (long x = 0; x < m; x++)
+		for (long u = 0; u < n; u++) {
+
+			std::complex<double> s = 0.;
+
+			for (long f = 0; f < n; f++) {
+
+				const long g = f + p;
+				s += std::polar(1., 2. * M_PI * (double)(g * x % m) / (double)m) * ec_fftmod(m, g, true)
+				     * ec_fftmod(n, f, false) * std::polar(1., -2. * M_PI * (double)(f * u % n) / (double)n);
+			}
+
+			s *= ec_fftmod(m, x, true) * ec_fftmod(n, u, false);
+			R[(size_t)(x * n + u)] = make_float2((float)s.real(), (float)s.imag());
+		}
+
+	return R;
+}
+
+// The kernel-image transform: zero-pad [kx, ky, kz] centred into
+// [xh, yh, zh], ifftmod, unnormalised inverse FFT (src/calib/calib.c
+// :1004-1057), as a [hd][kd] row-major matrix.
+static std::vector<float2> ec_kernel_dft(const long kd3[3], const long hd3[3])
+{
+	const long kd = kd3[0] * kd3[1] * kd3[2], hd = hd3[0] * hd3[1] * hd3[2];
+	std::vector<std::complex<double>> ax[3];
+
+	for (int a = 0; a < 3; a++) {
+
+		const long h = hd3[a], k = kd3[a], p = h / 2 - k / 2;
+		ax[a].resize((size_t)(h * k));
+
+		for (long x = 0; x < h; x++)
+			for (long u = 0; u < k; u++)
+				ax[a][(size_t)(x * k + u)] = std::polar(1., 2. * M_PI * (double)((u + p) * x % h) / (double)h) * ec_fftmod(h, u + p, true);
+	}
+
+	std::vector<float2> F((size_t)(hd * kd));
+
+	for (long x = 0; x < hd; x++)
+		for (long u = 0; u < kd; u++) {
+
+			const long x0 = x % hd3[0], x1 = (x / hd3[0]) % hd3[1], x2 = x / (hd3[0] * hd3[1]);
+			const long u0 = u % kd3[0], u1 = (u / kd3[0]) % kd3[1], u2 = u / (kd3[0] * kd3[1]);
+			const std::complex<double> v = ax[0][(size_t)(x0 * kd3[0] + u0)] * ax[1][(size_t)(x1 * kd3[1] + u1)] * ax[2][(size_t)(x2 * kd3[2] + u2)];
+			F[(size_t)(x * kd + u)] = make_float2((float)v.real(), (float)v.imag());
+		}
+
+	return F;
+}
+
+// The calibration region (src/misc/mri2.c:100-160, 26-...): inside the
+// centre block tmp [tdims, C] (host copy), grow a centred fully sampled
+// block one line at a time per dimension up to calsize, then slide along
+// the readout to the position of largest energy (first maximum).
+static void ec_calib_geom(const std::vector<float2>& tmp, const long td[3], long C, const long calsize[3], long cal[3], long pos[3])
+{
+	const long tn = td[0] * td[1] * td[2];
+	std::vector<char> pat((size_t)tn, 0);
+
+	for (long i = 0; i < tn; i++) {
+
+		float s = 0.f;
+
+		for (long c = 0; c < C; c++) {
+
+			const float2 v = tmp[(size_t)(i + tn * c)];
+			s += v.x * v.x + v.y * v.y;
+		}
+
+		pat[(size_t)i] = (0.f != s);
+	}
+
+	for (int i = 0; i < 3; i++) {
+
+		cal[i] = 1;
+		pos[i] = (td[i] - 1) / 2;
+	}
+
+	bool stop[3] = { false, false, false };
+
+	auto full = [&]() {
+
+		for (long z = 0; z < cal[2]; z++)
+			for (long y = 0; y < cal[1]; y++)
+				for (long x = 0; x < cal[0]; x++)
+					if (!pat[(size_t)((pos[0] + x) + td[0] * ((pos[1] + y) + td[1] * (pos[2] + z)))])
+						return false;
+		return true;
+	};
+
+	while (!(stop[0] && stop[1] && stop[2])) {
+
+		for (int i = 0; i < 3; i++) {
+
+			if (cal[i] == td[i] || cal[i] >= calsize[i])
+				stop[i] = true;
+
+			if (stop[i])
+				continue;
+
+			cal[i]++;
+			pos[i] = (td[i] - cal[i]) / 2;
+
+			if (!full()) {
+
+				cal[i]--;
+				pos[i] = (td[i] - cal[i]) / 2;
+				stop[i] = true;
+			}
+		}
+	}
+
+	long best = 0;
+	double beng = 0.;
+
+	for (long r = 0; r + cal[0] <= td[0]; r++) {
+
+		double e = 0.;
+
+		for (long c = 0; c < C; c++)
+			for (long z = 0; z < cal[2]; z++)
+				for (long y = 0; y < cal[1]; y++)
+					for (long x = 0; x < cal[0]; x++) {
+
+						const float2 v = tmp[(size_t)((r + x) + td[0] * ((pos[1] + y) + td[1] * ((pos[2] + z) + td[2] * c)))];
+						e += (double)v.x * v.x + (double)v.y * v.y;
+					}
+
+		if (std::sqrt(e) > beng) {
+
+			best = r;
+			beng = std::sqrt(e);
+		}
+	}
+
+	pos[0] = best;
+}
+
+struct EcBuf {
+
+	std::vector<void*> p;
+	~EcBuf() { for (void* q : p) cudaFree(q); }
+
+	template <class T>
+	int alloc(T** out, size_t n)
+	{
+		void* q = nullptr;
+
+		if (cudaSuccess != cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T))) {
+
+			cudaGetLastError();
+			return fail(BNUFFT_ERR_NOMEM, "ecalib: out of device memory (%zu bytes)", n * sizeof(T));
+		}
+
+		p.push_back(q);
+		*out = (T*)q;
+		return BNUFFT_OK;
+	}
+};
+
+template <int W>
+static int ec_launch_eigen(int X, int Y, int Z, int C, int M, int xh, int L, const float2* T, const float2* Rx,
+			   const float2* rot, int iters, float crop, int soft, float2* sens, float2* ev, cudaStream_t st)
+{
+	constexpr int PX = 8 * 32 / W;
+	const size_t smem = sizeof(float2) * ((size_t)xh * L + (size_t)PX * xh + (size_t)PX * M * C) + sizeof(float) * PX * M;
+
+	auto kern = (M <= 4) ? bn::k_ec_eigen<W, 4> : bn::k_ec_eigen<W, 8>;
+
+	if (smem > 227 * 1024)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: %d coils with a %d-point kernel grid need %zu bytes of shared memory", C, xh, smem);
+
+	if (smem > 48 * 1024)
+		CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+
+	dim3 grid((unsigned)(Y * Z), (unsigned)((X + PX - 1) / PX));
+	cudaEvent_t pe = prof_begin("ecalib_pixels", st);
+	kern<<<grid, 256, smem, st>>>(X, Y, Z, C, M, xh, L, T, Rx, rot, iters, crop, soft, sens, ev);
+	prof_end(pe, st);
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+static unsigned ec_blocks(long n) { return (unsigned)std::min<long>((n + 255) / 256, 148L * 16); }
+
+static int ec_gemm(bool conj_a, int M, int N, int K, const float2* A, long lda, const float2* B, long ldb, float2* Cm, long ldc, cudaStream_t st)
+{
+	dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
+
+	if (conj_a)
+		bn::k_ec_cgemm<true><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
+	else
+		bn::k_ec_cgemm<false><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
+
+	LAUNCHED();
+	return BNUFFT_OK;
+}
+
+extern "C" void bnufft_ecalib_defaults(struct bnufft_ecalib_conf* conf)
+{
+	for (int i = 0; i < 3; i++) {
+
+		conf->kdims[i] = 6;
+		conf->calsize[i] = 24;
+	}
+
+	conf->maps = 2;
+	conf->threshold = 0.001f;
+	conf->numsv = -1;
+	conf->percentsv = -1.f;
+	conf->crop = 0.8f;
+	conf->softcrop = 0;
+	conf->rotphase = 1;
+	conf->orthiter = 1;
+	conf->num_orthiter = 30;
+	conf->weighting = 0;
+	conf->intensity = 0;
+	conf->phase_normalize = 0;
+	conf->nystroem = 0;
+}
+
+extern "C" int bnufft_ecalib_dims(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], long sens_dims[], long emaps_dims[])
+{
+	if (nullptr == conf || N < 5 || nullptr == ksp_dims)
+		return fail(BNUFFT_ERR_ARG, "ecalib: bad arguments");
+
+	for (int i = 0; i < N; i++) {
+
+		if (nullptr != sens_dims)
+			sens_dims[i] = 1;
+
+		if (nullptr != emaps_dims)
+			emaps_dims[i] = 1;
+	}
+
+	for (int i = 0; i < 3; i++) {
+
+		const long k = (1 == ksp_dims[i]) ? 1 : conf->kdims[i];
+
+		if (nullptr != sens_dims)
+			sens_dims[i] = (k > 1) ? ksp_dims[i] : 1;
+
+		if (nullptr != emaps_dims)
+			emaps_dims[i] = (k > 1) ? ksp_dims[i] : 1;
+	}
+
+	if (nullptr != sens_dims) {
+
+		sens_dims[3] = ksp_dims[3];
+		sens_dims[4] = conf->maps;
+	}
+
+	if (nullptr != emaps_dims)
+		emaps_dims[4] = conf->maps;
+
+	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
+			     void* sens, void* emaps, float* svals, long* nkernels, long caldims[3], void* stream)
+{
+	using namespace bn;
+
+	if (nullptr == conf || nullptr == ksp_dims || nullptr == ksp || nullptr == sens || N < 5)
+		return fail(BNUFFT_ERR_ARG, "ecalib: bad arguments");
+
+	if (conf->weighting || conf->intensity || conf->phase_normalize || conf->nystroem || !conf->orthiter || conf->crop < 0.f)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: soft-weighting, automatic (SURE) crop, intensity and phase "
+			    "normalisation, Nystroem and the full point-wise eigen-decomposition are not built");
+
+	if (1 != ksp_dims[4])
+		return fail(BNUFFT_ERR_ARG, "ecalib: MAPS dimension is not of size one");
+
+	for (int i = 5; i < N; i++)
+		if (1 != ksp_dims[i])
+			return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: one calibration at a time (dimension %d has size %ld)", i, ksp_dims[i]);
+
+	const long X = ksp_dims[0], Y = ksp_dims[1], Z = ksp_dims[2], C = ksp_dims[3];
+	const int M = conf->maps;
+
+	if (X < 1 || Y < 1 || Z < 1 || C < 1)
+		return fail(BNUFFT_ERR_ARG, "ecalib: bad k-space dimensions");
+
+	if (C > 32)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: %ld coils (at most 32 are built)", C);
+
+	if (M < 1 || M > C || M > 8)
+		return fail(BNUFFT_ERR_ARG, "ecalib: %d maps for %ld coils (1 <= maps <= min(coils, 8))", M, C);
+
+	long kd3[3], od[3];
+
+	for (int i = 0; i < 3; i++) {
+
+		kd3[i] = (1 == ksp_dims[i]) ? 1 : conf->kdims[i];
+
+		if (kd3[i] < 1 || conf->calsize[i] < 1)
+			return fail(BNUFFT_ERR_ARG, "ecalib: bad kernel or calibration size");
+
+		od[i] = (kd3[i] > 1) ? ksp_dims[i] : 1;
+
+		if (kd3[i] > 1 && ksp_dims[i] < 2 * kd3[i])
+			return fail(BNUFFT_ERR_ARG, "ecalib: image size %ld below twice the kernel size %ld", ksp_dims[i], kd3[i]);
+	}
+
+	cudaStream_t st = (cudaStream_t)stream;
+	EcBuf buf;
+	const long nksp = X * Y * Z * C;
+	const float2* dksp = (const float2*)ksp;
+
+	if (!on_device(ksp)) {
+
+		float2* t = nullptr;
+		TRY(buf.alloc(&t, (size_t)nksp));
+		CUDA_TRY(cudaMemcpyAsync(t, ksp, sizeof(float2) * nksp, cudaMemcpyHostToDevice, st));
+		dksp = t;
+	}
+
+	// 1. centre block (full readout) to the host, calibration region there
+	const long td[3] = { X, std::min(conf->calsize[1], Y), std::min(conf->calsize[2], Z) };
+	const long tp[3] = { 0, (Y - td[1]) / 2, (Z - td[2]) / 2 };
+	const long tn = td[0] * td[1] * td[2] * C;
+	float2* dtmp = nullptr;
+	TRY(buf.alloc(&dtmp, (size_t)tn));
+	k_ec_gather<<<ec_blocks(tn), 256, 0, st>>>(dksp, X, Y, Z, (int)C, (int)tp[0], (int)tp[1], (int)tp[2], (int)td[0], (int)td[1], (int)td[2], dtmp);
+	LAUNCHED();
+	std::vector<float2> htmp((size_t)tn);
+	CUDA_TRY(cudaMemcpyAsync(htmp.data(), dtmp, sizeof(float2) * tn, cudaMemcpyDeviceToHost, st));
+	CUDA_TRY(cudaStreamSynchronize(st));
+
+	long cal[3], cpos[3];
+	const long cs3[3] = { conf->calsize[0], conf->calsize[1], conf->calsize[2] };
+	ec_calib_geom(htmp, td, C, cs3, cal, cpos);
+
+	for (int i = 0; i < 3; i++) {
+
+		if (1 == cal[i] && 1 != ksp_dims[i])
+			return fail(BNUFFT_ERR_ARG, "ecalib: Calibration region not found!");
+
+		if (cal[i] < kd3[i])
+			return fail(BNUFFT_ERR_ARG, "ecalib: calibration region %ld smaller than the kernel %ld", cal[i], kd3[i]);
+	}
+
+	if (nullptr != caldims)
+		for (int i = 0; i < 3; i++)
+			caldims[i] = cal[i];
+
+	const long csize = cal[0] * cal[1] * cal[2];
+	float2* dcal = nullptr;
+	TRY(buf.alloc(&dcal, (size_t)(csize * C)));
+	k_ec_gather<<<ec_blocks(csize * C), 256, 0, st>>>(dksp, X, Y, Z, (int)C, (int)(tp[0] + cpos[0]), (int)(tp[1] + cpos[1]), (int)(tp[2] + cpos[2]),
+							 (int)cal[0], (int)cal[1], (int)cal[2], dcal);
+	LAUNCHED();
+
+	// 2. Casorati matrix and its Gram matrix G = A^H A (row-major)
+	const long kd = kd3[0] * kd3[1] * kd3[2];
+	const long Ncol = kd * C;
+	const long P = (cal[0] - kd3[0] + 1) * (cal[1] - kd3[1] + 1) * (cal[2] - kd3[2] + 1);
+
+	if (Ncol > 16384)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: calibration matrix with %ld columns", Ncol);
+
+	float2 *dA = nullptr, *dG = nullptr;
+	float* dw = nullptr;
+	TRY(buf.alloc(&dA, (size_t)(P * Ncol)));
+	TRY(buf.alloc(&dG, (size_t)(Ncol * Ncol)));
+	TRY(buf.alloc(&dw, (size_t)Ncol));
+	cudaEvent_t pe = prof_begin("ecalib_gram", st);
+	k_ec_casorati<<<ec_blocks(P * Ncol), 256, 0, st>>>(dcal, (int)cal[0], (int)cal[1], (int)cal[2], (int)kd3[0], (int)kd3[1], (int)kd3[2], (int)C, dA);
+	LAUNCHED();
+	TRY(ec_gemm(true, (int)Ncol, (int)Ncol, (int)P, dA, Ncol, dA, Ncol, dG, Ncol, st));
+	prof_end(pe, st);
+
+	// 3. eigen-decomposition (of conj(G), as LAPACK sees the reference's
+	// row-major array), kernels above the threshold
+	pe = prof_begin("ecalib_eig", st);
+	TRY(ec_heevd((int)Ncol, dG, dw, st));
+	prof_end(pe, st);
+	std::vector<float> w((size_t)Ncol);
+	CUDA_TRY(cudaMemcpyAsync(w.data(), dw, sizeof(float) * Ncol, cudaMemcpyDeviceToHost, st));
+	CUDA_TRY(cudaStreamSynchronize(st));
+
+	std::vector<float> val((size_t)Ncol);
+
+	for (long i = 0; i < Ncol; i++) {
+
+		const float e = w[(size_t)(Ncol - 1 - i)];
+		val[(size_t)i] = (e < 0.f) ? 0.f : sqrtf(e);
+	}
+
+	if (val[0] <= 0.f)
+		return fail(BNUFFT_ERR_ARG, "ecalib: No signal.");
+
+	long n = 0;
+
+	if (-1 != conf->numsv)
+		n = conf->numsv;
+	else if (-1.f != conf->percentsv)
+		n = (long)((float)Ncol * conf->percentsv / 100.f);
+	else
+		for (long i = 0; i < Ncol; i++)
+			if (val[(size_t)i] / val[0] > sqrtf(conf->threshold))
+				n++;
+
+	if (n < 1 || n > Ncol)
+		return fail(BNUFFT_ERR_ARG, "ecalib: %ld kernels selected (of %ld)", n, Ncol);
+
+	if (nullptr != svals)
+		for (long i = 0; i < Ncol; i++)
+			svals[i] = val[(size_t)i];
+
+	if (nullptr != nkernels)
+		*nkernels = n;
+
+	// 4. kernel images on the (2k)^d grid and their per-pixel Gram matrices
+	const long hd3[3] = { kd3[0] > 1 ? 2 * kd3[0] : 1, kd3[1] > 1 ? 2 * kd3[1] : 1, kd3[2] > 1 ? 2 * kd3[2] : 1 };
+	const long hd = hd3[0] * hd3[1] * hd3[2];
+	const long L = C * (C + 1) / 2;
+	float2 *dKT = nullptr, *dF = nullptr, *dKimg = nullptr, *dcov = nullptr;
+	TRY(buf.alloc(&dKT, (size_t)(kd * C * n)));
+	TRY(buf.alloc(&dF, (size_t)(hd * kd)));
+	TRY(buf.alloc(&dKimg, (size_t)(hd * C * n)));
+	TRY(buf.alloc(&dcov, (size_t)(hd * L)));
+	const std::vector<float2> F = ec_kernel_dft(kd3, hd3);
+	CUDA_TRY(cudaMemcpyAsync(dF, F.data(), sizeof(float2) * F.size(), cudaMemcpyHostToDevice, st));
+	pe = prof_begin("ecalib_imgcov", st);
+	k_ec_kern_perm<<<ec_blocks(kd * C * n), 256, 0, st>>>(dG, (int)Ncol, (int)kd, (int)C, (int)n, dKT);
+	LAUNCHED();
+	TRY(ec_gemm(false, (int)hd, (int)(C * n), (int)kd, dF, kd, dKT, C * n, dKimg, C * n, st));
+	const float scale = (float)(1. / ((double)kd * (double)hd));
+	k_ec_pixgram<<<(unsigned)hd, 256, 0, st>>>(dKimg, (int)C, (int)n, scale, dcov);
+	LAUNCHED();
+	prof_end(pe, st);
+
+	// 5. sinc interpolation along y and z to every image row
+	const std::vector<float2> Rx = ec_sinc_matrix(hd3[0], od[0]);
+	const std::vector<float2> Ry = ec_sinc_matrix(hd3[1], od[1]);
+	const std::vector<float2> Rz = ec_sinc_matrix(hd3[2], od[2]);
+	float2 *dRx = nullptr, *dRy = nullptr, *dRz = nullptr, *dT = nullptr, *drot = nullptr;
+	TRY(buf.alloc(&dRx, Rx.size()));
+	TRY(buf.alloc(&dRy, Ry.size()));
+	TRY(buf.alloc(&dRz, Rz.size()));
+	TRY(buf.alloc(&dT, (size_t)(od[1] * od[2] * hd3[0] * L)));
+	TRY(buf.alloc(&drot, (size_t)C));
+	CUDA_TRY(cudaMemcpyAsync(dRx, Rx.data(), sizeof(float2) * Rx.size(), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(dRy, Ry.data(), sizeof(float2) * Ry.size(), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(dRz, Rz.data(), sizeof(float2) * Rz.size(), cudaMemcpyHostToDevice, st));
+	pe = prof_begin("ecalib_interp", st);
+	k_ec_interp_yz<<<(unsigned)(od[1] * od[2]), 256, 0, st>>>(dcov, (int)hd3[0], (int)hd3[1], (int)hd3[2], (int)L, (int)od[1], dRy, dRz, dT);
+	prof_end(pe, st);
+	LAUNCHED();
+
+	// 6. phase reference: first principal coil component of the
+	// calibration data (src/calib/cc.c:45-62), last component real >= 0
+	std::vector<float2> rot((size_t)C, make_float2(0.f, 0.f));
+
+	if (conf->rotphase) {
+
+		float2* dGc = nullptr;
+		float* dwc = nullptr;
+		TRY(buf.alloc(&dGc, (size_t)(C * C)));
+		TRY(buf.alloc(&dwc, (size_t)C));
+		k_ec_coilcov<<<(unsigned)(C * C), 256, 0, st>>>(dcal, csize, (int)C, dGc);
+		LAUNCHED();
+		TRY(ec_heevd((int)C, dGc, dwc, st));
+		CUDA_TRY(cudaMemcpyAsync(rot.data(), dGc + (C - 1) * C, sizeof(float2) * C, cudaMemcpyDeviceToHost, st));
+		CUDA_TRY(cudaStreamSynchronize(st));
+		const std::complex<double> last(rot[(size_t)(C - 1)].x, rot[(size_t)(C - 1)].y);
+
+		if (std::abs(last) > 0.) {
+
+			const std::complex<double> f = std::conj(last) / std::abs(last);
+
+			for (long c = 0; c < C; c++) {
+
+				const std::complex<double> r = std::complex<double>(rot[(size_t)c].x, rot[(size_t)c].y) * f;
+				rot[(size_t)c] = make_float2((float)r.real(), (float)r.imag());
+			}
+		}
+
+	} else {
+
+		rot[0] = make_float2(1.f, 0.f);
+	}
+
+	CUDA_TRY(cudaMemcpyAsync(drot, rot.data(), sizeof(float2) * C, cudaMemcpyHostToDevice, st));
+
+	// 7. the fused per-pixel pass
+	const long npix = od[0] * od[1] * od[2];
+	const bool sdev = on_device(sens), edev = (nullptr == emaps) || on_device(emaps);
+	float2* dsens = (float2*)sens;
+	float2* dev_ev = (float2*)emaps;
+
+	if (!sdev)
+		TRY(buf.alloc(&dsens, (size_t)(npix * C * M)));
+
+	if (!edev)
+		TRY(buf.alloc(&dev_ev, (size_t)(npix * M)));
+
+	const int W = (C <= 8) ? 8 : (C <= 16) ? 16 : 32;
+	auto go = [&](auto w) -> int {
+		return ec_launch_eigen<decltype(w)::value>((int)od[0], (int)od[1], (int)od[2], (int)C, M, (int)hd3[0], (int)L, dT, dRx, drot,
+							   conf->num_orthiter, conf->crop, conf->softcrop, dsens, dev_ev, st);
+	};
+
+	if (8 == W)
+		TRY(go(std::integral_constant<int, 8>()));
+	else if (16 == W)
+		TRY(go(std::integral_constant<int, 16>()));
+	else
+		TRY(go(std::integral_constant<int, 32>()));
+
+	if (!sdev)
+		CUDA_TRY(cudaMemcpyAsync(sens, dsens, sizeof(float2) * npix * C * M, cudaMemcpyDeviceToHost, st));
+
+	if (!edev)
+		CUDA_TRY(cudaMemcpyAsync(emaps, dev_ev, sizeof(float2) * npix * M, cudaMemcpyDeviceToHost, st));
+
+	// the temporaries are freed when this returns: finish the work first
+	CUDA_TRY(cudaStreamSynchronize(st));
+	return BNUFFT_OK;
+}

@@ -130,3 +130,27 @@ def random_image(n: int, rng: np.random.Generator, ndim: int = 2) -> np.ndarray:
     """i.i.d. standard complex Gaussian image (the NUFFT benchmark input)."""
     shape = (n,) * ndim + (1,) * (3 - ndim)
     return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+def cartesian_ksp(img: np.ndarray, sens: np.ndarray, rng: np.random.Generator, snr_db: float = 40.0,
+                  calib: int = 24, accel: int = 2) -> np.ndarray:
+    """Cartesian multi-coil k-space ``[X, Y, Z, C]`` of ``img * sens``: the
+    centred DFT (DC at n/2) of every coil image, complex Gaussian noise, a
+    fully sampled centre of ``calib`` lines along every phase-encoding
+    dimension (1 and 2) and every ``accel``-th line outside it; the readout
+    (dimension 0) is fully sampled. The input of ``bart ecalib``."""
+    X, Y, Z, C = sens.shape
+    cim = img.reshape(X, Y, Z, 1) * sens
+    axes = tuple(a for a, n in enumerate((X, Y, Z)) if n > 1)
+    k = np.fft.fftshift(np.fft.fftn(np.fft.ifftshift(cim, axes=axes), axes=axes, norm="ortho"), axes=axes)
+    k = add_noise(k, snr_db, rng)
+    mask = np.ones((X, Y, Z), dtype=bool)
+    for a, n in ((1, Y), (2, Z)):
+        if n == 1:
+            continue
+        idx = np.arange(n)
+        keep = (np.abs(idx - n // 2) < calib // 2 + (idx >= n // 2) * (calib % 2)) | (idx % accel == 0)
+        shape = [1, 1, 1]
+        shape[a] = n
+        mask &= keep.reshape(shape)
+    return (k * mask[..., None]).astype(np.complex64)

@@ -267,6 +267,87 @@ def run_normal3d(dev, steps, warmup, coils=8, N=128, spokes=2000):
             "hbm_peak_gbs": peak, "peak_source": peak_src, "passes": passes}
 
 
+def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True):
+    """ESPIRiT calibration with the reference's ecalib defaults (6 x 6
+    kernel, calibration region up to 24 x 24, threshold 0.001, 2 maps, 30
+    orthogonal iterations, crop 0.8) of 2D Cartesian k-space: N x N, `coils`
+    coils, ellipse phantom, polynomial maps, 40 dB noise, 24 fully sampled
+    centre lines and every other line outside. One step = one calibration
+    from device k-space to device maps (value); e2e = from host k-space to
+    host maps and eigenvalue maps. Per-stage device times by CUDA events;
+    the per-pixel pass against the FP32 FMA peak (its arithmetic: the C x C
+    matrix from 12 x-interpolation terms per entry, then 30 x maps x C^2
+    complex multiply-adds of the orthogonal iteration). cpu_baseline: the
+    reference's ecalib built from its sources, whole command with .cfl
+    I/O, all host cores."""
+    import ctypes
+    import torch
+    from bart_b200 import _lib, synth
+    from bart_b200.espirit import ecalib
+    rng = np.random.default_rng(11)
+    img = synth.ellipse_phantom(N, 20, rng)
+    k = synth.cartesian_ksp(img, synth.coil_maps(N, coils, rng), rng, 40.0, 24, 2)
+    dims = list(k.shape)
+    kt = torch.from_numpy(np.asfortranarray(k).ravel(order="F").copy()).to(dev)
+    lib = _lib.load()
+    for _ in range(max(3, warmup)):
+        ecalib(kt, dims=dims)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = lib.bnufft_launch_count()
+    with ClockSampler(dev.index or 0) as clk:
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            sens, ev, info = ecalib(kt, dims=dims)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    launches = int(lib.bnufft_launch_count() - n0)
+    stages = {}
+    for kind in ("ecalib_gram", "ecalib_eig", "ecalib_imgcov", "ecalib_interp", "ecalib_pixels"):
+        lib.bnufft_prof_start(kind.encode())
+        ecalib(kt, dims=dims)
+        kms, kn = ctypes.c_double(), ctypes.c_long()
+        lib.bnufft_prof_stop(ctypes.byref(kms), ctypes.byref(kn))
+        stages[kind] = {"ms": kms.value, "launches": kn.value}
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ecalib(k)
+    e2e_s = (time.perf_counter() - t0) / steps
+    M, C, xh, it = 2, coils, 12, 30
+    flop = N * N * (C * C * xh + it * M * C * C) * 8.0
+    px_ms = stages["ecalib_pixels"]["ms"]
+    out_bytes = N * N * (C * M + M) * 8
+    t_bytes = N * xh * (C * (C + 1) // 2) * 8
+    res = {"workload": f"ecalib2d_{N}_c{coils}", "metric": "ESPIRiT calibrations/s", "unit": "calibrations/s",
+           "value": 1e3 / ms, "ms_per_calibration": ms, "gpu_launches": launches // steps,
+           "nkernels": info["nkernels"], "caldims": list(info["caldims"]),
+           "e2e": {"value": 1.0 / e2e_s, "unit": "calibrations/s", "h2d_bytes_per_step": int(k.nbytes),
+                   "d2h_bytes_per_step": int(N * N * (C * M + M) * 8)},
+           "stages": stages,
+           "pixels_kernel": {"flop": flop, "tflops": flop / (px_ms * 1e-3) / 1e12 if px_ms > 0 else None,
+                             "fp32_peak_tflops": FP32_PEAK_TFLOPS,
+                             "fp32_frac": flop / (px_ms * 1e-3) / 1e12 / FP32_PEAK_TFLOPS if px_ms > 0 else None,
+                             "hbm_bytes": out_bytes + t_bytes},
+           "clocks": clk.summary()}
+    exe = os.path.join(ROOT, "oracle", "_ref", "bin", "ecalib")
+    if cpu_base and os.path.exists(exe):
+        from bart_b200.cfl import writecfl
+        env = dict(os.environ)
+        env["OMP_NUM_THREADS"] = str(os.cpu_count())
+        with tempfile.TemporaryDirectory() as d:
+            writecfl(os.path.join(d, "k"), k)
+            t0 = time.perf_counter()
+            r = subprocess.run([exe, "k", "s", "e"], cwd=d, env=env, capture_output=True, text=True)
+            dt = time.perf_counter() - t0
+        if r.returncode == 0:
+            res["cpu_baseline"] = {"value": 1.0 / dt, "unit": "calibrations/s", "cores": os.cpu_count(),
+                                   "kind": "reference", "sample": "1 calibration with the reference's CPU ecalib "
+                                   "(OpenMP, MKL eigen-decomposition), wall incl. .cfl I/O"}
+    return res
+
+
 def run_nufft3d(dev, steps, warmup, spokes=20000):
     """3D radial kooshball NUFFT: 128^3 image, 8 coils,
     20000 spokes x 256 samples on 3D golden means (5.12 M samples per coil).
@@ -831,8 +912,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "normal3d", "batch", "scatter"])
-    ap.add_argument("--coils", type=int, default=8, help="normal3d: coils")
+    ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "normal3d", "batch", "scatter", "ecalib"])
+    ap.add_argument("--coils", type=int, default=None, help="normal3d (default 8) / ecalib (default 16): coils")
     ap.add_argument("--analysis", action="store_true",
                     help="batch: also the solves spread over streams and timed alone per embedding size")
     ap.add_argument("--spokes", type=int, default=20000, help="nufft3d: kooshball spokes")
@@ -873,7 +954,13 @@ def main():
 
     if args.workload == "normal3d":
         if rank == 0:
-            print(json.dumps(run_normal3d(dev, args.steps, args.warmup, args.coils)), flush=True)
+            print(json.dumps(run_normal3d(dev, args.steps, args.warmup, args.coils or 8)), flush=True)
+        return
+
+    if args.workload == "ecalib":
+        if rank == 0:
+            print(json.dumps(run_ecalib(dev, args.steps, args.warmup, coils=args.coils or 16,
+                                        cpu_base=not args.no_cpu_baseline)), flush=True)
         return
 
     if args.workload == "scatter":

@@ -1,0 +1,76 @@
+/* bespirit: ESPIRiT calibration of coil sensitivities (bart ecalib) on the
+ * GPU, C ABI. Part of libbnufft; statuses and bnufft_last_error() as in
+ * bnufft.h.
+ *
+ * Replaces the reference's calibration entry points (mrirecon/bart
+ * v1.0.00): extract_calib (src/misc/mri2.c:220-225) followed by calib
+ * (src/calib/calib.c:797-800, declared in src/calib/calib.h), as main_ecalib
+ * calls them (src/ecalib.c:150-253).
+ */
+#ifndef BESPIRIT_H
+#define BESPIRIT_H
+
+#include "bnufft.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* struct ecalib_conf (src/calib/calib.h) with the options of main_ecalib
+ * (src/ecalib.c:64-97). Defaults as ecalib_defaults
+ * (src/calib/calib.c:693-714) and main_ecalib: kdims 6x6x6 (-k), calsize
+ * 24x24x24 (-r), maps 2 (-m), threshold 0.001 (-t), numsv -1 (-n),
+ * percentsv -1 (-p), crop 0.8 (-c), softcrop 0 (-S), rotphase 1 (-P clears
+ * it), orthiter 1 with num_orthiter 30. The remaining switches (weighting
+ * -W, automatic -a / a negative crop (SURE), intensity -I, phase_normalize
+ * -N, nystroem -A, orthiter 0) are not built: a call that sets one returns
+ * BNUFFT_ERR_UNSUPPORTED. */
+struct bnufft_ecalib_conf {
+
+	long kdims[3];
+	long calsize[3];
+	int maps;
+	float threshold;
+	int numsv;
+	float percentsv;
+	float crop;
+	int softcrop;
+	int rotphase;
+	int orthiter;
+	int num_orthiter;
+	int weighting;
+	int intensity;
+	int phase_normalize;
+	int nystroem;
+};
+
+void bnufft_ecalib_defaults(struct bnufft_ecalib_conf* conf);
+
+/* Output dimensions for k-space ksp_dims[N] (N >= 5): sens [X, Y, Z, C,
+ * maps], emaps [X, Y, Z, 1, maps], where a spatial dimension is 1 if the
+ * k-space (hence the kernel) has size 1 there (src/ecalib.c:210-225). */
+int bnufft_ecalib_dims(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], long sens_dims[], long emaps_dims[]);
+
+/* ESPIRiT maps of Cartesian k-space ksp (dims[N], N >= 5, [X, Y, Z, C] with
+ * dims 4.. of size 1; C <= 32): the calibration region is the largest fully
+ * sampled centred block up to calsize, moved along the readout to its
+ * largest energy. sens (and emaps, if not NULL) receive the maps and their
+ * eigenvalues in the layout of bnufft_ecalib_dims. svals (host, if not
+ * NULL) receives the kx*ky*kz*C singular values of the calibration matrix
+ * in descending order, nkernels (if not NULL) the number of kernels kept,
+ * caldims (if not NULL) the calibration region's size. ksp, sens and emaps
+ * may be host or device memory. The call returns when the results are
+ * written. Same results as the reference's ecalib up to float rounding;
+ * the maps' global sign follows the convention that the first principal
+ * coil component's last entry is real and positive (the reference takes
+ * that sign from its LAPACK). The calibration matrix's eigen-decomposition
+ * runs in cuSOLVER (loaded on first use); everything else in the library's
+ * own kernels. */
+int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
+		  void* sens, void* emaps, float* svals, long* nkernels, long caldims[3], void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -11,5 +11,6 @@ STUB(lapack_schur_double)
 STUB(lapack_solve_real)
 STUB(lapack_svd)
 STUB(lapack_svd_econ)
+STUB(lapack_qr_econ)
 STUB(lapack_sylvester)
 STUB(lapack_trimat_solve)

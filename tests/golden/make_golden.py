@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures from the reference's own CPU tools.
 
 Runs the mrirecon/bart v1.0.00 tools built by ``oracle/refbuild/Makefile``
-(``oracle/_ref/bin``: nufft, pics, traj and the refnormal checker) on
+(``oracle/_ref/bin``: nufft, pics, traj, ecalib and the refnormal checker) on
 seeded synthetic inputs and stores inputs and outputs as compressed .npz
 files next to this script. Only needed when the fixtures change; the tests
 read the .npz files and never run the reference.
@@ -16,6 +16,7 @@ read the .npz files and never run the reference.
     python tests/golden/make_golden.py --basis         # subspace basis (nufft / pics -B)
     python tests/golden/make_golden.py --chain         # oversampling other than 2 (nufft -o)
     python tests/golden/make_golden.py --stream        # a k-space stream (copy --stream | tee -b)
+    python tests/golden/make_golden.py --ecalib        # ESPIRiT calibration (ecalib)
 """
 
 from __future__ import annotations
@@ -438,7 +439,56 @@ def basis_cases():
     basis_pics_case("pics2d_n32_basis", tf, ksp, sens.astype(np.complex64), basis, pat2)
 
 
+def ecalib_case(name, ksp, args):
+    """The reference's ecalib (with -V: singular values) on Cartesian
+    k-space; stores the inputs, the maps, the eigenvalue maps, the singular
+    values, the number of kernels and the calibration region (its debug
+    output)."""
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "k"), ksp)
+        r = subprocess.run([os.path.join(BIN, "ecalib"), "-d4", "-V"] + args + ["k", "s", "e"], cwd=d,
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(r.stderr)
+        sens, ev = readcfl(os.path.join(d, "s")), readcfl(os.path.join(d, "e"))
+    svals = np.array([float(ln.split()[2]) for ln in r.stdout.splitlines() if ln.startswith("SVALS ")],
+                     dtype=np.float32)
+    nk = cd = None
+    for ln in r.stderr.splitlines():
+        if ln.startswith("Using "):
+            nk = int(ln.split()[1].split("/")[0])
+        if ln.startswith("Calibration region"):
+            cd = [int(v) for v in ln.split("size: ")[1].split(",")[0].split("x")]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), ksp=ksp, sens=sens, emaps=ev, svals=svals,
+                        nkernels=np.int64(nk), caldims=np.array(cd), args=np.array(args))
+    print(name, ksp.shape, sens.shape, "kernels", nk, "caldims", cd)
+
+
+def ecalib_cases():
+    """Cartesian k-space of ellipse phantoms and polynomial coil maps, 40 dB
+    noise, a fully sampled centre and every other line outside it."""
+    rng = np.random.default_rng(9001)
+    N, C = 64, 8
+    img = synth.ellipse_phantom(N, 12, rng)
+    k = synth.cartesian_ksp(img, synth.coil_maps(N, C, rng), rng, 40.0, 24, 2)
+    ecalib_case("ecalib2d_n64_c8", k, [])
+    ecalib_case("ecalib2d_n64_c8_m3_soft", k, ["-m", "3", "-c", "0.1", "-S"])
+    ecalib_case("ecalib2d_n64_c8_k5_r20_n30_P", k, ["-k", "5", "-r", "20", "-n", "30", "-P", "-c", "0.3"])
+    X, Y, C = 40, 48, 20
+    img = synth.ellipse_phantom(48, 10, rng)[4:44, :, :]
+    maps = synth.coil_maps(48, C, rng)[4:44]
+    k = synth.cartesian_ksp(img, maps, rng, 40.0, 20, 3)
+    ecalib_case("ecalib2d_40x48_c20", k, ["-r", "20", "-c", "0.5"])
+    N, C = 24, 4
+    img = synth.ellipse_phantom(N, 6, rng, ndim=3)
+    k = synth.cartesian_ksp(img, synth.coil_maps(N, C, rng, ndim=3), rng, 40.0, 12, 2)
+    ecalib_case("ecalib3d_n24_c4", k, ["-r", "12", "-k", "4", "-c", "0.4"])
+
+
 def main():
+    if "--ecalib" in sys.argv:
+        ecalib_cases()
+        return
     if "--basis" in sys.argv:
         basis_cases()
         return
@@ -485,6 +535,7 @@ def main():
     fullsize_cases()
     gpu_gridding_case()
     kooshball_case()
+    ecalib_cases()
 
 
 if __name__ == "__main__":

@@ -1,4 +1,4 @@
-"""The C-ABI library loads and exports every entry point include/bnufft.h declares.
+"""The C-ABI library loads and exports every entry point include/*.h declares.
 
 Runs without a GPU: no compute call is made, except argument checks that
 fail before touching the device.
@@ -14,7 +14,8 @@ from conftest import ROOT
 
 
 def declared_symbols():
-    src = open(os.path.join(ROOT, "include", "bnufft.h")).read()
+    inc = os.path.join(ROOT, "include")
+    src = "".join(open(os.path.join(inc, f)).read() for f in sorted(os.listdir(inc)) if f.endswith(".h"))
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(bnufft_\w+)\s*\(", src)))
 
@@ -22,7 +23,8 @@ def declared_symbols():
 def test_header_declares_entry_points():
     syms = declared_symbols()
     for s in ["bnufft_create2", "bnufft_apply_forward", "bnufft_apply_adjoint", "bnufft_apply_normal",
-              "bnufft_pics_create", "bnufft_pics_run", "bnufft_free", "bnufft_last_error"]:
+              "bnufft_pics_create", "bnufft_pics_run", "bnufft_free", "bnufft_last_error", "bnufft_ecalib",
+              "bnufft_ecalib_dims", "bnufft_ecalib_defaults"]:
         assert s in syms
 
 
@@ -46,6 +48,21 @@ def test_argument_errors_without_device():
     assert "trajectory" in lib.bnufft_last_error().decode()
     with pytest.raises(_lib.BnufftError):
         _lib.check(st)
+
+
+def test_ecalib_host_side_without_device():
+    """The ESPIRiT defaults and output dimensions are host-only calls; bad
+    arguments come back as status codes."""
+    from bart_b200.espirit import EcalibConf, output_dims
+    sd, ed = output_dims([64, 48, 1, 8], EcalibConf(maps=3))
+    assert sd[:5] == [64, 48, 1, 8, 3] and ed[:5] == [64, 48, 1, 1, 3]
+    sd, ed = output_dims([1, 48, 40, 4])
+    assert sd[:5] == [1, 48, 40, 4, 2]
+    from bart_b200 import _lib
+    lib = _lib.load()
+    c = EcalibConf().to_c()
+    assert lib.bnufft_ecalib(ctypes.byref(c), 16, _lib.dims_array([8] * 16), None, None, None, None, None, None,
+                             None) == 1
 
 
 def test_kb_table_bitwise_library():

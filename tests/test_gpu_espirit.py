@@ -1,0 +1,115 @@
+"""ESPIRiT calibration on the GPU (include/bespirit.h) against the
+reference's ecalib outputs and against the oracle at larger sizes."""
+
+import numpy as np
+import pytest
+
+from conftest import golden, rel
+from test_espirit_oracle import CASES, ecalib_kwargs, map_error
+
+pytestmark = pytest.mark.gpu
+
+
+def conf_of(kw):
+    from bart_b200.espirit import EcalibConf
+    return EcalibConf(**kw)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_ecalib_vs_reference(cuda, name):
+    """Maps, eigenvalue maps, kept singular values, kernel count and
+    calibration region equal the reference's (maps up to its LAPACK sign).
+    The bars: the principal map and all eigenvalue maps to 1e-4; lower maps,
+    which 30 orthogonal iterations leave unconverged and which follow the
+    float rounding of the covariance more closely, to 1e-3."""
+    from bart_b200.espirit import ecalib
+    g = golden(name)
+    kw = ecalib_kwargs(g["args"])
+    sens, ev, info = ecalib(g["ksp"], conf_of(kw))
+    assert info["nkernels"] == int(g["nkernels"])
+    assert list(info["caldims"]) == list(g["caldims"])
+    n = info["nkernels"]
+    assert rel(info["svals"][:n], g["svals"][:n]) < 1e-4
+    rs = g["sens"].reshape(sens.shape, order="F")
+    re = g["emaps"].reshape(ev.shape, order="F")
+    for m in range(sens.shape[4]):
+        assert rel(ev[..., m], re[..., m]) < 1e-4, (m, rel(ev[..., m], re[..., m]))
+        err = map_error(sens[..., m], rs[..., m])
+        assert err < (1e-4 if m == 0 else 1e-3), (m, err)
+
+
+@pytest.mark.parametrize("N,C,ndim,extra", [(96, 32, 2, {}), (128, 16, 2, {"maps": 3, "crop": 0.3}),
+                                            (32, 8, 3, {"calsize": (16, 16, 16), "kdims": (5, 5, 5)})])
+def test_ecalib_vs_oracle(cuda, N, C, ndim, extra):
+    """16- and 32-lane pixel groups (16 and 32 coils) and a 3D case against
+    the float64 oracle."""
+    from bart_b200 import synth
+    from bart_b200.espirit import ecalib
+    from oracle import espirit_oracle as eo
+    rng = np.random.default_rng(N + C + ndim)
+    img = synth.ellipse_phantom(N, 12, rng, ndim=ndim)
+    k = synth.cartesian_ksp(img, synth.coil_maps(N, C, rng, ndim=ndim), rng, 40.0, 24 if ndim == 2 else 16, 2)
+    sens, ev, info = ecalib(k, conf_of(extra))
+    s, e, val, n, cd = eo.ecalib(k, **extra)
+    assert info["nkernels"] == n and tuple(info["caldims"]) == tuple(cd)
+    sens = sens.reshape(s.shape, order="F")
+    ev = ev.reshape(e.shape, order="F")
+    for m in range(s.shape[-1]):
+        assert rel(ev[..., m], e[..., m]) < 1e-4, (m, rel(ev[..., m], e[..., m]))
+        err = map_error(sens[..., m], s[..., m])
+        assert err < (1e-4 if m == 0 else 2e-3), (m, err)
+
+
+def test_ecalib_device_tensors_equal_host_arrays(cuda):
+    """k-space and maps in device memory (a torch tensor and its dims) give
+    the same bits as host arrays."""
+    import torch
+    from bart_b200.espirit import ecalib
+    g = golden("ecalib2d_n64_c8")
+    k = g["ksp"]
+    s_host, e_host, _ = ecalib(k)
+    kt = torch.from_numpy(np.asfortranarray(k).ravel(order="F").copy()).to(cuda)
+    s_dev, e_dev, info = ecalib(kt, dims=list(k.shape))
+    torch.cuda.synchronize()
+    assert np.array_equal(s_dev.cpu().numpy(), s_host.ravel(order="F"))
+    assert np.array_equal(e_dev.cpu().numpy(), e_host.ravel(order="F"))
+
+
+def test_ecalib_cli(cuda, tmp_path):
+    """python -m bart_b200 ecalib -m 3 -c 0.1 -S ksp sens emaps writes what
+    the reference's ecalib writes."""
+    from bart_b200 import __main__ as cli
+    from bart_b200.cfl import readcfl, writecfl
+    g = golden("ecalib2d_n64_c8_m3_soft")
+    d = str(tmp_path)
+    writecfl(d + "/k", g["ksp"])
+    assert 0 == cli.main(["ecalib"] + [str(a) for a in g["args"]] + [d + "/k", d + "/s", d + "/e"])
+    s, e = readcfl(d + "/s"), readcfl(d + "/e")
+    assert s.shape == g["sens"].shape and e.shape == g["emaps"].shape
+    first = (slice(None),) * 4 + (0,)
+    assert map_error(s[first], g["sens"][first]) < 1e-4
+    assert rel(e, g["emaps"]) < 1e-4
+
+
+def test_ecalib_errors(cuda):
+    """Options that are not built and invalid inputs return their status
+    without touching the outputs' contents beyond the call."""
+    from bart_b200._lib import BnufftError
+    from bart_b200.espirit import EcalibConf, ecalib
+    g = golden("ecalib2d_n64_c8")
+    k = g["ksp"]
+    for bad in (dict(weighting=True), dict(intensity=True), dict(crop=-1.0), dict(orthiter=False)):
+        with pytest.raises(BnufftError) as e:
+            ecalib(k, EcalibConf(**bad))
+        assert e.value.status == 2
+    with pytest.raises(BnufftError) as e:		# 33 coils
+        ecalib(np.concatenate([k, k[..., :25]], axis=3))
+    assert e.value.status == 2
+    with pytest.raises(BnufftError) as e:		# no fully sampled centre
+        z = k.copy()
+        z[:, 32] = 0
+        ecalib(z)
+    assert e.value.status == 1
+    with pytest.raises(BnufftError) as e:		# more maps than coils
+        ecalib(k[..., :2], EcalibConf(maps=3))
+    assert e.value.status == 1
