@@ -12,6 +12,10 @@
 //   -> one fused pass per image pixel: sinc interpolation along x, the
 //      orthogonal iteration, eigenvalue crop and phase alignment, written
 //      straight to the maps [X, Y, Z, C, maps].
+// The covariance is accumulated and interpolated in float64 (it is small
+// and the result of cancellation away from the object); the GEMMs, the
+// eigen-decomposition and the orthogonal iteration run in float32, as the
+// reference's do.
 //
 // This file is included into bnufft.cu and uses its error and launch
 // helpers (fail, CUDA_TRY, LAUNCHED, TRY, on_device).
@@ -176,7 +180,7 @@ __global__ void k_ec_kern_perm(const float2* __restrict__ E, int Ncol, int kd, i
 // low-resolution pixel: cov[x][l(a, b)] = sum_i conj(K[x][a n + i])
 // K[x][b n + i] * scale, l(a, b) = a (a + 1) / 2 + b, b <= a
 // (src/calib/calib.c:1072-1088, src/num/linalg.c:642-664, 1211-1232).
-__global__ void k_ec_pixgram(const float2* __restrict__ Kimg, int C, int n, float scale, float2* __restrict__ cov)
+__global__ void k_ec_pixgram(const float2* __restrict__ Kimg, int C, int n, double scale, double2* __restrict__ cov)
 {
 	const int x = blockIdx.x;
 	const int L = C * (C + 1) / 2;
@@ -195,24 +199,27 @@ __global__ void k_ec_pixgram(const float2* __restrict__ Kimg, int C, int n, floa
 		const int b = l - a * (a + 1) / 2;
 		const float2* ka = K + (long)a * n;
 		const float2* kb = K + (long)b * n;
-		float sr = 0.f, si = 0.f;
+		double sr = 0., si = 0.;
 
 		for (int i = 0; i < n; i++) {
 
 			const float2 p = ka[i], q = kb[i];	// conj(p) q
-			sr = fmaf(p.x, q.x, fmaf(p.y, q.y, sr));
-			si = fmaf(p.x, q.y, fmaf(-p.y, q.x, si));
+			sr = fma((double)p.x, (double)q.x, fma((double)p.y, (double)q.y, sr));
+			si = fma((double)p.x, (double)q.y, fma(-(double)p.y, (double)q.x, si));
 		}
 
-		cov[(long)x * L + l] = make_float2(sr * scale, si * scale);
+		cov[(long)x * L + l] = make_double2(sr * scale, si * scale);
 	}
 }
 
 // sinc interpolation along y and z (the reference's sinc_zeropad,
 // src/misc/resize.c:234-292, written as its per-axis linear maps):
 // T[(z Y + y)][u][l] = sum_{v, w} Ry[y][v] Rz[z][w] cov[(w yh + v) xh + u][l].
-__global__ void k_ec_interp_yz(const float2* __restrict__ cov, int xh, int yh, int zh, int L, int Y,
-			       const float2* __restrict__ Ry, const float2* __restrict__ Rz, float2* __restrict__ T)
+// In float64: away from the object the interpolated covariance is a small
+// difference of order-one terms, and its relative error there sets the
+// accuracy of the maps wherever the eigenvalues lie close together.
+__global__ void k_ec_interp_yz(const double2* __restrict__ cov, int xh, int yh, int zh, int L, int Y,
+			       const double2* __restrict__ Ry, const double2* __restrict__ Rz, double2* __restrict__ T)
 {
 	const int row = blockIdx.x;
 	const int y = row % Y, z = row / Y;
@@ -221,18 +228,19 @@ __global__ void k_ec_interp_yz(const float2* __restrict__ cov, int xh, int yh, i
 	for (int t = threadIdx.x; t < n; t += blockDim.x) {
 
 		const int u = t / L, l = t % L;
-		float2 s = make_float2(0.f, 0.f);
+		double2 s = make_double2(0., 0.);
 
 		for (int w = 0; w < zh; w++) {
 
-			const float2 rz = Rz[(long)z * zh + w];
+			const double2 rz = Rz[(long)z * zh + w];
 
 			for (int v = 0; v < yh; v++) {
 
-				const float2 r = ec_cmul(Ry[(long)y * yh + v], rz);
-				const float2 c = cov[((long)(w * yh + v) * xh + u) * L + l];
-				s.x = fmaf(r.x, c.x, fmaf(-r.y, c.y, s.x));
-				s.y = fmaf(r.x, c.y, fmaf(r.y, c.x, s.y));
+				const double2 ry = Ry[(long)y * yh + v];
+				const double2 r = make_double2(ry.x * rz.x - ry.y * rz.y, ry.x * rz.y + ry.y * rz.x);
+				const double2 c = cov[((long)(w * yh + v) * xh + u) * L + l];
+				s.x = fma(r.x, c.x, fma(-r.y, c.y, s.x));
+				s.y = fma(r.x, c.y, fma(r.y, c.x, s.y));
 			}
 		}
 
@@ -268,21 +276,21 @@ __device__ __forceinline__ float ec_group_sum(float v)
 //   5. staged through shared memory and written coalesced along x.
 template <int W, int MMAX>
 __global__ void __launch_bounds__(256) k_ec_eigen(int X, int Y, int Z, int C, int M, int xh, int L,
-						  const float2* __restrict__ T, const float2* __restrict__ Rx,
+						  const double2* __restrict__ T, const double2* __restrict__ Rx,
 						  const float2* __restrict__ rot, int iters, float crop, int soft,
 						  float2* __restrict__ sens, float2* __restrict__ ev)
 {
 	constexpr int PX = 8 * 32 / W;
-	extern __shared__ float2 ec_smem[];
-	float2* sT = ec_smem;				// [xh][L]
-	float2* sR = sT + (long)xh * L;			// [PX][xh]
-	float2* sO = sR + PX * xh;			// [PX][M][C]
+	extern __shared__ double2 ec_smem[];
+	double2* sT = ec_smem;				// [xh][L]
+	double2* sR = sT + (long)xh * L;		// [PX][xh]
+	float2* sO = (float2*)(sR + PX * xh);		// [PX][M][C]
 	float* sE = (float*)(sO + PX * M * C);		// [PX][M]
 
 	const int row = blockIdx.x;
 	const int y = row % Y, z = row / Y;
 	const int x0 = blockIdx.y * PX;
-	const float2* Trow = T + (long)row * xh * L;
+	const double2* Trow = T + (long)row * xh * L;
 
 	for (int t = threadIdx.x; t < xh * L; t += blockDim.x)
 		sT[t] = Trow[t];
@@ -290,7 +298,7 @@ __global__ void __launch_bounds__(256) k_ec_eigen(int X, int Y, int Z, int C, in
 	for (int t = threadIdx.x; t < PX * xh; t += blockDim.x) {
 
 		const int px = t / xh, u = t % xh;
-		sR[t] = (x0 + px < X) ? Rx[(long)(x0 + px) * xh + u] : make_float2(0.f, 0.f);
+		sR[t] = (x0 + px < X) ? Rx[(long)(x0 + px) * xh + u] : make_double2(0., 0.);
 	}
 
 	__syncthreads();
@@ -299,14 +307,14 @@ __global__ void __launch_bounds__(256) k_ec_eigen(int X, int Y, int Z, int C, in
 	const int c = lane % W;
 	const int px = (threadIdx.x / 32) * (32 / W) + lane / W;
 	const bool act = c < C;
-	const float2* rx = sR + px * xh;
+	const double2* rx = sR + px * xh;
 
 	float2 Hc[W];
 
 #pragma unroll
 	for (int k = 0; k < W; k++) {
 
-		float2 s = make_float2(0.f, 0.f);
+		double2 s = make_double2(0., 0.);
 
 		if (act && k < C) {
 
@@ -315,16 +323,16 @@ __global__ void __launch_bounds__(256) k_ec_eigen(int X, int Y, int Z, int C, in
 
 			for (int u = 0; u < xh; u++) {
 
-				const float2 r = rx[u], v = sT[u * L + l];
-				s.x = fmaf(r.x, v.x, fmaf(-r.y, v.y, s.x));
-				s.y = fmaf(r.x, v.y, fmaf(r.y, v.x, s.y));
+				const double2 r = rx[u], v = sT[u * L + l];
+				s.x = fma(r.x, v.x, fma(-r.y, v.y, s.x));
+				s.y = fma(r.x, v.y, fma(r.y, v.x, s.y));
 			}
 
 			if (!lo)
 				s.y = -s.y;
 		}
 
-		Hc[k] = s;
+		Hc[k] = make_float2((float)s.x, (float)s.y);
 	}
 
 	float2 v[MMAX];
@@ -546,6 +554,49 @@ static int ec_solver(const EcSolver** out)
 	return BNUFFT_OK;
 }
 
+// the calibration's own stream-ordered memory pool per device: no
+// device-wide synchronisation per allocation, and (release threshold
+// unlimited) the memory stays mapped for the next calibration instead of
+// going back to the system at every synchronisation
+static cudaMemPool_t ec_pool()
+{
+	static std::mutex mu;
+	static std::map<int, cudaMemPool_t> pools;
+	std::lock_guard<std::mutex> lock(mu);
+	int dev = 0;
+
+	if (cudaSuccess != cudaGetDevice(&dev))
+		return nullptr;
+
+	cudaMemPool_t& p = pools[dev];
+
+	if (nullptr == p) {
+
+		cudaMemPoolProps props = {};
+		props.allocType = cudaMemAllocationTypePinned;
+		props.location.type = cudaMemLocationTypeDevice;
+		props.location.id = dev;
+
+		if (cudaSuccess != cudaMemPoolCreate(&p, &props)) {
+
+			cudaGetLastError();
+			p = nullptr;
+			return nullptr;
+		}
+
+		unsigned long long keep = ~0ull;
+		cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+	}
+
+	return p;
+}
+
+static cudaError_t ec_malloc(void** q, size_t bytes, cudaStream_t st)
+{
+	cudaMemPool_t p = ec_pool();
+	return p ? cudaMallocFromPoolAsync(q, bytes, p, st) : cudaMallocAsync(q, bytes, st);
+}
+
 // Hermitian eigen-decomposition of the n x n matrix that the column-major
 // view of A shows (for a row-major Hermitian G that is conj(G), what the
 // reference hands LAPACK): eigenvalues ascending in w, eigenvector i in
@@ -555,24 +606,33 @@ static int ec_heevd(int n, float2* A, float* w, cudaStream_t st)
 	const EcSolver* api = nullptr;
 	TRY(ec_solver(&api));
 
-	cusolverDnHandle_t h = nullptr;
+	// one handle per device for the life of the process (creating one per
+	// call costs more than a small decomposition); calls are serialised
+	static std::mutex hmu;
+	static std::map<int, cusolverDnHandle_t> handles;
+	std::lock_guard<std::mutex> lock(hmu);
+	int dev = 0;
+	CUDA_TRY(cudaGetDevice(&dev));
+	cusolverDnHandle_t& h = handles[dev];
 
-	if (CUSOLVER_STATUS_SUCCESS != api->create(&h))
+	if (nullptr == h && CUSOLVER_STATUS_SUCCESS != api->create(&h)) {
+
+		h = nullptr;
 		return fail(BNUFFT_ERR_CUDA, "ecalib: cusolverDnCreate failed");
+	}
 
 	int status = BNUFFT_OK;
 	int lwork = 0;
 	cuComplex* work = nullptr;
 	int* info = nullptr;
 	int hinfo = 0;
-
 	if (CUSOLVER_STATUS_SUCCESS != api->set_stream(h, st)
 	    || CUSOLVER_STATUS_SUCCESS != api->heevd_size(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, (const cuComplex*)A, n, w, &lwork)) {
 
 		status = fail(BNUFFT_ERR_CUDA, "ecalib: cheevd workspace query failed");
 
-	} else if (cudaSuccess != cudaMalloc(&work, sizeof(cuComplex) * (size_t)std::max(lwork, 1))
-		   || cudaSuccess != cudaMalloc(&info, sizeof(int))) {
+	} else if (cudaSuccess != ec_malloc((void**)&work, sizeof(cuComplex) * (size_t)std::max(lwork, 1), st)
+		   || cudaSuccess != ec_malloc((void**)&info, sizeof(int), st)) {
 
 		status = fail(BNUFFT_ERR_NOMEM, "ecalib: cheevd workspace (%d) allocation failed", lwork);
 
@@ -587,9 +647,12 @@ static int ec_heevd(int n, float2* A, float* w, cudaStream_t st)
 		status = fail(BNUFFT_ERR_CUDA, "ecalib: cheevd info %d", hinfo);
 	}
 
-	cudaFree(work);
-	cudaFree(info);
-	api->destroy(h);
+	if (work)
+		cudaFreeAsync(work, st);
+
+	if (info)
+		cudaFreeAsync(info, st);
+
 	return status;
 }
 
@@ -620,35 +683,52 @@ static std::complex<double> ec_fftmod(long n, long j, bool inv)
 // points (src/misc/resize.c:234-261: fftmod, FFT, fftmod, centred
 // zero-padding, ifftmod, unnormalised inverse FFT, ifftmod), [m][n]
 // row-major.
-static std::vector<float2> ec_sinc_matrix(long n, long m)
+static std::vector<double2> ec_sinc_matrix(long n, long m)
 {
-	std::vector<float2> R((size_t)(m * n));
+	std::vector<double2> R((size_t)(m * n), make_double2(0., 0.));
 
 	if (n == m) {
 
 		for (long i = 0; i < n; i++)
-			R[(size_t)(i * n + i)] = make_float2(1.f, 0.f);
+			R[(size_t)(i * n + i)] = make_double2(1., 0.);
 
 		return R;
 	}
 
 	const long p = m / 2 - n / 2;
+	std::vector<std::complex<double>> em((size_t)m), en((size_t)n), pm((size_t)m), pn((size_t)n), a((size_t)n);
 
-	for (long x = 0; x < m; x++)
-		for (long u = 0; u < n; u++) {
+	for (long k = 0; k < m; k++) {
+
+		em[(size_t)k] = std::polar(1., 2. * M_PI * (double)k / (double)m);
+		pm[(size_t)k] = ec_fftmod(m, k, true);
+	}
+
+	for (long k = 0; k < n; k++) {
+
+		en[(size_t)k] = std::polar(1., -2. * M_PI * (double)k / (double)n);
+		pn[(size_t)k] = ec_fftmod(n, k, false);
+	}
+
+	for (long u = 0; u < n; u++) {
+
+		for (long f = 0; f < n; f++)		// forward half: fftmod, DFT, fftmod
+			a[(size_t)f] = pn[(size_t)f] * en[(size_t)(f * u % n)] * pn[(size_t)u];
+
+		for (long x = 0; x < m; x++) {		// centred padding, ifftmod, inverse DFT, ifftmod
 
 			std::complex<double> s = 0.;
 
 			for (long f = 0; f < n; f++) {
 
 				const long g = f + p;
-				s += std::polar(1., 2. * M_PI * (double)(g * x % m) / (double)m) * ec_fftmod(m, g, true)
-				     * ec_fftmod(n, f, false) * std::polar(1., -2. * M_PI * (double)(f * u % n) / (double)n);
+				s += em[(size_t)(g * x % m)] * pm[(size_t)g] * a[(size_t)f];
 			}
 
-			s *= ec_fftmod(m, x, true) * ec_fftmod(n, u, false);
-			R[(size_t)(x * n + u)] = make_float2((float)s.real(), (float)s.imag());
+			s *= pm[(size_t)x];
+			R[(size_t)(x * n + u)] = make_double2(s.real(), s.imag());
 		}
+	}
 
 	return R;
 }
@@ -775,15 +855,17 @@ static void ec_calib_geom(const std::vector<float2>& tmp, const long td[3], long
 
 struct EcBuf {
 
+	cudaStream_t st;
 	std::vector<void*> p;
-	~EcBuf() { for (void* q : p) cudaFree(q); }
+	explicit EcBuf(cudaStream_t s) : st(s) {}
+	~EcBuf() { for (void* q : p) cudaFreeAsync(q, st); }
 
 	template <class T>
 	int alloc(T** out, size_t n)
 	{
 		void* q = nullptr;
 
-		if (cudaSuccess != cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T))) {
+		if (cudaSuccess != ec_malloc(&q, std::max<size_t>(n, 1) * sizeof(T), st)) {
 
 			cudaGetLastError();
 			return fail(BNUFFT_ERR_NOMEM, "ecalib: out of device memory (%zu bytes)", n * sizeof(T));
@@ -796,11 +878,11 @@ struct EcBuf {
 };
 
 template <int W>
-static int ec_launch_eigen(int X, int Y, int Z, int C, int M, int xh, int L, const float2* T, const float2* Rx,
+static int ec_launch_eigen(int X, int Y, int Z, int C, int M, int xh, int L, const double2* T, const double2* Rx,
 			   const float2* rot, int iters, float crop, int soft, float2* sens, float2* ev, cudaStream_t st)
 {
 	constexpr int PX = 8 * 32 / W;
-	const size_t smem = sizeof(float2) * ((size_t)xh * L + (size_t)PX * xh + (size_t)PX * M * C) + sizeof(float) * PX * M;
+	const size_t smem = sizeof(double2) * ((size_t)xh * L + (size_t)PX * xh) + sizeof(float2) * (size_t)PX * M * C + sizeof(float) * PX * M;
 
 	auto kern = (M <= 4) ? bn::k_ec_eigen<W, 4> : bn::k_ec_eigen<W, 8>;
 
@@ -940,7 +1022,7 @@ extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const
 	}
 
 	cudaStream_t st = (cudaStream_t)stream;
-	EcBuf buf;
+	EcBuf buf(st);
 	const long nksp = X * Y * Z * C;
 	const float2* dksp = (const float2*)ksp;
 
@@ -1052,7 +1134,8 @@ extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const
 	const long hd3[3] = { kd3[0] > 1 ? 2 * kd3[0] : 1, kd3[1] > 1 ? 2 * kd3[1] : 1, kd3[2] > 1 ? 2 * kd3[2] : 1 };
 	const long hd = hd3[0] * hd3[1] * hd3[2];
 	const long L = C * (C + 1) / 2;
-	float2 *dKT = nullptr, *dF = nullptr, *dKimg = nullptr, *dcov = nullptr;
+	float2 *dKT = nullptr, *dF = nullptr, *dKimg = nullptr;
+	double2* dcov = nullptr;
 	TRY(buf.alloc(&dKT, (size_t)(kd * C * n)));
 	TRY(buf.alloc(&dF, (size_t)(hd * kd)));
 	TRY(buf.alloc(&dKimg, (size_t)(hd * C * n)));
@@ -1063,24 +1146,25 @@ extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const
 	k_ec_kern_perm<<<ec_blocks(kd * C * n), 256, 0, st>>>(dG, (int)Ncol, (int)kd, (int)C, (int)n, dKT);
 	LAUNCHED();
 	TRY(ec_gemm(false, (int)hd, (int)(C * n), (int)kd, dF, kd, dKT, C * n, dKimg, C * n, st));
-	const float scale = (float)(1. / ((double)kd * (double)hd));
+	const double scale = 1. / ((double)kd * (double)hd);
 	k_ec_pixgram<<<(unsigned)hd, 256, 0, st>>>(dKimg, (int)C, (int)n, scale, dcov);
 	LAUNCHED();
 	prof_end(pe, st);
 
 	// 5. sinc interpolation along y and z to every image row
-	const std::vector<float2> Rx = ec_sinc_matrix(hd3[0], od[0]);
-	const std::vector<float2> Ry = ec_sinc_matrix(hd3[1], od[1]);
-	const std::vector<float2> Rz = ec_sinc_matrix(hd3[2], od[2]);
-	float2 *dRx = nullptr, *dRy = nullptr, *dRz = nullptr, *dT = nullptr, *drot = nullptr;
+	const std::vector<double2> Rx = ec_sinc_matrix(hd3[0], od[0]);
+	const std::vector<double2> Ry = ec_sinc_matrix(hd3[1], od[1]);
+	const std::vector<double2> Rz = ec_sinc_matrix(hd3[2], od[2]);
+	double2 *dRx = nullptr, *dRy = nullptr, *dRz = nullptr, *dT = nullptr;
+	float2* drot = nullptr;
 	TRY(buf.alloc(&dRx, Rx.size()));
 	TRY(buf.alloc(&dRy, Ry.size()));
 	TRY(buf.alloc(&dRz, Rz.size()));
 	TRY(buf.alloc(&dT, (size_t)(od[1] * od[2] * hd3[0] * L)));
 	TRY(buf.alloc(&drot, (size_t)C));
-	CUDA_TRY(cudaMemcpyAsync(dRx, Rx.data(), sizeof(float2) * Rx.size(), cudaMemcpyHostToDevice, st));
-	CUDA_TRY(cudaMemcpyAsync(dRy, Ry.data(), sizeof(float2) * Ry.size(), cudaMemcpyHostToDevice, st));
-	CUDA_TRY(cudaMemcpyAsync(dRz, Rz.data(), sizeof(float2) * Rz.size(), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(dRx, Rx.data(), sizeof(double2) * Rx.size(), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(dRy, Ry.data(), sizeof(double2) * Ry.size(), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(dRz, Rz.data(), sizeof(double2) * Rz.size(), cudaMemcpyHostToDevice, st));
 	pe = prof_begin("ecalib_interp", st);
 	k_ec_interp_yz<<<(unsigned)(od[1] * od[2]), 256, 0, st>>>(dcov, (int)hd3[0], (int)hd3[1], (int)hd3[2], (int)L, (int)od[1], dRy, dRz, dT);
 	prof_end(pe, st);

@@ -293,24 +293,28 @@ def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True):
     for _ in range(max(3, warmup)):
         ecalib(kt, dims=dims)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev_pairs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     n0 = lib.bnufft_launch_count()
     with ClockSampler(dev.index or 0) as clk:
         torch.cuda.synchronize()
-        e0.record()
-        for _ in range(steps):
+        for a, b in ev_pairs:
+            a.record()
             sens, ev, info = ecalib(kt, dims=dims)
-        e1.record()
+            b.record()
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
+    per = sorted(a.elapsed_time(b) for a, b in ev_pairs)
+    ms = float(np.mean(per))
     launches = int(lib.bnufft_launch_count() - n0)
     stages = {}
     for kind in ("ecalib_gram", "ecalib_eig", "ecalib_imgcov", "ecalib_interp", "ecalib_pixels"):
-        lib.bnufft_prof_start(kind.encode())
-        ecalib(kt, dims=dims)
-        kms, kn = ctypes.c_double(), ctypes.c_long()
-        lib.bnufft_prof_stop(ctypes.byref(kms), ctypes.byref(kn))
-        stages[kind] = {"ms": kms.value, "launches": kn.value}
+        t = []
+        for _ in range(5):		# median of 5 calls
+            lib.bnufft_prof_start(kind.encode())
+            ecalib(kt, dims=dims)
+            kms, kn = ctypes.c_double(), ctypes.c_long()
+            lib.bnufft_prof_stop(ctypes.byref(kms), ctypes.byref(kn))
+            t.append(kms.value)
+        stages[kind] = {"ms": sorted(t)[2], "ms_min": min(t), "ms_max": max(t), "launches": kn.value}
     t0 = time.perf_counter()
     for _ in range(steps):
         ecalib(k)
@@ -321,7 +325,8 @@ def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True):
     out_bytes = N * N * (C * M + M) * 8
     t_bytes = N * xh * (C * (C + 1) // 2) * 8
     res = {"workload": f"ecalib2d_{N}_c{coils}", "metric": "ESPIRiT calibrations/s", "unit": "calibrations/s",
-           "value": 1e3 / ms, "ms_per_calibration": ms, "gpu_launches": launches // steps,
+           "value": 1e3 / ms, "ms_per_calibration": ms, "ms_min": per[0], "ms_median": per[len(per) // 2],
+           "ms_max": per[-1], "gpu_launches": launches // steps,
            "nkernels": info["nkernels"], "caldims": list(info["caldims"]),
            "e2e": {"value": 1.0 / e2e_s, "unit": "calibrations/s", "h2d_bytes_per_step": int(k.nbytes),
                    "d2h_bytes_per_step": int(N * N * (C * M + M) * 8)},
