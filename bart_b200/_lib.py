@@ -105,6 +105,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     sig("bnufft_ecalib_defaults", None, ctypes.POINTER(EcalibConfC))
     sig("bnufft_ecalib_dims", i, ctypes.POINTER(EcalibConfC), i, cl, cl, cl)
     sig("bnufft_ecalib", i, ctypes.POINTER(EcalibConfC), i, cl, vp, vp, vp, fp, cl, cl, vp)
+    sig("bnufft_calib", i, ctypes.POINTER(EcalibConfC), i, cl, vp, vp, i, fp, cl, vp, vp)
     sig("bnufft_last_error", ctypes.c_char_p)
     sig("bnufft_launch_count", ctypes.c_long)
     sig("bnufft_prof_start", i, ctypes.c_char_p)

@@ -78,10 +78,11 @@ __global__ void k_ec_casorati(const float2* __restrict__ cal, int cx, int cy, in
 	}
 }
 
-// C [M][N] = op(A) [M][K] * B [K][N], row-major complex float, 64 x 64
+// C [M][N] = op(A) [M][K] * op(B) [K][N], row-major complex float, 64 x 64
 // tiles, 4 x 4 outputs per thread. CONJ_A: op(A) = A^H with A stored
-// [K][M]; else A stored [M][K].
-template <bool CONJ_A>
+// [K][M]; else A stored [M][K]. CONJ_BT: op(B) = B^H with B stored [N][K];
+// else B stored [K][N].
+template <bool CONJ_A, bool CONJ_BT>
 __global__ void __launch_bounds__(256) k_ec_cgemm(int M, int N, int K, const float2* __restrict__ A, long lda,
 						  const float2* __restrict__ B, long ldb, float2* __restrict__ Cm, long ldc)
 {
@@ -122,8 +123,14 @@ __global__ void __launch_bounds__(256) k_ec_cgemm(int M, int N, int K, const flo
 
 			As[kk][mm] = a;
 
-			const int nn = e % 64, kb = e / 64, gn = n0 + nn, gkb = k0 + kb;
-			Bs[kb][nn] = (gn < N && gkb < K) ? B[gkb * ldb + gn] : make_float2(0.f, 0.f);
+			const int nn = CONJ_BT ? e / 16 : e % 64, kb = CONJ_BT ? e % 16 : e / 64;
+			const int gn = n0 + nn, gkb = k0 + kb;
+			float2 b = make_float2(0.f, 0.f);
+
+			if (gn < N && gkb < K)
+				b = CONJ_BT ? ec_conj(B[gn * ldb + gkb]) : B[gkb * ldb + gn];
+
+			Bs[kb][nn] = b;
 		}
 
 		__syncthreads();
@@ -173,6 +180,35 @@ __global__ void k_ec_kern_perm(const float2* __restrict__ E, int Ncol, int kd, i
 		const int r = (int)(t % ((long)C * n));
 		const int c = r / n, i = r % n;
 		KT[t] = E[(long)(Ncol - 1 - i) * Ncol + u + (long)kd * c];
+	}
+}
+
+// The same arrangement when the eigenvectors u_i are those of the P x P
+// matrix A A^H (fewer patches than kernel entries): kernel i is
+// A^T u_(P-1-i) / sigma_i, the right singular vector of conj(A), i.e. the
+// eigenvector of conj(G) that LAPACK returns in the reference.
+__global__ void k_ec_kern_left(const float2* __restrict__ A, const float2* __restrict__ E, int P, int Ncol, int kd, int C,
+			       int n, const float* __restrict__ inv_sigma, float2* __restrict__ KT)
+{
+	const long tot = (long)kd * C * n;
+
+	for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
+
+		const int u = (int)(t / ((long)C * n));
+		const int r = (int)(t % ((long)C * n));
+		const int c = r / n, i = r % n;
+		const long j = u + (long)kd * c;
+		const float2* e = E + (long)(P - 1 - i) * P;
+		double sr = 0., si = 0.;
+
+		for (int p = 0; p < P; p++) {
+
+			const float2 a = A[(long)p * Ncol + j], w = e[p];
+			sr += (double)a.x * w.x - (double)a.y * w.y;
+			si += (double)a.x * w.y + (double)a.y * w.x;
+		}
+
+		KT[t] = make_float2((float)(sr * inv_sigma[i]), (float)(si * inv_sigma[i]));
 	}
 }
 
@@ -902,14 +938,17 @@ static int ec_launch_eigen(int X, int Y, int Z, int C, int M, int xh, int L, con
 
 static unsigned ec_blocks(long n) { return (unsigned)std::min<long>((n + 255) / 256, 148L * 16); }
 
-static int ec_gemm(bool conj_a, int M, int N, int K, const float2* A, long lda, const float2* B, long ldb, float2* Cm, long ldc, cudaStream_t st)
+// mode 0: A B; 1: A^H B (the Gram A^H A); 2: A B^H (A A^H)
+static int ec_gemm(int mode, int M, int N, int K, const float2* A, long lda, const float2* B, long ldb, float2* Cm, long ldc, cudaStream_t st)
 {
 	dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
 
-	if (conj_a)
-		bn::k_ec_cgemm<true><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
+	if (1 == mode)
+		bn::k_ec_cgemm<true, false><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
+	else if (2 == mode)
+		bn::k_ec_cgemm<false, true><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
 	else
-		bn::k_ec_cgemm<false><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
+		bn::k_ec_cgemm<false, false><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
 
 	LAUNCHED();
 	return BNUFFT_OK;
@@ -975,30 +1014,15 @@ extern "C" int bnufft_ecalib_dims(const struct bnufft_ecalib_conf* conf, int N, 
 	return BNUFFT_OK;
 }
 
-extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
-			     void* sens, void* emaps, float* svals, long* nkernels, long caldims[3], void* stream)
+// the options and sizes this build implements (src/ecalib.c:64-97)
+static int ec_check(const struct bnufft_ecalib_conf* conf, long C, int M)
 {
-	using namespace bn;
-
-	if (nullptr == conf || nullptr == ksp_dims || nullptr == ksp || nullptr == sens || N < 5)
-		return fail(BNUFFT_ERR_ARG, "ecalib: bad arguments");
-
 	if (conf->weighting || conf->intensity || conf->phase_normalize || conf->nystroem || !conf->orthiter || conf->crop < 0.f)
 		return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: soft-weighting, automatic (SURE) crop, intensity and phase "
 			    "normalisation, Nystroem and the full point-wise eigen-decomposition are not built");
 
-	if (1 != ksp_dims[4])
-		return fail(BNUFFT_ERR_ARG, "ecalib: MAPS dimension is not of size one");
-
-	for (int i = 5; i < N; i++)
-		if (1 != ksp_dims[i])
-			return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: one calibration at a time (dimension %d has size %ld)", i, ksp_dims[i]);
-
-	const long X = ksp_dims[0], Y = ksp_dims[1], Z = ksp_dims[2], C = ksp_dims[3];
-	const int M = conf->maps;
-
-	if (X < 1 || Y < 1 || Z < 1 || C < 1)
-		return fail(BNUFFT_ERR_ARG, "ecalib: bad k-space dimensions");
+	if (C < 1)
+		return fail(BNUFFT_ERR_ARG, "ecalib: no coils");
 
 	if (C > 32)
 		return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: %ld coils (at most 32 are built)", C);
@@ -1006,69 +1030,20 @@ extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const
 	if (M < 1 || M > C || M > 8)
 		return fail(BNUFFT_ERR_ARG, "ecalib: %d maps for %ld coils (1 <= maps <= min(coils, 8))", M, C);
 
-	long kd3[3], od[3];
+	return BNUFFT_OK;
+}
 
-	for (int i = 0; i < 3; i++) {
-
-		kd3[i] = (1 == ksp_dims[i]) ? 1 : conf->kdims[i];
-
-		if (kd3[i] < 1 || conf->calsize[i] < 1)
-			return fail(BNUFFT_ERR_ARG, "ecalib: bad kernel or calibration size");
-
-		od[i] = (kd3[i] > 1) ? ksp_dims[i] : 1;
-
-		if (kd3[i] > 1 && ksp_dims[i] < 2 * kd3[i])
-			return fail(BNUFFT_ERR_ARG, "ecalib: image size %ld below twice the kernel size %ld", ksp_dims[i], kd3[i]);
-	}
-
-	cudaStream_t st = (cudaStream_t)stream;
-	EcBuf buf(st);
-	const long nksp = X * Y * Z * C;
-	const float2* dksp = (const float2*)ksp;
-
-	if (!on_device(ksp)) {
-
-		float2* t = nullptr;
-		TRY(buf.alloc(&t, (size_t)nksp));
-		CUDA_TRY(cudaMemcpyAsync(t, ksp, sizeof(float2) * nksp, cudaMemcpyHostToDevice, st));
-		dksp = t;
-	}
-
-	// 1. centre block (full readout) to the host, calibration region there
-	const long td[3] = { X, std::min(conf->calsize[1], Y), std::min(conf->calsize[2], Z) };
-	const long tp[3] = { 0, (Y - td[1]) / 2, (Z - td[2]) / 2 };
-	const long tn = td[0] * td[1] * td[2] * C;
-	float2* dtmp = nullptr;
-	TRY(buf.alloc(&dtmp, (size_t)tn));
-	k_ec_gather<<<ec_blocks(tn), 256, 0, st>>>(dksp, X, Y, Z, (int)C, (int)tp[0], (int)tp[1], (int)tp[2], (int)td[0], (int)td[1], (int)td[2], dtmp);
-	LAUNCHED();
-	std::vector<float2> htmp((size_t)tn);
-	CUDA_TRY(cudaMemcpyAsync(htmp.data(), dtmp, sizeof(float2) * tn, cudaMemcpyDeviceToHost, st));
-	CUDA_TRY(cudaStreamSynchronize(st));
-
-	long cal[3], cpos[3];
-	const long cs3[3] = { conf->calsize[0], conf->calsize[1], conf->calsize[2] };
-	ec_calib_geom(htmp, td, C, cs3, cal, cpos);
-
-	for (int i = 0; i < 3; i++) {
-
-		if (1 == cal[i] && 1 != ksp_dims[i])
-			return fail(BNUFFT_ERR_ARG, "ecalib: Calibration region not found!");
-
-		if (cal[i] < kd3[i])
-			return fail(BNUFFT_ERR_ARG, "ecalib: calibration region %ld smaller than the kernel %ld", cal[i], kd3[i]);
-	}
-
-	if (nullptr != caldims)
-		for (int i = 0; i < 3; i++)
-			caldims[i] = cal[i];
+// Steps 2-7 from the calibration data on the device (cal [cx, cy, cz, C]):
+// the Gram matrix of the Casorati matrix, its eigen-decomposition, the
+// kernels, their images and per-pixel Gram matrices, the interpolation and
+// the per-pixel pass into sens [od, C, M] and emaps [od, 1, M].
+static int ec_from_calibration(const struct bnufft_ecalib_conf* conf, const long kd3[3], const long od[3], long C, int M,
+			       const float2* dcal, const long cal[3], float* svals, long* nkernels, void* sens, void* emaps,
+			       cudaStream_t st, EcBuf& buf)
+{
+	using namespace bn;
 
 	const long csize = cal[0] * cal[1] * cal[2];
-	float2* dcal = nullptr;
-	TRY(buf.alloc(&dcal, (size_t)(csize * C)));
-	k_ec_gather<<<ec_blocks(csize * C), 256, 0, st>>>(dksp, X, Y, Z, (int)C, (int)(tp[0] + cpos[0]), (int)(tp[1] + cpos[1]), (int)(tp[2] + cpos[2]),
-							 (int)cal[0], (int)cal[1], (int)cal[2], dcal);
-	LAUNCHED();
 
 	// 2. Casorati matrix and its Gram matrix G = A^H A (row-major)
 	const long kd = kd3[0] * kd3[1] * kd3[2];
@@ -1078,31 +1053,43 @@ extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const
 	if (Ncol > 16384)
 		return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: calibration matrix with %ld columns", Ncol);
 
+	// With fewer patches than kernel entries (2D with 11 coils or more) the
+	// P x P matrix A A^H has the same nonzero eigenvalues and a smaller
+	// decomposition; the kernels follow from its eigenvectors (step 4).
+	const bool left = P < Ncol;
+	const long R = left ? P : Ncol;
 	float2 *dA = nullptr, *dG = nullptr;
 	float* dw = nullptr;
 	TRY(buf.alloc(&dA, (size_t)(P * Ncol)));
-	TRY(buf.alloc(&dG, (size_t)(Ncol * Ncol)));
-	TRY(buf.alloc(&dw, (size_t)Ncol));
+	TRY(buf.alloc(&dG, (size_t)(R * R)));
+	TRY(buf.alloc(&dw, (size_t)R));
 	cudaEvent_t pe = prof_begin("ecalib_gram", st);
 	k_ec_casorati<<<ec_blocks(P * Ncol), 256, 0, st>>>(dcal, (int)cal[0], (int)cal[1], (int)cal[2], (int)kd3[0], (int)kd3[1], (int)kd3[2], (int)C, dA);
 	LAUNCHED();
-	TRY(ec_gemm(true, (int)Ncol, (int)Ncol, (int)P, dA, Ncol, dA, Ncol, dG, Ncol, st));
+
+	if (left)
+		TRY(ec_gemm(2, (int)P, (int)P, (int)Ncol, dA, Ncol, dA, Ncol, dG, P, st));
+	else
+		TRY(ec_gemm(1, (int)Ncol, (int)Ncol, (int)P, dA, Ncol, dA, Ncol, dG, Ncol, st));
+
 	prof_end(pe, st);
 
-	// 3. eigen-decomposition (of conj(G), as LAPACK sees the reference's
-	// row-major array), kernels above the threshold
+	// 3. eigen-decomposition of the matrix the column-major view shows:
+	// conj(G) as LAPACK sees the reference's row-major array, or conj(A A^H)
+	// whose eigenvectors give conj(G)'s through A; kernels above the
+	// threshold
 	pe = prof_begin("ecalib_eig", st);
-	TRY(ec_heevd((int)Ncol, dG, dw, st));
+	TRY(ec_heevd((int)R, dG, dw, st));
 	prof_end(pe, st);
-	std::vector<float> w((size_t)Ncol);
-	CUDA_TRY(cudaMemcpyAsync(w.data(), dw, sizeof(float) * Ncol, cudaMemcpyDeviceToHost, st));
+	std::vector<float> w((size_t)R);
+	CUDA_TRY(cudaMemcpyAsync(w.data(), dw, sizeof(float) * R, cudaMemcpyDeviceToHost, st));
 	CUDA_TRY(cudaStreamSynchronize(st));
 
-	std::vector<float> val((size_t)Ncol);
+	std::vector<float> val((size_t)Ncol, 0.f);
 
-	for (long i = 0; i < Ncol; i++) {
+	for (long i = 0; i < R; i++) {
 
-		const float e = w[(size_t)(Ncol - 1 - i)];
+		const float e = w[(size_t)(R - 1 - i)];
 		val[(size_t)i] = (e < 0.f) ? 0.f : sqrtf(e);
 	}
 
@@ -1120,8 +1107,8 @@ extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const
 			if (val[(size_t)i] / val[0] > sqrtf(conf->threshold))
 				n++;
 
-	if (n < 1 || n > Ncol)
-		return fail(BNUFFT_ERR_ARG, "ecalib: %ld kernels selected (of %ld)", n, Ncol);
+	if (n < 1 || n > R || val[(size_t)(n - 1)] <= 0.f)
+		return fail(BNUFFT_ERR_ARG, "ecalib: %ld kernels selected (of %ld, rank at most %ld)", n, Ncol, R);
 
 	if (nullptr != svals)
 		for (long i = 0; i < Ncol; i++)
@@ -1142,10 +1129,28 @@ extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const
 	TRY(buf.alloc(&dcov, (size_t)(hd * L)));
 	const std::vector<float2> F = ec_kernel_dft(kd3, hd3);
 	CUDA_TRY(cudaMemcpyAsync(dF, F.data(), sizeof(float2) * F.size(), cudaMemcpyHostToDevice, st));
+	float* dinv = nullptr;
+
+	if (left) {
+
+		std::vector<float> inv((size_t)n);
+
+		for (long i = 0; i < n; i++)
+			inv[(size_t)i] = 1.f / val[(size_t)i];
+
+		TRY(buf.alloc(&dinv, (size_t)n));
+		CUDA_TRY(cudaMemcpyAsync(dinv, inv.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+	}
+
 	pe = prof_begin("ecalib_imgcov", st);
-	k_ec_kern_perm<<<ec_blocks(kd * C * n), 256, 0, st>>>(dG, (int)Ncol, (int)kd, (int)C, (int)n, dKT);
+
+	if (left)
+		k_ec_kern_left<<<ec_blocks(kd * C * n), 256, 0, st>>>(dA, dG, (int)P, (int)Ncol, (int)kd, (int)C, (int)n, dinv, dKT);
+	else
+		k_ec_kern_perm<<<ec_blocks(kd * C * n), 256, 0, st>>>(dG, (int)Ncol, (int)kd, (int)C, (int)n, dKT);
+
 	LAUNCHED();
-	TRY(ec_gemm(false, (int)hd, (int)(C * n), (int)kd, dF, kd, dKT, C * n, dKimg, C * n, st));
+	TRY(ec_gemm(0, (int)hd, (int)(C * n), (int)kd, dF, kd, dKT, C * n, dKimg, C * n, st));
 	const double scale = 1. / ((double)kd * (double)hd);
 	k_ec_pixgram<<<(unsigned)hd, 256, 0, st>>>(dKimg, (int)C, (int)n, scale, dcov);
 	LAUNCHED();
@@ -1239,4 +1244,149 @@ extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const
 	// the temporaries are freed when this returns: finish the work first
 	CUDA_TRY(cudaStreamSynchronize(st));
 	return BNUFFT_OK;
+}
+
+extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
+			     void* sens, void* emaps, float* svals, long* nkernels, long caldims[3], void* stream)
+{
+	using namespace bn;
+
+	if (nullptr == conf || nullptr == ksp_dims || nullptr == ksp || nullptr == sens || N < 5)
+		return fail(BNUFFT_ERR_ARG, "ecalib: bad arguments");
+
+	if (1 != ksp_dims[4])
+		return fail(BNUFFT_ERR_ARG, "ecalib: MAPS dimension is not of size one");
+
+	for (int i = 5; i < N; i++)
+		if (1 != ksp_dims[i])
+			return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: one calibration at a time (dimension %d has size %ld)", i, ksp_dims[i]);
+
+	const long X = ksp_dims[0], Y = ksp_dims[1], Z = ksp_dims[2], C = ksp_dims[3];
+	const int M = conf->maps;
+
+	if (X < 1 || Y < 1 || Z < 1 || C < 1)
+		return fail(BNUFFT_ERR_ARG, "ecalib: bad k-space dimensions");
+
+	TRY(ec_check(conf, C, M));
+
+	long kd3[3], od[3];
+
+	for (int i = 0; i < 3; i++) {
+
+		kd3[i] = (1 == ksp_dims[i]) ? 1 : conf->kdims[i];
+
+		if (kd3[i] < 1 || conf->calsize[i] < 1)
+			return fail(BNUFFT_ERR_ARG, "ecalib: bad kernel or calibration size");
+
+		od[i] = (kd3[i] > 1) ? ksp_dims[i] : 1;
+
+		if (kd3[i] > 1 && ksp_dims[i] < 2 * kd3[i])
+			return fail(BNUFFT_ERR_ARG, "ecalib: image size %ld below twice the kernel size %ld", ksp_dims[i], kd3[i]);
+	}
+
+	cudaStream_t st = (cudaStream_t)stream;
+	EcBuf buf(st);
+	const long nksp = X * Y * Z * C;
+	const float2* dksp = (const float2*)ksp;
+
+	if (!on_device(ksp)) {
+
+		float2* t = nullptr;
+		TRY(buf.alloc(&t, (size_t)nksp));
+		CUDA_TRY(cudaMemcpyAsync(t, ksp, sizeof(float2) * nksp, cudaMemcpyHostToDevice, st));
+		dksp = t;
+	}
+
+	// 1. centre block (full readout) to the host, calibration region there
+	const long td[3] = { X, std::min(conf->calsize[1], Y), std::min(conf->calsize[2], Z) };
+	const long tp[3] = { 0, (Y - td[1]) / 2, (Z - td[2]) / 2 };
+	const long tn = td[0] * td[1] * td[2] * C;
+	float2* dtmp = nullptr;
+	TRY(buf.alloc(&dtmp, (size_t)tn));
+	k_ec_gather<<<ec_blocks(tn), 256, 0, st>>>(dksp, X, Y, Z, (int)C, (int)tp[0], (int)tp[1], (int)tp[2], (int)td[0], (int)td[1], (int)td[2], dtmp);
+	LAUNCHED();
+	std::vector<float2> htmp((size_t)tn);
+	CUDA_TRY(cudaMemcpyAsync(htmp.data(), dtmp, sizeof(float2) * tn, cudaMemcpyDeviceToHost, st));
+	CUDA_TRY(cudaStreamSynchronize(st));
+
+	long cal[3], cpos[3];
+	const long cs3[3] = { conf->calsize[0], conf->calsize[1], conf->calsize[2] };
+	ec_calib_geom(htmp, td, C, cs3, cal, cpos);
+
+	for (int i = 0; i < 3; i++) {
+
+		if (1 == cal[i] && 1 != ksp_dims[i])
+			return fail(BNUFFT_ERR_ARG, "ecalib: Calibration region not found!");
+
+		if (cal[i] < kd3[i])
+			return fail(BNUFFT_ERR_ARG, "ecalib: calibration region %ld smaller than the kernel %ld", cal[i], kd3[i]);
+	}
+
+	if (nullptr != caldims)
+		for (int i = 0; i < 3; i++)
+			caldims[i] = cal[i];
+
+	const long csize = cal[0] * cal[1] * cal[2];
+	float2* dcal = nullptr;
+	TRY(buf.alloc(&dcal, (size_t)(csize * C)));
+	k_ec_gather<<<ec_blocks(csize * C), 256, 0, st>>>(dksp, X, Y, Z, (int)C, (int)(tp[0] + cpos[0]), (int)(tp[1] + cpos[1]), (int)(tp[2] + cpos[2]),
+							 (int)cal[0], (int)cal[1], (int)cal[2], dcal);
+	LAUNCHED();
+
+	return ec_from_calibration(conf, kd3, od, C, M, dcal, cal, svals, nkernels, sens, emaps, st, buf);
+}
+
+extern "C" int bnufft_calib(const struct bnufft_ecalib_conf* conf, int N, const long out_dims[], void* sens, void* emaps,
+			    int SN, float* svals, const long cal_dims[], const void* cal, void* stream)
+{
+	using namespace bn;
+
+	if (nullptr == conf || nullptr == out_dims || nullptr == cal_dims || nullptr == cal || nullptr == sens || N < 5)
+		return fail(BNUFFT_ERR_ARG, "calib: bad arguments");
+
+	for (int i = 5; i < N; i++)
+		if (1 != out_dims[i] || 1 != cal_dims[i])
+			return fail(BNUFFT_ERR_UNSUPPORTED, "calib: one calibration at a time (dimension %d)", i);
+
+	const long C = cal_dims[3];
+	const int M = (int)out_dims[4];
+
+	if (1 != cal_dims[4] || out_dims[3] != C)
+		return fail(BNUFFT_ERR_ARG, "calib: output coils %ld, calibration coils %ld", out_dims[3], C);
+
+	TRY(ec_check(conf, C, M));
+
+	long kd3[3], od[3], calv[3];
+
+	for (int i = 0; i < 3; i++) {
+
+		calv[i] = cal_dims[i];
+		kd3[i] = (1 == cal_dims[i]) ? 1 : conf->kdims[i];
+		od[i] = out_dims[i];
+
+		if (kd3[i] < 1 || calv[i] < kd3[i])
+			return fail(BNUFFT_ERR_ARG, "calib: calibration region %ld smaller than the kernel %ld", calv[i], kd3[i]);
+
+		if (od[i] < ((kd3[i] > 1) ? 2 * kd3[i] : 1))
+			return fail(BNUFFT_ERR_ARG, "calib: image size %ld below twice the kernel size %ld", od[i], kd3[i]);
+	}
+
+	if (nullptr != svals && SN < kd3[0] * kd3[1] * kd3[2] * C)
+		return fail(BNUFFT_ERR_ARG, "calib: %d singular values for a %ld-column calibration matrix", SN, kd3[0] * kd3[1] * kd3[2] * C);
+
+	cudaStream_t st = (cudaStream_t)stream;
+	EcBuf buf(st);
+	const long n = calv[0] * calv[1] * calv[2] * C;
+	const float2* dcal = (const float2*)cal;
+
+	if (!on_device(cal)) {
+
+		float2* t = nullptr;
+		TRY(buf.alloc(&t, (size_t)n));
+		CUDA_TRY(cudaMemcpyAsync(t, cal, sizeof(float2) * n, cudaMemcpyHostToDevice, st));
+		dcal = t;
+	}
+
+	long nk = 0;
+	return ec_from_calibration(conf, kd3, od, C, M, dcal, calv, svals, &nk, sens, emaps, st, buf);
 }

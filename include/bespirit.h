@@ -5,7 +5,8 @@
  * Replaces the reference's calibration entry points (mrirecon/bart
  * v1.0.00): extract_calib (src/misc/mri2.c:220-225) followed by calib
  * (src/calib/calib.c:797-800, declared in src/calib/calib.h), as main_ecalib
- * calls them (src/ecalib.c:150-253).
+ * calls them (src/ecalib.c:150-253): bnufft_ecalib does both,
+ * bnufft_calib the second alone.
  */
 #ifndef BESPIRIT_H
 #define BESPIRIT_H
@@ -68,6 +69,16 @@ int bnufft_ecalib_dims(const struct bnufft_ecalib_conf* conf, int N, const long 
  * own kernels. */
 int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
 		  void* sens, void* emaps, float* svals, long* nkernels, long caldims[3], void* stream);
+
+/* calib (src/calib/calib.c:797-800, src/calib/calib.h): the same from the
+ * calibration region's data cal (cal_dims[N]: [cx, cy, cz, C]) the caller
+ * has extracted, into sens [X, Y, Z, C, maps] and emaps [X, Y, Z, 1, maps]
+ * with X, Y, Z and maps from out_dims (out_dims[3] = C; conf->maps and
+ * conf->calsize are not used). svals (host, SN >= kx*ky*kz*C entries, or
+ * NULL) as for bnufft_ecalib. The kernel is 1 along a dimension where the
+ * calibration data have size 1. */
+int bnufft_calib(const struct bnufft_ecalib_conf* conf, int N, const long out_dims[], void* sens, void* emaps,
+		 int SN, float* svals, const long cal_dims[], const void* cal, void* stream);
 
 #ifdef __cplusplus
 }

@@ -7,7 +7,10 @@ lop_fun_t callbacks. Outputs are compared with the reference's own CPU
 results on the golden fixtures: 1e-5 per operator apply, 1e-4 for
 reconstructions.
 
-The binaries (oracle/_ref/bin/{nufft,pics}_bnufft) are built by
+The reference's `ecalib` is built the same way with its calib() call
+bound to bnufft_calib (oracle/refbuild/calib_bnufft.c).
+
+The binaries (oracle/_ref/bin/{nufft,pics,ecalib}_bnufft) are built by
 `make -f oracle/refbuild/Makefile` after `python -m bart_b200.build`.
 """
 
@@ -158,3 +161,30 @@ def test_dropin_nufft_oversampling():
             _run(d, exe, "-o", str(o), "-a", "-x64:64:1", "t", "y", "a")
             assert rel(readcfl(os.path.join(d, "k")), g[f"fwd_{i}"]) < 1e-5, o
             assert rel(readcfl(os.path.join(d, "a")), g[f"adj_{i}"]) < 1e-5, o
+
+
+@pytest.mark.parametrize("name", ["ecalib2d_n64_c8", "ecalib2d_n64_c8_m3_soft", "ecalib2d_40x48_c20",
+                                  "ecalib3d_n24_c4"])
+def test_dropin_ecalib(name):
+    """The reference's own ecalib (option parsing, .cfl I/O, its
+    calibration-region extraction) with calib() bound to bnufft_calib
+    (oracle/refbuild/calib_bnufft.c) writes the maps and eigenvalue maps of
+    the reference's CPU ecalib: the principal map and its eigenvalues to
+    1e-4, lower maps and theirs to 1e-3, up to the global sign the reference takes from its
+    LAPACK."""
+    from test_espirit_oracle import map_error
+    exe = _tool("ecalib_bnufft")
+    g = golden(name)
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "k"), g["ksp"])
+        _run(d, exe, *[str(a) for a in g["args"]], "k", "s", "e")
+        s, e = readcfl(os.path.join(d, "s")), readcfl(os.path.join(d, "e"))
+    assert s.shape == g["sens"].shape and e.shape == g["emaps"].shape
+    sh = s.shape[:5]
+    s, e = s.reshape(sh, order="F"), e.reshape(sh[:3] + (1, sh[4]), order="F")
+    rs = g["sens"].reshape(sh, order="F")
+    re = g["emaps"].reshape(e.shape, order="F")
+    for m in range(sh[4]):
+        bar = 1e-4 if m == 0 else 1e-3
+        assert rel(e[..., m], re[..., m]) < bar, (m, rel(e[..., m], re[..., m]))
+        assert map_error(s[..., m], rs[..., m]) < bar, m
