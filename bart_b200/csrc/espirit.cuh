@@ -1,7 +1,7 @@
 // ESPIRiT calibration (bart ecalib) on the GPU: the reference's default
 // path (src/ecalib.c:46-262, src/calib/calib.c) as
 //
-//   calibration region (host search over the centre block's pattern)
+//   calibration region (host search over the centre block's coil energies)
 //   -> Casorati matrix of the region's kernel-sized patches
 //   -> Gram matrix (tiled complex GEMM)
 //   -> Hermitian eigen-decomposition (cuSOLVER cheevd, the one library
@@ -53,6 +53,31 @@ __global__ void k_ec_gather(const float2* __restrict__ src, long X, long Y, long
 		const int z = (int)(t % bz);
 		const int c = (int)(t / bz);
 		dst[i] = src[(ox + x) + X * ((oy + y) + Y * ((oz + z) + Z * (long)c))];
+	}
+}
+
+// Coil energy of every voxel of the centre block [bx, by, bz] of a
+// [X, Y, Z, C] array at (ox, oy, oz): e = sum_c |v|^2 (double sums rounded
+// once). Zero exactly where the reference's pattern (root-sum-of-squares
+// != 0, src/misc/mri2.c:39-57) is zero.
+__global__ void k_ec_energy(const float2* __restrict__ src, long X, long Y, long Z, int C, int ox, int oy, int oz,
+			    int bx, int by, int bz, float* __restrict__ e)
+{
+	const long n = (long)bx * by * bz;
+
+	for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+
+		const int x = (int)(i % bx), y = (int)((i / bx) % by), z = (int)(i / ((long)bx * by));
+		const float2* p = src + (ox + x) + X * ((oy + y) + Y * (long)(oz + z));
+		double s = 0.;
+
+		for (int c = 0; c < C; c++) {
+
+			const float2 v = p[X * Y * Z * (long)c];
+			s += (double)v.x * v.x + (double)v.y * v.y;
+		}
+
+		e[i] = (float)s;
 	}
 }
 
@@ -801,28 +826,12 @@ static std::vector<float2> ec_kernel_dft(const long kd3[3], const long hd3[3])
 	return F;
 }
 
-// The calibration region (src/misc/mri2.c:100-160, 26-...): inside the
-// centre block tmp [tdims, C] (host copy), grow a centred fully sampled
-// block one line at a time per dimension up to calsize, then slide along
-// the readout to the position of largest energy (first maximum).
-static void ec_calib_geom(const std::vector<float2>& tmp, const long td[3], long C, const long calsize[3], long cal[3], long pos[3])
+// The calibration region (src/misc/mri2.c:100-160): inside the centre
+// block td (per-voxel coil energies e, host copy), grow a centred fully
+// sampled block one line at a time per dimension up to calsize, then slide
+// along the readout to the position of largest energy (first maximum).
+static void ec_calib_geom(const std::vector<float>& e, const long td[3], const long calsize[3], long cal[3], long pos[3])
 {
-	const long tn = td[0] * td[1] * td[2];
-	std::vector<char> pat((size_t)tn, 0);
-
-	for (long i = 0; i < tn; i++) {
-
-		float s = 0.f;
-
-		for (long c = 0; c < C; c++) {
-
-			const float2 v = tmp[(size_t)(i + tn * c)];
-			s += v.x * v.x + v.y * v.y;
-		}
-
-		pat[(size_t)i] = (0.f != s);
-	}
-
 	for (int i = 0; i < 3; i++) {
 
 		cal[i] = 1;
@@ -836,7 +845,7 @@ static void ec_calib_geom(const std::vector<float2>& tmp, const long td[3], long
 		for (long z = 0; z < cal[2]; z++)
 			for (long y = 0; y < cal[1]; y++)
 				for (long x = 0; x < cal[0]; x++)
-					if (!pat[(size_t)((pos[0] + x) + td[0] * ((pos[1] + y) + td[1] * (pos[2] + z)))])
+					if (0.f == e[(size_t)((pos[0] + x) + td[0] * ((pos[1] + y) + td[1] * (pos[2] + z)))])
 						return false;
 		return true;
 	};
@@ -863,26 +872,30 @@ static void ec_calib_geom(const std::vector<float2>& tmp, const long td[3], long
 		}
 	}
 
+	// readout sweep: energy of every readout line inside the y/z window,
+	// then window sums by a running sum
+	std::vector<double> line((size_t)td[0], 0.);
+
+	for (long z = 0; z < cal[2]; z++)
+		for (long y = 0; y < cal[1]; y++)
+			for (long x = 0; x < td[0]; x++)
+				line[(size_t)x] += e[(size_t)(x + td[0] * ((pos[1] + y) + td[1] * (pos[2] + z)))];
+
 	long best = 0;
-	double beng = 0.;
+	double beng = 0., win = 0.;
+
+	for (long x = 0; x < cal[0]; x++)
+		win += line[(size_t)x];
 
 	for (long r = 0; r + cal[0] <= td[0]; r++) {
 
-		double e = 0.;
+		if (r > 0)
+			win += line[(size_t)(r + cal[0] - 1)] - line[(size_t)(r - 1)];
 
-		for (long c = 0; c < C; c++)
-			for (long z = 0; z < cal[2]; z++)
-				for (long y = 0; y < cal[1]; y++)
-					for (long x = 0; x < cal[0]; x++) {
-
-						const float2 v = tmp[(size_t)((r + x) + td[0] * ((pos[1] + y) + td[1] * ((pos[2] + z) + td[2] * c)))];
-						e += (double)v.x * v.x + (double)v.y * v.y;
-					}
-
-		if (std::sqrt(e) > beng) {
+		if (std::sqrt(std::max(win, 0.)) > beng) {
 
 			best = r;
-			beng = std::sqrt(e);
+			beng = std::sqrt(std::max(win, 0.));
 		}
 	}
 
@@ -1297,21 +1310,22 @@ extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const
 		dksp = t;
 	}
 
-	// 1. centre block (full readout) to the host, calibration region there
+	// 1. coil energies of the centre block (full readout) to the host,
+	// calibration region there
 	const long td[3] = { X, std::min(conf->calsize[1], Y), std::min(conf->calsize[2], Z) };
 	const long tp[3] = { 0, (Y - td[1]) / 2, (Z - td[2]) / 2 };
-	const long tn = td[0] * td[1] * td[2] * C;
-	float2* dtmp = nullptr;
-	TRY(buf.alloc(&dtmp, (size_t)tn));
-	k_ec_gather<<<ec_blocks(tn), 256, 0, st>>>(dksp, X, Y, Z, (int)C, (int)tp[0], (int)tp[1], (int)tp[2], (int)td[0], (int)td[1], (int)td[2], dtmp);
+	const long tn = td[0] * td[1] * td[2];
+	float* den = nullptr;
+	TRY(buf.alloc(&den, (size_t)tn));
+	k_ec_energy<<<ec_blocks(tn), 256, 0, st>>>(dksp, X, Y, Z, (int)C, (int)tp[0], (int)tp[1], (int)tp[2], (int)td[0], (int)td[1], (int)td[2], den);
 	LAUNCHED();
-	std::vector<float2> htmp((size_t)tn);
-	CUDA_TRY(cudaMemcpyAsync(htmp.data(), dtmp, sizeof(float2) * tn, cudaMemcpyDeviceToHost, st));
+	std::vector<float> hen((size_t)tn);
+	CUDA_TRY(cudaMemcpyAsync(hen.data(), den, sizeof(float) * tn, cudaMemcpyDeviceToHost, st));
 	CUDA_TRY(cudaStreamSynchronize(st));
 
 	long cal[3], cpos[3];
 	const long cs3[3] = { conf->calsize[0], conf->calsize[1], conf->calsize[2] };
-	ec_calib_geom(htmp, td, C, cs3, cal, cpos);
+	ec_calib_geom(hen, td, cs3, cal, cpos);
 
 	for (int i = 0; i < 3; i++) {
 

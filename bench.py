@@ -1164,13 +1164,17 @@ def main():
             line["cpu_baseline"] = cpu_baseline(traj, sens, ksp, method_lines["cg"]["iterations"])
         if world == 1 and not args.lean:
             # the other configs' workloads, timed in the same run: 3D
-            # kooshball NUFFT + CG-SENSE, and the batch of 512 uneven problems
+            # kooshball NUFFT + CG-SENSE, the batch of 512 uneven problems and
+            # the ESPIRiT calibration
             torch.cuda.empty_cache()
             line["kooshball3d"] = run_nufft3d(dev, 3, 2)
             torch.cuda.empty_cache()
             line["kooshball3d"]["normal3d"] = run_normal3d(dev, 5, 3)
             torch.cuda.empty_cache()
             line["batch512"] = run_batch(dev, 2, 3, cpu_base=not args.no_cpu_baseline)
+            torch.cuda.empty_cache()
+            # ESPIRiT calibration of the maps (bart ecalib defaults), 256^2, 16 coils
+            line["ecalib2d"] = run_ecalib(dev, 10, 3, coils=16, cpu_base=not args.no_cpu_baseline)
         print(json.dumps(line), flush=True)
 
     if world > 1:
