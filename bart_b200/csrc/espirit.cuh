@@ -330,7 +330,8 @@ __device__ __forceinline__ float ec_group_sum(float v)
 //      Gram-Schmidt from the last row to the first (src/num/linalg.c
 //      :1235-1313); the last row is the principal eigenvector;
 //   3. map u = row M-1-u with eigenvalue = that row's last norm
-//      (src/calib/calib.c:474-483); weight 0/1 for |e| >= crop, or the
+//      (src/calib/calib.c:474-483); with intensity correction scaled to
+//      l1 norm sqrt(C) over the coils; weight 0/1 for |e| >= crop, or the
 //      reference's soft s-curve (src/calib/calib.c:88-134);
 //   4. phase: times conj of the phase of sum_c map[c] conj(rot[c])
 //      (src/misc/utils.c:148-174);
@@ -338,7 +339,7 @@ __device__ __forceinline__ float ec_group_sum(float v)
 template <int W, int MMAX>
 __global__ void __launch_bounds__(256) k_ec_eigen(int X, int Y, int Z, int C, int M, int xh, int L,
 						  const double2* __restrict__ T, const double2* __restrict__ Rx,
-						  const float2* __restrict__ rot, int iters, float crop, int soft,
+						  const float2* __restrict__ rot, int iters, float crop, int soft, int intensity,
 						  float2* __restrict__ sens, float2* __restrict__ ev)
 {
 	constexpr int PX = 8 * 32 / W;
@@ -470,6 +471,14 @@ __global__ void __launch_bounds__(256) k_ec_eigen(int X, int Y, int Z, int C, in
 				mv = v[q];
 				e = val[q];
 			}
+
+		if (intensity) {	// l1 norm over the coils to sqrt(C), src/misc/utils.c:83-109
+
+			const float l1 = ec_group_sum<W>(sqrtf(mv.x * mv.x + mv.y * mv.y));
+			const float f = (0.f == l1) ? 0.f : sqrtf((float)C) / l1;
+			mv.x *= f;
+			mv.y *= f;
+		}
 
 		float w;
 
@@ -928,7 +937,7 @@ struct EcBuf {
 
 template <int W>
 static int ec_launch_eigen(int X, int Y, int Z, int C, int M, int xh, int L, const double2* T, const double2* Rx,
-			   const float2* rot, int iters, float crop, int soft, float2* sens, float2* ev, cudaStream_t st)
+			   const float2* rot, int iters, float crop, int soft, int intensity, float2* sens, float2* ev, cudaStream_t st)
 {
 	constexpr int PX = 8 * 32 / W;
 	const size_t smem = sizeof(double2) * ((size_t)xh * L + (size_t)PX * xh) + sizeof(float2) * (size_t)PX * M * C + sizeof(float) * PX * M;
@@ -943,7 +952,7 @@ static int ec_launch_eigen(int X, int Y, int Z, int C, int M, int xh, int L, con
 
 	dim3 grid((unsigned)(Y * Z), (unsigned)((X + PX - 1) / PX));
 	cudaEvent_t pe = prof_begin("ecalib_pixels", st);
-	kern<<<grid, 256, smem, st>>>(X, Y, Z, C, M, xh, L, T, Rx, rot, iters, crop, soft, sens, ev);
+	kern<<<grid, 256, smem, st>>>(X, Y, Z, C, M, xh, L, T, Rx, rot, iters, crop, soft, intensity, sens, ev);
 	prof_end(pe, st);
 	LAUNCHED();
 	return BNUFFT_OK;
@@ -1030,9 +1039,9 @@ extern "C" int bnufft_ecalib_dims(const struct bnufft_ecalib_conf* conf, int N, 
 // the options and sizes this build implements (src/ecalib.c:64-97)
 static int ec_check(const struct bnufft_ecalib_conf* conf, long C, int M)
 {
-	if (conf->weighting || conf->intensity || conf->phase_normalize || conf->nystroem || !conf->orthiter || conf->crop < 0.f)
-		return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: soft-weighting, automatic (SURE) crop, intensity and phase "
-			    "normalisation, Nystroem and the full point-wise eigen-decomposition are not built");
+	if (conf->weighting || conf->phase_normalize || conf->nystroem || !conf->orthiter || conf->crop < 0.f)
+		return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: soft-weighting, automatic (SURE) crop, phase normalisation, "
+			    "Nystroem and the full point-wise eigen-decomposition are not built");
 
 	if (C < 1)
 		return fail(BNUFFT_ERR_ARG, "ecalib: no coils");
@@ -1238,7 +1247,7 @@ static int ec_from_calibration(const struct bnufft_ecalib_conf* conf, const long
 	const int W = (C <= 8) ? 8 : (C <= 16) ? 16 : 32;
 	auto go = [&](auto w) -> int {
 		return ec_launch_eigen<decltype(w)::value>((int)od[0], (int)od[1], (int)od[2], (int)C, M, (int)hd3[0], (int)L, dT, dRx, drot,
-							   conf->num_orthiter, conf->crop, conf->softcrop, dsens, dev_ev, st);
+							   conf->num_orthiter, conf->crop, conf->softcrop, conf->intensity, dsens, dev_ev, st);
 	};
 
 	if (8 == W)

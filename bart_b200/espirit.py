@@ -32,9 +32,9 @@ class EcalibConf:
     softcrop: bool = False		# -S
     rotphase: bool = True		# -P clears
     num_orthiter: int = 30
+    intensity: bool = False		# -I
     # not built (the call fails with BNUFFT_ERR_UNSUPPORTED)
     weighting: bool = False		# -W
-    intensity: bool = False		# -I
     phase_normalize: bool = False	# -N
     nystroem: bool = False		# -A
     orthiter: bool = True		# hidden -O clears

@@ -22,10 +22,10 @@ extern "C" {
  * (src/calib/calib.c:693-714) and main_ecalib: kdims 6x6x6 (-k), calsize
  * 24x24x24 (-r), maps 2 (-m), threshold 0.001 (-t), numsv -1 (-n),
  * percentsv -1 (-p), crop 0.8 (-c), softcrop 0 (-S), rotphase 1 (-P clears
- * it), orthiter 1 with num_orthiter 30. The remaining switches (weighting
- * -W, automatic -a / a negative crop (SURE), intensity -I, phase_normalize
- * -N, nystroem -A, orthiter 0) are not built: a call that sets one returns
- * BNUFFT_ERR_UNSUPPORTED. */
+ * it), intensity 0 (-I), orthiter 1 with num_orthiter 30. The remaining
+ * switches (weighting -W, automatic -a / a negative crop (SURE),
+ * phase_normalize -N, nystroem -A, orthiter 0) are not built: a call that
+ * sets one returns BNUFFT_ERR_UNSUPPORTED. */
 struct bnufft_ecalib_conf {
 
 	long kdims[3];

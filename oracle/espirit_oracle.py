@@ -24,7 +24,9 @@ It restates the reference's default ecalib path in float64 NumPy:
    identity with a recursive Gram-Schmidt (src/calib/calib.c:73-86,
    src/num/linalg.c:1235-1313), the maps in order of decreasing eigenvalue
    (src/calib/calib.c:418-487).
-6. Crop where the eigenvalue is below ``crop`` (hard or soft), and the phase
+6. Optionally (-I) each map divided by its l1 norm over the coils times
+   sqrt(C) (src/calib/calib.c:754-769, src/misc/utils.c:83-109); crop where
+   the eigenvalue is below ``crop`` (hard or soft), and the phase
    of every map aligned to the first principal coil component of the
    calibration data (src/calib/calib.c:136-164, 770-795, src/calib/cc.c:45-75,
    src/misc/utils.c:148-174).
@@ -282,7 +284,7 @@ def _scurve(t):
 
 
 def ecalib(ksp, kdims=(6, 6, 6), calsize=(24, 24, 24), maps=2, threshold=0.001, numsv=-1, percentsv=-1.0,
-           crop=0.8, softcrop=False, rotphase=True, num_orthiter=30):
+           crop=0.8, softcrop=False, rotphase=True, num_orthiter=30, intensity=False):
     """The reference's ``ecalib`` (src/ecalib.c:46-262): (maps [X, Y, Z, C,
     maps] with X etc. 1 where the kernel is 1, eigenvalue maps [X, Y, Z, 1,
     maps], singular values, number of kernels, caldims)."""
@@ -304,6 +306,9 @@ def ecalib(ksp, kdims=(6, 6, 6), calsize=(24, 24, 24), maps=2, threshold=0.001, 
     for u in range(maps):
         sens[..., u] = x[..., maps - 1 - u, :]
         ev[..., 0, u] = v[..., maps - 1 - u]
+    if intensity:							# normalizel1 * sqrt(C), src/calib/calib.c:754-769
+        l1 = np.sum(np.abs(sens), axis=3, keepdims=True)
+        sens = np.where(l1 == 0.0, 0.0, sens / np.where(l1 == 0.0, 1.0, l1)) * math.sqrt(C)
     a = np.abs(ev)							# crop_sens
     if softcrop:
         w = _scurve((np.sqrt(a) - crop) / (1.0 - crop))

@@ -474,6 +474,7 @@ def ecalib_cases():
     ecalib_case("ecalib2d_n64_c8", k, [])
     ecalib_case("ecalib2d_n64_c8_m3_soft", k, ["-m", "3", "-c", "0.1", "-S"])
     ecalib_case("ecalib2d_n64_c8_k5_r20_n30_P", k, ["-k", "5", "-r", "20", "-n", "30", "-P", "-c", "0.3"])
+    ecalib_case("ecalib2d_n64_c8_I", k, ["-I", "-c", "0.5"])
     X, Y, C = 40, 48, 20
     img = synth.ellipse_phantom(48, 10, rng)[4:44, :, :]
     maps = synth.coil_maps(48, C, rng)[4:44]

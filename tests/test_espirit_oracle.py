@@ -8,7 +8,7 @@ from conftest import golden, rel
 from oracle import espirit_oracle as eo
 
 CASES = ["ecalib2d_n64_c8", "ecalib2d_n64_c8_m3_soft", "ecalib2d_n64_c8_k5_r20_n30_P", "ecalib2d_40x48_c20",
-         "ecalib3d_n24_c4"]
+         "ecalib3d_n24_c4", "ecalib2d_n64_c8_I"]
 
 
 def ecalib_kwargs(args):
@@ -34,6 +34,8 @@ def ecalib_kwargs(args):
             continue
         if a == "-S":
             kw["softcrop"] = True
+        elif a == "-I":
+            kw["intensity"] = True
         elif a == "-P":
             kw["rotphase"] = False
         i += 1

@@ -100,7 +100,7 @@ def test_ecalib_errors(cuda):
     from bart_b200.espirit import EcalibConf, ecalib
     g = golden("ecalib2d_n64_c8")
     k = g["ksp"]
-    for bad in (dict(weighting=True), dict(intensity=True), dict(crop=-1.0), dict(orthiter=False)):
+    for bad in (dict(weighting=True), dict(phase_normalize=True), dict(crop=-1.0), dict(orthiter=False)):
         with pytest.raises(BnufftError) as e:
             ecalib(k, EcalibConf(**bad))
         assert e.value.status == 2
