@@ -326,9 +326,10 @@ __device__ __forceinline__ float ec_group_sum(float v)
 //      the row's y/z-interpolated packed covariance (shared memory) and
 //      the x-interpolation row Rx[x] (the upper triangle is the conjugate
 //      of the lower, src/calib/calib.c:73-86);
-//   2. iters steps of orthogonal iteration: rows v_m <- v_m H, then
-//      Gram-Schmidt from the last row to the first (src/num/linalg.c
-//      :1235-1313); the last row is the principal eigenvector;
+//   2. iters steps of orthogonal iteration: rows v_m <- v_m H (the
+//      coefficients broadcast through shared memory), then Gram-Schmidt
+//      from the last row to the first (src/num/linalg.c:1235-1313); the
+//      last row is the principal eigenvector;
 //   3. map u = row M-1-u with eigenvalue = that row's last norm
 //      (src/calib/calib.c:474-483); with intensity correction scaled to
 //      l1 norm sqrt(C) over the coils; weight 0/1 for |e| >= crop, or the
@@ -343,10 +344,12 @@ __global__ void __launch_bounds__(256) k_ec_eigen(int X, int Y, int Z, int C, in
 						  float2* __restrict__ sens, float2* __restrict__ ev)
 {
 	constexpr int PX = 8 * 32 / W;
+	constexpr int G = 32 / W;			// pixels per warp
 	extern __shared__ double2 ec_smem[];
 	double2* sT = ec_smem;				// [xh][L]
 	double2* sR = sT + (long)xh * L;		// [PX][xh]
-	float2* sO = (float2*)(sR + PX * xh);		// [PX][M][C]
+	float2* sV = (float2*)(sR + PX * xh);		// [warp][k][g][MMAX]: the iterates, for broadcast
+	float2* sO = sV + 8 * W * G * MMAX;		// [PX][M][C]
 	float* sE = (float*)(sO + PX * M * C);		// [PX][M]
 
 	const int row = blockIdx.x;
@@ -367,7 +370,9 @@ __global__ void __launch_bounds__(256) k_ec_eigen(int X, int Y, int Z, int C, in
 
 	const int lane = threadIdx.x % 32;
 	const int c = lane % W;
-	const int px = (threadIdx.x / 32) * (32 / W) + lane / W;
+	const int g = lane / W;
+	const int px = (threadIdx.x / 32) * G + g;
+	float2* vw = sV + (threadIdx.x / 32) * (W * G * MMAX);
 	const bool act = c < C;
 	const double2* rx = sR + px * xh;
 
@@ -409,23 +414,62 @@ __global__ void __launch_bounds__(256) k_ec_eigen(int X, int Y, int Z, int C, in
 
 	for (int it = 0; it < iters; it++) {
 
-#pragma unroll
-		for (int m = 0; m < MMAX; m++) {
-
-			if (m >= M)
-				continue;
-
-			float2 s = make_float2(0.f, 0.f);
+		// rows v_m <- v_m H. With 16 or 32 lanes per pixel the coefficients
+		// v_m[k] reach every lane through shared memory, two rows per
+		// 16-byte load; with 8 (four pixels per warp) by shuffles, which
+		// measured faster there.
+		if (W >= 16) {
 
 #pragma unroll
-			for (int k = 0; k < W; k++) {
+			for (int m = 0; m < MMAX; m++)
+				vw[(c * G + g) * MMAX + m] = v[m];
 
-				const float2 a = make_float2(__shfl_sync(0xffffffffu, v[m].x, k, W), __shfl_sync(0xffffffffu, v[m].y, k, W));
-				s.x = fmaf(a.x, Hc[k].x, fmaf(-a.y, Hc[k].y, s.x));
-				s.y = fmaf(a.x, Hc[k].y, fmaf(a.y, Hc[k].x, s.y));
+			__syncwarp();
+
+#pragma unroll
+			for (int p = 0; p < MMAX / 2; p++) {
+
+				if (2 * p >= M)
+					continue;
+
+				float4 e = make_float4(0.f, 0.f, 0.f, 0.f);	// (row 2p, row 2p+1)
+
+#pragma unroll
+				for (int k = 0; k < W; k++) {
+
+					const float4 a = *(const float4*)&vw[(k * G + g) * MMAX + 2 * p];
+					e.x = fmaf(a.x, Hc[k].x, fmaf(-a.y, Hc[k].y, e.x));
+					e.y = fmaf(a.x, Hc[k].y, fmaf(a.y, Hc[k].x, e.y));
+					e.z = fmaf(a.z, Hc[k].x, fmaf(-a.w, Hc[k].y, e.z));
+					e.w = fmaf(a.z, Hc[k].y, fmaf(a.w, Hc[k].x, e.w));
+				}
+
+				v[2 * p] = make_float2(e.x, e.y);
+				v[2 * p + 1] = make_float2(e.z, e.w);
 			}
 
-			v[m] = s;
+			__syncwarp();
+
+		} else {
+
+#pragma unroll
+			for (int m = 0; m < MMAX; m++) {
+
+				if (m >= M)
+					continue;
+
+				float2 t = make_float2(0.f, 0.f);
+
+#pragma unroll
+				for (int k = 0; k < W; k++) {
+
+					const float2 a = make_float2(__shfl_sync(0xffffffffu, v[m].x, k, W), __shfl_sync(0xffffffffu, v[m].y, k, W));
+					t.x = fmaf(a.x, Hc[k].x, fmaf(-a.y, Hc[k].y, t.x));
+					t.y = fmaf(a.x, Hc[k].y, fmaf(a.y, Hc[k].x, t.y));
+				}
+
+				v[m] = t;
+			}
 		}
 
 #pragma unroll
@@ -940,7 +984,9 @@ static int ec_launch_eigen(int X, int Y, int Z, int C, int M, int xh, int L, con
 			   const float2* rot, int iters, float crop, int soft, int intensity, float2* sens, float2* ev, cudaStream_t st)
 {
 	constexpr int PX = 8 * 32 / W;
-	const size_t smem = sizeof(double2) * ((size_t)xh * L + (size_t)PX * xh) + sizeof(float2) * (size_t)PX * M * C + sizeof(float) * PX * M;
+	const int mmax = (M <= 4) ? 4 : 8;
+	const size_t smem = sizeof(double2) * ((size_t)xh * L + (size_t)PX * xh) + sizeof(float2) * (size_t)(8 * 32 * mmax)
+			    + sizeof(float2) * (size_t)PX * M * C + sizeof(float) * PX * M;
 
 	auto kern = (M <= 4) ? bn::k_ec_eigen<W, 4> : bn::k_ec_eigen<W, 8>;
 
