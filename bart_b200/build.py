@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "lib", "libbnufft.so")
 SOURCES = [os.path.join(HERE, "csrc", "bnufft.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("fft_core.cuh", "nufft_kernels.cuh", "cg_kernels.cuh", "gridding.cuh",
                                                    "precnet.cuh", "nudft.cuh", "precond_cluster.cuh", "fft512.cuh",
-                                                   "precnet_tc.cuh", "espirit.cuh")] + \
+                                                   "precnet_tc.cuh", "espirit.cuh", "cgext.cuh")] + \
     [os.path.join(ROOT, "include", f) for f in ("bnufft.h", "bespirit.h")]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

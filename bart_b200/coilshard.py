@@ -59,8 +59,15 @@ def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, redu
     unconverged iterates more closely. With ``precond(r)`` (the same
     operator on every rank, e.g. the padded-circulant one, which depends
     only on the trajectory's PSF and lambda) it is preconditioned CG with
-    float64 scalars, the library's precond-3 solve."""
+    float64 scalars, the library's precond-3 solve.
+
+    CUDA tensors run the library's fused CG passes with device scalars
+    (bnufft_cg_*: two or three launches per iteration besides A p and the
+    all-reduce); CPU tensors (the multi-process tests on gloo ranks) run the
+    same recurrence in torch operations."""
     import torch
+    if b.is_cuda:
+        return _sharded_cg_device(normal_local, b, lam, maxiter, tol, reduce, precond, f32_scalars)
     x = torch.zeros_like(b)
     r = b.clone()
     z = precond(r) if precond is not None else r
@@ -105,6 +112,44 @@ def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, redu
             break
         p = beta * p + (r if precond is None else z)
     return x, it
+
+
+def _sharded_cg_device(normal_local, b, lam, maxiter, tol, reduce, precond, f32_scalars):
+    """sharded_cg on the library's fused CG passes (include/bnufft.h,
+    bnufft_cg_*)."""
+    import ctypes
+    import torch
+    from . import _lib
+    lib = _lib.load()
+    st = ctypes.c_void_p(torch.cuda.current_stream(b.device).cuda_stream)
+    b = b.contiguous()
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None	# noqa: E731
+    h = ctypes.c_void_p()
+    f32 = bool(f32_scalars) and precond is None
+    _lib.check(lib.bnufft_cg_create(ctypes.byref(h), b.numel(), float(lam), float(tol), int(f32), st))
+    try:
+        x, r, p = torch.empty_like(b), torch.empty_like(b), torch.empty_like(b)
+        z = precond(b).contiguous() if precond is not None else None
+        _lib.check(lib.bnufft_cg_start(h, ptr(x), ptr(r), ptr(p), ptr(b), ptr(z), st))
+        done, iters = ctypes.c_int(0), ctypes.c_int(0)
+        _lib.check(lib.bnufft_cg_status(h, ctypes.byref(done), ctypes.byref(iters), None, st))
+        if done.value:
+            return x, 0
+        for _ in range(maxiter):
+            q = normal_local(p).contiguous()
+            if reduce is not None:
+                reduce(q)
+            _lib.check(lib.bnufft_cg_update(h, ptr(x), ptr(r), ptr(p), ptr(q), st))
+            z = precond(r).contiguous() if precond is not None else None
+            _lib.check(lib.bnufft_cg_direction(h, ptr(p), ptr(r), ptr(z), st))
+            if tol > 0:		# the stopping test needs the device flag each iteration
+                _lib.check(lib.bnufft_cg_status(h, ctypes.byref(done), ctypes.byref(iters), None, st))
+                if done.value:
+                    break
+        _lib.check(lib.bnufft_cg_status(h, ctypes.byref(done), ctypes.byref(iters), None, st))
+        return x, int(iters.value)
+    finally:
+        lib.bnufft_cg_free(h)
 
 
 def allreduce_sum(t) -> None:

@@ -4894,5 +4894,8 @@ extern "C" int bnufft_forward2d_noalloc(long X, long Y, long M, const void* traj
 	return BNUFFT_OK;
 }
 
+// CG for an operator applied by the caller (bnufft_cg_*)
+#include "cgext.cuh"
+
 // ESPIRiT calibration (include/bespirit.h)
 #include "espirit.cuh"

@@ -305,6 +305,32 @@ double bnufft_calc_beta(float os, float width);
 int bnufft_kb_precompute(double beta, int n, float* table);
 int bnufft_rolloff_axis(float os, float width, long n, double* roll);
 
+/* CG on (A + lambda I) x = b for an operator A that the caller applies
+ * between the calls, with the library's fused vector passes and its device
+ * float64 scalars (the reference's conjgrad, src/iter/italgos.c:497-572;
+ * f32_scalars: alpha, beta and the residual norms rounded to float as it
+ * stores them). No counterpart in the reference: this is the solve of the
+ * coil-sharded CG-SENSE, where A p is each GPU's coil share of the normal
+ * operator summed by an all-reduce (its --md-split-mpi-dims with
+ * mpi_reduce_zsum, src/num/mpi_ops.c:680-735). All vectors are device
+ * arrays of n complex floats on the same stream.
+ *   bnufft_cg_start: x = 0, r = b, p = z (z = M b for PCG, or NULL: b);
+ *   per iteration, with q = A p (without lambda) from the caller:
+ *   bnufft_cg_update: alpha = <r, z> / <p, q + lambda p>, x += alpha p,
+ *     r -= alpha (q + lambda p);
+ *   bnufft_cg_direction (z = M r for PCG, or NULL): stop when ||r|| <= tol
+ *     ||b||, else p = z + beta p, beta = <r, z>_new / <r, z>_old.
+ * Once stopped (or at p^H (A + lambda) p = 0) the calls leave x unchanged;
+ * bnufft_cg_status reads (and synchronises on) the stop flag, the
+ * iterations done and ||r||. */
+typedef struct bnufft_cg_s* bnufft_cg_t;
+int bnufft_cg_create(bnufft_cg_t* cg, long n, float lambda, float tol, int f32_scalars, void* stream);
+int bnufft_cg_start(bnufft_cg_t cg, void* x, void* r, void* p, const void* b, const void* z, void* stream);
+int bnufft_cg_update(bnufft_cg_t cg, void* x, void* r, const void* p, const void* q, void* stream);
+int bnufft_cg_direction(bnufft_cg_t cg, void* p, const void* r, const void* z, void* stream);
+int bnufft_cg_status(bnufft_cg_t cg, int* done, int* iters, float* rnorm, void* stream);
+void bnufft_cg_free(bnufft_cg_t cg);
+
 /* Message of the last failure on this thread ("" if none). */
 const char* bnufft_last_error(void);
 
