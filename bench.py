@@ -267,7 +267,7 @@ def run_normal3d(dev, steps, warmup, coils=8, N=128, spokes=2000):
             "hbm_peak_gbs": peak, "peak_source": peak_src, "passes": passes}
 
 
-def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True):
+def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True, ndim=2):
     """ESPIRiT calibration with the reference's ecalib defaults (6 x 6
     kernel, calibration region up to 24 x 24, threshold 0.001, 2 maps, 30
     orthogonal iterations, crop 0.8) of 2D Cartesian k-space: N x N, `coils`
@@ -279,14 +279,16 @@ def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True):
     matrix from 12 x-interpolation terms per entry, then 30 x maps x C^2
     complex multiply-adds of the orthogonal iteration). cpu_baseline: the
     reference's ecalib built from its sources, whole command with .cfl
-    I/O, all host cores."""
+    I/O, all host cores. ndim 3: an N^3 volume, 24 fully sampled centre
+    lines in y and z (the reference then splits the point-wise step along
+    z, src/ecalib.c:137-138)."""
     import ctypes
     import torch
     from bart_b200 import _lib, synth
     from bart_b200.espirit import ecalib
     rng = np.random.default_rng(11)
-    img = synth.ellipse_phantom(N, 20, rng)
-    k = synth.cartesian_ksp(img, synth.coil_maps(N, coils, rng), rng, 40.0, 24, 2)
+    img = synth.ellipse_phantom(N, 20, rng, ndim=ndim)
+    k = synth.cartesian_ksp(img, synth.coil_maps(N, coils, rng, ndim=ndim), rng, 40.0, 24, 2)
     dims = list(k.shape)
     kt = torch.from_numpy(np.asfortranarray(k).ravel(order="F").copy()).to(dev)
     lib = _lib.load()
@@ -320,16 +322,17 @@ def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True):
         ecalib(k)
     e2e_s = (time.perf_counter() - t0) / steps
     M, C, xh, it = 2, coils, 12, 30
-    flop = N * N * (C * C * xh + it * M * C * C) * 8.0
+    npix = N ** ndim
+    flop = npix * (C * C * xh + it * M * C * C) * 8.0
     px_ms = stages["ecalib_pixels"]["ms"]
-    out_bytes = N * N * (C * M + M) * 8
-    t_bytes = N * xh * (C * (C + 1) // 2) * 8
-    res = {"workload": f"ecalib2d_{N}_c{coils}", "metric": "ESPIRiT calibrations/s", "unit": "calibrations/s",
+    out_bytes = npix * (C * M + M) * 8
+    t_bytes = (npix // N) * xh * (C * (C + 1) // 2) * 16
+    res = {"workload": f"ecalib{ndim}d_{N}_c{coils}", "metric": "ESPIRiT calibrations/s", "unit": "calibrations/s",
            "value": 1e3 / ms, "ms_per_calibration": ms, "ms_min": per[0], "ms_median": per[len(per) // 2],
            "ms_max": per[-1], "gpu_launches": launches // steps,
            "nkernels": info["nkernels"], "caldims": list(info["caldims"]),
            "e2e": {"value": 1.0 / e2e_s, "unit": "calibrations/s", "h2d_bytes_per_step": int(k.nbytes),
-                   "d2h_bytes_per_step": int(N * N * (C * M + M) * 8)},
+                   "d2h_bytes_per_step": int(npix * (C * M + M) * 8)},
            "stages": stages,
            "pixels_kernel": {"flop": flop, "tflops": flop / (px_ms * 1e-3) / 1e12 if px_ms > 0 else None,
                              "fp32_peak_tflops": FP32_PEAK_TFLOPS,
@@ -919,6 +922,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "normal3d", "batch", "scatter", "ecalib"])
     ap.add_argument("--coils", type=int, default=None, help="normal3d (default 8) / ecalib (default 16): coils")
+    ap.add_argument("--ndim", type=int, default=None, choices=[2, 3],
+                    help="ecalib: 2 (256^2, 16 coils) or 3 (128^3, 8 coils)")
     ap.add_argument("--analysis", action="store_true",
                     help="batch: also the solves spread over streams and timed alone per embedding size")
     ap.add_argument("--spokes", type=int, default=20000, help="nufft3d: kooshball spokes")
@@ -964,7 +969,9 @@ def main():
 
     if args.workload == "ecalib":
         if rank == 0:
-            print(json.dumps(run_ecalib(dev, args.steps, args.warmup, coils=args.coils or 16,
+            nd = args.ndim or 2
+            print(json.dumps(run_ecalib(dev, args.steps, args.warmup, N=256 if nd == 2 else 128,
+                                        coils=args.coils or (16 if nd == 2 else 8), ndim=nd,
                                         cpu_base=not args.no_cpu_baseline)), flush=True)
         return
 
