@@ -480,6 +480,11 @@ def ecalib_cases():
     maps = synth.coil_maps(48, C, rng)[4:44]
     k = synth.cartesian_ksp(img, maps, rng, 40.0, 20, 3)
     ecalib_case("ecalib2d_40x48_c20", k, ["-r", "20", "-c", "0.5"])
+    # odd image sides (odd-length centring of the sinc interpolation), six maps
+    rng2 = np.random.default_rng(77)
+    img = synth.ellipse_phantom(64, 10, rng2)[7:57, 9:54]
+    k = synth.cartesian_ksp(img, synth.coil_maps(64, 8, rng2)[7:57, 9:54], rng2, 40.0, 20, 2)
+    ecalib_case("ecalib2d_50x45_c8_m6", k, ["-r", "20", "-m", "6", "-c", "0.2"])
     N, C = 24, 4
     img = synth.ellipse_phantom(N, 6, rng, ndim=3)
     k = synth.cartesian_ksp(img, synth.coil_maps(N, C, rng, ndim=3), rng, 40.0, 12, 2)

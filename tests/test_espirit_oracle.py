@@ -8,7 +8,7 @@ from conftest import golden, rel
 from oracle import espirit_oracle as eo
 
 CASES = ["ecalib2d_n64_c8", "ecalib2d_n64_c8_m3_soft", "ecalib2d_n64_c8_k5_r20_n30_P", "ecalib2d_40x48_c20",
-         "ecalib3d_n24_c4", "ecalib2d_n64_c8_I"]
+         "ecalib3d_n24_c4", "ecalib2d_n64_c8_I", "ecalib2d_50x45_c8_m6"]
 
 
 def ecalib_kwargs(args):
@@ -67,7 +67,9 @@ def test_oracle_matches_reference_ecalib(name):
     rs = g["sens"].reshape(sens.shape, order="F")
     re = g["emaps"].reshape(ev.shape, order="F")
     for m in range(M):
-        assert rel(ev[..., m], re[..., m]) < 2e-5, (m, rel(ev[..., m], re[..., m]))
+        # from the third map on, 30 orthogonal iterations leave the
+        # eigenvalues far from converged and the float32 rounding shows
+        assert rel(ev[..., m], re[..., m]) < (2e-5 if m < 2 else 1e-3), (m, rel(ev[..., m], re[..., m]))
         # lower maps converge less in 30 orthogonal iterations and follow
         # the float rounding more closely
         assert map_error(sens[..., m], rs[..., m]) < (1e-5 if m == 0 else 1e-4), (m, map_error(sens[..., m], rs[..., m]))

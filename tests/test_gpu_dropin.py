@@ -164,7 +164,7 @@ def test_dropin_nufft_oversampling():
 
 
 @pytest.mark.parametrize("name", ["ecalib2d_n64_c8", "ecalib2d_n64_c8_m3_soft", "ecalib2d_40x48_c20",
-                                  "ecalib3d_n24_c4", "ecalib2d_n64_c8_I"])
+                                  "ecalib3d_n24_c4", "ecalib2d_n64_c8_I", "ecalib2d_50x45_c8_m6"])
 def test_dropin_ecalib(name):
     """The reference's own ecalib (option parsing, .cfl I/O, its
     calibration-region extraction) with calib() bound to bnufft_calib
