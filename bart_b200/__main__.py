@@ -5,7 +5,7 @@
   python -m bart_b200 pics -l2 -r lambda [-i iter] -t traj [-w scale] [-S]
                            [--no-toeplitz] ksp sens output
   python -m bart_b200 -l flags pics ...   (or -p flags: the same here)
-  python -m bart_b200 ecalib [-k k] [-r cal] [-m maps] [-t thr] [-c crop] [-S] [-P]
+  python -m bart_b200 ecalib [-k k] [-r cal] [-m maps] [-t thr] [-c crop] [-S] [-P] [-I] [-1]
                              [-n numsv] [-p percent] [-V] kspace sens [emaps]
 
 The k-space argument of pics may be "-": a stream of the reference's
@@ -277,9 +277,6 @@ def main_ecalib(argv) -> int:
     ap.add_argument("sens")
     ap.add_argument("emaps", nargs="?")
     a = ap.parse_args(argv)
-    if a.one:
-        sys.stderr.write("ecalib: -1 (first part only) is not built\n")
-        return 1
     conf = EcalibConf(kdims=tuple(a.kdims), calsize=tuple(a.calsize), maps=a.maps, threshold=a.threshold,
                       numsv=a.numsv, percentsv=a.percentsv, crop=a.crop, softcrop=a.softcrop,
                       rotphase=not a.norotphase, num_orthiter=a.num_orthiter, intensity=a.intensity,
@@ -290,10 +287,15 @@ def main_ecalib(argv) -> int:
     if a.weighting:
         conf.weighting = True
     ksp = readcfl(a.kspace)
-    sens, ev, info = ecalib(ksp, conf, emaps=a.emaps is not None)
-    writecfl(a.sens, sens)
-    if a.emaps is not None:
-        writecfl(a.emaps, ev)
+    if a.one:					# the first part alone (src/ecalib.c:171-190)
+        from .espirit import calone
+        cov, info = calone(ksp, conf)
+        writecfl(a.sens, cov)
+    else:
+        sens, ev, info = ecalib(ksp, conf, emaps=a.emaps is not None)
+        writecfl(a.sens, sens)
+        if a.emaps is not None:
+            writecfl(a.emaps, ev)
     if a.print_svals:
         for i, v in enumerate(info["svals"]):
             print(f"SVALS {i} {v:f}")

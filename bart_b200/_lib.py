@@ -106,6 +106,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     sig("bnufft_ecalib_dims", i, ctypes.POINTER(EcalibConfC), i, cl, cl, cl)
     sig("bnufft_ecalib", i, ctypes.POINTER(EcalibConfC), i, cl, vp, vp, vp, fp, cl, cl, vp)
     sig("bnufft_calib", i, ctypes.POINTER(EcalibConfC), i, cl, vp, vp, i, fp, cl, vp, vp)
+    sig("bnufft_calone", i, ctypes.POINTER(EcalibConfC), i, cl, vp, vp, fp, cl, cl, vp)
     sig("bnufft_cg_create", i, ctypes.POINTER(vp), ctypes.c_long, ctypes.c_float, ctypes.c_float, i, vp)
     sig("bnufft_cg_start", i, vp, vp, vp, vp, vp, vp, vp)
     sig("bnufft_cg_update", i, vp, vp, vp, vp, vp, vp)

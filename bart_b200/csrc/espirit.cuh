@@ -273,6 +273,17 @@ __global__ void k_ec_pixgram(const float2* __restrict__ Kimg, int C, int n, doub
 	}
 }
 
+// [hd][L] float64 -> [L][hd] float32 (calone's output layout)
+__global__ void k_ec_cov_layout(const double2* __restrict__ cov, long hd, long L, float2* __restrict__ out)
+{
+	for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < hd * L; t += (long)gridDim.x * blockDim.x) {
+
+		const long x = t % hd, l = t / hd;
+		const double2 v = cov[x * L + l];
+		out[t] = make_float2((float)v.x, (float)v.y);
+	}
+}
+
 // sinc interpolation along y and z (the reference's sinc_zeropad,
 // src/misc/resize.c:234-292, written as its per-axis linear maps):
 // T[(z Y + y)][u][l] = sum_{v, w} Ry[y][v] Rz[z][w] cov[(w yh + v) xh + u][l].
@@ -1105,9 +1116,12 @@ static int ec_check(const struct bnufft_ecalib_conf* conf, long C, int M)
 // the Gram matrix of the Casorati matrix, its eigen-decomposition, the
 // kernels, their images and per-pixel Gram matrices, the interpolation and
 // the per-pixel pass into sens [od, C, M] and emaps [od, 1, M].
+// cov_out (not NULL): stop after step 4 and write the low-resolution
+// covariance there in the reference's calone layout [xh, yh, zh, C(C+1)/2]
+// (the pixel index fastest; host or device memory).
 static int ec_from_calibration(const struct bnufft_ecalib_conf* conf, const long kd3[3], const long od[3], long C, int M,
 			       const float2* dcal, const long cal[3], float* svals, long* nkernels, void* sens, void* emaps,
-			       cudaStream_t st, EcBuf& buf)
+			       cudaStream_t st, EcBuf& buf, void* cov_out = nullptr)
 {
 	using namespace bn;
 
@@ -1224,6 +1238,24 @@ static int ec_from_calibration(const struct bnufft_ecalib_conf* conf, const long
 	LAUNCHED();
 	prof_end(pe, st);
 
+	if (nullptr != cov_out) {
+
+		float2* dout = (float2*)cov_out;
+		const bool odev = on_device(cov_out);
+
+		if (!odev)
+			TRY(buf.alloc(&dout, (size_t)(hd * L)));
+
+		k_ec_cov_layout<<<ec_blocks(hd * L), 256, 0, st>>>(dcov, hd, L, dout);
+		LAUNCHED();
+
+		if (!odev)
+			CUDA_TRY(cudaMemcpyAsync(cov_out, dout, sizeof(float2) * hd * L, cudaMemcpyDeviceToHost, st));
+
+		CUDA_TRY(cudaStreamSynchronize(st));
+		return BNUFFT_OK;
+	}
+
 	// 5. sinc interpolation along y and z to every image row
 	const std::vector<double2> Rx = ec_sinc_matrix(hd3[0], od[0]);
 	const std::vector<double2> Ry = ec_sinc_matrix(hd3[1], od[1]);
@@ -1314,12 +1346,12 @@ static int ec_from_calibration(const struct bnufft_ecalib_conf* conf, const long
 	return BNUFFT_OK;
 }
 
-extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
-			     void* sens, void* emaps, float* svals, long* nkernels, long caldims[3], void* stream)
+static int ec_ecalib(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
+		     void* sens, void* emaps, float* svals, long* nkernels, long caldims[3], void* stream, void* cov_out)
 {
 	using namespace bn;
 
-	if (nullptr == conf || nullptr == ksp_dims || nullptr == ksp || nullptr == sens || N < 5)
+	if (nullptr == conf || nullptr == ksp_dims || nullptr == ksp || (nullptr == sens && nullptr == cov_out) || N < 5)
 		return fail(BNUFFT_ERR_ARG, "ecalib: bad arguments");
 
 	if (1 != ksp_dims[4])
@@ -1402,7 +1434,25 @@ extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const
 							 (int)cal[0], (int)cal[1], (int)cal[2], dcal);
 	LAUNCHED();
 
-	return ec_from_calibration(conf, kd3, od, C, M, dcal, cal, svals, nkernels, sens, emaps, st, buf);
+	return ec_from_calibration(conf, kd3, od, C, M, dcal, cal, svals, nkernels, sens, emaps, st, buf, cov_out);
+}
+
+extern "C" int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
+			     void* sens, void* emaps, float* svals, long* nkernels, long caldims[3], void* stream)
+{
+	if (nullptr == sens)
+		return fail(BNUFFT_ERR_ARG, "ecalib: bad arguments");
+
+	return ec_ecalib(conf, N, ksp_dims, ksp, sens, emaps, svals, nkernels, caldims, stream, nullptr);
+}
+
+extern "C" int bnufft_calone(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
+			     void* cov, float* svals, long* nkernels, long caldims[3], void* stream)
+{
+	if (nullptr == cov)
+		return fail(BNUFFT_ERR_ARG, "calone: bad arguments");
+
+	return ec_ecalib(conf, N, ksp_dims, ksp, nullptr, nullptr, svals, nkernels, caldims, stream, cov);
 }
 
 extern "C" int bnufft_calib(const struct bnufft_ecalib_conf* conf, int N, const long out_dims[], void* sens, void* emaps,

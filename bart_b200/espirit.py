@@ -110,3 +110,22 @@ def ecalib(ksp, conf: EcalibConf | None = None, dims=None, emaps: bool = True, s
     del keep
     info = {"svals": np.array(sv[:ncol], dtype=np.float32), "nkernels": int(nk.value), "caldims": tuple(cd)}
     return sens, ev, info
+
+
+def calone(ksp, conf: EcalibConf | None = None):
+    """``ecalib -1``: (the kernels' low-resolution covariance [xh, yh, zh,
+    C(C+1)/2] as a NumPy array, info) for NumPy k-space in BART order."""
+    conf = conf or EcalibConf()
+    lib = _lib.load()
+    arr = np.asfortranarray(np.asarray(ksp).astype(np.complex64, copy=False))
+    kdims = list(arr.shape) + [1] * (16 - arr.ndim)
+    kd = [1 if kdims[i] == 1 else int(conf.kdims[i]) for i in range(3)]
+    C = int(kdims[3])
+    cov = np.zeros([1 if k == 1 else 2 * k for k in kd] + [C * (C + 1) // 2], dtype=np.complex64, order="F")
+    ncol = int(np.prod(kd)) * C
+    sv = (ctypes.c_float * max(ncol, 1))()
+    nk = ctypes.c_long(0)
+    cd = (ctypes.c_long * 3)()
+    _lib.check(lib.bnufft_calone(ctypes.byref(conf.to_c()), 16, _lib.dims_array(kdims), ctypes.c_void_p(arr.ctypes.data),
+                                 ctypes.c_void_p(cov.ctypes.data), sv, ctypes.byref(nk), cd, None))
+    return cov, {"svals": np.array(sv[:ncol], dtype=np.float32), "nkernels": int(nk.value), "caldims": tuple(cd)}

@@ -70,6 +70,14 @@ int bnufft_ecalib_dims(const struct bnufft_ecalib_conf* conf, int N, const long 
 int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
 		  void* sens, void* emaps, float* svals, long* nkernels, long caldims[3], void* stream);
 
+/* ecalib -1 (src/ecalib.c:171-190, calone src/calib/calib.c:388-415): only
+ * the first part, the kernels' low-resolution covariance, written to cov
+ * as [xh, yh, zh, C(C+1)/2] (xh = 2 kx, or 1 where the k-space has size 1;
+ * the packed lower triangle of each pixel's C x C matrix, the pixel index
+ * fastest). svals, nkernels and caldims as for bnufft_ecalib. */
+int bnufft_calone(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
+		  void* cov, float* svals, long* nkernels, long caldims[3], void* stream);
+
 /* calib (src/calib/calib.c:797-800, src/calib/calib.h): the same from the
  * calibration region's data cal (cal_dims[N]: [cx, cy, cz, C]) the caller
  * has extracted, into sens [X, Y, Z, C, maps] and emaps [X, Y, Z, 1, maps]

@@ -464,6 +464,16 @@ def ecalib_case(name, ksp, args):
     print(name, ksp.shape, sens.shape, "kernels", nk, "caldims", cd)
 
 
+def calone_case(name, ksp, args):
+    """The reference's ecalib -1: the kernels' low-resolution covariance."""
+    with tempfile.TemporaryDirectory() as d:
+        writecfl(os.path.join(d, "k"), ksp)
+        run("ecalib", "-1", *args, "k", "c", cwd=d)
+        cov = readcfl(os.path.join(d, "c"))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), ksp=ksp, cov=cov, args=np.array(args))
+    print(name, ksp.shape, cov.shape)
+
+
 def ecalib_cases():
     """Cartesian k-space of ellipse phantoms and polynomial coil maps, 40 dB
     noise, a fully sampled centre and every other line outside it."""
@@ -475,6 +485,7 @@ def ecalib_cases():
     ecalib_case("ecalib2d_n64_c8_m3_soft", k, ["-m", "3", "-c", "0.1", "-S"])
     ecalib_case("ecalib2d_n64_c8_k5_r20_n30_P", k, ["-k", "5", "-r", "20", "-n", "30", "-P", "-c", "0.3"])
     ecalib_case("ecalib2d_n64_c8_I", k, ["-I", "-c", "0.5"])
+    calone_case("calone2d_n64_c8", k, [])
     X, Y, C = 40, 48, 20
     img = synth.ellipse_phantom(48, 10, rng)[4:44, :, :]
     maps = synth.coil_maps(48, C, rng)[4:44]

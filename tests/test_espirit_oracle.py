@@ -96,3 +96,15 @@ def test_oracle_calibration_region_search():
     cal, cd, pos = eo.calib_region(k, (10, 24, 24))
     assert cd == (10, 6, 1)
     assert pos[1] == 13
+
+
+def test_oracle_calone_matches_reference():
+    """ecalib -1: the kernels' low-resolution covariance [12, 12, 1, 36]."""
+    g = golden("calone2d_n64_c8")
+    k = g["ksp"]
+    kd = eo.kernel_dims(k.shape[:3], (6, 6, 6))
+    cal, _, _ = eo.calib_region(k, (24, 24, 24))
+    kern, _ = eo.compute_kernels(cal, kd)
+    cov = eo.compute_imgcov(kern, kd, k.shape[3])
+    assert cov.shape == g["cov"].shape[:4]
+    assert rel(cov, g["cov"]) < 1e-5

@@ -115,3 +115,19 @@ def test_ecalib_errors(cuda):
     with pytest.raises(BnufftError) as e:		# more maps than coils
         ecalib(k[..., :2], EcalibConf(maps=3))
     assert e.value.status == 1
+
+
+def test_calone_vs_reference(cuda, tmp_path):
+    """ecalib -1 through the library (bnufft_calone) and the CLI: the
+    reference's low-resolution covariance."""
+    from bart_b200 import __main__ as cli
+    from bart_b200.cfl import readcfl, writecfl
+    from bart_b200.espirit import calone
+    g = golden("calone2d_n64_c8")
+    cov, info = calone(g["ksp"])
+    assert cov.shape == g["cov"].shape[:4]
+    assert rel(cov, g["cov"]) < 1e-4
+    d = str(tmp_path)
+    writecfl(d + "/k", g["ksp"])
+    assert 0 == cli.main(["ecalib", "-1", d + "/k", d + "/c"])
+    assert rel(readcfl(d + "/c"), g["cov"]) < 1e-4
