@@ -34,7 +34,6 @@ namespace bn {
 // device kernels
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ float2 ec_cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 __device__ __forceinline__ float2 ec_cmulc(float2 a, float2 b) { return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }	// a conj(b)
 __device__ __forceinline__ float2 ec_conj(float2 a) { return make_float2(a.x, -a.y); }
 
