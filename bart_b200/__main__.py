@@ -5,6 +5,7 @@
   python -m bart_b200 pics -l2 -r lambda [-i iter] -t traj [-w scale] [-S]
                            [--no-toeplitz] ksp sens output
   python -m bart_b200 -l flags pics ...   (or -p flags: the same here)
+  python -m bart_b200 -l flags ecalib ... (one calibration per slice)
   python -m bart_b200 ecalib [-k k] [-r cal] [-m maps] [-t thr] [-c crop] [-S] [-P] [-I] [-1]
                              [-n numsv] [-p percent] [-V] kspace sens [emaps]
 
@@ -249,8 +250,9 @@ def _vec3_or_one(s: str):
     return [int(v[0])] * 3
 
 
-def main_ecalib(argv) -> int:
-    """bart ecalib (src/ecalib.c:46-262)."""
+def main_ecalib(argv, loop_flags: int = 0) -> int:
+    """bart ecalib (src/ecalib.c:46-262); with loop flags (bart -l / -p) one
+    calibration per index of the flagged dims."""
     from .espirit import EcalibConf, ecalib
     ap = argparse.ArgumentParser(prog="ecalib")
     ap.add_argument("-t", dest="threshold", type=float, default=0.001)
@@ -287,6 +289,16 @@ def main_ecalib(argv) -> int:
     if a.weighting:
         conf.weighting = True
     ksp = readcfl(a.kspace)
+    if loop_flags:
+        if a.one:
+            sys.stderr.write("ecalib: -1 inside a slice loop is not built\n")
+            return 1
+        from .loop import loop_ecalib
+        sens, ev = loop_ecalib(loop_flags, ksp, conf, emaps=a.emaps is not None)
+        writecfl(a.sens, sens)
+        if a.emaps is not None:
+            writecfl(a.emaps, ev)
+        return 0
     if a.one:					# the first part alone (src/ecalib.c:171-190)
         from .espirit import calone
         cov, info = calone(ksp, conf)
@@ -311,11 +323,11 @@ def main(argv=None) -> int:
             return 2
         flags |= int(argv[1])
         argv = argv[2:]
-    if not argv or argv[0] not in ("nufft", "pics", "ecalib") or (flags and argv[0] != "pics"):
+    if not argv or argv[0] not in ("nufft", "pics", "ecalib") or (flags and argv[0] == "nufft"):
         sys.stderr.write(__doc__)
         return 2
     if "ecalib" == argv[0]:
-        return main_ecalib(argv[1:])
+        return main_ecalib(argv[1:], flags)
     if "pics" == argv[0]:
         return main_pics(argv[1:], flags)
     return main_nufft(argv[1:])

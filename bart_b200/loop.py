@@ -174,3 +174,33 @@ def stream_pics(flags: int, a) -> np.ndarray:
         finally:
             p.free()
     return out
+
+
+def loop_ecalib(flags: int, ksp: np.ndarray, conf, emaps: bool = True):
+    """``bart -l flags ecalib ...``: one calibration per index of the
+    flagged dims (which must lie outside the k-space's own dims 0-4), the
+    maps and eigenvalue maps joined along them. The calibrations run one
+    after another (each is a few milliseconds of GPU work with three host
+    synchronisations). Returns (maps, emaps or None)."""
+    from .espirit import ecalib, output_dims
+
+    dims = loop_dims(flags)
+    if any(d < 5 for d in dims):
+        raise ValueError("ecalib: looped dims must be >= 5 (dims 0-4 are the image, coil and maps axes)")
+    sizes = loop_sizes([ksp.shape], dims)
+    one = list(dims16(ksp.shape))
+    for d in dims:
+        one[d] = 1
+    sd, ed = output_dims(one, conf)
+    for d, n in zip(dims, sizes):
+        sd[d] = n
+        ed[d] = n
+    sens = np.zeros(sd, dtype=np.complex64, order="F")
+    ev = np.zeros(ed, dtype=np.complex64, order="F") if emaps else None
+    for idx in loop_indices(sizes):
+        k = slice_at(ksp, dims, idx)
+        s, e, _ = ecalib(k.reshape(one, order="F"), conf, emaps=emaps)
+        place_at(sens, dims, idx, s)
+        if emaps:
+            place_at(ev, dims, idx, e)
+    return sens, ev

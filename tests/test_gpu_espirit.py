@@ -131,3 +131,26 @@ def test_calone_vs_reference(cuda, tmp_path):
     writecfl(d + "/k", g["ksp"])
     assert 0 == cli.main(["ecalib", "-1", d + "/k", d + "/c"])
     assert rel(readcfl(d + "/c"), g["cov"]) < 1e-4
+
+
+def test_cli_ecalib_slice_loop(cuda, tmp_path):
+    """python -m bart_b200 -l 8192 ecalib: every slice (dim 13) calibrated
+    on its own, the maps joined along dim 13, bit for bit the single-slice
+    results."""
+    from bart_b200 import __main__ as cli
+    from bart_b200.cfl import readcfl, writecfl
+    from bart_b200.espirit import ecalib
+    g = golden("ecalib2d_n64_c8")
+    k = g["ksp"].reshape(list(g["ksp"].shape) + [1] * 12, order="F")
+    rng = np.random.default_rng(3)
+    slices = [k, k * np.complex64(0.5), k * np.exp(1j * rng.uniform(0, 6.28, size=(1, 1, 1, 8) + (1,) * 12)).astype(np.complex64)]
+    d = str(tmp_path)
+    writecfl(d + "/k", np.concatenate(slices, axis=13))
+    assert 0 == cli.main(["-l", "8192", "ecalib", "-m", "1", d + "/k", d + "/s", d + "/e"])
+    s, e = readcfl(d + "/s"), readcfl(d + "/e")
+    assert s.shape[13] == 3 and s.shape[:5] == (64, 64, 1, 8, 1)
+    for i, ks in enumerate(slices):
+        from bart_b200.espirit import EcalibConf
+        si, ei, _ = ecalib(ks, EcalibConf(maps=1))
+        assert np.array_equal(s[..., i, :, :].reshape(si.shape[:5], order="F"), si.reshape(si.shape[:5], order="F")), i
+        assert np.array_equal(e[..., i, :, :].reshape(ei.shape[:5], order="F"), ei.reshape(ei.shape[:5], order="F")), i
