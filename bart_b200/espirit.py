@@ -70,11 +70,13 @@ def output_dims(ksp_dims, conf: EcalibConf | None = None):
     return list(sd), list(ed)
 
 
-def ecalib(ksp, conf: EcalibConf | None = None, dims=None, emaps: bool = True, stream=None):
+def ecalib(ksp, conf: EcalibConf | None = None, dims=None, emaps: bool = True, stream=None, out=None):
     """(sens, emaps or None, info). ``dims`` is required for a torch tensor
     (BART order); outputs are NumPy arrays (F order) for NumPy input and
-    flat CUDA tensors for tensor input. info: ``svals`` (descending),
-    ``nkernels``, ``caldims``."""
+    flat CUDA tensors for tensor input. ``out`` (NumPy input only): a pair
+    (sens, emaps or None) of F-contiguous complex64 arrays of the output
+    shapes to write into (e.g. views of pinned host memory). info:
+    ``svals`` (descending), ``nkernels``, ``caldims``."""
     conf = conf or EcalibConf()
     lib = _lib.load()
     if _is_torch(ksp):
@@ -95,8 +97,16 @@ def ecalib(ksp, conf: EcalibConf | None = None, dims=None, emaps: bool = True, s
         arr = np.asfortranarray(np.asarray(ksp).astype(np.complex64, copy=False))
         kdims = list(arr.shape) + [1] * (16 - arr.ndim)
         sd, ed = output_dims(kdims, conf)
-        sens = np.zeros(sd, dtype=np.complex64, order="F")
-        ev = np.zeros(ed, dtype=np.complex64, order="F") if emaps else None
+        if out is not None:
+            sens, ev = out
+            for a_, d_ in ((sens, sd), (ev, ed)):
+                if a_ is not None and not (a_.dtype == np.complex64 and a_.flags.f_contiguous
+                                           and a_.size == int(np.prod(d_))):
+                    raise ValueError("ecalib: out arrays must be F-contiguous complex64 of the output sizes")
+            emaps = ev is not None
+        else:
+            sens = np.zeros(sd, dtype=np.complex64, order="F")
+            ev = np.zeros(ed, dtype=np.complex64, order="F") if emaps else None
         pk, ps = ctypes.c_void_p(arr.ctypes.data), ctypes.c_void_p(sens.ctypes.data)
         pe = ctypes.c_void_p(ev.ctypes.data) if emaps else None
         st = stream

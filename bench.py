@@ -273,8 +273,8 @@ def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True, ndim=2):
     orthogonal iterations, crop 0.8) of 2D Cartesian k-space: N x N, `coils`
     coils, ellipse phantom, polynomial maps, 40 dB noise, 24 fully sampled
     centre lines and every other line outside. One step = one calibration
-    from device k-space to device maps (value); e2e = from host k-space to
-    host maps and eigenvalue maps. Per-stage device times by CUDA events;
+    from device k-space to device maps (value); e2e = from pinned host
+    k-space to pinned host maps and eigenvalue maps. Per-stage device times by CUDA events;
     the per-pixel pass against the FP32 FMA peak (its arithmetic: the C x C
     matrix from 12 x-interpolation terms per entry, then 30 x maps x C^2
     complex multiply-adds of the orthogonal iteration). cpu_baseline: the
@@ -317,9 +317,20 @@ def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True, ndim=2):
             lib.bnufft_prof_stop(ctypes.byref(kms), ctypes.byref(kn))
             t.append(kms.value)
         stages[kind] = {"ms": sorted(t)[2], "ms_min": min(t), "ms_max": max(t), "launches": kn.value}
+    # end to end from pinned host k-space to pinned host maps and eigenvalue maps
+    def pinned(shape):
+        t = torch.empty(int(np.prod(shape)), dtype=torch.complex64, pin_memory=True)
+        return t, t.numpy().reshape(shape, order="F")
+
+    from bart_b200.espirit import output_dims
+    sd, ed = output_dims(dims)
+    keep = [pinned(k.shape), pinned(sd), pinned(ed)]
+    k_h, s_h, e_h = (v for _, v in keep)
+    k_h[...] = k
+    ecalib(k_h, out=(s_h, e_h))
     t0 = time.perf_counter()
     for _ in range(steps):
-        ecalib(k)
+        ecalib(k_h, out=(s_h, e_h))
     e2e_s = (time.perf_counter() - t0) / steps
     M, C, xh, it = 2, coils, 12, 30
     npix = N ** ndim

@@ -63,8 +63,8 @@ def test_ecalib_vs_oracle(cuda, N, C, ndim, extra):
 
 
 def test_ecalib_device_tensors_equal_host_arrays(cuda):
-    """k-space and maps in device memory (a torch tensor and its dims) give
-    the same bits as host arrays."""
+    """k-space and maps in device memory (a torch tensor and its dims), or
+    caller-provided host outputs, give the same bits as host arrays."""
     import torch
     from bart_b200.espirit import ecalib
     g = golden("ecalib2d_n64_c8")
@@ -75,6 +75,11 @@ def test_ecalib_device_tensors_equal_host_arrays(cuda):
     torch.cuda.synchronize()
     assert np.array_equal(s_dev.cpu().numpy(), s_host.ravel(order="F"))
     assert np.array_equal(e_dev.cpu().numpy(), e_host.ravel(order="F"))
+    # caller-provided host outputs (here pinned memory)
+    s_pin = torch.empty(s_host.size, dtype=torch.complex64, pin_memory=True).numpy().reshape(s_host.shape, order="F")
+    e_pin = torch.empty(e_host.size, dtype=torch.complex64, pin_memory=True).numpy().reshape(e_host.shape, order="F")
+    ecalib(k, out=(s_pin, e_pin))
+    assert np.array_equal(s_pin, s_host) and np.array_equal(e_pin, e_host)
 
 
 def test_ecalib_cli(cuda, tmp_path):
