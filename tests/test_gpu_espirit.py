@@ -41,9 +41,10 @@ def test_ecalib_vs_reference(cuda, name):
 
 
 @pytest.mark.parametrize("N,C,ndim,extra", [(96, 32, 2, {}), (128, 16, 2, {"maps": 3, "crop": 0.3}),
-                                            (32, 8, 3, {"calsize": (16, 16, 16), "kdims": (5, 5, 5)})])
+                                            (32, 8, 3, {"calsize": (16, 16, 16), "kdims": (5, 5, 5)}),
+                                            (48, 8, 3, {"calsize": (20, 20, 20), "maps": 2, "crop": 0.5})])
 def test_ecalib_vs_oracle(cuda, N, C, ndim, extra):
-    """16- and 32-lane pixel groups (16 and 32 coils) and a 3D case against
+    """16- and 32-lane pixel groups (16 and 32 coils) and 3D cases against
     the float64 oracle."""
     from bart_b200 import synth
     from bart_b200.espirit import ecalib
