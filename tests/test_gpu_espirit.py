@@ -57,10 +57,18 @@ def test_ecalib_vs_oracle(cuda, N, C, ndim, extra):
     assert info["nkernels"] == n and tuple(info["caldims"]) == tuple(cd)
     sens = sens.reshape(s.shape, order="F")
     ev = ev.reshape(e.shape, order="F")
+    crop = extra.get("crop", 0.8)
     for m in range(s.shape[-1]):
         assert rel(ev[..., m], e[..., m]) < 1e-4, (m, rel(ev[..., m], e[..., m]))
-        err = map_error(sens[..., m], s[..., m])
-        assert err < (1e-4 if m == 0 else 2e-3), (m, err)
+        # the hard crop keeps a pixel's map or zeroes it: a pixel whose
+        # eigenvalue lies within float rounding of the threshold may fall on
+        # either side (one such pixel among 10^5 moves the relative error by
+        # ~5e-3), so the maps are compared away from the threshold
+        near = np.abs(np.abs(e[..., m]) - crop) < 1e-4
+        assert near.sum() <= max(4, 1e-3 * near.size), near.sum()
+        keep = ~near
+        err = map_error(sens[..., m] * keep, s[..., m] * keep)
+        assert err < (1e-4 if m == 0 else 2e-3), (m, err, int(near.sum()))
 
 
 def test_ecalib_device_tensors_equal_host_arrays(cuda):
