@@ -1000,11 +1000,10 @@ static int ec_launch_eigen(int X, int Y, int Z, int C, int M, int xh, int L, con
 
 	auto kern = (M <= 4) ? bn::k_ec_eigen<W, 4> : bn::k_ec_eigen<W, 8>;
 
-	if (smem > 227 * 1024)
+	if (smem > 200 * 1024)		// the opt-in prep_kernel sets, once per kernel and device
 		return fail(BNUFFT_ERR_UNSUPPORTED, "ecalib: %d coils with a %d-point kernel grid need %zu bytes of shared memory", C, xh, smem);
 
-	if (smem > 48 * 1024)
-		CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+	TRY(prep_kernel(kern, smem));
 
 	dim3 grid((unsigned)(Y * Z), (unsigned)((X + PX - 1) / PX));
 	cudaEvent_t pe = prof_begin("ecalib_pixels", st);
