@@ -83,3 +83,54 @@ def test_loop_split_follows_the_cost_model():
     shards = partition(costs, 2)
     assert 3 in shards[0] and 2 in shards[1]      # the two largest on different ranks
     assert sorted(shards[0] + shards[1]) == list(range(len(sizes)))
+
+
+def _oracle_ecalib(ksp, conf=None, emaps=True, **kw):
+    """Stand-in for the library call in the host-logic tests: the oracle's
+    ecalib with the library's output shapes (16 dims)."""
+    from oracle import espirit_oracle as eo
+    from bart_b200.espirit import EcalibConf, output_dims
+    conf = conf or EcalibConf()
+    k = np.asarray(ksp)
+    s, e, val, n, cd = eo.ecalib(k.reshape(k.shape[:4], order="F") if k.ndim > 4 else k,
+                                 kdims=conf.kdims, calsize=conf.calsize, maps=conf.maps, crop=conf.crop,
+                                 softcrop=conf.softcrop, rotphase=conf.rotphase, intensity=conf.intensity)
+    sd, ed = output_dims(list(k.shape), conf)
+    return (s.astype(np.complex64).reshape(sd, order="F"),
+            e.astype(np.complex64).reshape(ed, order="F") if emaps else None,
+            {"svals": val, "nkernels": n, "caldims": cd})
+
+
+def test_ecalib_slice_loop_joins_per_slice_calibrations(tmp_path, monkeypatch):
+    """python -m bart_b200 -l 8192 ecalib: each slice (dim 13) calibrated on
+    its own, maps and eigenvalue maps joined along dim 13 at their slice
+    index, with the options parsed as the reference's ecalib does (here -m 1
+    -k 5 -r 20:20:1). The calibration itself is stubbed by the oracle."""
+    import bart_b200.espirit as esp
+    from bart_b200 import synth
+    from bart_b200.cfl import readcfl, writecfl
+    monkeypatch.setattr(esp, "ecalib", _oracle_ecalib)
+    rng = np.random.default_rng(12)
+    slices = []
+    for _ in range(2):
+        img = synth.ellipse_phantom(32, 6, rng)
+        k = synth.cartesian_ksp(img, synth.coil_maps(32, 4, rng), rng, 40.0, 20, 2)
+        slices.append(k.reshape(list(k.shape) + [1] * 12, order="F"))
+    d = str(tmp_path)
+    writecfl(d + "/k", np.concatenate(slices, axis=13))
+    assert 0 == cli.main(["-l", "8192", "ecalib", "-m", "1", "-k", "5", "-r", "20:20:1", d + "/k", d + "/s", d + "/e"])
+    s, e = readcfl(d + "/s"), readcfl(d + "/e")
+    assert s.shape[:5] == (32, 32, 1, 4, 1) and s.shape[13] == 2 and e.shape[:5] == (32, 32, 1, 1, 1)
+    from bart_b200.espirit import EcalibConf
+    for i, k in enumerate(slices):
+        si, ei, _ = _oracle_ecalib(k, EcalibConf(maps=1, kdims=(5, 5, 5), calsize=(20, 20, 1)))
+        assert np.array_equal(s[..., i, :, :].reshape(si.shape[:5], order="F"), si.reshape(si.shape[:5], order="F"))
+        assert np.array_equal(e[..., i, :, :].reshape(ei.shape[:5], order="F"), ei.reshape(ei.shape[:5], order="F"))
+
+
+def test_ecalib_loop_rejects_inner_dims():
+    """The looped dims must lie outside the k-space's own dims 0-4."""
+    from bart_b200.espirit import EcalibConf
+    from bart_b200.loop import loop_ecalib
+    with pytest.raises(ValueError):
+        loop_ecalib(1 << 3, np.zeros((8, 8, 1, 2), dtype=np.complex64), EcalibConf())
