@@ -53,11 +53,12 @@ def sharded_cg(normal_local, b, lam: float, maxiter: int, tol: float = 0.0, redu
     ||r|| <= tol ||b|| (tol > 0 reads the residual on the host each
     iteration). Returns (x, iterations run).
 
-    Without ``precond`` this is the reference's CG with float64 alpha and
-    beta, as the library's single-GPU CG keeps them; ``f32_scalars`` rounds
-    them to float32 as the reference stores them, which reproduces its
-    unconverged iterates more closely. With ``precond(r)`` (the same
-    operator on every rank, e.g. the padded-circulant one, which depends
+    Without ``precond`` this is the reference's CG; ``f32_scalars`` keeps
+    alpha, beta and the residual norms in float32 as the reference stores
+    them (the library's one-GPU pics default, which reproduces its
+    unconverged iterates closely), else they stay in float64. With
+    ``precond(r)`` (the same operator on every rank, e.g. the
+    padded-circulant one, which depends
     only on the trajectory's PSF and lambda) it is preconditioned CG with
     float64 scalars, the library's precond-3 solve.
 
@@ -169,12 +170,13 @@ class CoilShardedPics:
     complex64 CUDA tensor) on every rank."""
 
     def __init__(self, traj, sens_local, ksp_dims, lam=0.01, maxiter=30, tol=0.0, scaling=0.0,
-                 rescale=False, toeplitz=True, traj_dims=None, sens_dims=None, precond=0):
+                 rescale=False, toeplitz=True, traj_dims=None, sens_dims=None, precond=0, ref_scalars=True):
         from .pics import Pics, PicsConf
         if precond not in (0, 3) or (precond == 3 and not toeplitz):
             raise ValueError("CoilShardedPics: precond 0 (CG) or 3 (padded-circulant PCG, Toeplitz only)")
         self.lam, self.maxiter, self.tol = float(lam), int(maxiter), float(tol)
         self.scaling, self.rescale, self.precond = float(scaling), bool(rescale), int(precond)
+        self.ref_scalars = bool(ref_scalars)	# plain CG: float32 scalars as the reference (PicsConf default)
         # scaling 1: rhs() returns this rank's A_r^H y unscaled; the scale is
         # estimated on the reduced sum. The padded-circulant preconditioner
         # depends only on the trajectory and lambda, so every rank's model
@@ -194,7 +196,8 @@ class CoilShardedPics:
         scale = self.scaling if self.scaling != 0.0 else scaling_from_adjoint(b)
         b = b / scale
         x, self.iters = sharded_cg(self.model.normal, b, self.lam, self.maxiter, self.tol, allreduce_sum,
-                                   precond=self.model.precond if self.precond else None)
+                                   precond=self.model.precond if self.precond else None,
+                                   f32_scalars=self.ref_scalars)
         self.scale = scale
         return x * scale if self.rescale else x
 

@@ -42,9 +42,10 @@ def test_coil_shares_add_up_to_the_whole(cuda):
 
 
 def test_sharded_solve_one_rank_vs_reference(cuda):
-    """Without a process group the sharded solve holds every coil: 5
-    iterations at scaling 1 give the reference's pics -i5 -w1; with the
-    scaling estimated it uses the scaling of the library's own pics."""
+    """Without a process group the sharded solve holds every coil: 5 and 30
+    iterations at scaling 1 give the reference's pics -i5 -w1 and -i30 -w1;
+    with the scaling estimated it uses the scaling of the library's own
+    pics."""
     from bart_b200.coilshard import CoilShardedPics
     from bart_b200.pics import Pics, PicsConf
     g = golden("pics2d_n64_c4")
@@ -54,6 +55,13 @@ def test_sharded_solve_one_rank_vs_reference(cuda):
     x = cs.run(ksp).cpu().numpy()
     assert cs.iters == 5
     assert rel(x, g["x5_w1"]) < 1e-5
+    cs.free()
+    # 30 unconverged iterations: the reference's float32 scalars (the
+    # default) keep the iterates on the reference's, as for the one-GPU pics
+    cs = CoilShardedPics(traj, sens, list(g["ksp"].shape), lam=0.01, maxiter=30, scaling=1.0, **dims)
+    x = cs.run(ksp).cpu().numpy()
+    assert cs.iters == 30
+    assert rel(x, g["x30_w1"]) < 1e-4, rel(x, g["x30_w1"])
     cs.free()
     cs = CoilShardedPics(traj, sens, list(g["ksp"].shape), lam=0.01, maxiter=30, **dims)
     cs.run(ksp)
