@@ -960,8 +960,8 @@ __global__ void __launch_bounds__(32 * TG_WARPS, 4) k_grid6_tiles(const int* __r
 				const int i0 = s0 + (int)(a - off), i1 = s0 + (int)(e - off);
 				off += s1 - s0;
 
-				// rounds of 32 candidates; the next round's footprint start
-				// and coil values are loaded while this round accumulates
+				// batches of 32 candidates; the next batch's footprint start
+				// and coil values are loaded while this batch accumulates
 				float4 f0n = make_float4(0.f, 0.f, 0.f, 0.f);
 				float2 vn[CW];
 
