@@ -106,7 +106,11 @@ __global__ void k_ec_casorati(const float2* __restrict__ cal, int cx, int cy, in
 // tiles, 4 x 4 outputs per thread. CONJ_A: op(A) = A^H with A stored
 // [K][M]; else A stored [M][K]. CONJ_BT: op(B) = B^H with B stored [N][K];
 // else B stored [K][N].
-template <bool CONJ_A, bool CONJ_BT>
+// LOWER: only the tiles that hold entries with row >= column are computed
+// (a Hermitian Gram matrix for the eigen-decomposition, which reads the
+// row-major lower triangle: UPLO 'U' of its column-major view); the tiles
+// above are written as zeros.
+template <bool CONJ_A, bool CONJ_BT, bool LOWER = false>
 __global__ void __launch_bounds__(256) k_ec_cgemm(int M, int N, int K, const float2* __restrict__ A, long lda,
 						  const float2* __restrict__ B, long ldb, float2* __restrict__ Cm, long ldc)
 {
@@ -115,6 +119,20 @@ __global__ void __launch_bounds__(256) k_ec_cgemm(int M, int N, int K, const flo
 
 	const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
 	const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+
+	if (LOWER && n0 > m0 + 63) {
+
+		for (int i = 0; i < 4; i++)
+			for (int j = 0; j < 4; j++) {
+
+				const int gm = m0 + ty * 4 + i, gn = n0 + tx * 4 + j;
+
+				if (gm < M && gn < N)
+					Cm[gm * ldc + gn] = make_float2(0.f, 0.f);
+			}
+
+		return;
+	}
 
 	float2 acc[4][4];
 
@@ -1015,15 +1033,16 @@ static int ec_launch_eigen(int X, int Y, int Z, int C, int M, int xh, int L, con
 
 static unsigned ec_blocks(long n) { return (unsigned)std::min<long>((n + 255) / 256, 148L * 16); }
 
-// mode 0: A B; 1: A^H B (the Gram A^H A); 2: A B^H (A A^H)
+// mode 0: A B; 1: A^H B (the Gram A^H A); 2: A B^H (A A^H); the two Gram
+// modes compute the lower triangle only (see k_ec_cgemm)
 static int ec_gemm(int mode, int M, int N, int K, const float2* A, long lda, const float2* B, long ldb, float2* Cm, long ldc, cudaStream_t st)
 {
 	dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64));
 
 	if (1 == mode)
-		bn::k_ec_cgemm<true, false><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
+		bn::k_ec_cgemm<true, false, true><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
 	else if (2 == mode)
-		bn::k_ec_cgemm<false, true><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
+		bn::k_ec_cgemm<false, true, true><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
 	else
 		bn::k_ec_cgemm<false, false><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, Cm, ldc);
 
