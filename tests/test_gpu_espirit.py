@@ -168,3 +168,32 @@ def test_cli_ecalib_slice_loop(cuda, tmp_path):
         si, ei, _ = ecalib(ks, EcalibConf(maps=1))
         assert np.array_equal(s[..., i, :, :].reshape(si.shape[:5], order="F"), si.reshape(si.shape[:5], order="F")), i
         assert np.array_equal(e[..., i, :, :].reshape(ei.shape[:5], order="F"), ei.reshape(ei.shape[:5], order="F")), i
+
+
+def test_ecalib_properties_full_size(cuda):
+    """256^2, 32 coils, 2 maps, crop 0.3: wherever a map is kept it has unit
+    norm over the coils and the two maps are orthogonal (the orthogonal
+    iteration's Gram-Schmidt, up to the phase factor, which keeps both);
+    maps below the crop are zero; with -I the kept maps have l1 norm
+    sqrt(C) over the coils."""
+    from bart_b200 import synth
+    from bart_b200.espirit import EcalibConf, ecalib
+    rng = np.random.default_rng(256)
+    N, C = 256, 32
+    k = synth.cartesian_ksp(synth.ellipse_phantom(N, 20, rng), synth.coil_maps(N, C, rng), rng, 40.0, 24, 2)
+    s, e, _ = ecalib(k, EcalibConf(maps=2, crop=0.3))
+    s = s.reshape(N * N, C, 2, order="F")
+    e = np.abs(e.reshape(N * N, 2, order="F"))
+    nrm = np.linalg.norm(s, axis=1)
+    kept = e >= 0.3
+    assert kept[:, 0].mean() > 0.3 and kept[:, 1].any()
+    assert np.max(np.abs(nrm[kept] - 1.0)) < 1e-5
+    assert np.max(nrm[~kept]) == 0.0
+    both = kept[:, 0] & kept[:, 1]
+    ip = np.abs(np.sum(np.conj(s[both, :, 0]) * s[both, :, 1], axis=1))
+    assert np.max(ip) < 1e-5
+    s1, e1, _ = ecalib(k, EcalibConf(maps=1, crop=0.3, intensity=True))
+    s1 = s1.reshape(N * N, C, order="F")
+    k1 = np.abs(e1.reshape(N * N, order="F")) >= 0.3
+    l1 = np.sum(np.abs(s1), axis=1)
+    assert np.max(np.abs(l1[k1] - np.sqrt(C))) < 1e-4 * np.sqrt(C)
