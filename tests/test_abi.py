@@ -86,3 +86,29 @@ def test_kb_table_bitwise_library():
         r = np.zeros(n, dtype=np.float64)
         _lib.check(lib.bnufft_rolloff_axis(2.0, 6.0, n, r.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         assert np.array_equal(r.astype(np.float32).view(np.uint32), g[f"roll_{n}"].view(np.uint32)), n
+
+
+def test_ecalib_argument_statuses_without_device():
+    """bnufft_ecalib rejects bad inputs before any device work: options that
+    are not built (2), more than 32 coils (2), more maps than coils (1), a
+    MAPS dimension other than 1 (1), an image side below twice the kernel
+    (1), a missing output (1)."""
+    import numpy as np
+    from bart_b200 import _lib
+    from bart_b200.espirit import EcalibConf
+    lib = _lib.load()
+    buf = np.zeros(16, dtype=np.complex64)
+    p = ctypes.c_void_p(buf.ctypes.data)
+
+    def status(dims, conf, sens=p):
+        d = _lib.dims_array(list(dims) + [1] * (16 - len(dims)))
+        return lib.bnufft_ecalib(ctypes.byref(conf.to_c()), 16, d, p, sens, None, None, None, None, None)
+
+    assert status([64, 64, 1, 8], EcalibConf(weighting=True)) == 2
+    assert status([64, 64, 1, 8], EcalibConf(crop=-1.0)) == 2
+    assert status([64, 64, 1, 33], EcalibConf()) == 2
+    assert status([64, 64, 1, 2], EcalibConf(maps=3)) == 1
+    assert status([64, 64, 1, 8, 2], EcalibConf()) == 1
+    assert status([10, 64, 1, 8], EcalibConf()) == 1
+    assert status([64, 64, 1, 8], EcalibConf(), sens=None) == 1
+    assert "maps" in lib.bnufft_last_error().decode() or "arguments" in lib.bnufft_last_error().decode()
