@@ -112,3 +112,34 @@ def test_ecalib_argument_statuses_without_device():
     assert status([10, 64, 1, 8], EcalibConf()) == 1
     assert status([64, 64, 1, 8], EcalibConf(), sens=None) == 1
     assert "maps" in lib.bnufft_last_error().decode() or "arguments" in lib.bnufft_last_error().decode()
+
+
+def test_calib_and_cg_argument_statuses_without_device():
+    """bnufft_calib / bnufft_calone / bnufft_cg_* report bad arguments as
+    status 1 before touching the device."""
+    import numpy as np
+    from bart_b200 import _lib
+    from bart_b200.espirit import EcalibConf
+    lib = _lib.load()
+    buf = np.zeros(16, dtype=np.complex64)
+    p = ctypes.c_void_p(buf.ctypes.data)
+    c = EcalibConf().to_c()
+
+    def d16(dims):
+        return _lib.dims_array(list(dims) + [1] * (16 - len(dims)))
+
+    # output coils differ from the calibration data's
+    assert lib.bnufft_calib(ctypes.byref(c), 16, d16([64, 64, 1, 4, 2]), p, None, 0, None, d16([24, 24, 1, 8]), p,
+                            None) == 1
+    # calibration region smaller than the kernel
+    assert lib.bnufft_calib(ctypes.byref(c), 16, d16([64, 64, 1, 8, 2]), p, None, 0, None, d16([4, 24, 1, 8]), p,
+                            None) == 1
+    # too few singular-value slots for the 6x6x8-column calibration matrix
+    assert lib.bnufft_calib(ctypes.byref(c), 16, d16([64, 64, 1, 8, 2]), p, None, 5,
+                            (ctypes.c_float * 5)(), d16([24, 24, 1, 8]), p, None) == 1
+    assert lib.bnufft_calone(ctypes.byref(c), 16, d16([64, 64, 1, 8]), p, None, None, None, None, None) == 1
+    h = ctypes.c_void_p()
+    assert lib.bnufft_cg_create(ctypes.byref(h), 0, 0.01, 0.0, 0, None) == 1
+    assert lib.bnufft_cg_create(ctypes.byref(h), 16, -1.0, 0.0, 0, None) == 1
+    assert lib.bnufft_cg_update(None, p, p, p, p, None) == 1
+    assert lib.bnufft_cg_status(None, None, None, None, None) == 1
