@@ -24,6 +24,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <thread>
 #include <type_traits>
 
 #include "../../include/bespirit.h"
@@ -748,19 +749,27 @@ static int ec_heevd(int n, float2* A, float* w, cudaStream_t st)
 	const EcSolver* api = nullptr;
 	TRY(ec_solver(&api));
 
-	// one handle per device for the life of the process (creating one per
-	// call costs more than a small decomposition); calls are serialised
+	// one handle per device and host thread for the life of the process
+	// (creating one per call costs more than a small decomposition):
+	// calibrations on several threads, each on its own stream, run their
+	// decompositions concurrently
 	static std::mutex hmu;
-	static std::map<int, cusolverDnHandle_t> handles;
-	std::lock_guard<std::mutex> lock(hmu);
+	static std::map<std::pair<int, std::thread::id>, cusolverDnHandle_t> handles;
 	int dev = 0;
 	CUDA_TRY(cudaGetDevice(&dev));
-	cusolverDnHandle_t& h = handles[dev];
+	cusolverDnHandle_t h = nullptr;
 
-	if (nullptr == h && CUSOLVER_STATUS_SUCCESS != api->create(&h)) {
+	{
+		std::lock_guard<std::mutex> lock(hmu);
+		cusolverDnHandle_t& slot = handles[std::make_pair(dev, std::this_thread::get_id())];
 
-		h = nullptr;
-		return fail(BNUFFT_ERR_CUDA, "ecalib: cusolverDnCreate failed");
+		if (nullptr == slot && CUSOLVER_STATUS_SUCCESS != api->create(&slot)) {
+
+			slot = nullptr;
+			return fail(BNUFFT_ERR_CUDA, "ecalib: cusolverDnCreate failed");
+		}
+
+		h = slot;
 	}
 
 	int status = BNUFFT_OK;

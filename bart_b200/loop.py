@@ -176,12 +176,17 @@ def stream_pics(flags: int, a) -> np.ndarray:
     return out
 
 
-def loop_ecalib(flags: int, ksp: np.ndarray, conf, emaps: bool = True):
+def loop_ecalib(flags: int, ksp: np.ndarray, conf, emaps: bool = True, workers: int = 4):
     """``bart -l flags ecalib ...``: one calibration per index of the
     flagged dims (which must lie outside the k-space's own dims 0-4), the
-    maps and eigenvalue maps joined along them. The calibrations run one
-    after another (each is a few milliseconds of GPU work with three host
-    synchronisations). Returns (maps, emaps or None)."""
+    maps and eigenvalue maps joined along them. Up to ``workers``
+    calibrations run at once, each on a host thread with its own CUDA
+    stream (a calibration is a few milliseconds of mostly latency-bound GPU
+    work with three host synchronisations, so several overlap well); the
+    results are those of one calibration after another. Returns (maps,
+    emaps or None)."""
+    import ctypes
+    from concurrent.futures import ThreadPoolExecutor
     from .espirit import ecalib, output_dims
 
     dims = loop_dims(flags)
@@ -197,9 +202,30 @@ def loop_ecalib(flags: int, ksp: np.ndarray, conf, emaps: bool = True):
         ed[d] = n
     sens = np.zeros(sd, dtype=np.complex64, order="F")
     ev = np.zeros(ed, dtype=np.complex64, order="F") if emaps else None
-    for idx in loop_indices(sizes):
+    import torch
+    idxs = loop_indices(sizes)
+    nw = max(1, min(int(workers), len(idxs)))
+    streams = {}
+    own_streams = nw > 1 and torch.cuda.is_available()
+
+    def calibrate(idx):
+        import threading
+        stream = None
+        if own_streams:
+            t = threading.get_ident()
+            if t not in streams:
+                streams[t] = torch.cuda.Stream()
+            stream = ctypes.c_void_p(streams[t].cuda_stream)
         k = slice_at(ksp, dims, idx)
-        s, e, _ = ecalib(k.reshape(one, order="F"), conf, emaps=emaps)
+        s, e, _ = ecalib(k.reshape(one, order="F"), conf, emaps=emaps, stream=stream)
+        return idx, s, e
+
+    if nw == 1:
+        results = [calibrate(idx) for idx in idxs]
+    else:
+        with ThreadPoolExecutor(max_workers=nw) as pool:
+            results = list(pool.map(calibrate, idxs))
+    for idx, s, e in results:
         place_at(sens, dims, idx, s)
         if emaps:
             place_at(ev, dims, idx, e)

@@ -267,7 +267,7 @@ def run_normal3d(dev, steps, warmup, coils=8, N=128, spokes=2000):
             "hbm_peak_gbs": peak, "peak_source": peak_src, "passes": passes}
 
 
-def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True, ndim=2):
+def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True, ndim=2, slices=0):
     """ESPIRiT calibration with the reference's ecalib defaults (6 x 6
     kernel, calibration region up to 24 x 24, threshold 0.001, 2 maps, 30
     orthogonal iterations, crop 0.8) of 2D Cartesian k-space: N x N, `coils`
@@ -350,6 +350,21 @@ def run_ecalib(dev, steps, warmup, N=256, coils=16, cpu_base=True, ndim=2):
                              "fp32_frac": flop / (px_ms * 1e-3) / 1e12 / FP32_PEAK_TFLOPS if px_ms > 0 else None,
                              "hbm_bytes": out_bytes + t_bytes},
            "clocks": clk.summary()}
+    if slices > 0:
+        # bart -l 8192 ecalib over `slices` slices (the k-space scaled per
+        # slice): one worker (one calibration after another) against four
+        # (threads with their own streams), host arrays in and out
+        from bart_b200.espirit import EcalibConf
+        from bart_b200.loop import loop_ecalib
+        ks = np.concatenate([(k * np.complex64(1.0 + 0.1 * i)).reshape(list(k.shape) + [1] * (13 - k.ndim) + [1])
+                             for i in range(slices)], axis=13)
+        res["slice_loop"] = {"slices": slices}
+        for w in (1, 4):
+            loop_ecalib(8192, ks[..., :2], EcalibConf(), workers=w)
+            t0 = time.perf_counter()
+            loop_ecalib(8192, ks, EcalibConf(), workers=w)
+            dt = time.perf_counter() - t0
+            res["slice_loop"][f"workers{w}_ms_per_slice"] = dt / slices * 1e3
     exe = os.path.join(ROOT, "oracle", "_ref", "bin", "ecalib")
     if cpu_base and os.path.exists(exe):
         from bart_b200.cfl import writecfl
@@ -933,6 +948,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="cgsense2d", choices=["cgsense2d", "nufft3d", "normal3d", "batch", "scatter", "ecalib"])
     ap.add_argument("--coils", type=int, default=None, help="normal3d (default 8) / ecalib (default 16): coils")
+    ap.add_argument("--slices", type=int, default=0,
+                    help="ecalib: also time the bart -l slice loop over this many slices, 1 and 4 workers")
     ap.add_argument("--ndim", type=int, default=None, choices=[2, 3],
                     help="ecalib: 2 (256^2, 16 coils) or 3 (128^3, 8 coils)")
     ap.add_argument("--analysis", action="store_true",
@@ -983,7 +1000,7 @@ def main():
             nd = args.ndim or 2
             print(json.dumps(run_ecalib(dev, args.steps, args.warmup, N=256 if nd == 2 else 128,
                                         coils=args.coils or (16 if nd == 2 else 8), ndim=nd,
-                                        cpu_base=not args.no_cpu_baseline)), flush=True)
+                                        cpu_base=not args.no_cpu_baseline, slices=args.slices)), flush=True)
         return
 
     if args.workload == "scatter":

@@ -65,9 +65,10 @@ int bnufft_ecalib_dims(const struct bnufft_ecalib_conf* conf, int N, const long 
  * the maps' global sign follows the convention that the first principal
  * coil component's last entry is real and positive (the reference takes
  * that sign from its LAPACK). The calibration matrix's eigen-decomposition
- * runs in cuSOLVER (loaded on first use, one handle per device kept for the
- * life of the process: concurrent calibrations on one device take turns for
- * that step); everything else in the library's own kernels. Temporaries
+ * runs in cuSOLVER (loaded on first use, one handle per device and host
+ * thread kept for the life of the process: calibrations on several threads,
+ * each on its own stream, run concurrently); everything else in the
+ * library's own kernels. Temporaries
  * come from a stream-ordered memory pool of the calibration's own, which
  * keeps its memory between calls. */
 int bnufft_ecalib(const struct bnufft_ecalib_conf* conf, int N, const long ksp_dims[], const void* ksp,
