@@ -288,6 +288,10 @@ def main_ecalib(argv, loop_flags: int = 0) -> int:
         conf.weighting = True
     if a.weighting:
         conf.weighting = True
+    # under torchrun the slices are not split over the ranks: rank 0 alone
+    # calibrates and writes the outputs, the others exit without work
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
     ksp = readcfl(a.kspace)
     if loop_flags:
         if a.one:

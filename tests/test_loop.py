@@ -134,3 +134,14 @@ def test_ecalib_loop_rejects_inner_dims():
     from bart_b200.loop import loop_ecalib
     with pytest.raises(ValueError):
         loop_ecalib(1 << 3, np.zeros((8, 8, 1, 2), dtype=np.complex64), EcalibConf())
+
+
+def test_ecalib_under_torchrun_runs_on_rank_0_only(tmp_path, monkeypatch):
+    """Launched with several ranks, ecalib does not split its work: ranks
+    other than 0 exit without reading or writing anything."""
+    d = str(tmp_path)
+    monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    assert 0 == cli.main(["ecalib", d + "/missing", d + "/s"])
+    import os
+    assert not os.path.exists(d + "/s.cfl")
